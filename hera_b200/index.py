@@ -1,0 +1,180 @@
+"""hera's k-mer hash index: build, read and write it in the reference layout.
+
+The reference index (src/hash_align.c:1060-1159, loaded at :1169-1234) is a
+direct-mapped table of H = 2^27 buckets.  The bucket of a 31-mer id is its
+low 27 bits; each bucket is an array of ``Bucket{u64 id; u32 start, end}``
+sorted by id, and ``[start, end)`` indexes two parallel occurrence arrays
+``pos`` (transcript id) and ``p`` (offset of the k-mer's last base).
+
+Layout facts that fix parity:
+
+* index k-mers mask N to A (``ascii_table[c] & 3``, src/hash_align.c:1082);
+* buckets are laid out in (bucket, id) order and occurrence lists follow that
+  order, each list in (transcript, offset) order (src/hash_align.c:1070-1095);
+* the file is ``n, name_len, len[n], find[n], names, seq, n_bucket[H],
+  buckets, n_pos, pos[n_pos], p[n_pos]`` (src/hash_align.c:1130-1159).
+
+``build_index`` reproduces that layout from a ``Transcriptome`` (a stable
+sort of every occurrence by (bucket, id)), byte-identical to ``hera index``.
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import List, Optional
+
+import numpy as np
+
+KMER = 31
+HBITS = 27
+H = 1 << HBITS
+BUCKET_DTYPE = np.dtype([("id", "<u8"), ("start", "<u4"), ("end", "<u4")])
+
+_CODE = np.full(256, 4, dtype=np.uint8)
+for _i, _c in enumerate(b"ACGT"):
+    _CODE[_c] = _i
+    _CODE[_c + 32] = _i
+
+
+@dataclasses.dataclass
+class HeraIndex:
+    n_trans: int
+    name_len: int
+    names: bytes                 # n_trans * name_len, NUL padded
+    length: np.ndarray           # uint32
+    find: np.ndarray             # uint32 exclusive end offsets
+    seq: np.ndarray              # uint8 ASCII, find[-1] bytes
+    bucket_n: np.ndarray         # uint32[H] entries per bucket
+    buckets: np.ndarray          # BUCKET_DTYPE
+    pos: np.ndarray              # uint32
+    p: np.ndarray                # uint32
+
+    @property
+    def n_pos(self) -> int:
+        return int(self.pos.shape[0])
+
+    def bucket_off(self) -> np.ndarray:
+        off = np.zeros(H + 1, dtype=np.uint64)
+        np.cumsum(self.bucket_n, dtype=np.uint64, out=off[1:])
+        return off
+
+    def seq_padded(self, pad: int = 64) -> np.ndarray:
+        """Transcript bytes followed by `pad` zero bytes (the suffix DP window
+        may run up to 7 bytes past the last transcript)."""
+        out = np.zeros(self.seq.shape[0] + pad, dtype=np.uint8)
+        out[:self.seq.shape[0]] = self.seq
+        return out
+
+    def transcript_name(self, i: int) -> str:
+        raw = self.names[i * self.name_len:(i + 1) * self.name_len]
+        return raw.split(b"\0", 1)[0].decode()
+
+
+def _kmer_ids(codes: np.ndarray) -> np.ndarray:
+    """id[k] of the 31-mer ending at k (valid for k >= 30), by doubling:
+    1+2+4+8+16 = 31 characters combined from shifted windows."""
+    c = codes.astype(np.uint64)
+    n = c.shape[0]
+
+    def shifted(a, k):
+        out = np.zeros_like(a)
+        if k < n:
+            out[k:] = a[:n - k]
+        return out
+
+    w1 = c
+    w2 = (shifted(w1, 1) << np.uint64(2)) | w1
+    w4 = (shifted(w2, 2) << np.uint64(4)) | w2
+    w8 = (shifted(w4, 4) << np.uint64(8)) | w4
+    w16 = (shifted(w8, 8) << np.uint64(16)) | w8
+    return ((shifted(w16, 15) << np.uint64(30)) | (shifted(w8, 7) << np.uint64(14)) |
+            (shifted(w4, 3) << np.uint64(6)) | (shifted(w2, 1) << np.uint64(2)) | w1)
+
+
+def _occurrences(seq: np.ndarray, length: np.ndarray, find: np.ndarray):
+    """All (id, transcript, offset) triples in (transcript, offset) order."""
+    codes = _CODE[seq] & np.uint8(3)
+    ids = _kmer_ids(codes)
+    starts = find.astype(np.int64) - length.astype(np.int64)
+    tid = np.repeat(np.arange(length.shape[0], dtype=np.uint32), length.astype(np.int64))
+    off = (np.arange(seq.shape[0], dtype=np.int64) - np.repeat(starts, length.astype(np.int64)))
+    keep = off >= KMER - 1
+    return ids[keep], tid[keep], off[keep].astype(np.uint32)
+
+
+def _stable_order(composite: np.ndarray, device: Optional[str]) -> np.ndarray:
+    if device is not None and device.startswith("cuda"):
+        import torch
+        t = torch.from_numpy(composite.view(np.int64)).to(device)
+        _, order = torch.sort(t, stable=True)
+        return order.cpu().numpy()
+    return np.argsort(composite, kind="stable")
+
+
+def build_index(tx, device: Optional[str] = None) -> HeraIndex:
+    """Index a Transcriptome exactly as ``hera index`` would
+    (get_ref_seq + construct_hash, src/hash_align.c:1060-1128).
+    `device="cuda"` sorts on the GPU (same result, faster at large sizes)."""
+    ids, tid, off = _occurrences(tx.seq, tx.length, tx.find)
+    mask = np.uint64(H - 1)
+    # (bucket, id) order as one 62-bit key: bucket in the high 27 bits
+    composite = ((ids & mask) << np.uint64(62 - HBITS)) | (ids >> np.uint64(HBITS))
+    order = _stable_order(composite, device)
+    sc = composite[order]
+    pos = tid[order]
+    p = off[order]
+    del composite, ids
+    if sc.shape[0]:
+        brk = np.empty(sc.shape[0], dtype=bool)
+        brk[0] = True
+        np.not_equal(sc[1:], sc[:-1], out=brk[1:])
+        first = np.nonzero(brk)[0]
+    else:
+        first = np.zeros(0, dtype=np.int64)
+    uk = sc[first]
+    counts = np.diff(np.append(first, sc.shape[0])).astype(np.uint32)
+    uid = ((uk & np.uint64((1 << (62 - HBITS)) - 1)) << np.uint64(HBITS)) | (uk >> np.uint64(62 - HBITS))
+    buckets = np.empty(uk.shape[0], dtype=BUCKET_DTYPE)
+    buckets["id"] = uid
+    buckets["start"] = first.astype(np.uint32)
+    buckets["end"] = (first + counts).astype(np.uint32)
+    bucket_n = np.bincount((uid & mask).astype(np.int64), minlength=H).astype(np.uint32)
+    names = [n.encode() for n in tx.names]
+    name_len = max(len(n) for n in names) + 1
+    nb = b"".join(n + b"\0" * (name_len - len(n)) for n in names)
+    return HeraIndex(len(names), name_len, nb, tx.length.astype(np.uint32),
+                     tx.find.astype(np.uint32), tx.seq.astype(np.uint8),
+                     bucket_n, buckets, pos.astype(np.uint32), p.astype(np.uint32))
+
+
+def write_index(ix: HeraIndex, path: str) -> None:
+    """Write the reference's index file (src/hash_align.c:1130-1159)."""
+    with open(path, "wb") as f:
+        f.write(np.array([ix.n_trans, ix.name_len], dtype=np.uint32).tobytes())
+        f.write(ix.length.astype(np.uint32).tobytes())
+        f.write(ix.find.astype(np.uint32).tobytes())
+        f.write(ix.names)
+        f.write(ix.seq.tobytes())
+        f.write(ix.bucket_n.astype(np.uint32).tobytes())
+        f.write(ix.buckets.tobytes())
+        f.write(np.array([ix.n_pos], dtype=np.uint32).tobytes())
+        f.write(ix.pos.astype(np.uint32).tobytes())
+        f.write(ix.p.astype(np.uint32).tobytes())
+
+
+def read_index(path: str) -> HeraIndex:
+    """Read the reference's index file (src/hash_align.c:1195-1234)."""
+    with open(path, "rb") as f:
+        n, name_len = np.frombuffer(f.read(8), dtype=np.uint32)
+        n, name_len = int(n), int(name_len)
+        length = np.frombuffer(f.read(4 * n), dtype=np.uint32).copy()
+        find = np.frombuffer(f.read(4 * n), dtype=np.uint32).copy()
+        names = f.read(n * name_len)
+        seq = np.frombuffer(f.read(int(find[-1])), dtype=np.uint8).copy()
+        bucket_n = np.frombuffer(f.read(4 * H), dtype=np.uint32).copy()
+        nb = int(bucket_n.sum(dtype=np.uint64))
+        buckets = np.frombuffer(f.read(16 * nb), dtype=BUCKET_DTYPE).copy()
+        n_pos = int(np.frombuffer(f.read(4), dtype=np.uint32)[0])
+        pos = np.frombuffer(f.read(4 * n_pos), dtype=np.uint32).copy()
+        p = np.frombuffer(f.read(4 * n_pos), dtype=np.uint32).copy()
+    return HeraIndex(n, name_len, names, length, find, seq, bucket_n, buckets, pos, p)

@@ -1,0 +1,124 @@
+/*
+ * hera_oracle.h -- CPU restatement of hera's transcriptome read-alignment
+ * hot path (k-mer seeding, anchor chaining, SW_align gap fill, ssw_align mate
+ * rescue, pairing).  TEST INFRASTRUCTURE ONLY: the parity checker for the
+ * CUDA path.  Nothing in the hera_b200 product links, loads or calls this.
+ *
+ * Parity of this restatement is pinned against the reference program itself
+ * (compiled from its own sources into oracle/_ref by oracle/Makefile) through
+ * golden vectors committed under tests/golden/ and live comparisons in the
+ * CPU test suite.
+ *
+ * All structures here are the oracle's own; the result record layout matches
+ * the product's `hera_cand_rec` field for field so tests can compare them.
+ */
+#ifndef HERA_ORACLE_H
+#define HERA_ORACLE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HO_KMER 31
+#define HO_ERR 7
+#define HO_MAX_FRAG 1000
+#define HO_HBITS 27
+
+/* One bucket entry, identical in size and order to the reference's Bucket
+ * (src/hash_align.h:138-142): 64-bit k-mer id, [start, end) into pos/p. */
+typedef struct {
+	uint64_t id;
+	uint32_t start;
+	uint32_t end;
+} ho_bucket;
+
+/* Read-only view of a loaded index (src/hash_align.c:1195-1234 layout,
+ * with the per-bucket counts n[] replaced by their prefix sums). */
+typedef struct {
+	uint32_t n_trans;
+	const uint32_t *len;        /* transcript lengths */
+	const uint32_t *find;       /* exclusive end offset of each transcript in seq */
+	const char *seq;            /* concatenated transcripts, >= 8 zero bytes after */
+	const uint64_t *bucket_off; /* (1<<27)+1 prefix sums of bucket sizes */
+	const ho_bucket *buckets;
+	const uint32_t *pos;        /* occurrence transcript ids */
+	const uint32_t *p;          /* occurrence offsets (last base of the k-mer) */
+} ho_index;
+
+/* Flat result record: one per Candidate (two per read pair, one per single
+ * read).  Lists live in pools at list_off; CIGAR ops are (count << 4) | op. */
+typedef struct {
+	int32_t n[2];
+	int32_t err[2];
+	int32_t pair;
+	uint32_t list_off[2];
+	uint32_t cig_off[2];
+	uint32_t miss_off[2];
+	uint16_t n_cigar[2];
+	uint16_t n_miss[2];
+} ho_rec;
+
+typedef struct {
+	ho_rec *recs;
+	uint32_t *pos_pool;
+	int32_t *p_pool;
+	uint32_t *op_pool;
+	char *miss_pool;
+	uint64_t list_cap, op_cap, miss_cap;   /* pool capacities (entries) */
+	uint64_t list_used, op_used, miss_used;
+} ho_result;
+
+/* Batch of reads: read i is seq[off[i] .. off[i]+len[i]). */
+typedef struct {
+	const char *seq;
+	const int64_t *off;
+	const int32_t *len;
+} ho_reads;
+
+/* Front half of align_pair_read (src/hash_align.c:1724-1733) per pair:
+ * check_in_transcriptome then the two intersect2 calls.  write_bam carries
+ * the reference's WRITE_BAM global (1 = score-only DP, the no `-w` mode).
+ * Returns 0, or -1 when a result pool is too small (nothing is partial:
+ * the caller retries with larger pools).  `reads1`/`reads2` are modified
+ * exactly as the reference modifies read->seq (lower-case ACGT upper-cased). */
+int ho_align_pairs(const ho_index *ix, int write_bam, int n,
+		   char *seq1, const int64_t *off1, const int32_t *len1,
+		   char *seq2, const int64_t *off2, const int32_t *len2,
+		   ho_result *out);
+
+/* Front half of align_single_read (src/hash_align.c:1819-1823). */
+int ho_align_single(const ho_index *ix, int write_bam, int n,
+		    char *seq, const int64_t *off, const int32_t *len,
+		    ho_result *out);
+
+/* Unit entry points (one call of the reference function each). */
+int ho_sw_align(const char *ref, uint32_t rstart, const char *q,
+		uint32_t ref_len, uint32_t len, int err, int write_bam,
+		uint32_t *ops, int *n_ops, char *miss, int *n_miss, int cap);
+int ho_ssw_align(const char *ref, int32_t ref_len, const char *read,
+		 int32_t read_len, int *skip,
+		 uint32_t *ops, int *n_ops, char *miss, int *n_miss, int cap);
+uint64_t ho_get_index(const char *seq, uint32_t start);
+uint32_t ho_hash_get(const ho_index *ix, uint64_t id, uint32_t *found);
+
+/* Counters of the algorithmic work done by the last ho_align_* call. */
+typedef struct {
+	uint64_t lookups, hits, probes, occurrences;
+	uint64_t sw_calls, sw_cells, ssw_calls, ssw_cells;
+} ho_stats;
+void ho_get_stats(ho_stats *s);
+
+/* Multi-threaded timing entry: same as ho_align_pairs but splits pairs over
+ * nthreads and discards results (used only for the CPU baseline leg). */
+int ho_align_pairs_mt(const ho_index *ix, int write_bam, int n,
+		      char *seq1, const int64_t *off1, const int32_t *len1,
+		      char *seq2, const int64_t *off2, const int32_t *len2,
+		      int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

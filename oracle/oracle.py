@@ -1,0 +1,264 @@
+"""ctypes bindings to the test-side checkers built by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the hera_b200 product.
+
+* ``Oracle``    -- oracle/_ref/libhera_oracle.so, the C restatement
+                   (hera_oracle.c) of the reference's hot path;
+* ``Reference`` -- oracle/_ref/libhera_ref.so, the reference's own sources
+                   plus ref_harness.c (only where the reference was built).
+
+Both return results as ``Result`` objects holding the flat record arrays
+(the same layout the product returns), which ``canonical()`` turns into
+plain tuples for comparison.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(REF_DIR, "libhera_oracle.so")
+REFERENCE_SO = os.path.join(REF_DIR, "libhera_ref.so")
+REFERENCE_BIN = os.path.join(REF_DIR, "hera")
+
+REC_DTYPE = np.dtype([
+    ("n", "<i4", (2,)), ("err", "<i4", (2,)), ("pair", "<i4"),
+    ("list_off", "<u4", (2,)), ("cig_off", "<u4", (2,)), ("miss_off", "<u4", (2,)),
+    ("n_cigar", "<u2", (2,)), ("n_miss", "<u2", (2,)),
+])
+assert REC_DTYPE.itemsize == 52
+
+CIGAR_CHARS = "MIDNSHP=XB"
+
+
+class _Index(C.Structure):
+    _fields_ = [("n_trans", C.c_uint32), ("len", C.c_void_p), ("find", C.c_void_p),
+                ("seq", C.c_void_p), ("bucket_off", C.c_void_p), ("buckets", C.c_void_p),
+                ("pos", C.c_void_p), ("p", C.c_void_p)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("recs", C.c_void_p), ("pos_pool", C.c_void_p), ("p_pool", C.c_void_p),
+                ("op_pool", C.c_void_p), ("miss_pool", C.c_void_p),
+                ("list_cap", C.c_uint64), ("op_cap", C.c_uint64), ("miss_cap", C.c_uint64),
+                ("list_used", C.c_uint64), ("op_used", C.c_uint64), ("miss_used", C.c_uint64)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("lookups", "hits", "probes", "occurrences",
+                                           "sw_calls", "sw_cells", "ssw_calls", "ssw_cells")]
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Result:
+    """Flat candidate records plus pools (one record per Candidate)."""
+
+    def __init__(self, n_recs: int, list_cap: int, op_cap: int, miss_cap: int):
+        self.recs = np.zeros(n_recs, dtype=REC_DTYPE)
+        self.pos_pool = np.zeros(max(list_cap, 1), np.uint32)
+        self.p_pool = np.zeros(max(list_cap, 1), np.int32)
+        self.op_pool = np.zeros(max(op_cap, 1), np.uint32)
+        self.miss_pool = np.zeros(max(miss_cap, 1), np.uint8)
+        self.c = _Result(_ptr(self.recs), _ptr(self.pos_pool), _ptr(self.p_pool),
+                         _ptr(self.op_pool), _ptr(self.miss_pool),
+                         list_cap, op_cap, miss_cap, 0, 0, 0)
+
+    def candidate(self, i: int):
+        """(pair, [(n, err, pos list, p list, cigar string, miss bytes)] x 2)."""
+        r = self.recs[i]
+        out = []
+        for s in range(2):
+            n = int(r["n"][s])
+            lo = int(r["list_off"][s])
+            co, nc = int(r["cig_off"][s]), int(r["n_cigar"][s])
+            mo, nm = int(r["miss_off"][s]), int(r["n_miss"][s])
+            ops = self.op_pool[co:co + nc]
+            cig = "".join(f"{int(o) >> 4}{CIGAR_CHARS[int(o) & 15]}" for o in ops)
+            out.append((n, int(r["err"][s]), tuple(self.pos_pool[lo:lo + n].tolist()),
+                        tuple(self.p_pool[lo:lo + n].tolist()), cig,
+                        bytes(self.miss_pool[mo:mo + nm])))
+        return (int(r["pair"]), tuple(out))
+
+    def canonical(self) -> List[tuple]:
+        return [self.candidate(i) for i in range(self.recs.shape[0])]
+
+
+def _pool_caps(n_recs: int, total_len: int):
+    return n_recs * 64 + 1024, n_recs * 16 + total_len * 2 + 1024, total_len * 2 + 1024
+
+
+class Oracle:
+    """The C restatement (oracle/hera_oracle.c) bound to one index."""
+
+    def __init__(self, ix, so_path: str = ORACLE_SO):
+        self.lib = C.CDLL(so_path)
+        self.ix = ix
+        self._seq = ix.seq_padded()
+        self._boff = ix.bucket_off()
+        self._buckets = np.ascontiguousarray(ix.buckets)
+        self._len = np.ascontiguousarray(ix.length, dtype=np.uint32)
+        self._find = np.ascontiguousarray(ix.find, dtype=np.uint32)
+        self._pos = np.ascontiguousarray(ix.pos, dtype=np.uint32)
+        self._p = np.ascontiguousarray(ix.p, dtype=np.uint32)
+        self.cix = _Index(ix.n_trans, _ptr(self._len), _ptr(self._find), _ptr(self._seq),
+                          _ptr(self._boff), _ptr(self._buckets), _ptr(self._pos), _ptr(self._p))
+        L = self.lib
+        L.ho_align_pairs.restype = C.c_int
+        L.ho_align_single.restype = C.c_int
+        L.ho_sw_align.restype = C.c_int
+        L.ho_ssw_align.restype = C.c_int
+        L.ho_get_index.restype = C.c_uint64
+        L.ho_hash_get.restype = C.c_uint32
+
+    def align_pairs(self, r1, r2, write_bam: int = 1) -> Result:
+        """Front half of align_pair_read for every pair.  r1/r2 are
+        synth.ReadSet objects; their sequences are modified in place exactly
+        as the reference modifies them (lower-case ACGT become upper-case)."""
+        n = r1.n
+        res = Result(2 * n, *_pool_caps(2 * n, int(r1.len.sum() + r2.len.sum())))
+        rc = self.lib.ho_align_pairs(C.byref(self.cix), write_bam, n,
+                                     C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+                                     C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+                                     C.byref(res.c))
+        if rc != 0:
+            raise RuntimeError("oracle result pools too small")
+        return res
+
+    def align_single(self, rs, write_bam: int = 1) -> Result:
+        n = rs.n
+        res = Result(n, *_pool_caps(n, int(rs.len.sum())))
+        rc = self.lib.ho_align_single(C.byref(self.cix), write_bam, n,
+                                      C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
+                                      C.byref(res.c))
+        if rc != 0:
+            raise RuntimeError("oracle result pools too small")
+        return res
+
+    def align_pairs_mt(self, r1, r2, write_bam: int, nthreads: int) -> None:
+        self.lib.ho_align_pairs_mt(C.byref(self.cix), write_bam, r1.n,
+                                   C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+                                   C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+                                   nthreads)
+
+    def stats(self) -> dict:
+        s = _Stats()
+        self.lib.ho_get_stats(C.byref(s))
+        return {k: getattr(s, k) for k, _ in _Stats._fields_}
+
+    def sw_align(self, ref: bytes, rstart: int, q: bytes, ref_len: int, qlen: int, err: int,
+                 write_bam: int = 0):
+        return _unit_sw(self.lib.ho_sw_align, None, ref, rstart, q, ref_len, qlen, err, write_bam)
+
+    def ssw_align(self, ref: bytes, read: bytes):
+        return _unit_ssw(self.lib.ho_ssw_align, ref, read)
+
+    def get_index(self, seq: bytes, start: int) -> int:
+        b = np.frombuffer(seq, dtype=np.uint8).copy()
+        return int(self.lib.ho_get_index(C.c_void_p(_ptr(b)), start))
+
+
+def _unit_sw(fn, write_bam_first, ref, rstart, q, ref_len, qlen, err, write_bam):
+    cap = 4096
+    rb = np.frombuffer(ref + b"\0" * 64, dtype=np.uint8).copy()
+    qb = np.frombuffer(q + b"\0", dtype=np.uint8).copy()
+    ops = np.zeros(cap, np.uint32)
+    miss = np.zeros(cap, np.uint8)
+    n_ops, n_miss = C.c_int(0), C.c_int(0)
+    if write_bam_first is None:
+        score = fn(C.c_void_p(_ptr(rb)), C.c_uint32(rstart), C.c_void_p(_ptr(qb)), C.c_uint32(ref_len),
+                   C.c_uint32(qlen), C.c_int(err), C.c_int(write_bam), C.c_void_p(_ptr(ops)),
+                   C.byref(n_ops), C.c_void_p(_ptr(miss)), C.byref(n_miss), C.c_int(cap))
+    else:
+        score = fn(C.c_int(write_bam), C.c_void_p(_ptr(rb)), C.c_uint32(rstart), C.c_void_p(_ptr(qb)),
+                   C.c_uint32(ref_len), C.c_uint32(qlen), C.c_int(err), C.c_void_p(_ptr(ops)),
+                   C.byref(n_ops), C.c_void_p(_ptr(miss)), C.byref(n_miss), C.c_int(cap))
+    cig = "".join(f"{int(o) >> 4}{CIGAR_CHARS[int(o) & 15]}" for o in ops[:n_ops.value])
+    return score, cig, bytes(miss[:n_miss.value])
+
+
+def _unit_ssw(fn, ref, read):
+    cap = 8192
+    rb = np.frombuffer(ref + b"\0" * 8, dtype=np.uint8).copy()
+    qb = np.frombuffer(read + b"\0", dtype=np.uint8).copy()
+    ops = np.zeros(cap, np.uint32)
+    miss = np.zeros(cap, np.uint8)
+    n_ops, n_miss, skip = C.c_int(0), C.c_int(0), C.c_int(0)
+    score = fn(C.c_void_p(_ptr(rb)), C.c_int32(len(ref)), C.c_void_p(_ptr(qb)), C.c_int32(len(read)),
+               C.byref(skip), C.c_void_p(_ptr(ops)), C.byref(n_ops), C.c_void_p(_ptr(miss)),
+               C.byref(n_miss), C.c_int(cap))
+    cig = "".join(f"{int(o) >> 4}{CIGAR_CHARS[int(o) & 15]}" for o in ops[:n_ops.value])
+    return score, skip.value, cig, bytes(miss[:n_miss.value])
+
+
+def reference_available() -> bool:
+    return os.path.exists(REFERENCE_SO)
+
+
+class Reference:
+    """The reference's own code (oracle/_ref/libhera_ref.so).  The reference
+    keeps its index in process globals, so one index per process."""
+
+    _lib = None
+
+    def __init__(self, ix=None, index_dir: Optional[str] = None):
+        if Reference._lib is None:
+            Reference._lib = C.CDLL(REFERENCE_SO)
+        self.lib = Reference._lib
+        self.lib.refh_sw_align.restype = C.c_int
+        self.lib.refh_ssw_align.restype = C.c_int
+        if index_dir is not None:
+            self.lib.refh_load_index(index_dir.encode())
+        elif ix is not None:
+            self._keep = [ix.seq_padded(), np.ascontiguousarray(ix.length, dtype=np.uint32),
+                          np.ascontiguousarray(ix.find, dtype=np.uint32),
+                          np.ascontiguousarray(ix.bucket_n, dtype=np.uint32),
+                          np.ascontiguousarray(ix.buckets),
+                          np.ascontiguousarray(ix.pos, dtype=np.uint32),
+                          np.ascontiguousarray(ix.p, dtype=np.uint32)]
+            seq, ln, fd, bn, bk, pos, p = self._keep
+            self.lib.refh_set_index(C.c_uint32(ix.n_trans), C.c_uint32(ix.name_len),
+                                    C.c_void_p(_ptr(ln)), C.c_void_p(_ptr(fd)), C.c_void_p(_ptr(seq)),
+                                    C.c_void_p(_ptr(bn)), C.c_void_p(_ptr(bk)), C.c_void_p(_ptr(pos)),
+                                    C.c_void_p(_ptr(p)), C.c_uint32(ix.n_pos))
+
+    def align_pairs(self, r1, r2, write_bam: int = 1) -> Result:
+        n = r1.n
+        res = Result(2 * n, *_pool_caps(2 * n, int(r1.len.sum() + r2.len.sum())))
+        rc = self.lib.refh_align_pairs(write_bam, n,
+                                       C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+                                       C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+                                       C.byref(res.c))
+        if rc != 0:
+            raise RuntimeError("reference result pools too small")
+        return res
+
+    def align_single(self, rs, write_bam: int = 1) -> Result:
+        n = rs.n
+        res = Result(n, *_pool_caps(n, int(rs.len.sum())))
+        rc = self.lib.refh_align_single(write_bam, n,
+                                        C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
+                                        C.byref(res.c))
+        if rc != 0:
+            raise RuntimeError("reference result pools too small")
+        return res
+
+    def align_pairs_mt(self, r1, r2, write_bam: int, nthreads: int) -> None:
+        self.lib.refh_align_pairs_mt(write_bam, r1.n,
+                                     C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+                                     C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+                                     nthreads)
+
+    def sw_align(self, ref: bytes, rstart: int, q: bytes, ref_len: int, qlen: int, err: int,
+                 write_bam: int = 0):
+        return _unit_sw(self.lib.refh_sw_align, True, ref, rstart, q, ref_len, qlen, err, write_bam)
+
+    def ssw_align(self, ref: bytes, read: bytes):
+        return _unit_ssw(self.lib.refh_ssw_align, ref, read)

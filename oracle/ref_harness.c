@@ -1,0 +1,298 @@
+/*
+ * ref_harness.c -- ctypes entry points into the reference program, compiled
+ * together with the reference's own sources into oracle/_ref/libhera_ref.so
+ * by oracle/Makefile.  TEST INFRASTRUCTURE ONLY (golden vectors and the CPU
+ * baseline timing); the product never links or loads it.
+ *
+ * Every alignment result here comes from the reference's functions run
+ * unchanged: check_in_transcriptome + intersect2 (the front half of
+ * align_pair_read, src/hash_align.c:1724-1733), get_position x2 (front half
+ * of align_single_read, src/hash_align.c:1819-1823), SW_align and ssw_align.
+ * This file only sets the reference's globals and flattens its Candidate
+ * structs into the records the tests compare.
+ */
+#include "hash_align.h"
+#include "ssw.h"
+
+#include <stdint.h>
+#include <pthread.h>
+
+/* defined in src/hash_align.c without a header prototype */
+void check_in_transcriptome(struct read_inf *r1, struct read_inf *r2, Candidate *r[]);
+void intersect2(Candidate *r, struct read_inf *read1, struct read_inf *read2, unsigned int add);
+void destroy_candidate(Candidate *read);
+Cigar *ssw_align(char *ref_seq, int32_t ref_len, char *read_seq, int32_t read_len,
+		 int *score, int *skip);
+
+typedef struct {
+	int32_t n[2];
+	int32_t err[2];
+	int32_t pair;
+	uint32_t list_off[2];
+	uint32_t cig_off[2];
+	uint32_t miss_off[2];
+	uint16_t n_cigar[2];
+	uint16_t n_miss[2];
+} refh_rec;
+
+typedef struct {
+	refh_rec *recs;
+	uint32_t *pos_pool;
+	int32_t *p_pool;
+	uint32_t *op_pool;
+	char *miss_pool;
+	uint64_t list_cap, op_cap, miss_cap;
+	uint64_t list_used, op_used, miss_used;
+} refh_result;
+
+/* Load <dir>/index with the reference's own loader (src/hash_align.c:1195). */
+int refh_load_index(const char *dir)
+{
+	init_refInf();
+	init_hash();
+	load_index((char *)dir, NULL);
+	return 0;
+}
+
+/* Install an index held in caller memory into the reference's globals, in
+ * the layout load_hash builds (src/hash_align.c:1169-1193).  `seq` must stay
+ * alive and carry zero bytes after the last transcript.  Arrays are
+ * borrowed, not copied. */
+int refh_set_index(uint32_t n_trans, uint32_t name_len, uint32_t *len,
+		   uint32_t *find, char *seq, uint32_t *bucket_n,
+		   Bucket *buckets, uint32_t *pos, uint32_t *p, uint32_t n_pos)
+{
+	uint64_t i, count = 0;
+
+	REF_INF = calloc(1, sizeof(Ref_inf));
+	REF_INF->n = n_trans;
+	REF_INF->name_len = name_len;
+	REF_INF->len = len;
+	REF_INF->find = find;
+	REF_INF->seq = seq;
+	REF_INF->count = calloc(n_trans, sizeof(int));
+	REF_INF->eff_len = calloc(n_trans, sizeof(double));
+
+	KMER_HASH = calloc(1, sizeof(Kmer_hash));
+	KMER_HASH->n = bucket_n;
+	KMER_HASH->bucket = calloc((uint64_t)H + 1, sizeof(Bucket *));
+	KMER_HASH->sentinel = buckets;
+	for (i = 0; i < H; ++i) {
+		KMER_HASH->bucket[i] = buckets + count;
+		count += bucket_n[i];
+	}
+	KMER_HASH->pos = pos;
+	KMER_HASH->p = p;
+	KMER_HASH->n_pos = n_pos;
+	KMER_HASH->is_loaded = 1;
+	FMINDEX = NULL;
+	return 0;
+}
+
+/* Copy the loaded index out (used to check an index builder against
+ * `hera index`): sizes first with NULL buffers. */
+int refh_index_sizes(uint32_t *n_trans, uint32_t *name_len, uint64_t *seq_len,
+		     uint64_t *n_buckets, uint32_t *n_pos)
+{
+	uint64_t i, count = 0;
+	*n_trans = REF_INF->n;
+	*name_len = REF_INF->name_len;
+	*seq_len = REF_INF->find[REF_INF->n - 1];
+	for (i = 0; i < H; ++i)
+		count += KMER_HASH->n[i];
+	*n_buckets = count;
+	*n_pos = KMER_HASH->n_pos;
+	return 0;
+}
+
+void refh_set_write_bam(int v)
+{
+	WRITE_BAM = (unsigned)v;
+}
+
+static int emit(refh_result *out, uint64_t ri, Candidate *c)
+{
+	refh_rec *rec = &out->recs[ri];
+	int s;
+
+	rec->pair = c->pair;
+	for (s = 0; s < 2; ++s) {
+		Cigar *g = c->cigar[s];
+		int j;
+		rec->n[s] = (int32_t)c->n[s];
+		rec->err[s] = c->err[s];
+		if (out->list_used + c->n[s] > out->list_cap ||
+		    out->op_used + g->n_cigar > out->op_cap ||
+		    out->miss_used + g->n_miss > out->miss_cap)
+			return -1;
+		rec->list_off[s] = (uint32_t)out->list_used;
+		if (c->n[s]) {
+			memcpy(out->pos_pool + out->list_used, c->pos[s], c->n[s] * sizeof(uint32_t));
+			memcpy(out->p_pool + out->list_used, c->p[s], c->n[s] * sizeof(int32_t));
+		}
+		out->list_used += c->n[s];
+		rec->cig_off[s] = (uint32_t)out->op_used;
+		rec->n_cigar[s] = g->n_cigar;
+		for (j = 0; j < g->n_cigar; ++j)
+			out->op_pool[out->op_used + j] =
+				((uint32_t)g->count[j] << 4) | (uint32_t)(uint8_t)g->type[j];
+		out->op_used += g->n_cigar;
+		rec->miss_off[s] = (uint32_t)out->miss_used;
+		rec->n_miss[s] = g->n_miss;
+		if (g->n_miss)
+			memcpy(out->miss_pool + out->miss_used, g->miss, g->n_miss);
+		out->miss_used += g->n_miss;
+	}
+	return 0;
+}
+
+static void front_half_pair(struct read_inf *a, struct read_inf *b, Candidate *r[2])
+{
+	r[0] = init_candidate();
+	r[1] = init_candidate();
+	check_in_transcriptome(a, b, r);
+	if (r[0]->n[0] > 0 && r[0]->n[1] > 0)
+		intersect2(r[0], a, b, MAX_FRAG);
+	if (r[1]->n[0] > 0 && r[1]->n[1] > 0)
+		intersect2(r[1], b, a, MAX_FRAG);
+}
+
+int refh_align_pairs(int write_bam, int n,
+		     char *seq1, const int64_t *off1, const int32_t *len1,
+		     char *seq2, const int64_t *off2, const int32_t *len2,
+		     refh_result *out)
+{
+	int i, rc = 0;
+	char name[] = "r";
+
+	WRITE_BAM = (unsigned)write_bam;
+	out->list_used = out->op_used = out->miss_used = 0;
+	for (i = 0; i < n && rc == 0; ++i) {
+		struct read_inf a = {seq1 + off1[i], name, NULL, len1[i]};
+		struct read_inf b = {seq2 + off2[i], name, NULL, len2[i]};
+		Candidate *r[2];
+		front_half_pair(&a, &b, r);
+		rc = emit(out, 2 * (uint64_t)i, r[0]);
+		if (rc == 0)
+			rc = emit(out, 2 * (uint64_t)i + 1, r[1]);
+		destroy_candidate(r[0]);
+		destroy_candidate(r[1]);
+	}
+	return rc;
+}
+
+int refh_align_single(int write_bam, int n, char *seq, const int64_t *off,
+		      const int32_t *len, refh_result *out)
+{
+	int i, rc = 0;
+	char name[] = "r";
+
+	WRITE_BAM = (unsigned)write_bam;
+	out->list_used = out->op_used = out->miss_used = 0;
+	for (i = 0; i < n && rc == 0; ++i) {
+		struct read_inf a = {seq + off[i], name, NULL, len[i]};
+		Candidate *r = init_candidate();
+		get_position(&a, r, 0, 2 * ERR);
+		get_position(&a, r, 1, 2 * ERR);
+		rc = emit(out, (uint64_t)i, r);
+		destroy_candidate(r);
+	}
+	return rc;
+}
+
+static int export_cigar(Cigar *c, uint32_t *ops, int *n_ops, char *miss,
+			int *n_miss, int cap)
+{
+	int j;
+	if (c->n_cigar > cap || c->n_miss > cap)
+		return -1;
+	for (j = 0; j < c->n_cigar; ++j)
+		ops[j] = ((uint32_t)c->count[j] << 4) | (uint32_t)(uint8_t)c->type[j];
+	*n_ops = c->n_cigar;
+	if (c->n_miss)
+		memcpy(miss, c->miss, c->n_miss);
+	*n_miss = c->n_miss;
+	return 0;
+}
+
+int refh_sw_align(int write_bam, char *ref, uint32_t rstart, char *q,
+		  uint32_t ref_len, uint32_t len, int err,
+		  uint32_t *ops, int *n_ops, char *miss, int *n_miss, int cap)
+{
+	int score = 0, rc;
+	Cigar *c;
+	WRITE_BAM = (unsigned)write_bam;
+	c = SW_align(ref, rstart, q, ref_len, len, &score, (short)err);
+	rc = export_cigar(c, ops, n_ops, miss, n_miss, cap);
+	free_cigar(c);
+	return rc < 0 ? -1000000 : score;
+}
+
+int refh_ssw_align(char *ref, int32_t ref_len, char *read, int32_t read_len,
+		   int *skip, uint32_t *ops, int *n_ops, char *miss, int *n_miss,
+		   int cap)
+{
+	int score = 0, rc;
+	Cigar *c = ssw_align(ref, ref_len, read, read_len, &score, skip);
+	rc = export_cigar(c, ops, n_ops, miss, n_miss, cap);
+	free_cigar(c);
+	return rc < 0 ? -1000000 : score;
+}
+
+/* ---- multi-threaded timing (CPU baseline): results are discarded ---- */
+typedef struct {
+	int lo, hi;
+	char *seq1, *seq2;
+	const int64_t *off1, *off2;
+	const int32_t *len1, *len2;
+} refh_job;
+
+static void *refh_worker(void *arg)
+{
+	refh_job *j = arg;
+	char name[] = "r";
+	int i;
+	for (i = j->lo; i < j->hi; ++i) {
+		struct read_inf a = {j->seq1 + j->off1[i], name, NULL, j->len1[i]};
+		struct read_inf b = {j->seq2 + j->off2[i], name, NULL, j->len2[i]};
+		Candidate *r[2];
+		front_half_pair(&a, &b, r);
+		destroy_candidate(r[0]);
+		destroy_candidate(r[1]);
+	}
+	return NULL;
+}
+
+int refh_align_pairs_mt(int write_bam, int n,
+			char *seq1, const int64_t *off1, const int32_t *len1,
+			char *seq2, const int64_t *off2, const int32_t *len2,
+			int nthreads)
+{
+	pthread_t *th;
+	refh_job *jobs;
+	pthread_attr_t attr;
+	int t;
+
+	WRITE_BAM = (unsigned)write_bam;
+	if (nthreads < 1)
+		nthreads = 1;
+	th = calloc(nthreads, sizeof(pthread_t));
+	jobs = calloc(nthreads, sizeof(refh_job));
+	pthread_attr_init(&attr);
+	pthread_attr_setstacksize(&attr, THREAD_STACK_SIZE);
+	for (t = 0; t < nthreads; ++t) {
+		refh_job *j = &jobs[t];
+		j->lo = (int)((int64_t)n * t / nthreads);
+		j->hi = (int)((int64_t)n * (t + 1) / nthreads);
+		j->seq1 = seq1; j->seq2 = seq2;
+		j->off1 = off1; j->off2 = off2;
+		j->len1 = len1; j->len2 = len2;
+		pthread_create(&th[t], &attr, refh_worker, j);
+	}
+	for (t = 0; t < nthreads; ++t)
+		pthread_join(th[t], NULL);
+	pthread_attr_destroy(&attr);
+	free(th);
+	free(jobs);
+	return 0;
+}
