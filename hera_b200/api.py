@@ -1,0 +1,234 @@
+"""Python mirror of the C ABI in include/hera_gpu.h (ctypes).
+
+``Context`` owns one device copy of a hera index and runs the hot path:
+``align_pairs`` is the batched replacement of the per-pair
+check_in_transcriptome + intersect2 front half of hera's align_pair_read
+(src/hash_align.c:1724-1733), ``align_single`` of align_single_read's two
+get_position calls (src/hash_align.c:1822-1823).  Results come back as
+``Result`` objects holding the flat hera_cand_rec records.
+
+The library is hera_b200/libhera_b200.so, built in-tree by hera_b200.build.
+There is no CPU fallback: a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+HERA_GPU_OK = 0
+ERRORS = {-1: "ENODEV", -2: "ECUDA", -3: "ENOMEM", -4: "EINVAL", -5: "ECAPACITY", -6: "ETIMEOUT"}
+MAX_READ = 320
+CIGAR_CHARS = "MIDNSHP=XB"
+
+REC_DTYPE = np.dtype([
+    ("n", "<i4", (2,)), ("err", "<i4", (2,)), ("pair", "<i4"),
+    ("list_off", "<u4", (2,)), ("cig_off", "<u4", (2,)), ("miss_off", "<u4", (2,)),
+    ("n_cigar", "<u2", (2,)), ("n_miss", "<u2", (2,)),
+])
+
+
+class HeraGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hera_gpu {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _IndexView(C.Structure):
+    _fields_ = [("n_trans", C.c_uint32), ("len", C.c_void_p), ("find", C.c_void_p),
+                ("seq", C.c_void_p), ("bucket_n", C.c_void_p), ("buckets", C.c_void_p),
+                ("n_buckets", C.c_uint64), ("pos", C.c_void_p), ("p", C.c_void_p),
+                ("n_pos", C.c_uint32)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_batch", C.c_uint32), ("scratch_bytes", C.c_uint64)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("recs", C.c_void_p), ("pos_pool", C.c_void_p), ("p_pool", C.c_void_p),
+                ("op_pool", C.c_void_p), ("miss_pool", C.c_void_p),
+                ("list_cap", C.c_uint64), ("op_cap", C.c_uint64), ("miss_cap", C.c_uint64),
+                ("list_used", C.c_uint64), ("op_used", C.c_uint64), ("miss_used", C.c_uint64)]
+
+
+class _Reads(C.Structure):
+    _fields_ = [("seq", C.c_void_p), ("off", C.c_void_p), ("len", C.c_void_p)]
+
+
+class Timing(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("h2d_ms", "seed_ms", "position_ms", "resolve_ms",
+                                         "rescue_ms", "pack_ms", "d2h_ms", "total_ms")] + [
+        ("launches", C.c_uint32), ("rescue_rounds", C.c_uint32), ("lookups", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libhera_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: run `python -m hera_b200.build`")
+    lib = C.CDLL(path)
+    lib.hera_gpu_abi_version.restype = C.c_int
+    lib.hera_gpu_ctx_create.restype = C.c_int
+    lib.hera_gpu_ctx_create.argtypes = [C.POINTER(_IndexView), C.POINTER(_Options), C.POINTER(C.c_void_p)]
+    lib.hera_gpu_ctx_destroy.argtypes = [C.c_void_p]
+    lib.hera_gpu_last_error.restype = C.c_char_p
+    lib.hera_gpu_last_error.argtypes = [C.c_void_p]
+    lib.hera_gpu_align_pairs_flat.argtypes = [C.c_void_p, C.POINTER(_Reads), C.POINTER(_Reads),
+                                              C.c_int32, C.c_int, C.POINTER(_Result)]
+    lib.hera_gpu_align_single_flat.argtypes = [C.c_void_p, C.POINTER(_Reads), C.c_int32, C.c_int,
+                                               C.POINTER(_Result)]
+    lib.hera_gpu_align_pairs_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int32, C.c_int32, C.c_int, C.c_void_p]
+    lib.hera_gpu_fetch_result.argtypes = [C.c_void_p, C.POINTER(_Result)]
+    lib.hera_gpu_get_timing.argtypes = [C.c_void_p, C.POINTER(Timing)]
+    lib.hera_gpu_stream.restype = C.c_void_p
+    lib.hera_gpu_stream.argtypes = [C.c_void_p]
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Result:
+    """Flat Candidate records (hera_cand_rec) plus their pools."""
+
+    def __init__(self, n_recs: int, list_cap: int, op_cap: int, miss_cap: int):
+        self.recs = np.zeros(max(n_recs, 1), dtype=REC_DTYPE)[:n_recs]
+        self._alloc(list_cap, op_cap, miss_cap)
+
+    def _alloc(self, list_cap, op_cap, miss_cap):
+        self.pos_pool = np.zeros(max(list_cap, 1), np.uint32)
+        self.p_pool = np.zeros(max(list_cap, 1), np.int32)
+        self.op_pool = np.zeros(max(op_cap, 1), np.uint32)
+        self.miss_pool = np.zeros(max(miss_cap, 1), np.uint8)
+        base = self.recs.ctypes.data if self.recs.shape[0] else 0
+        self.c = _Result(base, _ptr(self.pos_pool), _ptr(self.p_pool), _ptr(self.op_pool),
+                         _ptr(self.miss_pool), list_cap, op_cap, miss_cap, 0, 0, 0)
+
+    def candidate(self, i: int):
+        """(pair, ((n, err, pos, p, cigar, miss) for strand 0, 1))."""
+        r = self.recs[i]
+        out = []
+        for s in range(2):
+            n = int(r["n"][s])
+            lo = int(r["list_off"][s])
+            co, nc = int(r["cig_off"][s]), int(r["n_cigar"][s])
+            mo, nm = int(r["miss_off"][s]), int(r["n_miss"][s])
+            cig = "".join(f"{int(o) >> 4}{CIGAR_CHARS[int(o) & 15]}" for o in self.op_pool[co:co + nc])
+            out.append((n, int(r["err"][s]), tuple(self.pos_pool[lo:lo + n].tolist()),
+                        tuple(self.p_pool[lo:lo + n].tolist()), cig,
+                        bytes(self.miss_pool[mo:mo + nm])))
+        return (int(r["pair"]), tuple(out))
+
+    def canonical(self) -> List[tuple]:
+        return [self.candidate(i) for i in range(self.recs.shape[0])]
+
+
+class Context:
+    """One hera index resident on one GPU."""
+
+    def __init__(self, index, device: int = 0, max_batch: int = 0, scratch_bytes: int = 0):
+        self.lib = load_library()
+        self.index = index
+        v = _IndexView()
+        self._keep = [np.ascontiguousarray(index.length, np.uint32),
+                      np.ascontiguousarray(index.find, np.uint32),
+                      np.ascontiguousarray(index.seq, np.uint8),
+                      np.ascontiguousarray(index.bucket_n, np.uint32),
+                      np.ascontiguousarray(index.buckets),
+                      np.ascontiguousarray(index.pos, np.uint32),
+                      np.ascontiguousarray(index.p, np.uint32)]
+        ln, fd, sq, bn, bk, pos, p = self._keep
+        v.n_trans, v.len, v.find, v.seq = index.n_trans, _ptr(ln), _ptr(fd), _ptr(sq)
+        v.bucket_n, v.buckets, v.n_buckets = _ptr(bn), _ptr(bk), bk.shape[0]
+        v.pos, v.p, v.n_pos = _ptr(pos), _ptr(p), pos.shape[0]
+        opt = _Options(device, max_batch, scratch_bytes)
+        h = C.c_void_p()
+        rc = self.lib.hera_gpu_ctx_create(C.byref(v), C.byref(opt), C.byref(h))
+        if rc != HERA_GPU_OK:
+            raise HeraGpuError(rc, "context creation failed")
+        self.h = h
+        self._keep = None
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hera_gpu_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != HERA_GPU_OK:
+            raise HeraGpuError(rc, self.lib.hera_gpu_last_error(self.h).decode())
+
+    @staticmethod
+    def _reads(rs) -> _Reads:
+        return _Reads(_ptr(rs.seq), _ptr(rs.off), _ptr(rs.len))
+
+    def _run(self, fn, n_recs, total_len, args) -> Result:
+        res = Result(n_recs, n_recs * 8 + 1024, n_recs * 8 + 1024, total_len // 4 + 1024)
+        rc = fn(*args, C.byref(res.c))
+        if rc == -5 and (res.c.list_used > res.c.list_cap or res.c.op_used > res.c.op_cap
+                         or res.c.miss_used > res.c.miss_cap):
+            res._alloc(res.c.list_used + 1, res.c.op_used + 1, res.c.miss_used + 1)
+            rc = fn(*args, C.byref(res.c))
+        self._check(rc)
+        return res
+
+    def align_pairs(self, r1, r2, write_bam: int = 1) -> Result:
+        """Paired reads (synth.ReadSet-like: seq, off, len) -> 2 records per pair."""
+        a, b = self._reads(r1), self._reads(r2)
+        return self._run(self.lib.hera_gpu_align_pairs_flat, 2 * r1.n,
+                         int(r1.len.sum()) + int(r2.len.sum()),
+                         (self.h, C.byref(a), C.byref(b), r1.n, write_bam))
+
+    def align_single(self, rs, write_bam: int = 1) -> Result:
+        a = self._reads(rs)
+        return self._run(self.lib.hera_gpu_align_single_flat, rs.n, int(rs.len.sum()),
+                         (self.h, C.byref(a), rs.n, write_bam))
+
+    def align_pairs_device(self, d_seq: int, d_off: int, d_len: int, n: int, max_len: int,
+                           write_bam: int = 1, stream: Optional[int] = None) -> None:
+        """Device-resident batch: pointers into HBM (2n reads, mates
+        interleaved).  Results stay on the device until fetch()."""
+        self._check(self.lib.hera_gpu_align_pairs_device(self.h, d_seq, d_off, d_len, n, max_len,
+                                                         write_bam, stream))
+
+    def fetch(self, n_recs: int) -> Result:
+        res = Result(n_recs, n_recs * 8 + 1024, n_recs * 8 + 1024, n_recs * 8 + 1024)
+        rc = self.lib.hera_gpu_fetch_result(self.h, C.byref(res.c))
+        if rc == -5:
+            res._alloc(res.c.list_used + 1, res.c.op_used + 1, res.c.miss_used + 1)
+            rc = self.lib.hera_gpu_fetch_result(self.h, C.byref(res.c))
+        self._check(rc)
+        return res
+
+    def timing(self) -> dict:
+        t = Timing()
+        self.lib.hera_gpu_get_timing(self.h, C.byref(t))
+        return t.as_dict()
+
+    @property
+    def stream(self) -> int:
+        return self.lib.hera_gpu_stream(self.h) or 0

@@ -1,0 +1,852 @@
+// hera_device.cuh -- device-side algorithms of the hera read-alignment hot
+// path for sm_100a.  One CUDA thread runs one task (a get_position call, a
+// pair's control flow, or one mate rescue); per-task working sets live in
+// local memory (L1-backed), per-pair Candidate state in HBM.
+//
+// Each routine restates one reference function; the cited file:line is the
+// behaviour it must reproduce bit for bit (reference = bioturing/hera).
+#pragma once
+
+#include <cstdint>
+
+namespace hg {
+
+constexpr int KMER = 31;
+constexpr int ERR = 7;
+constexpr int MAX_FRAG = 1000;
+constexpr int HBITS = 27;
+constexpr uint64_t HMASK = (1ull << HBITS) - 1;
+constexpr int MAX_READ = 320;          // HERA_GPU_MAX_READ
+constexpr int MAX_DP_ROWS = MAX_READ;  // rows of one gap DP (<= read length)
+constexpr int BW = 24;                 // gap-DP band width (bound: 2*error+2 = 18)
+constexpr int ACAP = 256;              // anchors of one get_position call
+constexpr int LCAP = 64;               // hits kept per Candidate strand
+constexpr int CCAP = 96;               // CIGAR ops per Candidate strand
+constexpr int MCAP = 96;               // miss chars per Candidate strand
+
+enum : int { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4, OP_X = 8 };
+
+// capacity / consistency flags (OR-ed into one word per batch)
+enum : int {
+	F_ACAP = 1, F_LCAP = 2, F_CCAP = 4, F_MCAP = 8, F_BAND = 16, F_READ = 32,
+	F_SCRATCH = 64, F_QUEUE = 128
+};
+
+struct DevIndex {
+	const uint32_t *boff;    // [2^27 + 1] bucket start offsets
+	const uint4 *bk;         // buckets {id lo, id hi, start, end}
+	const uint2 *occ;        // occurrences {transcript, offset}
+	const uint8_t *seq;      // transcript ASCII, zero padded
+	const uint8_t *code;     // transcript codes 0..4, padded with 4
+	const uint32_t *tlen;    // transcript lengths
+	const uint32_t *tstart;  // transcript start offsets in seq
+	uint32_t n_trans;
+};
+
+// ascii_table (src/hash_align.c:6-23): A/a 0, C/c 1, G/g 2, T/t 3, else 4
+__device__ __forceinline__ uint8_t code_of(uint8_t c)
+{
+	uint8_t x = c | 0x20;
+	return x == 'a' ? 0 : x == 'c' ? 1 : x == 'g' ? 2 : x == 't' ? 3 : 4;
+}
+
+__device__ __forceinline__ uint8_t comp_code(uint8_t c)
+{
+	return c < 4 ? (uint8_t)(3 - c) : c;
+}
+
+// ---------------------------------------------------------------------
+// CIGAR algebra
+// ---------------------------------------------------------------------
+struct DCig {
+	int n, nm;
+	uint32_t op[CCAP];       // (count << 4) | op
+	uint8_t miss[MCAP];
+};
+
+__device__ __forceinline__ int op_type(uint32_t o) { return (int)(o & 15u); }
+__device__ __forceinline__ unsigned op_cnt(uint32_t o) { return o >> 4; }
+
+// add_cigar (src/hash_align.c:526-565)
+__device__ inline void cig_add(DCig &c, int type, unsigned add, const uint8_t *mc, int &flags)
+{
+	add &= 0xffffu;
+	if (add == 0)
+		return;
+	if (c.n > 1 && op_type(c.op[c.n - 1]) == OP_S) {
+		if (type != OP_D)
+			c.op[c.n - 1] = (((op_cnt(c.op[c.n - 1]) + add) & 0xffffu) << 4) | OP_S;
+		return;
+	}
+	if (mc) {
+		if (c.nm + (int)add > MCAP) {
+			flags |= F_MCAP;
+		} else {
+			for (unsigned t = 0; t < add; ++t)
+				c.miss[c.nm + t] = mc[t];
+			c.nm += (int)add;
+		}
+	}
+	if (c.n > 0 && op_type(c.op[c.n - 1]) == type) {
+		c.op[c.n - 1] = (((op_cnt(c.op[c.n - 1]) + add) & 0xffffu) << 4) | (uint32_t)type;
+		return;
+	}
+	if (c.n == CCAP) {
+		flags |= F_CCAP;
+		return;
+	}
+	c.op[c.n++] = (add << 4) | (uint32_t)type;
+}
+
+// reverse_cigar (src/hash_align.c:567-587)
+__device__ inline void cig_reverse(DCig &c)
+{
+	for (int i = 0; i < c.n / 2; ++i) {
+		uint32_t t = c.op[i];
+		c.op[i] = c.op[c.n - 1 - i];
+		c.op[c.n - 1 - i] = t;
+	}
+	for (int i = 0; i < c.nm / 2; ++i) {
+		uint8_t t = c.miss[i];
+		c.miss[i] = c.miss[c.nm - 1 - i];
+		c.miss[c.nm - 1 - i] = t;
+	}
+}
+
+// concat_cigar (src/hash_align.c:589-603)
+__device__ inline void cig_concat(DCig &d, DCig &t, int &flags)
+{
+	cig_reverse(t);
+	int k = 0;
+	for (int i = 0; i < t.n; ++i) {
+		int ty = op_type(t.op[i]);
+		unsigned cnt = op_cnt(t.op[i]);
+		if (ty == OP_D || ty == OP_X) {
+			cig_add(d, ty, cnt, t.miss + k, flags);
+			k += (int)cnt;
+		} else {
+			cig_add(d, ty, cnt, nullptr, flags);
+		}
+	}
+}
+
+__device__ inline void cig_copy(DCig &d, const DCig &s)
+{
+	d.n = s.n;
+	d.nm = s.nm;
+	for (int i = 0; i < s.n; ++i)
+		d.op[i] = s.op[i];
+	for (int i = 0; i < s.nm; ++i)
+		d.miss[i] = s.miss[i];
+}
+
+// ---------------------------------------------------------------------
+// Gap DP: SW_align (src/hash_align.c:627-760), banded.
+//
+// The reference fills a zeroed (len+1) x (ref_len+1) u16 matrix; row k only
+// ever writes columns [s_k, b_k] plus one marker, and every computed cell
+// satisfies |k - c| <= M[k][c] <= error, so b_k - s_k <= 2*error + 1.  Here
+// each row keeps just its written band (lo = s_k, width); any other cell
+// reads as the zeroed matrix would, including row 0 (M[0][c] = c for
+// c <= error+1) and its spill into later rows of the flat array.
+// ---------------------------------------------------------------------
+struct SwWork {
+	uint8_t band[(MAX_DP_ROWS + 1) * BW];
+	uint16_t lo[MAX_DP_ROWS + 1];
+	uint8_t wid[MAX_DP_ROWS + 1];
+};
+
+struct SwView {
+	const SwWork *w;
+	unsigned W, error;
+	__device__ __forceinline__ unsigned get(int k, int c) const
+	{
+		unsigned rel = (unsigned)(c - (int)w->lo[k]);
+		if (rel < w->wid[k])
+			return w->band[k * BW + rel];
+		long long flat = (long long)k * W + c;
+		return flat <= (long long)error + 1 ? (unsigned)flat : 0u;
+	}
+};
+
+// Reference window accessor: x in [0, ref_len), reversed for prefix DPs.
+struct RefWin {
+	const uint8_t *code;
+	const uint8_t *ascii;
+	uint32_t start, len;
+	bool rev;
+	__device__ __forceinline__ uint32_t at(int x) const { return rev ? start + len - 1 - x : start + x; }
+	__device__ __forceinline__ uint8_t c(int x) const { return code[at(x)]; }
+	__device__ __forceinline__ const uint8_t *a(int x) const { return ascii + at(x); }
+};
+
+// q: query codes (already oriented), qlen; qrev: read q backwards (prefix DP)
+__device__ inline int sw_align(const DevIndex &ix, uint32_t rstart, const uint8_t *q,
+			       uint32_t ref_len, uint32_t len, int err, bool score_only,
+			       DCig &cig, SwWork &w, int &flags)
+{
+	cig.n = 0;
+	cig.nm = 0;
+	if (len == 0)
+		return 0;
+	if (len > (uint32_t)MAX_DP_ROWS) {
+		flags |= F_READ;
+		return 0;
+	}
+	const unsigned error = (unsigned)(err < 0 ? -err : err) + 1;
+	const bool rev = err < 0;
+	RefWin r{ix.code, ix.seq, rstart, ref_len, rev};
+	auto qc = [&](int x) -> uint8_t { return rev ? q[len - 1 - x] : q[x]; };
+	SwView M{&w, ref_len + 1, error};
+
+	// row 0: M[0][c] = c for c <= error+1 (the rest of the row is zero)
+	{
+		unsigned wd = (ref_len < error + 1 ? ref_len : error + 1) + 1;
+		w.lo[0] = 0;
+		w.wid[0] = (uint8_t)wd;
+		for (unsigned c = 0; c < wd; ++c)
+			w.band[c] = (uint8_t)c;
+	}
+
+	unsigned s = 0, min = 0, xmin = 0;
+	int i = 0, k, j, ferr = -1, score = 0;
+	for (k = 1; k <= (int)len; ++k) {
+		uint8_t *cb = w.band + k * BW;
+		const int plo = w.lo[k - 1];
+		const unsigned pwd = w.wid[k - 1];
+		const uint8_t *pb = w.band + (k - 1) * BW;
+		auto pget = [&](int c) -> unsigned {
+			unsigned rel = (unsigned)(c - plo);
+			if (rel < pwd)
+				return pb[rel];
+			long long flat = (long long)(k - 1) * (ref_len + 1) + c;
+			return flat <= (long long)error + 1 ? (unsigned)flat : 0u;
+		};
+		const uint8_t qk = qc(k - 1);
+		min = error;
+		j = 0;
+		w.lo[k] = (uint16_t)s;
+		unsigned left = pget((int)s) + 1;
+		cb[0] = (uint8_t)left;
+		unsigned wd = 1;
+		unsigned d = pget((int)s);
+		for (i = (int)s + 1; i <= (int)ref_len; ++i) {
+			unsigned rel = (unsigned)i - s;
+			if (rel >= (unsigned)BW) {
+				flags |= F_BAND;
+				break;
+			}
+			unsigned up = pget(i);
+			if (d == error + 1) {
+				cb[rel] = (uint8_t)(error + 1);
+				wd = rel + 1;
+				break;
+			}
+			unsigned pen = 0;
+			if (d < error)
+				pen = r.c(i - 1) == qk ? 0u : 1u;
+			unsigned v = d + pen;
+			if (left + 1 < v)
+				v = left + 1;
+			if (up + 1 < v)
+				v = up + 1;
+			cb[rel] = (uint8_t)v;
+			wd = rel + 1;
+			if (v == error && j == 0)
+				j = i;
+			if (v < error)
+				j = 0;
+			if (v <= min) {
+				min = v;
+				xmin = (unsigned)i;
+			}
+			if (ferr == -1 && i == k && v > 0)
+				ferr = i;
+			left = v;
+			d = up;
+		}
+		w.wid[k] = (uint8_t)wd;
+		if (min == error) {
+			++k;
+			break;
+		}
+		while (M.get(k, (int)s) >= error && s < (unsigned)i)
+			++s;
+		if ((unsigned)j > xmin && (unsigned)j < ref_len)
+			cb[(unsigned)j - w.lo[k]] = (uint8_t)(error + 1);
+	}
+	--k;
+
+	if (min >= error) {
+		// early stop: shrink the aligned query prefix (:698-711); the
+		// reference's r[-1] read at column 0 cannot change the outcome
+		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+			--k;
+			int jj = 0;
+			for (int c = 0; (unsigned)c < ref_len; ++c) {
+				unsigned v = M.get(k, c);
+				if (v == error + 1)
+					break;
+				if (v > 0)
+					jj = (int)error;
+				if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) &&
+				    v == M.get(k - 1, c - 1)) {
+					min = v;
+					xmin = (unsigned)c;
+				}
+			}
+		}
+		if (k < 5) {
+			cig_add(cig, OP_S, len, nullptr, flags);
+			return (int)len;
+		}
+		cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
+		score = (int)len - k;
+		i = k;
+	} else {
+		if (xmin < len && k == (int)len) {
+			min += len - xmin;
+			xmin = len;
+		}
+		i = (int)len;
+	}
+	k = (int)xmin;
+	score += (int)min;
+
+	if (score_only) {   // WRITE_BAM == 1 (:731-734)
+		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
+		return score;
+	}
+	while (i > 0 && k > 0) {   // traceback (:736-758)
+		unsigned cur = M.get(i, k);
+		unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
+		if (cur == M.get(i - 1, k - 1) + pen) {
+			if (pen == 0)
+				cig_add(cig, OP_M, 1, nullptr, flags);
+			else
+				cig_add(cig, OP_X, 1, r.a(k - 1), flags);
+			--i;
+			--k;
+		} else if (cur == M.get(i - 1, k) + 1) {
+			cig_add(cig, OP_I, 1, nullptr, flags);
+			--i;
+		} else {
+			cig_add(cig, OP_D, 1, r.a(k - 1), flags);
+			--k;
+		}
+	}
+	if (i > 0)
+		cig_add(cig, OP_I, (unsigned)i, nullptr, flags);
+	for (int t = 1; t <= k; ++t)
+		cig_add(cig, OP_D, 1, r.a(k - t), flags);
+	return score;
+}
+
+// ---------------------------------------------------------------------
+// Seed-table probe: hash_get with add = 0 (src/hash_align.c:862-895).
+// Returns {start, count} of the k-mer's occurrence list, count 0 on a miss.
+// Buckets are sorted by id, so any search that finds the equal id returns
+// the reference's slot.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ uint2 probe(const DevIndex &ix, uint64_t id)
+{
+	const uint32_t mod = (uint32_t)(id & HMASK);
+	uint32_t lo = __ldg(ix.boff + mod);
+	uint32_t hi = __ldg(ix.boff + mod + 1);
+	while (lo < hi) {
+		uint32_t mid = (lo + hi) >> 1;
+		uint4 b = __ldg(ix.bk + mid);
+		uint64_t bid = ((uint64_t)b.y << 32) | b.x;
+		if (bid == id)
+			return make_uint2(b.z, b.w - b.z);
+		if (bid > id)
+			hi = mid;
+		else
+			lo = mid + 1;
+	}
+	return make_uint2(0, 0);
+}
+
+// get_index (src/hash_align.c:997-1006): codes shifted in unmasked
+__device__ __forceinline__ uint64_t kmer_at(const uint8_t *rd, int i)
+{
+	uint64_t id = 0;
+#pragma unroll
+	for (int t = 0; t < KMER; ++t)
+		id = (id << 2) | rd[i + t];
+	return id;
+}
+
+// ---------------------------------------------------------------------
+// Per-pair Candidate state in HBM
+// ---------------------------------------------------------------------
+struct DSlot {              // one strand of a Candidate (src/hash_align.h:90-97)
+	int32_t n, err;
+	uint32_t t[LCAP];       // transcript ids   (Candidate.pos)
+	int32_t p[LCAP];        // positions        (Candidate.p)
+	DCig cig;
+};
+
+struct DPair {
+	DSlot s[2][2];          // [candidate r[0]/r[1]][strand]
+	int32_t pair[2];
+	int32_t stage;
+	int32_t rm_ret;
+	int32_t rm_i;
+	int32_t pad;
+};
+
+// Anchors of one get_position call: pos2[0..2] of the reference.
+struct Anchors {
+	uint32_t t[ACAP], tp[ACAP], off[ACAP];
+};
+
+struct GpWork {
+	Anchors a[2];
+	DCig c1, c2;
+	SwWork sw;
+	uint8_t rd[MAX_READ];
+};
+
+// merge_sort (src/hash_align.c:257-297): new hit list (all at read offset
+// idx) merged into the anchors by transcript; on an equal transcript the
+// existing anchor goes first when the unsigned wrapped diagonal difference
+// is < 2*ERR, else the smaller tpos.
+__device__ inline int merge_hits(const Anchors &A, int na, Anchors &B, const uint2 *occ,
+				 uint32_t nh, uint32_t idx, int &flags)
+{
+	if (na + (int)nh > ACAP) {
+		flags |= F_ACAP;
+		nh = (uint32_t)(ACAP - na);
+	}
+	int i = 0, n = 0;
+	uint32_t k = 0;
+	uint2 h = nh ? __ldg(occ) : make_uint2(0, 0);
+	while (i < na && k < nh) {
+		bool take_a;
+		if (A.t[i] < h.x) {
+			take_a = true;
+		} else if (A.t[i] > h.x) {
+			take_a = false;
+		} else {
+			uint32_t dis = (h.y - A.tp[i]) - (idx - A.off[i]);
+			take_a = dis < 2 * ERR ? true : !(A.tp[i] > h.y);
+		}
+		if (take_a) {
+			B.t[n] = A.t[i]; B.tp[n] = A.tp[i]; B.off[n] = A.off[i];
+			++i;
+		} else {
+			B.t[n] = h.x; B.tp[n] = h.y; B.off[n] = idx;
+			++k;
+			if (k < nh)
+				h = __ldg(occ + k);
+		}
+		++n;
+	}
+	while (i < na) {
+		B.t[n] = A.t[i]; B.tp[n] = A.tp[i]; B.off[n] = A.off[i];
+		++i; ++n;
+	}
+	while (k < nh) {
+		h = __ldg(occ + k);
+		B.t[n] = h.x; B.tp[n] = h.y; B.off[n] = idx;
+		++k; ++n;
+	}
+	return n;
+}
+
+// get_SWalign (src/hash_align.c:1242-1320)
+__device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rlen, Anchors &A,
+				   uint32_t id, uint32_t n, uint32_t &store, uint32_t &max,
+				   DSlot &S, bool score_only, GpWork &w, int &flags)
+{
+	if (n > 1 && A.tp[id + n - 1] - A.tp[id] > (uint32_t)rlen)
+		return;
+	const uint32_t tr = A.t[id];
+	int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
+	if (start < 0 || (uint32_t)(start + rlen) > __ldg(ix.tlen + tr))
+		return;
+	uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
+	const uint32_t ref_start = __ldg(ix.tstart + tr) + (uint32_t)start;
+	int err = 0, sub = 0, score;
+	DCig &cig = w.c1;
+	DCig &tmp = w.c2;
+	cig.n = cig.nm = 0;
+	if (A.off[id] > 0) {
+		const uint32_t o0 = A.off[id];
+		score = sw_align(ix, ref_start - add, rd, o0 + add, o0, o0 < 2 * ERR ? -3 : -ERR,
+				 score_only, cig, w.sw, flags);
+		err += score;
+		if (err > rlen / 2 || (uint32_t)err > max)
+			return;
+		for (int t = 0; t < cig.n; ++t) {
+			int ty = op_type(cig.op[t]);
+			if (ty == OP_I || ty == OP_S)
+				sub += (int)op_cnt(cig.op[t]);
+			else if (ty == OP_D)
+				sub -= (int)op_cnt(cig.op[t]);
+		}
+	}
+	for (uint32_t i = 0; i < n; ++i) {
+		uint32_t s0 = i;
+		while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
+			++i;
+		cig_add(cig, OP_M, A.off[id + i] - A.off[id + s0] + KMER, nullptr, flags);
+		uint32_t seg = A.off[id + i] + KMER;
+		uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)rlen) - seg;
+		uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
+		score = sw_align(ix, ref_start + seg, rd + seg, len + ad, len, len < 2 * ERR ? 3 : ERR,
+				 score_only, tmp, w.sw, flags);
+		err += score;
+		if (err > rlen / 2 || (uint32_t)err > max + 1)
+			return;
+		cig_concat(cig, tmp, flags);
+	}
+	if (max == (uint32_t)(rlen / 2) || (uint32_t)err < max) {
+		cig_copy(S.cig, cig);
+		store = 0;
+		max = (uint32_t)err;
+	}
+	A.t[store] = A.t[id];
+	A.tp[store] = A.tp[id] - (A.off[id] + KMER - 1) + (uint32_t)sub;
+	++store;
+}
+
+__device__ __forceinline__ bool chain_next(const Anchors &A, int na, uint32_t i, uint32_t n,
+					   int rlen, bool stop_consumed)
+{
+	if (i + 1 >= (uint32_t)na)
+		return false;
+	if (A.t[i] != A.t[i + 1] || !(A.off[i + 1] > A.off[i]))
+		return false;
+	if (!(A.tp[i + 1] > A.tp[i + 1 - n]))
+		return false;
+	if (!(A.tp[i + 1] - A.tp[i + 1 - n] < (uint32_t)rlen))
+		return false;
+	if (stop_consumed && A.off[i + 1] == (uint32_t)rlen)
+		return false;
+	return true;
+}
+
+// get_position (src/hash_align.c:1322-1467).  `rd` holds the read already
+// in the strand's orientation (reverse complement for str 1).  Seed hits
+// come from `pre` (one {start, count} per seed) when given, else are probed.
+__device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int rlen, DPair &P,
+				    int c, int str, int space, const uint2 *pre, bool score_only,
+				    GpWork &w, int &flags)
+{
+	DSlot &S = P.s[c][str];
+	const DSlot &Mt = P.s[c][1 - str];
+	int cur = 0, na = 0;
+	const uint32_t step = (uint32_t)(space < 0 ? -space : space);
+
+	int sj = 0;
+	for (uint32_t i = 0; i + KMER <= (uint32_t)rlen; i += step, ++sj) {
+		uint2 h = pre ? pre[sj] : probe(ix, kmer_at(rd, (int)i));
+		if (h.y == 0)
+			continue;
+		const uint2 *occ = ix.occ + h.x;
+		if (na == 0) {
+			uint32_t nh = h.y;
+			if (nh > (uint32_t)ACAP) {
+				flags |= F_ACAP;
+				nh = ACAP;
+			}
+			Anchors &A = w.a[cur];
+			for (uint32_t k = 0; k < nh; ++k) {
+				uint2 o = __ldg(occ + k);
+				A.t[k] = o.x;
+				A.tp[k] = o.y;
+				A.off[k] = i;
+			}
+			na = (int)nh;
+			continue;
+		}
+		na = merge_hits(w.a[cur], na, w.a[cur ^ 1], occ, h.y, i, flags);
+		cur ^= 1;
+	}
+	Anchors &A = w.a[cur];
+	uint32_t n1 = 0, max = 0, n;
+	if (na == 0)
+		goto miss;
+
+	// pass A, mate-guided (:1367-1390)
+	if (Mt.n > 0 && space < KMER && space > 0) {
+		const uint32_t mn = (uint32_t)Mt.n;
+		uint32_t k = 0;
+		max = (uint32_t)(rlen / 2);
+		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+			if (A.t[i] < Mt.t[k])
+				continue;
+			while (k < mn && A.t[i] > Mt.t[k])
+				++k;
+			if (k == mn)
+				break;
+			n = 1;
+			while (chain_next(A, na, i, n, rlen, false)) {
+				++i;
+				++n;
+			}
+			get_swalign(ix, rd, rlen, A, i + 1 - n, n, n1, max, S, score_only, w, flags);
+			for (; n > 0; --n)
+				A.off[i + 1 - n] = (uint32_t)rlen;
+		}
+	}
+	// pass B, chains of >= 2 anchors (:1392-1412)
+	if (n1 == 0) {
+		max = (uint32_t)(rlen / 2);
+		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+			if (A.off[i] == (uint32_t)rlen)
+				continue;
+			n = 1;
+			while (chain_next(A, na, i, n, rlen, true)) {
+				++i;
+				++n;
+			}
+			if (n < 2 && rlen / KMER > 2)
+				continue;
+			get_swalign(ix, rd, rlen, A, i - n + 1, n, n1, max, S, score_only, w, flags);
+		}
+	}
+	// pass C, singletons (:1414-1434)
+	if (n1 == 0 && space < KMER) {
+		max = (uint32_t)(rlen / 2);
+		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+			if (A.off[i] == (uint32_t)rlen)
+				continue;
+			n = 1;
+			while (chain_next(A, na, i, n, rlen, true)) {
+				++i;
+				++n;
+			}
+			if (n >= 2)
+				continue;
+			get_swalign(ix, rd, rlen, A, i, n, n1, max, S, score_only, w, flags);
+		}
+	}
+	if (n1 == 0)
+		goto miss;
+	if (n1 > (uint32_t)LCAP) {
+		flags |= F_LCAP;
+		n1 = LCAP;
+	}
+	for (uint32_t t = 0; t < n1; ++t) {
+		S.t[t] = A.t[t];
+		S.p[t] = (int32_t)A.tp[t];
+	}
+	S.n = (int32_t)n1;
+	S.err = (int32_t)max;
+	return;
+miss:
+	S.n = 0;
+	S.err = rlen;
+}
+
+// intersect2 list step (src/hash_align.c:1528-1556): returns the number of
+// pairs kept (lists compacted in place), 0 if none.
+__device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
+{
+	DSlot &A = P.s[c][0];
+	DSlot &B = P.s[c][1];
+	int i = 0, k = 0, n = 0;
+	while (i < A.n && k < B.n) {
+		if (A.t[i] < B.t[k]) {
+			++i;
+		} else if (A.t[i] > B.t[k]) {
+			++k;
+		} else {
+			int d = A.p[i] - B.p[k];
+			uint32_t dis = (uint32_t)(d < 0 ? -d : d);
+			if (dis <= add || add == 0) {
+				++n;
+				A.t[n - 1] = A.t[i];
+				A.p[n - 1] = A.p[i];
+				B.t[n - 1] = B.t[k];
+				B.p[n - 1] = B.p[k];
+				++i;
+				++k;
+			} else if (A.p[i] < B.p[k]) {
+				++i;
+			} else {
+				++k;
+			}
+		}
+	}
+	if (n > 0) {
+		A.n = B.n = n;
+		P.pair[c] = 2;
+	}
+	return n;
+}
+
+// ---------------------------------------------------------------------
+// Mate rescue DP: ssw_align (src/ssw.c:81-321), one thread per call.
+// Local SW on saturating u8 (+1 match incl. N==N, -2 mismatch, linear gap
+// 4), the full H matrix kept in HBM scratch for the quirky traceback.
+// H is stored column-major: column y (0..ref_len) holds rows 0..rstride-1.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ int mat_score(uint8_t a, uint8_t b)
+{
+	if (a == 4 || b == 4)
+		return 0;
+	return a == b ? 1 : -2;
+}
+
+struct SswWork {
+	uint8_t pc[MAX_READ + 4];    // previous column
+	uint8_t cc[MAX_READ + 4];    // current column
+};
+
+__device__ inline int ssw_align(const DevIndex &ix, uint32_t wstart, int ref_len, const uint8_t *rd,
+				int rlen, int &skip, DCig &cig, uint8_t *H, SswWork &w, int &flags)
+{
+	cig.n = cig.nm = 0;
+	const int rs = (rlen + 3) & ~3;
+	const uint8_t *rf = ix.code + wstart;
+	const uint8_t *ra = ix.seq + wstart;
+	for (int x = 0; x < rs; ++x)
+		w.pc[x] = 0;
+	for (int x = 0; x < rs; x += 4)
+		*reinterpret_cast<uint32_t *>(H + x) = 0u;
+	unsigned max = 0;
+	int end_ref = -1, pos_max = 0, end_read = rlen - 1;
+	int max_x = 0;
+	uint8_t *pc = w.pc, *cc = w.cc;
+	for (int y = 1; y <= ref_len; ++y) {
+		const uint8_t rc = rf[y - 1];
+		unsigned cmax = 0;
+		int cx = 0;
+		int f = 0;
+		unsigned dprev = 0;   // H[y-1][x-1]
+		uint32_t pack = 0;
+		uint8_t *Hc = H + (size_t)y * rs;
+		for (int x = 0; x < rs; ++x) {
+			unsigned v = 0;
+			unsigned up_prev = pc[x];
+			if (x < rlen) {
+				int h = (int)dprev + (rd[x] == rc ? 3 : 0);
+				if (h > 255)
+					h = 255;
+				h = h >= 2 ? h - 2 : 0;
+				int e = (int)up_prev >= 4 ? (int)up_prev - 4 : 0;
+				int vv = h > e ? h : e;
+				vv = vv > f ? vv : f;
+				v = (unsigned)vv;
+				f = vv >= 4 ? vv - 4 : 0;
+				if (v > cmax) {
+					cmax = v;
+					cx = x;
+				}
+			}
+			cc[x] = (uint8_t)v;
+			dprev = up_prev;
+			pack |= v << (8 * (x & 3));
+			if ((x & 3) == 3) {
+				*reinterpret_cast<uint32_t *>(Hc + x - 3) = pack;
+				pack = 0;
+			}
+		}
+		if (cmax > max) {
+			max = cmax;
+			end_ref = y - 1;
+			pos_max = y;
+			max_x = cx;
+		}
+		uint8_t *t = pc;
+		pc = cc;
+		cc = t;
+	}
+	(void)pos_max;
+	int begin_ref = end_ref;
+	int score = 0;
+	if (max < (unsigned)(rlen >> 2) || max == 0) {
+		score = rlen;
+		cig_add(cig, OP_S, (unsigned)rlen, nullptr, flags);
+		skip = begin_ref;
+		return score;
+	}
+	if (max_x < end_read)
+		end_read = max_x;
+	int x_pos = end_read, y_pos = end_ref + 1, begin_read = end_read;
+	int right = rlen - end_read - 1;
+	if (right > 0) {
+		if (right < 5) {
+			for (int i = rlen - 1, j = end_ref + right; i > end_read; --i, --j) {
+				if (j >= ref_len) {
+					cig_add(cig, OP_S, 1, nullptr, flags);
+					++score;
+				} else if (rd[i] == rf[j]) {
+					cig_add(cig, OP_M, 1, nullptr, flags);
+				} else {
+					cig_add(cig, OP_X, 1, ra + j, flags);
+					++score;
+				}
+			}
+		} else {
+			score += right;
+			cig_add(cig, OP_S, (unsigned)right, nullptr, flags);
+		}
+	}
+	auto HV = [&](int x, int y) -> int { return H[(size_t)y * rs + x]; };
+	int cur = HV(x_pos, y_pos), dir = 0;
+	for (;;) {
+		if (dir == 0) {
+			if (rd[begin_read] == rf[begin_ref]) {
+				cig_add(cig, OP_M, 1, nullptr, flags);
+			} else {
+				cig_add(cig, OP_X, 1, ra + begin_ref, flags);
+				++score;
+			}
+		} else if (dir == 1) {
+			++score;
+			cig_add(cig, OP_I, 1, nullptr, flags);
+		} else {
+			++score;
+			cig_add(cig, OP_D, 1, ra + begin_ref, flags);
+		}
+		if (x_pos == 0 || y_pos == 1)
+			break;
+		int diag = HV(x_pos - 1, y_pos - 1);
+		int up = HV(x_pos - 1, y_pos);
+		int left = HV(x_pos, y_pos - 1);
+		if (cur == diag + mat_score(rd[begin_read], rf[begin_ref])) {
+			if (!diag)
+				break;
+			cur = diag;
+			--begin_read; --begin_ref; --x_pos; --y_pos;
+			dir = 0;
+		} else if (cur == left - 4) {
+			if (!left)
+				break;
+			cur = left;
+			--y_pos; --begin_ref;
+			dir = 1;
+		} else {
+			if (!up)
+				break;
+			cur = up;
+			--x_pos; --begin_read;
+			dir = 2;
+		}
+	}
+	if (begin_read < 5) {
+		for (--begin_read, --begin_ref; begin_read >= 0; --begin_read, --begin_ref) {
+			if (begin_ref < 0) {
+				cig_add(cig, OP_S, 1, nullptr, flags);
+				++score;
+			} else if (rd[begin_read] == rf[begin_ref]) {
+				cig_add(cig, OP_M, 1, nullptr, flags);
+			} else {
+				cig_add(cig, OP_X, 1, ra + begin_ref, flags);
+				++score;
+			}
+		}
+	} else if (begin_read > 0) {
+		score += begin_read;
+		cig_add(cig, OP_S, (unsigned)begin_read, nullptr, flags);
+	}
+	skip = begin_ref;
+	return score;
+}
+
+}  // namespace hg

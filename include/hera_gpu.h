@@ -1,0 +1,220 @@
+/*
+ * hera_gpu.h -- C ABI of the B200 (sm_100a) read-alignment hot path for hera.
+ *
+ * The library replaces, batch-wise, the per-pair front half of hera's
+ * alignment worker: for every read pair it produces the two Candidate
+ * records exactly as hera leaves them after check_in_transcriptome and the
+ * two intersect2 calls (src/hash_align.c:1724-1733), and for every single
+ * read the Candidate after its two get_position calls
+ * (src/hash_align.c:1819-1823).  The host tail of align_pair_read
+ * (src/hash_align.c:1735-1811: pair choice, BAM records, add_class,
+ * counters) and everything around it stay hera's own C code.
+ *
+ * Plain C types and pointers only.  Every entry point returns 0 on success
+ * or a negative HERA_GPU_E* code; hera_gpu_last_error() describes the last
+ * failure on a context.  There is no CPU fallback: without a usable CUDA
+ * device every entry point fails with HERA_GPU_ENODEV.
+ */
+#ifndef HERA_GPU_H
+#define HERA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HERA_GPU_ABI_VERSION 1
+
+/* status codes */
+#define HERA_GPU_OK 0
+#define HERA_GPU_ENODEV (-1)      /* no CUDA device / driver */
+#define HERA_GPU_ECUDA (-2)       /* a CUDA call failed */
+#define HERA_GPU_ENOMEM (-3)      /* device or host allocation failed */
+#define HERA_GPU_EINVAL (-4)      /* bad argument (NULL, size, read too long) */
+#define HERA_GPU_ECAPACITY (-5)   /* a per-read capacity was exceeded */
+#define HERA_GPU_ETIMEOUT (-6)    /* a bounded device wait expired */
+
+/* Longest read the device path accepts (hera itself has no limit; reads
+ * longer than this are rejected with HERA_GPU_EINVAL). */
+#define HERA_GPU_MAX_READ 320
+
+/* ---- reference-layout types (identical in size and field order) ------- */
+
+/* struct read_inf, src/read.h:16-21 */
+typedef struct hera_read_inf {
+	char *seq;
+	char *name;
+	char *qual;
+	int32_t len;
+} hera_read_inf;
+
+/* Cigar, src/hash_align.h:82-88 (arrays malloc'ed, freed by free_cigar) */
+typedef struct hera_cigar {
+	unsigned short n_cigar;
+	unsigned short n_miss;
+	unsigned short *count;
+	char *type;
+	char *miss;
+} hera_cigar;
+
+/* Candidate, src/hash_align.h:90-97 (arrays malloc'ed, freed by
+ * destroy_candidate; pos/p are only allocated when n > 0) */
+typedef struct hera_candidate {
+	int *p[2];
+	unsigned int *pos[2];
+	unsigned int n[2];
+	int err[2];
+	hera_cigar *cigar[2];
+	int pair;
+} hera_candidate;
+
+/* Bucket, src/hash_align.h:138-142 */
+typedef struct hera_bucket {
+	uint64_t id;
+	uint32_t start;
+	uint32_t end;
+} hera_bucket;
+
+/* The loaded index as hera holds it after load_index
+ * (src/hash_align.c:1195-1234): Ref_inf (n, len, find, seq) and
+ * Kmer_hash (n[H] per-bucket counts, buckets back to back in bucket order,
+ * pos/p occurrence arrays).  Host memory; copied to the device. */
+typedef struct hera_gpu_index_view {
+	uint32_t n_trans;
+	const uint32_t *len;         /* REF_INF->len  [n_trans] */
+	const uint32_t *find;        /* REF_INF->find [n_trans] (exclusive ends) */
+	const char *seq;             /* REF_INF->seq  [find[n_trans-1]] */
+	const uint32_t *bucket_n;    /* KMER_HASH->n  [1<<27] */
+	const hera_bucket *buckets;  /* KMER_HASH->sentinel, sum(bucket_n) entries */
+	uint64_t n_buckets;
+	const uint32_t *pos;         /* KMER_HASH->pos [n_pos] */
+	const uint32_t *p;           /* KMER_HASH->p   [n_pos] */
+	uint32_t n_pos;
+} hera_gpu_index_view;
+
+/* ---- flat results ------------------------------------------------------ */
+
+/* One record per Candidate: two per pair ([2i] = r[0], [2i+1] = r[1]), one
+ * per single read.  List i of strand s is pos_pool/p_pool[list_off[s] ..
+ * +n[s]); CIGAR ops are op_pool[cig_off[s] .. +n_cigar[s]] encoded
+ * (count << 4) | op with op in "MIDNSHP=XB"; miss chars (reference bases of
+ * X and D runs) are miss_pool[miss_off[s] .. +n_miss[s]]. */
+typedef struct hera_cand_rec {
+	int32_t n[2];
+	int32_t err[2];
+	int32_t pair;
+	uint32_t list_off[2];
+	uint32_t cig_off[2];
+	uint32_t miss_off[2];
+	uint16_t n_cigar[2];
+	uint16_t n_miss[2];
+} hera_cand_rec;
+
+/* Caller-owned host buffers for flat results.  On return *_used hold the
+ * pool sizes; if a pool is too small the call returns HERA_GPU_ECAPACITY
+ * with *_used set to the sizes needed. */
+typedef struct hera_gpu_result {
+	hera_cand_rec *recs;
+	uint32_t *pos_pool;
+	int32_t *p_pool;
+	uint32_t *op_pool;
+	char *miss_pool;
+	uint64_t list_cap, op_cap, miss_cap;
+	uint64_t list_used, op_used, miss_used;
+} hera_gpu_result;
+
+/* Reads of one batch, back to back in host memory: read i is
+ * seq[off[i] .. off[i] + len[i]). */
+typedef struct hera_gpu_reads {
+	const char *seq;
+	const int64_t *off;
+	const int32_t *len;
+} hera_gpu_reads;
+
+typedef struct hera_gpu_ctx hera_gpu_ctx;
+
+typedef struct hera_gpu_options {
+	int device;              /* CUDA device ordinal */
+	uint32_t max_batch;      /* pairs (or single reads) per device pass; 0 = 1<<20 */
+	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 1 GiB */
+} hera_gpu_options;
+
+/* Per-stage device time of the last call, milliseconds (CUDA events). */
+typedef struct hera_gpu_timing {
+	float h2d_ms, seed_ms, position_ms, resolve_ms, rescue_ms, pack_ms, d2h_ms, total_ms;
+	uint32_t launches;       /* kernels launched by the last call */
+	uint32_t rescue_rounds;
+	uint64_t lookups;        /* seed-table lookups issued by seed_probe */
+} hera_gpu_timing;
+
+/* ---- entry points ------------------------------------------------------ */
+
+/* Library ABI version (HERA_GPU_ABI_VERSION). */
+int hera_gpu_abi_version(void);
+
+/* Create a context and copy the index to the device.  Replaces nothing in
+ * hera: called once after load_index (src/hash_align.c:1195) with the
+ * loaded KMER_HASH / REF_INF arrays.  `opt` may be NULL. */
+int hera_gpu_ctx_create(const hera_gpu_index_view *ix, const hera_gpu_options *opt,
+			hera_gpu_ctx **out);
+
+/* Release the context and its device memory. */
+void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx);
+
+/* Human-readable description of the last failure on `ctx` (never NULL). */
+const char *hera_gpu_last_error(const hera_gpu_ctx *ctx);
+
+/* Paired reads -> flat records.  Replaces, for `n` pairs, the calls
+ * check_in_transcriptome + intersect2 x2 made per pair by align_pair_read
+ * (src/hash_align.c:1728-1733).  write_bam is hera's WRITE_BAM global
+ * (src/hash_align.c:32; 1 = no `-w`, score-only gap DP; 0 = `-w`, full
+ * traceback).  r1/r2 sequences are read only. */
+int hera_gpu_align_pairs_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1,
+			      const hera_gpu_reads *r2, int32_t n, int write_bam,
+			      hera_gpu_result *out);
+
+/* Single reads -> flat records: the two get_position calls of
+ * align_single_read (src/hash_align.c:1822-1823). */
+int hera_gpu_align_single_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *reads,
+			       int32_t n, int write_bam, hera_gpu_result *out);
+
+/* Drop-in form of hera_gpu_align_pairs_flat for hera's worker loop
+ * (align_pool_pair, src/hash_align.c:1878-1929): reads as struct read_inf,
+ * results as heap-allocated Candidate pairs (out[2i] = r[0],
+ * out[2i+1] = r[1]) ready for the unchanged host tail; free each with
+ * hera's destroy_candidate (src/hash_align.c:973).  Like the reference,
+ * lower-case a/c/g/t in r1[i].seq and r2[i].seq become upper-case. */
+int hera_gpu_align_pairs(hera_gpu_ctx *ctx, hera_read_inf *r1, hera_read_inf *r2,
+			 int32_t n, int write_bam, hera_candidate **out);
+
+/* Drop-in form for align_pool_single (src/hash_align.c:1966-1998). */
+int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, int32_t n,
+			  int write_bam, hera_candidate **out);
+
+/* Device-resident batch (inputs already in HBM): the same computation as
+ * hera_gpu_align_pairs_flat on device pointers (seq, off, len for 2n reads:
+ * read 2i is mate 1 and read 2i+1 mate 2 of pair i; reads back to back with
+ * rising offsets; no read longer than max_read_len <= HERA_GPU_MAX_READ).
+ * Results stay on the device; hera_gpu_fetch_result copies them out.
+ * `stream` is a cudaStream_t (NULL = the context's own stream). */
+int hera_gpu_align_pairs_device(hera_gpu_ctx *ctx, const uint8_t *d_seq,
+				const int64_t *d_off, const int32_t *d_len,
+				int32_t n, int32_t max_read_len, int write_bam,
+				void *stream);
+
+/* Copy the results of the last device-resident call into `out`. */
+int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out);
+
+/* Per-stage timing of the last call on `ctx`. */
+int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+ * order work around the library's launches. */
+void *hera_gpu_stream(hera_gpu_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,52 @@
+"""Shared fixtures.  `-m gpu` tests need a CUDA device and the in-tree
+libhera_b200.so; everything else runs on CPU.  The oracle (oracle/_ref,
+built by `make -C oracle`) is the checker for both."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libhera_b200.so")
+
+
+def gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def config1():
+    """Config-1 shaped data: 2 Mbp genome, 200 genes, 500 isoforms."""
+    from hera_b200 import synth, index
+    ann = synth.make_annotation(seed=1, genome_len=2_000_000, n_genes=200, n_transcripts=500)
+    tx = synth.transcriptome(ann)
+    ix = index.build_index(tx)
+    return ann, tx, ix
+
+
+@pytest.fixture(scope="session")
+def oracle1(config1):
+    import oracle
+    if not os.path.exists(oracle.ORACLE_SO):
+        pytest.skip("oracle not built (make -C oracle)")
+    return oracle.Oracle(config1[2])
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx1(config1):
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ctx = api.Context(config1[2], max_batch=1 << 16)
+    yield ctx
+    ctx.close()
