@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the hera read-alignment hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config2] [--chunk 1000000] [--write-bam 1]
+
+A step is one pass of the hot path over one chunk of read pairs (default
+1M pairs of the transcriptome-scale workload).  `value` is device-timed
+throughput with the chunk already resident in HBM; `e2e` is the same metric
+through the public C ABI with host buffers (H2D of the reads and D2H of the
+Candidate records inside the timed region).  Under torchrun each rank runs a
+replica of the index on its own GPU over its own chunks (weak scaling, no
+data-path collective); the reported time is the max over ranks.
+
+`--impl reference` times the reference program's own CPU implementation of
+the same path (oracle/_ref/libhera_ref.so: check_in_transcriptome +
+intersect2 per pair) on all host cores over bounded samples of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "aligned read pairs/s"
+UNIT = "pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--chunk", type=int, default=1_000_000)
+    ap.add_argument("--distinct", type=int, default=3, help="distinct chunks generated per rank")
+    ap.add_argument("--write-bam", type=int, default=1, help="hera WRITE_BAM (1 = no -w)")
+    ap.add_argument("--cpu-sample", type=int, default=200_000, help="pairs per CPU-baseline slice")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle samples while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_chunks(name, ann, tx, chunk, distinct, seed0):
+    from hera_b200 import workloads
+    out = []
+    for k in range(distinct):
+        t = time.time()
+        r1, r2 = workloads.pairs(name, ann, tx, chunk, seed0 + k)
+        out.append((r1, r2))
+        log(f"chunk {k}: {chunk} pairs in {time.time() - t:.1f}s")
+    return out
+
+
+def cpu_baseline(ix, chunks, sample: int, write_bam: int, target_s: float = 10.0):
+    """The reference's own code on all host cores over a bounded sample."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    ref = oracle.Reference(ix)
+    threads = os.cpu_count() or 1
+    done, elapsed = 0, 0.0
+    k = 0
+    while elapsed < target_s and k < 4 * len(chunks):
+        r1, r2 = chunks[k % len(chunks)]
+        lo = (k // len(chunks)) * sample
+        if lo + sample > r1.n:
+            break
+        idx = np.arange(lo, lo + sample)
+        a, b = r1.subset(idx), r2.subset(idx)
+        t = time.perf_counter()
+        ref.align_pairs_mt(a, b, write_bam, threads)
+        elapsed += time.perf_counter() - t
+        done += sample
+        k += 1
+    return {"value": done / elapsed, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{done} pairs of the workload in slices of {sample} "
+                      f"(reference check_in_transcriptome+intersect2, {threads} threads, "
+                      f"{elapsed:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from hera_b200 import workloads
+    import oracle
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhera_ref.so not built"}))
+        return
+    t = time.time()
+    ann, tx, ix = workloads.build(args.workload, device=None if args.workload != "config2" else _maybe_cuda())
+    log(f"index {time.time() - t:.1f}s")
+    ref = oracle.Reference(ix)
+    threads = os.cpu_count() or 1
+    sample = args.cpu_sample
+    chunks = make_chunks(args.workload, ann, tx, sample, min(args.distinct, args.steps + args.warmup), 1000)
+    times = []
+    for s in range(args.warmup + args.steps):
+        r1, r2 = chunks[s % len(chunks)]
+        a, b = r1.copy(), r2.copy()
+        t0 = time.perf_counter()
+        ref.align_pairs_mt(a, b, args.write_bam, threads)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = sample * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {workloads.DESCRIPTION[args.workload]}",
+                   "pairs_per_step": sample, "write_bam": args.write_bam},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{sample} pairs per step, reference code on {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _maybe_cuda():
+    try:
+        import torch
+        return "cuda" if torch.cuda.is_available() else None
+    except Exception:
+        return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    import torch.distributed as dist
+    from hera_b200 import api, workloads
+    if not torch.cuda.is_available():
+        print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
+        sys.exit(1)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    t = time.time()
+    ann, tx, ix = workloads.build(args.workload, device=f"cuda:{local}")
+    log(f"[{rank}] index: {ix.n_trans} transcripts, {ix.buckets.shape[0]} k-mers, "
+        f"{ix.n_pos} occurrences in {time.time() - t:.1f}s")
+    ctx = api.Context(ix, device=local, max_batch=args.chunk)
+    chunks = make_chunks(args.workload, ann, tx, args.chunk, args.distinct, 100 + 1000 * rank)
+
+    # device-resident copies (mates interleaved) for the `value` measurement
+    dev = []
+    max_len = 0
+    for r1, r2 in chunks:
+        seq, off, lens = workloads.interleave(r1, r2)
+        max_len = max(max_len, int(lens.max()))
+        dev.append((torch.from_numpy(seq).cuda(), torch.from_numpy(off).cuda(),
+                    torch.from_numpy(lens).cuda()))
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step(i):
+        s, o, ln = dev[i % len(dev)]
+        ctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
+                               args.write_bam, ctx.stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches = 0
+    stage = {"seed_ms": 0.0, "position_ms": 0.0, "resolve_ms": 0.0, "rescue_ms": 0.0, "pack_ms": 0.0}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(i)
+        tm = ctx.timing()
+        launches += int(tm["launches"])
+        for k in stage:
+            stage[k] += float(tm[k])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    total_pairs = args.chunk * args.steps * world
+    value = total_pairs / (ms / 1000.0)
+
+    # end to end through the public C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        r1, r2 = chunks[0]
+        ctx.align_pairs(r1, r2, args.write_bam)   # warm the staging buffers
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        h2d = d2h = 0
+        for i in range(args.steps):
+            r1, r2 = chunks[i % len(chunks)]
+            res = ctx.align_pairs(r1, r2, args.write_bam)
+            h2d += int(r1.len.sum() + r2.len.sum()) + 12 * 2 * r1.n
+            d2h += (res.recs.nbytes + 8 * int(res.c.list_used) + 4 * int(res.c.op_used)
+                    + int(res.c.miss_used))
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": args.chunk * args.steps * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(ix, chunks, args.cpu_sample, args.write_bam)
+        except Exception as e:   # the checker is optional on a box without it
+            log(f"cpu baseline failed: {e}")
+
+    # roofline of the dominant stage
+    dom = max(stage, key=stage.get)
+    roof = roofline(dom, stage, args, ix)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {workloads.DESCRIPTION[args.workload]}",
+                       "pairs_per_step": args.chunk, "write_bam": args.write_bam,
+                       "path": "plain (one pipeline pass per chunk)",
+                       "l2": "inputs larger than L2 (reads 200 MB/step, index in HBM)",
+                       "parallelism": f"replicas x{world}"},
+            "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def roofline(dom, stage, args, ix):
+    """Roofline of the dominant stage against the measured HBM copy peak."""
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    ms = stage[dom] / args.steps
+    return {"kernel": dom.replace("_ms", ""), "bound": "hbm", "achieved": None, "peak": hbm,
+            "unit": "GB/s", "frac": None, "traffic": None, "peak_source": src,
+            "ms_per_step": ms}
+
+
+if __name__ == "__main__":
+    main()

@@ -680,11 +680,19 @@ __device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
 }
 
 // ---------------------------------------------------------------------
-// Mate rescue DP: ssw_align (src/ssw.c:81-321), one thread per call.
-// Local SW on saturating u8 (+1 match incl. N==N, -2 mismatch, linear gap
-// 4), the full H matrix kept in HBM scratch for the quirky traceback.
-// H is stored column-major: column y (0..ref_len) holds rows 0..rstride-1.
+// Mate rescue DP: ssw_align (src/ssw.c:81-321), one warp per call.
+//
+// Local SW on saturating u8: H = max(0, min(255, diag + 3*[codes equal]) - 2,
+// left - 4, up - 4) (+1 match incl. N==N, -2 mismatch, linear gap 4), which
+// is what the reference's striped SSE2 loop with lazy-F converges to.  The
+// warp sweeps anti-diagonally: lane l owns read rows [l*R, l*R+R) and works
+// on column y = t - l + 1 at step t; the row above its block comes from lane
+// l-1 by shuffle one step later.  H is kept in HBM scratch in step-major
+// order (coalesced stores) for the reference's traceback, which one lane
+// then replays.
 // ---------------------------------------------------------------------
+constexpr int SSW_RMAX = (MAX_READ + 31) / 32;   // rows per lane, <= 10
+
 __device__ __forceinline__ int mat_score(uint8_t a, uint8_t b)
 {
 	if (a == 4 || b == 4)
@@ -692,161 +700,209 @@ __device__ __forceinline__ int mat_score(uint8_t a, uint8_t b)
 	return a == b ? 1 : -2;
 }
 
-struct SswWork {
-	uint8_t pc[MAX_READ + 4];    // previous column
-	uint8_t cc[MAX_READ + 4];    // current column
+struct SswOut {
+	int32_t score, skip, pstart, ok;
+	DCig cig;
 };
 
-__device__ inline int ssw_align(const DevIndex &ix, uint32_t wstart, int ref_len, const uint8_t *rd,
-				int rlen, int &skip, DCig &cig, uint8_t *H, SswWork &w, int &flags)
+// oriented read code x of read (o, L)
+__device__ __forceinline__ uint8_t read_code(const uint8_t *code, int64_t o, int L, int orient, int x)
 {
-	cig.n = cig.nm = 0;
-	const int rs = (rlen + 3) & ~3;
+	return orient ? comp_code(code[o + L - 1 - x]) : code[o + x];
+}
+
+// bytes of HBM scratch one call needs
+__host__ __device__ inline size_t ssw_scratch_bytes(int max_len)
+{
+	const int R = (max_len + 31) / 32;
+	const int Rp = (R + 3) & ~3;
+	return (size_t)(MAX_FRAG + 32) * 32 * (size_t)(Rp ? Rp : 4);
+}
+
+// Called by all 32 lanes of a warp.  Fills `out` (lane 0 writes).
+__device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code,
+				int64_t roff, int L, int orient, int start, uint32_t tl,
+				uint8_t *__restrict__ Hs, SswOut &out, int &flags)
+{
+	const unsigned FULL = 0xffffffffu;
+	const int lane = threadIdx.x & 31;
+	const int R = (L + 31) / 32;
+	const int Rp = (R + 3) & ~3;
+	const int x0 = lane * R;
+	uint8_t rdl[SSW_RMAX];
+	int Hl[SSW_RMAX];
+#pragma unroll
+	for (int r = 0; r < SSW_RMAX; ++r) {
+		const int x = x0 + r;
+		rdl[r] = (r < R && x < L) ? read_code(code, roff, L, orient, x) : (uint8_t)5;
+		Hl[r] = 0;
+	}
+	int bot = 0, up_prev = 0;
+	int best_v = 0, best_y = 0, best_x = 0;
 	const uint8_t *rf = ix.code + wstart;
-	const uint8_t *ra = ix.seq + wstart;
-	for (int x = 0; x < rs; ++x)
-		w.pc[x] = 0;
-	for (int x = 0; x < rs; x += 4)
-		*reinterpret_cast<uint32_t *>(H + x) = 0u;
-	unsigned max = 0;
-	int end_ref = -1, pos_max = 0, end_read = rlen - 1;
-	int max_x = 0;
-	uint8_t *pc = w.pc, *cc = w.cc;
-	for (int y = 1; y <= ref_len; ++y) {
-		const uint8_t rc = rf[y - 1];
-		unsigned cmax = 0;
-		int cx = 0;
-		int f = 0;
-		unsigned dprev = 0;   // H[y-1][x-1]
-		uint32_t pack = 0;
-		uint8_t *Hc = H + (size_t)y * rs;
-		for (int x = 0; x < rs; ++x) {
-			unsigned v = 0;
-			unsigned up_prev = pc[x];
-			if (x < rlen) {
-				int h = (int)dprev + (rd[x] == rc ? 3 : 0);
-				if (h > 255)
-					h = 255;
-				h = h >= 2 ? h - 2 : 0;
-				int e = (int)up_prev >= 4 ? (int)up_prev - 4 : 0;
-				int vv = h > e ? h : e;
-				vv = vv > f ? vv : f;
-				v = (unsigned)vv;
-				f = vv >= 4 ? vv - 4 : 0;
-				if (v > cmax) {
-					cmax = v;
-					cx = x;
+	const int steps = ln > 0 ? ln + 31 : 0;
+	for (int t = 0; t < steps; ++t) {
+		const int y = t - lane + 1;
+		int up_in = __shfl_up_sync(FULL, bot, 1);
+		if (lane == 0)
+			up_in = 0;
+		const int diag_in = up_prev;
+		up_prev = up_in;
+		if (y >= 1 && y <= ln) {
+			const uint8_t rc = rf[y - 1];
+			int d = diag_in, up = up_in;
+			uint32_t pack[SSW_RMAX / 4 + 1];
+#pragma unroll
+			for (int w = 0; w < SSW_RMAX / 4 + 1; ++w)
+				pack[w] = 0;
+#pragma unroll
+			for (int r = 0; r < SSW_RMAX; ++r) {
+				if (r < R) {
+					const int x = x0 + r;
+					const int left = Hl[r];
+					int e = left - 4;
+					e = e > 0 ? e : 0;
+					int f = up - 4;
+					f = f > 0 ? f : 0;
+					int h = d + (rdl[r] == rc ? 3 : 0);
+					h = h < 255 ? h : 255;
+					h = h > 2 ? h - 2 : 0;
+					int v = h > e ? h : e;
+					v = v > f ? v : f;
+					if (x >= L)
+						v = 0;
+					d = left;
+					Hl[r] = v;
+					up = v;
+					if (v > best_v) {
+						best_v = v;
+						best_y = y;
+						best_x = x;
+					}
+					pack[r >> 2] |= (uint32_t)v << (8 * (r & 3));
 				}
 			}
-			cc[x] = (uint8_t)v;
-			dprev = up_prev;
-			pack |= v << (8 * (x & 3));
-			if ((x & 3) == 3) {
-				*reinterpret_cast<uint32_t *>(Hc + x - 3) = pack;
-				pack = 0;
+			bot = Hl[R - 1];
+			uint32_t *dst = reinterpret_cast<uint32_t *>(Hs + ((size_t)t * 32 + lane) * Rp);
+#pragma unroll
+			for (int w = 0; w < SSW_RMAX / 4 + 1; ++w)
+				if (w * 4 < Rp)
+					dst[w] = pack[w];
+		} else {
+			bot = 0;
+		}
+	}
+	// max over all cells; first column reaching it; first row in that column
+	const int max_v = __reduce_max_sync(FULL, best_v);
+	const int min_y = __reduce_min_sync(FULL, best_v == max_v ? best_y : 0x7fffffff);
+	const int min_x = __reduce_min_sync(FULL, (best_v == max_v && best_y == min_y) ? best_x : 0x7fffffff);
+	__syncwarp();
+	if (lane != 0)
+		return;
+
+	DCig &cig = out.cig;
+	cig.n = cig.nm = 0;
+	const uint8_t *ra = ix.seq + wstart;
+	auto HV = [&](int x, int yy) -> int {
+		if (yy == 0)
+			return 0;
+		const int l = x / R, r = x - l * R;
+		return Hs[((size_t)(yy + l - 1) * 32 + l) * Rp + r];
+	};
+	auto RD = [&](int x) -> uint8_t { return read_code(code, roff, L, orient, x); };
+	const int end_ref = max_v > 0 ? min_y - 1 : -1;
+	int begin_ref = end_ref, score = 0, end_read = L - 1;
+	if (max_v < (L >> 2) || max_v == 0) {
+		score = L;
+		cig_add(cig, OP_S, (unsigned)L, nullptr, flags);
+	} else {
+		if (min_x < end_read)
+			end_read = min_x;
+		int x_pos = end_read, y_pos = end_ref + 1, begin_read = end_read;
+		const int right = L - end_read - 1;
+		if (right > 0) {
+			if (right < 5) {
+				for (int i = L - 1, j = end_ref + right; i > end_read; --i, --j) {
+					if (j >= ln) {
+						cig_add(cig, OP_S, 1, nullptr, flags);
+						++score;
+					} else if (RD(i) == rf[j]) {
+						cig_add(cig, OP_M, 1, nullptr, flags);
+					} else {
+						cig_add(cig, OP_X, 1, ra + j, flags);
+						++score;
+					}
+				}
+			} else {
+				score += right;
+				cig_add(cig, OP_S, (unsigned)right, nullptr, flags);
 			}
 		}
-		if (cmax > max) {
-			max = cmax;
-			end_ref = y - 1;
-			pos_max = y;
-			max_x = cx;
-		}
-		uint8_t *t = pc;
-		pc = cc;
-		cc = t;
-	}
-	(void)pos_max;
-	int begin_ref = end_ref;
-	int score = 0;
-	if (max < (unsigned)(rlen >> 2) || max == 0) {
-		score = rlen;
-		cig_add(cig, OP_S, (unsigned)rlen, nullptr, flags);
-		skip = begin_ref;
-		return score;
-	}
-	if (max_x < end_read)
-		end_read = max_x;
-	int x_pos = end_read, y_pos = end_ref + 1, begin_read = end_read;
-	int right = rlen - end_read - 1;
-	if (right > 0) {
-		if (right < 5) {
-			for (int i = rlen - 1, j = end_ref + right; i > end_read; --i, --j) {
-				if (j >= ref_len) {
-					cig_add(cig, OP_S, 1, nullptr, flags);
-					++score;
-				} else if (rd[i] == rf[j]) {
+		int cur = HV(x_pos, y_pos), dir = 0;
+		for (;;) {
+			const uint8_t qb = RD(begin_read), rb = rf[begin_ref];
+			if (dir == 0) {
+				if (qb == rb) {
 					cig_add(cig, OP_M, 1, nullptr, flags);
 				} else {
-					cig_add(cig, OP_X, 1, ra + j, flags);
+					cig_add(cig, OP_X, 1, ra + begin_ref, flags);
+					++score;
+				}
+			} else if (dir == 1) {   // a step along the reference
+				++score;
+				cig_add(cig, OP_I, 1, nullptr, flags);
+			} else {                 // a step along the read
+				++score;
+				cig_add(cig, OP_D, 1, ra + begin_ref, flags);
+			}
+			if (x_pos == 0 || y_pos == 1)
+				break;
+			const int diag = HV(x_pos - 1, y_pos - 1);
+			const int up = HV(x_pos - 1, y_pos);
+			const int left = HV(x_pos, y_pos - 1);
+			if (cur == diag + mat_score(qb, rb)) {
+				if (!diag)
+					break;
+				cur = diag;
+				--begin_read; --begin_ref; --x_pos; --y_pos;
+				dir = 0;
+			} else if (cur == left - 4) {
+				if (!left)
+					break;
+				cur = left;
+				--y_pos; --begin_ref;
+				dir = 1;
+			} else {
+				if (!up)
+					break;
+				cur = up;
+				--x_pos; --begin_read;
+				dir = 2;
+			}
+		}
+		if (begin_read < 5) {
+			for (--begin_read, --begin_ref; begin_read >= 0; --begin_read, --begin_ref) {
+				if (begin_ref < 0) {
+					cig_add(cig, OP_S, 1, nullptr, flags);
+					++score;
+				} else if (RD(begin_read) == rf[begin_ref]) {
+					cig_add(cig, OP_M, 1, nullptr, flags);
+				} else {
+					cig_add(cig, OP_X, 1, ra + begin_ref, flags);
 					++score;
 				}
 			}
-		} else {
-			score += right;
-			cig_add(cig, OP_S, (unsigned)right, nullptr, flags);
+		} else if (begin_read > 0) {
+			score += begin_read;
+			cig_add(cig, OP_S, (unsigned)begin_read, nullptr, flags);
 		}
 	}
-	auto HV = [&](int x, int y) -> int { return H[(size_t)y * rs + x]; };
-	int cur = HV(x_pos, y_pos), dir = 0;
-	for (;;) {
-		if (dir == 0) {
-			if (rd[begin_read] == rf[begin_ref]) {
-				cig_add(cig, OP_M, 1, nullptr, flags);
-			} else {
-				cig_add(cig, OP_X, 1, ra + begin_ref, flags);
-				++score;
-			}
-		} else if (dir == 1) {
-			++score;
-			cig_add(cig, OP_I, 1, nullptr, flags);
-		} else {
-			++score;
-			cig_add(cig, OP_D, 1, ra + begin_ref, flags);
-		}
-		if (x_pos == 0 || y_pos == 1)
-			break;
-		int diag = HV(x_pos - 1, y_pos - 1);
-		int up = HV(x_pos - 1, y_pos);
-		int left = HV(x_pos, y_pos - 1);
-		if (cur == diag + mat_score(rd[begin_read], rf[begin_ref])) {
-			if (!diag)
-				break;
-			cur = diag;
-			--begin_read; --begin_ref; --x_pos; --y_pos;
-			dir = 0;
-		} else if (cur == left - 4) {
-			if (!left)
-				break;
-			cur = left;
-			--y_pos; --begin_ref;
-			dir = 1;
-		} else {
-			if (!up)
-				break;
-			cur = up;
-			--x_pos; --begin_read;
-			dir = 2;
-		}
-	}
-	if (begin_read < 5) {
-		for (--begin_read, --begin_ref; begin_read >= 0; --begin_read, --begin_ref) {
-			if (begin_ref < 0) {
-				cig_add(cig, OP_S, 1, nullptr, flags);
-				++score;
-			} else if (rd[begin_read] == rf[begin_ref]) {
-				cig_add(cig, OP_M, 1, nullptr, flags);
-			} else {
-				cig_add(cig, OP_X, 1, ra + begin_ref, flags);
-				++score;
-			}
-		}
-	} else if (begin_read > 0) {
-		score += begin_read;
-		cig_add(cig, OP_S, (unsigned)begin_read, nullptr, flags);
-	}
-	skip = begin_ref;
-	return score;
+	const int skip = begin_ref;
+	out.score = score;
+	out.skip = skip;
+	out.pstart = start + skip;
+	// acceptance test of re_mapSW (src/hash_align.c:788-792)
+	out.ok = !(score > L / 2 || start + skip < 0 || (uint32_t)(start + skip + L) > tl);
 }
 
 }  // namespace hg

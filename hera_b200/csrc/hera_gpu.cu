@@ -7,8 +7,9 @@
 //   k_position   the four independent space-31 get_position calls per pair
 //   k_resolve    per-pair control flow (retries, get_position2, intersect2,
 //                re_map) up to the point a mate rescue is needed
-//   k_rescue     re_mapSW: ssw_align over each mate hit; rounds of
-//                k_resolve/k_rescue alternate until no pair is waiting
+//   k_rescue_*   re_mapSW: one warp-wide ssw_align per (request, mate hit),
+//                then per-request selection; rounds of k_resolve and the
+//                rescue alternate until no pair is waiting
 //   k_count/k_emit  compact the Candidate records into flat pools
 #include "hera_device.cuh"
 #include "../../include/hera_gpu.h"
@@ -250,9 +251,60 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 	}
 }
 
-// re_mapSW (src/hash_align.c:762-846) for one queued request
-__global__ void __launch_bounds__(TPB) k_rescue(Batch b, const RmReq *__restrict__ q, int nq,
-						 uint8_t *__restrict__ scratch, size_t per)
+// re_mapSW (src/hash_align.c:762-846), in three steps.
+// 1) one ssw_align call per (queued request, mate hit)
+__global__ void k_rescue_expand(Batch b, const RmReq *__restrict__ q, int nq, int2 *__restrict__ calls,
+				int *__restrict__ base, int *__restrict__ ncalls)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= nq)
+		return;
+	const RmReq rq = q[t];
+	const int n = b.P[rq.pair].s[rq.c][1 - rq.str].n;
+	const int at = atomicAdd(ncalls, n);
+	base[t] = at;
+	for (int i = 0; i < n; ++i)
+		calls[at + i] = make_int2(t, i);
+}
+
+// 2) one warp per call: local SW over the MAX_FRAG window at the mate hit
+__global__ void __launch_bounds__(128) k_rescue_sw(Batch b, const RmReq *__restrict__ q,
+						    const int2 *__restrict__ calls, int c0, int nc,
+						    SswOut *__restrict__ out, uint8_t *__restrict__ scratch,
+						    size_t per)
+{
+	const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // warp within launch
+	if (wl >= nc)
+		return;
+	const int2 cl = calls[c0 + wl];
+	const RmReq rq = q[cl.x];
+	const DPair &P = b.P[rq.pair];
+	const int c = rq.c, str = rq.str;
+	const int type = str == 0 ? -1 : 1;
+	const int ri = 2 * rq.pair + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	const DSlot &M = P.s[c][1 - str];
+	const uint32_t tr = M.t[cl.y];
+	const uint32_t tl = __ldg(b.ix.tlen + tr);
+	int start = M.p[cl.y] + (type > 0 ? 0 : L - MAX_FRAG);
+	if (start < 0)
+		start = 0;
+	int ln = MAX_FRAG;
+	if ((uint32_t)(start + MAX_FRAG) > tl)
+		ln = (int)tl - start;
+	if (ln < 0)
+		ln = 0;
+	int flags = 0;
+	ssw_warp(b.ix, __ldg(b.ix.tstart + tr) + (uint32_t)start, ln, b.code, b.off[ri], L, str, start, tl,
+		 scratch + (size_t)wl * per, out[c0 + wl], flags);
+	if ((threadIdx.x & 31) == 0)
+		flag(b.flags, flags);
+}
+
+// 3) per request: min score wins, ties append in hit order; the mate's list
+// is compacted to the rescued subset (src/hash_align.c:794-845)
+__global__ void k_rescue_fin(Batch b, const RmReq *__restrict__ q, int nq, const int *__restrict__ base,
+			     const SswOut *__restrict__ out)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= nq)
@@ -260,52 +312,29 @@ __global__ void __launch_bounds__(TPB) k_rescue(Batch b, const RmReq *__restrict
 	const RmReq rq = q[t];
 	DPair &P = b.P[rq.pair];
 	const int c = rq.c, str = rq.str;
-	const int type = str == 0 ? -1 : 1;
-	const int ri = 2 * rq.pair + ((c ^ str) == 0 ? 0 : 1);
-	uint8_t rd[MAX_READ];
-	SswWork sw;
-	DCig best, cur;
-	int flags = 0;
-	const int L = load_read(b, ri, str, rd);
 	DSlot &S = P.s[c][str];
 	DSlot &M = P.s[c][1 - str];
-	uint8_t *H = scratch + (size_t)t * per;
-	const int range = type > 0 ? 0 : L - MAX_FRAG;
-	int new_n = 0, score2 = 0;
-	best.n = best.nm = 0;
-	for (int i = 0; i < M.n; ++i) {
+	const int n = M.n, b0 = base[t];
+	int new_n = 0, score2 = 0, best = -1;
+	for (int i = 0; i < n; ++i) {
+		const SswOut &o = out[b0 + i];
+		if (!o.ok)
+			continue;
 		const uint32_t tr = M.t[i];
-		const uint32_t tl = __ldg(b.ix.tlen + tr);
-		int start = M.p[i] + range;
-		if (start < 0)
-			start = 0;
-		int ln = MAX_FRAG;
-		if ((uint32_t)(start + MAX_FRAG) > tl)
-			ln = (int)tl - start;
-		if (ln < 0)
-			ln = 0;
-		if ((size_t)(ln + 1) * (size_t)((L + 3) & ~3) > per) {
-			flags |= F_SCRATCH;
-			continue;
-		}
-		int skip = 0;
-		const int score1 = ssw_align(b.ix, __ldg(b.ix.tstart + tr) + (uint32_t)start, ln, rd, L,
-					     skip, cur, H, sw, flags);
-		if (score1 > L / 2 || start + skip < 0 || (uint32_t)(start + skip + L) > tl)
-			continue;
-		if (new_n == 0 || score1 < score2) {
-			cig_copy(best, cur);
-			score2 = score1;
-			M.t[0] = M.t[i];
-			M.p[0] = M.p[i];
+		const int32_t mp = M.p[i];
+		if (new_n == 0 || o.score < score2) {
+			best = i;
+			score2 = o.score;
+			M.t[0] = tr;
+			M.p[0] = mp;
 			S.t[0] = tr;
-			S.p[0] = start + skip;
+			S.p[0] = o.pstart;
 			new_n = 1;
-		} else if (score1 == score2) {
-			M.t[new_n] = M.t[i];
-			M.p[new_n] = M.p[i];
+		} else if (o.score == score2) {
+			M.t[new_n] = tr;
+			M.p[new_n] = mp;
 			S.t[new_n] = tr;
-			S.p[new_n] = start + skip;
+			S.p[new_n] = o.pstart;
 			++new_n;
 		}
 	}
@@ -313,11 +342,10 @@ __global__ void __launch_bounds__(TPB) k_rescue(Batch b, const RmReq *__restrict
 	if (new_n > 0) {
 		M.n = S.n = new_n;
 		S.err = score2;
-		if (type <= 0)
-			cig_reverse(best);
-		cig_copy(S.cig, best);
+		cig_copy(S.cig, out[b0 + best].cig);
+		if (str == 0)   // type <= 0: CIGAR reversed (:839-840)
+			cig_reverse(S.cig);
 	}
-	flag(b.flags, flags);
 }
 
 // align_single_read front half (src/hash_align.c:1822-1823)
@@ -473,7 +501,7 @@ struct hera_gpu_ctx {
 	uint8_t *d_seq = nullptr, *d_tcode = nullptr;
 	uint32_t *d_tlen = nullptr, *d_tstart = nullptr;
 	uint32_t max_batch = 1u << 20;
-	uint64_t scratch_bytes = 1ull << 30;
+	uint64_t scratch_bytes = 2ull << 30;
 
 	// per-batch device buffers
 	DBuf<uint8_t> seq, code;
@@ -486,6 +514,9 @@ struct hera_gpu_ctx {
 	DBuf<uint32_t> cnt;     // 3 * (items+1) counts, then 3 * (items+1) offsets
 	DBuf<uint8_t> cub_tmp;
 	DBuf<uint8_t> scratch;
+	DBuf<int2> calls;
+	DBuf<int> rq_base;
+	DBuf<SswOut> ssw_out;
 	DBuf<hera_cand_rec> recs;
 	DBuf<uint32_t> pos_pool, op_pool;
 	DBuf<int32_t> p_pool;
@@ -571,6 +602,7 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	ctx->seq.release(); ctx->code.release(); ctx->off.release(); ctx->len.release();
 	ctx->hits.release(); ctx->pairs.release(); ctx->q[0].release(); ctx->q[1].release();
 	ctx->counters.release(); ctx->cnt.release(); ctx->cub_tmp.release(); ctx->scratch.release();
+	ctx->calls.release(); ctx->rq_base.release(); ctx->ssw_out.release();
 	ctx->recs.release(); ctx->pos_pool.release(); ctx->op_pool.release(); ctx->p_pool.release();
 	ctx->miss_pool.release();
 	ctx->h_seq.release(); ctx->h_off.release(); ctx->h_len.release(); ctx->h_small.release();
@@ -748,19 +780,35 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 			if (nq == 0)
 				break;
 			++rounds;
-			const size_t per = (size_t)(MAX_FRAG + 1) * (size_t)((max_len + 3) & ~3);
+			// expand requests into calls
+			CK(ctx->calls.ensure((size_t)nq * LCAP), "rescue calls");
+			CK(ctx->rq_base.ensure(nq), "rescue bases");
+			int *d_nc = ctx->counters.p + 4;
+			CK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
+			cudaEventRecord(e0, st);
+			k_rescue_expand<<<blocks_for(nq, 256), 256, 0, st>>>(b, ctx->q[qi].p, nq, ctx->calls.p,
+									      ctx->rq_base.p, d_nc);
+			++launches;
+			CK(cudaMemcpyAsync(ctx->h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
+			CK(cudaStreamSynchronize(st), "rescue expand");
+			const int ncalls = ctx->h_small.p[1];
+			CK(ctx->ssw_out.ensure(ncalls + 1), "rescue outputs");
+			const size_t per = ssw_scratch_bytes(max_len);
 			size_t slots = ctx->scratch_bytes / per;
 			if (slots < 1)
 				slots = 1;
-			if (slots > (size_t)nq)
-				slots = (size_t)nq;
+			if (slots > (size_t)ncalls)
+				slots = (size_t)(ncalls > 0 ? ncalls : 1);
 			CK(ctx->scratch.ensure(slots * per), "rescue scratch");
-			cudaEventRecord(e0, st);
-			for (int s0 = 0; s0 < nq; s0 += (int)slots) {
-				const int m = (int)((size_t)(nq - s0) < slots ? (size_t)(nq - s0) : slots);
-				k_rescue<<<blocks_for(m), TPB, 0, st>>>(b, ctx->q[qi].p + s0, m, ctx->scratch.p, per);
+			for (int c0 = 0; c0 < ncalls; c0 += (int)slots) {
+				const int m = (int)((size_t)(ncalls - c0) < slots ? (size_t)(ncalls - c0) : slots);
+				k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, ctx->q[qi].p, ctx->calls.p, c0, m,
+											 ctx->ssw_out.p, ctx->scratch.p, per);
 				++launches;
 			}
+			k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, ctx->q[qi].p, nq, ctx->rq_base.p,
+									   ctx->ssw_out.p);
+			++launches;
 			cudaEventRecord(e1, st);
 			CK(cudaStreamSynchronize(st), "rescue");
 			cudaEventElapsedTime(&ms, e0, e1);

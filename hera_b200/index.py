@@ -102,24 +102,77 @@ def _occurrences(seq: np.ndarray, length: np.ndarray, find: np.ndarray):
     return ids[keep], tid[keep], off[keep].astype(np.uint32)
 
 
-def _stable_order(composite: np.ndarray, device: Optional[str]) -> np.ndarray:
-    if device is not None and device.startswith("cuda"):
-        import torch
-        t = torch.from_numpy(composite.view(np.int64)).to(device)
-        _, order = torch.sort(t, stable=True)
-        return order.cpu().numpy()
-    return np.argsort(composite, kind="stable")
+def _build_index_torch(tx, device: str) -> HeraIndex:
+    """Same layout as build_index, computed with torch on a GPU (index
+    construction is set-up work, not the hot path)."""
+    import torch
+    dev = torch.device(device)
+    seq = torch.from_numpy(np.ascontiguousarray(tx.seq)).to(dev)
+    lut = torch.from_numpy(_CODE & np.uint8(3)).to(dev)
+    c = lut[seq.long()].long()
+    n = c.shape[0]
+
+    def shifted(a, k):
+        out = torch.zeros_like(a)
+        if k < n:
+            out[k:] = a[:n - k]
+        return out
+
+    w1 = c
+    w2 = (shifted(w1, 1) << 2) | w1
+    w4 = (shifted(w2, 2) << 4) | w2
+    w8 = (shifted(w4, 4) << 8) | w4
+    w16 = (shifted(w8, 8) << 16) | w8
+    ids = ((shifted(w16, 15) << 30) | (shifted(w8, 7) << 14) | (shifted(w4, 3) << 6) |
+           (shifted(w2, 1) << 2) | w1)
+    del w2, w4, w8, w16, c
+    length = torch.from_numpy(tx.length.astype(np.int64)).to(dev)
+    starts = torch.cumsum(length, 0) - length
+    tid = torch.repeat_interleave(torch.arange(length.shape[0], device=dev), length)
+    off = torch.arange(n, device=dev) - starts[tid]
+    keep = off >= KMER - 1
+    ids, tid, off = ids[keep], tid[keep], off[keep]
+    mask = H - 1
+    composite = ((ids & mask) << (62 - HBITS)) | (ids >> HBITS)
+    del ids
+    sc, order = torch.sort(composite, stable=True)
+    del composite
+    pos = tid[order].to(torch.int32)
+    p = off[order].to(torch.int32)
+    del tid, off, order
+    uk, counts = torch.unique_consecutive(sc, return_counts=True)
+    del sc
+    first = torch.cumsum(counts, 0) - counts
+    uid = ((uk & ((1 << (62 - HBITS)) - 1)) << HBITS) | (uk >> (62 - HBITS))
+    bucket_n = torch.bincount(uid & mask, minlength=H).to(torch.int32)
+    buckets = np.empty(uk.shape[0], dtype=BUCKET_DTYPE)
+    buckets["id"] = uid.cpu().numpy().view(np.uint64)
+    buckets["start"] = first.to(torch.int32).cpu().numpy().view(np.uint32)
+    buckets["end"] = (first + counts).to(torch.int32).cpu().numpy().view(np.uint32)
+    names = [nm.encode() for nm in tx.names]
+    name_len = max(len(nm) for nm in names) + 1
+    nb = b"".join(nm + b"\0" * (name_len - len(nm)) for nm in names)
+    out = HeraIndex(len(names), name_len, nb, tx.length.astype(np.uint32),
+                    tx.find.astype(np.uint32), tx.seq.astype(np.uint8),
+                    bucket_n.cpu().numpy().view(np.uint32), buckets,
+                    pos.cpu().numpy().view(np.uint32), p.cpu().numpy().view(np.uint32))
+    del uk, counts, first, uid, bucket_n, pos, p
+    torch.cuda.empty_cache()
+    return out
 
 
 def build_index(tx, device: Optional[str] = None) -> HeraIndex:
     """Index a Transcriptome exactly as ``hera index`` would
     (get_ref_seq + construct_hash, src/hash_align.c:1060-1128).
-    `device="cuda"` sorts on the GPU (same result, faster at large sizes)."""
+    `device="cuda"` builds it with torch on the GPU (same bytes, faster at
+    transcriptome scale)."""
+    if device is not None and device.startswith("cuda"):
+        return _build_index_torch(tx, device)
     ids, tid, off = _occurrences(tx.seq, tx.length, tx.find)
     mask = np.uint64(H - 1)
     # (bucket, id) order as one 62-bit key: bucket in the high 27 bits
     composite = ((ids & mask) << np.uint64(62 - HBITS)) | (ids >> np.uint64(HBITS))
-    order = _stable_order(composite, device)
+    order = np.argsort(composite, kind="stable")
     sc = composite[order]
     pos = tid[order]
     p = off[order]

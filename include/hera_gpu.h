@@ -138,7 +138,7 @@ typedef struct hera_gpu_ctx hera_gpu_ctx;
 typedef struct hera_gpu_options {
 	int device;              /* CUDA device ordinal */
 	uint32_t max_batch;      /* pairs (or single reads) per device pass; 0 = 1<<20 */
-	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 1 GiB */
+	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 2 GiB */
 } hera_gpu_options;
 
 /* Per-stage device time of the last call, milliseconds (CUDA events). */
