@@ -48,7 +48,12 @@ class _IndexView(C.Structure):
 
 
 class _Options(C.Structure):
-    _fields_ = [("device", C.c_int), ("max_batch", C.c_uint32), ("scratch_bytes", C.c_uint64)]
+    _fields_ = [("device", C.c_int), ("max_batch", C.c_uint32), ("scratch_bytes", C.c_uint64),
+                ("path", C.c_int)]
+
+
+PATH_BATCHED = 0
+PATH_PLAIN = 1
 
 
 class _Result(C.Structure):
@@ -64,8 +69,10 @@ class _Reads(C.Structure):
 
 class Timing(C.Structure):
     _fields_ = [(k, C.c_float) for k in ("h2d_ms", "seed_ms", "position_ms", "resolve_ms",
-                                         "rescue_ms", "pack_ms", "d2h_ms", "total_ms")] + [
-        ("launches", C.c_uint32), ("rescue_rounds", C.c_uint32), ("lookups", C.c_uint64)]
+                                         "rescue_ms", "pack_ms", "d2h_ms", "total_ms",
+                                         "build_ms", "dp_ms")] + [
+        ("launches", C.c_uint32), ("rescue_rounds", C.c_uint32), ("lookups", C.c_uint64),
+        ("dp_jobs", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -144,7 +151,8 @@ class Result:
 class Context:
     """One hera index resident on one GPU."""
 
-    def __init__(self, index, device: int = 0, max_batch: int = 0, scratch_bytes: int = 0):
+    def __init__(self, index, device: int = 0, max_batch: int = 0, scratch_bytes: int = 0,
+                 path: str = "batched"):
         self.lib = load_library()
         self.index = index
         v = _IndexView()
@@ -159,7 +167,10 @@ class Context:
         v.n_trans, v.len, v.find, v.seq = index.n_trans, _ptr(ln), _ptr(fd), _ptr(sq)
         v.bucket_n, v.buckets, v.n_buckets = _ptr(bn), _ptr(bk), bk.shape[0]
         v.pos, v.p, v.n_pos = _ptr(pos), _ptr(p), pos.shape[0]
-        opt = _Options(device, max_batch, scratch_bytes)
+        if path not in ("batched", "plain"):
+            raise ValueError(f"unknown path {path!r}")
+        self.path = path
+        opt = _Options(device, max_batch, scratch_bytes, PATH_PLAIN if path == "plain" else PATH_BATCHED)
         h = C.c_void_p()
         rc = self.lib.hera_gpu_ctx_create(C.byref(v), C.byref(opt), C.byref(h))
         if rc != HERA_GPU_OK:

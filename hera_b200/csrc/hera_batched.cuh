@@ -1,0 +1,684 @@
+// hera_batched.cuh -- the batched form of get_position.
+//
+// In hera, one get_position call (src/hash_align.c:1322-1467) seeds the
+// read, merges the hit lists into anchors, forms chains in up to three
+// passes, and for every chain runs get_SWalign (:1242-1320): a prefix
+// SW_align plus one SW_align per gap, with early exits and a keep / append /
+// reset rule on the running best error.  The inputs of every SW_align call
+// are fixed by the chain structure; only the bookkeeping around them is
+// sequential.  So the batched form splits a round of get_position calls
+// into:
+//   k_build   per call: seeds, anchor merge, chain enumeration of all
+//             passes, one DP job per SW_align the call could make;
+//   k_bin_*   counting sort of the jobs by (error cap, gap length);
+//   k_dp      one thread per job, neighbouring threads on equal-shaped DPs
+//             (register form of SW_align);
+//   k_replay  per call: the reference's pass / early-exit / keep rules
+//             over the job results, then the kept chain's CIGAR.
+// Pair-level control flow (k_resolve_b) requests get_position calls and
+// mate rescues and suspends until the round that serves them has run.
+#pragma once
+
+// (included inside hera_gpu.cu's unnamed namespace, after Batch/RmReq)
+
+constexpr int JCAP = 32;          // CIGAR ops kept per DP job (traceback mode)
+constexpr int NBIN = 2 * (MAX_READ + 1);
+
+struct GpReq {
+	int32_t pair;
+	int16_t c, str;
+};
+
+struct TaskInfo {
+	int32_t chain0;
+	int32_t nch;              // -1: no anchors (miss), -2: buffers overflowed
+};
+
+struct Chain {
+	uint32_t t, tp, off;      // head anchor
+	int32_t job0;             // first DP job; jobs of a chain are contiguous
+	int16_t njob;
+	int8_t pass;              // 0 mate-guided, 1 chains, 2 singletons
+	int8_t viable;            // 0: get_SWalign returns before any DP
+	int8_t has_prefix;
+	int8_t pad[3];
+};
+
+struct DpJob {
+	uint32_t rstart;          // reference window start (offset in seq)
+	uint16_t ref_len, len;
+	uint16_t qoff, mrun;      // query offset in the oriented read; M run before the gap
+	int8_t err, orient;
+	int16_t pad;
+	int32_t read;
+};
+
+struct DpResHdr {
+	int16_t score, sub;
+	uint8_t n, nm, pad[2];
+};
+
+__host__ __device__ inline int res_stride(int cap)
+{
+	return (int)sizeof(DpResHdr) + 4 * cap + ((cap + 3) & ~3);
+}
+
+struct Round {
+	const GpReq *req;         // null: round 0 (task t = pair t>>2, c (t>>1)&1, str t&1)
+	int ntask;
+	int space;
+	const uint2 *hits;        // precomputed seeds (round 0) or null
+	int spr;
+	TaskInfo *tinfo;
+	Chain *chains;
+	DpJob *jobs;
+	int *cnt;                 // [0] chains, [1] jobs
+	int chain_cap, job_cap;
+	uint8_t *res;
+	int rcap;                 // CIGAR ops per job result
+};
+
+__device__ __forceinline__ void task_of(const Round &R, int t, int &pi, int &c, int &str)
+{
+	if (R.req) {
+		pi = R.req[t].pair;
+		c = R.req[t].c;
+		str = R.req[t].str;
+	} else {
+		pi = t >> 2;
+		c = (t >> 1) & 1;
+		str = t & 1;
+	}
+}
+
+// Enumerate the chains of one get_position call in the reference's order
+// (pass A :1367-1390, pass B :1392-1412, pass C :1414-1434); pass A's
+// consumed marks are kept in a bitmask so the walk can be repeated.
+template <class Emit>
+__device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, int space, int rlen,
+				   uint32_t *used, Emit emit)
+{
+	for (int w = 0; w < ACAP / 32; ++w)
+		used[w] = 0;
+	auto is_used = [&](uint32_t i) { return (used[i >> 5] >> (i & 31)) & 1u; };
+	auto next = [&](uint32_t i, uint32_t n, bool stop_used) -> bool {
+		if (i + 1 >= (uint32_t)na)
+			return false;
+		if (A.t[i] != A.t[i + 1])
+			return false;
+		// read offsets of used anchors read as rlen in the reference
+		const uint32_t o0 = is_used(i) ? (uint32_t)rlen : A.off[i];
+		const uint32_t o1 = is_used(i + 1) ? (uint32_t)rlen : A.off[i + 1];
+		if (!(o1 > o0))
+			return false;
+		if (!(A.tp[i + 1] > A.tp[i + 1 - n]))
+			return false;
+		if (!(A.tp[i + 1] - A.tp[i + 1 - n] < (uint32_t)rlen))
+			return false;
+		if (stop_used && o1 == (uint32_t)rlen)
+			return false;
+		return true;
+	};
+	bool passA = Mt.n > 0 && space < KMER && space > 0;
+	if (passA) {
+		const uint32_t mn = (uint32_t)Mt.n;
+		uint32_t k = 0;
+		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+			if (A.t[i] < Mt.t[k])
+				continue;
+			while (k < mn && A.t[i] > Mt.t[k])
+				++k;
+			if (k == mn)
+				break;
+			uint32_t n = 1;
+			while (next(i, n, false)) {
+				++i;
+				++n;
+			}
+			emit(0, i + 1 - n, n);
+			for (uint32_t q = i + 1 - n; q <= i; ++q)
+				used[q >> 5] |= 1u << (q & 31);
+		}
+	}
+	for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+		if (is_used(i) || A.off[i] == (uint32_t)rlen)
+			continue;
+		uint32_t n = 1;
+		while (next(i, n, true)) {
+			++i;
+			++n;
+		}
+		if (n < 2 && rlen / KMER > 2)
+			continue;
+		emit(1, i - n + 1, n);
+	}
+	if (space < KMER) {
+		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
+			if (is_used(i) || A.off[i] == (uint32_t)rlen)
+				continue;
+			uint32_t n = 1;
+			while (next(i, n, true)) {
+				++i;
+				++n;
+			}
+			if (n >= 2)
+				continue;
+			emit(2, i, n);
+		}
+	}
+}
+
+struct BuildWork {
+	Anchors a[2];
+	uint32_t used[ACAP / 32];
+};
+
+__global__ void __launch_bounds__(128) k_build(Batch b, Round R)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= R.ntask)
+		return;
+	int pi, c, str;
+	task_of(R, t, pi, c, str);
+	DPair &P = b.P[pi];
+	DSlot &S = P.s[c][str];
+	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	int flags = 0;
+	if (!R.req) {   // round 0 starts the pair's Candidate state
+		S.n = 0;
+		S.err = 0;
+		S.cig.n = S.cig.nm = 0;
+		if (str == 0)
+			P.pair[c] = 0;
+		if (t % 4 == 0) {
+			P.stage = 0;
+			P.rm_ret = 0;
+		}
+	}
+	R.tinfo[t].chain0 = 0;
+	R.tinfo[t].nch = -1;
+	if (L > b.max_len) {
+		flag(b.flags, F_READ);
+		return;
+	}
+	const uint8_t *rd = (str ? b.code_r : b.code) + b.off[ri];
+	const uint32_t step = (uint32_t)R.space;
+	BuildWork w;
+	int cur = 0, na = 0, sj = 0;
+	for (uint32_t i = 0; i + KMER <= (uint32_t)L; i += step, ++sj) {
+		uint2 h = R.hits ? R.hits[((int64_t)ri * 2 + str) * R.spr + sj] : probe(b.ix, kmer_at(rd, (int)i));
+		if (h.y == 0)
+			continue;
+		const uint2 *occ = b.ix.occ + h.x;
+		if (na == 0) {
+			uint32_t nh = h.y;
+			if (nh > (uint32_t)ACAP) {
+				flags |= F_ACAP;
+				nh = ACAP;
+			}
+			for (uint32_t k = 0; k < nh; ++k) {
+				uint2 o = __ldg(occ + k);
+				w.a[cur].t[k] = o.x;
+				w.a[cur].tp[k] = o.y;
+				w.a[cur].off[k] = i;
+			}
+			na = (int)nh;
+			continue;
+		}
+		na = merge_hits(w.a[cur], na, w.a[cur ^ 1], occ, h.y, i, flags);
+		cur ^= 1;
+	}
+	if (na == 0) {
+		flag(b.flags, flags);
+		return;
+	}
+	const Anchors &A = w.a[cur];
+	const DSlot &Mt = P.s[c][1 - str];
+	// a chain's DP jobs: prefix (off0 > 0) plus one per gap after a merged run
+	auto jobs_of = [&](uint32_t id, uint32_t n, int &viable, int &has_prefix, int &runs) {
+		viable = 0;
+		has_prefix = 0;
+		runs = 0;
+		if (n > 1 && A.tp[id + n - 1] - A.tp[id] > (uint32_t)L)
+			return;
+		const int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
+		if (start < 0 || (uint32_t)(start + L) > __ldg(b.ix.tlen + A.t[id]))
+			return;
+		viable = 1;
+		has_prefix = A.off[id] > 0;
+		for (uint32_t i = 0; i < n; ++i) {
+			while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
+				++i;
+			++runs;
+		}
+	};
+	int nch = 0, nj = 0;
+	enum_chains(A, na, Mt, R.space, L, w.used, [&](int pass, uint32_t id, uint32_t n) {
+		int v, hp, runs;
+		jobs_of(id, n, v, hp, runs);
+		++nch;
+		const bool reuse = pass == 2 && L / KMER <= 2;   // pass B aligned the same singletons
+		if (v && !reuse)
+			nj += hp + runs;
+	});
+	const int at = atomicAdd(R.cnt, nch);
+	const int jt = atomicAdd(R.cnt + 1, nj);
+	if (at + nch > R.chain_cap || jt + nj > R.job_cap) {
+		R.tinfo[t].nch = -2;
+		flag(b.flags, flags);
+		return;
+	}
+	R.tinfo[t].chain0 = at;
+	R.tinfo[t].nch = nch;
+	int ci = at, ji = jt;
+	enum_chains(A, na, Mt, R.space, L, w.used, [&](int pass, uint32_t id, uint32_t n) {
+		int v, hp, runs;
+		jobs_of(id, n, v, hp, runs);
+		Chain ch;
+		ch.t = A.t[id];
+		ch.tp = A.tp[id];
+		ch.off = A.off[id];
+		ch.pass = (int8_t)pass;
+		ch.viable = (int8_t)v;
+		ch.has_prefix = (int8_t)hp;
+		ch.job0 = -1;
+		ch.njob = 0;
+		if (v) {
+			const bool reuse = pass == 2 && L / KMER <= 2;
+			if (reuse) {
+				// find the pass-B chain with the same head (chains of a
+				// task are stored in emission order)
+				for (int q = at; q < ci; ++q) {
+					const Chain &o = R.chains[q];
+					if (o.pass == 1 && o.t == ch.t && o.tp == ch.tp && o.off == ch.off) {
+						ch.job0 = o.job0;
+						ch.njob = o.njob;
+						break;
+					}
+				}
+			} else {
+				ch.job0 = ji;
+				ch.njob = (int16_t)(hp + runs);
+				const int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
+				const uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
+				const uint32_t ref_start = __ldg(b.ix.tstart + A.t[id]) + (uint32_t)start;
+				if (hp) {
+					DpJob j;
+					const uint32_t o0 = A.off[id];
+					j.rstart = ref_start - add;
+					j.ref_len = (uint16_t)(o0 + add);
+					j.len = (uint16_t)o0;
+					j.qoff = 0;
+					j.mrun = 0;
+					j.err = (int8_t)(o0 < 2 * ERR ? -3 : -ERR);
+					j.orient = (int8_t)str;
+					j.read = ri;
+					j.pad = 0;
+					R.jobs[ji++] = j;
+				}
+				for (uint32_t i = 0; i < n; ++i) {
+					const uint32_t s0 = i;
+					while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
+						++i;
+					const uint32_t seg = A.off[id + i] + KMER;
+					const uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)L) - seg;
+					const uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
+					DpJob j;
+					j.rstart = ref_start + seg;
+					j.ref_len = (uint16_t)(len + ad);
+					j.len = (uint16_t)len;
+					j.qoff = (uint16_t)seg;
+					j.mrun = (uint16_t)(A.off[id + i] - A.off[id + s0] + KMER);
+					j.err = (int8_t)(len < 2 * ERR ? 3 : ERR);
+					j.orient = (int8_t)str;
+					j.read = ri;
+					j.pad = 0;
+					R.jobs[ji++] = j;
+				}
+			}
+		}
+		R.chains[ci++] = ch;
+	});
+	flag(b.flags, flags);
+}
+
+__device__ __forceinline__ int job_bin(const DpJob &j)
+{
+	const int e = j.err < 0 ? -j.err : j.err;
+	return (e == 7 ? 1 : 0) * (MAX_READ + 1) + (j.len <= MAX_READ ? j.len : MAX_READ);
+}
+
+__global__ void k_bin_count(const DpJob *__restrict__ jobs, int n, int *__restrict__ hist)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < n)
+		atomicAdd(hist + job_bin(jobs[t]), 1);
+}
+
+// exclusive scan of the (small) histogram, one block
+__global__ void k_bin_scan(int *__restrict__ hist, int nbin)
+{
+	__shared__ int part[1024];
+	const int tid = threadIdx.x;
+	const int per = (nbin + blockDim.x - 1) / blockDim.x;
+	int s = 0;
+	for (int i = tid * per; i < (tid + 1) * per && i < nbin; ++i)
+		s += hist[i];
+	part[tid] = s;
+	__syncthreads();
+	if (tid == 0) {
+		int acc = 0;
+		for (int i = 0; i < (int)blockDim.x; ++i) {
+			const int v = part[i];
+			part[i] = acc;
+			acc += v;
+		}
+	}
+	__syncthreads();
+	int acc = part[tid];
+	for (int i = tid * per; i < (tid + 1) * per && i < nbin; ++i) {
+		const int v = hist[i];
+		hist[i] = acc;
+		acc += v;
+	}
+}
+
+__global__ void k_bin_scatter(const DpJob *__restrict__ jobs, int n, int *__restrict__ cursor,
+			      int *__restrict__ perm)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < n)
+		perm[atomicAdd(cursor + job_bin(jobs[t]), 1)] = t;
+}
+
+struct DpWork {
+	uint8_t rows[(MAX_DP_ROWS + 1) * 20];
+	DCig cig;
+	SwWork sw;     // only for the general banded form
+};
+
+// one thread per job, jobs in (error cap, length) order
+__global__ void __launch_bounds__(128) k_dp(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm,
+					    int n, uint8_t *__restrict__ res, int rcap)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n)
+		return;
+	const int id = perm[t];
+	const DpJob jb = jobs[id];
+	DpWork w;
+	int flags = 0;
+	const bool so = b.score_only != 0;
+	const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+	const uint32_t ref_len = jb.ref_len, len = jb.len;
+	int score;
+	w.cig.n = w.cig.nm = 0;
+	if (len == 0) {
+		score = 0;
+	} else {
+		const bool rev = jb.err < 0;
+		const int e = rev ? -jb.err : jb.err;
+		RefWin r{b.ix.code, b.ix.seq, jb.rstart, ref_len, rev};
+		QView qv{rev ? q + (len - 1) : q, rev ? -1 : 1};
+		if (e == 7 && ref_len >= 9)
+			score = sw_align_reg<8>(r, qv, ref_len, len, so, w.cig, w.rows, flags);
+		else if (e == 3 && ref_len >= 5)
+			score = sw_align_reg<4>(r, qv, ref_len, len, so, w.cig, w.rows, flags);
+		else
+			score = sw_align(b.ix, jb.rstart, q, ref_len, len, jb.err, so, w.cig, w.sw, flags);
+	}
+	uint8_t *o = res + (size_t)id * res_stride(rcap);
+	DpResHdr h;
+	int sub = 0;
+	for (int k = 0; k < w.cig.n; ++k) {
+		const int ty = op_type(w.cig.op[k]);
+		if (ty == OP_I || ty == OP_S)
+			sub += (int)op_cnt(w.cig.op[k]);
+		else if (ty == OP_D)
+			sub -= (int)op_cnt(w.cig.op[k]);
+	}
+	if (w.cig.n > rcap || w.cig.nm > rcap)
+		flags |= F_CCAP;
+	h.score = (int16_t)score;
+	h.sub = (int16_t)sub;
+	h.n = (uint8_t)(w.cig.n < rcap ? w.cig.n : rcap);
+	h.nm = (uint8_t)(w.cig.nm < rcap ? w.cig.nm : rcap);
+	h.pad[0] = h.pad[1] = 0;
+	*reinterpret_cast<DpResHdr *>(o) = h;
+	uint32_t *ops = reinterpret_cast<uint32_t *>(o + sizeof(DpResHdr));
+	for (int k = 0; k < h.n; ++k)
+		ops[k] = w.cig.op[k];
+	uint8_t *miss = o + sizeof(DpResHdr) + 4 * rcap;
+	for (int k = 0; k < h.nm; ++k)
+		miss[k] = w.cig.miss[k];
+	flag(b.flags, flags);
+}
+
+__device__ inline void load_res_cig(const uint8_t *o, int rcap, DCig &c)
+{
+	const DpResHdr h = *reinterpret_cast<const DpResHdr *>(o);
+	const uint32_t *ops = reinterpret_cast<const uint32_t *>(o + sizeof(DpResHdr));
+	const uint8_t *miss = o + sizeof(DpResHdr) + 4 * rcap;
+	c.n = h.n;
+	c.nm = h.nm;
+	for (int k = 0; k < h.n; ++k)
+		c.op[k] = ops[k];
+	for (int k = 0; k < h.nm; ++k)
+		c.miss[k] = miss[k];
+}
+
+// get_position's pass / early-exit / keep rules over the job results
+__global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= R.ntask)
+		return;
+	int pi, c, str;
+	task_of(R, t, pi, c, str);
+	DPair &P = b.P[pi];
+	DSlot &S = P.s[c][str];
+	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	const TaskInfo ti = R.tinfo[t];
+	if (ti.nch == -2)
+		return;
+	int flags = 0;
+	uint32_t n1 = 0, max = 0;
+	int keep = -1;
+	const int stride = res_stride(R.rcap);
+	for (int pass = 0; pass < 3 && ti.nch > 0; ++pass) {
+		bool runs;
+		if (pass == 0)
+			runs = P.s[c][1 - str].n > 0 && R.space < KMER && R.space > 0;
+		else if (pass == 1)
+			runs = n1 == 0;
+		else
+			runs = n1 == 0 && R.space < KMER;
+		if (!runs)
+			continue;
+		n1 = 0;
+		max = (uint32_t)(L / 2);
+		for (int q = 0; q < ti.nch; ++q) {
+			const Chain ch = R.chains[ti.chain0 + q];
+			if (ch.pass != pass || !ch.viable)
+				continue;
+			int err = 0, sub = 0, j = ch.job0;
+			bool ok = true;
+			if (ch.has_prefix) {
+				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)j * stride);
+				err += h.score;
+				if (err > L / 2 || (uint32_t)err > max)
+					ok = false;
+				sub = h.sub;
+				++j;
+			}
+			for (; ok && j < ch.job0 + ch.njob; ++j) {
+				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)j * stride);
+				err += h.score;
+				if (err > L / 2 || (uint32_t)err > max + 1)
+					ok = false;
+			}
+			if (!ok)
+				continue;
+			if (max == (uint32_t)(L / 2) || (uint32_t)err < max) {
+				keep = ti.chain0 + q;
+				n1 = 0;
+				max = (uint32_t)err;
+			}
+			if (n1 < (uint32_t)LCAP) {
+				S.t[n1] = ch.t;
+				S.p[n1] = (int32_t)(ch.tp - (ch.off + KMER - 1) + (uint32_t)sub);
+			} else {
+				flags |= F_LCAP;
+			}
+			++n1;
+		}
+	}
+	if (n1 == 0) {   // miss exit (src/hash_align.c:1461-1466)
+		S.n = 0;
+		S.err = L;
+		flag(b.flags, flags);
+		return;
+	}
+	S.n = (int32_t)(n1 < (uint32_t)LCAP ? n1 : (uint32_t)LCAP);
+	S.err = (int32_t)max;
+	// the kept chain's CIGAR: prefix DP, then an M run and the gap DP per
+	// segment (get_SWalign :1262-1305)
+	DCig cig, tmp;
+	const Chain ch = R.chains[keep];
+	int j = ch.job0;
+	cig.n = cig.nm = 0;
+	if (ch.has_prefix) {
+		load_res_cig(R.res + (size_t)j * stride, R.rcap, cig);
+		++j;
+	}
+	for (; j < ch.job0 + ch.njob; ++j) {
+		const DpJob jb = R.jobs[j];
+		cig_add(cig, OP_M, jb.mrun, nullptr, flags);
+		load_res_cig(R.res + (size_t)j * stride, R.rcap, tmp);
+		cig_concat(cig, tmp, flags);
+	}
+	cig_copy(S.cig, cig);
+	flag(b.flags, flags);
+}
+
+// pair control flow of the batched form: the same decisions as k_resolve,
+// but every get_position at spacing 14 is requested (GpReq) like a rescue
+__global__ void __launch_bounds__(128) k_resolve_b(Batch b, const GpReq *__restrict__ res_g, int ng,
+						    const RmReq *__restrict__ res_r, int nr, int all,
+						    GpReq *__restrict__ qg, int *__restrict__ qng,
+						    RmReq *__restrict__ qr, int *__restrict__ qnr)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= ng + nr)
+		return;
+	const int pi = all ? t : (t < ng ? res_g[t].pair : res_r[t - ng].pair);
+	DPair &P = b.P[pi];
+	auto gp = [&](int c, int str, int next) {
+		const int k = atomicAdd(qng, 1);
+		qg[k].pair = pi;
+		qg[k].c = (int16_t)c;
+		qg[k].str = (int16_t)str;
+		P.stage = next;
+	};
+	auto rm = [&](int c, int str, int next) {
+		const int k = atomicAdd(qnr, 1);
+		qr[k].pair = pi;
+		qr[k].c = (int16_t)c;
+		qr[k].str = (int16_t)str;
+		P.stage = next;
+	};
+	if (b.len[2 * pi] > b.max_len || b.len[2 * pi + 1] > b.max_len) {
+		P.stage = 8;
+		return;
+	}
+	int st = P.stage;
+	for (;;) {
+		switch (st) {
+		case 0:   // retry r[0] at spacing 14 (:1672-1676)
+			if (P.s[0][0].n == 0 && P.s[0][1].n == 0 && P.s[1][0].err + P.s[1][1].err > ERR) {
+				gp(0, 0, 100);
+				return;
+			}
+			st = 1;
+			break;
+		case 100:
+			gp(0, 1, 101);
+			return;
+		case 101:
+			st = 1;
+			break;
+		case 1:   // retry r[1] (:1677-1681)
+			if (P.s[1][0].n == 0 && P.s[1][1].n == 0 && P.s[0][0].err + P.s[0][1].err > ERR) {
+				gp(1, 1, 110);
+				return;
+			}
+			st = 2;
+			break;
+		case 110:
+			gp(1, 0, 111);
+			return;
+		case 111:
+			st = 2;
+			break;
+		case 2: case 3: case 4: case 5: {   // get_position2 x4 (:1683-1694)
+			const int c = (st - 2) >> 1, s = (st - 2) & 1;
+			const DSlot &X = P.s[c][s], &Y = P.s[c][1 - s];
+			const DSlot &O0 = P.s[1 - c][0], &O1 = P.s[1 - c][1];
+			if (X.n == 0 && Y.n > 0 && Y.err < ERR && O0.err + O1.err > ERR) {
+				gp(c, s, 200 + st);
+				return;
+			}
+			st = st + 1;
+			break;
+		}
+		case 202: case 203: case 204: case 205: {
+			const int k = st - 200, c = (k - 2) >> 1, s = (k - 2) & 1;
+			if (P.s[c][s].n == 0) {
+				rm(c, s, 210 + k);
+				return;
+			}
+			st = k + 1;
+			break;
+		}
+		case 212: case 213: case 214: case 215:
+			st = st - 210 + 1;
+			break;
+		case 6: case 7: {   // intersect2 (:1730-1733)
+			const int c = st - 6;
+			if (P.s[c][0].n > 0 && P.s[c][1].n > 0) {
+				if (intersect_lists(P, c, MAX_FRAG) == 0 && intersect_lists(P, c, 0) == 0) {
+					const int i = P.s[c][0].err < P.s[c][1].err ? 1 : 0;   // re_map
+					P.rm_i = i;
+					rm(c, i, 20 + 2 * c);
+					return;
+				}
+			}
+			st = st + 1;
+			break;
+		}
+		case 20: case 22: {
+			const int c = (st - 20) >> 1;
+			if (P.rm_ret == 0) {
+				rm(c, 1 - P.rm_i, st + 1);
+				return;
+			}
+			P.pair[c] = 2;
+			st = 7 + c;
+			break;
+		}
+		case 21: case 23: {
+			const int c = (st - 21) >> 1;
+			if (P.rm_ret > 0)
+				P.pair[c] = 2;
+			st = 7 + c;
+			break;
+		}
+		default:
+			P.stage = 8;
+			return;
+		}
+	}
+}
+

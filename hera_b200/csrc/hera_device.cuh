@@ -343,6 +343,239 @@ __device__ inline int sw_align(const DevIndex &ix, uint32_t rstart, const uint8_
 }
 
 // ---------------------------------------------------------------------
+// Gap DP, register form.  Same semantics as sw_align above, for the two
+// error caps the live calls use (err = +-3 -> error 4, err = +-7 ->
+// error 8) when ref_len >= error + 1 (no row-0 spill).
+//
+// Every written cell of row k lies on a diagonal d = c - k in
+// [-error, error + 1] (computed cells satisfy |d| <= M <= error; the break
+// and j markers sit at most one diagonal further), so a row is held as
+// W = 2*error + 2 diagonal slots in registers.  In slot terms the diag,
+// up and left neighbours are the fixed offsets P[q], P[q+1], V[q-1]: each
+// row is one fully unrolled, predicated pass with no dynamic indexing, and
+// the reference bases slide through a register window (one load per row).
+// Rows are written to local memory only for the early-stop shrink loop and
+// the traceback.
+// ---------------------------------------------------------------------
+struct QView {   // query codes: q(x) = p[x * step]
+	const uint8_t *p;
+	int step;
+	__device__ __forceinline__ uint8_t operator()(int x) const { return p[x * step]; }
+};
+
+template <int E>
+__device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
+				   bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags)
+{
+	constexpr int W = 2 * E + 2;
+	constexpr unsigned error = E;
+	// reference code at window position x, clamped (values outside the
+	// window are never used, the clamp only keeps the address valid)
+	auto rcode = [&](int x) -> int {
+		x = x < 0 ? 0 : (x >= (int)ref_len ? (int)ref_len - 1 : x);
+		return r.c(x);
+	};
+	int P[W], V[W], RC[W];
+#pragma unroll
+	for (int q = 0; q < W; ++q) {
+		const int d = q - E;
+		P[q] = (d >= 0) ? d : 0;          // row 0: M[0][c] = c, c <= error+1
+		RC[q] = rcode(q - E);             // row 1 needs r[c-1], c = 1 + q - E
+	}
+	{
+		uint32_t *o = reinterpret_cast<uint32_t *>(rows);
+#pragma unroll
+		for (int w = 0; w < (W + 3) / 4; ++w) {
+			uint32_t pk = 0;
+#pragma unroll
+			for (int b = 0; b < 4; ++b)
+				if (w * 4 + b < W)
+					pk |= (uint32_t)P[w * 4 + b] << (8 * b);
+			o[w] = pk;
+		}
+	}
+	constexpr int RS = ((W + 3) / 4) * 4;   // bytes per stored row
+	auto get = [&](int k, int c) -> unsigned {
+		const int q = c - k + E;
+		return (q >= 0 && q < W) ? rows[k * RS + q] : 0u;
+	};
+
+	int s = 0, ferr = -1, k, i = 0;
+	unsigned min = 0, xmin = 0;
+	for (k = 1; k <= (int)len; ++k) {
+		if (k > 1) {
+#pragma unroll
+			for (int q = 0; q < W - 1; ++q)
+				RC[q] = RC[q + 1];
+			RC[W - 1] = rcode(k + W - 2 - E);
+		}
+		const int qk = qc(k - 1);
+		min = error;
+		int j = 0, left = 0, brk = -1;
+		bool broken = false;
+		if (s - k < -E) {   // outside the proven band: cannot happen
+			flags |= F_BAND;
+			return 0;
+		}
+#pragma unroll
+		for (int q = 0; q < W; ++q) {
+			const int c = k + q - E;
+			const int up = (q + 1 < W) ? P[q + 1] : 0;
+			int v = 0;
+			if (c == s) {
+				v = up + 1;   // left edge: M[k-1][s] + 1
+			} else if (c > s && !broken && c <= (int)ref_len) {
+				const int dg = P[q];
+				if (dg == (int)error + 1) {
+					v = error + 1;
+					broken = true;
+					brk = c;
+				} else {
+					const int pen = (dg < (int)error && RC[q] != qk) ? 1 : 0;
+					v = dg + pen;
+					v = (left + 1 < v) ? left + 1 : v;
+					v = (up + 1 < v) ? up + 1 : v;
+					if (v == (int)error && j == 0)
+						j = c;
+					if (v < (int)error)
+						j = 0;
+					if ((unsigned)v <= min) {
+						min = (unsigned)v;
+						xmin = (unsigned)c;
+					}
+					if (q == E && ferr == -1 && v > 0)
+						ferr = c;
+				}
+			}
+			V[q] = v;
+			left = v;
+		}
+		i = broken ? brk : (int)ref_len + 1;
+		if (min != error) {
+			// while (M[k][s] >= error && s < i) ++s
+			bool go = true;
+#pragma unroll
+			for (int q = 0; q < W; ++q) {
+				const int c = k + q - E;
+				if (go && c == s) {
+					if (V[q] >= (int)error && s < i)
+						++s;
+					else
+						go = false;
+				}
+			}
+			if ((unsigned)j > xmin && (unsigned)j < ref_len) {
+#pragma unroll
+				for (int q = 0; q < W; ++q)
+					if (k + q - E == j)
+						V[q] = error + 1;
+			}
+		}
+		{
+			uint32_t *o = reinterpret_cast<uint32_t *>(rows + k * RS);
+#pragma unroll
+			for (int w = 0; w < (W + 3) / 4; ++w) {
+				uint32_t pk = 0;
+#pragma unroll
+				for (int b = 0; b < 4; ++b)
+					if (w * 4 + b < W)
+						pk |= (uint32_t)V[w * 4 + b] << (8 * b);
+				o[w] = pk;
+			}
+		}
+		if (min == error) {
+			++k;
+			break;
+		}
+#pragma unroll
+		for (int q = 0; q < W; ++q)
+			P[q] = V[q];
+	}
+	--k;
+
+	int score = 0;
+	if (min >= error) {
+		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+			--k;
+			int jj = 0;
+			for (int c = 0; (unsigned)c < ref_len; ++c) {
+				const unsigned v = get(k, c);
+				if (v == error + 1)
+					break;
+				if (v > 0)
+					jj = (int)error;
+				if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
+					min = v;
+					xmin = (unsigned)c;
+				}
+			}
+		}
+		if (k < 5) {
+			cig_add(cig, OP_S, len, nullptr, flags);
+			return (int)len;
+		}
+		cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
+		score = (int)len - k;
+		i = k;
+	} else {
+		if (xmin < len && k == (int)len) {
+			min += len - xmin;
+			xmin = len;
+		}
+		i = (int)len;
+	}
+	k = (int)xmin;
+	score += (int)min;
+	if (score_only) {
+		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
+		return score;
+	}
+	while (i > 0 && k > 0) {
+		const unsigned cur = get(i, k);
+		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
+		if (cur == get(i - 1, k - 1) + pen) {
+			if (pen == 0)
+				cig_add(cig, OP_M, 1, nullptr, flags);
+			else
+				cig_add(cig, OP_X, 1, r.a(k - 1), flags);
+			--i;
+			--k;
+		} else if (cur == get(i - 1, k) + 1) {
+			cig_add(cig, OP_I, 1, nullptr, flags);
+			--i;
+		} else {
+			cig_add(cig, OP_D, 1, r.a(k - 1), flags);
+			--k;
+		}
+	}
+	if (i > 0)
+		cig_add(cig, OP_I, (unsigned)i, nullptr, flags);
+	for (int t = 1; t <= k; ++t)
+		cig_add(cig, OP_D, 1, r.a(k - t), flags);
+	return score;
+}
+
+// Entry used by the per-task (plain) path: the banded form, which keeps the
+// register footprint small where neighbouring threads diverge.  The batched
+// path runs sw_align_reg on length-sorted jobs instead.  q: oriented read
+// codes of the gap.
+__device__ inline int gap_dp(const DevIndex &ix, uint32_t rstart, const uint8_t *q, int qstep,
+			     uint32_t ref_len, uint32_t len, int err, bool score_only, DCig &cig,
+			     SwWork &w, int &flags)
+{
+	cig.n = 0;
+	cig.nm = 0;
+	if (len == 0)
+		return 0;
+	if (len > (uint32_t)MAX_DP_ROWS) {
+		flags |= F_READ;
+		return 0;
+	}
+	(void)qstep;
+	return sw_align(ix, rstart, q, ref_len, len, err, score_only, cig, w, flags);
+}
+
+// ---------------------------------------------------------------------
 // Seed-table probe: hash_get with add = 0 (src/hash_align.c:862-895).
 // Returns {start, count} of the k-mer's occurrence list, count 0 on a miss.
 // Buckets are sorted by id, so any search that finds the equal id returns
@@ -474,8 +707,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 	cig.n = cig.nm = 0;
 	if (A.off[id] > 0) {
 		const uint32_t o0 = A.off[id];
-		score = sw_align(ix, ref_start - add, rd, o0 + add, o0, o0 < 2 * ERR ? -3 : -ERR,
-				 score_only, cig, w.sw, flags);
+		score = gap_dp(ix, ref_start - add, rd, 1, o0 + add, o0, o0 < 2 * ERR ? -3 : -ERR,
+			       score_only, cig, w.sw, flags);
 		err += score;
 		if (err > rlen / 2 || (uint32_t)err > max)
 			return;
@@ -495,8 +728,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 		uint32_t seg = A.off[id + i] + KMER;
 		uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)rlen) - seg;
 		uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
-		score = sw_align(ix, ref_start + seg, rd + seg, len + ad, len, len < 2 * ERR ? 3 : ERR,
-				 score_only, tmp, w.sw, flags);
+		score = gap_dp(ix, ref_start + seg, rd + seg, 1, len + ad, len, len < 2 * ERR ? 3 : ERR,
+			       score_only, tmp, w.sw, flags);
 		err += score;
 		if (err > rlen / 2 || (uint32_t)err > max + 1)
 			return;

@@ -37,6 +37,7 @@ struct RmReq {
 struct Batch {
 	DevIndex ix;
 	const uint8_t *code;     // read codes
+	const uint8_t *code_r;   // reverse-complement codes (read i at the same offset)
 	const int64_t *off;      // read offsets (2 per pair: mate 1, mate 2)
 	const int32_t *len;
 	DPair *P;
@@ -74,6 +75,20 @@ __global__ void k_codes(const uint8_t *__restrict__ ascii, uint8_t *__restrict__
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
 	     i += (int64_t)gridDim.x * blockDim.x)
 		code[i] = code_of(ascii[i]);
+}
+
+// reverse-complement codes of every read, at the read's own offset
+__global__ void k_rc(const uint8_t *__restrict__ code, const int64_t *__restrict__ off,
+		     const int32_t *__restrict__ len, int n_reads, int max_len, uint8_t *__restrict__ rc)
+{
+	const int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r >= n_reads)
+		return;
+	const int64_t o = off[r];
+	int L = len[r];
+	L = L < max_len ? L : max_len;
+	for (int x = 0; x < L; ++x)
+		rc[o + x] = comp_code(code[o + L - 1 - x]);
 }
 
 // seed_probe: thread per (read, strand, seed) at spacing 31
@@ -143,8 +158,16 @@ __global__ void __launch_bounds__(TPB) k_position(Batch b, int n_pairs, int spr,
 		S.err = b.len[ri];
 		return;
 	}
-	const int L = load_read(b, ri, str, w.rd);
 	const uint2 *pre = hits + ((int64_t)ri * 2 + str) * spr;
+	const int L0 = b.len[ri];
+	bool any = false;
+	for (int j = 0; j * KMER + KMER <= L0; ++j)
+		any |= pre[j].y != 0;
+	if (!any) {   // no seed hit: get_position's miss exit (src/hash_align.c:1364-1365)
+		S.err = L0;
+		return;
+	}
+	const int L = load_read(b, ri, str, w.rd);
 	get_position(b.ix, w.rd, L, P, c, str, KMER, pre, b.score_only != 0, w, flags);
 	flag(b.flags, flags);
 }
@@ -431,6 +454,8 @@ __global__ void k_emit(const DPair *__restrict__ P, int n_items, int ncand,
 	recs[t] = r;
 }
 
+#include "hera_batched.cuh"
+
 }  // namespace
 
 // ===========================================================================
@@ -514,6 +539,15 @@ struct hera_gpu_ctx {
 	DBuf<uint32_t> cnt;     // 3 * (items+1) counts, then 3 * (items+1) offsets
 	DBuf<uint8_t> cub_tmp;
 	DBuf<uint8_t> scratch;
+	DBuf<uint8_t> code_r;
+	DBuf<GpReq> qg[2];
+	DBuf<TaskInfo> tinfo;
+	DBuf<Chain> chains;
+	DBuf<DpJob> jobs;
+	DBuf<uint8_t> res;
+	DBuf<int> perm, hist;
+	size_t chain_cap = 0, job_cap = 0;
+	int batched = 1;
 	DBuf<int2> calls;
 	DBuf<int> rq_base;
 	DBuf<SswOut> ssw_out;
@@ -603,6 +637,8 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	ctx->hits.release(); ctx->pairs.release(); ctx->q[0].release(); ctx->q[1].release();
 	ctx->counters.release(); ctx->cnt.release(); ctx->cub_tmp.release(); ctx->scratch.release();
 	ctx->calls.release(); ctx->rq_base.release(); ctx->ssw_out.release();
+	ctx->code_r.release(); ctx->qg[0].release(); ctx->qg[1].release(); ctx->tinfo.release();
+	ctx->chains.release(); ctx->jobs.release(); ctx->res.release(); ctx->perm.release(); ctx->hist.release();
 	ctx->recs.release(); ctx->pos_pool.release(); ctx->op_pool.release(); ctx->p_pool.release();
 	ctx->miss_pool.release();
 	ctx->h_seq.release(); ctx->h_off.release(); ctx->h_len.release(); ctx->h_small.release();
@@ -632,6 +668,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 			ctx->max_batch = opt->max_batch;
 		if (opt->scratch_bytes)
 			ctx->scratch_bytes = opt->scratch_bytes;
+		ctx->batched = opt->path == HERA_GPU_PATH_PLAIN ? 0 : 1;
 	}
 	auto bail = [&](int rc) {
 		std::string e = ctx->err;
@@ -701,9 +738,119 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	return HERA_GPU_OK;
 }
 
-// Run the device pipeline on reads already staged in ctx->seq/off/len
-// (2 * n_pairs reads for pairs, n singles otherwise).  Leaves the packed
-// results in the device pools and their sizes in last_*.
+// ---- pipeline pieces --------------------------------------------------
+
+// one rescue round (re_mapSW for every queued request)
+static int rescue_round(hera_gpu_ctx *ctx, const Batch &b, const RmReq *q, int nq, int max_len,
+			cudaStream_t st, uint32_t &launches, float &ms_acc)
+{
+	CK(ctx->calls.ensure((size_t)nq * LCAP), "rescue calls");
+	CK(ctx->rq_base.ensure(nq), "rescue bases");
+	int *d_nc = ctx->counters.p + 4;
+	CK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
+	cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+	cudaEventRecord(e0, st);
+	k_rescue_expand<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, ctx->calls.p, ctx->rq_base.p, d_nc);
+	++launches;
+	CK(cudaMemcpyAsync(ctx->h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
+	CK(cudaStreamSynchronize(st), "rescue expand");
+	const int ncalls = ctx->h_small.p[1];
+	CK(ctx->ssw_out.ensure(ncalls + 1), "rescue outputs");
+	const size_t per = ssw_scratch_bytes(max_len);
+	size_t slots = ctx->scratch_bytes / per;
+	if (slots < 1)
+		slots = 1;
+	if (slots > (size_t)ncalls)
+		slots = (size_t)(ncalls > 0 ? ncalls : 1);
+	CK(ctx->scratch.ensure(slots * per), "rescue scratch");
+	for (int c0 = 0; c0 < ncalls; c0 += (int)slots) {
+		const int m = (int)((size_t)(ncalls - c0) < slots ? (size_t)(ncalls - c0) : slots);
+		k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, q, ctx->calls.p, c0, m, ctx->ssw_out.p,
+									 ctx->scratch.p, per);
+		++launches;
+	}
+	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, ctx->rq_base.p, ctx->ssw_out.p);
+	++launches;
+	cudaEventRecord(e1, st);
+	CK(cudaStreamSynchronize(st), "rescue");
+	float ms = 0;
+	cudaEventElapsedTime(&ms, e0, e1);
+	ms_acc += ms;
+	return HERA_GPU_OK;
+}
+
+// one round of batched get_position calls: build, bin, DP, replay
+static int gp_round(hera_gpu_ctx *ctx, const Batch &b, Round R, cudaStream_t st, uint32_t &launches,
+		    float &build_ms, float &dp_ms)
+{
+	if (R.ntask <= 0)
+		return HERA_GPU_OK;
+	const int rcap = b.score_only ? 2 : JCAP;
+	CK(ctx->tinfo.ensure(R.ntask), "task info");
+	if (ctx->chain_cap < 2 * (size_t)R.ntask)
+		ctx->chain_cap = 2 * (size_t)R.ntask;
+	if (ctx->job_cap < 3 * (size_t)R.ntask)
+		ctx->job_cap = 3 * (size_t)R.ntask;
+	int *d_cnt = ctx->counters.p + 5;
+	cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+	int nch = 0, nj = 0;
+	cudaEventRecord(e0, st);
+	for (int attempt = 0; attempt < 2; ++attempt) {
+		CK(ctx->chains.ensure(ctx->chain_cap), "chains");
+		CK(ctx->jobs.ensure(ctx->job_cap), "dp jobs");
+		R.tinfo = ctx->tinfo.p;
+		R.chains = ctx->chains.p;
+		R.jobs = ctx->jobs.p;
+		R.cnt = d_cnt;
+		R.chain_cap = (int)ctx->chain_cap;
+		R.job_cap = (int)ctx->job_cap;
+		CK(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int), st), "memset");
+		k_build<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
+		++launches;
+		CK(cudaMemcpyAsync(ctx->h_small.p + 6, d_cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
+		CK(cudaStreamSynchronize(st), "build");
+		nch = ctx->h_small.p[6];
+		nj = ctx->h_small.p[7];
+		if ((size_t)nch <= ctx->chain_cap && (size_t)nj <= ctx->job_cap)
+			break;
+		ctx->chain_cap = (size_t)nch + 16;
+		ctx->job_cap = (size_t)nj + 16;
+		if (attempt == 1)
+			return fail(ctx, HERA_GPU_ECAPACITY, "dp job buffers");
+	}
+	cudaEventRecord(e1, st);
+	float ms = 0;
+	CK(cudaEventSynchronize(e1), "build");
+	cudaEventElapsedTime(&ms, e0, e1);
+	build_ms += ms;
+	cudaEventRecord(e0, st);
+	R.res = nullptr;
+	R.rcap = rcap;
+	if (nj > 0) {
+		CK(ctx->res.ensure((size_t)nj * res_stride(rcap)), "dp results");
+		CK(ctx->perm.ensure(nj), "dp order");
+		CK(ctx->hist.ensure(NBIN), "dp bins");
+		CK(cudaMemsetAsync(ctx->hist.p, 0, NBIN * sizeof(int), st), "memset");
+		k_bin_count<<<blocks_for(nj, 256), 256, 0, st>>>(ctx->jobs.p, nj, ctx->hist.p);
+		k_bin_scan<<<1, 256, 0, st>>>(ctx->hist.p, NBIN);
+		k_bin_scatter<<<blocks_for(nj, 256), 256, 0, st>>>(ctx->jobs.p, nj, ctx->hist.p, ctx->perm.p);
+		k_dp<<<blocks_for(nj), 128, 0, st>>>(b, ctx->jobs.p, ctx->perm.p, nj, ctx->res.p, rcap);
+		launches += 4;
+		R.res = ctx->res.p;
+	}
+	k_replay<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
+	++launches;
+	cudaEventRecord(e1, st);
+	CK(cudaEventSynchronize(e1), "replay");
+	cudaEventElapsedTime(&ms, e0, e1);
+	dp_ms += ms;
+	ctx->timing.dp_jobs += (uint64_t)nj;
+	return HERA_GPU_OK;
+}
+
+// Run the device pipeline on staged reads (2 * n reads for pairs, n
+// singles otherwise).  Leaves the packed results in the device pools and
+// their sizes in last_*.
 static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_off,
 		     const int32_t *d_len, int32_t n, bool paired, int write_bam, int max_len,
 		     int64_t seq_bytes, cudaStream_t st)
@@ -711,23 +858,27 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 	const int n_reads = paired ? 2 * n : n;
 	const int ncand = paired ? 2 : 1;
 	const int items = n * ncand;
+	const bool batched = ctx->batched && paired;
 	hera_gpu_timing &T = ctx->timing;
 	uint32_t launches = 0;
 
 	CK(ctx->code.ensure(seq_bytes + 64), "read code buffer");
+	if (batched)
+		CK(ctx->code_r.ensure(seq_bytes + 64), "read code buffer");
 	CK(ctx->pairs.ensure(n), "pair state");
-	CK(ctx->counters.ensure(8), "counters");
+	CK(ctx->counters.ensure(16), "counters");
 	CK(ctx->q[0].ensure(n), "rescue queue");
 	CK(ctx->q[1].ensure(n), "rescue queue");
 	CK(ctx->cnt.ensure(6 * (size_t)(items + 1)), "count buffer");
 	CK(ctx->recs.ensure(items), "records");
-	CK(ctx->h_small.ensure(8), "host counters");
+	CK(ctx->h_small.ensure(16), "host counters");
 	int *d_flags = ctx->counters.p;
-	CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(int), st), "memset");
+	CK(cudaMemsetAsync(ctx->counters.p, 0, 16 * sizeof(int), st), "memset");
 
 	Batch b;
 	b.ix = ctx->ix;
 	b.code = ctx->code.p;
+	b.code_r = batched ? ctx->code_r.p : nullptr;
 	b.off = d_off;
 	b.len = d_len;
 	b.P = ctx->pairs.p;
@@ -739,6 +890,11 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 	if (seq_bytes > 0) {
 		k_codes<<<1184, 256, 0, st>>>(d_seq, ctx->code.p, seq_bytes);
 		++launches;
+		if (batched) {
+			k_rc<<<blocks_for(n_reads, 256), 256, 0, st>>>(ctx->code.p, d_off, d_len, n_reads, max_len,
+									ctx->code_r.p);
+			++launches;
+		}
 	}
 	const int spr = max_len >= KMER ? (max_len - KMER) / KMER + 1 : 1;
 	if (paired) {
@@ -747,20 +903,20 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, ctx->code.p, d_off, d_len, n_reads, spr,
 							     ctx->hits.p);
 		++launches;
-		T.lookups = (uint64_t)ns;
+		T.lookups += (uint64_t)ns;
 	}
 	cudaEventRecord(ctx->ev[2], st);
-	if (paired) {
-		k_position<<<blocks_for((int64_t)n * 4), TPB, 0, st>>>(b, n, spr, ctx->hits.p);
-		++launches;
-	} else {
+	float resolve_ms = 0, rescue_ms = 0, build_ms = 0, dp_ms = 0;
+	uint32_t rounds = 0;
+	if (!paired) {
 		k_single<<<blocks_for(n), TPB, 0, st>>>(b, n);
 		++launches;
-	}
-	cudaEventRecord(ctx->ev[3], st);
-	float resolve_ms = 0, rescue_ms = 0;
-	uint32_t rounds = 0;
-	if (paired) {
+		cudaEventRecord(ctx->ev[3], st);
+	} else if (!batched) {
+		// plain form: one thread per get_position call / pair
+		k_position<<<blocks_for((int64_t)n * 4), TPB, 0, st>>>(b, n, spr, ctx->hits.p);
+		++launches;
+		cudaEventRecord(ctx->ev[3], st);
 		const RmReq *resume = nullptr;
 		int nact = n, qi = 0;
 		while (nact > 0) {
@@ -780,41 +936,66 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 			if (nq == 0)
 				break;
 			++rounds;
-			// expand requests into calls
-			CK(ctx->calls.ensure((size_t)nq * LCAP), "rescue calls");
-			CK(ctx->rq_base.ensure(nq), "rescue bases");
-			int *d_nc = ctx->counters.p + 4;
-			CK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
-			cudaEventRecord(e0, st);
-			k_rescue_expand<<<blocks_for(nq, 256), 256, 0, st>>>(b, ctx->q[qi].p, nq, ctx->calls.p,
-									      ctx->rq_base.p, d_nc);
-			++launches;
-			CK(cudaMemcpyAsync(ctx->h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
-			CK(cudaStreamSynchronize(st), "rescue expand");
-			const int ncalls = ctx->h_small.p[1];
-			CK(ctx->ssw_out.ensure(ncalls + 1), "rescue outputs");
-			const size_t per = ssw_scratch_bytes(max_len);
-			size_t slots = ctx->scratch_bytes / per;
-			if (slots < 1)
-				slots = 1;
-			if (slots > (size_t)ncalls)
-				slots = (size_t)(ncalls > 0 ? ncalls : 1);
-			CK(ctx->scratch.ensure(slots * per), "rescue scratch");
-			for (int c0 = 0; c0 < ncalls; c0 += (int)slots) {
-				const int m = (int)((size_t)(ncalls - c0) < slots ? (size_t)(ncalls - c0) : slots);
-				k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, ctx->q[qi].p, ctx->calls.p, c0, m,
-											 ctx->ssw_out.p, ctx->scratch.p, per);
-				++launches;
-			}
-			k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, ctx->q[qi].p, nq, ctx->rq_base.p,
-									   ctx->ssw_out.p);
-			++launches;
-			cudaEventRecord(e1, st);
-			CK(cudaStreamSynchronize(st), "rescue");
-			cudaEventElapsedTime(&ms, e0, e1);
-			rescue_ms += ms;
+			int rc = rescue_round(ctx, b, ctx->q[qi].p, nq, max_len, st, launches, rescue_ms);
+			if (rc)
+				return rc;
 			resume = ctx->q[qi].p;
 			nact = nq;
+			qi ^= 1;
+		}
+	} else {
+		// batched form: rounds of batched get_position calls and rescues
+		CK(ctx->qg[0].ensure(n), "gp queue");
+		CK(ctx->qg[1].ensure(n), "gp queue");
+		Round R{};
+		R.req = nullptr;
+		R.ntask = 4 * n;
+		R.space = KMER;
+		R.hits = ctx->hits.p;
+		R.spr = spr;
+		int rc = gp_round(ctx, b, R, st, launches, build_ms, dp_ms);
+		if (rc)
+			return rc;
+		cudaEventRecord(ctx->ev[3], st);
+		int ng = n, nr = 0, qi = 0;
+		bool all = true;
+		for (;;) {
+			int *qng = ctx->counters.p + 8 + 2 * qi, *qnr = qng + 1;
+			CK(cudaMemsetAsync(qng, 0, 2 * sizeof(int), st), "memset");
+			cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+			cudaEventRecord(e0, st);
+			k_resolve_b<<<blocks_for(ng + nr), 128, 0, st>>>(b, ctx->qg[qi ^ 1].p, ng, ctx->q[qi ^ 1].p, nr,
+									  all ? 1 : 0, ctx->qg[qi].p, qng,
+									  ctx->q[qi].p, qnr);
+			++launches;
+			cudaEventRecord(e1, st);
+			CK(cudaMemcpyAsync(ctx->h_small.p + 10, qng, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "queues");
+			CK(cudaStreamSynchronize(st), "resolve");
+			float ms = 0;
+			cudaEventElapsedTime(&ms, e0, e1);
+			resolve_ms += ms;
+			all = false;
+			ng = ctx->h_small.p[10];
+			nr = ctx->h_small.p[11];
+			if (ng + nr == 0)
+				break;
+			++rounds;
+			if (ng) {
+				Round G{};
+				G.req = ctx->qg[qi].p;
+				G.ntask = ng;
+				G.space = 2 * ERR;
+				G.hits = nullptr;
+				G.spr = 0;
+				rc = gp_round(ctx, b, G, st, launches, build_ms, dp_ms);
+				if (rc)
+					return rc;
+			}
+			if (nr) {
+				rc = rescue_round(ctx, b, ctx->q[qi].p, nr, max_len, st, launches, rescue_ms);
+				if (rc)
+					return rc;
+			}
 			qi ^= 1;
 		}
 	}
@@ -853,8 +1034,14 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 	float ms = 0;
 	cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
 	T.seed_ms += ms;
-	cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
-	T.position_ms += ms;
+	if (!batched) {
+		cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+		T.position_ms += ms;
+	} else {
+		T.position_ms += build_ms + dp_ms;
+		T.build_ms += build_ms;
+		T.dp_ms += dp_ms;
+	}
 	T.resolve_ms += resolve_ms;
 	T.rescue_ms += rescue_ms;
 	cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);

@@ -212,22 +212,26 @@ def _pack_matrix(m: np.ndarray) -> ReadSet:
                    np.full(n, L, dtype=np.int32))
 
 
-def _mutate(rng, tmpl: np.ndarray, L: int, sub: float, indel: float, indel_len) -> np.ndarray:
-    """Read of length L from a template (>= L + slack bases) with per-base
-    substitution rate `sub` and indel event rate `indel`."""
-    out = []
-    i = 0
-    while len(out) < L and i < tmpl.shape[0]:
-        if indel > 0 and rng.random() < indel:
-            k = int(rng.integers(indel_len[0], indel_len[1] + 1))
-            if rng.random() < 0.5:   # insertion
-                out.extend(_ACGT[rng.integers(0, 4, k)].tolist())
-            else:                    # deletion
-                i += k
-            continue
-        out.append(int(tmpl[i]))
-        i += 1
-    r = np.array(out[:L], dtype=np.uint8)
+def _mutate(rng, tmpl: np.ndarray, L: int, indel: float, indel_len) -> np.ndarray:
+    """Read of length L from a template (>= L + slack bases) with at least
+    one indel event (rate `indel` per base), events placed uniformly."""
+    n_ev = max(1, int(rng.binomial(L, indel)))
+    pos = np.sort(rng.choice(L, size=min(n_ev, L), replace=False))
+    out, i, have = [], 0, 0
+    for p in pos:
+        take = int(p) - have
+        if take > 0:
+            out.append(tmpl[i:i + take])
+            i += take
+            have += take
+        k = int(rng.integers(indel_len[0], indel_len[1] + 1))
+        if rng.random() < 0.5:   # insertion
+            out.append(_ACGT[rng.integers(0, 4, k)])
+            have += k
+        else:                    # deletion
+            i += k
+    out.append(tmpl[i:i + max(L - have, 0)])
+    r = np.concatenate(out)[:L]
     if r.shape[0] < L:
         r = np.concatenate([r, tmpl[:L - r.shape[0]]])
     return r
@@ -292,22 +296,22 @@ def simulate_pairs(tx: Transcriptome, n: int, seed: int, read_len: int = 100,
         rate = rng.uniform(sub_rate[0], sub_rate[1], n)
     else:
         rate = np.asarray(sub_rate, dtype=np.float64)
+    if indel_rate > 0:
+        ev = rng.random((n, 2)) < 1.0 - (1.0 - indel_rate) ** L
+        ends = tx.find.astype(np.int64)[t]
+        starts_t = tx.starts()[t]
+        for i, m in zip(*np.nonzero(ev)):
+            fwd = (m == 0) != bool(flip[i])
+            if fwd:
+                a = int(gstart[i])
+                tm = tx.seq[a:min(a + L + 40, int(ends[i]))]
+            else:
+                b = int(gstart[i] + flen[i])
+                tm = revcomp(tx.seq[max(b - L - 40, int(starts_t[i])):b])
+            if tm.shape[0] >= L:
+                (r1 if m == 0 else r2)[i] = _mutate(rng, tm, L, indel_rate, indel_len)
     _substitute(rng, r1, rate)
     _substitute(rng, r2, rate)
-    if indel_rate > 0:
-        ev = rng.poisson(indel_rate * L * 2, n) > 0
-        ends = tx.find.astype(np.int64)[t]
-        for i in np.nonzero(ev)[0]:
-            for which, m in ((0, r1), (1, r2)):
-                if which == 0 and not flip[i] or which == 1 and flip[i]:
-                    a = int(gstart[i])
-                    tm = tx.seq[a:min(a + L + 30, int(ends[i]))]
-                else:
-                    b = int(gstart[i] + flen[i])
-                    s0 = int(tx.starts()[t[i]])
-                    tm = revcomp(tx.seq[max(b - L - 30, s0):b])
-                if tm.shape[0] >= L:
-                    m[i] = _mutate(rng, tm, L, 0.0, indel_rate, indel_len)
     return _pack_matrix(r1), _pack_matrix(r2)
 
 

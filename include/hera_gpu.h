@@ -135,18 +135,28 @@ typedef struct hera_gpu_reads {
 
 typedef struct hera_gpu_ctx hera_gpu_ctx;
 
+/* Execution forms of the same computation (results are identical).
+ * PLAIN: one thread per get_position call and per pair, one pipeline pass
+ * per chunk.  BATCHED: get_position split into build / length-binned DP
+ * jobs / replay rounds, pair control flow suspended between rounds. */
+#define HERA_GPU_PATH_BATCHED 0
+#define HERA_GPU_PATH_PLAIN 1
+
 typedef struct hera_gpu_options {
 	int device;              /* CUDA device ordinal */
 	uint32_t max_batch;      /* pairs (or single reads) per device pass; 0 = 1<<20 */
 	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 2 GiB */
+	int path;                /* HERA_GPU_PATH_BATCHED (default) or _PLAIN */
 } hera_gpu_options;
 
 /* Per-stage device time of the last call, milliseconds (CUDA events). */
 typedef struct hera_gpu_timing {
 	float h2d_ms, seed_ms, position_ms, resolve_ms, rescue_ms, pack_ms, d2h_ms, total_ms;
+	float build_ms, dp_ms;   /* batched form: build and DP+replay parts of position_ms */
 	uint32_t launches;       /* kernels launched by the last call */
-	uint32_t rescue_rounds;
+	uint32_t rescue_rounds;  /* control-flow rounds after the first */
 	uint64_t lookups;        /* seed-table lookups issued by seed_probe */
+	uint64_t dp_jobs;        /* batched form: gap-DP jobs run */
 } hera_gpu_timing;
 
 /* ---- entry points ------------------------------------------------------ */

@@ -41,11 +41,12 @@ def oracle1(config1):
     return oracle.Oracle(config1[2])
 
 
-@pytest.fixture(scope="session")
-def gpu_ctx1(config1):
+@pytest.fixture(scope="session", params=["batched", "plain"])
+def gpu_ctx1(request, config1):
+    """A device context over the config-1 index, for each execution form."""
     if not gpu_available():
         pytest.skip("no CUDA device")
     from hera_b200 import api
-    ctx = api.Context(config1[2], max_batch=1 << 16)
+    ctx = api.Context(config1[2], max_batch=1 << 16, path=request.param)
     yield ctx
     ctx.close()

@@ -91,7 +91,7 @@ def test_batch_split_invariance(config1, gpu_ctx1):
     ann, tx, ix = config1
     r1, r2 = workloads.pairs("config1", ann, tx, 5000, seed=21)
     a = gpu_ctx1.align_pairs(r1, r2, 0).canonical()
-    small = api.Context(ix, max_batch=777)
+    small = api.Context(ix, max_batch=777, path=gpu_ctx1.path)
     try:
         b = small.align_pairs(r1, r2, 0).canonical()
     finally:
