@@ -72,7 +72,7 @@ class Timing(C.Structure):
                                          "rescue_ms", "pack_ms", "d2h_ms", "total_ms",
                                          "build_ms", "dp_ms")] + [
         ("launches", C.c_uint32), ("rescue_rounds", C.c_uint32), ("lookups", C.c_uint64),
-        ("dp_jobs", C.c_uint64)]
+        ("dp_jobs", C.c_uint64), ("dp_calls", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -36,18 +36,24 @@ struct TaskInfo {
 
 struct Chain {
 	uint32_t t, tp, off;      // head anchor
-	int32_t job0;             // first DP job; jobs of a chain are contiguous
-	int16_t njob;
+	int32_t js0;              // first job slot (slots of a chain are contiguous)
+	int16_t njs;              // job slots: prefix (if any) then one per gap
 	int8_t pass;              // 0 mate-guided, 1 chains, 2 singletons
 	int8_t viable;            // 0: get_SWalign returns before any DP
 	int8_t has_prefix;
 	int8_t pad[3];
 };
 
+struct JobSlot {              // one SW_align call of a chain
+	int32_t job;              // the (deduplicated) DP job computing it
+	uint16_t mrun;            // M run added before this gap (0 for the prefix)
+	uint16_t pad;
+};
+
 struct DpJob {
 	uint32_t rstart;          // reference window start (offset in seq)
 	uint16_t ref_len, len;
-	uint16_t qoff, mrun;      // query offset in the oriented read; M run before the gap
+	uint16_t qoff, pad0;      // query offset in the oriented read
 	int8_t err, orient;
 	int16_t pad;
 	int32_t read;
@@ -71,9 +77,10 @@ struct Round {
 	int spr;
 	TaskInfo *tinfo;
 	Chain *chains;
+	JobSlot *slots;
 	DpJob *jobs;
-	int *cnt;                 // [0] chains, [1] jobs
-	int chain_cap, job_cap;
+	int *cnt;                 // [0] chains, [1] jobs, [2] job slots
+	int chain_cap, job_cap, slot_cap;
 	uint8_t *res;
 	int rcap;                 // CIGAR ops per job result
 };
@@ -168,9 +175,16 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 	}
 }
 
+constexpr int LCH = 128;       // chains of one get_position call
+constexpr int LJS = 256;       // SW_align calls of one get_position call
+constexpr int LJ = 256;        // distinct DP jobs of one get_position call
+
 struct BuildWork {
 	Anchors a[2];
 	uint32_t used[ACAP / 32];
+	Chain ch[LCH];
+	JobSlot js[LJS];
+	DpJob jb[LJ];
 };
 
 __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
@@ -235,111 +249,115 @@ __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 	}
 	const Anchors &A = w.a[cur];
 	const DSlot &Mt = P.s[c][1 - str];
-	// a chain's DP jobs: prefix (off0 > 0) plus one per gap after a merged run
-	auto jobs_of = [&](uint32_t id, uint32_t n, int &viable, int &has_prefix, int &runs) {
-		viable = 0;
-		has_prefix = 0;
-		runs = 0;
+	int nch = 0, ns = 0, nj = 0;
+	// one SW_align call -> a job slot; identical calls (same query span,
+	// caps and reference bytes) share one DP job
+	auto add_job = [&](const DpJob &j, uint16_t mrun) {
+		if (ns >= LJS) {
+			flags |= F_ACAP;
+			return;
+		}
+		int hit = -1;
+		for (int q = 0; q < nj && hit < 0; ++q) {
+			const DpJob &o = w.jb[q];
+			if (o.qoff != j.qoff || o.len != j.len || o.ref_len != j.ref_len || o.err != j.err)
+				continue;
+			bool same = true;
+			for (uint32_t x = 0; x < j.ref_len && same; ++x)
+				same = __ldg(b.ix.seq + o.rstart + x) == __ldg(b.ix.seq + j.rstart + x);
+			if (same)
+				hit = q;
+		}
+		if (hit < 0) {
+			if (nj >= LJ) {
+				flags |= F_ACAP;
+				return;
+			}
+			w.jb[nj] = j;
+			hit = nj++;
+		}
+		w.js[ns].job = hit;
+		w.js[ns].mrun = mrun;
+		w.js[ns].pad = 0;
+		++ns;
+	};
+	enum_chains(A, na, Mt, R.space, L, w.used, [&](int pass, uint32_t id, uint32_t n) {
+		if (nch >= LCH) {
+			flags |= F_ACAP;
+			return;
+		}
+		Chain &ch = w.ch[nch++];
+		ch.t = A.t[id];
+		ch.tp = A.tp[id];
+		ch.off = A.off[id];
+		ch.pass = (int8_t)pass;
+		ch.viable = 0;
+		ch.has_prefix = 0;
+		ch.js0 = ns;
+		ch.njs = 0;
+		// get_SWalign's early returns before any DP (:1250-1256)
 		if (n > 1 && A.tp[id + n - 1] - A.tp[id] > (uint32_t)L)
 			return;
 		const int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
 		if (start < 0 || (uint32_t)(start + L) > __ldg(b.ix.tlen + A.t[id]))
 			return;
-		viable = 1;
-		has_prefix = A.off[id] > 0;
-		for (uint32_t i = 0; i < n; ++i) {
+		ch.viable = 1;
+		const uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
+		const uint32_t ref_start = __ldg(b.ix.tstart + A.t[id]) + (uint32_t)start;
+		DpJob j;
+		j.orient = (int8_t)str;
+		j.read = ri;
+		j.pad = 0;
+		j.pad0 = 0;
+		const int ns0 = ns;
+		if (A.off[id] > 0) {   // prefix DP on the reversed strings (:1262-1266)
+			const uint32_t o0 = A.off[id];
+			ch.has_prefix = 1;
+			j.rstart = ref_start - add;
+			j.ref_len = (uint16_t)(o0 + add);
+			j.len = (uint16_t)o0;
+			j.qoff = 0;
+			j.err = (int8_t)(o0 < 2 * ERR ? -3 : -ERR);
+			add_job(j, 0);
+		}
+		for (uint32_t i = 0; i < n; ++i) {   // merged runs and their gaps (:1282-1305)
+			const uint32_t s0 = i;
 			while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
 				++i;
-			++runs;
+			const uint32_t seg = A.off[id + i] + KMER;
+			const uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)L) - seg;
+			const uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
+			j.rstart = ref_start + seg;
+			j.ref_len = (uint16_t)(len + ad);
+			j.len = (uint16_t)len;
+			j.qoff = (uint16_t)seg;
+			j.err = (int8_t)(len < 2 * ERR ? 3 : ERR);
+			add_job(j, (uint16_t)(A.off[id + i] - A.off[id + s0] + KMER));
 		}
-	};
-	int nch = 0, nj = 0;
-	enum_chains(A, na, Mt, R.space, L, w.used, [&](int pass, uint32_t id, uint32_t n) {
-		int v, hp, runs;
-		jobs_of(id, n, v, hp, runs);
-		++nch;
-		const bool reuse = pass == 2 && L / KMER <= 2;   // pass B aligned the same singletons
-		if (v && !reuse)
-			nj += hp + runs;
+		ch.njs = (int16_t)(ns - ns0);
 	});
 	const int at = atomicAdd(R.cnt, nch);
 	const int jt = atomicAdd(R.cnt + 1, nj);
-	if (at + nch > R.chain_cap || jt + nj > R.job_cap) {
+	const int st = atomicAdd(R.cnt + 2, ns);
+	if (at + nch > R.chain_cap || jt + nj > R.job_cap || st + ns > R.slot_cap) {
 		R.tinfo[t].nch = -2;
 		flag(b.flags, flags);
 		return;
 	}
 	R.tinfo[t].chain0 = at;
 	R.tinfo[t].nch = nch;
-	int ci = at, ji = jt;
-	enum_chains(A, na, Mt, R.space, L, w.used, [&](int pass, uint32_t id, uint32_t n) {
-		int v, hp, runs;
-		jobs_of(id, n, v, hp, runs);
-		Chain ch;
-		ch.t = A.t[id];
-		ch.tp = A.tp[id];
-		ch.off = A.off[id];
-		ch.pass = (int8_t)pass;
-		ch.viable = (int8_t)v;
-		ch.has_prefix = (int8_t)hp;
-		ch.job0 = -1;
-		ch.njob = 0;
-		if (v) {
-			const bool reuse = pass == 2 && L / KMER <= 2;
-			if (reuse) {
-				// find the pass-B chain with the same head (chains of a
-				// task are stored in emission order)
-				for (int q = at; q < ci; ++q) {
-					const Chain &o = R.chains[q];
-					if (o.pass == 1 && o.t == ch.t && o.tp == ch.tp && o.off == ch.off) {
-						ch.job0 = o.job0;
-						ch.njob = o.njob;
-						break;
-					}
-				}
-			} else {
-				ch.job0 = ji;
-				ch.njob = (int16_t)(hp + runs);
-				const int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
-				const uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
-				const uint32_t ref_start = __ldg(b.ix.tstart + A.t[id]) + (uint32_t)start;
-				if (hp) {
-					DpJob j;
-					const uint32_t o0 = A.off[id];
-					j.rstart = ref_start - add;
-					j.ref_len = (uint16_t)(o0 + add);
-					j.len = (uint16_t)o0;
-					j.qoff = 0;
-					j.mrun = 0;
-					j.err = (int8_t)(o0 < 2 * ERR ? -3 : -ERR);
-					j.orient = (int8_t)str;
-					j.read = ri;
-					j.pad = 0;
-					R.jobs[ji++] = j;
-				}
-				for (uint32_t i = 0; i < n; ++i) {
-					const uint32_t s0 = i;
-					while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
-						++i;
-					const uint32_t seg = A.off[id + i] + KMER;
-					const uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)L) - seg;
-					const uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
-					DpJob j;
-					j.rstart = ref_start + seg;
-					j.ref_len = (uint16_t)(len + ad);
-					j.len = (uint16_t)len;
-					j.qoff = (uint16_t)seg;
-					j.mrun = (uint16_t)(A.off[id + i] - A.off[id + s0] + KMER);
-					j.err = (int8_t)(len < 2 * ERR ? 3 : ERR);
-					j.orient = (int8_t)str;
-					j.read = ri;
-					j.pad = 0;
-					R.jobs[ji++] = j;
-				}
-			}
-		}
-		R.chains[ci++] = ch;
-	});
+	for (int q = 0; q < nj; ++q)
+		R.jobs[jt + q] = w.jb[q];
+	for (int q = 0; q < ns; ++q) {
+		JobSlot js = w.js[q];
+		js.job += jt;
+		R.slots[st + q] = js;
+	}
+	for (int q = 0; q < nch; ++q) {
+		Chain ch = w.ch[q];
+		ch.js0 += st;
+		R.chains[at + q] = ch;
+	}
 	flag(b.flags, flags);
 }
 
@@ -503,18 +521,18 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 			const Chain ch = R.chains[ti.chain0 + q];
 			if (ch.pass != pass || !ch.viable)
 				continue;
-			int err = 0, sub = 0, j = ch.job0;
+			int err = 0, sub = 0, j = ch.js0;
 			bool ok = true;
 			if (ch.has_prefix) {
-				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)j * stride);
+				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)R.slots[j].job * stride);
 				err += h.score;
 				if (err > L / 2 || (uint32_t)err > max)
 					ok = false;
 				sub = h.sub;
 				++j;
 			}
-			for (; ok && j < ch.job0 + ch.njob; ++j) {
-				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)j * stride);
+			for (; ok && j < ch.js0 + ch.njs; ++j) {
+				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)R.slots[j].job * stride);
 				err += h.score;
 				if (err > L / 2 || (uint32_t)err > max + 1)
 					ok = false;
@@ -547,16 +565,16 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 	// segment (get_SWalign :1262-1305)
 	DCig cig, tmp;
 	const Chain ch = R.chains[keep];
-	int j = ch.job0;
+	int j = ch.js0;
 	cig.n = cig.nm = 0;
 	if (ch.has_prefix) {
-		load_res_cig(R.res + (size_t)j * stride, R.rcap, cig);
+		load_res_cig(R.res + (size_t)R.slots[j].job * stride, R.rcap, cig);
 		++j;
 	}
-	for (; j < ch.job0 + ch.njob; ++j) {
-		const DpJob jb = R.jobs[j];
-		cig_add(cig, OP_M, jb.mrun, nullptr, flags);
-		load_res_cig(R.res + (size_t)j * stride, R.rcap, tmp);
+	for (; j < ch.js0 + ch.njs; ++j) {
+		const JobSlot js = R.slots[j];
+		cig_add(cig, OP_M, js.mrun, nullptr, flags);
+		load_res_cig(R.res + (size_t)js.job * stride, R.rcap, tmp);
 		cig_concat(cig, tmp, flags);
 	}
 	cig_copy(S.cig, cig);

@@ -77,17 +77,19 @@ __global__ void k_codes(const uint8_t *__restrict__ ascii, uint8_t *__restrict__
 		code[i] = code_of(ascii[i]);
 }
 
-// reverse-complement codes of every read, at the read's own offset
+// reverse-complement codes of every read, at the read's own offset (one
+// warp per read, lanes over bases: coalesced)
 __global__ void k_rc(const uint8_t *__restrict__ code, const int64_t *__restrict__ off,
 		     const int32_t *__restrict__ len, int n_reads, int max_len, uint8_t *__restrict__ rc)
 {
-	const int r = blockIdx.x * blockDim.x + threadIdx.x;
+	const int r = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+	const int lane = threadIdx.x & 31;
 	if (r >= n_reads)
 		return;
 	const int64_t o = off[r];
 	int L = len[r];
 	L = L < max_len ? L : max_len;
-	for (int x = 0; x < L; ++x)
+	for (int x = lane; x < L; x += 32)
 		rc[o + x] = comp_code(code[o + L - 1 - x]);
 }
 
@@ -544,9 +546,10 @@ struct hera_gpu_ctx {
 	DBuf<TaskInfo> tinfo;
 	DBuf<Chain> chains;
 	DBuf<DpJob> jobs;
+	DBuf<JobSlot> slots;
 	DBuf<uint8_t> res;
 	DBuf<int> perm, hist;
-	size_t chain_cap = 0, job_cap = 0;
+	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
 	int batched = 1;
 	DBuf<int2> calls;
 	DBuf<int> rq_base;
@@ -638,7 +641,7 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	ctx->counters.release(); ctx->cnt.release(); ctx->cub_tmp.release(); ctx->scratch.release();
 	ctx->calls.release(); ctx->rq_base.release(); ctx->ssw_out.release();
 	ctx->code_r.release(); ctx->qg[0].release(); ctx->qg[1].release(); ctx->tinfo.release();
-	ctx->chains.release(); ctx->jobs.release(); ctx->res.release(); ctx->perm.release(); ctx->hist.release();
+	ctx->chains.release(); ctx->jobs.release(); ctx->slots.release(); ctx->res.release(); ctx->perm.release(); ctx->hist.release();
 	ctx->recs.release(); ctx->pos_pool.release(); ctx->op_pool.release(); ctx->p_pool.release();
 	ctx->miss_pool.release();
 	ctx->h_seq.release(); ctx->h_off.release(); ctx->h_len.release(); ctx->h_small.release();
@@ -791,30 +794,39 @@ static int gp_round(hera_gpu_ctx *ctx, const Batch &b, Round R, cudaStream_t st,
 		ctx->chain_cap = 2 * (size_t)R.ntask;
 	if (ctx->job_cap < 3 * (size_t)R.ntask)
 		ctx->job_cap = 3 * (size_t)R.ntask;
-	int *d_cnt = ctx->counters.p + 5;
+	if (ctx->slot_cap < 4 * (size_t)R.ntask)
+		ctx->slot_cap = 4 * (size_t)R.ntask;
+	int *d_cnt = ctx->counters.p + 12;
 	cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
 	int nch = 0, nj = 0;
 	cudaEventRecord(e0, st);
 	for (int attempt = 0; attempt < 2; ++attempt) {
 		CK(ctx->chains.ensure(ctx->chain_cap), "chains");
 		CK(ctx->jobs.ensure(ctx->job_cap), "dp jobs");
+		CK(ctx->slots.ensure(ctx->slot_cap), "job slots");
 		R.tinfo = ctx->tinfo.p;
 		R.chains = ctx->chains.p;
+		R.slots = ctx->slots.p;
 		R.jobs = ctx->jobs.p;
 		R.cnt = d_cnt;
 		R.chain_cap = (int)ctx->chain_cap;
 		R.job_cap = (int)ctx->job_cap;
-		CK(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int), st), "memset");
+		R.slot_cap = (int)ctx->slot_cap;
+		CK(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(int), st), "memset");
 		k_build<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
 		++launches;
-		CK(cudaMemcpyAsync(ctx->h_small.p + 6, d_cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
+		CK(cudaMemcpyAsync(ctx->h_small.p + 12, d_cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
 		CK(cudaStreamSynchronize(st), "build");
-		nch = ctx->h_small.p[6];
-		nj = ctx->h_small.p[7];
-		if ((size_t)nch <= ctx->chain_cap && (size_t)nj <= ctx->job_cap)
+		nch = ctx->h_small.p[12];
+		nj = ctx->h_small.p[13];
+		const int ns = ctx->h_small.p[14];
+		ctx->timing.dp_calls += (uint64_t)ns;
+		if ((size_t)nch <= ctx->chain_cap && (size_t)nj <= ctx->job_cap && (size_t)ns <= ctx->slot_cap)
 			break;
+		ctx->timing.dp_calls -= (uint64_t)ns;
 		ctx->chain_cap = (size_t)nch + 16;
 		ctx->job_cap = (size_t)nj + 16;
+		ctx->slot_cap = (size_t)ns + 16;
 		if (attempt == 1)
 			return fail(ctx, HERA_GPU_ECAPACITY, "dp job buffers");
 	}
@@ -891,8 +903,8 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 		k_codes<<<1184, 256, 0, st>>>(d_seq, ctx->code.p, seq_bytes);
 		++launches;
 		if (batched) {
-			k_rc<<<blocks_for(n_reads, 256), 256, 0, st>>>(ctx->code.p, d_off, d_len, n_reads, max_len,
-									ctx->code_r.p);
+			k_rc<<<blocks_for((int64_t)n_reads * 32, 256), 256, 0, st>>>(ctx->code.p, d_off, d_len, n_reads,
+										      max_len, ctx->code_r.p);
 			++launches;
 		}
 	}

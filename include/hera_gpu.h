@@ -156,7 +156,8 @@ typedef struct hera_gpu_timing {
 	uint32_t launches;       /* kernels launched by the last call */
 	uint32_t rescue_rounds;  /* control-flow rounds after the first */
 	uint64_t lookups;        /* seed-table lookups issued by seed_probe */
-	uint64_t dp_jobs;        /* batched form: gap-DP jobs run */
+	uint64_t dp_jobs;        /* batched form: gap-DP jobs run (after deduplication) */
+	uint64_t dp_calls;       /* batched form: SW_align calls those jobs served */
 } hera_gpu_timing;
 
 /* ---- entry points ------------------------------------------------------ */

@@ -1,0 +1,38 @@
+"""Live cross-check of the oracle against the reference program built here
+(oracle/_ref/libhera_ref.so); skipped where the reference was not built."""
+import numpy as np
+import pytest
+
+import oracle
+from hera_b200 import synth, workloads
+
+pytestmark = pytest.mark.skipif(not oracle.reference_available(), reason="reference not built")
+
+
+@pytest.fixture(scope="module")
+def both(config1):
+    ann, tx, ix = config1
+    return ann, tx, oracle.Oracle(ix), oracle.Reference(ix)
+
+
+@pytest.mark.parametrize("wl", ["config1", "config3", "config4"])
+def test_pairs_match_reference(both, wl):
+    ann, tx, o, ref = both
+    r1, r2 = workloads.pairs(wl, ann, tx, 3000, seed=101)
+    for wb in (1, 0):
+        a = o.align_pairs(r1.copy(), r2.copy(), wb).canonical()
+        b = ref.align_pairs(r1.copy(), r2.copy(), wb).canonical()
+        assert a == b
+
+
+def test_reads_modified_like_reference(both):
+    """Lower-case a/c/g/t come back upper-case from the front half."""
+    ann, tx, o, ref = both
+    r1, r2 = synth.simulate_pairs(tx, 500, seed=102)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    r1.seq[:] = np.where(np.isin(r1.seq, acgt), r1.seq + 32, r1.seq)
+    a1, a2, b1, b2 = r1.copy(), r2.copy(), r1.copy(), r2.copy()
+    o.align_pairs(a1, a2, 1)
+    ref.align_pairs(b1, b2, 1)
+    assert np.array_equal(a1.seq, b1.seq) and np.array_equal(a2.seq, b2.seq)
+    assert not np.isin(a1.seq, np.frombuffer(b"acgt", np.uint8)).any()
