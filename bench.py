@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=200_000, help="pairs per CPU-baseline slice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--paths", default="plain,batched", help="execution forms to time (batched last)")
+    ap.add_argument("--lanes", type=int, default=0, help="concurrent sub-batches (0 = library default)")
     return ap.parse_args()
 
 
@@ -238,7 +240,7 @@ def main():
     torch.cuda.synchronize()
 
     def measure(path):
-        ctx = api.Context(ix, device=local, max_batch=args.chunk, path=path)
+        ctx = api.Context(ix, device=local, path=path, lanes=args.lanes)
         stream = torch.cuda.ExternalStream(ctx.stream)
 
         def step(i):
@@ -280,17 +282,21 @@ def main():
                "dp_jobs": jobs, "dp_calls": calls, "lookups": lookups, "clocks": clocks}
         return ctx, out
 
-    ctx_p, plain = measure("plain")
-    ctx_p.close()
-    ctx, batched = measure("batched")
+    paths = [p for p in args.paths.split(",") if p]
+    plain = None
+    if "plain" in paths:
+        ctx_p, plain = measure("plain")
+        ctx_p.close()
+    main_path = "batched" if "batched" in paths else "plain"
+    ctx, batched = measure(main_path)
     value = args.chunk * args.steps * world / (batched["ms"] / 1000.0)
-    plain_value = args.chunk * args.steps * world / (plain["ms"] / 1000.0)
+    plain_value = args.chunk * args.steps * world / (plain["ms"] / 1000.0) if plain else None
 
     # end to end through the public C ABI with host buffers
     e2e = None
     if not args.no_e2e:
         r1, r2 = chunks[0]
-        ctx.align_pairs(r1, r2, args.write_bam)   # warm the staging buffers
+        out = ctx.align_pairs(r1, r2, args.write_bam)   # warm staging and result buffers
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -298,7 +304,7 @@ def main():
         h2d = d2h = 0
         for i in range(args.steps):
             r1, r2 = chunks[i % len(chunks)]
-            res = ctx.align_pairs(r1, r2, args.write_bam)
+            res = ctx.align_pairs(r1, r2, args.write_bam, out=out)
             h2d += int(r1.len.sum() + r2.len.sum()) + 12 * 2 * r1.n
             d2h += (res.recs.nbytes + 8 * int(res.c.list_used) + 4 * int(res.c.op_used)
                     + int(res.c.miss_used))
@@ -325,13 +331,15 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {workloads.DESCRIPTION[args.workload]}",
                        "pairs_per_step": args.chunk, "write_bam": args.write_bam,
-                       "path": "batched (build / length-binned DP jobs / replay rounds)",
+                       "path": ("batched (build / length-binned DP jobs / replay rounds)"
+                                if main_path == "batched" else "plain (thread per call / pair)"),
                        "l2": "inputs larger than L2 (reads 200 MB/step, index in HBM)",
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": per[len(per) // 2], "p99": per[min(len(per) - 1, int(0.99 * len(per)))]},
-            "plain": {"value": plain_value, "ms_per_step": plain["ms"] / args.steps,
-                      "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
-                      "gpu_launches": plain["launches"]},
+            "plain": None if plain is None else {
+                "value": plain_value, "ms_per_step": plain["ms"] / args.steps,
+                "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
+                "gpu_launches": plain["launches"]},
             "stage_ms_per_step": {k: v / args.steps for k, v in st.items()},
             "dp_jobs_per_step": batched["dp_jobs"] // args.steps,
             "dp_calls_per_step": batched["dp_calls"] // args.steps,

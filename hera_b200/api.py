@@ -49,7 +49,7 @@ class _IndexView(C.Structure):
 
 class _Options(C.Structure):
     _fields_ = [("device", C.c_int), ("max_batch", C.c_uint32), ("scratch_bytes", C.c_uint64),
-                ("path", C.c_int)]
+                ("path", C.c_int), ("lanes", C.c_int)]
 
 
 PATH_BATCHED = 0
@@ -117,17 +117,29 @@ class Result:
     """Flat Candidate records (hera_cand_rec) plus their pools."""
 
     def __init__(self, n_recs: int, list_cap: int, op_cap: int, miss_cap: int):
-        self.recs = np.zeros(max(n_recs, 1), dtype=REC_DTYPE)[:n_recs]
+        self._rec_buf = np.empty(max(n_recs, 1), dtype=REC_DTYPE)
+        self.recs = self._rec_buf[:n_recs]
         self._alloc(list_cap, op_cap, miss_cap)
 
     def _alloc(self, list_cap, op_cap, miss_cap):
-        self.pos_pool = np.zeros(max(list_cap, 1), np.uint32)
-        self.p_pool = np.zeros(max(list_cap, 1), np.int32)
-        self.op_pool = np.zeros(max(op_cap, 1), np.uint32)
-        self.miss_pool = np.zeros(max(miss_cap, 1), np.uint8)
+        self.pos_pool = np.empty(max(list_cap, 1), np.uint32)
+        self.p_pool = np.empty(max(list_cap, 1), np.int32)
+        self.op_pool = np.empty(max(op_cap, 1), np.uint32)
+        self.miss_pool = np.empty(max(miss_cap, 1), np.uint8)
+        self._bind(list_cap, op_cap, miss_cap)
+
+    def _bind(self, list_cap, op_cap, miss_cap):
         base = self.recs.ctypes.data if self.recs.shape[0] else 0
         self.c = _Result(base, _ptr(self.pos_pool), _ptr(self.p_pool), _ptr(self.op_pool),
                          _ptr(self.miss_pool), list_cap, op_cap, miss_cap, 0, 0, 0)
+
+    def reuse(self, n_recs: int) -> "Result":
+        """Make room for n_recs records, keeping the pools' storage."""
+        if self._rec_buf.shape[0] < n_recs:
+            self._rec_buf = np.empty(n_recs, dtype=REC_DTYPE)
+        self.recs = self._rec_buf[:n_recs]
+        self._bind(self.pos_pool.shape[0], self.op_pool.shape[0], self.miss_pool.shape[0])
+        return self
 
     def candidate(self, i: int):
         """(pair, ((n, err, pos, p, cigar, miss) for strand 0, 1))."""
@@ -152,7 +164,7 @@ class Context:
     """One hera index resident on one GPU."""
 
     def __init__(self, index, device: int = 0, max_batch: int = 0, scratch_bytes: int = 0,
-                 path: str = "batched"):
+                 path: str = "batched", lanes: int = 0):
         self.lib = load_library()
         self.index = index
         v = _IndexView()
@@ -170,7 +182,8 @@ class Context:
         if path not in ("batched", "plain"):
             raise ValueError(f"unknown path {path!r}")
         self.path = path
-        opt = _Options(device, max_batch, scratch_bytes, PATH_PLAIN if path == "plain" else PATH_BATCHED)
+        opt = _Options(device, max_batch, scratch_bytes, PATH_PLAIN if path == "plain" else PATH_BATCHED,
+                       lanes)
         h = C.c_void_p()
         rc = self.lib.hera_gpu_ctx_create(C.byref(v), C.byref(opt), C.byref(h))
         if rc != HERA_GPU_OK:
@@ -197,8 +210,11 @@ class Context:
     def _reads(rs) -> _Reads:
         return _Reads(_ptr(rs.seq), _ptr(rs.off), _ptr(rs.len))
 
-    def _run(self, fn, n_recs, total_len, args) -> Result:
-        res = Result(n_recs, n_recs * 8 + 1024, n_recs * 8 + 1024, total_len // 4 + 1024)
+    def _run(self, fn, n_recs, total_len, args, out: Optional[Result] = None) -> Result:
+        if out is not None:
+            res = out.reuse(n_recs)
+        else:
+            res = Result(n_recs, n_recs * 4 + 1024, n_recs * 4 + 1024, total_len // 8 + 1024)
         rc = fn(*args, C.byref(res.c))
         if rc == -5 and (res.c.list_used > res.c.list_cap or res.c.op_used > res.c.op_cap
                          or res.c.miss_used > res.c.miss_cap):
@@ -207,17 +223,18 @@ class Context:
         self._check(rc)
         return res
 
-    def align_pairs(self, r1, r2, write_bam: int = 1) -> Result:
-        """Paired reads (synth.ReadSet-like: seq, off, len) -> 2 records per pair."""
+    def align_pairs(self, r1, r2, write_bam: int = 1, out: Optional[Result] = None) -> Result:
+        """Paired reads (synth.ReadSet-like: seq, off, len) -> 2 records per
+        pair.  `out`: a Result to reuse (its storage is overwritten)."""
         a, b = self._reads(r1), self._reads(r2)
         return self._run(self.lib.hera_gpu_align_pairs_flat, 2 * r1.n,
                          int(r1.len.sum()) + int(r2.len.sum()),
-                         (self.h, C.byref(a), C.byref(b), r1.n, write_bam))
+                         (self.h, C.byref(a), C.byref(b), r1.n, write_bam), out)
 
-    def align_single(self, rs, write_bam: int = 1) -> Result:
+    def align_single(self, rs, write_bam: int = 1, out: Optional[Result] = None) -> Result:
         a = self._reads(rs)
         return self._run(self.lib.hera_gpu_align_single_flat, rs.n, int(rs.len.sum()),
-                         (self.h, C.byref(a), rs.n, write_bam))
+                         (self.h, C.byref(a), rs.n, write_bam), out)
 
     def align_pairs_device(self, d_seq: int, d_off: int, d_len: int, n: int, max_len: int,
                            write_bam: int = 1, stream: Optional[int] = None) -> None:

@@ -71,6 +71,8 @@ __host__ __device__ inline int res_stride(int cap)
 
 struct Round {
 	const GpReq *req;         // null: round 0 (task t = pair t>>2, c (t>>1)&1, str t&1)
+	const int *list;          // round 0: the tasks k_build runs (those with seed hits)
+	const int *nlist;         // ... and their number (device)
 	int ntask;
 	int space;
 	const uint2 *hits;        // precomputed seeds (round 0) or null
@@ -84,6 +86,42 @@ struct Round {
 	uint8_t *res;
 	int rcap;                 // CIGAR ops per job result
 };
+
+// round 0: reset every pair's Candidate state and list the get_position
+// calls that have at least one seed hit (the others take the miss exit)
+__global__ void k_task_list(Batch b, int ntask, const uint2 *__restrict__ hits, int spr,
+			    TaskInfo *__restrict__ tinfo, int *__restrict__ list, int *__restrict__ nlist)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= ntask)
+		return;
+	const int pi = t >> 2, c = (t >> 1) & 1, str = t & 1;
+	DPair &P = b.P[pi];
+	DSlot &S = P.s[c][str];
+	S.n = 0;
+	S.err = 0;
+	S.cig.n = S.cig.nm = 0;
+	if (str == 0)
+		P.pair[c] = 0;
+	if ((t & 3) == 0) {
+		P.stage = 0;
+		P.rm_ret = 0;
+	}
+	tinfo[t].chain0 = 0;
+	tinfo[t].nch = -1;
+	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	if (L > b.max_len) {
+		flag(b.flags, F_READ);
+		return;
+	}
+	const uint2 *h = hits + ((int64_t)ri * 2 + str) * spr;
+	bool any = false;
+	for (int j = 0; j * KMER + KMER <= L; ++j)
+		any |= h[j].y != 0;
+	if (any)
+		list[atomicAdd(nlist, 1)] = t;
+}
 
 __device__ __forceinline__ void task_of(const Round &R, int t, int &pi, int &c, int &str)
 {
@@ -111,16 +149,16 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 	auto next = [&](uint32_t i, uint32_t n, bool stop_used) -> bool {
 		if (i + 1 >= (uint32_t)na)
 			return false;
-		if (A.t[i] != A.t[i + 1])
+		if (A.a[i].t != A.a[i + 1].t)
 			return false;
 		// read offsets of used anchors read as rlen in the reference
-		const uint32_t o0 = is_used(i) ? (uint32_t)rlen : A.off[i];
-		const uint32_t o1 = is_used(i + 1) ? (uint32_t)rlen : A.off[i + 1];
+		const uint32_t o0 = is_used(i) ? (uint32_t)rlen : A.a[i].off;
+		const uint32_t o1 = is_used(i + 1) ? (uint32_t)rlen : A.a[i + 1].off;
 		if (!(o1 > o0))
 			return false;
-		if (!(A.tp[i + 1] > A.tp[i + 1 - n]))
+		if (!(A.a[i + 1].tp > A.a[i + 1 - n].tp))
 			return false;
-		if (!(A.tp[i + 1] - A.tp[i + 1 - n] < (uint32_t)rlen))
+		if (!(A.a[i + 1].tp - A.a[i + 1 - n].tp < (uint32_t)rlen))
 			return false;
 		if (stop_used && o1 == (uint32_t)rlen)
 			return false;
@@ -131,9 +169,9 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 		const uint32_t mn = (uint32_t)Mt.n;
 		uint32_t k = 0;
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (A.t[i] < Mt.t[k])
+			if (A.a[i].t < Mt.t[k])
 				continue;
-			while (k < mn && A.t[i] > Mt.t[k])
+			while (k < mn && A.a[i].t > Mt.t[k])
 				++k;
 			if (k == mn)
 				break;
@@ -148,7 +186,7 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 		}
 	}
 	for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-		if (is_used(i) || A.off[i] == (uint32_t)rlen)
+		if (is_used(i) || A.a[i].off == (uint32_t)rlen)
 			continue;
 		uint32_t n = 1;
 		while (next(i, n, true)) {
@@ -161,7 +199,7 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 	}
 	if (space < KMER) {
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (is_used(i) || A.off[i] == (uint32_t)rlen)
+			if (is_used(i) || A.a[i].off == (uint32_t)rlen)
 				continue;
 			uint32_t n = 1;
 			while (next(i, n, true)) {
@@ -189,27 +227,20 @@ struct BuildWork {
 
 __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 {
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= R.ntask)
+	int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (R.list) {
+		if (t >= *R.nlist)
+			return;
+		t = R.list[t];
+	} else if (t >= R.ntask) {
 		return;
+	}
 	int pi, c, str;
 	task_of(R, t, pi, c, str);
 	DPair &P = b.P[pi];
-	DSlot &S = P.s[c][str];
 	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
 	const int L = b.len[ri];
 	int flags = 0;
-	if (!R.req) {   // round 0 starts the pair's Candidate state
-		S.n = 0;
-		S.err = 0;
-		S.cig.n = S.cig.nm = 0;
-		if (str == 0)
-			P.pair[c] = 0;
-		if (t % 4 == 0) {
-			P.stage = 0;
-			P.rm_ret = 0;
-		}
-	}
 	R.tinfo[t].chain0 = 0;
 	R.tinfo[t].nch = -1;
 	if (L > b.max_len) {
@@ -233,9 +264,9 @@ __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 			}
 			for (uint32_t k = 0; k < nh; ++k) {
 				uint2 o = __ldg(occ + k);
-				w.a[cur].t[k] = o.x;
-				w.a[cur].tp[k] = o.y;
-				w.a[cur].off[k] = i;
+				w.a[cur].a[k].t = o.x;
+				w.a[cur].a[k].tp = o.y;
+				w.a[cur].a[k].off = i;
 			}
 			na = (int)nh;
 			continue;
@@ -287,31 +318,31 @@ __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 			return;
 		}
 		Chain &ch = w.ch[nch++];
-		ch.t = A.t[id];
-		ch.tp = A.tp[id];
-		ch.off = A.off[id];
+		ch.t = A.a[id].t;
+		ch.tp = A.a[id].tp;
+		ch.off = A.a[id].off;
 		ch.pass = (int8_t)pass;
 		ch.viable = 0;
 		ch.has_prefix = 0;
 		ch.js0 = ns;
 		ch.njs = 0;
 		// get_SWalign's early returns before any DP (:1250-1256)
-		if (n > 1 && A.tp[id + n - 1] - A.tp[id] > (uint32_t)L)
+		if (n > 1 && A.a[id + n - 1].tp - A.a[id].tp > (uint32_t)L)
 			return;
-		const int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
-		if (start < 0 || (uint32_t)(start + L) > __ldg(b.ix.tlen + A.t[id]))
+		const int start = (int)(A.a[id].tp - (A.a[id].off + KMER - 1));
+		if (start < 0 || (uint32_t)(start + L) > __ldg(b.ix.tlen + A.a[id].t))
 			return;
 		ch.viable = 1;
 		const uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
-		const uint32_t ref_start = __ldg(b.ix.tstart + A.t[id]) + (uint32_t)start;
+		const uint32_t ref_start = __ldg(b.ix.tstart + A.a[id].t) + (uint32_t)start;
 		DpJob j;
 		j.orient = (int8_t)str;
 		j.read = ri;
 		j.pad = 0;
 		j.pad0 = 0;
 		const int ns0 = ns;
-		if (A.off[id] > 0) {   // prefix DP on the reversed strings (:1262-1266)
-			const uint32_t o0 = A.off[id];
+		if (A.a[id].off > 0) {   // prefix DP on the reversed strings (:1262-1266)
+			const uint32_t o0 = A.a[id].off;
 			ch.has_prefix = 1;
 			j.rstart = ref_start - add;
 			j.ref_len = (uint16_t)(o0 + add);
@@ -322,17 +353,17 @@ __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 		}
 		for (uint32_t i = 0; i < n; ++i) {   // merged runs and their gaps (:1282-1305)
 			const uint32_t s0 = i;
-			while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
+			while (i + 1 < n && A.a[id + i].off + KMER >= A.a[id + i + 1].off)
 				++i;
-			const uint32_t seg = A.off[id + i] + KMER;
-			const uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)L) - seg;
+			const uint32_t seg = A.a[id + i].off + KMER;
+			const uint32_t len = ((i + 1) < n ? A.a[id + i + 1].off : (uint32_t)L) - seg;
 			const uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
 			j.rstart = ref_start + seg;
 			j.ref_len = (uint16_t)(len + ad);
 			j.len = (uint16_t)len;
 			j.qoff = (uint16_t)seg;
 			j.err = (int8_t)(len < 2 * ERR ? 3 : ERR);
-			add_job(j, (uint16_t)(A.off[id + i] - A.off[id + s0] + KMER));
+			add_job(j, (uint16_t)(A.a[id + i].off - A.a[id + s0].off + KMER));
 		}
 		ch.njs = (int16_t)(ns - ns0);
 	});
@@ -367,11 +398,19 @@ __device__ __forceinline__ int job_bin(const DpJob &j)
 	return (e == 7 ? 1 : 0) * (MAX_READ + 1) + (j.len <= MAX_READ ? j.len : MAX_READ);
 }
 
+// histogram of job bins: per-block shared counts, one global atomic per bin
 __global__ void k_bin_count(const DpJob *__restrict__ jobs, int n, int *__restrict__ hist)
 {
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t < n)
-		atomicAdd(hist + job_bin(jobs[t]), 1);
+	__shared__ int h[NBIN];
+	for (int i = threadIdx.x; i < NBIN; i += blockDim.x)
+		h[i] = 0;
+	__syncthreads();
+	for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+		atomicAdd(h + job_bin(jobs[t]), 1);
+	__syncthreads();
+	for (int i = threadIdx.x; i < NBIN; i += blockDim.x)
+		if (h[i])
+			atomicAdd(hist + i, h[i]);
 }
 
 // exclusive scan of the (small) histogram, one block
@@ -402,74 +441,119 @@ __global__ void k_bin_scan(int *__restrict__ hist, int nbin)
 	}
 }
 
+// scatter jobs into bin order: per-block shared counts reserve a range of
+// each bin with one global atomic, then threads take slots in shared memory
 __global__ void k_bin_scatter(const DpJob *__restrict__ jobs, int n, int *__restrict__ cursor,
 			      int *__restrict__ perm)
 {
+	__shared__ int h[NBIN];
+	__shared__ int base[NBIN];
+	for (int i = threadIdx.x; i < NBIN; i += blockDim.x)
+		h[i] = 0;
+	__syncthreads();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	int bin = -1, rank = 0;
+	if (t < n) {
+		bin = job_bin(jobs[t]);
+		rank = atomicAdd(h + bin, 1);
+	}
+	__syncthreads();
+	for (int i = threadIdx.x; i < NBIN; i += blockDim.x)
+		if (h[i])
+			base[i] = atomicAdd(cursor + i, h[i]);
+	__syncthreads();
 	if (t < n)
-		perm[atomicAdd(cursor + job_bin(jobs[t]), 1)] = t;
+		perm[base[bin] + rank] = t;
 }
 
-struct DpWork {
-	uint8_t rows[(MAX_DP_ROWS + 1) * 20];
-	DCig cig;
-	SwWork sw;     // only for the general banded form
-};
+__device__ inline void store_res(const DCig &cig, int score, uint8_t *o, int rcap, int &flags)
+{
+	DpResHdr h;
+	int sub = 0;
+	for (int k = 0; k < cig.n; ++k) {
+		const int ty = op_type(cig.op[k]);
+		if (ty == OP_I || ty == OP_S)
+			sub += (int)op_cnt(cig.op[k]);
+		else if (ty == OP_D)
+			sub -= (int)op_cnt(cig.op[k]);
+	}
+	if (cig.n > rcap || cig.nm > rcap)
+		flags |= F_CCAP;
+	h.score = (int16_t)score;
+	h.sub = (int16_t)sub;
+	h.n = (uint8_t)(cig.n < rcap ? cig.n : rcap);
+	h.nm = (uint8_t)(cig.nm < rcap ? cig.nm : rcap);
+	h.pad[0] = h.pad[1] = 0;
+	*reinterpret_cast<DpResHdr *>(o) = h;
+	uint32_t *ops = reinterpret_cast<uint32_t *>(o + sizeof(DpResHdr));
+	for (int k = 0; k < h.n; ++k)
+		ops[k] = cig.op[k];
+	uint8_t *miss = o + sizeof(DpResHdr) + 4 * rcap;
+	for (int k = 0; k < h.nm; ++k)
+		miss[k] = cig.miss[k];
+}
 
-// one thread per job, jobs in (error cap, length) order
-__global__ void __launch_bounds__(128) k_dp(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm,
-					    int n, uint8_t *__restrict__ res, int rcap)
+// which kernel computes a job: the register form for the two live error
+// caps (when no row-0 spill can occur), the general banded form otherwise
+__device__ __forceinline__ int job_form(const DpJob &j)
+{
+	const int e = j.err < 0 ? -j.err : j.err;
+	if (j.len == 0)
+		return 0;
+	if (e == 7 && j.ref_len >= 9)
+		return 8;
+	if (e == 3 && j.ref_len >= 5)
+		return 4;
+	return 0;
+}
+
+// one thread per job, jobs in (error cap, length) order; threads whose job
+// is not of cap E leave at once (whole warps, the order is by cap)
+template <int E>
+__global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
+k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
+	 int rcap)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n)
 		return;
 	const int id = perm[t];
 	const DpJob jb = jobs[id];
-	DpWork w;
+	if (job_form(jb) != E)
+		return;
+	__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
+	DCig cig;
 	int flags = 0;
-	const bool so = b.score_only != 0;
+	cig.n = cig.nm = 0;
+	const bool rev = jb.err < 0;
 	const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
-	const uint32_t ref_len = jb.ref_len, len = jb.len;
-	int score;
-	w.cig.n = w.cig.nm = 0;
-	if (len == 0) {
-		score = 0;
-	} else {
-		const bool rev = jb.err < 0;
-		const int e = rev ? -jb.err : jb.err;
-		RefWin r{b.ix.code, b.ix.seq, jb.rstart, ref_len, rev};
-		QView qv{rev ? q + (len - 1) : q, rev ? -1 : 1};
-		if (e == 7 && ref_len >= 9)
-			score = sw_align_reg<8>(r, qv, ref_len, len, so, w.cig, w.rows, flags);
-		else if (e == 3 && ref_len >= 5)
-			score = sw_align_reg<4>(r, qv, ref_len, len, so, w.cig, w.rows, flags);
-		else
-			score = sw_align(b.ix, jb.rstart, q, ref_len, len, jb.err, so, w.cig, w.sw, flags);
+	RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
+	QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
+	const int score = sw_align_fast<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags);
+	store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+	flag(b.flags, flags);
+}
+
+// the jobs outside the register form (empty gaps, spill cases)
+__global__ void __launch_bounds__(128) k_dp_generic(Batch b, const DpJob *__restrict__ jobs, int n,
+						    uint8_t *__restrict__ res, int rcap)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
+		return;
+	const DpJob jb = jobs[id];
+	if (job_form(jb) != 0)
+		return;
+	SwWork sw;
+	DCig cig;
+	int flags = 0;
+	cig.n = cig.nm = 0;
+	int score = 0;
+	if (jb.len > 0) {
+		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+		score = sw_align(b.ix, jb.rstart, q, jb.ref_len, jb.len, jb.err, b.score_only != 0, cig, sw, flags);
 	}
-	uint8_t *o = res + (size_t)id * res_stride(rcap);
-	DpResHdr h;
-	int sub = 0;
-	for (int k = 0; k < w.cig.n; ++k) {
-		const int ty = op_type(w.cig.op[k]);
-		if (ty == OP_I || ty == OP_S)
-			sub += (int)op_cnt(w.cig.op[k]);
-		else if (ty == OP_D)
-			sub -= (int)op_cnt(w.cig.op[k]);
-	}
-	if (w.cig.n > rcap || w.cig.nm > rcap)
-		flags |= F_CCAP;
-	h.score = (int16_t)score;
-	h.sub = (int16_t)sub;
-	h.n = (uint8_t)(w.cig.n < rcap ? w.cig.n : rcap);
-	h.nm = (uint8_t)(w.cig.nm < rcap ? w.cig.nm : rcap);
-	h.pad[0] = h.pad[1] = 0;
-	*reinterpret_cast<DpResHdr *>(o) = h;
-	uint32_t *ops = reinterpret_cast<uint32_t *>(o + sizeof(DpResHdr));
-	for (int k = 0; k < h.n; ++k)
-		ops[k] = w.cig.op[k];
-	uint8_t *miss = o + sizeof(DpResHdr) + 4 * rcap;
-	for (int k = 0; k < h.nm; ++k)
-		miss[k] = w.cig.miss[k];
+	store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
 	flag(b.flags, flags);
 }
 

@@ -363,27 +363,30 @@ struct QView {   // query codes: q(x) = p[x * step]
 	__device__ __forceinline__ uint8_t operator()(int x) const { return p[x * step]; }
 };
 
-template <int E>
+template <int E, bool STORE>
 __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
 				   bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags)
 {
 	constexpr int W = 2 * E + 2;
 	constexpr unsigned error = E;
+	constexpr int RS = ((W + 3) / 4) * 4;   // bytes per stored row
 	// reference code at window position x, clamped (values outside the
 	// window are never used, the clamp only keeps the address valid)
 	auto rcode = [&](int x) -> int {
 		x = x < 0 ? 0 : (x >= (int)ref_len ? (int)ref_len - 1 : x);
 		return r.c(x);
 	};
-	int P[W], V[W], RC[W];
+	// P: the previous row, updated in place into the current row (slot q
+	// reads P[q] and P[q+1] before it is overwritten)
+	int P[W], RC[W];
 #pragma unroll
 	for (int q = 0; q < W; ++q) {
 		const int d = q - E;
 		P[q] = (d >= 0) ? d : 0;          // row 0: M[0][c] = c, c <= error+1
 		RC[q] = rcode(q - E);             // row 1 needs r[c-1], c = 1 + q - E
 	}
-	{
-		uint32_t *o = reinterpret_cast<uint32_t *>(rows);
+	auto store_row = [&](int k) {
+		uint32_t *o = reinterpret_cast<uint32_t *>(rows + k * RS);
 #pragma unroll
 		for (int w = 0; w < (W + 3) / 4; ++w) {
 			uint32_t pk = 0;
@@ -393,8 +396,9 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 					pk |= (uint32_t)P[w * 4 + b] << (8 * b);
 			o[w] = pk;
 		}
-	}
-	constexpr int RS = ((W + 3) / 4) * 4;   // bytes per stored row
+	};
+	if (STORE)
+		store_row(0);
 	auto get = [&](int k, int c) -> unsigned {
 		const int q = c - k + E;
 		return (q >= 0 && q < W) ? rows[k * RS + q] : 0u;
@@ -421,11 +425,11 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 		for (int q = 0; q < W; ++q) {
 			const int c = k + q - E;
 			const int up = (q + 1 < W) ? P[q + 1] : 0;
+			const int dg = P[q];
 			int v = 0;
 			if (c == s) {
 				v = up + 1;   // left edge: M[k-1][s] + 1
 			} else if (c > s && !broken && c <= (int)ref_len) {
-				const int dg = P[q];
 				if (dg == (int)error + 1) {
 					v = error + 1;
 					broken = true;
@@ -447,7 +451,7 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 						ferr = c;
 				}
 			}
-			V[q] = v;
+			P[q] = v;
 			left = v;
 		}
 		i = broken ? brk : (int)ref_len + 1;
@@ -458,7 +462,7 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 			for (int q = 0; q < W; ++q) {
 				const int c = k + q - E;
 				if (go && c == s) {
-					if (V[q] >= (int)error && s < i)
+					if (P[q] >= (int)error && s < i)
 						++s;
 					else
 						go = false;
@@ -468,28 +472,17 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 #pragma unroll
 				for (int q = 0; q < W; ++q)
 					if (k + q - E == j)
-						V[q] = error + 1;
+						P[q] = error + 1;
 			}
 		}
-		{
-			uint32_t *o = reinterpret_cast<uint32_t *>(rows + k * RS);
-#pragma unroll
-			for (int w = 0; w < (W + 3) / 4; ++w) {
-				uint32_t pk = 0;
-#pragma unroll
-				for (int b = 0; b < 4; ++b)
-					if (w * 4 + b < W)
-						pk |= (uint32_t)V[w * 4 + b] << (8 * b);
-				o[w] = pk;
-			}
-		}
+		if (STORE)
+			store_row(k);
 		if (min == error) {
+			if (!STORE)
+				return -1;   // early stop: the shrink loop needs the rows
 			++k;
 			break;
 		}
-#pragma unroll
-		for (int q = 0; q < W; ++q)
-			P[q] = V[q];
 	}
 	--k;
 
@@ -530,6 +523,8 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}
+	if (!STORE)
+		return -1;
 	while (i > 0 && k > 0) {
 		const unsigned cur = get(i, k);
 		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
@@ -553,6 +548,22 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 	for (int t = 1; t <= k; ++t)
 		cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	return score;
+}
+
+// Register-form SW_align: a forward pass without row storage first (enough
+// for the score-only mode unless the DP stops early); otherwise rerun with
+// the rows kept for the shrink loop and the traceback.
+template <int E>
+__device__ inline int sw_align_fast(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
+				    bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags)
+{
+	if (score_only) {
+		const int sc = sw_align_reg<E, false>(r, qc, ref_len, len, true, cig, rows, flags);
+		if (sc >= 0)
+			return sc;
+		cig.n = cig.nm = 0;
+	}
+	return sw_align_reg<E, true>(r, qc, ref_len, len, score_only, cig, rows, flags);
 }
 
 // Entry used by the per-task (plain) path: the banded form, which keeps the
@@ -629,9 +640,13 @@ struct DPair {
 	int32_t pad;
 };
 
-// Anchors of one get_position call: pos2[0..2] of the reference.
+// Anchors of one get_position call: pos2[0..2] of the reference, one
+// 12-byte record per anchor so a call's few anchors share cache lines.
+struct Anc {
+	uint32_t t, tp, off;    // transcript, transcript position, read offset
+};
 struct Anchors {
-	uint32_t t[ACAP], tp[ACAP], off[ACAP];
+	Anc a[ACAP];
 };
 
 struct GpWork {
@@ -657,19 +672,19 @@ __device__ inline int merge_hits(const Anchors &A, int na, Anchors &B, const uin
 	uint2 h = nh ? __ldg(occ) : make_uint2(0, 0);
 	while (i < na && k < nh) {
 		bool take_a;
-		if (A.t[i] < h.x) {
+		if (A.a[i].t < h.x) {
 			take_a = true;
-		} else if (A.t[i] > h.x) {
+		} else if (A.a[i].t > h.x) {
 			take_a = false;
 		} else {
-			uint32_t dis = (h.y - A.tp[i]) - (idx - A.off[i]);
-			take_a = dis < 2 * ERR ? true : !(A.tp[i] > h.y);
+			uint32_t dis = (h.y - A.a[i].tp) - (idx - A.a[i].off);
+			take_a = dis < 2 * ERR ? true : !(A.a[i].tp > h.y);
 		}
 		if (take_a) {
-			B.t[n] = A.t[i]; B.tp[n] = A.tp[i]; B.off[n] = A.off[i];
+			B.a[n].t = A.a[i].t; B.a[n].tp = A.a[i].tp; B.a[n].off = A.a[i].off;
 			++i;
 		} else {
-			B.t[n] = h.x; B.tp[n] = h.y; B.off[n] = idx;
+			B.a[n].t = h.x; B.a[n].tp = h.y; B.a[n].off = idx;
 			++k;
 			if (k < nh)
 				h = __ldg(occ + k);
@@ -677,12 +692,12 @@ __device__ inline int merge_hits(const Anchors &A, int na, Anchors &B, const uin
 		++n;
 	}
 	while (i < na) {
-		B.t[n] = A.t[i]; B.tp[n] = A.tp[i]; B.off[n] = A.off[i];
+		B.a[n].t = A.a[i].t; B.a[n].tp = A.a[i].tp; B.a[n].off = A.a[i].off;
 		++i; ++n;
 	}
 	while (k < nh) {
 		h = __ldg(occ + k);
-		B.t[n] = h.x; B.tp[n] = h.y; B.off[n] = idx;
+		B.a[n].t = h.x; B.a[n].tp = h.y; B.a[n].off = idx;
 		++k; ++n;
 	}
 	return n;
@@ -693,10 +708,10 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 				   uint32_t id, uint32_t n, uint32_t &store, uint32_t &max,
 				   DSlot &S, bool score_only, GpWork &w, int &flags)
 {
-	if (n > 1 && A.tp[id + n - 1] - A.tp[id] > (uint32_t)rlen)
+	if (n > 1 && A.a[id + n - 1].tp - A.a[id].tp > (uint32_t)rlen)
 		return;
-	const uint32_t tr = A.t[id];
-	int start = (int)(A.tp[id] - (A.off[id] + KMER - 1));
+	const uint32_t tr = A.a[id].t;
+	int start = (int)(A.a[id].tp - (A.a[id].off + KMER - 1));
 	if (start < 0 || (uint32_t)(start + rlen) > __ldg(ix.tlen + tr))
 		return;
 	uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
@@ -705,8 +720,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 	DCig &cig = w.c1;
 	DCig &tmp = w.c2;
 	cig.n = cig.nm = 0;
-	if (A.off[id] > 0) {
-		const uint32_t o0 = A.off[id];
+	if (A.a[id].off > 0) {
+		const uint32_t o0 = A.a[id].off;
 		score = gap_dp(ix, ref_start - add, rd, 1, o0 + add, o0, o0 < 2 * ERR ? -3 : -ERR,
 			       score_only, cig, w.sw, flags);
 		err += score;
@@ -722,11 +737,11 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 	}
 	for (uint32_t i = 0; i < n; ++i) {
 		uint32_t s0 = i;
-		while (i + 1 < n && A.off[id + i] + KMER >= A.off[id + i + 1])
+		while (i + 1 < n && A.a[id + i].off + KMER >= A.a[id + i + 1].off)
 			++i;
-		cig_add(cig, OP_M, A.off[id + i] - A.off[id + s0] + KMER, nullptr, flags);
-		uint32_t seg = A.off[id + i] + KMER;
-		uint32_t len = ((i + 1) < n ? A.off[id + i + 1] : (uint32_t)rlen) - seg;
+		cig_add(cig, OP_M, A.a[id + i].off - A.a[id + s0].off + KMER, nullptr, flags);
+		uint32_t seg = A.a[id + i].off + KMER;
+		uint32_t len = ((i + 1) < n ? A.a[id + i + 1].off : (uint32_t)rlen) - seg;
 		uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
 		score = gap_dp(ix, ref_start + seg, rd + seg, 1, len + ad, len, len < 2 * ERR ? 3 : ERR,
 			       score_only, tmp, w.sw, flags);
@@ -740,8 +755,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 		store = 0;
 		max = (uint32_t)err;
 	}
-	A.t[store] = A.t[id];
-	A.tp[store] = A.tp[id] - (A.off[id] + KMER - 1) + (uint32_t)sub;
+	A.a[store].t = A.a[id].t;
+	A.a[store].tp = A.a[id].tp - (A.a[id].off + KMER - 1) + (uint32_t)sub;
 	++store;
 }
 
@@ -750,13 +765,13 @@ __device__ __forceinline__ bool chain_next(const Anchors &A, int na, uint32_t i,
 {
 	if (i + 1 >= (uint32_t)na)
 		return false;
-	if (A.t[i] != A.t[i + 1] || !(A.off[i + 1] > A.off[i]))
+	if (A.a[i].t != A.a[i + 1].t || !(A.a[i + 1].off > A.a[i].off))
 		return false;
-	if (!(A.tp[i + 1] > A.tp[i + 1 - n]))
+	if (!(A.a[i + 1].tp > A.a[i + 1 - n].tp))
 		return false;
-	if (!(A.tp[i + 1] - A.tp[i + 1 - n] < (uint32_t)rlen))
+	if (!(A.a[i + 1].tp - A.a[i + 1 - n].tp < (uint32_t)rlen))
 		return false;
-	if (stop_consumed && A.off[i + 1] == (uint32_t)rlen)
+	if (stop_consumed && A.a[i + 1].off == (uint32_t)rlen)
 		return false;
 	return true;
 }
@@ -788,9 +803,9 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 			Anchors &A = w.a[cur];
 			for (uint32_t k = 0; k < nh; ++k) {
 				uint2 o = __ldg(occ + k);
-				A.t[k] = o.x;
-				A.tp[k] = o.y;
-				A.off[k] = i;
+				A.a[k].t = o.x;
+				A.a[k].tp = o.y;
+				A.a[k].off = i;
 			}
 			na = (int)nh;
 			continue;
@@ -809,9 +824,9 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 		uint32_t k = 0;
 		max = (uint32_t)(rlen / 2);
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (A.t[i] < Mt.t[k])
+			if (A.a[i].t < Mt.t[k])
 				continue;
-			while (k < mn && A.t[i] > Mt.t[k])
+			while (k < mn && A.a[i].t > Mt.t[k])
 				++k;
 			if (k == mn)
 				break;
@@ -822,14 +837,14 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 			}
 			get_swalign(ix, rd, rlen, A, i + 1 - n, n, n1, max, S, score_only, w, flags);
 			for (; n > 0; --n)
-				A.off[i + 1 - n] = (uint32_t)rlen;
+				A.a[i + 1 - n].off = (uint32_t)rlen;
 		}
 	}
 	// pass B, chains of >= 2 anchors (:1392-1412)
 	if (n1 == 0) {
 		max = (uint32_t)(rlen / 2);
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (A.off[i] == (uint32_t)rlen)
+			if (A.a[i].off == (uint32_t)rlen)
 				continue;
 			n = 1;
 			while (chain_next(A, na, i, n, rlen, true)) {
@@ -845,7 +860,7 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 	if (n1 == 0 && space < KMER) {
 		max = (uint32_t)(rlen / 2);
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (A.off[i] == (uint32_t)rlen)
+			if (A.a[i].off == (uint32_t)rlen)
 				continue;
 			n = 1;
 			while (chain_next(A, na, i, n, rlen, true)) {
@@ -864,8 +879,8 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 		n1 = LCAP;
 	}
 	for (uint32_t t = 0; t < n1; ++t) {
-		S.t[t] = A.t[t];
-		S.p[t] = (int32_t)A.tp[t];
+		S.t[t] = A.a[t].t;
+		S.p[t] = (int32_t)A.a[t].tp;
 	}
 	S.n = (int32_t)n1;
 	S.err = (int32_t)max;
@@ -879,26 +894,26 @@ miss:
 // pairs kept (lists compacted in place), 0 if none.
 __device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
 {
-	DSlot &A = P.s[c][0];
-	DSlot &B = P.s[c][1];
+	DSlot &X = P.s[c][0];
+	DSlot &Y = P.s[c][1];
 	int i = 0, k = 0, n = 0;
-	while (i < A.n && k < B.n) {
-		if (A.t[i] < B.t[k]) {
+	while (i < X.n && k < Y.n) {
+		if (X.t[i] < Y.t[k]) {
 			++i;
-		} else if (A.t[i] > B.t[k]) {
+		} else if (X.t[i] > Y.t[k]) {
 			++k;
 		} else {
-			int d = A.p[i] - B.p[k];
+			int d = X.p[i] - Y.p[k];
 			uint32_t dis = (uint32_t)(d < 0 ? -d : d);
 			if (dis <= add || add == 0) {
 				++n;
-				A.t[n - 1] = A.t[i];
-				A.p[n - 1] = A.p[i];
-				B.t[n - 1] = B.t[k];
-				B.p[n - 1] = B.p[k];
+				X.t[n - 1] = X.t[i];
+				X.p[n - 1] = X.p[i];
+				Y.t[n - 1] = Y.t[k];
+				Y.p[n - 1] = Y.p[k];
 				++i;
 				++k;
-			} else if (A.p[i] < B.p[k]) {
+			} else if (X.p[i] < Y.p[k]) {
 				++i;
 			} else {
 				++k;
@@ -906,7 +921,7 @@ __device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
 		}
 	}
 	if (n > 0) {
-		A.n = B.n = n;
+		X.n = Y.n = n;
 		P.pair[c] = 2;
 	}
 	return n;
@@ -983,7 +998,7 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 		up_prev = up_in;
 		if (y >= 1 && y <= ln) {
 			const uint8_t rc = rf[y - 1];
-			int d = diag_in, up = up_in;
+			int d = diag_in, up = up_in, cmax = 0;
 			uint32_t pack[SSW_RMAX / 4 + 1];
 #pragma unroll
 			for (int w = 0; w < SSW_RMAX / 4 + 1; ++w)
@@ -991,29 +1006,28 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 #pragma unroll
 			for (int r = 0; r < SSW_RMAX; ++r) {
 				if (r < R) {
-					const int x = x0 + r;
 					const int left = Hl[r];
-					int e = left - 4;
-					e = e > 0 ? e : 0;
-					int f = up - 4;
-					f = f > 0 ? f : 0;
-					int h = d + (rdl[r] == rc ? 3 : 0);
-					h = h < 255 ? h : 255;
-					h = h > 2 ? h - 2 : 0;
-					int v = h > e ? h : e;
-					v = v > f ? v : f;
-					if (x >= L)
+					// max(0, min(255, d + 3*eq) - 2, left - 4, up - 4), d <= 253
+					const int a = __viaddmin_s32(d, rdl[r] == rc ? 1 : -2, 253);
+					int v = __vimax3_s32_relu(a, left - 4, up - 4);
+					if (x0 + r >= L)
 						v = 0;
 					d = left;
 					Hl[r] = v;
 					up = v;
-					if (v > best_v) {
-						best_v = v;
-						best_y = y;
-						best_x = x;
-					}
+					cmax = __vimax_s32_relu(cmax, v);
 					pack[r >> 2] |= (uint32_t)v << (8 * (r & 3));
 				}
+			}
+			if (cmax > best_v) {   // first row of this column reaching it
+				int fx = 0;
+#pragma unroll
+				for (int r = SSW_RMAX - 1; r >= 0; --r)
+					if (r < R && Hl[r] == cmax)
+						fx = r;
+				best_v = cmax;
+				best_y = y;
+				best_x = x0 + fx;
 			}
 			bot = Hl[R - 1];
 			uint32_t *dst = reinterpret_cast<uint32_t *>(Hs + ((size_t)t * 32 + lane) * Rp);

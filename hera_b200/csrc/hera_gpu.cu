@@ -20,7 +20,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace hg;
@@ -465,7 +469,7 @@ __global__ void k_emit(const DPair *__restrict__ P, int n_items, int ncand,
 // ===========================================================================
 
 template <typename T>
-struct DBuf {
+struct DBuf {   // growable device buffer
 	T *p = nullptr;
 	size_t cap = 0;
 	cudaError_t ensure(size_t n)
@@ -492,7 +496,7 @@ struct DBuf {
 };
 
 template <typename T>
-struct HBuf {   // pinned host staging
+struct HBuf {   // growable pinned host buffer
 	T *p = nullptr;
 	size_t cap = 0;
 	cudaError_t ensure(size_t n)
@@ -518,80 +522,114 @@ struct HBuf {   // pinned host staging
 	}
 };
 
+// One lane: a stream, the per-batch device buffers, pinned staging and a
+// host thread of its own.  A call deals its sub-batches to the lanes so the
+// copies, kernels and host synchronisations of one sub-batch overlap those
+// of the others.
+struct Lane {
+	cudaStream_t stream = nullptr;
+	cudaEvent_t ev[8]{};
+	DBuf<uint8_t> seq, code, code_r;
+	DBuf<int64_t> off;
+	DBuf<int32_t> len;
+	DBuf<uint2> hits;
+	DBuf<DPair> pairs;
+	DBuf<RmReq> q[2];
+	DBuf<GpReq> qg[2];
+	DBuf<int> counters;
+	DBuf<uint32_t> cnt;
+	DBuf<uint8_t> cub_tmp, scratch;
+	DBuf<int2> calls;
+	DBuf<int> rq_base;
+	DBuf<SswOut> ssw_out;
+	DBuf<TaskInfo> tinfo;
+	DBuf<Chain> chains;
+	DBuf<JobSlot> slots;
+	DBuf<DpJob> jobs;
+	DBuf<uint8_t> res;
+	DBuf<int> perm, hist, tlist;
+	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
+	DBuf<hera_cand_rec> recs;
+	DBuf<uint32_t> pos_pool, op_pool;
+	DBuf<int32_t> p_pool;
+	DBuf<uint8_t> miss_pool;
+	HBuf<uint8_t> h_seq;
+	HBuf<int64_t> h_off;
+	HBuf<int32_t> h_len;
+	HBuf<int> h_small;
+	HBuf<hera_cand_rec> h_recs;
+	HBuf<uint32_t> h_pos, h_ops;
+	HBuf<int32_t> h_p;
+	HBuf<uint8_t> h_miss;
+	hera_gpu_timing timing{};
+	std::string err;
+	// result of the last batch this lane ran (held in its device pools)
+	int32_t items = 0, ncand = 0;
+	uint64_t nl = 0, no = 0, nm = 0;
+
+	void release()
+	{
+		seq.release(); code.release(); code_r.release(); off.release(); len.release();
+		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
+		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release(); scratch.release();
+		calls.release(); rq_base.release(); ssw_out.release(); tinfo.release(); chains.release();
+		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
+		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
+		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
+		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
+		for (auto &e : ev)
+			if (e)
+				cudaEventDestroy(e);
+		if (stream)
+			cudaStreamDestroy(stream);
+	}
+};
+
 struct hera_gpu_ctx {
 	int device = 0;
-	cudaStream_t stream = nullptr;
+	cudaStream_t stream = nullptr;    // the context's default stream
 	DevIndex ix{};
 	uint32_t *d_boff = nullptr;
 	uint4 *d_bk = nullptr;
 	uint2 *d_occ = nullptr;
 	uint8_t *d_seq = nullptr, *d_tcode = nullptr;
 	uint32_t *d_tlen = nullptr, *d_tstart = nullptr;
-	uint32_t max_batch = 1u << 20;
+	uint32_t max_batch = 1u << 18;    // pairs per sub-batch
 	uint64_t scratch_bytes = 2ull << 30;
-
-	// per-batch device buffers
-	DBuf<uint8_t> seq, code;
-	DBuf<int64_t> off;
-	DBuf<int32_t> len;
-	DBuf<uint2> hits;
-	DBuf<DPair> pairs;
-	DBuf<RmReq> q[2];
-	DBuf<int> counters;     // [0] flags, [1..2] queue sizes
-	DBuf<uint32_t> cnt;     // 3 * (items+1) counts, then 3 * (items+1) offsets
-	DBuf<uint8_t> cub_tmp;
-	DBuf<uint8_t> scratch;
-	DBuf<uint8_t> code_r;
-	DBuf<GpReq> qg[2];
-	DBuf<TaskInfo> tinfo;
-	DBuf<Chain> chains;
-	DBuf<DpJob> jobs;
-	DBuf<JobSlot> slots;
-	DBuf<uint8_t> res;
-	DBuf<int> perm, hist;
-	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
 	int batched = 1;
-	DBuf<int2> calls;
-	DBuf<int> rq_base;
-	DBuf<SswOut> ssw_out;
-	DBuf<hera_cand_rec> recs;
-	DBuf<uint32_t> pos_pool, op_pool;
-	DBuf<int32_t> p_pool;
-	DBuf<uint8_t> miss_pool;
-
-	// pinned staging
-	HBuf<uint8_t> h_seq;
-	HBuf<int64_t> h_off;
-	HBuf<int32_t> h_len;
-	HBuf<int> h_small;
-
-	cudaEvent_t ev[8]{};
+	std::vector<Lane *> lanes;
 	hera_gpu_timing timing{};
 	std::string err = "no error";
-
-	// device-resident result of the last hera_gpu_align_pairs_device call
-	int32_t last_items = 0, last_ncand = 0;
-	uint64_t last_l = 0, last_o = 0, last_m = 0;
+	// device-resident results of the last hera_gpu_align_pairs_device call:
+	// sub-batch k is held by lane k
+	int nparts = 0;
 };
 
-static int fail(hera_gpu_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess)
+static int set_err(std::string &dst, int code, const char *what, cudaError_t e = cudaSuccess)
 {
-	if (c) {
-		char buf[512];
-		if (e != cudaSuccess)
-			snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
-		else
-			snprintf(buf, sizeof buf, "%s", what);
-		c->err = buf;
-	}
+	char buf[512];
+	if (e != cudaSuccess)
+		snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+	else
+		snprintf(buf, sizeof buf, "%s", what);
+	dst = buf;
 	return code;
 }
 
-#define CK(call, what)                                                    \
-	do {                                                              \
-		cudaError_t e_ = (call);                                  \
-		if (e_ != cudaSuccess)                                    \
-			return fail(ctx, e_ == cudaErrorMemoryAllocation ? HERA_GPU_ENOMEM : HERA_GPU_ECUDA, what, e_); \
+static int fail(hera_gpu_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess)
+{
+	if (c)
+		set_err(c->err, code, what, e);
+	return code;
+}
+
+// CUDA call inside a lane: record the failure on the lane
+#define LK(call, what)                                                                             \
+	do {                                                                                       \
+		cudaError_t e_ = (call);                                                           \
+		if (e_ != cudaSuccess)                                                             \
+			return set_err(L.err, e_ == cudaErrorMemoryAllocation ? HERA_GPU_ENOMEM : HERA_GPU_ECUDA, \
+				       what, e_);                                                  \
 	} while (0)
 
 static unsigned blocks_for(int64_t n, int tpb = TPB)
@@ -627,8 +665,7 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	if (!ctx)
 		return;
 	cudaSetDevice(ctx->device);
-	if (ctx->stream)
-		cudaStreamSynchronize(ctx->stream);
+	cudaDeviceSynchronize();
 	cudaFree(ctx->d_boff);
 	cudaFree(ctx->d_bk);
 	cudaFree(ctx->d_occ);
@@ -636,18 +673,10 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	cudaFree(ctx->d_tcode);
 	cudaFree(ctx->d_tlen);
 	cudaFree(ctx->d_tstart);
-	ctx->seq.release(); ctx->code.release(); ctx->off.release(); ctx->len.release();
-	ctx->hits.release(); ctx->pairs.release(); ctx->q[0].release(); ctx->q[1].release();
-	ctx->counters.release(); ctx->cnt.release(); ctx->cub_tmp.release(); ctx->scratch.release();
-	ctx->calls.release(); ctx->rq_base.release(); ctx->ssw_out.release();
-	ctx->code_r.release(); ctx->qg[0].release(); ctx->qg[1].release(); ctx->tinfo.release();
-	ctx->chains.release(); ctx->jobs.release(); ctx->slots.release(); ctx->res.release(); ctx->perm.release(); ctx->hist.release();
-	ctx->recs.release(); ctx->pos_pool.release(); ctx->op_pool.release(); ctx->p_pool.release();
-	ctx->miss_pool.release();
-	ctx->h_seq.release(); ctx->h_off.release(); ctx->h_len.release(); ctx->h_small.release();
-	for (auto &e : ctx->ev)
-		if (e)
-			cudaEventDestroy(e);
+	for (Lane *L : ctx->lanes) {
+		L->release();
+		delete L;
+	}
 	if (ctx->stream)
 		cudaStreamDestroy(ctx->stream);
 	delete ctx;
@@ -656,7 +685,6 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_options *opt,
 				   hera_gpu_ctx **out)
 {
-	hera_gpu_ctx *ctx = nullptr;
 	if (!out || !v || !v->len || !v->find || !v->seq || !v->bucket_n || !v->pos || !v->p ||
 	    v->n_trans == 0)
 		return HERA_GPU_EINVAL;
@@ -664,7 +692,8 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
 		return HERA_GPU_ENODEV;
-	ctx = new hera_gpu_ctx();
+	hera_gpu_ctx *ctx = new hera_gpu_ctx();
+	int nlanes = 3;
 	if (opt) {
 		ctx->device = opt->device;
 		if (opt->max_batch)
@@ -672,19 +701,27 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		if (opt->scratch_bytes)
 			ctx->scratch_bytes = opt->scratch_bytes;
 		ctx->batched = opt->path == HERA_GPU_PATH_PLAIN ? 0 : 1;
+		if (opt->lanes > 0)
+			nlanes = opt->lanes;
 	}
+	if (nlanes > 8)
+		nlanes = 8;
 	auto bail = [&](int rc) {
-		std::string e = ctx->err;
 		hera_gpu_ctx_destroy(ctx);
-		(void)e;
 		return rc;
 	};
 	if (cudaSetDevice(ctx->device) != cudaSuccess)
 		return bail(HERA_GPU_ENODEV);
 	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
-	for (auto &e : ctx->ev)
-		cudaEventCreate(&e);
+	for (int i = 0; i < nlanes; ++i) {
+		Lane *L = new Lane();
+		ctx->lanes.push_back(L);
+		if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess)
+			return bail(HERA_GPU_ECUDA);
+		for (auto &e : L->ev)
+			cudaEventCreate(&e);
+	}
 
 	const uint64_t H = 1ull << HBITS;
 	const uint32_t n = v->n_trans;
@@ -725,8 +762,8 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	    (e = cudaMemcpy(ctx->d_tlen, v->len, n * 4ull, cudaMemcpyHostToDevice)) != cudaSuccess ||
 	    (e = cudaMemcpy(ctx->d_tstart, tstart.data(), n * 4ull, cudaMemcpyHostToDevice)) != cudaSuccess)
 		return bail(fail(ctx, HERA_GPU_ECUDA, "index upload", e));
+	// transcript codes; the zero padding after the last transcript codes as 4
 	k_codes<<<1184, 256, 0, ctx->stream>>>(ctx->d_seq, ctx->d_tcode, (int64_t)(seq_len + pad));
-	// padding after the last transcript codes as 4 (k_codes maps 0 -> 4)
 	if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
 		return bail(fail(ctx, HERA_GPU_ECUDA, "index codes", e));
 	ctx->ix.boff = ctx->d_boff;
@@ -744,38 +781,39 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 // ---- pipeline pieces --------------------------------------------------
 
 // one rescue round (re_mapSW for every queued request)
-static int rescue_round(hera_gpu_ctx *ctx, const Batch &b, const RmReq *q, int nq, int max_len,
-			cudaStream_t st, uint32_t &launches, float &ms_acc)
+static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq *q, int nq,
+			int max_len, uint32_t &launches, float &ms_acc)
 {
-	CK(ctx->calls.ensure((size_t)nq * LCAP), "rescue calls");
-	CK(ctx->rq_base.ensure(nq), "rescue bases");
-	int *d_nc = ctx->counters.p + 4;
-	CK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
-	cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+	cudaStream_t st = L.stream;
+	LK(L.calls.ensure((size_t)nq * LCAP), "rescue calls");
+	LK(L.rq_base.ensure(nq), "rescue bases");
+	int *d_nc = L.counters.p + 4;
+	LK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
+	cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
 	cudaEventRecord(e0, st);
-	k_rescue_expand<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, ctx->calls.p, ctx->rq_base.p, d_nc);
+	k_rescue_expand<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.calls.p, L.rq_base.p, d_nc);
 	++launches;
-	CK(cudaMemcpyAsync(ctx->h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
-	CK(cudaStreamSynchronize(st), "rescue expand");
-	const int ncalls = ctx->h_small.p[1];
-	CK(ctx->ssw_out.ensure(ncalls + 1), "rescue outputs");
+	LK(cudaMemcpyAsync(L.h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
+	LK(cudaStreamSynchronize(st), "rescue expand");
+	const int ncalls = L.h_small.p[1];
+	LK(L.ssw_out.ensure(ncalls + 1), "rescue outputs");
 	const size_t per = ssw_scratch_bytes(max_len);
-	size_t slots = ctx->scratch_bytes / per;
+	size_t slots = (ctx->scratch_bytes / ctx->lanes.size()) / per;
 	if (slots < 1)
 		slots = 1;
 	if (slots > (size_t)ncalls)
 		slots = (size_t)(ncalls > 0 ? ncalls : 1);
-	CK(ctx->scratch.ensure(slots * per), "rescue scratch");
+	LK(L.scratch.ensure(slots * per), "rescue scratch");
 	for (int c0 = 0; c0 < ncalls; c0 += (int)slots) {
 		const int m = (int)((size_t)(ncalls - c0) < slots ? (size_t)(ncalls - c0) : slots);
-		k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, q, ctx->calls.p, c0, m, ctx->ssw_out.p,
-									 ctx->scratch.p, per);
+		k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, q, L.calls.p, c0, m, L.ssw_out.p,
+									 L.scratch.p, per);
 		++launches;
 	}
-	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, ctx->rq_base.p, ctx->ssw_out.p);
+	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.rq_base.p, L.ssw_out.p);
 	++launches;
 	cudaEventRecord(e1, st);
-	CK(cudaStreamSynchronize(st), "rescue");
+	LK(cudaStreamSynchronize(st), "rescue");
 	float ms = 0;
 	cudaEventElapsedTime(&ms, e0, e1);
 	ms_acc += ms;
@@ -783,271 +821,278 @@ static int rescue_round(hera_gpu_ctx *ctx, const Batch &b, const RmReq *q, int n
 }
 
 // one round of batched get_position calls: build, bin, DP, replay
-static int gp_round(hera_gpu_ctx *ctx, const Batch &b, Round R, cudaStream_t st, uint32_t &launches,
-		    float &build_ms, float &dp_ms)
+static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float &build_ms, float &dp_ms)
 {
 	if (R.ntask <= 0)
 		return HERA_GPU_OK;
+	cudaStream_t st = L.stream;
 	const int rcap = b.score_only ? 2 : JCAP;
-	CK(ctx->tinfo.ensure(R.ntask), "task info");
-	if (ctx->chain_cap < 2 * (size_t)R.ntask)
-		ctx->chain_cap = 2 * (size_t)R.ntask;
-	if (ctx->job_cap < 3 * (size_t)R.ntask)
-		ctx->job_cap = 3 * (size_t)R.ntask;
-	if (ctx->slot_cap < 4 * (size_t)R.ntask)
-		ctx->slot_cap = 4 * (size_t)R.ntask;
-	int *d_cnt = ctx->counters.p + 12;
-	cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
-	int nch = 0, nj = 0;
+	LK(L.tinfo.ensure(R.ntask), "task info");
+	if (L.chain_cap < 2 * (size_t)R.ntask)
+		L.chain_cap = 2 * (size_t)R.ntask;
+	if (L.job_cap < 3 * (size_t)R.ntask)
+		L.job_cap = 3 * (size_t)R.ntask;
+	if (L.slot_cap < 4 * (size_t)R.ntask)
+		L.slot_cap = 4 * (size_t)R.ntask;
+	int *d_cnt = L.counters.p + 12;
+	cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
+	int nch = 0, nj = 0, ns = 0;
 	cudaEventRecord(e0, st);
+	if (!R.req) {   // round 0: reset the pairs, list the calls with seed hits
+		LK(L.tlist.ensure(R.ntask), "task list");
+		int *d_nl = L.counters.p + 15;
+		LK(cudaMemsetAsync(d_nl, 0, sizeof(int), st), "memset");
+		k_task_list<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R.ntask, R.hits, R.spr, L.tinfo.p, L.tlist.p, d_nl);
+		++launches;
+		R.list = L.tlist.p;
+		R.nlist = d_nl;
+	}
 	for (int attempt = 0; attempt < 2; ++attempt) {
-		CK(ctx->chains.ensure(ctx->chain_cap), "chains");
-		CK(ctx->jobs.ensure(ctx->job_cap), "dp jobs");
-		CK(ctx->slots.ensure(ctx->slot_cap), "job slots");
-		R.tinfo = ctx->tinfo.p;
-		R.chains = ctx->chains.p;
-		R.slots = ctx->slots.p;
-		R.jobs = ctx->jobs.p;
+		LK(L.chains.ensure(L.chain_cap), "chains");
+		LK(L.jobs.ensure(L.job_cap), "dp jobs");
+		LK(L.slots.ensure(L.slot_cap), "job slots");
+		R.tinfo = L.tinfo.p;
+		R.chains = L.chains.p;
+		R.slots = L.slots.p;
+		R.jobs = L.jobs.p;
 		R.cnt = d_cnt;
-		R.chain_cap = (int)ctx->chain_cap;
-		R.job_cap = (int)ctx->job_cap;
-		R.slot_cap = (int)ctx->slot_cap;
-		CK(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(int), st), "memset");
+		R.chain_cap = (int)L.chain_cap;
+		R.job_cap = (int)L.job_cap;
+		R.slot_cap = (int)L.slot_cap;
+		LK(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(int), st), "memset");
 		k_build<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
 		++launches;
-		CK(cudaMemcpyAsync(ctx->h_small.p + 12, d_cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
-		CK(cudaStreamSynchronize(st), "build");
-		nch = ctx->h_small.p[12];
-		nj = ctx->h_small.p[13];
-		const int ns = ctx->h_small.p[14];
-		ctx->timing.dp_calls += (uint64_t)ns;
-		if ((size_t)nch <= ctx->chain_cap && (size_t)nj <= ctx->job_cap && (size_t)ns <= ctx->slot_cap)
+		LK(cudaMemcpyAsync(L.h_small.p + 12, d_cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
+		LK(cudaStreamSynchronize(st), "build");
+		nch = L.h_small.p[12];
+		nj = L.h_small.p[13];
+		ns = L.h_small.p[14];
+		if ((size_t)nch <= L.chain_cap && (size_t)nj <= L.job_cap && (size_t)ns <= L.slot_cap)
 			break;
-		ctx->timing.dp_calls -= (uint64_t)ns;
-		ctx->chain_cap = (size_t)nch + 16;
-		ctx->job_cap = (size_t)nj + 16;
-		ctx->slot_cap = (size_t)ns + 16;
+		L.chain_cap = (size_t)nch + 16;
+		L.job_cap = (size_t)nj + 16;
+		L.slot_cap = (size_t)ns + 16;
 		if (attempt == 1)
-			return fail(ctx, HERA_GPU_ECAPACITY, "dp job buffers");
+			return set_err(L.err, HERA_GPU_ECAPACITY, "dp job buffers");
 	}
+	L.timing.dp_calls += (uint64_t)ns;
 	cudaEventRecord(e1, st);
 	float ms = 0;
-	CK(cudaEventSynchronize(e1), "build");
+	LK(cudaEventSynchronize(e1), "build");
 	cudaEventElapsedTime(&ms, e0, e1);
 	build_ms += ms;
 	cudaEventRecord(e0, st);
 	R.res = nullptr;
 	R.rcap = rcap;
 	if (nj > 0) {
-		CK(ctx->res.ensure((size_t)nj * res_stride(rcap)), "dp results");
-		CK(ctx->perm.ensure(nj), "dp order");
-		CK(ctx->hist.ensure(NBIN), "dp bins");
-		CK(cudaMemsetAsync(ctx->hist.p, 0, NBIN * sizeof(int), st), "memset");
-		k_bin_count<<<blocks_for(nj, 256), 256, 0, st>>>(ctx->jobs.p, nj, ctx->hist.p);
-		k_bin_scan<<<1, 256, 0, st>>>(ctx->hist.p, NBIN);
-		k_bin_scatter<<<blocks_for(nj, 256), 256, 0, st>>>(ctx->jobs.p, nj, ctx->hist.p, ctx->perm.p);
-		k_dp<<<blocks_for(nj), 128, 0, st>>>(b, ctx->jobs.p, ctx->perm.p, nj, ctx->res.p, rcap);
-		launches += 4;
-		R.res = ctx->res.p;
+		LK(L.res.ensure((size_t)nj * res_stride(rcap)), "dp results");
+		LK(L.perm.ensure(nj), "dp order");
+		LK(L.hist.ensure(NBIN), "dp bins");
+		LK(cudaMemsetAsync(L.hist.p, 0, NBIN * sizeof(int), st), "memset");
+		k_bin_count<<<148, 512, 0, st>>>(L.jobs.p, nj, L.hist.p);
+		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
+		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
+		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
+		launches += 6;
+		R.res = L.res.p;
 	}
 	k_replay<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
 	++launches;
 	cudaEventRecord(e1, st);
-	CK(cudaEventSynchronize(e1), "replay");
+	LK(cudaEventSynchronize(e1), "replay");
 	cudaEventElapsedTime(&ms, e0, e1);
 	dp_ms += ms;
-	ctx->timing.dp_jobs += (uint64_t)nj;
+	L.timing.dp_jobs += (uint64_t)nj;
 	return HERA_GPU_OK;
 }
 
-// Run the device pipeline on staged reads (2 * n reads for pairs, n
-// singles otherwise).  Leaves the packed results in the device pools and
-// their sizes in last_*.
-static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_off,
+// Run the device pipeline for one sub-batch on lane L.  Reads: d_seq holds
+// seq_bytes bytes, d_off/d_len are lane-local (offsets into d_seq), 2n
+// reads for pairs (mates interleaved), n for singles.  Leaves the packed
+// records in L's device pools and their sizes in L.items/nl/no/nm.
+static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int64_t *d_off,
 		     const int32_t *d_len, int32_t n, bool paired, int write_bam, int max_len,
-		     int64_t seq_bytes, cudaStream_t st)
+		     int64_t seq_bytes)
 {
+	cudaStream_t st = L.stream;
 	const int n_reads = paired ? 2 * n : n;
 	const int ncand = paired ? 2 : 1;
 	const int items = n * ncand;
 	const bool batched = ctx->batched && paired;
-	hera_gpu_timing &T = ctx->timing;
+	hera_gpu_timing &T = L.timing;
 	uint32_t launches = 0;
 
-	CK(ctx->code.ensure(seq_bytes + 64), "read code buffer");
+	LK(L.code.ensure(seq_bytes + 64), "read code buffer");
 	if (batched)
-		CK(ctx->code_r.ensure(seq_bytes + 64), "read code buffer");
-	CK(ctx->pairs.ensure(n), "pair state");
-	CK(ctx->counters.ensure(16), "counters");
-	CK(ctx->q[0].ensure(n), "rescue queue");
-	CK(ctx->q[1].ensure(n), "rescue queue");
-	CK(ctx->cnt.ensure(6 * (size_t)(items + 1)), "count buffer");
-	CK(ctx->recs.ensure(items), "records");
-	CK(ctx->h_small.ensure(16), "host counters");
-	int *d_flags = ctx->counters.p;
-	CK(cudaMemsetAsync(ctx->counters.p, 0, 16 * sizeof(int), st), "memset");
+		LK(L.code_r.ensure(seq_bytes + 64), "read code buffer");
+	LK(L.pairs.ensure(n), "pair state");
+	LK(L.counters.ensure(16), "counters");
+	LK(L.q[0].ensure(n), "rescue queue");
+	LK(L.q[1].ensure(n), "rescue queue");
+	LK(L.cnt.ensure(6 * (size_t)(items + 1)), "count buffer");
+	LK(L.recs.ensure(items), "records");
+	LK(L.h_small.ensure(16), "host counters");
+	int *d_flags = L.counters.p;
+	LK(cudaMemsetAsync(L.counters.p, 0, 16 * sizeof(int), st), "memset");
 
 	Batch b;
 	b.ix = ctx->ix;
-	b.code = ctx->code.p;
-	b.code_r = batched ? ctx->code_r.p : nullptr;
+	b.code = L.code.p;
+	b.code_r = batched ? L.code_r.p : nullptr;
 	b.off = d_off;
 	b.len = d_len;
-	b.P = ctx->pairs.p;
+	b.P = L.pairs.p;
 	b.flags = d_flags;
 	b.score_only = write_bam == 1;
 	b.max_len = max_len;
 
-	cudaEventRecord(ctx->ev[1], st);
+	cudaEventRecord(L.ev[1], st);
 	if (seq_bytes > 0) {
-		k_codes<<<1184, 256, 0, st>>>(d_seq, ctx->code.p, seq_bytes);
+		k_codes<<<592, 256, 0, st>>>(d_seq, L.code.p, seq_bytes);
 		++launches;
 		if (batched) {
-			k_rc<<<blocks_for((int64_t)n_reads * 32, 256), 256, 0, st>>>(ctx->code.p, d_off, d_len, n_reads,
-										      max_len, ctx->code_r.p);
+			k_rc<<<blocks_for((int64_t)n_reads * 32, 256), 256, 0, st>>>(L.code.p, d_off, d_len, n_reads,
+										      max_len, L.code_r.p);
 			++launches;
 		}
 	}
 	const int spr = max_len >= KMER ? (max_len - KMER) / KMER + 1 : 1;
 	if (paired) {
-		CK(ctx->hits.ensure((size_t)n_reads * 2 * spr), "seed hits");
+		LK(L.hits.ensure((size_t)n_reads * 2 * spr), "seed hits");
 		const int64_t ns = (int64_t)n_reads * 2 * spr;
-		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, ctx->code.p, d_off, d_len, n_reads, spr,
-							     ctx->hits.p);
+		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, L.code.p, d_off, d_len, n_reads, spr, L.hits.p);
 		++launches;
 		T.lookups += (uint64_t)ns;
 	}
-	cudaEventRecord(ctx->ev[2], st);
+	cudaEventRecord(L.ev[2], st);
 	float resolve_ms = 0, rescue_ms = 0, build_ms = 0, dp_ms = 0;
 	uint32_t rounds = 0;
 	if (!paired) {
 		k_single<<<blocks_for(n), TPB, 0, st>>>(b, n);
 		++launches;
-		cudaEventRecord(ctx->ev[3], st);
+		cudaEventRecord(L.ev[3], st);
 	} else if (!batched) {
 		// plain form: one thread per get_position call / pair
-		k_position<<<blocks_for((int64_t)n * 4), TPB, 0, st>>>(b, n, spr, ctx->hits.p);
+		k_position<<<blocks_for((int64_t)n * 4), TPB, 0, st>>>(b, n, spr, L.hits.p);
 		++launches;
-		cudaEventRecord(ctx->ev[3], st);
+		cudaEventRecord(L.ev[3], st);
 		const RmReq *resume = nullptr;
 		int nact = n, qi = 0;
 		while (nact > 0) {
-			int *qn = ctx->counters.p + 1 + qi;
-			CK(cudaMemsetAsync(qn, 0, sizeof(int), st), "memset");
-			cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+			int *qn = L.counters.p + 1 + qi;
+			LK(cudaMemsetAsync(qn, 0, sizeof(int), st), "memset");
+			cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
 			cudaEventRecord(e0, st);
-			k_resolve<<<blocks_for(nact), TPB, 0, st>>>(b, resume, nact, ctx->q[qi].p, qn);
+			k_resolve<<<blocks_for(nact), TPB, 0, st>>>(b, resume, nact, L.q[qi].p, qn);
 			++launches;
 			cudaEventRecord(e1, st);
-			CK(cudaMemcpyAsync(ctx->h_small.p, qn, sizeof(int), cudaMemcpyDeviceToHost, st), "queue size");
-			CK(cudaStreamSynchronize(st), "resolve");
+			LK(cudaMemcpyAsync(L.h_small.p, qn, sizeof(int), cudaMemcpyDeviceToHost, st), "queue size");
+			LK(cudaStreamSynchronize(st), "resolve");
 			float ms = 0;
 			cudaEventElapsedTime(&ms, e0, e1);
 			resolve_ms += ms;
-			const int nq = ctx->h_small.p[0];
+			const int nq = L.h_small.p[0];
 			if (nq == 0)
 				break;
 			++rounds;
-			int rc = rescue_round(ctx, b, ctx->q[qi].p, nq, max_len, st, launches, rescue_ms);
+			int rc = rescue_round(ctx, L, b, L.q[qi].p, nq, max_len, launches, rescue_ms);
 			if (rc)
 				return rc;
-			resume = ctx->q[qi].p;
+			resume = L.q[qi].p;
 			nact = nq;
 			qi ^= 1;
 		}
 	} else {
 		// batched form: rounds of batched get_position calls and rescues
-		CK(ctx->qg[0].ensure(n), "gp queue");
-		CK(ctx->qg[1].ensure(n), "gp queue");
+		LK(L.qg[0].ensure(n), "gp queue");
+		LK(L.qg[1].ensure(n), "gp queue");
 		Round R{};
 		R.req = nullptr;
 		R.ntask = 4 * n;
 		R.space = KMER;
-		R.hits = ctx->hits.p;
+		R.hits = L.hits.p;
 		R.spr = spr;
-		int rc = gp_round(ctx, b, R, st, launches, build_ms, dp_ms);
+		int rc = gp_round(L, b, R, launches, build_ms, dp_ms);
 		if (rc)
 			return rc;
-		cudaEventRecord(ctx->ev[3], st);
+		cudaEventRecord(L.ev[3], st);
 		int ng = n, nr = 0, qi = 0;
 		bool all = true;
 		for (;;) {
-			int *qng = ctx->counters.p + 8 + 2 * qi, *qnr = qng + 1;
-			CK(cudaMemsetAsync(qng, 0, 2 * sizeof(int), st), "memset");
-			cudaEvent_t e0 = ctx->ev[6], e1 = ctx->ev[7];
+			int *qng = L.counters.p + 8 + 2 * qi, *qnr = qng + 1;
+			LK(cudaMemsetAsync(qng, 0, 2 * sizeof(int), st), "memset");
+			cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
 			cudaEventRecord(e0, st);
-			k_resolve_b<<<blocks_for(ng + nr), 128, 0, st>>>(b, ctx->qg[qi ^ 1].p, ng, ctx->q[qi ^ 1].p, nr,
-									  all ? 1 : 0, ctx->qg[qi].p, qng,
-									  ctx->q[qi].p, qnr);
+			k_resolve_b<<<blocks_for(ng + nr), 128, 0, st>>>(b, L.qg[qi ^ 1].p, ng, L.q[qi ^ 1].p, nr,
+									  all ? 1 : 0, L.qg[qi].p, qng, L.q[qi].p, qnr);
 			++launches;
 			cudaEventRecord(e1, st);
-			CK(cudaMemcpyAsync(ctx->h_small.p + 10, qng, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "queues");
-			CK(cudaStreamSynchronize(st), "resolve");
+			LK(cudaMemcpyAsync(L.h_small.p + 10, qng, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "queues");
+			LK(cudaStreamSynchronize(st), "resolve");
 			float ms = 0;
 			cudaEventElapsedTime(&ms, e0, e1);
 			resolve_ms += ms;
 			all = false;
-			ng = ctx->h_small.p[10];
-			nr = ctx->h_small.p[11];
+			ng = L.h_small.p[10];
+			nr = L.h_small.p[11];
 			if (ng + nr == 0)
 				break;
 			++rounds;
 			if (ng) {
 				Round G{};
-				G.req = ctx->qg[qi].p;
+				G.req = L.qg[qi].p;
 				G.ntask = ng;
 				G.space = 2 * ERR;
-				G.hits = nullptr;
-				G.spr = 0;
-				rc = gp_round(ctx, b, G, st, launches, build_ms, dp_ms);
+				rc = gp_round(L, b, G, launches, build_ms, dp_ms);
 				if (rc)
 					return rc;
 			}
 			if (nr) {
-				rc = rescue_round(ctx, b, ctx->q[qi].p, nr, max_len, st, launches, rescue_ms);
+				rc = rescue_round(ctx, L, b, L.q[qi].p, nr, max_len, launches, rescue_ms);
 				if (rc)
 					return rc;
 			}
 			qi ^= 1;
 		}
 	}
-	cudaEventRecord(ctx->ev[4], st);
+	cudaEventRecord(L.ev[4], st);
 	// pack
-	uint32_t *cl = ctx->cnt.p, *co = cl + (items + 1), *cm = co + (items + 1);
+	uint32_t *cl = L.cnt.p, *co = cl + (items + 1), *cm = co + (items + 1);
 	uint32_t *xl = cm + (items + 1), *xo = xl + (items + 1), *xm = xo + (items + 1);
-	CK(cudaMemsetAsync(cl, 0, 3 * sizeof(uint32_t) * (items + 1), st), "memset");
-	k_count<<<blocks_for(items, 256), 256, 0, st>>>(ctx->pairs.p, n, ncand, cl, co, cm);
+	LK(cudaMemsetAsync(cl, 0, 3 * sizeof(uint32_t) * (items + 1), st), "memset");
+	k_count<<<blocks_for(items, 256), 256, 0, st>>>(L.pairs.p, n, ncand, cl, co, cm);
 	++launches;
 	size_t tmp_bytes = 0;
 	cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cl, xl, items + 1, st);
-	CK(ctx->cub_tmp.ensure(tmp_bytes), "scan scratch");
-	cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp_bytes, cl, xl, items + 1, st);
-	cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp_bytes, co, xo, items + 1, st);
-	cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp_bytes, cm, xm, items + 1, st);
-	CK(cudaMemcpyAsync(ctx->h_small.p + 2, xl + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	CK(cudaMemcpyAsync(ctx->h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	CK(cudaMemcpyAsync(ctx->h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	CK(cudaMemcpyAsync(ctx->h_small.p + 5, d_flags, 4, cudaMemcpyDeviceToHost, st), "flags");
-	CK(cudaStreamSynchronize(st), "scan");
-	const uint32_t tl = (uint32_t)ctx->h_small.p[2], to = (uint32_t)ctx->h_small.p[3],
-		       tm = (uint32_t)ctx->h_small.p[4];
-	const int fl = ctx->h_small.p[5];
-	CK(ctx->pos_pool.ensure(tl + 1), "list pool");
-	CK(ctx->p_pool.ensure(tl + 1), "list pool");
-	CK(ctx->op_pool.ensure(to + 1), "op pool");
-	CK(ctx->miss_pool.ensure(tm + 1), "miss pool");
-	k_emit<<<blocks_for(items, 256), 256, 0, st>>>(ctx->pairs.p, n, ncand, xl, xo, xm, ctx->recs.p,
-							ctx->pos_pool.p, ctx->p_pool.p, ctx->op_pool.p,
-							ctx->miss_pool.p, 0, 0, 0);
+	LK(L.cub_tmp.ensure(tmp_bytes), "scan scratch");
+	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cl, xl, items + 1, st);
+	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, co, xo, items + 1, st);
+	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cm, xm, items + 1, st);
+	LK(cudaMemcpyAsync(L.h_small.p + 2, xl + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+	LK(cudaMemcpyAsync(L.h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+	LK(cudaMemcpyAsync(L.h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+	LK(cudaMemcpyAsync(L.h_small.p + 5, d_flags, 4, cudaMemcpyDeviceToHost, st), "flags");
+	LK(cudaStreamSynchronize(st), "scan");
+	const uint32_t tl = (uint32_t)L.h_small.p[2], to = (uint32_t)L.h_small.p[3],
+		       tm = (uint32_t)L.h_small.p[4];
+	const int fl = L.h_small.p[5];
+	LK(L.pos_pool.ensure(tl + 1), "list pool");
+	LK(L.p_pool.ensure(tl + 1), "list pool");
+	LK(L.op_pool.ensure(to + 1), "op pool");
+	LK(L.miss_pool.ensure(tm + 1), "miss pool");
+	k_emit<<<blocks_for(items, 256), 256, 0, st>>>(L.pairs.p, n, ncand, xl, xo, xm, L.recs.p, L.pos_pool.p,
+							L.p_pool.p, L.op_pool.p, L.miss_pool.p, 0, 0, 0);
 	++launches;
-	cudaEventRecord(ctx->ev[5], st);
-	CK(cudaGetLastError(), "kernel launch");
-	CK(cudaStreamSynchronize(st), "pack");
+	cudaEventRecord(L.ev[5], st);
+	LK(cudaGetLastError(), "kernel launch");
+	LK(cudaStreamSynchronize(st), "pack");
 	float ms = 0;
-	cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+	cudaEventElapsedTime(&ms, L.ev[1], L.ev[2]);
 	T.seed_ms += ms;
 	if (!batched) {
-		cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+		cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]);
 		T.position_ms += ms;
 	} else {
 		T.position_ms += build_ms + dp_ms;
@@ -1056,102 +1101,212 @@ static int run_batch(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_o
 	}
 	T.resolve_ms += resolve_ms;
 	T.rescue_ms += rescue_ms;
-	cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+	cudaEventElapsedTime(&ms, L.ev[4], L.ev[5]);
 	T.pack_ms += ms;
 	T.launches += launches;
 	T.rescue_rounds += rounds;
-	ctx->last_items = items;
-	ctx->last_ncand = ncand;
-	ctx->last_l = tl;
-	ctx->last_o = to;
-	ctx->last_m = tm;
+	L.items = items;
+	L.ncand = ncand;
+	L.nl = tl;
+	L.no = to;
+	L.nm = tm;
 	if (fl) {
 		char buf[160];
 		snprintf(buf, sizeof buf, "per-read capacity exceeded (flags 0x%x)", fl);
-		return fail(ctx, HERA_GPU_ECAPACITY, buf);
+		return set_err(L.err, HERA_GPU_ECAPACITY, buf);
 	}
 	return HERA_GPU_OK;
 }
 
-// copy the packed device results into `out` at record `rec0`, shifting
-// pool offsets by what `out` already holds
-static int copy_out(hera_gpu_ctx *ctx, hera_gpu_result *out, uint64_t rec0, cudaStream_t st,
-		    bool *fits)
+// D2H of lane L's packed records into `out` at record rec0 and pool
+// offsets (bl, bo, bm), through the lane's pinned staging
+static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, uint64_t bo, uint64_t bm)
 {
-	const uint64_t bl = out->list_used, bo = out->op_used, bm = out->miss_used;
-	const int items = ctx->last_items;
-	*fits = bl + ctx->last_l <= out->list_cap && bo + ctx->last_o <= out->op_cap &&
-		bm + ctx->last_m <= out->miss_cap;
-	if (*fits) {
-		CK(cudaMemcpyAsync(out->recs + rec0, ctx->recs.p, items * sizeof(hera_cand_rec),
-				   cudaMemcpyDeviceToHost, st), "records D2H");
-		if (ctx->last_l) {
-			CK(cudaMemcpyAsync(out->pos_pool + bl, ctx->pos_pool.p, ctx->last_l * 4, cudaMemcpyDeviceToHost, st), "D2H");
-			CK(cudaMemcpyAsync(out->p_pool + bl, ctx->p_pool.p, ctx->last_l * 4, cudaMemcpyDeviceToHost, st), "D2H");
+	cudaStream_t st = L.stream;
+	const int items = L.items;
+	LK(L.h_recs.ensure(items + 1), "pinned records");
+	LK(L.h_pos.ensure(L.nl + 1), "pinned pools");
+	LK(L.h_p.ensure(L.nl + 1), "pinned pools");
+	LK(L.h_ops.ensure(L.no + 1), "pinned pools");
+	LK(L.h_miss.ensure(L.nm + 1), "pinned pools");
+	cudaEventRecord(L.ev[6], st);
+	LK(cudaMemcpyAsync(L.h_recs.p, L.recs.p, items * sizeof(hera_cand_rec), cudaMemcpyDeviceToHost, st), "D2H");
+	if (L.nl) {
+		LK(cudaMemcpyAsync(L.h_pos.p, L.pos_pool.p, L.nl * 4, cudaMemcpyDeviceToHost, st), "D2H");
+		LK(cudaMemcpyAsync(L.h_p.p, L.p_pool.p, L.nl * 4, cudaMemcpyDeviceToHost, st), "D2H");
+	}
+	if (L.no)
+		LK(cudaMemcpyAsync(L.h_ops.p, L.op_pool.p, L.no * 4, cudaMemcpyDeviceToHost, st), "D2H");
+	if (L.nm)
+		LK(cudaMemcpyAsync(L.h_miss.p, L.miss_pool.p, L.nm, cudaMemcpyDeviceToHost, st), "D2H");
+	cudaEventRecord(L.ev[7], st);
+	LK(cudaStreamSynchronize(st), "D2H");
+	float ms = 0;
+	cudaEventElapsedTime(&ms, L.ev[6], L.ev[7]);
+	L.timing.d2h_ms += ms;
+	hera_cand_rec *dst = out->recs + rec0;
+	for (int i = 0; i < items; ++i) {
+		hera_cand_rec r = L.h_recs.p[i];
+		for (int s = 0; s < 2; ++s) {
+			r.list_off[s] += (uint32_t)bl;
+			r.cig_off[s] += (uint32_t)bo;
+			r.miss_off[s] += (uint32_t)bm;
 		}
-		if (ctx->last_o)
-			CK(cudaMemcpyAsync(out->op_pool + bo, ctx->op_pool.p, ctx->last_o * 4, cudaMemcpyDeviceToHost, st), "D2H");
-		if (ctx->last_m)
-			CK(cudaMemcpyAsync(out->miss_pool + bm, ctx->miss_pool.p, ctx->last_m, cudaMemcpyDeviceToHost, st), "D2H");
-		CK(cudaStreamSynchronize(st), "D2H");
-		if (bl | bo | bm) {
-			for (int i = 0; i < items; ++i) {
-				hera_cand_rec &r = out->recs[rec0 + i];
-				for (int s = 0; s < 2; ++s) {
-					r.list_off[s] += (uint32_t)bl;
-					r.cig_off[s] += (uint32_t)bo;
-					r.miss_off[s] += (uint32_t)bm;
-				}
+		dst[i] = r;
+	}
+	if (L.nl) {
+		memcpy(out->pos_pool + bl, L.h_pos.p, L.nl * 4);
+		memcpy(out->p_pool + bl, L.h_p.p, L.nl * 4);
+	}
+	if (L.no)
+		memcpy(out->op_pool + bo, L.h_ops.p, L.no * 4);
+	if (L.nm)
+		memcpy(out->miss_pool + bm, L.h_miss.p, L.nm);
+	return HERA_GPU_OK;
+}
+
+// stage host reads of [lo, lo+n) into lane L's pinned memory and device
+// buffers; mates interleaved in the offset table, sequences as blocks
+static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b, int32_t lo, int32_t n,
+		       int64_t *bytes, int *max_len)
+{
+	cudaStream_t st = L.stream;
+	const int per = b ? 2 : 1;
+	const hera_gpu_reads *src[2] = {a, b};
+	int64_t total = 0;
+	int ml = 0;
+	bool contig[2] = {true, true};
+	for (int m = 0; m < per; ++m) {
+		const hera_gpu_reads *r = src[m];
+		for (int32_t i = lo; i < lo + n; ++i) {
+			if (r->len[i] < 0)
+				return set_err(L.err, HERA_GPU_EINVAL, "negative read length");
+			total += r->len[i];
+			ml = r->len[i] > ml ? r->len[i] : ml;
+			if (i > lo && r->off[i] != r->off[i - 1] + r->len[i - 1])
+				contig[m] = false;
+		}
+	}
+	if (ml > MAX_READ)
+		return set_err(L.err, HERA_GPU_EINVAL, "read longer than HERA_GPU_MAX_READ");
+	LK(L.h_seq.ensure(total + 1), "pinned reads");
+	LK(L.h_off.ensure((size_t)n * per), "pinned offsets");
+	LK(L.h_len.ensure((size_t)n * per), "pinned lengths");
+	int64_t o = 0;
+	for (int m = 0; m < per; ++m) {
+		const hera_gpu_reads *r = src[m];
+		if (contig[m] && n > 0) {
+			const int64_t len_m = r->off[lo + n - 1] + r->len[lo + n - 1] - r->off[lo];
+			memcpy(L.h_seq.p + o, r->seq + r->off[lo], (size_t)len_m);
+			const int64_t shift = o - r->off[lo];
+			for (int32_t i = 0; i < n; ++i) {
+				L.h_off.p[(size_t)i * per + m] = r->off[lo + i] + shift;
+				L.h_len.p[(size_t)i * per + m] = r->len[lo + i];
+			}
+			o += len_m;
+		} else {
+			for (int32_t i = 0; i < n; ++i) {
+				const int32_t Ln = r->len[lo + i];
+				memcpy(L.h_seq.p + o, r->seq + r->off[lo + i], (size_t)Ln);
+				L.h_off.p[(size_t)i * per + m] = o;
+				L.h_len.p[(size_t)i * per + m] = Ln;
+				o += Ln;
 			}
 		}
 	}
-	out->list_used = bl + ctx->last_l;
-	out->op_used = bo + ctx->last_o;
-	out->miss_used = bm + ctx->last_m;
-	return HERA_GPU_OK;
-}
-
-// stage host reads (pairs interleaved) into pinned memory and the device
-static int stage_reads(hera_gpu_ctx *ctx, const hera_gpu_reads *a, const hera_gpu_reads *b,
-		       int32_t lo, int32_t n, int64_t *bytes, int *max_len, cudaStream_t st)
-{
-	const int per = b ? 2 : 1;
-	int64_t total = 0;
-	int ml = 0;
-	for (int32_t i = lo; i < lo + n; ++i) {
-		if (a->len[i] < 0 || (b && b->len[i] < 0))
-			return fail(ctx, HERA_GPU_EINVAL, "negative read length");
-		total += a->len[i] + (b ? b->len[i] : 0);
-		ml = a->len[i] > ml ? a->len[i] : ml;
-		if (b)
-			ml = b->len[i] > ml ? b->len[i] : ml;
-	}
-	if (ml > MAX_READ)
-		return fail(ctx, HERA_GPU_EINVAL, "read longer than HERA_GPU_MAX_READ");
-	CK(ctx->h_seq.ensure(total + 1), "pinned reads");
-	CK(ctx->h_off.ensure((size_t)n * per), "pinned offsets");
-	CK(ctx->h_len.ensure((size_t)n * per), "pinned lengths");
-	int64_t o = 0;
-	for (int32_t i = 0; i < n; ++i) {
-		const hera_gpu_reads *src[2] = {a, b};
-		for (int m = 0; m < per; ++m) {
-			const hera_gpu_reads *r = src[m];
-			const int32_t L = r->len[lo + i];
-			memcpy(ctx->h_seq.p + o, r->seq + r->off[lo + i], (size_t)L);
-			ctx->h_off.p[(size_t)i * per + m] = o;
-			ctx->h_len.p[(size_t)i * per + m] = L;
-			o += L;
-		}
-	}
-	CK(ctx->seq.ensure(total + 64), "device reads");
-	CK(ctx->off.ensure((size_t)n * per), "device offsets");
-	CK(ctx->len.ensure((size_t)n * per), "device lengths");
-	CK(cudaMemcpyAsync(ctx->seq.p, ctx->h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
-	CK(cudaMemcpyAsync(ctx->off.p, ctx->h_off.p, (size_t)n * per * 8, cudaMemcpyHostToDevice, st), "H2D");
-	CK(cudaMemcpyAsync(ctx->len.p, ctx->h_len.p, (size_t)n * per * 4, cudaMemcpyHostToDevice, st), "H2D");
+	LK(L.seq.ensure(total + 64), "device reads");
+	LK(L.off.ensure((size_t)n * per), "device offsets");
+	LK(L.len.ensure((size_t)n * per), "device lengths");
+	cudaEventRecord(L.ev[0], st);
+	LK(cudaMemcpyAsync(L.seq.p, L.h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
+	LK(cudaMemcpyAsync(L.off.p, L.h_off.p, (size_t)n * per * 8, cudaMemcpyHostToDevice, st), "H2D");
+	LK(cudaMemcpyAsync(L.len.p, L.h_len.p, (size_t)n * per * 4, cudaMemcpyHostToDevice, st), "H2D");
+	cudaEventRecord(L.ev[1], st);
+	LK(cudaEventSynchronize(L.ev[1]), "H2D");
+	float ms = 0;
+	cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]);
+	L.timing.h2d_ms += ms;
 	*bytes = total;
 	*max_len = ml;
 	return HERA_GPU_OK;
+}
+
+// ---- sub-batch scheduling over the lanes --------------------------------
+
+struct Sched {
+	std::mutex mu;
+	std::condition_variable cv;
+	std::vector<int> ready;             // sub-batch k's sizes are known
+	std::vector<uint64_t> nl, no, nm;
+	bool abort = false;
+	int rc = HERA_GPU_OK;
+	std::string err;
+	void publish(int k, uint64_t l, uint64_t o, uint64_t m)
+	{
+		std::lock_guard<std::mutex> g(mu);
+		nl[k] = l;
+		no[k] = o;
+		nm[k] = m;
+		ready[k] = 1;
+		cv.notify_all();
+	}
+	void failed(int k, int code, const std::string &e)
+	{
+		std::lock_guard<std::mutex> g(mu);
+		if (!abort) {
+			abort = true;
+			rc = code;
+			err = e;
+		}
+		ready[k] = 1;
+		cv.notify_all();
+	}
+	// wait for the sizes of every sub-batch before k; false on abort
+	bool prefix(int k, uint64_t &bl, uint64_t &bo, uint64_t &bm)
+	{
+		std::unique_lock<std::mutex> g(mu);
+		cv.wait(g, [&] {
+			if (abort)
+				return true;
+			for (int q = 0; q < k; ++q)
+				if (!ready[q])
+					return false;
+			return true;
+		});
+		if (abort)
+			return false;
+		bl = bo = bm = 0;
+		for (int q = 0; q < k; ++q) {
+			bl += nl[q];
+			bo += no[q];
+			bm += nm[q];
+		}
+		return true;
+	}
+};
+
+static void sum_timing(hera_gpu_ctx *ctx)
+{
+	hera_gpu_timing t{};
+	for (Lane *L : ctx->lanes) {
+		const hera_gpu_timing &a = L->timing;
+		t.h2d_ms += a.h2d_ms;
+		t.seed_ms += a.seed_ms;
+		t.position_ms += a.position_ms;
+		t.resolve_ms += a.resolve_ms;
+		t.rescue_ms += a.rescue_ms;
+		t.pack_ms += a.pack_ms;
+		t.d2h_ms += a.d2h_ms;
+		t.build_ms += a.build_ms;
+		t.dp_ms += a.dp_ms;
+		t.launches += a.launches;
+		t.rescue_rounds += a.rescue_rounds;
+		t.lookups += a.lookups;
+		t.dp_jobs += a.dp_jobs;
+		t.dp_calls += a.dp_calls;
+	}
+	t.total_ms = ctx->timing.total_ms;
+	ctx->timing = t;
 }
 
 static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gpu_reads *r2, int32_t n,
@@ -1161,39 +1316,70 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
 	if (cudaSetDevice(ctx->device) != cudaSuccess)
 		return fail(ctx, HERA_GPU_ENODEV, "cudaSetDevice");
-	cudaStream_t st = ctx->stream;
+	const auto t0 = std::chrono::steady_clock::now();
 	const bool paired = r2 != nullptr;
 	const int ncand = paired ? 2 : 1;
-	memset(&ctx->timing, 0, sizeof(ctx->timing));
-	out->list_used = out->op_used = out->miss_used = 0;
-	bool all_fit = true;
-	cudaEventRecord(ctx->ev[0], st);
-	for (int32_t lo = 0; lo < n; lo += (int32_t)ctx->max_batch) {
-		const int32_t m = (n - lo) < (int32_t)ctx->max_batch ? (n - lo) : (int32_t)ctx->max_batch;
-		int64_t bytes = 0;
-		int max_len = 0;
-		int rc = stage_reads(ctx, r1, r2, lo, m, &bytes, &max_len, st);
-		if (rc)
-			return rc;
-		rc = run_batch(ctx, ctx->seq.p, ctx->off.p, ctx->len.p, m, paired, write_bam, max_len, bytes, st);
-		if (rc)
-			return rc;
-		bool fits = true;
-		if (all_fit) {
-			rc = copy_out(ctx, out, (uint64_t)lo * ncand, st, &fits);
-			if (rc)
-				return rc;
-			all_fit = fits;
-		} else {
-			out->list_used += ctx->last_l;
-			out->op_used += ctx->last_o;
-			out->miss_used += ctx->last_m;
+	for (Lane *L : ctx->lanes)
+		L->timing = hera_gpu_timing{};
+	const int32_t sub = (int32_t)ctx->max_batch;
+	const int nsub = (int)((n + (int64_t)sub - 1) / sub);
+	Sched S;
+	S.ready.assign(nsub, 0);
+	S.nl.assign(nsub, 0);
+	S.no.assign(nsub, 0);
+	S.nm.assign(nsub, 0);
+	const int nl = (int)ctx->lanes.size() < nsub ? (int)ctx->lanes.size() : nsub;
+	const int dev = ctx->device;
+	auto worker = [&](int li) {
+		cudaSetDevice(dev);
+		Lane &L = *ctx->lanes[li];
+		for (int k = li; k < nsub; k += nl) {
+			const int32_t lo = (int32_t)((int64_t)k * sub);
+			const int32_t m = (n - lo) < sub ? (n - lo) : sub;
+			int64_t bytes = 0;
+			int max_len = 0;
+			int rc = stage_reads(L, r1, r2, lo, m, &bytes, &max_len);
+			if (!rc)
+				rc = run_batch(ctx, L, L.seq.p, L.off.p, L.len.p, m, paired, write_bam, max_len, bytes);
+			if (rc) {
+				S.failed(k, rc, L.err);
+				return;
+			}
+			S.publish(k, L.nl, L.no, L.nm);
+			uint64_t bl, bo, bm;
+			if (!S.prefix(k, bl, bo, bm))
+				return;
+			if (bl + L.nl <= out->list_cap && bo + L.no <= out->op_cap && bm + L.nm <= out->miss_cap) {
+				rc = copy_out(L, out, (uint64_t)lo * ncand, bl, bo, bm);
+				if (rc) {
+					S.failed(k, rc, L.err);
+					return;
+				}
+			}
 		}
+	};
+	std::vector<std::thread> th;
+	for (int i = 1; i < nl; ++i)
+		th.emplace_back(worker, i);
+	if (nl > 0)
+		worker(0);
+	for (auto &t : th)
+		t.join();
+	ctx->timing.total_ms =
+		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+	sum_timing(ctx);
+	if (S.abort)
+		return fail(ctx, S.rc, S.err.c_str());
+	uint64_t tl = 0, to = 0, tm = 0;
+	for (int k = 0; k < nsub; ++k) {
+		tl += S.nl[k];
+		to += S.no[k];
+		tm += S.nm[k];
 	}
-	cudaEventRecord(ctx->ev[1], st);
-	cudaEventSynchronize(ctx->ev[1]);
-	cudaEventElapsedTime(&ctx->timing.total_ms, ctx->ev[0], ctx->ev[1]);
-	if (!all_fit)
+	out->list_used = tl;
+	out->op_used = to;
+	out->miss_used = tm;
+	if (tl > out->list_cap || to > out->op_cap || tm > out->miss_cap)
 		return fail(ctx, HERA_GPU_ECAPACITY, "result pools too small (see *_used for the sizes needed)");
 	return HERA_GPU_OK;
 }
@@ -1213,6 +1399,14 @@ extern "C" int hera_gpu_align_single_flat(hera_gpu_ctx *ctx, const hera_gpu_read
 	return align_flat(ctx, reads, nullptr, n, write_bam, out);
 }
 
+// lane-local offsets of a device-resident sub-batch
+__global__ void k_rebase(const int64_t *__restrict__ in, int64_t n, int64_t base, int64_t *__restrict__ out)
+{
+	const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (t < n)
+		out[t] = in[t] - base;
+}
+
 extern "C" int hera_gpu_align_pairs_device(hera_gpu_ctx *ctx, const uint8_t *d_seq, const int64_t *d_off,
 					   const int32_t *d_len, int32_t n, int32_t max_read_len, int write_bam,
 					   void *stream)
@@ -1222,33 +1416,101 @@ extern "C" int hera_gpu_align_pairs_device(hera_gpu_ctx *ctx, const uint8_t *d_s
 		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
 	if (cudaSetDevice(ctx->device) != cudaSuccess)
 		return fail(ctx, HERA_GPU_ENODEV, "cudaSetDevice");
-	cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-	memset(&ctx->timing, 0, sizeof(ctx->timing));
-	// total bytes and max read length of the device batch
+	const auto t0 = std::chrono::steady_clock::now();
+	cudaStream_t caller = stream ? (cudaStream_t)stream : ctx->stream;
+	for (Lane *L : ctx->lanes)
+		L->timing = hera_gpu_timing{};
+	ctx->nparts = 0;
 	if (n == 0)
 		return HERA_GPU_OK;
-	int64_t last_off = 0;
-	int32_t last_len = 0;
-	CK(cudaMemcpyAsync(&last_off, d_off + 2 * (int64_t)n - 1, 8, cudaMemcpyDeviceToHost, st), "D2H");
-	CK(cudaMemcpyAsync(&last_len, d_len + 2 * (int64_t)n - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
-	CK(cudaStreamSynchronize(st), "sync");
-	cudaEventRecord(ctx->ev[0], st);
-	int rc = run_batch(ctx, d_seq, d_off, d_len, n, true, write_bam, max_read_len, last_off + last_len, st);
-	cudaEventRecord(ctx->ev[1], st);
-	cudaEventSynchronize(ctx->ev[1]);
-	cudaEventElapsedTime(&ctx->timing.total_ms, ctx->ev[0], ctx->ev[1]);
-	return rc;
+	// one contiguous sub-batch per lane (results stay in the lane's pools)
+	const int nl = (int)ctx->lanes.size();
+	int parts = nl;
+	while (parts > 1 && n / parts < 4096)
+		--parts;
+	std::vector<int32_t> lo(parts + 1);
+	for (int k = 0; k <= parts; ++k)
+		lo[k] = (int32_t)((int64_t)n * k / parts);
+	// the sub-batches' byte ranges: [off of first read, end of last read)
+	std::vector<int64_t> first(parts), last(parts);
+	std::vector<int32_t> last_len(parts);
+	cudaEvent_t start_ev;
+	cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming);
+	cudaEventRecord(start_ev, caller);
+	for (int k = 0; k < parts; ++k) {
+		cudaMemcpyAsync(&first[k], d_off + 2 * (int64_t)lo[k], 8, cudaMemcpyDeviceToHost, caller);
+		cudaMemcpyAsync(&last[k], d_off + 2 * (int64_t)lo[k + 1] - 1, 8, cudaMemcpyDeviceToHost, caller);
+		cudaMemcpyAsync(&last_len[k], d_len + 2 * (int64_t)lo[k + 1] - 1, 4, cudaMemcpyDeviceToHost, caller);
+	}
+	if (cudaStreamSynchronize(caller) != cudaSuccess) {
+		cudaEventDestroy(start_ev);
+		return fail(ctx, HERA_GPU_ECUDA, "offsets");
+	}
+	std::vector<int> rcs(parts, HERA_GPU_OK);
+	const int dev = ctx->device;
+	auto worker = [&](int k) {
+		cudaSetDevice(dev);
+		Lane &L = *ctx->lanes[k];
+		cudaStreamWaitEvent(L.stream, start_ev, 0);
+		const int32_t m = lo[k + 1] - lo[k];
+		const int64_t base = first[k];
+		const int64_t bytes = last[k] + last_len[k] - base;
+		int rc = HERA_GPU_OK;
+		if (L.off.ensure((size_t)2 * m) != cudaSuccess || L.len.ensure(1) != cudaSuccess) {
+			rcs[k] = set_err(L.err, HERA_GPU_ENOMEM, "offsets");
+			return;
+		}
+		k_rebase<<<blocks_for(2 * (int64_t)m, 256), 256, 0, L.stream>>>(d_off + 2 * (int64_t)lo[k], 2 * (int64_t)m,
+										 base, L.off.p);
+		rc = run_batch(ctx, L, d_seq + base, L.off.p, d_len + 2 * (int64_t)lo[k], m, true, write_bam,
+			       max_read_len, bytes);
+		rcs[k] = rc;
+	};
+	std::vector<std::thread> th;
+	for (int k = 1; k < parts; ++k)
+		th.emplace_back(worker, k);
+	worker(0);
+	for (auto &t : th)
+		t.join();
+	cudaEventDestroy(start_ev);
+	ctx->timing.total_ms =
+		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+	sum_timing(ctx);
+	for (int k = 0; k < parts; ++k)
+		if (rcs[k] != HERA_GPU_OK)
+			return fail(ctx, rcs[k], ctx->lanes[k]->err.c_str());
+	// order later work on the caller's stream after the lanes
+	for (int k = 0; k < parts; ++k) {
+		cudaEventRecord(ctx->lanes[k]->ev[5], ctx->lanes[k]->stream);
+		cudaStreamWaitEvent(caller, ctx->lanes[k]->ev[5], 0);
+	}
+	ctx->nparts = parts;
+	return HERA_GPU_OK;
 }
 
 extern "C" int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out)
 {
 	if (!ctx || !out)
 		return HERA_GPU_EINVAL;
-	out->list_used = out->op_used = out->miss_used = 0;
+	uint64_t bl = 0, bo = 0, bm = 0, rec = 0;
 	bool fits = true;
-	int rc = copy_out(ctx, out, 0, ctx->stream, &fits);
-	if (rc)
-		return rc;
+	for (int k = 0; k < ctx->nparts; ++k) {
+		Lane &L = *ctx->lanes[k];
+		if (fits && bl + L.nl <= out->list_cap && bo + L.no <= out->op_cap && bm + L.nm <= out->miss_cap) {
+			int rc = copy_out(L, out, rec, bl, bo, bm);
+			if (rc)
+				return fail(ctx, rc, L.err.c_str());
+		} else {
+			fits = false;
+		}
+		rec += (uint64_t)L.items;
+		bl += L.nl;
+		bo += L.no;
+		bm += L.nm;
+	}
+	out->list_used = bl;
+	out->op_used = bo;
+	out->miss_used = bm;
 	return fits ? HERA_GPU_OK : fail(ctx, HERA_GPU_ECAPACITY, "result pools too small");
 }
 

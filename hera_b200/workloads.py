@@ -8,6 +8,8 @@ config1  small transcriptome: 2 Mbp genome (GC 0.41), 200 genes of 2-8
 config2  transcriptome scale: 400 Mbp genome in 8 chromosomes, 60k genes,
          200k transcripts (~300 Mbp transcriptome, ~1.5 kb mean); 2x100 bp
          pairs, 0.5% substitutions, 0.02% indels; 1M-pair chunks.
+config2s config 2's gene and read model on a 40 Mbp genome (6k genes,
+         20k transcripts): the profiling case.
 config3  config1 index; mixed 50/75/100/150 bp reads (1:1:2:1), half paired
          and half single-end, per-read substitution rate U(0.1%, 2%),
          0.05% indels.
@@ -31,12 +33,17 @@ ANNOTATIONS = {
     "config2": dict(seed=2, genome_len=400_000_000, n_genes=60_000, n_transcripts=200_000,
                     n_chrom=8, exons=(2, 16), exon_median=180.0, intron=(200, 3000)),
 }
+# config 2's gene and read model on a tenth of the genome (profiling case:
+# same isoform structure, ~1 GB of index on the device)
+ANNOTATIONS["config2s"] = dict(seed=2, genome_len=40_000_000, n_genes=6_000, n_transcripts=20_000,
+                               n_chrom=2, exons=(2, 16), exon_median=180.0, intron=(200, 3000))
 ANNOTATIONS["config3"] = ANNOTATIONS["config1"]
 ANNOTATIONS["config4"] = ANNOTATIONS["config1"]
 
 DESCRIPTION = {
     "config1": "2 Mbp genome, 200 genes, 500 isoforms; 2x100 bp, 0.5% subs, 0.01% indels",
     "config2": "400 Mbp genome, 60k genes, 200k transcripts; 2x100 bp, 0.5% subs, 0.02% indels",
+    "config2s": "40 Mbp genome, 6k genes, 20k transcripts; config-2 read model",
     "config3": "config1 index; 50/75/100/150 bp mixed, U(0.1-2%) subs, 0.05% indels",
     "config4": "config1 index; 2x150 bp, 3% subs, 0.5% 1-8 bp indels, 5% mutated loci",
 }
@@ -59,7 +66,7 @@ def pairs(name: str, ann, tx, n: int, seed: int):
     if name == "config1":
         return synth.simulate_pairs(tx, n, seed, read_len=100, sub_rate=0.005,
                                     indel_rate=0.0001, indel_len=(1, 3))
-    if name == "config2":
+    if name in ("config2", "config2s"):
         return synth.simulate_pairs(tx, n, seed, read_len=100, sub_rate=0.005,
                                     indel_rate=0.0002, indel_len=(1, 3))
     if name == "config3":

@@ -144,12 +144,14 @@ typedef struct hera_gpu_ctx hera_gpu_ctx;
 
 typedef struct hera_gpu_options {
 	int device;              /* CUDA device ordinal */
-	uint32_t max_batch;      /* pairs (or single reads) per device pass; 0 = 1<<20 */
+	uint32_t max_batch;      /* pairs (or single reads) per sub-batch; 0 = 1<<18 */
 	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 2 GiB */
 	int path;                /* HERA_GPU_PATH_BATCHED (default) or _PLAIN */
+	int lanes;               /* concurrent sub-batches (stream + host thread each); 0 = 3 */
 } hera_gpu_options;
 
-/* Per-stage device time of the last call, milliseconds (CUDA events). */
+/* Per-stage device time of the last call, milliseconds (CUDA events,
+ * summed over the lanes that ran concurrently); total_ms is wall time. */
 typedef struct hera_gpu_timing {
 	float h2d_ms, seed_ms, position_ms, resolve_ms, rescue_ms, pack_ms, d2h_ms, total_ms;
 	float build_ms, dp_ms;   /* batched form: build and DP+replay parts of position_ms */
@@ -221,8 +223,9 @@ int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out);
 /* Per-stage timing of the last call on `ctx`. */
 int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out);
 
-/* The context's CUDA stream (a cudaStream_t), for callers that time or
- * order work around the library's launches. */
+/* The context's CUDA stream (a cudaStream_t): the default caller stream of
+ * hera_gpu_align_pairs_device, for callers that time or order work around
+ * the library's launches.  Calls on one context must not overlap. */
 void *hera_gpu_stream(hera_gpu_ctx *ctx);
 
 #ifdef __cplusplus
