@@ -64,7 +64,7 @@ struct DpResHdr {
 	uint8_t n, nm, pad[2];
 };
 
-__host__ __device__ inline int res_stride(int cap)
+__host__ __device__ constexpr int res_stride(int cap)
 {
 	return (int)sizeof(DpResHdr) + 4 * cap + ((cap + 3) & ~3);
 }

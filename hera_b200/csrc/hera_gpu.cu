@@ -472,10 +472,19 @@ template <typename T>
 struct DBuf {   // growable device buffer
 	T *p = nullptr;
 	size_t cap = 0;
+	bool fixed = false;   // bound to memory the buffer does not own: never grows
+	void bind(void *ptr, size_t n)
+	{
+		p = static_cast<T *>(ptr);
+		cap = n;
+		fixed = true;
+	}
 	cudaError_t ensure(size_t n)
 	{
 		if (n <= cap)
 			return cudaSuccess;
+		if (fixed)
+			return cudaErrorMemoryAllocation;
 		if (p)
 			cudaFree(p);
 		p = nullptr;
@@ -488,10 +497,11 @@ struct DBuf {   // growable device buffer
 	}
 	void release()
 	{
-		if (p)
+		if (p && !fixed)
 			cudaFree(p);
 		p = nullptr;
 		cap = 0;
+		fixed = false;
 	}
 };
 
@@ -598,6 +608,7 @@ struct hera_gpu_ctx {
 	uint64_t scratch_bytes = 2ull << 30;
 	int batched = 1;
 	std::vector<Lane *> lanes;
+	Lane *na = nullptr;               // lane of hera_gpu_align_pairs_device_noalloc
 	hera_gpu_timing timing{};
 	std::string err = "no error";
 	// device-resident results of the last hera_gpu_align_pairs_device call:
@@ -677,6 +688,10 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 		L->release();
 		delete L;
 	}
+	if (ctx->na) {
+		ctx->na->release();
+		delete ctx->na;
+	}
 	if (ctx->stream)
 		cudaStreamDestroy(ctx->stream);
 	delete ctx;
@@ -722,6 +737,14 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		for (auto &e : L->ev)
 			cudaEventCreate(&e);
 	}
+	// the allocation-free entry's lane: its stream, events and 16 pinned
+	// counters are made here, so that entry point itself allocates nothing
+	ctx->na = new Lane();
+	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	    ctx->na->h_small.ensure(16) != cudaSuccess)
+		return bail(HERA_GPU_ECUDA);
+	for (auto &e : ctx->na->ev)
+		cudaEventCreate(&e);
 
 	const uint64_t H = 1ull << HBITS;
 	const uint32_t n = v->n_trans;
@@ -798,7 +821,7 @@ static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const 
 	const int ncalls = L.h_small.p[1];
 	LK(L.ssw_out.ensure(ncalls + 1), "rescue outputs");
 	const size_t per = ssw_scratch_bytes(max_len);
-	size_t slots = (ctx->scratch_bytes / ctx->lanes.size()) / per;
+	size_t slots = (L.scratch.fixed ? L.scratch.cap : ctx->scratch_bytes / ctx->lanes.size()) / per;
 	if (slots < 1)
 		slots = 1;
 	if (slots > (size_t)ncalls)
@@ -1078,6 +1101,10 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	const uint32_t tl = (uint32_t)L.h_small.p[2], to = (uint32_t)L.h_small.p[3],
 		       tm = (uint32_t)L.h_small.p[4];
 	const int fl = L.h_small.p[5];
+	L.items = items;
+	L.nl = tl;
+	L.no = to;
+	L.nm = tm;
 	LK(L.pos_pool.ensure(tl + 1), "list pool");
 	LK(L.p_pool.ensure(tl + 1), "list pool");
 	LK(L.op_pool.ensure(to + 1), "op pool");
@@ -1512,6 +1539,162 @@ extern "C" int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out)
 	out->op_used = bo;
 	out->miss_used = bm;
 	return fits ? HERA_GPU_OK : fail(ctx, HERA_GPU_ECAPACITY, "result pools too small");
+}
+
+// ---- allocation-free variant of the device-resident entry ---------------
+//
+// For callers that cannot allocate device memory while they align (see
+// include/hera_gpu.h).  Every per-batch buffer -- the mate-rescue DP's H
+// matrix scratch, the DP jobs and results, the per-pair Candidate state, the
+// queues -- is carved from one file-scope device array; records go straight
+// into the caller's device buffers.  Sized for HERA_GPU_NOALLOC_MAX_PAIRS
+// pairs of reads up to HERA_GPU_MAX_READ.
+
+namespace na {
+constexpr size_t A(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t PAIRS = HERA_GPU_NOALLOC_MAX_PAIRS;
+constexpr size_t READS = 2 * PAIRS;
+constexpr size_t TASKS = 4 * PAIRS;
+constexpr size_t ITEMS = 2 * PAIRS;
+constexpr size_t SPR = (MAX_READ - KMER) / KMER + 1;
+constexpr size_t SEQ = READS * MAX_READ + 64;
+constexpr size_t CHAINS = 32 * PAIRS;
+constexpr size_t JOBS = 32 * PAIRS;
+constexpr size_t SLOTS = 64 * PAIRS;
+constexpr size_t CALLS = 8 * PAIRS;
+constexpr size_t CUB = 64 << 10;
+constexpr size_t H = 16 << 20;     // mate-rescue DP scratch
+constexpr size_t BYTES =
+	2 * A(SEQ) + A(READS * 8) + A(READS * 2 * SPR * sizeof(uint2)) + A(PAIRS * sizeof(DPair)) +
+	2 * A(PAIRS * sizeof(RmReq)) + 2 * A(PAIRS * sizeof(GpReq)) + A(16 * sizeof(int)) +
+	A(6 * (ITEMS + 1) * sizeof(uint32_t)) + A(CUB) + A(TASKS * sizeof(TaskInfo)) + A(TASKS * sizeof(int)) +
+	A(CHAINS * sizeof(Chain)) + A(JOBS * sizeof(DpJob)) + A(SLOTS * sizeof(JobSlot)) +
+	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
+	A(PAIRS * LCAP * sizeof(int2)) + A(PAIRS * sizeof(int)) + A(CALLS * sizeof(SswOut)) + A(H);
+}  // namespace na
+
+// the scratch: every GPU that loads this library holds it until exit
+static __device__ __align__(256) uint8_t g_noalloc_scratch[na::BYTES];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64];   // device address of the scratch, per device
+
+// once per device, with that device current: the scratch's device address
+// (the host-side symbol is only a stand-in and must never reach a kernel)
+static int noalloc_scratch(int dev, uint8_t **out)
+{
+	std::lock_guard<std::mutex> g(g_noalloc_mu);
+	if (dev < 0 || dev >= 64)
+		return HERA_GPU_EINVAL;
+	if (!g_noalloc_ptr[dev]) {
+		void *p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return HERA_GPU_ECUDA;
+		g_noalloc_ptr[dev] = p;
+	}
+	*out = static_cast<uint8_t *>(g_noalloc_ptr[dev]);
+	return HERA_GPU_OK;
+}
+
+extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint8_t *d_seq,
+						   const int64_t *d_off, const int32_t *d_len, int32_t n,
+						   int32_t max_read_len, int write_bam,
+						   hera_gpu_result *d_out, void *stream)
+{
+	if (!ctx || !ctx->na || !d_seq || !d_off || !d_len || !d_out || !d_out->recs ||
+	    (write_bam != 0 && write_bam != 1) || max_read_len < 1 || max_read_len > MAX_READ)
+		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
+	if (n < 0 || n > (int32_t)na::PAIRS)
+		return fail(ctx, HERA_GPU_EINVAL,
+			    "allocation-free entry: more than HERA_GPU_NOALLOC_MAX_PAIRS (1024) pairs");
+	d_out->list_used = d_out->op_used = d_out->miss_used = 0;
+	if (n == 0)
+		return HERA_GPU_OK;
+	if (cudaSetDevice(ctx->device) != cudaSuccess)
+		return fail(ctx, HERA_GPU_ENODEV, "cudaSetDevice");
+	uint8_t *arena = nullptr;
+	if (noalloc_scratch(ctx->device, &arena) != HERA_GPU_OK)
+		return fail(ctx, HERA_GPU_ECUDA, "cudaGetSymbolAddress of the allocation-free scratch");
+	Lane &L = *ctx->na;
+	cudaStream_t caller = stream ? (cudaStream_t)stream : ctx->stream;
+	// byte range of the batch's reads (pinned counters of the lane)
+	int64_t *hb = reinterpret_cast<int64_t *>(L.h_small.p);
+	cudaMemcpyAsync(hb, d_off, 8, cudaMemcpyDeviceToHost, caller);
+	cudaMemcpyAsync(hb + 1, d_off + 2 * (int64_t)n - 1, 8, cudaMemcpyDeviceToHost, caller);
+	cudaMemcpyAsync(L.h_small.p + 4, d_len + 2 * (int64_t)n - 1, 4, cudaMemcpyDeviceToHost, caller);
+	if (cudaStreamSynchronize(caller) != cudaSuccess)
+		return fail(ctx, HERA_GPU_ECUDA, "read offsets");
+	const int64_t base = hb[0];
+	const int64_t bytes = hb[1] + L.h_small.p[4] - base;
+	if (bytes < 0 || (size_t)bytes + 64 > na::SEQ)
+		return fail(ctx, HERA_GPU_EINVAL, "allocation-free entry: reads exceed 2048 x HERA_GPU_MAX_READ bytes");
+
+	// carve the scratch
+	uint8_t *q = arena;
+	auto take = [&](size_t b) {
+		uint8_t *r = q;
+		q += na::A(b);
+		return r;
+	};
+	L.code.bind(take(na::SEQ), na::SEQ);
+	L.code_r.bind(take(na::SEQ), na::SEQ);
+	L.off.bind(take(na::READS * 8), na::READS);
+	L.hits.bind(take(na::READS * 2 * na::SPR * sizeof(uint2)), na::READS * 2 * na::SPR);
+	L.pairs.bind(take(na::PAIRS * sizeof(DPair)), na::PAIRS);
+	for (int k = 0; k < 2; ++k)
+		L.q[k].bind(take(na::PAIRS * sizeof(RmReq)), na::PAIRS);
+	for (int k = 0; k < 2; ++k)
+		L.qg[k].bind(take(na::PAIRS * sizeof(GpReq)), na::PAIRS);
+	L.counters.bind(take(16 * sizeof(int)), 16);
+	L.cnt.bind(take(6 * (na::ITEMS + 1) * sizeof(uint32_t)), 6 * (na::ITEMS + 1));
+	L.cub_tmp.bind(take(na::CUB), na::CUB);
+	L.tinfo.bind(take(na::TASKS * sizeof(TaskInfo)), na::TASKS);
+	L.tlist.bind(take(na::TASKS * sizeof(int)), na::TASKS);
+	L.chains.bind(take(na::CHAINS * sizeof(Chain)), na::CHAINS);
+	L.jobs.bind(take(na::JOBS * sizeof(DpJob)), na::JOBS);
+	L.slots.bind(take(na::SLOTS * sizeof(JobSlot)), na::SLOTS);
+	L.res.bind(take(na::JOBS * (size_t)res_stride(JCAP)), na::JOBS * (size_t)res_stride(JCAP));
+	L.perm.bind(take(na::JOBS * sizeof(int)), na::JOBS);
+	L.hist.bind(take(NBIN * sizeof(int)), NBIN);
+	L.calls.bind(take(na::PAIRS * LCAP * sizeof(int2)), na::PAIRS * LCAP);
+	L.rq_base.bind(take(na::PAIRS * sizeof(int)), na::PAIRS);
+	L.ssw_out.bind(take(na::CALLS * sizeof(SswOut)), na::CALLS);
+	L.scratch.bind(take(na::H), na::H);
+	L.chain_cap = na::CHAINS;
+	L.job_cap = na::JOBS;
+	L.slot_cap = na::SLOTS;
+	// outputs: the caller's device buffers (records: 2 n entries)
+	L.recs.bind(d_out->recs, 2 * (size_t)n);
+	L.pos_pool.bind(d_out->pos_pool, d_out->pos_pool ? d_out->list_cap + 1 : 0);
+	L.p_pool.bind(d_out->p_pool, d_out->p_pool ? d_out->list_cap + 1 : 0);
+	L.op_pool.bind(d_out->op_pool, d_out->op_pool ? d_out->op_cap + 1 : 0);
+	L.miss_pool.bind(d_out->miss_pool, d_out->miss_pool ? d_out->miss_cap + 1 : 0);
+
+	L.timing = hera_gpu_timing{};
+	L.err.clear();
+	cudaEventRecord(L.ev[0], caller);
+	cudaStreamWaitEvent(L.stream, L.ev[0], 0);
+	k_rebase<<<blocks_for(2 * (int64_t)n, 256), 256, 0, L.stream>>>(d_off, 2 * (int64_t)n, base, L.off.p);
+	const int rc = run_batch(ctx, L, d_seq + base, L.off.p, d_len, n, true, write_bam, max_read_len, bytes);
+	cudaEventRecord(L.ev[5], L.stream);
+	cudaStreamWaitEvent(caller, L.ev[5], 0);
+	ctx->timing = L.timing;
+	if (rc == HERA_GPU_ENOMEM) {
+		d_out->list_used = L.nl;
+		d_out->op_used = L.no;
+		d_out->miss_used = L.nm;
+		return fail(ctx, HERA_GPU_ECAPACITY,
+			    (std::string("allocation-free entry: fixed scratch or output buffer too small (") + L.err +
+			     "); *_used hold the pool sizes needed")
+				    .c_str());
+	}
+	if (rc != HERA_GPU_OK)
+		return fail(ctx, rc, L.err.c_str());
+	d_out->list_used = L.nl;
+	d_out->op_used = L.no;
+	d_out->miss_used = L.nm;
+	return HERA_GPU_OK;
 }
 
 // ---- drop-in Candidate form -------------------------------------------

@@ -220,6 +220,36 @@ int hera_gpu_align_pairs_device(hera_gpu_ctx *ctx, const uint8_t *d_seq,
 /* Copy the results of the last device-resident call into `out`. */
 int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out);
 
+/* Most pairs one hera_gpu_align_pairs_device_noalloc call accepts. */
+#define HERA_GPU_NOALLOC_MAX_PAIRS 1024
+
+/* No counterpart in the reference.  The same computation as
+ * hera_gpu_align_pairs_device for callers that must not allocate device
+ * memory while they align: code that runs inside a memory pool it does not
+ * own, or where a cudaMalloc would synchronise the device or fail under a
+ * hard memory budget.  This call allocates nothing.  Its working memory
+ * (the mate-rescue DP's matrix scratch, DP jobs, per-pair state, queues)
+ * is one static device array of 33.4 MiB, which every GPU that loads
+ * this library holds until the process exits.  The caller passes the reads
+ * in device memory (as for hera_gpu_align_pairs_device) and an output in
+ * device memory: d_out->recs with room for 2n records and the three pools
+ * with their capacities; *_used returns the pool sizes.
+ *   - n <= HERA_GPU_NOALLOC_MAX_PAIRS, reads <= HERA_GPU_MAX_READ bytes;
+ *     larger batches fail with HERA_GPU_EINVAL.  A batch whose internal
+ *     work (DP jobs, rescue calls) outgrows the static array, or whose
+ *     output outgrows d_out, fails with HERA_GPU_ECAPACITY (*_used then
+ *     give the pool sizes needed).
+ *   - The first call on a device looks up the static array's device
+ *     address (cudaGetSymbolAddress); make that first call before any
+ *     stream capture.
+ *   - Every call shares the one array and its state persists between calls
+ *     (each call initialises what it reads).  Calls that overlap on the GPU
+ *     -- from two threads, or two contexts on one device -- race. */
+int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint8_t *d_seq,
+					const int64_t *d_off, const int32_t *d_len,
+					int32_t n, int32_t max_read_len, int write_bam,
+					hera_gpu_result *d_out, void *stream);
+
 /* Per-stage timing of the last call on `ctx`. */
 int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out);
 
