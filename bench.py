@@ -33,6 +33,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "aligned read pairs/s"
+STAGES = ("seed_ms", "position_ms", "build_ms", "dp_ms", "resolve_ms", "rescue_ms", "pack_ms")
+COUNTS = ("probes", "seed_hits", "sw_cells", "ssw_cells")
 UNIT = "pairs/s"
 
 
@@ -255,8 +257,8 @@ def main():
             dist.barrier()
         sampler = ClockSampler(local)
         sampler.start()
-        stage = {k: 0.0 for k in ("seed_ms", "position_ms", "build_ms", "dp_ms", "resolve_ms",
-                                  "rescue_ms", "pack_ms")}
+        stage = {k: 0.0 for k in STAGES}
+        counts = {k: 0 for k in COUNTS}
         launches, jobs, calls, lookups = 0, 0, 0, 0
         evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         torch.cuda.synchronize()
@@ -271,6 +273,8 @@ def main():
             lookups += int(tm["lookups"])
             for k in stage:
                 stage[k] += float(tm[k])
+            for k in counts:
+                counts[k] += int(tm[k])
         torch.cuda.synchronize()
         clocks = sampler.stop()
         per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
@@ -279,8 +283,22 @@ def main():
         if world > 1:
             dist.barrier()
         out = {"path": path, "ms": ms, "per_step_ms": per, "stage": stage, "launches": launches,
-               "dp_jobs": jobs, "dp_calls": calls, "lookups": lookups, "clocks": clocks}
+               "dp_jobs": jobs, "dp_calls": calls, "lookups": lookups, "counts": counts,
+               "clocks": clocks}
         return ctx, out
+
+    def kernel_pass():
+        """One step on a single-lane context, so each kernel's CUDA-event
+        duration is its own (the timed run overlaps three lanes)."""
+        kctx = api.Context(ix, device=local, path="batched", lanes=1)
+        s, o, ln = dev[0]
+        for _ in range(2):
+            kctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
+                                    args.write_bam, kctx.stream)
+        torch.cuda.synchronize()
+        tm = kctx.timing()
+        kctx.close()
+        return tm
 
     paths = [p for p in args.paths.split(",") if p]
     plain = None
@@ -321,7 +339,11 @@ def main():
             log(f"cpu baseline failed: {e}")
 
     st = batched["stage"]
-    roof = roofline(st, batched, args)
+    ctx.close()
+    ktm = kernel_pass() if main_path == "batched" else None
+    dpx = api.dpx_peak(local)
+    pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
+    roof, roof_seed, roof_rescue = roofline(ktm, dpx, args, pair_bytes, max_len)
 
     if rank == 0:
         per = sorted(batched["per_step_ms"])
@@ -343,19 +365,32 @@ def main():
             "stage_ms_per_step": {k: v / args.steps for k, v in st.items()},
             "dp_jobs_per_step": batched["dp_jobs"] // args.steps,
             "dp_calls_per_step": batched["dp_calls"] // args.steps,
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roof, "roofline_seed": roof_seed, "roofline_rescue": roof_rescue,
+            "kernel_ms_per_step": None if ktm is None else {
+                k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
+                                                     "rescue_kernel_ms", "resolve_ms", "pack_ms")},
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": batched["launches"], "clocks": batched["clocks"],
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
     if world > 1:
         dist.destroy_process_group()
 
 
-def roofline(stage, run, args):
-    """Roofline of the seed-table gather kernel against the measured HBM
-    copy peak; the DP stages are integer-issue bound and are reported by
-    cells/s beside it."""
+def roofline(tm, dpx_instr_s, args, read_bytes, max_len):
+    """Rooflines of one single-lane step of the batched form.
+
+    Gap DP (the dominant kernels): SW_align cells evaluated (counted the
+    way the reference visits them) per second of the DP kernels, against the
+    measured DPX roof: __viaddmin_s16x2 instructions/s x 2 lanes / 2 DPX
+    operations per cell (min3-with-add of the edit-distance cell update).
+    Seed-table gathers: sector bytes moved per second of seed_probe against
+    the measured HBM copy peak; per lookup one 32 B sector for the bucket
+    offsets and one per binary-search probe, plus the reads' codes, offsets
+    and the hit records written.  Mate rescue: ssw_align cells per second of
+    the rescue kernels against the same DPX roof."""
+    if tm is None:
+        return None, None, None
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -364,9 +399,54 @@ def roofline(stage, run, args):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     src = "measured" if "hbm_gbs" in peaks else "fallback"
-    return {"kernel": "dominant stage: " + max(stage, key=stage.get).replace("_ms", ""),
-            "bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
-            "traffic": None, "peak_source": src}
+    dpx_cells = dpx_instr_s * 2 / 2 / 1e9   # Gcell/s
+    traffic = _profile_traffic()
+
+    dp_s = float(tm["dp_kernel_ms"]) / 1e3
+    cells = int(tm["sw_cells"])
+    dp = {"kernel": "k_dp_reg<4|8> + k_dp_generic (gap DP, all rounds)", "bound": "dpx",
+          "achieved": cells / dp_s / 1e9 if dp_s > 0 else None, "peak": dpx_cells, "unit": "Gcell/s",
+          "frac": (cells / dp_s / 1e9) / dpx_cells if dp_s > 0 else None,
+          "traffic": traffic.get("k_dp_reg_bytes_per_cell", 0) * cells or None,
+          "peak_source": "measured: DPX probe (hera_gpu_dpx_peak) on this GPU",
+          "work": {"sw_cells": cells, "dp_jobs": int(tm["dp_jobs"]), "dp_calls": int(tm["dp_calls"]),
+                   "kernel_ms": float(tm["dp_kernel_ms"])}}
+
+    n_reads = 2 * args.chunk
+    lookups, probes = int(tm["lookups"]), int(tm["probes"])
+    spr = (max_len - 31) // 31 + 1 if max_len >= 31 else 1
+    slots = n_reads * 2 * spr
+    fixed = read_bytes + 12 * n_reads + 8 * slots
+    useful = fixed + 8 * lookups + 16 * probes
+    sectors = fixed + 32 * lookups + 32 * probes
+    sd_s = float(tm["seed_kernel_ms"]) / 1e3
+    seed = {"kernel": "k_seed (seed_probe: hash_get gathers, space 31)", "bound": "hbm",
+            "achieved": sectors / sd_s / 1e9 if sd_s > 0 else None, "peak": hbm, "unit": "GB/s",
+            "frac": (sectors / sd_s / 1e9) / hbm if sd_s > 0 else None,
+            "traffic": traffic.get("k_seed_bytes_per_lookup", 0) * lookups or None,
+            "peak_source": src,
+            "sector_efficiency": (8 * lookups + 16 * probes) / (32 * lookups + 32 * probes)
+            if lookups else None,
+            "work": {"lookups": lookups, "probes": probes, "seed_hits": int(tm["seed_hits"]),
+                     "useful_bytes": useful, "sector_bytes": sectors, "kernel_ms": float(tm["seed_kernel_ms"])}}
+
+    rs_s = float(tm["rescue_kernel_ms"]) / 1e3
+    sc = int(tm["ssw_cells"])
+    rescue = {"kernel": "k_rescue_sw (ssw_align, warp per call)", "bound": "dpx",
+              "achieved": sc / rs_s / 1e9 if rs_s > 0 else None, "peak": dpx_cells, "unit": "Gcell/s",
+              "frac": (sc / rs_s / 1e9) / dpx_cells if rs_s > 0 else None, "traffic": None,
+              "work": {"ssw_cells": sc, "kernel_ms": float(tm["rescue_kernel_ms"])}}
+    return dp, seed, rescue
+
+
+def _profile_traffic() -> dict:
+    """Per-unit DRAM traffic of the top kernels from the committed ncu
+    summary (profiles/traffic.json), scaled by the units of this run."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
 
 
 if __name__ == "__main__":

@@ -72,7 +72,10 @@ class Timing(C.Structure):
                                          "rescue_ms", "pack_ms", "d2h_ms", "total_ms",
                                          "build_ms", "dp_ms")] + [
         ("launches", C.c_uint32), ("rescue_rounds", C.c_uint32), ("lookups", C.c_uint64),
-        ("dp_jobs", C.c_uint64), ("dp_calls", C.c_uint64)]
+        ("dp_jobs", C.c_uint64), ("dp_calls", C.c_uint64)] + [
+        (k, C.c_float) for k in ("seed_kernel_ms", "dp_kernel_ms", "rescue_kernel_ms",
+                                 "host_stage_ms", "host_out_ms")] + [
+        (k, C.c_uint64) for k in ("probes", "seed_hits", "sw_cells", "ssw_cells")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -105,8 +108,20 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_get_timing.argtypes = [C.c_void_p, C.POINTER(Timing)]
     lib.hera_gpu_stream.restype = C.c_void_p
     lib.hera_gpu_stream.argtypes = [C.c_void_p]
+    lib.hera_gpu_dpx_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double)]
     _lib = lib
     return lib
+
+
+def dpx_peak(device: int = 0, ms: float = 50.0) -> float:
+    """Thread-level __viaddmin_s16x2 instructions per second on `device`
+    (each updates two 16-bit lanes): the measured DPX issue rate."""
+    lib = load_library()
+    out = C.c_double()
+    rc = lib.hera_gpu_dpx_peak(device, ms, C.byref(out))
+    if rc != HERA_GPU_OK:
+        raise HeraGpuError(rc, "DPX probe failed")
+    return out.value
 
 
 def _ptr(a: np.ndarray) -> int:

@@ -515,23 +515,24 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 	 int rcap)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= n)
-		return;
-	const int id = perm[t];
-	const DpJob jb = jobs[id];
-	if (job_form(jb) != E)
-		return;
-	__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
-	DCig cig;
-	int flags = 0;
-	cig.n = cig.nm = 0;
-	const bool rev = jb.err < 0;
-	const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
-	RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
-	QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-	const int score = sw_align_fast<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags);
-	store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-	flag(b.flags, flags);
+	uint32_t cells = 0;
+	const int id = t < n ? perm[t] : 0;
+	if (t < n && job_form(jobs[id]) == E) {
+		const DpJob jb = jobs[id];
+		__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
+		DCig cig;
+		int flags = 0;
+		cig.n = cig.nm = 0;
+		const bool rev = jb.err < 0;
+		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
+		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
+		const int score =
+			sw_align_fast<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, cells);
+		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+		flag(b.flags, flags);
+	}
+	warp_stat(b.stats + ST_SW_CELLS, cells);
 }
 
 // the jobs outside the register form (empty gaps, spill cases)
@@ -539,22 +540,23 @@ __global__ void __launch_bounds__(128) k_dp_generic(Batch b, const DpJob *__rest
 						    uint8_t *__restrict__ res, int rcap)
 {
 	const int id = blockIdx.x * blockDim.x + threadIdx.x;
-	if (id >= n)
-		return;
-	const DpJob jb = jobs[id];
-	if (job_form(jb) != 0)
-		return;
-	SwWork sw;
-	DCig cig;
-	int flags = 0;
-	cig.n = cig.nm = 0;
-	int score = 0;
-	if (jb.len > 0) {
-		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
-		score = sw_align(b.ix, jb.rstart, q, jb.ref_len, jb.len, jb.err, b.score_only != 0, cig, sw, flags);
+	uint32_t cells = 0;
+	if (id < n && job_form(jobs[id]) == 0) {
+		const DpJob jb = jobs[id];
+		SwWork sw;
+		DCig cig;
+		int flags = 0;
+		cig.n = cig.nm = 0;
+		int score = 0;
+		if (jb.len > 0) {
+			const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+			score = sw_align(b.ix, jb.rstart, q, jb.ref_len, jb.len, jb.err, b.score_only != 0, cig, sw,
+					 flags, &cells);
+		}
+		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+		flag(b.flags, flags);
 	}
-	store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-	flag(b.flags, flags);
+	warp_stat(b.stats + ST_SW_CELLS, cells);
 }
 
 __device__ inline void load_res_cig(const uint8_t *o, int rcap, DCig &c)

@@ -183,7 +183,7 @@ struct RefWin {
 // q: query codes (already oriented), qlen; qrev: read q backwards (prefix DP)
 __device__ inline int sw_align(const DevIndex &ix, uint32_t rstart, const uint8_t *q,
 			       uint32_t ref_len, uint32_t len, int err, bool score_only,
-			       DCig &cig, SwWork &w, int &flags)
+			       DCig &cig, SwWork &w, int &flags, uint32_t *cells = nullptr)
 {
 	cig.n = 0;
 	cig.nm = 0;
@@ -266,6 +266,8 @@ __device__ inline int sw_align(const DevIndex &ix, uint32_t rstart, const uint8_
 			d = up;
 		}
 		w.wid[k] = (uint8_t)wd;
+		if (cells && i > (int)s + 1)
+			*cells += (uint32_t)(i - (int)s - 1);
 		if (min == error) {
 			++k;
 			break;
@@ -365,7 +367,8 @@ struct QView {   // query codes: q(x) = p[x * step]
 
 template <int E, bool STORE>
 __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
-				   bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags)
+				   bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags,
+				   uint32_t &cells)
 {
 	constexpr int W = 2 * E + 2;
 	constexpr unsigned error = E;
@@ -455,6 +458,7 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 			left = v;
 		}
 		i = broken ? brk : (int)ref_len + 1;
+		cells += i > s + 1 ? (uint32_t)(i - s - 1) : 0u;   // the cells the reference visits
 		if (min != error) {
 			// while (M[k][s] >= error && s < i) ++s
 			bool go = true;
@@ -490,8 +494,14 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 	if (min >= error) {
 		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
 			--k;
+			// The reference scans row k from column 0 to its break.  Cells
+			// left of the window are zero there and here (no effect: jj
+			// stays 0), and the break marker or ref_len lies inside the
+			// window, so the scan covers the window only.
 			int jj = 0;
-			for (int c = 0; (unsigned)c < ref_len; ++c) {
+			const int c_lo = k - E > 0 ? k - E : 0;
+			const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
+			for (int c = c_lo; c < c_hi; ++c) {
 				const unsigned v = get(k, c);
 				if (v == error + 1)
 					break;
@@ -523,8 +533,9 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}
-	if (!STORE)
+	if constexpr (!STORE)
 		return -1;
+	else {
 	while (i > 0 && k > 0) {
 		const unsigned cur = get(i, k);
 		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
@@ -548,6 +559,7 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 	for (int t = 1; t <= k; ++t)
 		cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	return score;
+	}
 }
 
 // Register-form SW_align: a forward pass without row storage first (enough
@@ -555,15 +567,22 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 // the rows kept for the shrink loop and the traceback.
 template <int E>
 __device__ inline int sw_align_fast(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
-				    bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags)
+				    bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags,
+				    uint32_t &n_cells)
 {
+	uint32_t cells = 0;
 	if (score_only) {
-		const int sc = sw_align_reg<E, false>(r, qc, ref_len, len, true, cig, rows, flags);
-		if (sc >= 0)
+		const int sc = sw_align_reg<E, false>(r, qc, ref_len, len, true, cig, rows, flags, cells);
+		if (sc >= 0) {
+			n_cells += cells;
 			return sc;
+		}
 		cig.n = cig.nm = 0;
+		cells = 0;
 	}
-	return sw_align_reg<E, true>(r, qc, ref_len, len, score_only, cig, rows, flags);
+	const int sc = sw_align_reg<E, true>(r, qc, ref_len, len, score_only, cig, rows, flags, cells);
+	n_cells += cells;
+	return sc;
 }
 
 // Entry used by the per-task (plain) path: the banded form, which keeps the
@@ -592,13 +611,15 @@ __device__ inline int gap_dp(const DevIndex &ix, uint32_t rstart, const uint8_t 
 // Buckets are sorted by id, so any search that finds the equal id returns
 // the reference's slot.
 // ---------------------------------------------------------------------
-__device__ __forceinline__ uint2 probe(const DevIndex &ix, uint64_t id)
+__device__ __forceinline__ uint2 probe(const DevIndex &ix, uint64_t id, uint32_t *n_probes = nullptr)
 {
 	const uint32_t mod = (uint32_t)(id & HMASK);
 	uint32_t lo = __ldg(ix.boff + mod);
 	uint32_t hi = __ldg(ix.boff + mod + 1);
 	while (lo < hi) {
 		uint32_t mid = (lo + hi) >> 1;
+		if (n_probes)
+			++*n_probes;
 		uint4 b = __ldg(ix.bk + mid);
 		uint64_t bid = ((uint64_t)b.y << 32) | b.x;
 		if (bid == id)
@@ -935,11 +956,19 @@ __device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
 // is what the reference's striped SSE2 loop with lazy-F converges to.  The
 // warp sweeps anti-diagonally: lane l owns read rows [l*R, l*R+R) and works
 // on column y = t - l + 1 at step t; the row above its block comes from lane
-// l-1 by shuffle one step later.  H is kept in HBM scratch in step-major
-// order (coalesced stores) for the reference's traceback, which one lane
-// then replays.
+// l-1 by shuffle one step later.
+//
+// The sweep keeps no matrix.  It finds the maximum and its cell, and every
+// SSW_CK columns it saves the whole column in shared memory.  The
+// reference's traceback then walks back from the maximum; the warp
+// recomputes the SSW_CK-column block the walk is in from the checkpoint at
+// its left edge (exact: a column depends only on the column before it), so
+// the walk reads shared memory only.  The reference window, the read and the
+// CIGAR under construction also live in the warp's shared-memory area.
 // ---------------------------------------------------------------------
 constexpr int SSW_RMAX = (MAX_READ + 31) / 32;   // rows per lane, <= 10
+constexpr int SSW_CK = 32;                       // checkpoint spacing (columns)
+constexpr int SSW_NCK = MAX_FRAG / SSW_CK + 1;   // checkpoints at columns j*SSW_CK
 
 __device__ __forceinline__ int mat_score(uint8_t a, uint8_t b)
 {
@@ -959,109 +988,162 @@ __device__ __forceinline__ uint8_t read_code(const uint8_t *code, int64_t o, int
 	return orient ? comp_code(code[o + L - 1 - x]) : code[o + x];
 }
 
-// bytes of HBM scratch one call needs
-__host__ __device__ inline size_t ssw_scratch_bytes(int max_len)
+// rows per lane used for a read of length L (instantiated widths only)
+__host__ __device__ inline int ssw_rows(int L)
 {
-	const int R = (max_len + 31) / 32;
-	const int Rp = (R + 3) & ~3;
-	return (size_t)(MAX_FRAG + 32) * 32 * (size_t)(Rp ? Rp : 4);
+	const int R = (L + 31) / 32;
+	return R <= 6 ? (R < 1 ? 1 : R) : (R <= 8 ? 8 : 10);
 }
 
-// Called by all 32 lanes of a warp.  Fills `out` (lane 0 writes).
-__device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code,
-				int64_t roff, int L, int orient, int start, uint32_t tl,
-				uint8_t *__restrict__ Hs, SswOut &out, int &flags)
+// shared-memory layout of one warp's area
+constexpr int SSW_REF_B = ((MAX_FRAG + 32 + 15) / 16) * 16;
+constexpr int SSW_RD_B = ((MAX_READ + 15) / 16) * 16;
+constexpr int SSW_CIG_B = (int)((sizeof(DCig) + 15) / 16) * 16;
+__host__ __device__ inline size_t ssw_smem_per_warp(int max_len)
+{
+	const int R = ssw_rows(max_len);
+	const size_t col = (size_t)32 * R;   // bytes of one saved column
+	return SSW_REF_B + SSW_RD_B + SSW_CIG_B + SSW_NCK * col + (((SSW_CK + 1) * col + 15) / 16) * 16;
+}
+
+// One block of the sweep: columns nb+1 .. nb+ncol, starting from the column
+// nb held in Hl (lane's rows) and bot0 (its last row); column values go to
+// `store(y, lane rows)` and the running maximum to best_*.
+template <int R, bool TRACK, typename Store>
+__device__ __forceinline__ void ssw_sweep(const uint8_t *__restrict__ ref_s, const uint8_t (&rdl)[R], int L,
+					  int nb, int ncol, int nact, int (&Hl)[R], int &best_v, int &best_y,
+					  int &best_x, Store store)
 {
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
-	const int R = (L + 31) / 32;
-	const int Rp = (R + 3) & ~3;
 	const int x0 = lane * R;
-	uint8_t rdl[SSW_RMAX];
-	int Hl[SSW_RMAX];
-#pragma unroll
-	for (int r = 0; r < SSW_RMAX; ++r) {
-		const int x = x0 + r;
-		rdl[r] = (r < R && x < L) ? read_code(code, roff, L, orient, x) : (uint8_t)5;
-		Hl[r] = 0;
-	}
-	int bot = 0, up_prev = 0;
-	int best_v = 0, best_y = 0, best_x = 0;
-	const uint8_t *rf = ix.code + wstart;
-	const int steps = ln > 0 ? ln + 31 : 0;
+	// `bot` as of step -1: lane 0 then stands on the left-edge column nb
+	// (its saved last row feeds lane 1's first diagonal), the others before it
+	int bot = lane == 0 ? Hl[R - 1] : 0, up_prev = 0;
+	const int steps = ncol > 0 ? ncol + nact - 1 : 0;
 	for (int t = 0; t < steps; ++t) {
-		const int y = t - lane + 1;
+		const int y = nb + t - lane + 1;
 		int up_in = __shfl_up_sync(FULL, bot, 1);
 		if (lane == 0)
 			up_in = 0;
 		const int diag_in = up_prev;
 		up_prev = up_in;
-		if (y >= 1 && y <= ln) {
-			const uint8_t rc = rf[y - 1];
+		if (y > nb && y <= nb + ncol) {
+			const uint8_t rc = ref_s[y - 1];
 			int d = diag_in, up = up_in, cmax = 0;
-			uint32_t pack[SSW_RMAX / 4 + 1];
 #pragma unroll
-			for (int w = 0; w < SSW_RMAX / 4 + 1; ++w)
-				pack[w] = 0;
-#pragma unroll
-			for (int r = 0; r < SSW_RMAX; ++r) {
-				if (r < R) {
-					const int left = Hl[r];
-					// max(0, min(255, d + 3*eq) - 2, left - 4, up - 4), d <= 253
-					const int a = __viaddmin_s32(d, rdl[r] == rc ? 1 : -2, 253);
-					int v = __vimax3_s32_relu(a, left - 4, up - 4);
-					if (x0 + r >= L)
-						v = 0;
-					d = left;
-					Hl[r] = v;
-					up = v;
-					cmax = __vimax_s32_relu(cmax, v);
-					pack[r >> 2] |= (uint32_t)v << (8 * (r & 3));
-				}
+			for (int r = 0; r < R; ++r) {
+				const int left = Hl[r];
+				// max(0, min(255, d + 3*eq) - 2, left - 4, up - 4), d <= 253
+				const int a = __viaddmin_s32(d, rdl[r] == rc ? 1 : -2, 253);
+				int v = __vimax3_s32_relu(a, left - 4, up - 4);
+				if (x0 + r >= L)
+					v = 0;
+				d = left;
+				Hl[r] = v;
+				up = v;
+				cmax = __vimax_s32_relu(cmax, v);
 			}
-			if (cmax > best_v) {   // first row of this column reaching it
+			if (TRACK && cmax > best_v) {   // first row of this column reaching it
 				int fx = 0;
 #pragma unroll
-				for (int r = SSW_RMAX - 1; r >= 0; --r)
-					if (r < R && Hl[r] == cmax)
+				for (int r = R - 1; r >= 0; --r)
+					if (Hl[r] == cmax)
 						fx = r;
 				best_v = cmax;
 				best_y = y;
 				best_x = x0 + fx;
 			}
 			bot = Hl[R - 1];
-			uint32_t *dst = reinterpret_cast<uint32_t *>(Hs + ((size_t)t * 32 + lane) * Rp);
-#pragma unroll
-			for (int w = 0; w < SSW_RMAX / 4 + 1; ++w)
-				if (w * 4 < Rp)
-					dst[w] = pack[w];
+			store(y, Hl);
 		} else {
-			bot = 0;
+			// column nb is the block's left edge: the lane's saved last row
+			bot = y == nb ? Hl[R - 1] : 0;
 		}
 	}
+}
+
+// Called by all 32 lanes of a warp; `sm` is the warp's shared-memory area
+// (ssw_smem_per_warp(L) bytes at least).  Fills `out` (lane 0 writes the
+// scalars; the CIGAR is copied by the warp).
+template <int R>
+__device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff, int L,
+			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out, int &flags)
+{
+	const unsigned FULL = 0xffffffffu;
+	const int lane = threadIdx.x & 31;
+	const int x0 = lane * R;
+	const int COL = 32 * R;
+	uint8_t *ref_s = sm;
+	uint8_t *rd_s = sm + SSW_REF_B;
+	DCig &cig = *reinterpret_cast<DCig *>(sm + SSW_REF_B + SSW_RD_B);
+	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + SSW_CIG_B;
+	uint8_t *tb = ck + (size_t)SSW_NCK * COL;
+
+	for (int i = lane; i < ln; i += 32)
+		ref_s[i] = __ldg(ix.code + wstart + i);
+	for (int i = lane; i < L; i += 32)
+		rd_s[i] = read_code(code, roff, L, orient, i);
+	if (lane == 0)
+		cig.n = cig.nm = 0;
+	__syncwarp();
+	uint8_t rdl[R];
+	int Hl[R];
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		rdl[r] = x0 + r < L ? rd_s[x0 + r] : (uint8_t)5;
+		Hl[r] = 0;
+	}
+	const int nact = (L + R - 1) / R;   // lanes holding read rows
+	int best_v = 0, best_y = 0, best_x = 0;
+	ssw_sweep<R, true>(ref_s, rdl, L, 0, ln, nact, Hl, best_v, best_y, best_x, [&](int y, const int (&H)[R]) {
+		if ((y & (SSW_CK - 1)) == 0) {
+			uint8_t *c = ck + (size_t)(y / SSW_CK) * COL + x0;
+#pragma unroll
+			for (int r = 0; r < R; ++r)
+				c[r] = (uint8_t)H[r];
+		}
+	});
 	// max over all cells; first column reaching it; first row in that column
 	const int max_v = __reduce_max_sync(FULL, best_v);
 	const int min_y = __reduce_min_sync(FULL, best_v == max_v ? best_y : 0x7fffffff);
 	const int min_x = __reduce_min_sync(FULL, (best_v == max_v && best_y == min_y) ? best_x : 0x7fffffff);
 	__syncwarp();
-	if (lane != 0)
-		return;
 
-	DCig &cig = out.cig;
-	cig.n = cig.nm = 0;
 	const uint8_t *ra = ix.seq + wstart;
-	auto HV = [&](int x, int yy) -> int {
-		if (yy == 0)
-			return 0;
-		const int l = x / R, r = x - l * R;
-		return Hs[((size_t)(yy + l - 1) * 32 + l) * Rp + r];
+	const bool w0 = lane == 0;
+	auto add = [&](int type, unsigned n, const uint8_t *mc) {
+		if (w0)
+			cig_add(cig, type, n, mc, flags);
 	};
-	auto RD = [&](int x) -> uint8_t { return read_code(code, roff, L, orient, x); };
+	// block of saved columns [nb, nb + SSW_CK] around the walk
+	int nb = -1;
+	auto load_block = [&](int b) {
+		nb = b;
+		__syncwarp();
+		int H0[R];
+		const uint8_t *c0 = ck + (size_t)(b / SSW_CK) * COL;
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			H0[r] = b == 0 ? 0 : c0[x0 + r];
+			tb[x0 + r] = (uint8_t)H0[r];
+		}
+		int bv = 0, by = 0, bx = 0;
+		const int ncol = ln - b < SSW_CK ? ln - b : SSW_CK;
+		ssw_sweep<R, false>(ref_s, rdl, L, b, ncol, nact, H0, bv, by, bx, [&](int y, const int (&H)[R]) {
+			uint8_t *c = tb + (size_t)(y - b) * COL + x0;
+#pragma unroll
+			for (int r = 0; r < R; ++r)
+				c[r] = (uint8_t)H[r];
+		});
+		__syncwarp();
+	};
+	auto HV = [&](int x, int yy) -> int { return yy == 0 ? 0 : tb[(size_t)(yy - nb) * COL + x]; };
 	const int end_ref = max_v > 0 ? min_y - 1 : -1;
 	int begin_ref = end_ref, score = 0, end_read = L - 1;
 	if (max_v < (L >> 2) || max_v == 0) {
 		score = L;
-		cig_add(cig, OP_S, (unsigned)L, nullptr, flags);
+		add(OP_S, (unsigned)L, nullptr);
 	} else {
 		if (min_x < end_read)
 			end_read = min_x;
@@ -1071,39 +1153,42 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 			if (right < 5) {
 				for (int i = L - 1, j = end_ref + right; i > end_read; --i, --j) {
 					if (j >= ln) {
-						cig_add(cig, OP_S, 1, nullptr, flags);
+						add(OP_S, 1, nullptr);
 						++score;
-					} else if (RD(i) == rf[j]) {
-						cig_add(cig, OP_M, 1, nullptr, flags);
+					} else if (rd_s[i] == ref_s[j]) {
+						add(OP_M, 1, nullptr);
 					} else {
-						cig_add(cig, OP_X, 1, ra + j, flags);
+						add(OP_X, 1, ra + j);
 						++score;
 					}
 				}
 			} else {
 				score += right;
-				cig_add(cig, OP_S, (unsigned)right, nullptr, flags);
+				add(OP_S, (unsigned)right, nullptr);
 			}
 		}
+		load_block((y_pos - 1) / SSW_CK * SSW_CK);
 		int cur = HV(x_pos, y_pos), dir = 0;
 		for (;;) {
-			const uint8_t qb = RD(begin_read), rb = rf[begin_ref];
+			const uint8_t qb = rd_s[begin_read], rb = ref_s[begin_ref];
 			if (dir == 0) {
 				if (qb == rb) {
-					cig_add(cig, OP_M, 1, nullptr, flags);
+					add(OP_M, 1, nullptr);
 				} else {
-					cig_add(cig, OP_X, 1, ra + begin_ref, flags);
+					add(OP_X, 1, ra + begin_ref);
 					++score;
 				}
 			} else if (dir == 1) {   // a step along the reference
 				++score;
-				cig_add(cig, OP_I, 1, nullptr, flags);
+				add(OP_I, 1, nullptr);
 			} else {                 // a step along the read
 				++score;
-				cig_add(cig, OP_D, 1, ra + begin_ref, flags);
+				add(OP_D, 1, ra + begin_ref);
 			}
 			if (x_pos == 0 || y_pos == 1)
 				break;
+			if (y_pos - 1 < nb)   // the walk left the block: recompute the one before
+				load_block(nb - SSW_CK);
 			const int diag = HV(x_pos - 1, y_pos - 1);
 			const int up = HV(x_pos - 1, y_pos);
 			const int left = HV(x_pos, y_pos - 1);
@@ -1130,26 +1215,53 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 		if (begin_read < 5) {
 			for (--begin_read, --begin_ref; begin_read >= 0; --begin_read, --begin_ref) {
 				if (begin_ref < 0) {
-					cig_add(cig, OP_S, 1, nullptr, flags);
+					add(OP_S, 1, nullptr);
 					++score;
-				} else if (RD(begin_read) == rf[begin_ref]) {
-					cig_add(cig, OP_M, 1, nullptr, flags);
+				} else if (rd_s[begin_read] == ref_s[begin_ref]) {
+					add(OP_M, 1, nullptr);
 				} else {
-					cig_add(cig, OP_X, 1, ra + begin_ref, flags);
+					add(OP_X, 1, ra + begin_ref);
 					++score;
 				}
 			}
 		} else if (begin_read > 0) {
 			score += begin_read;
-			cig_add(cig, OP_S, (unsigned)begin_read, nullptr, flags);
+			add(OP_S, (unsigned)begin_read, nullptr);
 		}
 	}
-	const int skip = begin_ref;
-	out.score = score;
-	out.skip = skip;
-	out.pstart = start + skip;
-	// acceptance test of re_mapSW (src/hash_align.c:788-792)
-	out.ok = !(score > L / 2 || start + skip < 0 || (uint32_t)(start + skip + L) > tl);
+	__syncwarp();
+	const int n = cig.n, nm = cig.nm;
+	for (int k = lane; k < n; k += 32)
+		out.cig.op[k] = cig.op[k];
+	for (int k = lane; k < nm; k += 32)
+		out.cig.miss[k] = cig.miss[k];
+	if (w0) {
+		const int skip = begin_ref;
+		out.cig.n = n;
+		out.cig.nm = nm;
+		out.score = score;
+		out.skip = skip;
+		out.pstart = start + skip;
+		// acceptance test of re_mapSW (src/hash_align.c:788-792)
+		out.ok = !(score > L / 2 || start + skip < 0 || (uint32_t)(start + skip + L) > tl);
+	}
+}
+
+// the call's read length picks the rows-per-lane instantiation
+__device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff,
+				int L, int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out,
+				int &flags)
+{
+	switch (ssw_rows(L)) {
+	case 1: ssw_warp_r<1>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 2: ssw_warp_r<2>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 3: ssw_warp_r<3>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 4: ssw_warp_r<4>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 5: ssw_warp_r<5>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 6: ssw_warp_r<6>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 8: ssw_warp_r<8>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	default: ssw_warp_r<10>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	}
 }
 
 }  // namespace hg

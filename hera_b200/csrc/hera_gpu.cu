@@ -46,14 +46,26 @@ struct Batch {
 	const int32_t *len;
 	DPair *P;
 	int *flags;
+	unsigned long long *stats;   // work counters, ST_* slots
 	int score_only;
 	int max_len;             // longest read of the batch (seed table stride)
 };
+
+// work counters (hera_gpu_timing's probes .. ssw_cells)
+enum { ST_PROBES = 0, ST_SEED_HITS = 1, ST_SW_CELLS = 2, ST_SSW_CELLS = 3, ST_N = 4 };
 
 __device__ __forceinline__ void flag(int *f, int v)
 {
 	if (v)
 		atomicOr(f, v);
+}
+
+// add v over the whole warp to a counter (every lane of the warp calls it)
+__device__ __forceinline__ void warp_stat(unsigned long long *c, uint32_t v)
+{
+	v = __reduce_add_sync(0xffffffffu, v);
+	if ((threadIdx.x & 31) == 0 && v)
+		atomicAdd(c, (unsigned long long)v);
 }
 
 // read `ri` in orientation `orient` (1 = reverse complement) into rd
@@ -99,20 +111,20 @@ __global__ void k_rc(const uint8_t *__restrict__ code, const int64_t *__restrict
 
 // seed_probe: thread per (read, strand, seed) at spacing 31
 __global__ void k_seed(DevIndex ix, const uint8_t *__restrict__ code, const int64_t *__restrict__ off,
-		       const int32_t *__restrict__ len, int n_reads, int spr, uint2 *__restrict__ hits)
+		       const int32_t *__restrict__ len, int n_reads, int spr, uint2 *__restrict__ hits,
+		       unsigned long long *__restrict__ stats)
 {
 	const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
 	const int64_t total = (int64_t)n_reads * 2 * spr;
-	if (t >= total)
-		return;
+	uint32_t np = 0, found = 0;
 	const int j = (int)(t % spr);
 	const int64_t ro = t / spr;
 	const int orient = (int)(ro & 1);
 	const int ri = (int)(ro >> 1);
-	const int L = len[ri];
+	const int L = t < total ? len[ri] : 0;
 	const int i = j * KMER;
 	uint2 h = make_uint2(0, 0);
-	if (i + KMER <= L && j < spr) {
+	if (t < total && i + KMER <= L && j < spr) {
 		const uint8_t *src = code + off[ri];
 		uint64_t id = 0;
 		if (orient == 0) {
@@ -124,9 +136,13 @@ __global__ void k_seed(DevIndex ix, const uint8_t *__restrict__ code, const int6
 			for (int x = 0; x < KMER; ++x)
 				id = (id << 2) | comp_code(src[L - 1 - i - x]);
 		}
-		h = probe(ix, id);
+		h = probe(ix, id, &np);
+		found = h.y > 0;
 	}
-	hits[t] = h;
+	if (t < total)
+		hits[t] = h;
+	warp_stat(stats + ST_PROBES, np);
+	warp_stat(stats + ST_SEED_HITS, found);
 }
 
 __device__ __forceinline__ void slot_reset(DSlot &S)
@@ -296,12 +312,14 @@ __global__ void k_rescue_expand(Batch b, const RmReq *__restrict__ q, int nq, in
 		calls[at + i] = make_int2(t, i);
 }
 
-// 2) one warp per call: local SW over the MAX_FRAG window at the mate hit
-__global__ void __launch_bounds__(128) k_rescue_sw(Batch b, const RmReq *__restrict__ q,
-						    const int2 *__restrict__ calls, int c0, int nc,
-						    SswOut *__restrict__ out, uint8_t *__restrict__ scratch,
-						    size_t per)
+// 2) one warp per call: local SW over the MAX_FRAG window at the mate hit;
+// each warp works in its own `per` bytes of the block's shared memory
+constexpr int RESCUE_TPB = 128;
+__global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *__restrict__ q,
+							   const int2 *__restrict__ calls, int c0, int nc,
+							   SswOut *__restrict__ out, int per)
 {
+	extern __shared__ __align__(16) uint8_t ssw_sm[];
 	const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // warp within launch
 	if (wl >= nc)
 		return;
@@ -324,10 +342,20 @@ __global__ void __launch_bounds__(128) k_rescue_sw(Batch b, const RmReq *__restr
 	if (ln < 0)
 		ln = 0;
 	int flags = 0;
+	if (L < 0 || L > b.max_len) {   // longer than the batch's stated maximum: no room in the area
+		if ((threadIdx.x & 31) == 0) {
+			out[c0 + wl].ok = 0;
+			out[c0 + wl].cig.n = out[c0 + wl].cig.nm = 0;
+			flag(b.flags, F_READ);
+		}
+		return;
+	}
 	ssw_warp(b.ix, __ldg(b.ix.tstart + tr) + (uint32_t)start, ln, b.code, b.off[ri], L, str, start, tl,
-		 scratch + (size_t)wl * per, out[c0 + wl], flags);
-	if ((threadIdx.x & 31) == 0)
+		 ssw_sm + (size_t)(threadIdx.x >> 5) * per, out[c0 + wl], flags);
+	if ((threadIdx.x & 31) == 0) {
 		flag(b.flags, flags);
+		atomicAdd(b.stats + ST_SSW_CELLS, (unsigned long long)ln * (unsigned long long)L);
+	}
 }
 
 // 3) per request: min score wins, ties append in hit order; the mate's list
@@ -538,7 +566,7 @@ struct HBuf {   // growable pinned host buffer
 // of the others.
 struct Lane {
 	cudaStream_t stream = nullptr;
-	cudaEvent_t ev[8]{};
+	cudaEvent_t ev[12]{};
 	DBuf<uint8_t> seq, code, code_r;
 	DBuf<int64_t> off;
 	DBuf<int32_t> len;
@@ -548,7 +576,7 @@ struct Lane {
 	DBuf<GpReq> qg[2];
 	DBuf<int> counters;
 	DBuf<uint32_t> cnt;
-	DBuf<uint8_t> cub_tmp, scratch;
+	DBuf<uint8_t> cub_tmp;
 	DBuf<int2> calls;
 	DBuf<int> rq_base;
 	DBuf<SswOut> ssw_out;
@@ -581,7 +609,7 @@ struct Lane {
 	{
 		seq.release(); code.release(); code_r.release(); off.release(); len.release();
 		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
-		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release(); scratch.release();
+		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release();
 		calls.release(); rq_base.release(); ssw_out.release(); tinfo.release(); chains.release();
 		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
@@ -605,7 +633,7 @@ struct hera_gpu_ctx {
 	uint8_t *d_seq = nullptr, *d_tcode = nullptr;
 	uint32_t *d_tlen = nullptr, *d_tstart = nullptr;
 	uint32_t max_batch = 1u << 18;    // pairs per sub-batch
-	uint64_t scratch_bytes = 2ull << 30;
+	uint64_t scratch_bytes = 0;       // accepted for compatibility; unused
 	int batched = 1;
 	std::vector<Lane *> lanes;
 	Lane *na = nullptr;               // lane of hera_gpu_align_pairs_device_noalloc
@@ -729,6 +757,10 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		return bail(HERA_GPU_ENODEV);
 	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
+	// the rescue kernel's per-warp shared-memory areas (up to ~89 KiB a block)
+	if (cudaFuncSetAttribute(k_rescue_sw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				 (int)((RESCUE_TPB / 32) * ssw_smem_per_warp(MAX_READ))) != cudaSuccess)
+		return bail(fail(ctx, HERA_GPU_ECUDA, "rescue kernel shared-memory size"));
 	for (int i = 0; i < nlanes; ++i) {
 		Lane *L = new Lane();
 		ctx->lanes.push_back(L);
@@ -737,11 +769,11 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		for (auto &e : L->ev)
 			cudaEventCreate(&e);
 	}
-	// the allocation-free entry's lane: its stream, events and 16 pinned
+	// the allocation-free entry's lane: its stream, events and 32 pinned
 	// counters are made here, so that entry point itself allocates nothing
 	ctx->na = new Lane();
 	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
-	    ctx->na->h_small.ensure(16) != cudaSuccess)
+	    ctx->na->h_small.ensure(32) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
 	for (auto &e : ctx->na->ev)
 		cudaEventCreate(&e);
@@ -820,19 +852,14 @@ static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const 
 	LK(cudaStreamSynchronize(st), "rescue expand");
 	const int ncalls = L.h_small.p[1];
 	LK(L.ssw_out.ensure(ncalls + 1), "rescue outputs");
-	const size_t per = ssw_scratch_bytes(max_len);
-	size_t slots = (L.scratch.fixed ? L.scratch.cap : ctx->scratch_bytes / ctx->lanes.size()) / per;
-	if (slots < 1)
-		slots = 1;
-	if (slots > (size_t)ncalls)
-		slots = (size_t)(ncalls > 0 ? ncalls : 1);
-	LK(L.scratch.ensure(slots * per), "rescue scratch");
-	for (int c0 = 0; c0 < ncalls; c0 += (int)slots) {
-		const int m = (int)((size_t)(ncalls - c0) < slots ? (size_t)(ncalls - c0) : slots);
-		k_rescue_sw<<<blocks_for((int64_t)m * 32), TPB, 0, st>>>(b, q, L.calls.p, c0, m, L.ssw_out.p,
-									 L.scratch.p, per);
+	const int per = (int)ssw_smem_per_warp(max_len);
+	cudaEventRecord(L.ev[10], st);
+	if (ncalls > 0) {
+		k_rescue_sw<<<blocks_for((int64_t)ncalls * 32, RESCUE_TPB), RESCUE_TPB, (RESCUE_TPB / 32) * per, st>>>(
+			b, q, L.calls.p, 0, ncalls, L.ssw_out.p, per);
 		++launches;
 	}
+	cudaEventRecord(L.ev[11], st);
 	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.rq_base.p, L.ssw_out.p);
 	++launches;
 	cudaEventRecord(e1, st);
@@ -840,6 +867,8 @@ static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const 
 	float ms = 0;
 	cudaEventElapsedTime(&ms, e0, e1);
 	ms_acc += ms;
+	cudaEventElapsedTime(&ms, L.ev[10], L.ev[11]);
+	L.timing.rescue_kernel_ms += ms;
 	return HERA_GPU_OK;
 }
 
@@ -915,9 +944,11 @@ static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float 
 		k_bin_count<<<148, 512, 0, st>>>(L.jobs.p, nj, L.hist.p);
 		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
 		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
+		cudaEventRecord(L.ev[10], st);
 		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
 		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
 		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
+		cudaEventRecord(L.ev[11], st);
 		launches += 6;
 		R.res = L.res.p;
 	}
@@ -927,6 +958,10 @@ static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float 
 	LK(cudaEventSynchronize(e1), "replay");
 	cudaEventElapsedTime(&ms, e0, e1);
 	dp_ms += ms;
+	if (nj > 0) {
+		cudaEventElapsedTime(&ms, L.ev[10], L.ev[11]);
+		L.timing.dp_kernel_ms += ms;
+	}
 	L.timing.dp_jobs += (uint64_t)nj;
 	return HERA_GPU_OK;
 }
@@ -951,14 +986,15 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	if (batched)
 		LK(L.code_r.ensure(seq_bytes + 64), "read code buffer");
 	LK(L.pairs.ensure(n), "pair state");
-	LK(L.counters.ensure(16), "counters");
+	LK(L.counters.ensure(32), "counters");
 	LK(L.q[0].ensure(n), "rescue queue");
 	LK(L.q[1].ensure(n), "rescue queue");
 	LK(L.cnt.ensure(6 * (size_t)(items + 1)), "count buffer");
 	LK(L.recs.ensure(items), "records");
-	LK(L.h_small.ensure(16), "host counters");
+	LK(L.h_small.ensure(32), "host counters");
 	int *d_flags = L.counters.p;
-	LK(cudaMemsetAsync(L.counters.p, 0, 16 * sizeof(int), st), "memset");
+	unsigned long long *d_stats = reinterpret_cast<unsigned long long *>(L.counters.p + 16);
+	LK(cudaMemsetAsync(L.counters.p, 0, 32 * sizeof(int), st), "memset");
 
 	Batch b;
 	b.ix = ctx->ix;
@@ -968,6 +1004,7 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	b.len = d_len;
 	b.P = L.pairs.p;
 	b.flags = d_flags;
+	b.stats = d_stats;
 	b.score_only = write_bam == 1;
 	b.max_len = max_len;
 
@@ -985,7 +1022,10 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	if (paired) {
 		LK(L.hits.ensure((size_t)n_reads * 2 * spr), "seed hits");
 		const int64_t ns = (int64_t)n_reads * 2 * spr;
-		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, L.code.p, d_off, d_len, n_reads, spr, L.hits.p);
+		cudaEventRecord(L.ev[8], st);
+		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, L.code.p, d_off, d_len, n_reads, spr, L.hits.p,
+							     d_stats);
+		cudaEventRecord(L.ev[9], st);
 		++launches;
 		T.lookups += (uint64_t)ns;
 	}
@@ -1097,6 +1137,8 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	LK(cudaMemcpyAsync(L.h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
 	LK(cudaMemcpyAsync(L.h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
 	LK(cudaMemcpyAsync(L.h_small.p + 5, d_flags, 4, cudaMemcpyDeviceToHost, st), "flags");
+	LK(cudaMemcpyAsync(L.h_small.p + 16, d_stats, ST_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+	   "counters");
 	LK(cudaStreamSynchronize(st), "scan");
 	const uint32_t tl = (uint32_t)L.h_small.p[2], to = (uint32_t)L.h_small.p[3],
 		       tm = (uint32_t)L.h_small.p[4];
@@ -1118,6 +1160,17 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 	float ms = 0;
 	cudaEventElapsedTime(&ms, L.ev[1], L.ev[2]);
 	T.seed_ms += ms;
+	if (paired) {
+		cudaEventElapsedTime(&ms, L.ev[8], L.ev[9]);
+		T.seed_kernel_ms += ms;
+	}
+	{
+		const unsigned long long *hs = reinterpret_cast<const unsigned long long *>(L.h_small.p + 16);
+		T.probes += hs[ST_PROBES];
+		T.seed_hits += hs[ST_SEED_HITS];
+		T.sw_cells += hs[ST_SW_CELLS];
+		T.ssw_cells += hs[ST_SSW_CELLS];
+	}
 	if (!batched) {
 		cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]);
 		T.position_ms += ms;
@@ -1171,6 +1224,7 @@ static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, u
 	float ms = 0;
 	cudaEventElapsedTime(&ms, L.ev[6], L.ev[7]);
 	L.timing.d2h_ms += ms;
+	const auto h0 = std::chrono::steady_clock::now();
 	hera_cand_rec *dst = out->recs + rec0;
 	for (int i = 0; i < items; ++i) {
 		hera_cand_rec r = L.h_recs.p[i];
@@ -1189,6 +1243,8 @@ static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, u
 		memcpy(out->op_pool + bo, L.h_ops.p, L.no * 4);
 	if (L.nm)
 		memcpy(out->miss_pool + bm, L.h_miss.p, L.nm);
+	L.timing.host_out_ms +=
+		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - h0).count();
 	return HERA_GPU_OK;
 }
 
@@ -1219,6 +1275,7 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 	LK(L.h_seq.ensure(total + 1), "pinned reads");
 	LK(L.h_off.ensure((size_t)n * per), "pinned offsets");
 	LK(L.h_len.ensure((size_t)n * per), "pinned lengths");
+	const auto h0 = std::chrono::steady_clock::now();
 	int64_t o = 0;
 	for (int m = 0; m < per; ++m) {
 		const hera_gpu_reads *r = src[m];
@@ -1241,6 +1298,8 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 			}
 		}
 	}
+	L.timing.host_stage_ms +=
+		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - h0).count();
 	LK(L.seq.ensure(total + 64), "device reads");
 	LK(L.off.ensure((size_t)n * per), "device offsets");
 	LK(L.len.ensure((size_t)n * per), "device lengths");
@@ -1331,6 +1390,15 @@ static void sum_timing(hera_gpu_ctx *ctx)
 		t.lookups += a.lookups;
 		t.dp_jobs += a.dp_jobs;
 		t.dp_calls += a.dp_calls;
+		t.seed_kernel_ms += a.seed_kernel_ms;
+		t.dp_kernel_ms += a.dp_kernel_ms;
+		t.rescue_kernel_ms += a.rescue_kernel_ms;
+		t.host_stage_ms += a.host_stage_ms;
+		t.host_out_ms += a.host_out_ms;
+		t.probes += a.probes;
+		t.seed_hits += a.seed_hits;
+		t.sw_cells += a.sw_cells;
+		t.ssw_cells += a.ssw_cells;
 	}
 	t.total_ms = ctx->timing.total_ms;
 	ctx->timing = t;
@@ -1348,7 +1416,13 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 	const int ncand = paired ? 2 : 1;
 	for (Lane *L : ctx->lanes)
 		L->timing = hera_gpu_timing{};
-	const int32_t sub = (int32_t)ctx->max_batch;
+	// sub-batches of at most max_batch pairs, as many as a multiple of the
+	// lane count (each lane then carries an equal share of the call)
+	const int64_t nlanes = (int64_t)ctx->lanes.size();
+	int64_t ns = (n + (int64_t)ctx->max_batch - 1) / ctx->max_batch;
+	if (ns > 0 && n >= nlanes * 4096)
+		ns = (ns + nlanes - 1) / nlanes * nlanes;
+	const int32_t sub = ns > 0 ? (int32_t)((n + ns - 1) / ns) : 1;
 	const int nsub = (int)((n + (int64_t)sub - 1) / sub);
 	Sched S;
 	S.ready.assign(nsub, 0);
@@ -1544,8 +1618,8 @@ extern "C" int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out)
 // ---- allocation-free variant of the device-resident entry ---------------
 //
 // For callers that cannot allocate device memory while they align (see
-// include/hera_gpu.h).  Every per-batch buffer -- the mate-rescue DP's H
-// matrix scratch, the DP jobs and results, the per-pair Candidate state, the
+// include/hera_gpu.h).  Every per-batch buffer -- the mate-rescue calls'
+// outputs, the DP jobs and results, the per-pair Candidate state, the
 // queues -- is carved from one file-scope device array; records go straight
 // into the caller's device buffers.  Sized for HERA_GPU_NOALLOC_MAX_PAIRS
 // pairs of reads up to HERA_GPU_MAX_READ.
@@ -1563,14 +1637,13 @@ constexpr size_t JOBS = 32 * PAIRS;
 constexpr size_t SLOTS = 64 * PAIRS;
 constexpr size_t CALLS = 8 * PAIRS;
 constexpr size_t CUB = 64 << 10;
-constexpr size_t H = 16 << 20;     // mate-rescue DP scratch
 constexpr size_t BYTES =
 	2 * A(SEQ) + A(READS * 8) + A(READS * 2 * SPR * sizeof(uint2)) + A(PAIRS * sizeof(DPair)) +
-	2 * A(PAIRS * sizeof(RmReq)) + 2 * A(PAIRS * sizeof(GpReq)) + A(16 * sizeof(int)) +
+	2 * A(PAIRS * sizeof(RmReq)) + 2 * A(PAIRS * sizeof(GpReq)) + A(32 * sizeof(int)) +
 	A(6 * (ITEMS + 1) * sizeof(uint32_t)) + A(CUB) + A(TASKS * sizeof(TaskInfo)) + A(TASKS * sizeof(int)) +
 	A(CHAINS * sizeof(Chain)) + A(JOBS * sizeof(DpJob)) + A(SLOTS * sizeof(JobSlot)) +
 	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
-	A(PAIRS * LCAP * sizeof(int2)) + A(PAIRS * sizeof(int)) + A(CALLS * sizeof(SswOut)) + A(H);
+	A(PAIRS * LCAP * sizeof(int2)) + A(PAIRS * sizeof(int)) + A(CALLS * sizeof(SswOut));
 }  // namespace na
 
 // the scratch: every GPU that loads this library holds it until exit
@@ -1646,7 +1719,7 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 		L.q[k].bind(take(na::PAIRS * sizeof(RmReq)), na::PAIRS);
 	for (int k = 0; k < 2; ++k)
 		L.qg[k].bind(take(na::PAIRS * sizeof(GpReq)), na::PAIRS);
-	L.counters.bind(take(16 * sizeof(int)), 16);
+	L.counters.bind(take(32 * sizeof(int)), 32);
 	L.cnt.bind(take(6 * (na::ITEMS + 1) * sizeof(uint32_t)), 6 * (na::ITEMS + 1));
 	L.cub_tmp.bind(take(na::CUB), na::CUB);
 	L.tinfo.bind(take(na::TASKS * sizeof(TaskInfo)), na::TASKS);
@@ -1660,7 +1733,6 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 	L.calls.bind(take(na::PAIRS * LCAP * sizeof(int2)), na::PAIRS * LCAP);
 	L.rq_base.bind(take(na::PAIRS * sizeof(int)), na::PAIRS);
 	L.ssw_out.bind(take(na::CALLS * sizeof(SswOut)), na::CALLS);
-	L.scratch.bind(take(na::H), na::H);
 	L.chain_cap = na::CHAINS;
 	L.job_cap = na::JOBS;
 	L.slot_cap = na::SLOTS;
@@ -1834,4 +1906,92 @@ extern "C" int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, in
 				     hera_candidate **out)
 {
 	return align_dropin(ctx, reads, nullptr, n, write_bam, out);
+}
+
+// ---- DPX throughput probe ----------------------------------------------
+//
+// Eight independent chains of packed 16x2 add-then-min per thread, on
+// 8 resident blocks of 256 threads per SM: the instruction rate that bounds
+// a DP cell update built from __viaddmin_s16x2.
+
+namespace {
+constexpr int DPX_CHAINS = 8;
+
+__global__ void __launch_bounds__(256) k_dpx_peak(const unsigned *__restrict__ seed, int iters,
+						   unsigned *__restrict__ out)
+{
+	const unsigned b = seed[32], c = seed[33];
+	unsigned a[DPX_CHAINS];
+#pragma unroll
+	for (int k = 0; k < DPX_CHAINS; ++k)
+		a[k] = seed[(threadIdx.x + k) & 31];
+	for (int i = 0; i < iters; ++i) {
+#pragma unroll
+		for (int k = 0; k < DPX_CHAINS; ++k)
+			a[k] = __viaddmin_s16x2(a[k], b, c ^ (unsigned)k);
+	}
+	unsigned x = 0;
+#pragma unroll
+	for (int k = 0; k < DPX_CHAINS; ++k)
+		x ^= a[k];
+	out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+}
+}  // namespace
+
+extern "C" int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s)
+{
+	if (!instr_per_s || !(ms > 0))
+		return HERA_GPU_EINVAL;
+	*instr_per_s = 0;
+	if (cudaSetDevice(device) != cudaSuccess)
+		return HERA_GPU_ENODEV;
+	int sms = 0;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+		return HERA_GPU_ENODEV;
+	const int tpb = 256, blocks = sms * 8;
+	unsigned *d = nullptr;
+	const size_t n_out = (size_t)blocks * tpb;
+	if (cudaMalloc(&d, (n_out + 64) * sizeof(unsigned)) != cudaSuccess)
+		return HERA_GPU_ENOMEM;
+	unsigned *seed = d + n_out;
+	unsigned h_seed[64];
+	for (int i = 0; i < 64; ++i)
+		h_seed[i] = 0x00070003u * (unsigned)(i + 1);
+	h_seed[32] = 0x00010001u;   // +1 in both lanes
+	h_seed[33] = 0x7f007f00u;
+	cudaStream_t st = nullptr;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	int rc = HERA_GPU_OK;
+	if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+	    cudaMemcpyAsync(seed, h_seed, sizeof h_seed, cudaMemcpyHostToDevice, st) != cudaSuccess)
+		rc = HERA_GPU_ECUDA;
+	int iters = 1024;
+	float t = 0;
+	for (int pass = 0; pass < 3 && rc == HERA_GPU_OK; ++pass) {
+		cudaEventRecord(e0, st);
+		k_dpx_peak<<<blocks, tpb, 0, st>>>(seed, iters, d);
+		cudaEventRecord(e1, st);
+		if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+			rc = HERA_GPU_ECUDA;
+			break;
+		}
+		cudaEventElapsedTime(&t, e0, e1);
+		if (pass < 2) {   // scale the loop to the requested duration
+			double f = t > 0 ? ms / t : 64.0;
+			f = f < 0.5 ? 0.5 : (f > 64.0 ? 64.0 : f);
+			double ni = iters * f;
+			iters = ni > 1e8 ? 100000000 : (ni < 64 ? 64 : (int)ni);
+		}
+	}
+	if (rc == HERA_GPU_OK && t > 0)
+		*instr_per_s = (double)n_out * iters * DPX_CHAINS / (t * 1e-3);
+	if (e0)
+		cudaEventDestroy(e0);
+	if (e1)
+		cudaEventDestroy(e1);
+	if (st)
+		cudaStreamDestroy(st);
+	cudaFree(d);
+	return rc;
 }

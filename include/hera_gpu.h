@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define HERA_GPU_ABI_VERSION 1
+#define HERA_GPU_ABI_VERSION 2
 
 /* status codes */
 #define HERA_GPU_OK 0
@@ -145,7 +145,8 @@ typedef struct hera_gpu_ctx hera_gpu_ctx;
 typedef struct hera_gpu_options {
 	int device;              /* CUDA device ordinal */
 	uint32_t max_batch;      /* pairs (or single reads) per sub-batch; 0 = 1<<18 */
-	uint64_t scratch_bytes;  /* mate-rescue DP scratch budget; 0 = 2 GiB */
+	uint64_t scratch_bytes;  /* unused (the mate-rescue DP works in shared
+				    memory); kept for layout compatibility */
 	int path;                /* HERA_GPU_PATH_BATCHED (default) or _PLAIN */
 	int lanes;               /* concurrent sub-batches (stream + host thread each); 0 = 3 */
 } hera_gpu_options;
@@ -160,6 +161,19 @@ typedef struct hera_gpu_timing {
 	uint64_t lookups;        /* seed-table lookups issued by seed_probe */
 	uint64_t dp_jobs;        /* batched form: gap-DP jobs run (after deduplication) */
 	uint64_t dp_calls;       /* batched form: SW_align calls those jobs served */
+	/* kernel-level device time (CUDA events around the launches alone) */
+	float seed_kernel_ms;    /* seed_probe: the seed-table gathers */
+	float dp_kernel_ms;      /* batched form: the gap-DP kernels */
+	float rescue_kernel_ms;  /* mate-rescue local SW kernels */
+	/* host time inside the call (summed over lane threads) */
+	float host_stage_ms;     /* copying reads into pinned staging */
+	float host_out_ms;       /* unpacking records into the caller's result */
+	/* work counters (device atomics, one per warp) */
+	uint64_t probes;         /* bucket records read by the binary searches */
+	uint64_t seed_hits;      /* lookups that found their k-mer */
+	uint64_t sw_cells;       /* SW_align cells evaluated, counted the way
+				    src/hash_align.c:659-681 visits them */
+	uint64_t ssw_cells;      /* ssw_align cells: ref_len x read_len per call */
 } hera_gpu_timing;
 
 /* ---- entry points ------------------------------------------------------ */
@@ -228,8 +242,8 @@ int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out);
  * memory while they align: code that runs inside a memory pool it does not
  * own, or where a cudaMalloc would synchronise the device or fail under a
  * hard memory budget.  This call allocates nothing.  Its working memory
- * (the mate-rescue DP's matrix scratch, DP jobs, per-pair state, queues)
- * is one static device array of 33.4 MiB, which every GPU that loads
+ * (mate-rescue outputs, DP jobs, per-pair state, queues) is one static
+ * device array of 17.4 MiB, which every GPU that loads
  * this library holds until the process exits.  The caller passes the reads
  * in device memory (as for hera_gpu_align_pairs_device) and an output in
  * device memory: d_out->recs with room for 2n records and the three pools
@@ -252,6 +266,15 @@ int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint8_t *d_seq,
 
 /* Per-stage timing of the last call on `ctx`. */
 int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out);
+
+/* Measurement helper, no counterpart in hera: the device's throughput of
+ * the DPX instruction the gap DP's cell update is built on (packed 16x2
+ * add-then-min, __viaddmin_s16x2), measured with independent chains on
+ * every SM for about `ms` milliseconds.  *instr_per_s receives thread-level
+ * instructions per second (warp instructions x 32; each one updates two
+ * 16-bit lanes).  Allocates and frees a small output buffer, so it is not
+ * for use inside stream capture. */
+int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s);
 
 /* The context's CUDA stream (a cudaStream_t): the default caller stream of
  * hera_gpu_align_pairs_device, for callers that time or order work around
