@@ -339,6 +339,7 @@ def main():
             log(f"cpu baseline failed: {e}")
 
     st = batched["stage"]
+    tuning = ctx.tuning() if main_path == "batched" else None
     ctx.close()
     ktm = kernel_pass() if main_path == "batched" else None
     dpx = api.dpx_peak(local)
@@ -369,7 +370,7 @@ def main():
             "kernel_ms_per_step": None if ktm is None else {
                 k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
                                                      "rescue_kernel_ms", "resolve_ms", "pack_ms")},
-            "cpu_baseline": cpu, "e2e": e2e,
+            "tuning": tuning, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": batched["launches"], "clocks": batched["clocks"],
         }
         print(json.dumps(line), flush=True)

@@ -67,6 +67,52 @@ class _Reads(C.Structure):
     _fields_ = [("seq", C.c_void_p), ("off", C.c_void_p), ("len", C.c_void_p)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("build_blocks_per_sm", C.c_int), ("rescue_warps_per_block", C.c_int), ("state", C.c_int),
+                ("n_build", C.c_int), ("n_rescue", C.c_int), ("build_cand", C.c_int * 8),
+                ("build_ms", C.c_float * 8), ("rescue_cand", C.c_int * 4), ("rescue_ms", C.c_float * 4)]
+
+    def as_dict(self) -> dict:
+        return {"build_blocks_per_sm": self.build_blocks_per_sm,
+                "rescue_warps_per_block": self.rescue_warps_per_block,
+                "state": ("defaults", "autotuned", "pinned")[self.state],
+                "build_trials_ms": {int(self.build_cand[i]): round(float(self.build_ms[i]), 4)
+                                    for i in range(self.n_build)},
+                "rescue_trials_ms": {int(self.rescue_cand[i]): round(float(self.rescue_ms[i]), 4)
+                                     for i in range(self.n_rescue)}}
+
+
+class _ServerOptions(C.Structure):
+    _fields_ = [("batch_pairs", C.c_uint32), ("max_slots", C.c_int), ("hbm_reserve", C.c_uint64),
+                ("write_bam", C.c_int), ("max_samples", C.c_uint32)]
+
+
+class ChunkInfo(C.Structure):
+    _fields_ = [("sample", C.c_uint32), ("n", C.c_int32), ("submit_ms", C.c_double),
+                ("admit_ms", C.c_double), ("done_ms", C.c_double), ("batches", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SampleStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("pairs", "mapped", "paired", "hits", "cigar_ops")] + [
+        ("reserved", C.c_uint64 * 3)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_[:5]}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("slots", C.c_int), ("slot_bytes", C.c_uint64), ("chunks_done", C.c_uint64),
+                ("pairs_done", C.c_uint64), ("batches", C.c_uint64), ("p50_ms", C.c_float),
+                ("p99_ms", C.c_float), ("p50_wait_ms", C.c_float), ("p99_wait_ms", C.c_float),
+                ("pairs_per_s", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Timing(C.Structure):
     _fields_ = [(k, C.c_float) for k in ("h2d_ms", "seed_ms", "position_ms", "resolve_ms",
                                          "rescue_ms", "pack_ms", "d2h_ms", "total_ms",
@@ -109,6 +155,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_stream.restype = C.c_void_p
     lib.hera_gpu_stream.argtypes = [C.c_void_p]
     lib.hera_gpu_dpx_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double)]
+    lib.hera_gpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    lib.hera_gpu_server_create.argtypes = [C.c_void_p, C.POINTER(_ServerOptions), C.POINTER(C.c_void_p)]
+    lib.hera_gpu_server_submit.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_Reads), C.POINTER(_Reads),
+                                           C.c_int32, C.POINTER(C.c_uint64)]
+    lib.hera_gpu_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(_Result), C.POINTER(ChunkInfo)]
+    lib.hera_gpu_server_get_sample_stats.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(SampleStats)]
+    lib.hera_gpu_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+    lib.hera_gpu_server_destroy.argtypes = [C.c_void_p]
+    lib.hera_gpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
     _lib = lib
     return lib
 
@@ -272,6 +327,88 @@ class Context:
         self.lib.hera_gpu_get_timing(self.h, C.byref(t))
         return t.as_dict()
 
+    def tuning(self) -> dict:
+        """Launch shapes in use and the autotuner's trial timings."""
+        t = Tuning()
+        self._check(self.lib.hera_gpu_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, build_blocks_per_sm: int, rescue_warps_per_block: int) -> None:
+        """Pin the launch shapes (the autotuner then stays off)."""
+        t = Tuning()
+        t.build_blocks_per_sm, t.rescue_warps_per_block = build_blocks_per_sm, rescue_warps_per_block
+        self._check(self.lib.hera_gpu_set_tuning(self.h, C.byref(t)))
+
     @property
     def stream(self) -> int:
         return self.lib.hera_gpu_stream(self.h) or 0
+
+
+class Server:
+    """The serving loop of the C ABI (hera_gpu_server_*): chunks of read
+    pairs from many samples, continuously batched onto device slots sized by
+    free HBM, per-sample counters on the device."""
+
+    def __init__(self, ctx: "Context", batch_pairs: int = 0, max_slots: int = 0, write_bam: int = 1,
+                 max_samples: int = 0, hbm_reserve: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        opt = _ServerOptions(batch_pairs, max_slots, hbm_reserve, write_bam, max_samples)
+        h = C.c_void_p()
+        ctx._check(self.lib.hera_gpu_server_create(ctx.h, C.byref(opt), C.byref(h)))
+        self.h = h
+        self._sizes = {}
+
+    def submit(self, sample: int, r1, r2) -> int:
+        """Queue the pairs (r1[i], r2[i]) of `sample`; returns a ticket."""
+        a, b = Context._reads(r1), Context._reads(r2)
+        t = C.c_uint64()
+        self.ctx._check(self.lib.hera_gpu_server_submit(self.h, sample, C.byref(a), C.byref(b), r1.n,
+                                                        C.byref(t)))
+        self._sizes[t.value] = (r1.n, int(r1.len.sum()) + int(r2.len.sum()))
+        return t.value
+
+    def wait(self, ticket: int):
+        """(Result, info) of a chunk, blocking until it is done."""
+        n, total_len = self._sizes.pop(ticket)
+        res = Result(2 * n, 8 * n + 1024, 8 * n + 1024, total_len // 8 + 1024)
+        info = ChunkInfo()
+        rc = self.lib.hera_gpu_server_wait(self.h, ticket, C.byref(res.c), C.byref(info))
+        if rc == -5 and (res.c.list_used > res.c.list_cap or res.c.op_used > res.c.op_cap
+                         or res.c.miss_used > res.c.miss_cap):
+            res._alloc(res.c.list_used + 1, res.c.op_used + 1, res.c.miss_used + 1)
+            rc = self.lib.hera_gpu_server_wait(self.h, ticket, C.byref(res.c), C.byref(info))
+        self.ctx._check(rc)
+        return res, info.as_dict()
+
+    def sample_stats(self, sample: int) -> dict:
+        st = SampleStats()
+        self.ctx._check(self.lib.hera_gpu_server_get_sample_stats(self.h, sample, C.byref(st)))
+        return st.as_dict()
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self.ctx._check(self.lib.hera_gpu_server_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hera_gpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tally(res: Result) -> dict:
+    """The per-sample counters the server keeps on the device, computed on
+    the host from one chunk's records (for checking)."""
+    r = res.recs
+    a, b = r[0::2], r[1::2]
+    hits = a["n"].sum(axis=1).astype(np.int64) + b["n"].sum(axis=1)
+    return {"pairs": int(a.shape[0]), "mapped": int((hits > 0).sum()), "paired": int((a["pair"] == 2).sum()),
+            "hits": int(hits.sum()),
+            "cigar_ops": int(a["n_cigar"].astype(np.int64).sum() + b["n_cigar"].astype(np.int64).sum())}

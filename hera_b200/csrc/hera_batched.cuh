@@ -225,16 +225,11 @@ struct BuildWork {
 	DpJob jb[LJ];
 };
 
-__global__ void __launch_bounds__(128) k_build(Batch b, Round R)
+// one get_position call of the round (list position t)
+__device__ void build_one(const Batch &b, const Round &R, int t)
 {
-	int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (R.list) {
-		if (t >= *R.nlist)
-			return;
+	if (R.list)
 		t = R.list[t];
-	} else if (t >= R.ntask) {
-		return;
-	}
 	int pi, c, str;
 	task_of(R, t, pi, c, str);
 	DPair &P = b.P[pi];
@@ -392,6 +387,25 @@ __global__ void __launch_bounds__(128) k_build(Batch b, Round R)
 	flag(b.flags, flags);
 }
 
+// Persistent work-queue form: a grid of a few blocks per SM (the residency
+// the autotuner picked) whose warps take the round's calls 32 at a time
+// from `queue`; a warp held up by a heavy call delays only its own 32.
+__global__ void __launch_bounds__(128) k_build(Batch b, Round R, int *__restrict__ queue)
+{
+	const int n = R.list ? *R.nlist : R.ntask;
+	const int lane = threadIdx.x & 31;
+	for (;;) {
+		int base = 0;
+		if (lane == 0)
+			base = atomicAdd(queue, 32);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (base >= n)
+			break;
+		if (base + lane < n)
+			build_one(b, R, base + lane);
+	}
+}
+
 __device__ __forceinline__ int job_bin(const DpJob &j)
 {
 	const int e = j.err < 0 ? -j.err : j.err;
@@ -508,18 +522,20 @@ __device__ __forceinline__ int job_form(const DpJob &j)
 }
 
 // one thread per job, jobs in (error cap, length) order; threads whose job
-// is not of cap E leave at once (whole warps, the order is by cap)
+// is not of cap E leave at once (whole warps, the order is by cap).  In the
+// score-only mode the pass keeps no rows; a job whose DP stops early (the
+// shrink loop needs its rows) is queued on `redo` for k_dp_redo, so the
+// warps here stay converged.
 template <int E>
 __global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
-	 int rcap)
+	 int rcap, int *__restrict__ redo, int *__restrict__ n_redo)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t cells = 0;
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
 		const DpJob jb = jobs[id];
-		__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
 		DCig cig;
 		int flags = 0;
 		cig.n = cig.nm = 0;
@@ -527,12 +543,55 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
 		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
 		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-		const int score =
-			sw_align_fast<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, cells);
-		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-		flag(b.flags, flags);
+		int score;
+		if (b.score_only) {
+			score = sw_align_reg<E, false>(r, qv, jb.ref_len, jb.len, true, cig, nullptr, flags, cells);
+			if (score < 0) {
+				redo[atomicAdd(n_redo, 1)] = id;
+				cells = 0;   // counted by the rerun
+			}
+		} else {
+			__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
+			score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, false, cig, rows, flags, cells);
+		}
+		if (score >= 0) {
+			store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+			flag(b.flags, flags);
+		}
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
+}
+
+// the score-only jobs of cap E whose DP stopped early, rerun with the rows
+// kept (grid-stride over the device-side count)
+template <int E>
+__global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
+k_dp_redo(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ redo, const int *__restrict__ n_redo,
+	  uint8_t *__restrict__ res, int rcap)
+{
+	const int n = *n_redo;
+	const int span = gridDim.x * blockDim.x;
+	const int rounds = (n + span - 1) / span;   // every lane of a warp runs as many rounds
+	for (int k = 0; k < rounds; ++k) {
+		const int t = blockIdx.x * blockDim.x + threadIdx.x + k * span;
+		uint32_t cells = 0;
+		if (t < n) {
+			const int id = redo[t];
+			const DpJob jb = jobs[id];
+			__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
+			DCig cig;
+			int flags = 0;
+			cig.n = cig.nm = 0;
+			const bool rev = jb.err < 0;
+			const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+			RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
+			QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
+			const int score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, true, cig, rows, flags, cells);
+			store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+			flag(b.flags, flags);
+		}
+		warp_stat(b.stats + ST_SW_CELLS, cells);
+	}
 }
 
 // the jobs outside the register form (empty gaps, spill cases)

@@ -562,29 +562,6 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 	}
 }
 
-// Register-form SW_align: a forward pass without row storage first (enough
-// for the score-only mode unless the DP stops early); otherwise rerun with
-// the rows kept for the shrink loop and the traceback.
-template <int E>
-__device__ inline int sw_align_fast(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
-				    bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags,
-				    uint32_t &n_cells)
-{
-	uint32_t cells = 0;
-	if (score_only) {
-		const int sc = sw_align_reg<E, false>(r, qc, ref_len, len, true, cig, rows, flags, cells);
-		if (sc >= 0) {
-			n_cells += cells;
-			return sc;
-		}
-		cig.n = cig.nm = 0;
-		cells = 0;
-	}
-	const int sc = sw_align_reg<E, true>(r, qc, ref_len, len, score_only, cig, rows, flags, cells);
-	n_cells += cells;
-	return sc;
-}
-
 // Entry used by the per-task (plain) path: the banded form, which keeps the
 // register footprint small where neighbouring threads diverge.  The batched
 // path runs sw_align_reg on length-sorted jobs instead.  q: oriented read

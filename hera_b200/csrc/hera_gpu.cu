@@ -314,7 +314,7 @@ __global__ void k_rescue_expand(Batch b, const RmReq *__restrict__ q, int nq, in
 
 // 2) one warp per call: local SW over the MAX_FRAG window at the mate hit;
 // each warp works in its own `per` bytes of the block's shared memory
-constexpr int RESCUE_TPB = 128;
+constexpr int RESCUE_TPB = 256;   // at most 8 calls (warps) per block
 __global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *__restrict__ q,
 							   const int2 *__restrict__ calls, int c0, int nc,
 							   SswOut *__restrict__ out, int per)
@@ -585,7 +585,7 @@ struct Lane {
 	DBuf<JobSlot> slots;
 	DBuf<DpJob> jobs;
 	DBuf<uint8_t> res;
-	DBuf<int> perm, hist, tlist;
+	DBuf<int> perm, hist, tlist, redo;
 	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
 	DBuf<hera_cand_rec> recs;
 	DBuf<uint32_t> pos_pool, op_pool;
@@ -611,7 +611,7 @@ struct Lane {
 		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
 		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release();
 		calls.release(); rq_base.release(); ssw_out.release(); tinfo.release(); chains.release();
-		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
+		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release(); redo.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
 		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
@@ -642,7 +642,38 @@ struct hera_gpu_ctx {
 	// device-resident results of the last hera_gpu_align_pairs_device call:
 	// sub-batch k is held by lane k
 	int nparts = 0;
+	// launch shapes (autotuned on the first large batch, or set by the caller)
+	int sms = 148;
+	std::mutex tune_mu;
+	hera_gpu_tuning tune{};
+	int build_tuning = 0, rescue_tuning = 0;   // 0 open, 1 claimed by a lane, 2 done
 };
+
+// candidate launch shapes the autotuner times
+static const int BUILD_BPS[] = {2, 4, 6, 8, 12, 16};
+static const int RESCUE_WPB[] = {2, 4, 8};
+
+static int tuned_build_bps(hera_gpu_ctx *ctx)
+{
+	std::lock_guard<std::mutex> g(ctx->tune_mu);
+	return ctx->tune.build_blocks_per_sm;
+}
+
+static int tuned_rescue_wpb(hera_gpu_ctx *ctx)
+{
+	std::lock_guard<std::mutex> g(ctx->tune_mu);
+	return ctx->tune.rescue_warps_per_block;
+}
+
+// true for the one lane that gets to tune `what` (its flag goes to 1)
+static bool claim_tuning(hera_gpu_ctx *ctx, int &flag)
+{
+	std::lock_guard<std::mutex> g(ctx->tune_mu);
+	if (ctx->tune.state == 2 || flag != 0)
+		return false;
+	flag = 1;
+	return true;
+}
 
 static int set_err(std::string &dst, int code, const char *what, cudaError_t e = cudaSuccess)
 {
@@ -689,6 +720,29 @@ extern "C" const char *hera_gpu_last_error(const hera_gpu_ctx *ctx)
 extern "C" void *hera_gpu_stream(hera_gpu_ctx *ctx)
 {
 	return ctx ? (void *)ctx->stream : nullptr;
+}
+
+extern "C" int hera_gpu_get_tuning(const hera_gpu_ctx *ctx, hera_gpu_tuning *out)
+{
+	if (!ctx || !out)
+		return HERA_GPU_EINVAL;
+	std::lock_guard<std::mutex> g(const_cast<hera_gpu_ctx *>(ctx)->tune_mu);
+	*out = ctx->tune;
+	return HERA_GPU_OK;
+}
+
+extern "C" int hera_gpu_set_tuning(hera_gpu_ctx *ctx, const hera_gpu_tuning *in)
+{
+	if (!ctx || !in)
+		return HERA_GPU_EINVAL;
+	const int w = in->rescue_warps_per_block;
+	if (in->build_blocks_per_sm < 1 || in->build_blocks_per_sm > 16 || !(w == 1 || w == 2 || w == 4 || w == 8))
+		return fail(ctx, HERA_GPU_EINVAL, "tuning values out of range");
+	std::lock_guard<std::mutex> g(ctx->tune_mu);
+	ctx->tune.build_blocks_per_sm = in->build_blocks_per_sm;
+	ctx->tune.rescue_warps_per_block = w;
+	ctx->tune.state = 2;
+	return HERA_GPU_OK;
 }
 
 extern "C" int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out)
@@ -757,10 +811,15 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		return bail(HERA_GPU_ENODEV);
 	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
-	// the rescue kernel's per-warp shared-memory areas (up to ~89 KiB a block)
+	// the rescue kernel's per-warp shared-memory areas (up to ~177 KiB a block)
 	if (cudaFuncSetAttribute(k_rescue_sw, cudaFuncAttributeMaxDynamicSharedMemorySize,
 				 (int)((RESCUE_TPB / 32) * ssw_smem_per_warp(MAX_READ))) != cudaSuccess)
 		return bail(fail(ctx, HERA_GPU_ECUDA, "rescue kernel shared-memory size"));
+	if (cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess ||
+	    ctx->sms <= 0)
+		return bail(fail(ctx, HERA_GPU_ECUDA, "SM count"));
+	ctx->tune.build_blocks_per_sm = 8;
+	ctx->tune.rescue_warps_per_block = 4;
 	for (int i = 0; i < nlanes; ++i) {
 		Lane *L = new Lane();
 		ctx->lanes.push_back(L);
@@ -836,7 +895,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 // ---- pipeline pieces --------------------------------------------------
 
 // one rescue round (re_mapSW for every queued request)
-static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq *q, int nq,
+static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq *q, int nq,
 			int max_len, uint32_t &launches, float &ms_acc)
 {
 	cudaStream_t st = L.stream;
@@ -853,12 +912,43 @@ static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const 
 	const int ncalls = L.h_small.p[1];
 	LK(L.ssw_out.ensure(ncalls + 1), "rescue outputs");
 	const int per = (int)ssw_smem_per_warp(max_len);
-	cudaEventRecord(L.ev[10], st);
-	if (ncalls > 0) {
-		k_rescue_sw<<<blocks_for((int64_t)ncalls * 32, RESCUE_TPB), RESCUE_TPB, (RESCUE_TPB / 32) * per, st>>>(
+	auto launch = [&](int wpb) {
+		k_rescue_sw<<<blocks_for((int64_t)ncalls * 32, 32 * wpb), 32 * wpb, wpb * per, st>>>(
 			b, q, L.calls.p, 0, ncalls, L.ssw_out.p, per);
 		++launches;
+	};
+	// autotune: the first large rescue round times each candidate (every
+	// run writes the same outputs)
+	if (ncalls >= 2048 && claim_tuning(ctx, ctx->rescue_tuning)) {
+		int best = 0;
+		float best_ms = 0;
+		int nc = 0;
+		for (int wpb : RESCUE_WPB) {
+			cudaEventRecord(L.ev[10], st);
+			launch(wpb);
+			cudaEventRecord(L.ev[11], st);
+			LK(cudaEventSynchronize(L.ev[11]), "rescue tuning");
+			float ms = 0;
+			cudaEventElapsedTime(&ms, L.ev[10], L.ev[11]);
+			if (!best || ms < best_ms) {
+				best = wpb;
+				best_ms = ms;
+			}
+			std::lock_guard<std::mutex> g(ctx->tune_mu);
+			ctx->tune.rescue_cand[nc] = wpb;
+			ctx->tune.rescue_ms[nc] = ms;
+			ctx->tune.n_rescue = ++nc;
+		}
+		std::lock_guard<std::mutex> g(ctx->tune_mu);
+		if (ctx->tune.state != 2) {
+			ctx->tune.rescue_warps_per_block = best;
+			ctx->tune.state = 1;
+		}
+		ctx->rescue_tuning = 2;
 	}
+	cudaEventRecord(L.ev[10], st);
+	if (ncalls > 0)
+		launch(tuned_rescue_wpb(ctx));
 	cudaEventRecord(L.ev[11], st);
 	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.rq_base.p, L.ssw_out.p);
 	++launches;
@@ -873,7 +963,7 @@ static int rescue_round(const hera_gpu_ctx *ctx, Lane &L, const Batch &b, const 
 }
 
 // one round of batched get_position calls: build, bin, DP, replay
-static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float &build_ms, float &dp_ms)
+static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_t &launches, float &build_ms, float &dp_ms)
 {
 	if (R.ntask <= 0)
 		return HERA_GPU_OK;
@@ -911,9 +1001,45 @@ static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float 
 		R.chain_cap = (int)L.chain_cap;
 		R.job_cap = (int)L.job_cap;
 		R.slot_cap = (int)L.slot_cap;
-		LK(cudaMemsetAsync(d_cnt, 0, 3 * sizeof(int), st), "memset");
-		k_build<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
-		++launches;
+		int *d_queue = L.counters.p + 26;
+		auto launch = [&](int bps) {
+			cudaMemsetAsync(d_cnt, 0, 3 * sizeof(int), st);
+			cudaMemsetAsync(d_queue, 0, sizeof(int), st);
+			unsigned grid = (unsigned)(ctx->sms * bps);
+			const unsigned need = blocks_for(R.ntask);
+			k_build<<<grid < need ? grid : need, 128, 0, st>>>(b, R, d_queue);
+			++launches;
+		};
+		// autotune the persistent build kernel's residency on the first
+		// large round 0 (every run writes the same chains and jobs)
+		if (!R.req && R.ntask >= 4 * 16384 && claim_tuning(ctx, ctx->build_tuning)) {
+			int best = 0, nc = 0;
+			float best_ms = 0;
+			for (int bps : BUILD_BPS) {
+				cudaEventRecord(L.ev[8], st);
+				launch(bps);
+				cudaEventRecord(L.ev[9], st);
+				LK(cudaEventSynchronize(L.ev[9]), "build tuning");
+				float ms = 0;
+				cudaEventElapsedTime(&ms, L.ev[8], L.ev[9]);
+				if (!best || ms < best_ms) {
+					best = bps;
+					best_ms = ms;
+				}
+				std::lock_guard<std::mutex> g(ctx->tune_mu);
+				ctx->tune.build_cand[nc] = bps;
+				ctx->tune.build_ms[nc] = ms;
+				ctx->tune.n_build = ++nc;
+			}
+			std::lock_guard<std::mutex> g(ctx->tune_mu);
+			if (ctx->tune.state != 2) {
+				ctx->tune.build_blocks_per_sm = best;
+				ctx->tune.state = 1;
+			}
+			ctx->build_tuning = 2;
+		}
+		launch(tuned_build_bps(ctx));
+		LK(cudaGetLastError(), "build launch");
 		LK(cudaMemcpyAsync(L.h_small.p + 12, d_cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
 		LK(cudaStreamSynchronize(st), "build");
 		nch = L.h_small.p[12];
@@ -944,12 +1070,19 @@ static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float 
 		k_bin_count<<<148, 512, 0, st>>>(L.jobs.p, nj, L.hist.p);
 		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
 		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
+		LK(L.redo.ensure(2 * (size_t)nj), "dp reruns");
+		int *d_redo = L.counters.p + 24;   // [0] cap 4, [1] cap 8
+		LK(cudaMemsetAsync(d_redo, 0, 2 * sizeof(int), st), "memset");
+		const unsigned redo_grid = blocks_for(nj) < 148u * 6 ? blocks_for(nj) : 148u * 6;
 		cudaEventRecord(L.ev[10], st);
-		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
-		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap, L.redo.p, d_redo);
+		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap, L.redo.p + nj,
+							     d_redo + 1);
+		k_dp_redo<4><<<redo_grid, 128, 0, st>>>(b, L.jobs.p, L.redo.p, d_redo, L.res.p, rcap);
+		k_dp_redo<8><<<redo_grid, 128, 0, st>>>(b, L.jobs.p, L.redo.p + nj, d_redo + 1, L.res.p, rcap);
 		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
 		cudaEventRecord(L.ev[11], st);
-		launches += 6;
+		launches += 8;
 		R.res = L.res.p;
 	}
 	k_replay<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
@@ -970,7 +1103,7 @@ static int gp_round(Lane &L, const Batch &b, Round R, uint32_t &launches, float 
 // seq_bytes bytes, d_off/d_len are lane-local (offsets into d_seq), 2n
 // reads for pairs (mates interleaved), n for singles.  Leaves the packed
 // records in L's device pools and their sizes in L.items/nl/no/nm.
-static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int64_t *d_off,
+static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int64_t *d_off,
 		     const int32_t *d_len, int32_t n, bool paired, int write_bam, int max_len,
 		     int64_t seq_bytes)
 {
@@ -1077,7 +1210,7 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 		R.space = KMER;
 		R.hits = L.hits.p;
 		R.spr = spr;
-		int rc = gp_round(L, b, R, launches, build_ms, dp_ms);
+		int rc = gp_round(ctx, L, b, R, launches, build_ms, dp_ms);
 		if (rc)
 			return rc;
 		cudaEventRecord(L.ev[3], st);
@@ -1108,7 +1241,7 @@ static int run_batch(const hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, con
 				G.req = L.qg[qi].p;
 				G.ntask = ng;
 				G.space = 2 * ERR;
-				rc = gp_round(L, b, G, launches, build_ms, dp_ms);
+				rc = gp_round(ctx, L, b, G, launches, build_ms, dp_ms);
 				if (rc)
 					return rc;
 			}
@@ -1642,7 +1775,7 @@ constexpr size_t BYTES =
 	2 * A(PAIRS * sizeof(RmReq)) + 2 * A(PAIRS * sizeof(GpReq)) + A(32 * sizeof(int)) +
 	A(6 * (ITEMS + 1) * sizeof(uint32_t)) + A(CUB) + A(TASKS * sizeof(TaskInfo)) + A(TASKS * sizeof(int)) +
 	A(CHAINS * sizeof(Chain)) + A(JOBS * sizeof(DpJob)) + A(SLOTS * sizeof(JobSlot)) +
-	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
+	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(2 * JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
 	A(PAIRS * LCAP * sizeof(int2)) + A(PAIRS * sizeof(int)) + A(CALLS * sizeof(SswOut));
 }  // namespace na
 
@@ -1729,6 +1862,7 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 	L.slots.bind(take(na::SLOTS * sizeof(JobSlot)), na::SLOTS);
 	L.res.bind(take(na::JOBS * (size_t)res_stride(JCAP)), na::JOBS * (size_t)res_stride(JCAP));
 	L.perm.bind(take(na::JOBS * sizeof(int)), na::JOBS);
+	L.redo.bind(take(2 * na::JOBS * sizeof(int)), 2 * na::JOBS);
 	L.hist.bind(take(NBIN * sizeof(int)), NBIN);
 	L.calls.bind(take(na::PAIRS * LCAP * sizeof(int2)), na::PAIRS * LCAP);
 	L.rq_base.bind(take(na::PAIRS * sizeof(int)), na::PAIRS);
@@ -1995,3 +2129,5 @@ extern "C" int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s)
 	cudaFree(d);
 	return rc;
 }
+
+#include "hera_server.cuh"

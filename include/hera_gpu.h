@@ -267,6 +267,106 @@ int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint8_t *d_seq,
 /* Per-stage timing of the last call on `ctx`. */
 int hera_gpu_get_timing(const hera_gpu_ctx *ctx, hera_gpu_timing *out);
 
+/* Launch shapes of the batched form, no counterpart in hera.  The library
+ * times the candidates on a context's first large batch (at least 16384
+ * pairs) and keeps the fastest: the residency of the persistent build
+ * kernel (blocks per SM: more blocks hide more gather latency, fewer keep
+ * each thread's anchor and chain lists in cache) and the number of
+ * mate-rescue calls (warps) per block (shared-memory areas per SM).
+ * Results do not depend on these values. */
+typedef struct hera_gpu_tuning {
+	int build_blocks_per_sm;     /* default 8 until tuned */
+	int rescue_warps_per_block;  /* default 4 until tuned */
+	int state;                   /* 0 defaults, 1 tuned by the library, 2 set by the caller */
+	int n_build, n_rescue;       /* candidates timed */
+	int build_cand[8];
+	float build_ms[8];           /* build kernel time per candidate (one launch) */
+	int rescue_cand[4];
+	float rescue_ms[4];          /* rescue kernel time per candidate (one launch) */
+} hera_gpu_tuning;
+
+/* The context's launch shapes and, once tuned, the timings they came from. */
+int hera_gpu_get_tuning(const hera_gpu_ctx *ctx, hera_gpu_tuning *out);
+
+/* Pin the launch shapes (state becomes 2; the autotuner no longer runs).
+ * build_blocks_per_sm in 1..16, rescue_warps_per_block in {1, 2, 4, 8}. */
+int hera_gpu_set_tuning(hera_gpu_ctx *ctx, const hera_gpu_tuning *in);
+
+/* ---- serving loop (no counterpart in hera) ----------------------------- *
+ *
+ * hera aligns one sample per process.  The server keeps one context's index
+ * resident and aligns FASTQ chunks (read pairs) of many samples as they
+ * arrive.  Continuous batching: a device batch is cut from the head of the
+ * pending chunks whenever a batch slot frees up, so a batch may hold the
+ * tail of one sample's chunk and the head of another's, and chunks that
+ * arrive while others run join the next batch instead of waiting for a
+ * whole queue to drain.  Slots run concurrently (stream + host thread each);
+ * their number is fixed at creation from the free device memory.  Every
+ * chunk's records are exactly those hera_gpu_align_pairs_flat returns for
+ * it alone.  Per-sample counters are kept on the device. */
+typedef struct hera_gpu_server hera_gpu_server;
+
+typedef struct hera_gpu_server_options {
+	uint32_t batch_pairs;    /* pairs per device batch; 0 = 131072 */
+	int max_slots;           /* batches in flight at most; 0 = 6 */
+	uint64_t hbm_reserve;    /* device bytes to leave free; 0 = 4 GiB */
+	int write_bam;           /* hera's WRITE_BAM for every chunk */
+	uint32_t max_samples;    /* per-sample state slots; 0 = 1024 */
+} hera_gpu_server_options;
+
+typedef struct hera_gpu_chunk_info {
+	uint32_t sample;
+	int32_t n;               /* pairs */
+	double submit_ms;        /* server clock (ms since creation) */
+	double admit_ms;         /* first pair of the chunk entered a batch */
+	double done_ms;          /* last pair's records were on the host */
+	int32_t batches;         /* device batches the chunk was spread over */
+} hera_gpu_chunk_info;
+
+typedef struct hera_gpu_sample_stats {   /* kept on the device, per sample */
+	uint64_t pairs;          /* pairs aligned */
+	uint64_t mapped;         /* pairs with a hit for at least one mate */
+	uint64_t paired;         /* pairs whose r[0].pair == 2 (mates agree) */
+	uint64_t hits;           /* sum of n[0] + n[1] over both Candidates */
+	uint64_t cigar_ops;      /* sum of CIGAR ops over both Candidates */
+	uint64_t reserved[3];
+} hera_gpu_sample_stats;
+
+typedef struct hera_gpu_server_stats {
+	int slots;               /* batch slots (from free device memory) */
+	uint64_t slot_bytes;     /* device bytes budgeted per slot */
+	uint64_t chunks_done, pairs_done, batches;
+	float p50_ms, p99_ms;    /* chunk latency: submit to done */
+	float p50_wait_ms, p99_wait_ms;   /* submit to admission */
+	double pairs_per_s;      /* pairs_done / (last done - first submit) */
+} hera_gpu_server_stats;
+
+/* Start a server on `ctx` (the context must outlive it; do not run other
+ * calls on `ctx` while the server is alive).  `opt` may be NULL. */
+int hera_gpu_server_create(hera_gpu_ctx *ctx, const hera_gpu_server_options *opt,
+			   hera_gpu_server **out);
+
+/* Queue n pairs of `sample` (< max_samples).  The reads are copied, so the
+ * caller's buffers are free on return.  *ticket identifies the chunk. */
+int hera_gpu_server_submit(hera_gpu_server *s, uint32_t sample, const hera_gpu_reads *r1,
+			   const hera_gpu_reads *r2, int32_t n, uint64_t *ticket);
+
+/* Block until the chunk is done and copy its records into `out` (layout as
+ * hera_gpu_align_pairs_flat); the chunk is then released.  If a pool of
+ * `out` is too small, returns HERA_GPU_ECAPACITY with *_used set and keeps
+ * the chunk for another try.  One wait per ticket at a time (a second
+ * concurrent wait fails with HERA_GPU_EINVAL).  `info` may be NULL. */
+int hera_gpu_server_wait(hera_gpu_server *s, uint64_t ticket, hera_gpu_result *out,
+			 hera_gpu_chunk_info *info);
+
+/* Per-sample counters (read from the device) and server-wide figures. */
+int hera_gpu_server_get_sample_stats(hera_gpu_server *s, uint32_t sample, hera_gpu_sample_stats *out);
+int hera_gpu_server_get_stats(hera_gpu_server *s, hera_gpu_server_stats *out);
+
+/* Stop the slots after the batches in flight and free everything; chunks
+ * not yet waited for are dropped. */
+void hera_gpu_server_destroy(hera_gpu_server *s);
+
 /* Measurement helper, no counterpart in hera: the device's throughput of
  * the DPX instruction the gap DP's cell update is built on (packed 16x2
  * add-then-min, __viaddmin_s16x2), measured with independent chains on

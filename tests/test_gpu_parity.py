@@ -162,3 +162,46 @@ def test_dropin_candidate_entry(config1, oracle1, gpu_ctx1):
                             tuple(c.p[s][j] for j in range(k)), cig, miss))
         assert (c.pair, tuple(strands)) == o[i], i
     assert bufs[0].value.upper() == bufs[0].value
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (16, 8), (3, 2)])
+def test_launch_shapes_do_not_change_results(config1, oracle1, shape):
+    """The autotuner's choices (build residency, rescue calls per block) only
+    change speed: pinned extreme shapes give the oracle's records."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ann, tx, ix = config1
+    ctx = api.Context(ix, max_batch=1 << 16)
+    try:
+        ctx.set_tuning(*shape)
+        r1, r2 = workloads.pairs("config4", ann, tx, 6000, seed=31)
+        _assert_same(ctx.align_pairs(r1, r2, 0), oracle1.align_pairs(r1.copy(), r2.copy(), 0),
+                     f"shape {shape}")
+        t = ctx.tuning()
+        assert t["state"] == "pinned"
+        assert (t["build_blocks_per_sm"], t["rescue_warps_per_block"]) == shape
+    finally:
+        ctx.close()
+
+
+def test_autotuner_picks_a_timed_candidate(config1, oracle1):
+    """A batch of at least 16384 pairs on one lane makes the context time
+    every build-residency candidate and keep the fastest; results stay the
+    oracle's."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ann, tx, ix = config1
+    ctx = api.Context(ix, max_batch=1 << 16, lanes=1)
+    try:
+        assert ctx.tuning()["state"] == "defaults"
+        r1, r2 = workloads.pairs("config1", ann, tx, 20000, seed=32)
+        _assert_same(ctx.align_pairs(r1, r2, 1), oracle1.align_pairs(r1.copy(), r2.copy(), 1), "tuned")
+        t = ctx.tuning()
+        assert t["state"] == "autotuned"
+        trials = t["build_trials_ms"]
+        assert len(trials) >= 4 and all(v > 0 for v in trials.values())
+        assert t["build_blocks_per_sm"] == min(trials, key=trials.get)
+    finally:
+        ctx.close()
