@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--paths", default="plain,batched", help="execution forms to time (batched last)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent sub-batches (0 = library default)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--serve-scale", type=float, default=0.125,
+                    help="sample sizes of the serving leg as a fraction of 0.5M-8M pairs")
     return ap.parse_args()
 
 
@@ -346,6 +349,14 @@ def main():
     pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
     roof, roof_seed, roof_rescue = roofline(ktm, dpx, args, pair_bytes, max_len)
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        try:
+            serving = serve_bench(args, local)
+        except Exception as e:
+            log(f"serving leg failed: {e}")
+            serving = {"error": str(e)}
+
     if rank == 0:
         per = sorted(batched["per_step_ms"])
         line = {
@@ -370,12 +381,119 @@ def main():
             "kernel_ms_per_step": None if ktm is None else {
                 k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
                                                      "rescue_kernel_ms", "resolve_ms", "pack_ms")},
-            "tuning": tuning, "cpu_baseline": cpu, "e2e": e2e,
+            "tuning": tuning, "serving": serving, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": batched["launches"], "clocks": batched["clocks"],
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def serve_bench(args, local):
+    """The serving loop on the config-5 shape: the config-1 index resident,
+    64 samples of log-uniform 0.5M-8M pairs (times --serve-scale), read
+    lengths 75-150 bp, arriving as 131072-pair (256k-read) chunks by a
+    Poisson process at 1.5x the plain path's measured capacity."""
+    import types
+    from hera_b200 import api, synth, workloads
+    ann, tx, ix = workloads.build("config1")
+    CH = 131072
+    pool = []   # one chunk per read length; chunks of a sample reuse its pool chunk
+    for k, L in enumerate((75, 100, 125, 150)):
+        pool.append(synth.simulate_pairs(tx, CH, seed=500 + k, read_len=L, frag_mu=max(250.0, 2.5 * L),
+                                         frag_sd=25.0, sub_rate=0.005, indel_rate=0.0001))
+    # the plain path's capacity, host buffers in and out like the server's
+    pctx = api.Context(ix, device=local, path="plain")
+    pctx.align_pairs(*pool[1])
+    t = time.perf_counter()
+    for r1, r2 in pool:
+        pctx.align_pairs(r1, r2)
+    plain = len(pool) * CH / (time.perf_counter() - t)
+    pctx.close()
+    rate = 1.5 * plain
+    rng = np.random.default_rng(55)
+    sizes = np.exp(rng.uniform(np.log(5e5), np.log(8e6), 64)) * args.serve_scale
+    sizes = np.maximum(sizes.astype(np.int64), 1)
+    rlen = rng.integers(0, 4, 64)
+    plan = []   # (sample, n) in arrival order: samples interleaved
+    left = sizes.copy()
+    while left.sum() > 0:
+        for s in rng.permutation(64):
+            if left[s] > 0:
+                n = int(min(CH, left[s]))
+                plan.append((int(s), n))
+                left[s] -= n
+    gaps = rng.exponential(1.0, len(plan))
+    gaps *= np.array([n for _, n in plan]) / rate   # mean gap = chunk size / rate
+    ctx = api.Context(ix, device=local)
+    srv = api.Server(ctx, batch_pairs=CH, write_bam=args.write_bam, max_samples=64)
+    # warm the slots (buffers at the longest reads, autotuner) before the clock
+    warm = [srv.submit(0, *pool[3]) for _ in range(2 * srv.stats()["slots"])]
+    for tk in warm:
+        srv.wait(tk)
+    # capacity: the whole plan submitted at once
+    t = time.perf_counter()
+    sat = []
+    for s, n in plan:
+        r1, r2 = pool[rlen[s]]
+        if n < CH:
+            r1 = types.SimpleNamespace(n=n, seq=r1.seq, off=r1.off[:n], len=r1.len[:n])
+            r2 = types.SimpleNamespace(n=n, seq=r2.seq, off=r2.off[:n], len=r2.len[:n])
+        sat.append(srv.submit(s, r1, r2))
+    for tk in sat:
+        srv.wait(tk)
+    capacity = float(sizes.sum()) / (time.perf_counter() - t)
+    tickets, infos = [], []
+    lock = threading.Lock()
+    done = threading.Event()
+
+    def feed():
+        t0 = time.perf_counter()
+        due = 0.0
+        for (s, n), g in zip(plan, gaps):
+            due += g
+            d = due - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            r1, r2 = pool[rlen[s]]
+            if n < CH:
+                r1 = types.SimpleNamespace(n=n, seq=r1.seq, off=r1.off[:n], len=r1.len[:n])
+                r2 = types.SimpleNamespace(n=n, seq=r2.seq, off=r2.off[:n], len=r2.len[:n])
+            tk = srv.submit(s, r1, r2)
+            with lock:
+                tickets.append(tk)
+        done.set()
+
+    th = threading.Thread(target=feed)
+    t0 = time.perf_counter()
+    th.start()
+    k = 0
+    while True:
+        with lock:
+            tk = tickets[k] if k < len(tickets) else None
+        if tk is None:
+            if done.is_set() and k >= len(tickets):
+                break
+            time.sleep(0.0005)
+            continue
+        infos.append(srv.wait(tk)[1])
+        k += 1
+    th.join()
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+    wt = np.array([i["admit_ms"] - i["submit_ms"] for i in infos])
+    span_s = (max(i["done_ms"] for i in infos) - min(i["submit_ms"] for i in infos)) / 1e3
+    return {"workload": "config5 shape: config1 index, 64 samples of log-uniform 0.5M-8M pairs x "
+                        f"{args.serve_scale}, 75-150 bp, 131072-pair chunks, Poisson arrivals",
+            "samples": 64, "chunks": len(plan), "pairs": int(sizes.sum()),
+            "plain_pairs_per_s": plain, "arrival_pairs_per_s": rate, "capacity_pairs_per_s": capacity,
+            "sustained_pairs_per_s": float(sizes.sum()) / span_s, "wall_s": wall,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p50_wait_ms": float(np.percentile(wt, 50)), "p99_wait_ms": float(np.percentile(wt, 99)),
+            "slots": st["slots"], "batches": st["batches"], "batch_pairs": CH}
 
 
 def roofline(tm, dpx_instr_s, args, read_bytes, max_len):
