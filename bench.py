@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--paths", default="plain,batched", help="execution forms to time (batched last)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent sub-batches (0 = library default)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--pin-tuning", default="", help="BUILD_BLOCKS_PER_SM,RESCUE_WARPS_PER_BLOCK: "
+                    "fixed launch shapes instead of the autotuner (reproducible profiles)")
     ap.add_argument("--serve-scale", type=float, default=0.125,
                     help="sample sizes of the serving leg as a fraction of 0.5M-8M pairs")
     return ap.parse_args()
@@ -244,8 +246,15 @@ def main():
                     torch.from_numpy(lens).cuda()))
     torch.cuda.synchronize()
 
+    def pin(c):
+        if args.pin_tuning:
+            c.set_tuning(*[int(x) for x in args.pin_tuning.split(",")])
+        return c
+
     def measure(path):
-        ctx = api.Context(ix, device=local, path=path, lanes=args.lanes)
+        # the plain form is one pass per chunk: one lane
+        lanes = 1 if path == "plain" else args.lanes
+        ctx = pin(api.Context(ix, device=local, path=path, lanes=lanes, max_batch=args.chunk if path == "plain" else 0))
         stream = torch.cuda.ExternalStream(ctx.stream)
 
         def step(i):
@@ -293,7 +302,7 @@ def main():
     def kernel_pass():
         """One step on a single-lane context, so each kernel's CUDA-event
         duration is its own (the timed run overlaps three lanes)."""
-        kctx = api.Context(ix, device=local, path="batched", lanes=1)
+        kctx = pin(api.Context(ix, device=local, path="batched", lanes=1))
         s, o, ln = dev[0]
         for _ in range(2):
             kctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
@@ -403,7 +412,7 @@ def serve_bench(args, local):
         pool.append(synth.simulate_pairs(tx, CH, seed=500 + k, read_len=L, frag_mu=max(250.0, 2.5 * L),
                                          frag_sd=25.0, sub_rate=0.005, indel_rate=0.0001))
     # the plain path's capacity, host buffers in and out like the server's
-    pctx = api.Context(ix, device=local, path="plain")
+    pctx = api.Context(ix, device=local, path="plain", lanes=1, max_batch=CH)   # one launch per chunk
     pctx.align_pairs(*pool[1])
     t = time.perf_counter()
     for r1, r2 in pool:

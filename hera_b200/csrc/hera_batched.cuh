@@ -87,6 +87,68 @@ struct Round {
 	int rcap;                 // CIGAR ops per job result
 };
 
+// Anchors of the batched form, 8 bytes each: {transcript, position |
+// read offset << 23}; one load per anchor.  Transcripts must be shorter
+// than 2^23 bases (checked when the context is created).
+constexpr int TP_BITS = 23;
+constexpr uint32_t TP_MASK = (1u << TP_BITS) - 1;
+struct __align__(8) PA {
+	uint32_t t, w;
+	__device__ __forceinline__ uint32_t tp() const { return w & TP_MASK; }
+	__device__ __forceinline__ uint32_t off() const { return w >> TP_BITS; }
+};
+struct PAnchors {
+	PA a[ACAP];
+};
+__device__ __forceinline__ PA pa_make(uint32_t t, uint32_t tp, uint32_t off)
+{
+	return PA{t, tp | (off << TP_BITS)};
+}
+
+// merge_sort / add_sort (src/hash_align.c:247-297) of a k-mer's occurrence
+// list (read offset idx) into the anchors, as merge_hits does for the
+// plain form
+__device__ inline int merge_packed(const PAnchors &A, int na, PAnchors &B, const uint2 *occ, uint32_t nh,
+				   uint32_t idx, int &flags)
+{
+	if (na + (int)nh > ACAP) {
+		flags |= F_ACAP;
+		nh = (uint32_t)(ACAP - na);
+	}
+	int i = 0, n = 0;
+	uint32_t k = 0;
+	uint2 h = nh ? __ldg(occ) : make_uint2(0, 0);
+	PA a = na ? A.a[0] : PA{0, 0};
+	while (i < na && k < nh) {
+		bool take_a;
+		if (a.t < h.x) {
+			take_a = true;
+		} else if (a.t > h.x) {
+			take_a = false;
+		} else {
+			const uint32_t dis = (h.y - a.tp()) - (idx - a.off());
+			take_a = dis < 2 * ERR ? true : !(a.tp() > h.y);
+		}
+		if (take_a) {
+			B.a[n] = a;
+			if (++i < na)
+				a = A.a[i];
+		} else {
+			B.a[n] = pa_make(h.x, h.y, idx);
+			if (++k < nh)
+				h = __ldg(occ + k);
+		}
+		++n;
+	}
+	for (; i < na; ++i, ++n)
+		B.a[n] = A.a[i];
+	for (; k < nh; ++k, ++n) {
+		h = __ldg(occ + k);
+		B.a[n] = pa_make(h.x, h.y, idx);
+	}
+	return n;
+}
+
 // round 0: reset every pair's Candidate state and list the get_position
 // calls that have at least one seed hit (the others take the miss exit)
 __global__ void k_task_list(Batch b, int ntask, const uint2 *__restrict__ hits, int spr,
@@ -140,7 +202,7 @@ __device__ __forceinline__ void task_of(const Round &R, int t, int &pi, int &c, 
 // (pass A :1367-1390, pass B :1392-1412, pass C :1414-1434); pass A's
 // consumed marks are kept in a bitmask so the walk can be repeated.
 template <class Emit>
-__device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, int space, int rlen,
+__device__ inline void enum_chains(const PAnchors &A, int na, const DSlot &Mt, int space, int rlen,
 				   uint32_t *used, Emit emit)
 {
 	for (int w = 0; w < ACAP / 32; ++w)
@@ -149,16 +211,18 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 	auto next = [&](uint32_t i, uint32_t n, bool stop_used) -> bool {
 		if (i + 1 >= (uint32_t)na)
 			return false;
-		if (A.a[i].t != A.a[i + 1].t)
+		const PA a0 = A.a[i], a1 = A.a[i + 1];
+		if (a0.t != a1.t)
 			return false;
 		// read offsets of used anchors read as rlen in the reference
-		const uint32_t o0 = is_used(i) ? (uint32_t)rlen : A.a[i].off;
-		const uint32_t o1 = is_used(i + 1) ? (uint32_t)rlen : A.a[i + 1].off;
+		const uint32_t o0 = is_used(i) ? (uint32_t)rlen : a0.off();
+		const uint32_t o1 = is_used(i + 1) ? (uint32_t)rlen : a1.off();
 		if (!(o1 > o0))
 			return false;
-		if (!(A.a[i + 1].tp > A.a[i + 1 - n].tp))
+		const uint32_t tp1 = a1.tp(), tph = A.a[i + 1 - n].tp();
+		if (!(tp1 > tph))
 			return false;
-		if (!(A.a[i + 1].tp - A.a[i + 1 - n].tp < (uint32_t)rlen))
+		if (!(tp1 - tph < (uint32_t)rlen))
 			return false;
 		if (stop_used && o1 == (uint32_t)rlen)
 			return false;
@@ -186,7 +250,7 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 		}
 	}
 	for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-		if (is_used(i) || A.a[i].off == (uint32_t)rlen)
+		if (is_used(i) || A.a[i].off() == (uint32_t)rlen)
 			continue;
 		uint32_t n = 1;
 		while (next(i, n, true)) {
@@ -199,7 +263,7 @@ __device__ inline void enum_chains(const Anchors &A, int na, const DSlot &Mt, in
 	}
 	if (space < KMER) {
 		for (uint32_t i = 0; i < (uint32_t)na; ++i) {
-			if (is_used(i) || A.a[i].off == (uint32_t)rlen)
+			if (is_used(i) || A.a[i].off() == (uint32_t)rlen)
 				continue;
 			uint32_t n = 1;
 			while (next(i, n, true)) {
@@ -218,7 +282,7 @@ constexpr int LJS = 256;       // SW_align calls of one get_position call
 constexpr int LJ = 256;        // distinct DP jobs of one get_position call
 
 struct BuildWork {
-	Anchors a[2];
+	PAnchors a[2];
 	uint32_t used[ACAP / 32];
 	Chain ch[LCH];
 	JobSlot js[LJS];
@@ -247,7 +311,7 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 	BuildWork w;
 	int cur = 0, na = 0, sj = 0;
 	for (uint32_t i = 0; i + KMER <= (uint32_t)L; i += step, ++sj) {
-		uint2 h = R.hits ? R.hits[((int64_t)ri * 2 + str) * R.spr + sj] : probe(b.ix, kmer_at(rd, (int)i));
+		uint2 h = R.hits ? R.hits[((int64_t)ri * 2 + str) * R.spr + sj] : probe(b.ix, kmer_words(rd + i, false));
 		if (h.y == 0)
 			continue;
 		const uint2 *occ = b.ix.occ + h.x;
@@ -258,22 +322,20 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 				nh = ACAP;
 			}
 			for (uint32_t k = 0; k < nh; ++k) {
-				uint2 o = __ldg(occ + k);
-				w.a[cur].a[k].t = o.x;
-				w.a[cur].a[k].tp = o.y;
-				w.a[cur].a[k].off = i;
+				const uint2 o = __ldg(occ + k);
+				w.a[cur].a[k] = pa_make(o.x, o.y, i);
 			}
 			na = (int)nh;
 			continue;
 		}
-		na = merge_hits(w.a[cur], na, w.a[cur ^ 1], occ, h.y, i, flags);
+		na = merge_packed(w.a[cur], na, w.a[cur ^ 1], occ, h.y, i, flags);
 		cur ^= 1;
 	}
 	if (na == 0) {
 		flag(b.flags, flags);
 		return;
 	}
-	const Anchors &A = w.a[cur];
+	const PAnchors &A = w.a[cur];
 	const DSlot &Mt = P.s[c][1 - str];
 	int nch = 0, ns = 0, nj = 0;
 	// one SW_align call -> a job slot; identical calls (same query span,
@@ -288,10 +350,7 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 			const DpJob &o = w.jb[q];
 			if (o.qoff != j.qoff || o.len != j.len || o.ref_len != j.ref_len || o.err != j.err)
 				continue;
-			bool same = true;
-			for (uint32_t x = 0; x < j.ref_len && same; ++x)
-				same = __ldg(b.ix.seq + o.rstart + x) == __ldg(b.ix.seq + j.rstart + x);
-			if (same)
+			if (bytes_equal(b.ix.seq, o.rstart, j.rstart, j.ref_len))
 				hit = q;
 		}
 		if (hit < 0) {
@@ -314,17 +373,17 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 		}
 		Chain &ch = w.ch[nch++];
 		ch.t = A.a[id].t;
-		ch.tp = A.a[id].tp;
-		ch.off = A.a[id].off;
+		ch.tp = A.a[id].tp();
+		ch.off = A.a[id].off();
 		ch.pass = (int8_t)pass;
 		ch.viable = 0;
 		ch.has_prefix = 0;
 		ch.js0 = ns;
 		ch.njs = 0;
 		// get_SWalign's early returns before any DP (:1250-1256)
-		if (n > 1 && A.a[id + n - 1].tp - A.a[id].tp > (uint32_t)L)
+		if (n > 1 && A.a[id + n - 1].tp() - A.a[id].tp() > (uint32_t)L)
 			return;
-		const int start = (int)(A.a[id].tp - (A.a[id].off + KMER - 1));
+		const int start = (int)(A.a[id].tp() - (A.a[id].off() + KMER - 1));
 		if (start < 0 || (uint32_t)(start + L) > __ldg(b.ix.tlen + A.a[id].t))
 			return;
 		ch.viable = 1;
@@ -336,8 +395,8 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 		j.pad = 0;
 		j.pad0 = 0;
 		const int ns0 = ns;
-		if (A.a[id].off > 0) {   // prefix DP on the reversed strings (:1262-1266)
-			const uint32_t o0 = A.a[id].off;
+		if (A.a[id].off() > 0) {   // prefix DP on the reversed strings (:1262-1266)
+			const uint32_t o0 = A.a[id].off();
 			ch.has_prefix = 1;
 			j.rstart = ref_start - add;
 			j.ref_len = (uint16_t)(o0 + add);
@@ -348,17 +407,17 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 		}
 		for (uint32_t i = 0; i < n; ++i) {   // merged runs and their gaps (:1282-1305)
 			const uint32_t s0 = i;
-			while (i + 1 < n && A.a[id + i].off + KMER >= A.a[id + i + 1].off)
+			while (i + 1 < n && A.a[id + i].off() + KMER >= A.a[id + i + 1].off())
 				++i;
-			const uint32_t seg = A.a[id + i].off + KMER;
-			const uint32_t len = ((i + 1) < n ? A.a[id + i + 1].off : (uint32_t)L) - seg;
+			const uint32_t seg = A.a[id + i].off() + KMER;
+			const uint32_t len = ((i + 1) < n ? A.a[id + i + 1].off() : (uint32_t)L) - seg;
 			const uint32_t ad = (i + 1) < n ? 0u : (uint32_t)ERR;
 			j.rstart = ref_start + seg;
 			j.ref_len = (uint16_t)(len + ad);
 			j.len = (uint16_t)len;
 			j.qoff = (uint16_t)seg;
 			j.err = (int8_t)(len < 2 * ERR ? 3 : ERR);
-			add_job(j, (uint16_t)(A.a[id + i].off - A.a[id + s0].off + KMER));
+			add_job(j, (uint16_t)(A.a[id + i].off() - A.a[id + s0].off() + KMER));
 		}
 		ch.njs = (int16_t)(ns - ns0);
 	});

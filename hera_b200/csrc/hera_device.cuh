@@ -609,6 +609,60 @@ __device__ __forceinline__ uint2 probe(const DevIndex &ix, uint64_t id, uint32_t
 	return make_uint2(0, 0);
 }
 
+// 8 bytes at any address p, from the two aligned words around it (the
+// buffers this reads carry at least 16 bytes of padding past their data)
+__device__ __forceinline__ uint64_t load8(const uint8_t *p)
+{
+	const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+	const unsigned long long *w = reinterpret_cast<const unsigned long long *>(a & ~(uintptr_t)7);
+	const int s = (int)(a & 7) * 8;
+	const uint64_t lo = __ldg(w);
+	if (s == 0)
+		return lo;
+	return (lo >> s) | ((uint64_t)__ldg(w + 1) << (64 - s));
+}
+
+// get_index (src/hash_align.c:997-1006) over 31 codes at p, read as four
+// 8-byte words: id = OR of code[x] << 2*(30-x) (the reference shifts codes
+// in unmasked, so code 4 sets the low bit of the previous slot).  rev: the
+// reverse complement of the same 31 bytes (the k-mer that starts at the
+// last byte and runs backwards), id = OR of comp(code[x]) << 2*x.
+__device__ __forceinline__ uint64_t kmer_words(const uint8_t *p, bool rev)
+{
+	uint64_t W[4];
+#pragma unroll
+	for (int k = 0; k < 4; ++k)
+		W[k] = load8(p + 8 * k);
+	uint64_t id = 0;
+#pragma unroll
+	for (int x = 0; x < KMER; ++x) {
+		const uint8_t c = (uint8_t)(W[x >> 3] >> (8 * (x & 7)));
+		if (rev)
+			id |= (uint64_t)comp_code(c) << (2 * x);
+		else
+			id |= (uint64_t)c << (2 * (KMER - 1 - x));
+	}
+	return id;
+}
+
+// true if the n bytes at s+a and s+b are equal (8 at a time)
+__device__ __forceinline__ bool bytes_equal(const uint8_t *s, uint32_t a, uint32_t b, uint32_t n)
+{
+	if (a == b)
+		return true;
+	for (uint32_t x = 0; x < n; x += 8) {
+		uint64_t u = load8(s + a + x), v = load8(s + b + x);
+		if (n - x < 8) {
+			const uint64_t m = (1ull << (8 * (n - x))) - 1;
+			u &= m;
+			v &= m;
+		}
+		if (u != v)
+			return false;
+	}
+	return true;
+}
+
 // get_index (src/hash_align.c:997-1006): codes shifted in unmasked
 __device__ __forceinline__ uint64_t kmer_at(const uint8_t *rd, int i)
 {

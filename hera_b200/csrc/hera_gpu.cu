@@ -21,8 +21,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
+#include <atomic>
 #include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -126,16 +131,9 @@ __global__ void k_seed(DevIndex ix, const uint8_t *__restrict__ code, const int6
 	uint2 h = make_uint2(0, 0);
 	if (t < total && i + KMER <= L && j < spr) {
 		const uint8_t *src = code + off[ri];
-		uint64_t id = 0;
-		if (orient == 0) {
-#pragma unroll
-			for (int x = 0; x < KMER; ++x)
-				id = (id << 2) | src[i + x];
-		} else {
-#pragma unroll
-			for (int x = 0; x < KMER; ++x)
-				id = (id << 2) | comp_code(src[L - 1 - i - x]);
-		}
+		// orientation 1: the reverse complement's k-mer at i covers bytes
+		// [L-1-i-30, L-1-i] of the read
+		const uint64_t id = orient == 0 ? kmer_words(src + i, false) : kmer_words(src + (L - KMER - i), true);
 		h = probe(ix, id, &np);
 		found = h.y > 0;
 	}
@@ -647,6 +645,9 @@ struct hera_gpu_ctx {
 	std::mutex tune_mu;
 	hera_gpu_tuning tune{};
 	int build_tuning = 0, rescue_tuning = 0;   // 0 open, 1 claimed by a lane, 2 done
+	// lanes run their rounds under a shared lock; the autotuner's trials
+	// take it exclusively, so no other lane's kernels share the GPU with them
+	std::shared_mutex gate;
 };
 
 // candidate launch shapes the autotuner times
@@ -790,7 +791,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
 		return HERA_GPU_ENODEV;
 	hera_gpu_ctx *ctx = new hera_gpu_ctx();
-	int nlanes = 3;
+	int nlanes = 6;
 	if (opt) {
 		ctx->device = opt->device;
 		if (opt->max_batch)
@@ -854,8 +855,13 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	for (uint32_t i = 0; i < v->n_pos; ++i)
 		occ[i] = make_uint2(v->pos[i], v->p[i]);
 	std::vector<uint32_t> tstart(n);
-	for (uint32_t i = 0; i < n; ++i)
+	for (uint32_t i = 0; i < n; ++i) {
 		tstart[i] = v->find[i] - v->len[i];
+		// the batched form packs transcript positions into 23 bits
+		if (ctx->batched && v->len[i] >= (1u << TP_BITS))
+			return bail(fail(ctx, HERA_GPU_EINVAL,
+					 "a transcript of 2^23 bases or more: use HERA_GPU_PATH_PLAIN"));
+	}
 	const size_t pad = 64;
 	std::vector<uint8_t> seqp(seq_len + pad, 0);
 	memcpy(seqp.data(), v->seq, seq_len);
@@ -899,6 +905,7 @@ static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq 
 			int max_len, uint32_t &launches, float &ms_acc)
 {
 	cudaStream_t st = L.stream;
+	std::shared_lock<std::shared_mutex> shared(ctx->gate);
 	LK(L.calls.ensure((size_t)nq * LCAP), "rescue calls");
 	LK(L.rq_base.ensure(nq), "rescue bases");
 	int *d_nc = L.counters.p + 4;
@@ -919,10 +926,15 @@ static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq 
 	};
 	// autotune: the first large rescue round times each candidate (every
 	// run writes the same outputs)
+	std::unique_lock<std::shared_mutex> excl(ctx->gate, std::defer_lock);
 	if (ncalls >= 2048 && claim_tuning(ctx, ctx->rescue_tuning)) {
+		shared.unlock();   // nothing of this lane is in flight (synchronised above)
+		excl.lock();
 		int best = 0;
 		float best_ms = 0;
 		int nc = 0;
+		launch(tuned_rescue_wpb(ctx));   // untimed: first-launch costs
+		LK(cudaStreamSynchronize(st), "rescue tuning");
 		for (int wpb : RESCUE_WPB) {
 			cudaEventRecord(L.ev[10], st);
 			launch(wpb);
@@ -967,6 +979,13 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 {
 	if (R.ntask <= 0)
 		return HERA_GPU_OK;
+	const bool tune = !R.req && R.ntask >= 4 * 16384 && claim_tuning(ctx, ctx->build_tuning);
+	std::shared_lock<std::shared_mutex> shared(ctx->gate, std::defer_lock);
+	std::unique_lock<std::shared_mutex> excl(ctx->gate, std::defer_lock);
+	if (tune)
+		excl.lock();
+	else
+		shared.lock();
 	cudaStream_t st = L.stream;
 	const int rcap = b.score_only ? 2 : JCAP;
 	LK(L.tinfo.ensure(R.ntask), "task info");
@@ -1012,9 +1031,11 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		};
 		// autotune the persistent build kernel's residency on the first
 		// large round 0 (every run writes the same chains and jobs)
-		if (!R.req && R.ntask >= 4 * 16384 && claim_tuning(ctx, ctx->build_tuning)) {
+		if (tune && ctx->build_tuning == 1) {
 			int best = 0, nc = 0;
 			float best_ms = 0;
+			launch(tuned_build_bps(ctx));   // untimed: first-launch costs
+			LK(cudaStreamSynchronize(st), "build tuning");
 			for (int bps : BUILD_BPS) {
 				cudaEventRecord(L.ev[8], st);
 				launch(bps);
@@ -1331,6 +1352,117 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 	return HERA_GPU_OK;
 }
 
+// ---- host copy pool ------------------------------------------------------
+//
+// One host thread copies pageable memory at a few GB/s, far below what the
+// PCIe copies and the kernels sustain, so the large host copies of a call
+// (reads into pinned staging, records and pools out of it) are cut into
+// pieces that a process-wide pool of threads and the calling thread share.
+// Lanes submit concurrently; each waits for its own job only.
+class CopyPool {
+public:
+	static CopyPool &get()
+	{
+		static CopyPool p;
+		return p;
+	}
+	// run fn(0 .. n-1), the caller taking part
+	void run(size_t n, const std::function<void(size_t)> &fn)
+	{
+		if (n == 0)
+			return;
+		if (n == 1 || th_.empty()) {
+			for (size_t i = 0; i < n; ++i)
+				fn(i);
+			return;
+		}
+		auto j = std::make_shared<Job>();
+		j->fn = &fn;
+		j->n = n;
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			q_.push_back(j);
+		}
+		cv_.notify_all();
+		work(*j);
+		std::unique_lock<std::mutex> g(j->mu);
+		j->cv.wait(g, [&] { return j->done.load() == j->n; });
+	}
+	~CopyPool()
+	{
+		{
+			std::lock_guard<std::mutex> g(mu_);
+			stop_ = true;
+		}
+		cv_.notify_all();
+		for (auto &t : th_)
+			t.join();
+	}
+
+private:
+	struct Job {
+		const std::function<void(size_t)> *fn = nullptr;
+		size_t n = 0;
+		std::atomic<size_t> next{0}, done{0};
+		std::mutex mu;
+		std::condition_variable cv;
+	};
+	CopyPool()
+	{
+		unsigned n = std::thread::hardware_concurrency();
+		n = n > 16 ? 16 : n;
+		for (unsigned i = 1; i < n; ++i)
+			th_.emplace_back([this] { loop(); });
+	}
+	static void work(Job &j)
+	{
+		for (;;) {
+			const size_t i = j.next.fetch_add(1);
+			if (i >= j.n)
+				return;
+			(*j.fn)(i);
+			if (j.done.fetch_add(1) + 1 == j.n) {
+				std::lock_guard<std::mutex> g(j.mu);
+				j.cv.notify_all();
+			}
+		}
+	}
+	void loop()
+	{
+		for (;;) {
+			std::shared_ptr<Job> j;
+			{
+				std::unique_lock<std::mutex> g(mu_);
+				cv_.wait(g, [&] {
+					while (!q_.empty() && q_.front()->next.load() >= q_.front()->n)
+						q_.pop_front();
+					return stop_ || !q_.empty();
+				});
+				if (stop_)
+					return;
+				j = q_.front();
+			}
+			work(*j);
+		}
+	}
+	std::vector<std::thread> th_;
+	std::mutex mu_;
+	std::condition_variable cv_;
+	std::deque<std::shared_ptr<Job>> q_;
+	bool stop_ = false;
+};
+
+// memcpy in pieces of at most 4 MiB over the pool
+static void pcopy(void *dst, const void *src, size_t bytes)
+{
+	const size_t piece = 4u << 20;
+	const size_t n = (bytes + piece - 1) / piece;
+	CopyPool::get().run(n, [&](size_t i) {
+		const size_t a = i * piece, b = a + piece < bytes ? a + piece : bytes;
+		memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, b - a);
+	});
+}
+
 // D2H of lane L's packed records into `out` at record rec0 and pool
 // offsets (bl, bo, bm), through the lane's pinned staging
 static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, uint64_t bo, uint64_t bm)
@@ -1359,23 +1491,27 @@ static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, u
 	L.timing.d2h_ms += ms;
 	const auto h0 = std::chrono::steady_clock::now();
 	hera_cand_rec *dst = out->recs + rec0;
-	for (int i = 0; i < items; ++i) {
-		hera_cand_rec r = L.h_recs.p[i];
-		for (int s = 0; s < 2; ++s) {
-			r.list_off[s] += (uint32_t)bl;
-			r.cig_off[s] += (uint32_t)bo;
-			r.miss_off[s] += (uint32_t)bm;
+	const int per = 65536;   // records per piece
+	CopyPool::get().run(((size_t)items + per - 1) / per, [&](size_t k) {
+		const int a = (int)k * per, e = a + per < items ? a + per : items;
+		for (int i = a; i < e; ++i) {
+			hera_cand_rec r = L.h_recs.p[i];
+			for (int s = 0; s < 2; ++s) {
+				r.list_off[s] += (uint32_t)bl;
+				r.cig_off[s] += (uint32_t)bo;
+				r.miss_off[s] += (uint32_t)bm;
+			}
+			dst[i] = r;
 		}
-		dst[i] = r;
-	}
+	});
 	if (L.nl) {
-		memcpy(out->pos_pool + bl, L.h_pos.p, L.nl * 4);
-		memcpy(out->p_pool + bl, L.h_p.p, L.nl * 4);
+		pcopy(out->pos_pool + bl, L.h_pos.p, L.nl * 4);
+		pcopy(out->p_pool + bl, L.h_p.p, L.nl * 4);
 	}
 	if (L.no)
-		memcpy(out->op_pool + bo, L.h_ops.p, L.no * 4);
+		pcopy(out->op_pool + bo, L.h_ops.p, L.no * 4);
 	if (L.nm)
-		memcpy(out->miss_pool + bm, L.h_miss.p, L.nm);
+		pcopy(out->miss_pool + bm, L.h_miss.p, L.nm);
 	L.timing.host_out_ms +=
 		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - h0).count();
 	return HERA_GPU_OK;
@@ -1414,7 +1550,7 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 		const hera_gpu_reads *r = src[m];
 		if (contig[m] && n > 0) {
 			const int64_t len_m = r->off[lo + n - 1] + r->len[lo + n - 1] - r->off[lo];
-			memcpy(L.h_seq.p + o, r->seq + r->off[lo], (size_t)len_m);
+			pcopy(L.h_seq.p + o, r->seq + r->off[lo], (size_t)len_m);
 			const int64_t shift = o - r->off[lo];
 			for (int32_t i = 0; i < n; ++i) {
 				L.h_off.p[(size_t)i * per + m] = r->off[lo + i] + shift;

@@ -163,7 +163,7 @@ static int srv_stage(Lane &L, const std::vector<SrvPiece> &pc, int32_t npairs, i
 		for (int m = 0; m < 2; ++m) {
 			int64_t a, e;
 			range(c, m, q.lo, q.cnt, a, e);
-			memcpy(L.h_seq.p + o, c.seq[m].data() + a, (size_t)(e - a));
+			pcopy(L.h_seq.p + o, c.seq[m].data() + a, (size_t)(e - a));
 			for (int32_t i = 0; i < q.cnt; ++i) {
 				L.h_off.p[2 * (r + i) + m] = c.off[m][q.lo + i] - a + o;
 				L.h_len.p[2 * (r + i) + m] = c.len[m][q.lo + i];
@@ -405,7 +405,7 @@ extern "C" int hera_gpu_server_submit(hera_gpu_server *S, uint32_t sample, const
 		}
 		c->seq[m].resize((size_t)total + 1);
 		if (contig && n > 0) {   // one copy of the block
-			memcpy(c->seq[m].data(), R.seq + R.off[0], (size_t)total);
+			pcopy(c->seq[m].data(), R.seq + R.off[0], (size_t)total);
 			for (int32_t i = 0; i < n; ++i) {
 				c->off[m][i] = R.off[i] - R.off[0];
 				c->len[m][i] = R.len[i];

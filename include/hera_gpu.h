@@ -148,7 +148,7 @@ typedef struct hera_gpu_options {
 	uint64_t scratch_bytes;  /* unused (the mate-rescue DP works in shared
 				    memory); kept for layout compatibility */
 	int path;                /* HERA_GPU_PATH_BATCHED (default) or _PLAIN */
-	int lanes;               /* concurrent sub-batches (stream + host thread each); 0 = 3 */
+	int lanes;               /* concurrent sub-batches (stream + host thread each); 0 = 6 */
 } hera_gpu_options;
 
 /* Per-stage device time of the last call, milliseconds (CUDA events,
