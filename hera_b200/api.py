@@ -368,10 +368,12 @@ class Server:
         self._sizes[t.value] = (r1.n, int(r1.len.sum()) + int(r2.len.sum()))
         return t.value
 
-    def wait(self, ticket: int):
-        """(Result, info) of a chunk, blocking until it is done."""
+    def wait(self, ticket: int, out: Optional[Result] = None):
+        """(Result, info) of a chunk, blocking until it is done.  `out`: a
+        Result to reuse (its storage is overwritten)."""
         n, total_len = self._sizes.pop(ticket)
-        res = Result(2 * n, 8 * n + 1024, 8 * n + 1024, total_len // 8 + 1024)
+        res = out.reuse(2 * n) if out is not None else Result(2 * n, 8 * n + 1024, 8 * n + 1024,
+                                                               total_len // 8 + 1024)
         info = ChunkInfo()
         rc = self.lib.hera_gpu_server_wait(self.h, ticket, C.byref(res.c), C.byref(info))
         if rc == -5 and (res.c.list_used > res.c.list_cap or res.c.op_used > res.c.op_cap

@@ -581,20 +581,21 @@ __device__ __forceinline__ int job_form(const DpJob &j)
 }
 
 // one thread per job, jobs in (error cap, length) order; threads whose job
-// is not of cap E leave at once (whole warps, the order is by cap).  In the
-// score-only mode the pass keeps no rows; a job whose DP stops early (the
-// shrink loop needs its rows) is queued on `redo` for k_dp_redo, so the
-// warps here stay converged.
+// is not of cap E leave at once (whole warps, the order is by cap).  Every
+// row is kept (4 bits a slot, in local memory), so a DP that stops early runs
+// its shrink loop in place: in the score-only mode 18% of the error-8 calls
+// stop early, nearly every warp holds one, and a rerun would redo the DP.
 template <int E>
 __global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
-	 int rcap, int *__restrict__ redo, int *__restrict__ n_redo)
+	 int rcap)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t cells = 0;
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
 		const DpJob jb = jobs[id];
+		__align__(16) uint32_t rows[(MAX_DP_ROWS + 1) * ((2 * E + 2 + 7) / 8)];
 		DCig cig;
 		int flags = 0;
 		cig.n = cig.nm = 0;
@@ -602,55 +603,12 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
 		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
 		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-		int score;
-		if (b.score_only) {
-			score = sw_align_reg<E, false>(r, qv, jb.ref_len, jb.len, true, cig, nullptr, flags, cells);
-			if (score < 0) {
-				redo[atomicAdd(n_redo, 1)] = id;
-				cells = 0;   // counted by the rerun
-			}
-		} else {
-			__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
-			score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, false, cig, rows, flags, cells);
-		}
-		if (score >= 0) {
-			store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-			flag(b.flags, flags);
-		}
+		const int score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig,
+							reinterpret_cast<uint8_t *>(rows), flags, cells);
+		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+		flag(b.flags, flags);
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
-}
-
-// the score-only jobs of cap E whose DP stopped early, rerun with the rows
-// kept (grid-stride over the device-side count)
-template <int E>
-__global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
-k_dp_redo(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ redo, const int *__restrict__ n_redo,
-	  uint8_t *__restrict__ res, int rcap)
-{
-	const int n = *n_redo;
-	const int span = gridDim.x * blockDim.x;
-	const int rounds = (n + span - 1) / span;   // every lane of a warp runs as many rounds
-	for (int k = 0; k < rounds; ++k) {
-		const int t = blockIdx.x * blockDim.x + threadIdx.x + k * span;
-		uint32_t cells = 0;
-		if (t < n) {
-			const int id = redo[t];
-			const DpJob jb = jobs[id];
-			__align__(16) uint8_t rows[(MAX_DP_ROWS + 1) * (((2 * E + 2) + 3) / 4 * 4)];
-			DCig cig;
-			int flags = 0;
-			cig.n = cig.nm = 0;
-			const bool rev = jb.err < 0;
-			const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
-			RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
-			QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-			const int score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, true, cig, rows, flags, cells);
-			store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-			flag(b.flags, flags);
-		}
-		warp_stat(b.stats + ST_SW_CELLS, cells);
-	}
 }
 
 // the jobs outside the register form (empty gaps, spill cases)

@@ -372,7 +372,7 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 {
 	constexpr int W = 2 * E + 2;
 	constexpr unsigned error = E;
-	constexpr int RS = ((W + 3) / 4) * 4;   // bytes per stored row
+	constexpr int NW = (W + 7) / 8;        // 32-bit words per stored row (4 bits a slot)
 	// reference code at window position x, clamped (values outside the
 	// window are never used, the clamp only keeps the address valid)
 	auto rcode = [&](int x) -> int {
@@ -388,23 +388,24 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 		P[q] = (d >= 0) ? d : 0;          // row 0: M[0][c] = c, c <= error+1
 		RC[q] = rcode(q - E);             // row 1 needs r[c-1], c = 1 + q - E
 	}
+	// rows are kept 4 bits a slot (values <= error + 1 <= 9)
+	uint32_t *rw = reinterpret_cast<uint32_t *>(rows);
 	auto store_row = [&](int k) {
-		uint32_t *o = reinterpret_cast<uint32_t *>(rows + k * RS);
 #pragma unroll
-		for (int w = 0; w < (W + 3) / 4; ++w) {
+		for (int w = 0; w < NW; ++w) {
 			uint32_t pk = 0;
 #pragma unroll
-			for (int b = 0; b < 4; ++b)
-				if (w * 4 + b < W)
-					pk |= (uint32_t)P[w * 4 + b] << (8 * b);
-			o[w] = pk;
+			for (int b = 0; b < 8; ++b)
+				if (w * 8 + b < W)
+					pk |= (uint32_t)P[w * 8 + b] << (4 * b);
+			rw[k * NW + w] = pk;
 		}
 	};
 	if (STORE)
 		store_row(0);
 	auto get = [&](int k, int c) -> unsigned {
 		const int q = c - k + E;
-		return (q >= 0 && q < W) ? rows[k * RS + q] : 0u;
+		return (q >= 0 && q < W) ? (rw[k * NW + (q >> 3)] >> (4 * (q & 7))) & 15u : 0u;
 	};
 
 	int s = 0, ferr = -1, k, i = 0;

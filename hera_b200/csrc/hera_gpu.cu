@@ -583,7 +583,7 @@ struct Lane {
 	DBuf<JobSlot> slots;
 	DBuf<DpJob> jobs;
 	DBuf<uint8_t> res;
-	DBuf<int> perm, hist, tlist, redo;
+	DBuf<int> perm, hist, tlist;
 	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
 	DBuf<hera_cand_rec> recs;
 	DBuf<uint32_t> pos_pool, op_pool;
@@ -609,7 +609,7 @@ struct Lane {
 		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
 		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release();
 		calls.release(); rq_base.release(); ssw_out.release(); tinfo.release(); chains.release();
-		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release(); redo.release();
+		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
 		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
@@ -1091,19 +1091,12 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		k_bin_count<<<148, 512, 0, st>>>(L.jobs.p, nj, L.hist.p);
 		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
 		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
-		LK(L.redo.ensure(2 * (size_t)nj), "dp reruns");
-		int *d_redo = L.counters.p + 24;   // [0] cap 4, [1] cap 8
-		LK(cudaMemsetAsync(d_redo, 0, 2 * sizeof(int), st), "memset");
-		const unsigned redo_grid = blocks_for(nj) < 148u * 6 ? blocks_for(nj) : 148u * 6;
 		cudaEventRecord(L.ev[10], st);
-		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap, L.redo.p, d_redo);
-		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap, L.redo.p + nj,
-							     d_redo + 1);
-		k_dp_redo<4><<<redo_grid, 128, 0, st>>>(b, L.jobs.p, L.redo.p, d_redo, L.res.p, rcap);
-		k_dp_redo<8><<<redo_grid, 128, 0, st>>>(b, L.jobs.p, L.redo.p + nj, d_redo + 1, L.res.p, rcap);
+		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
 		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
 		cudaEventRecord(L.ev[11], st);
-		launches += 8;
+		launches += 6;
 		R.res = L.res.p;
 	}
 	k_replay<<<blocks_for(R.ntask), 128, 0, st>>>(b, R);
@@ -1911,7 +1904,7 @@ constexpr size_t BYTES =
 	2 * A(PAIRS * sizeof(RmReq)) + 2 * A(PAIRS * sizeof(GpReq)) + A(32 * sizeof(int)) +
 	A(6 * (ITEMS + 1) * sizeof(uint32_t)) + A(CUB) + A(TASKS * sizeof(TaskInfo)) + A(TASKS * sizeof(int)) +
 	A(CHAINS * sizeof(Chain)) + A(JOBS * sizeof(DpJob)) + A(SLOTS * sizeof(JobSlot)) +
-	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(2 * JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
+	A(JOBS * (size_t)res_stride(JCAP)) + A(JOBS * sizeof(int)) + A(NBIN * sizeof(int)) +
 	A(PAIRS * LCAP * sizeof(int2)) + A(PAIRS * sizeof(int)) + A(CALLS * sizeof(SswOut));
 }  // namespace na
 
@@ -1998,7 +1991,6 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 	L.slots.bind(take(na::SLOTS * sizeof(JobSlot)), na::SLOTS);
 	L.res.bind(take(na::JOBS * (size_t)res_stride(JCAP)), na::JOBS * (size_t)res_stride(JCAP));
 	L.perm.bind(take(na::JOBS * sizeof(int)), na::JOBS);
-	L.redo.bind(take(2 * na::JOBS * sizeof(int)), 2 * na::JOBS);
 	L.hist.bind(take(NBIN * sizeof(int)), NBIN);
 	L.calls.bind(take(na::PAIRS * LCAP * sizeof(int2)), na::PAIRS * LCAP);
 	L.rq_base.bind(take(na::PAIRS * sizeof(int)), na::PAIRS);

@@ -62,13 +62,32 @@ struct SrvSeg {   // one piece: its ranges in a batch's output
 	uint32_t l0 = 0, l1 = 0, o0 = 0, o1 = 0, m0 = 0, m1 = 0;   // pools
 };
 
+// host array without value-initialisation, reused across chunks (fresh
+// memory for every chunk would cost a page fault per 4 KiB on first touch)
+template <typename T>
+struct RawBuf {
+	std::unique_ptr<T[]> p;
+	size_t cap = 0;
+	void need(size_t n)
+	{
+		if (n > cap) {
+			p.reset(new T[n]);
+			cap = n;
+		}
+	}
+	T *data() { return p.get(); }
+	const T *data() const { return p.get(); }
+	T &operator[](size_t i) { return p[i]; }
+	const T &operator[](size_t i) const { return p[i]; }
+};
+
 struct SrvChunk {
 	uint64_t ticket = 0;
 	uint32_t sample = 0;
 	int32_t n = 0;
-	std::vector<char> seq[2];     // mate 1 and mate 2 reads, back to back
-	std::vector<int64_t> off[2];  // n each, into seq[m]
-	std::vector<int32_t> len[2];
+	RawBuf<char> seq[2];          // mate 1 and mate 2 reads, back to back
+	RawBuf<int64_t> off[2];       // n each, into seq[m]
+	RawBuf<int32_t> len[2];
 	int max_len = 0;
 	int32_t handed = 0, done = 0;
 	int32_t inflight = 0;         // pieces handed to batches and not filed yet
@@ -101,6 +120,7 @@ struct hera_gpu_server {
 	std::condition_variable cv_work, cv_done;
 	std::deque<SrvChunk *> pending;
 	std::unordered_map<uint64_t, SrvChunk *> chunks;
+	std::vector<SrvChunk *> spare;   // released chunks whose buffers are reused
 	uint64_t next_ticket = 1;
 	bool stop = false;
 	unsigned long long *d_samples = nullptr;
@@ -131,6 +151,30 @@ static uint64_t srv_slot_bytes(uint64_t P)
 	b += 2 * P * (sizeof(hera_cand_rec) + 24) + 2 * P * 16 * 8;   // records, counts, pools
 	b += P / 8 * LCAP * (sizeof(int2) + sizeof(SswOut));          // rescue calls
 	return b + (64ull << 20);
+}
+
+// a released chunk's state cleared for reuse (its buffers are kept)
+static void srv_reset(SrvChunk &c)
+{
+	c.ticket = 0;
+	c.handed = c.done = c.inflight = c.batches = 0;
+	c.waited = false;
+	c.max_len = 0;
+	c.t_admit = c.t_done = -1;
+	c.segs.clear();
+	c.rc = HERA_GPU_OK;
+	c.err.clear();
+}
+
+// keep a released chunk's buffers for the next submit (a bounded number)
+static void srv_release(hera_gpu_server *S, SrvChunk *c)
+{
+	c->segs.clear();   // drop the batch outputs now
+	std::lock_guard<std::mutex> g(S->mu);
+	if (S->spare.size() < 4 * S->slots.size() + 8)
+		S->spare.push_back(c);
+	else
+		delete c;
 }
 
 // stage a batch's pieces into lane L: per piece the mate-1 and mate-2
@@ -382,14 +426,25 @@ extern "C" int hera_gpu_server_submit(hera_gpu_server *S, uint32_t sample, const
 		return HERA_GPU_EINVAL;
 	if (sample >= S->max_samples)
 		return fail(S->ctx, HERA_GPU_EINVAL, "sample id beyond max_samples");
-	SrvChunk *c = new SrvChunk();
+	SrvChunk *c = nullptr;
+	{
+		std::lock_guard<std::mutex> g(S->mu);
+		if (!S->spare.empty()) {
+			c = S->spare.back();
+			S->spare.pop_back();
+		}
+	}
+	if (c)
+		srv_reset(*c);
+	else
+		c = new SrvChunk();
 	c->sample = sample;
 	c->n = n;
 	const hera_gpu_reads *src[2] = {r1, r2};
 	for (int m = 0; m < 2; ++m) {
 		const hera_gpu_reads &R = *src[m];
-		c->off[m].resize((size_t)n);
-		c->len[m].resize((size_t)n);
+		c->off[m].need((size_t)n);
+		c->len[m].need((size_t)n);
 		int64_t total = 0;
 		bool contig = true;
 		for (int32_t i = 0; i < n; ++i) {
@@ -403,7 +458,7 @@ extern "C" int hera_gpu_server_submit(hera_gpu_server *S, uint32_t sample, const
 			c->max_len = Ln > c->max_len ? Ln : c->max_len;
 			total += Ln;
 		}
-		c->seq[m].resize((size_t)total + 1);
+		c->seq[m].need((size_t)total + 1);
 		if (contig && n > 0) {   // one copy of the block
 			pcopy(c->seq[m].data(), R.seq + R.off[0], (size_t)total);
 			for (int32_t i = 0; i < n; ++i) {
@@ -512,7 +567,7 @@ extern "C" int hera_gpu_server_wait(hera_gpu_server *S, uint64_t ticket, hera_gp
 	g.lock();
 	S->chunks.erase(ticket);
 	g.unlock();
-	delete c;
+	srv_release(S, c);
 	return HERA_GPU_OK;
 }
 
@@ -590,6 +645,8 @@ extern "C" void hera_gpu_server_destroy(hera_gpu_server *S)
 	}
 	for (auto &kv : S->chunks)
 		delete kv.second;
+	for (SrvChunk *c : S->spare)
+		delete c;
 	if (S->d_samples)
 		cudaFree(S->d_samples);
 	delete S;
