@@ -156,6 +156,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_stream.argtypes = [C.c_void_p]
     lib.hera_gpu_dpx_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double)]
     lib.hera_gpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    lib.hera_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
+    lib.hera_gpu_host_unregister.argtypes = [C.c_void_p]
     lib.hera_gpu_server_create.argtypes = [C.c_void_p, C.POINTER(_ServerOptions), C.POINTER(C.c_void_p)]
     lib.hera_gpu_server_submit.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_Reads), C.POINTER(_Reads),
                                            C.c_int32, C.POINTER(C.c_uint64)]
@@ -177,6 +179,20 @@ def dpx_peak(device: int = 0, ms: float = 50.0) -> float:
     if rc != HERA_GPU_OK:
         raise HeraGpuError(rc, "DPX probe failed")
     return out.value
+
+
+def host_register(a: np.ndarray) -> None:
+    """Page-lock a numpy array reused across calls (reads or result pools):
+    calls then copy it to or from the device without the pinned staging."""
+    lib = load_library()
+    rc = lib.hera_gpu_host_register(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes))
+    if rc != HERA_GPU_OK:
+        raise HeraGpuError(rc, "cudaHostRegister failed")
+
+
+def host_unregister(a: np.ndarray) -> None:
+    lib = load_library()
+    lib.hera_gpu_host_unregister(C.c_void_p(a.ctypes.data))
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -202,6 +218,10 @@ class Result:
         base = self.recs.ctypes.data if self.recs.shape[0] else 0
         self.c = _Result(base, _ptr(self.pos_pool), _ptr(self.p_pool), _ptr(self.op_pool),
                          _ptr(self.miss_pool), list_cap, op_cap, miss_cap, 0, 0, 0)
+
+    def arrays(self):
+        """The host arrays a call writes (records and pools)."""
+        return [self._rec_buf, self.pos_pool, self.p_pool, self.op_pool, self.miss_pool]
 
     def reuse(self, n_recs: int) -> "Result":
         """Make room for n_recs records, keeping the pools' storage."""

@@ -723,6 +723,20 @@ extern "C" void *hera_gpu_stream(hera_gpu_ctx *ctx)
 	return ctx ? (void *)ctx->stream : nullptr;
 }
 
+extern "C" int hera_gpu_host_register(void *p, size_t bytes)
+{
+	if (!p || bytes == 0)
+		return HERA_GPU_EINVAL;
+	return cudaHostRegister(p, bytes, cudaHostRegisterPortable) == cudaSuccess ? HERA_GPU_OK : HERA_GPU_ECUDA;
+}
+
+extern "C" int hera_gpu_host_unregister(void *p)
+{
+	if (!p)
+		return HERA_GPU_EINVAL;
+	return cudaHostUnregister(p) == cudaSuccess ? HERA_GPU_OK : HERA_GPU_ECUDA;
+}
+
 extern "C" int hera_gpu_get_tuning(const hera_gpu_ctx *ctx, hera_gpu_tuning *out)
 {
 	if (!ctx || !out)
@@ -1456,12 +1470,67 @@ static void pcopy(void *dst, const void *src, size_t bytes)
 	});
 }
 
+// true if host range [p, p + bytes) is page-locked (cudaHostAlloc, or
+// cudaHostRegister / hera_gpu_host_register): copies can then use it
+// directly instead of going through the lane's pinned staging
+static bool host_pinned(const void *p, size_t bytes)
+{
+	if (!p || bytes == 0)
+		return false;
+	cudaPointerAttributes a{}, e{};
+	if (cudaPointerGetAttributes(&a, p) != cudaSuccess ||
+	    cudaPointerGetAttributes(&e, static_cast<const char *>(p) + bytes - 1) != cudaSuccess) {
+		cudaGetLastError();
+		return false;
+	}
+	return a.type == cudaMemoryTypeHost && e.type == cudaMemoryTypeHost;
+}
+
+// records of a sub-batch rebased to the caller's pool offsets on the device
+__global__ void k_rebase_recs(hera_cand_rec *__restrict__ r, int n, uint32_t bl, uint32_t bo, uint32_t bm)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	for (int s = 0; s < 2; ++s) {
+		r[i].list_off[s] += bl;
+		r[i].cig_off[s] += bo;
+		r[i].miss_off[s] += bm;
+	}
+}
+
 // D2H of lane L's packed records into `out` at record rec0 and pool
 // offsets (bl, bo, bm), through the lane's pinned staging
 static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, uint64_t bo, uint64_t bm)
 {
 	cudaStream_t st = L.stream;
 	const int items = L.items;
+	// caller buffers that are page-locked take the records straight from
+	// the device (offsets rebased there); otherwise through the staging
+	if (host_pinned(out->recs + rec0, (size_t)items * sizeof(hera_cand_rec)) &&
+	    (!L.nl || (host_pinned(out->pos_pool + bl, L.nl * 4) && host_pinned(out->p_pool + bl, L.nl * 4))) &&
+	    (!L.no || host_pinned(out->op_pool + bo, L.no * 4)) && (!L.nm || host_pinned(out->miss_pool + bm, L.nm))) {
+		cudaEventRecord(L.ev[6], st);
+		if (items > 0)
+			k_rebase_recs<<<blocks_for(items, 256), 256, 0, st>>>(L.recs.p, items, (uint32_t)bl, (uint32_t)bo,
+									       (uint32_t)bm);
+		LK(cudaMemcpyAsync(out->recs + rec0, L.recs.p, items * sizeof(hera_cand_rec), cudaMemcpyDeviceToHost, st),
+		   "D2H");
+		if (L.nl) {
+			LK(cudaMemcpyAsync(out->pos_pool + bl, L.pos_pool.p, L.nl * 4, cudaMemcpyDeviceToHost, st), "D2H");
+			LK(cudaMemcpyAsync(out->p_pool + bl, L.p_pool.p, L.nl * 4, cudaMemcpyDeviceToHost, st), "D2H");
+		}
+		if (L.no)
+			LK(cudaMemcpyAsync(out->op_pool + bo, L.op_pool.p, L.no * 4, cudaMemcpyDeviceToHost, st), "D2H");
+		if (L.nm)
+			LK(cudaMemcpyAsync(out->miss_pool + bm, L.miss_pool.p, L.nm, cudaMemcpyDeviceToHost, st), "D2H");
+		cudaEventRecord(L.ev[7], st);
+		LK(cudaStreamSynchronize(st), "D2H");
+		float ms = 0;
+		cudaEventElapsedTime(&ms, L.ev[6], L.ev[7]);
+		L.timing.d2h_ms += ms;
+		return HERA_GPU_OK;
+	}
 	LK(L.h_recs.ensure(items + 1), "pinned records");
 	LK(L.h_pos.ensure(L.nl + 1), "pinned pools");
 	LK(L.h_p.ensure(L.nl + 1), "pinned pools");
@@ -1539,11 +1608,18 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 	LK(L.h_len.ensure((size_t)n * per), "pinned lengths");
 	const auto h0 = std::chrono::steady_clock::now();
 	int64_t o = 0;
+	// a contiguous, page-locked mate block goes to the device directly
+	int64_t reg_o[2] = {0, 0}, reg_len[2] = {0, 0};
+	const char *direct[2] = {nullptr, nullptr};
 	for (int m = 0; m < per; ++m) {
 		const hera_gpu_reads *r = src[m];
+		reg_o[m] = o;
 		if (contig[m] && n > 0) {
 			const int64_t len_m = r->off[lo + n - 1] + r->len[lo + n - 1] - r->off[lo];
-			pcopy(L.h_seq.p + o, r->seq + r->off[lo], (size_t)len_m);
+			if (host_pinned(r->seq + r->off[lo], (size_t)len_m))
+				direct[m] = r->seq + r->off[lo];
+			else
+				pcopy(L.h_seq.p + o, r->seq + r->off[lo], (size_t)len_m);
 			const int64_t shift = o - r->off[lo];
 			for (int32_t i = 0; i < n; ++i) {
 				L.h_off.p[(size_t)i * per + m] = r->off[lo + i] + shift;
@@ -1559,6 +1635,7 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 				o += Ln;
 			}
 		}
+		reg_len[m] = o - reg_o[m];
 	}
 	L.timing.host_stage_ms +=
 		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - h0).count();
@@ -1566,7 +1643,16 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 	LK(L.off.ensure((size_t)n * per), "device offsets");
 	LK(L.len.ensure((size_t)n * per), "device lengths");
 	cudaEventRecord(L.ev[0], st);
-	LK(cudaMemcpyAsync(L.seq.p, L.h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
+	if (!direct[0] && !direct[1]) {
+		LK(cudaMemcpyAsync(L.seq.p, L.h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
+	} else {   // per mate block: from the caller's memory or from the staging
+		for (int m = 0; m < per; ++m) {
+			const void *from = direct[m] ? (const void *)direct[m] : (const void *)(L.h_seq.p + reg_o[m]);
+			if (reg_len[m] > 0)
+				LK(cudaMemcpyAsync(L.seq.p + reg_o[m], from, (size_t)reg_len[m], cudaMemcpyHostToDevice, st),
+				   "H2D reads");
+		}
+	}
 	LK(cudaMemcpyAsync(L.off.p, L.h_off.p, (size_t)n * per * 8, cudaMemcpyHostToDevice, st), "H2D");
 	LK(cudaMemcpyAsync(L.len.p, L.h_len.p, (size_t)n * per * 4, cudaMemcpyHostToDevice, st), "H2D");
 	cudaEventRecord(L.ev[1], st);

@@ -292,6 +292,16 @@ int hera_gpu_get_tuning(const hera_gpu_ctx *ctx, hera_gpu_tuning *out);
  * build_blocks_per_sm in 1..16, rescue_warps_per_block in {1, 2, 4, 8}. */
 int hera_gpu_set_tuning(hera_gpu_ctx *ctx, const hera_gpu_tuning *in);
 
+/* Page-lock host memory that is reused across calls (read buffers, result
+ * pools), no counterpart in hera.  Calls detect page-locked inputs and
+ * outputs by themselves (this or cudaHostAlloc / cudaHostRegister memory):
+ * a contiguous mate block then goes to the device without the copy into
+ * the library's pinned staging, and records and pools come back straight
+ * into the result, their offsets rebased on the device.  Unregister before
+ * freeing the memory. */
+int hera_gpu_host_register(void *p, size_t bytes);
+int hera_gpu_host_unregister(void *p);
+
 /* ---- serving loop (no counterpart in hera) ----------------------------- *
  *
  * hera aligns one sample per process.  The server keeps one context's index

@@ -205,3 +205,25 @@ def test_autotuner_picks_a_timed_candidate(config1, oracle1):
         assert t["build_blocks_per_sm"] == min(trials, key=trials.get)
     finally:
         ctx.close()
+
+
+def test_page_locked_buffers_same_records(config1, gpu_ctx1):
+    """Page-locked reads and result pools take the direct copy paths (no
+    pinned staging; records rebased on the device) and give the same
+    records as pageable ones."""
+    from hera_b200 import api
+    ann, tx, _ = config1
+    r1, r2 = workloads.pairs("config4", ann, tx, 12000, seed=41)
+    ref = gpu_ctx1.align_pairs(r1, r2, 0)
+    out = gpu_ctx1.align_pairs(r1, r2, 0)
+    arrs = [r1.seq, r2.seq] + out.arrays()
+    for a in arrs:
+        api.host_register(a)
+    try:
+        res = gpu_ctx1.align_pairs(r1, r2, 0, out=out)
+        assert res.canonical() == ref.canonical()
+        res = gpu_ctx1.align_pairs(r1, r2, 0, out=out)   # a second call over the same buffers
+        assert res.canonical() == ref.canonical()
+    finally:
+        for a in arrs:
+            api.host_unregister(a)
