@@ -157,6 +157,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_dpx_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double)]
     lib.hera_gpu_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
     lib.hera_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
+    lib.hera_gpu_unit_ssw.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.POINTER(C.c_int32)]
     lib.hera_gpu_host_unregister.argtypes = [C.c_void_p]
     lib.hera_gpu_server_create.argtypes = [C.c_void_p, C.POINTER(_ServerOptions), C.POINTER(C.c_void_p)]
     lib.hera_gpu_server_submit.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_Reads), C.POINTER(_Reads),
@@ -193,6 +196,35 @@ def host_register(a: np.ndarray) -> None:
 def host_unregister(a: np.ndarray) -> None:
     lib = load_library()
     lib.hera_gpu_host_unregister(C.c_void_p(a.ctypes.data))
+
+
+def unit_ssw(refs, reads, device: int = 0):
+    """ssw_align as the mate-rescue kernel computes it, for lists of ASCII
+    (window, read) pairs: [(score, skip, cigar, miss)] (a kernel-level check
+    against the reference's golden vectors)."""
+    lib = load_library()
+    n = len(refs)
+    rcat = np.frombuffer(b"".join(refs), np.uint8).copy()
+    qcat = np.frombuffer(b"".join(reads), np.uint8).copy()
+    roff = np.zeros(n + 1, np.int64)
+    roff[1:] = np.cumsum([len(r) for r in refs])
+    qoff = np.zeros(n + 1, np.int64)
+    qoff[1:] = np.cumsum([len(q) for q in reads])
+    score, skip = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    ops = np.zeros(n * 96, np.uint32)
+    miss = np.zeros(n * 96, np.uint8)
+    n_ops, n_miss = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    flags = C.c_int32(0)
+    rc = lib.hera_gpu_unit_ssw(device, _ptr(rcat), _ptr(roff), _ptr(qcat), _ptr(qoff), n, _ptr(score), _ptr(skip),
+                               _ptr(ops), _ptr(n_ops), _ptr(miss), _ptr(n_miss), C.byref(flags))
+    if rc != HERA_GPU_OK:
+        raise HeraGpuError(rc, "unit ssw failed")
+    out = []
+    for i in range(n):
+        o = ops[i * 96:i * 96 + min(int(n_ops[i]), 96)]
+        cig = "".join(f"{int(x) >> 4}{CIGAR_CHARS[int(x) & 15]}" for x in o)
+        out.append((int(score[i]), int(skip[i]), cig, bytes(miss[i * 96:i * 96 + min(int(n_miss[i]), 96)])))
+    return out, flags.value
 
 
 def _ptr(a: np.ndarray) -> int:

@@ -1020,12 +1020,11 @@ __device__ __forceinline__ uint8_t read_code(const uint8_t *code, int64_t o, int
 	return orient ? comp_code(code[o + L - 1 - x]) : code[o + x];
 }
 
-// rows per lane for a read of length L: ceil(L/32) rounded up to even
-// (two rows share a register)
+// rows per lane used for a read of length L (instantiated widths only)
 __host__ __device__ inline int ssw_rows(int L)
 {
 	const int R = (L + 31) / 32;
-	return R < 2 ? 2 : (R + 1) & ~1;
+	return R <= 6 ? (R < 1 ? 1 : R) : (R <= 8 ? 8 : 10);
 }
 
 // shared-memory layout of one warp's area
@@ -1039,91 +1038,71 @@ __host__ __device__ inline size_t ssw_smem_per_warp(int max_len)
 	return SSW_REF_B + SSW_RD_B + SSW_CIG_B + SSW_NCK * col + (((SSW_CK + 1) * col + 15) / 16) * 16;
 }
 
-// One block of the sweep, rows skewed: global row g (lane l's row i is
-// g = l*R + i, R = 2*NP) works on column y = nb + t - g + 1 at step t, so
-// all cells of a step are independent and two rows share a register as
-// 16-bit halves (pair j = rows 2j, 2j+1).  Row g is computed at steps
-// g .. g+ncol-1 and holds its left-edge value (column nb) before.
-//   up   (g-1, y)   : row g-1 after the previous step
-//   left (g, y-1)   : row g after the previous step
-//   diag (g-1, y-1) : the previous step's up
-// Row -1 of lane l is lane l-1's last row, by shuffle.
-template <int NP, bool TRACK, typename Store>
-__device__ __forceinline__ void ssw_sweep(const uint8_t *__restrict__ ref_s, const uint32_t (&RD)[NP],
-					  const uint32_t (&RM)[NP], int nb, int ncol, int G, uint32_t (&H)[NP],
-					  uint32_t (&BV)[NP], uint32_t (&BY)[NP], Store store)
+// One block of the sweep: columns nb+1 .. nb+ncol, starting from the column
+// nb held in Hl (lane's rows) and bot0 (its last row); column values go to
+// `store(y, lane rows)` and the running maximum to best_*.
+template <int R, bool TRACK, typename Store>
+__device__ __forceinline__ void ssw_sweep(const uint8_t *__restrict__ ref_s, const uint8_t (&rdl)[R], int L,
+					  int nb, int ncol, int nact, int (&Hl)[R], int &best_v, int &best_y,
+					  int &best_x, Store store)
 {
 	const unsigned FULL = 0xffffffffu;
-	constexpr int R = 2 * NP;
 	const int lane = threadIdx.x & 31;
-	const int g0 = lane * R;
-	const uint32_t M4 = 0xfffcfffcu, C253 = 0x00fd00fdu;
-	uint32_t U[NP], RW[NP];
-	{
-		uint32_t prev = 0;   // row -1
-#pragma unroll
-		for (int j = 0; j < NP; ++j) {
-			U[j] = __byte_perm(prev, H[j], 0x5432);
-			prev = H[j];
-			RW[j] = 0;
-		}
-	}
-	const int steps = ncol > 0 ? ncol + G - 1 : 0;
+	const int x0 = lane * R;
+	// `bot` as of step -1: lane 0 then stands on the left-edge column nb
+	// (its saved last row feeds lane 1's first diagonal), the others before it
+	int bot = lane == 0 ? Hl[R - 1] : 0, up_prev = 0;
+	const int steps = ncol > 0 ? ncol + nact - 1 : 0;
 	for (int t = 0; t < steps; ++t) {
-		uint32_t up_in = __shfl_up_sync(FULL, H[NP - 1] >> 16, 1);
+		const int y = nb + t - lane + 1;
+		int up_in = __shfl_up_sync(FULL, bot, 1);
 		if (lane == 0)
 			up_in = 0;
-		// reference codes: each row takes the one of the row above, row 0
-		// the next byte of the window
-		int ri = nb + t - g0;
-		ri = ri < 0 ? 0 : (ri > MAX_FRAG + 31 ? MAX_FRAG + 31 : ri);
-		const uint32_t rnew = ref_s[ri];
-		const bool ramp = t < G || t >= ncol;   // not every row is inside the block
-		uint32_t prevH = up_in << 16, prevR = rnew << 16;
+		const int diag_in = up_prev;
+		up_prev = up_in;
+		if (y > nb && y <= nb + ncol) {
+			const uint8_t rc = ref_s[y - 1];
+			int d = diag_in, up = up_in, cmax = 0;
 #pragma unroll
-		for (int j = 0; j < NP; ++j) {
-			const uint32_t up = __byte_perm(prevH, H[j], 0x5432);
-			const uint32_t rw = __byte_perm(prevR, RW[j], 0x5432);
-			prevH = H[j];
-			prevR = RW[j];
-			RW[j] = rw;
-			// +1 for equal codes (N == N included), -2 otherwise
-			const uint32_t z = __vimin3_u16x2(rw ^ RD[j], 0x00010001u, 0x00010001u);
-			const uint32_t sc = z * 0xfffdu + 0x00010001u;
-			const uint32_t a = __viaddmin_s16x2(U[j], sc, C253);
-			const uint32_t t1 = __viaddmax_s16x2(H[j], M4, a);
-			uint32_t v = __viaddmax_s16x2_relu(up, M4, t1) & RM[j];
-			U[j] = up;
-			if (ramp) {
-				const int g = g0 + 2 * j;
-				const uint32_t act = ((unsigned)(t - g) < (unsigned)ncol ? 0x0000ffffu : 0u) |
-						     ((unsigned)(t - g - 1) < (unsigned)ncol ? 0xffff0000u : 0u);
-				v &= act;
-				H[j] = v | (H[j] & ~act);
-			} else {
-				H[j] = v;
+			for (int r = 0; r < R; ++r) {
+				const int left = Hl[r];
+				// max(0, min(255, d + 3*eq) - 2, left - 4, up - 4), d <= 253
+				const int a = __viaddmin_s32(d, rdl[r] == rc ? 1 : -2, 253);
+				int v = __vimax3_s32_relu(a, left - 4, up - 4);
+				if (x0 + r >= L)
+					v = 0;
+				d = left;
+				Hl[r] = v;
+				up = v;
+				cmax = __vimax_s32_relu(cmax, v);
 			}
-			if (TRACK) {
-				bool ph, pl;
-				BV[j] = __vibmax_s16x2(BV[j], v, &ph, &pl);
-				const uint32_t T = (uint32_t)t * 0x00010001u;
-				const uint32_t hi = ph ? BY[j] : T, lo = pl ? BY[j] : T;
-				BY[j] = __byte_perm(lo, hi, 0x7610);
+			if (TRACK && cmax > best_v) {   // first row of this column reaching it
+				int fx = 0;
+#pragma unroll
+				for (int r = R - 1; r >= 0; --r)
+					if (Hl[r] == cmax)
+						fx = r;
+				best_v = cmax;
+				best_y = y;
+				best_x = x0 + fx;
 			}
+			bot = Hl[R - 1];
+			store(y, Hl);
+		} else {
+			// column nb is the block's left edge: the lane's saved last row
+			bot = y == nb ? Hl[R - 1] : 0;
 		}
-		store(t, H);
 	}
 }
 
 // Called by all 32 lanes of a warp; `sm` is the warp's shared-memory area
 // (ssw_smem_per_warp(L) bytes at least).  Fills `out` (lane 0 writes the
 // scalars; the CIGAR is copied by the warp).
-template <int NP>
+template <int R>
 __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff, int L,
 			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out, int &flags)
 {
 	const unsigned FULL = 0xffffffffu;
-	constexpr int R = 2 * NP;
 	const int lane = threadIdx.x & 31;
 	const int x0 = lane * R;
 	const int COL = 32 * R;
@@ -1140,47 +1119,24 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 	if (lane == 0)
 		cig.n = cig.nm = 0;
 	__syncwarp();
-	uint32_t RD[NP], RM[NP], H[NP], BV[NP], BY[NP];
+	uint8_t rdl[R];
+	int Hl[R];
 #pragma unroll
-	for (int j = 0; j < NP; ++j) {
-		const int a = x0 + 2 * j, b = a + 1;
-		RD[j] = (uint32_t)(a < L ? rd_s[a] : 5) | (uint32_t)(b < L ? rd_s[b] : 5) << 16;
-		RM[j] = (a < L ? 0x0000ffffu : 0u) | (b < L ? 0xffff0000u : 0u);
-		H[j] = BV[j] = BY[j] = 0;
+	for (int r = 0; r < R; ++r) {
+		rdl[r] = x0 + r < L ? rd_s[x0 + r] : (uint8_t)5;
+		Hl[r] = 0;
 	}
 	const int nact = (L + R - 1) / R;   // lanes holding read rows
-	const int G = nact * R;             // rows the skewed sweep spans
-	ssw_sweep<NP, true>(ref_s, RD, RM, 0, ln, G, H, BV, BY, [&](int t, const uint32_t (&Hs)[NP]) {
-		// save column y = t - g + 1 of the row g that reaches a multiple of SSW_CK
-		const int i = (t + 1 - x0) & (SSW_CK - 1);
-		if (i < R) {
-			const int g = x0 + i;
-			if ((unsigned)(t - g) < (unsigned)ln) {
-				uint32_t w = 0;
+	int best_v = 0, best_y = 0, best_x = 0;
+	ssw_sweep<R, true>(ref_s, rdl, L, 0, ln, nact, Hl, best_v, best_y, best_x, [&](int y, const int (&H)[R]) {
+		if ((y & (SSW_CK - 1)) == 0) {
+			uint8_t *c = ck + (size_t)(y / SSW_CK) * COL + x0;
 #pragma unroll
-				for (int j = 0; j < NP; ++j)
-					if ((i >> 1) == j)
-						w = Hs[j];
-				ck[(size_t)((t - g + 1) / SSW_CK) * COL + g] = (uint8_t)(w >> (16 * (i & 1)));
-			}
+			for (int r = 0; r < R; ++r)
+				c[r] = (uint8_t)H[r];
 		}
 	});
-	// per row: its max and the first column reaching it; the call's end is
-	// the max over all cells, the first column holding it, the first row there
-	int best_v = 0, best_y = 0x7fffffff, best_x = 0x7fffffff;
-#pragma unroll
-	for (int j = 0; j < NP; ++j)
-#pragma unroll
-		for (int h = 0; h < 2; ++h) {
-			const int v = (int)((BV[j] >> (16 * h)) & 0xffffu);
-			const int g = x0 + 2 * j + h;
-			const int y = (int)((BY[j] >> (16 * h)) & 0xffffu) - g + 1;
-			if (v > best_v || (v == best_v && (y < best_y || (y == best_y && g < best_x)))) {
-				best_v = v;
-				best_y = y;
-				best_x = g;
-			}
-		}
+	// max over all cells; first column reaching it; first row in that column
 	const int max_v = __reduce_max_sync(FULL, best_v);
 	const int min_y = __reduce_min_sync(FULL, best_v == max_v ? best_y : 0x7fffffff);
 	const int min_x = __reduce_min_sync(FULL, (best_v == max_v && best_y == min_y) ? best_x : 0x7fffffff);
@@ -1197,26 +1153,20 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 	auto load_block = [&](int b) {
 		nb = b;
 		__syncwarp();
-		uint32_t H0[NP], bv[NP], by[NP];
+		int H0[R];
 		const uint8_t *c0 = ck + (size_t)(b / SSW_CK) * COL;
 #pragma unroll
-		for (int j = 0; j < NP; ++j) {
-			const uint32_t lo = b == 0 ? 0u : c0[x0 + 2 * j], hi = b == 0 ? 0u : c0[x0 + 2 * j + 1];
-			H0[j] = lo | hi << 16;
-			tb[x0 + 2 * j] = (uint8_t)lo;
-			tb[x0 + 2 * j + 1] = (uint8_t)hi;
-			bv[j] = by[j] = 0;
+		for (int r = 0; r < R; ++r) {
+			H0[r] = b == 0 ? 0 : c0[x0 + r];
+			tb[x0 + r] = (uint8_t)H0[r];
 		}
+		int bv = 0, by = 0, bx = 0;
 		const int ncol = ln - b < SSW_CK ? ln - b : SSW_CK;
-		ssw_sweep<NP, false>(ref_s, RD, RM, b, ncol, G, H0, bv, by, [&](int t, const uint32_t (&Hs)[NP]) {
+		ssw_sweep<R, false>(ref_s, rdl, L, b, ncol, nact, H0, bv, by, bx, [&](int y, const int (&H)[R]) {
+			uint8_t *c = tb + (size_t)(y - b) * COL + x0;
 #pragma unroll
-			for (int j = 0; j < NP; ++j)
-#pragma unroll
-				for (int h = 0; h < 2; ++h) {
-					const int g = x0 + 2 * j + h;
-					if ((unsigned)(t - g) < (unsigned)ncol)
-						tb[(size_t)(t - g + 1) * COL + g] = (uint8_t)(Hs[j] >> (16 * h));
-				}
+			for (int r = 0; r < R; ++r)
+				c[r] = (uint8_t)H[r];
 		});
 		__syncwarp();
 	};
@@ -1335,11 +1285,14 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 				int &flags)
 {
 	switch (ssw_rows(L)) {
-	case 2: ssw_warp_r<1>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
-	case 4: ssw_warp_r<2>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
-	case 6: ssw_warp_r<3>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
-	case 8: ssw_warp_r<4>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
-	default: ssw_warp_r<5>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 1: ssw_warp_r<1>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 2: ssw_warp_r<2>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 3: ssw_warp_r<3>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 4: ssw_warp_r<4>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 5: ssw_warp_r<5>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 6: ssw_warp_r<6>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	case 8: ssw_warp_r<8>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
+	default: ssw_warp_r<10>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
 	}
 }
 

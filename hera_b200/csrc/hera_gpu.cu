@@ -38,6 +38,14 @@ namespace {
 
 constexpr int TPB = 128;
 
+// bytes of dynamic shared memory the running block was launched with
+__device__ __forceinline__ unsigned dyn_smem_bytes()
+{
+	unsigned r;
+	asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+	return r;
+}
+
 struct RmReq {
 	int32_t pair;
 	int16_t c, str;
@@ -340,7 +348,8 @@ __global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *
 	if (ln < 0)
 		ln = 0;
 	int flags = 0;
-	if (L < 0 || L > b.max_len) {   // longer than the batch's stated maximum: no room in the area
+	if (L < 0 || L > b.max_len || (size_t)((threadIdx.x >> 5) + 1) * per > dyn_smem_bytes()) {
+		// longer than the batch's stated maximum, or no room for the area
 		if ((threadIdx.x & 31) == 0) {
 			out[c0 + wl].ok = 0;
 			out[c0 + wl].cig.n = out[c0 + wl].cig.nm = 0;
@@ -2254,6 +2263,115 @@ extern "C" int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, in
 				     hera_candidate **out)
 {
 	return align_dropin(ctx, reads, nullptr, n, write_bam, out);
+}
+
+// ---- kernel-level check of the mate-rescue DP ----------------------------
+
+namespace {
+__global__ void __launch_bounds__(RESCUE_TPB) k_unit_ssw(DevIndex ix, const int64_t *__restrict__ ref_off,
+							  const uint8_t *__restrict__ rcode, const int64_t *__restrict__ read_off,
+							  int n, SswOut *__restrict__ out, int per, int *__restrict__ flags)
+{
+	extern __shared__ __align__(16) uint8_t ssw_sm[];
+	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (w >= n)
+		return;
+	const int ln = (int)(ref_off[w + 1] - ref_off[w]), L = (int)(read_off[w + 1] - read_off[w]);
+	int f = 0;
+	if ((size_t)((threadIdx.x >> 5) + 1) * per > dyn_smem_bytes() || (size_t)per < ssw_smem_per_warp(L)) {
+		if ((threadIdx.x & 31) == 0)
+			atomicOr(flags, F_SCRATCH);
+		return;
+	}
+	ssw_warp(ix, (uint32_t)ref_off[w], ln, rcode, read_off[w], L, 0, 0, 0xffffffffu,
+		 ssw_sm + (size_t)(threadIdx.x >> 5) * per, out[w], f);
+	if ((threadIdx.x & 31) == 0 && f)
+		atomicOr(flags, f);
+}
+}  // namespace
+
+extern "C" int hera_gpu_unit_ssw(int device, const char *refs, const int64_t *ref_off, const char *reads,
+				 const int64_t *read_off, int32_t n, int32_t *score, int32_t *skip, uint32_t *ops,
+				 int32_t *n_ops, char *miss, int32_t *n_miss, int32_t *flags)
+{
+	if (!refs || !ref_off || !reads || !read_off || n < 0 || !score || !skip || !ops || !n_ops || !miss ||
+	    !n_miss || !flags)
+		return HERA_GPU_EINVAL;
+	*flags = 0;
+	if (n == 0)
+		return HERA_GPU_OK;
+	if (cudaSetDevice(device) != cudaSuccess)
+		return HERA_GPU_ENODEV;
+	int max_len = 1;
+	for (int i = 0; i < n; ++i) {
+		const int64_t ln = ref_off[i + 1] - ref_off[i], L = read_off[i + 1] - read_off[i];
+		if (ln < 0 || ln > MAX_FRAG || L < 0 || L > MAX_READ)
+			return HERA_GPU_EINVAL;
+		max_len = L > max_len ? (int)L : max_len;
+	}
+	const int64_t rb = ref_off[n], qb = read_off[n];
+	std::vector<uint8_t> seq((size_t)rb + 64, 0);
+	memcpy(seq.data(), refs, (size_t)rb);
+	uint8_t *d = nullptr;
+	const size_t per = ssw_smem_per_warp(max_len);
+	const size_t bytes_s = 2 * ((size_t)rb + 64) + 2 * ((size_t)qb + 64);
+	const size_t off_s = (bytes_s + 255) & ~(size_t)255;
+	const size_t need = off_s + (size_t)(n + 1) * 16 + 256 + (size_t)n * sizeof(SswOut);
+	if (cudaMalloc(&d, need) != cudaSuccess)
+		return HERA_GPU_ENOMEM;
+	uint8_t *d_seq = d, *d_rcode = d_seq + rb + 64, *d_read = d_rcode + rb + 64, *d_qcode = d_read + qb + 64;
+	int64_t *d_roff = reinterpret_cast<int64_t *>(d + off_s);
+	int64_t *d_qoff = d_roff + n + 1;
+	int *d_flags = reinterpret_cast<int *>(d_qoff + n + 1);
+	SswOut *d_out = reinterpret_cast<SswOut *>(reinterpret_cast<uint8_t *>(d_flags) + 256);
+	int rc = HERA_GPU_OK;
+	cudaGetLastError();
+	if (cudaMemcpy(d_seq, seq.data(), rb + 64, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d_read, reads, qb, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemset(d_read + qb, 0, 64) != cudaSuccess ||
+	    cudaMemcpy(d_roff, ref_off, (n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d_qoff, read_off, (n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemset(d_flags, 0, 4) != cudaSuccess)
+		rc = HERA_GPU_ECUDA;
+	if (rc == HERA_GPU_OK) {
+		k_codes<<<64, 256>>>(d_seq, d_rcode, rb + 64);
+		k_codes<<<64, 256>>>(d_read, d_qcode, qb + 64);
+		DevIndex ix{};
+		ix.code = d_rcode;
+		ix.seq = d_seq;
+		const int wpb = 4;
+		const cudaError_t ea =
+			cudaFuncSetAttribute(k_unit_ssw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * per));
+		if (ea != cudaSuccess)
+			fprintf(stderr, "hera_gpu_unit_ssw: shared-memory size: %s\n", cudaGetErrorString(ea));
+		k_unit_ssw<<<(n + wpb - 1) / wpb, 32 * wpb, wpb * per>>>(ix, d_roff, d_qcode, d_qoff, n, d_out, (int)per,
+									   d_flags);
+		std::vector<SswOut> h((size_t)n);
+		cudaError_t e = cudaGetLastError();
+		if (e == cudaSuccess)
+			e = cudaDeviceSynchronize();
+		if (e == cudaSuccess)
+			e = cudaMemcpy(h.data(), d_out, n * sizeof(SswOut), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess)
+			e = cudaMemcpy(flags, d_flags, 4, cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) {
+			fprintf(stderr, "hera_gpu_unit_ssw: %s\n", cudaGetErrorString(e));
+			rc = HERA_GPU_ECUDA;
+		} else {
+			for (int i = 0; i < n; ++i) {
+				score[i] = h[i].score;
+				skip[i] = h[i].skip;
+				n_ops[i] = h[i].cig.n;
+				n_miss[i] = h[i].cig.nm;
+				for (int k = 0; k < h[i].cig.n && k < CCAP; ++k)
+					ops[(size_t)i * CCAP + k] = h[i].cig.op[k];
+				for (int k = 0; k < h[i].cig.nm && k < MCAP; ++k)
+					miss[(size_t)i * MCAP + k] = (char)h[i].cig.miss[k];
+			}
+		}
+	}
+	cudaFree(d);
+	return rc;
 }
 
 // ---- DPX throughput probe ----------------------------------------------

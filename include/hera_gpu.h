@@ -377,6 +377,16 @@ int hera_gpu_server_get_stats(hera_gpu_server *s, hera_gpu_server_stats *out);
  * not yet waited for are dropped. */
 void hera_gpu_server_destroy(hera_gpu_server *s);
 
+/* Kernel-level check, no counterpart in hera: ssw_align (src/ssw.c:81-321)
+ * as the mate-rescue kernel computes it, for n (window, read) cases given as
+ * ASCII strings back to back (refs[ref_off[i] .. ref_off[i+1]), same for
+ * reads; windows up to 1000 bases, reads up to HERA_GPU_MAX_READ).  Per case:
+ * score, skip, and the CIGAR (ops[i*96 ..], n_ops[i]; miss[i*96 ..],
+ * n_miss[i]); *flags ORs capacity flags.  Allocates device memory. */
+int hera_gpu_unit_ssw(int device, const char *refs, const int64_t *ref_off, const char *reads,
+		      const int64_t *read_off, int32_t n, int32_t *score, int32_t *skip, uint32_t *ops,
+		      int32_t *n_ops, char *miss, int32_t *n_miss, int32_t *flags);
+
 /* Measurement helper, no counterpart in hera: the device's throughput of
  * the DPX instruction the gap DP's cell update is built on (packed 16x2
  * add-then-min, __viaddmin_s16x2), measured with independent chains on

@@ -1,0 +1,37 @@
+"""Kernel-level GPU parity: the mate-rescue DP (ssw_align) as the device
+computes it, against the golden vectors the reference produced
+(tests/golden/ssw_align.npz): score, skip, CIGAR and miss chars."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _strs(a, off):
+    return [bytes(a[off[i]:off[i + 1]]) for i in range(len(off) - 1)]
+
+
+def test_rescue_dp_golden():
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    d = np.load(os.path.join(GOLD, "ssw_align.npz"))
+    refs, reads = _strs(d["ref"], d["ref_off"]), _strs(d["read"], d["read_off"])
+    cig, miss = _strs(d["cigar"], d["cigar_off"]), _strs(d["miss"], d["miss_off"])
+    got, flags = api.unit_ssw(refs, reads)
+    bad, capped = [], 0
+    for i, g in enumerate(got):
+        want = (int(d["score"][i]), int(d["skip"][i]), cig[i].decode(), miss[i])
+        if g != want:
+            # the device keeps at most 96 CIGAR ops / miss chars (it reports
+            # the overflow instead of a wrong record)
+            if cig[i].decode().count("M") + cig[i].decode().count("X") + cig[i].decode().count("I") + \
+                    cig[i].decode().count("D") + cig[i].decode().count("S") > 96 or len(miss[i]) > 96:
+                capped += 1
+                continue
+            bad.append(i)
+    assert not bad, f"{len(bad)} of {len(got)} rescue DPs differ; first {bad[0]}: {got[bad[0]]}"
+    assert capped <= 8
