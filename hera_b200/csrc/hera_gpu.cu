@@ -122,31 +122,69 @@ __global__ void k_rc(const uint8_t *__restrict__ code, const int64_t *__restrict
 		rc[o + x] = comp_code(code[o + L - 1 - x]);
 }
 
-// seed_probe: thread per (read, strand, seed) at spacing 31
-__global__ void k_seed(DevIndex ix, const uint8_t *__restrict__ code, const int64_t *__restrict__ off,
-		       const int32_t *__restrict__ len, int n_reads, int spr, uint2 *__restrict__ hits,
-		       unsigned long long *__restrict__ stats)
+// seed_probe: thread per (read, strand) over its S seeds at spacing 31.
+// The S lookups are independent, so their bucket-offset loads and then
+// their binary-search probes are issued together (hash_get,
+// src/hash_align.c:862-895; the same search and probe count as probe()).
+template <int S>
+__global__ void __launch_bounds__(256) k_seed(DevIndex ix, const uint8_t *__restrict__ code,
+					       const int64_t *__restrict__ off, const int32_t *__restrict__ len,
+					       int n_reads, uint2 *__restrict__ hits,
+					       unsigned long long *__restrict__ stats)
 {
 	const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-	const int64_t total = (int64_t)n_reads * 2 * spr;
 	uint32_t np = 0, found = 0;
-	const int j = (int)(t % spr);
-	const int64_t ro = t / spr;
-	const int orient = (int)(ro & 1);
-	const int ri = (int)(ro >> 1);
-	const int L = t < total ? len[ri] : 0;
-	const int i = j * KMER;
-	uint2 h = make_uint2(0, 0);
-	if (t < total && i + KMER <= L && j < spr) {
+	if (t < (int64_t)n_reads * 2) {
+		const int orient = (int)(t & 1);
+		const int ri = (int)(t >> 1);
+		const int L = len[ri];
 		const uint8_t *src = code + off[ri];
-		// orientation 1: the reverse complement's k-mer at i covers bytes
-		// [L-1-i-30, L-1-i] of the read
-		const uint64_t id = orient == 0 ? kmer_words(src + i, false) : kmer_words(src + (L - KMER - i), true);
-		h = probe(ix, id, &np);
-		found = h.y > 0;
+		uint64_t id[S];
+		uint32_t lo[S], hi[S];
+		uint2 h[S];
+#pragma unroll
+		for (int j = 0; j < S; ++j) {
+			const int i = j * KMER;
+			h[j] = make_uint2(0, 0);
+			lo[j] = hi[j] = 0;
+			id[j] = 0;
+			if (i + KMER <= L) {
+				// orientation 1: the reverse complement's k-mer at i covers
+				// bytes [L-1-i-30, L-1-i] of the read
+				id[j] = orient == 0 ? kmer_words(src + i, false) : kmer_words(src + (L - KMER - i), true);
+				const uint32_t mod = (uint32_t)(id[j] & HMASK);
+				lo[j] = __ldg(ix.boff + mod);
+				hi[j] = __ldg(ix.boff + mod + 1);
+			}
+		}
+		bool more = true;
+		while (more) {
+			more = false;
+#pragma unroll
+			for (int j = 0; j < S; ++j) {
+				if (lo[j] < hi[j]) {
+					const uint32_t mid = (lo[j] + hi[j]) >> 1;
+					++np;
+					const uint4 b = __ldg(ix.bk + mid);
+					const uint64_t bid = ((uint64_t)b.y << 32) | b.x;
+					if (bid == id[j]) {
+						h[j] = make_uint2(b.z, b.w - b.z);
+						hi[j] = lo[j];
+					} else if (bid > id[j]) {
+						hi[j] = mid;
+					} else {
+						lo[j] = mid + 1;
+					}
+					more |= lo[j] < hi[j];
+				}
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < S; ++j) {
+			hits[t * S + j] = h[j];
+			found += h[j].y > 0;
+		}
 	}
-	if (t < total)
-		hits[t] = h;
 	warp_stat(stats + ST_PROBES, np);
 	warp_stat(stats + ST_SEED_HITS, found);
 }
@@ -1193,8 +1231,18 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 		LK(L.hits.ensure((size_t)n_reads * 2 * spr), "seed hits");
 		const int64_t ns = (int64_t)n_reads * 2 * spr;
 		cudaEventRecord(L.ev[8], st);
-		k_seed<<<blocks_for(ns, 256), 256, 0, st>>>(ctx->ix, L.code.p, d_off, d_len, n_reads, spr, L.hits.p,
-							     d_stats);
+		const unsigned g = blocks_for((int64_t)n_reads * 2, 256);
+		switch (spr) {
+#define SEED_CASE(S)                                                                                              \
+	case S:                                                                                                   \
+		k_seed<S><<<g, 256, 0, st>>>(ctx->ix, L.code.p, d_off, d_len, n_reads, L.hits.p, d_stats);       \
+		break;
+		SEED_CASE(1) SEED_CASE(2) SEED_CASE(3) SEED_CASE(4) SEED_CASE(5)
+		SEED_CASE(6) SEED_CASE(7) SEED_CASE(8) SEED_CASE(9) SEED_CASE(10)
+#undef SEED_CASE
+		default:
+			return set_err(L.err, HERA_GPU_EINVAL, "seeds per read beyond HERA_GPU_MAX_READ");
+		}
 		cudaEventRecord(L.ev[9], st);
 		++launches;
 		T.lookups += (uint64_t)ns;
