@@ -287,6 +287,7 @@ struct BuildWork {
 	Chain ch[LCH];
 	JobSlot js[LJS];
 	DpJob jb[LJ];
+	uint64_t jkey[LJ];   // a job's (query offset, lengths, error cap) in one word, for the dedup scan
 };
 
 // one get_position call of the round (list position t)
@@ -345,20 +346,19 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 			flags |= F_ACAP;
 			return;
 		}
+		const uint64_t key = (uint64_t)j.qoff | (uint64_t)j.len << 16 | (uint64_t)j.ref_len << 32 |
+				     (uint64_t)(uint8_t)j.err << 48;
 		int hit = -1;
-		for (int q = 0; q < nj && hit < 0; ++q) {
-			const DpJob &o = w.jb[q];
-			if (o.qoff != j.qoff || o.len != j.len || o.ref_len != j.ref_len || o.err != j.err)
-				continue;
-			if (bytes_equal(b.ix.seq, o.rstart, j.rstart, j.ref_len))
+		for (int q = 0; q < nj && hit < 0; ++q)
+			if (w.jkey[q] == key && bytes_equal(b.ix.seq, w.jb[q].rstart, j.rstart, j.ref_len))
 				hit = q;
-		}
 		if (hit < 0) {
 			if (nj >= LJ) {
 				flags |= F_ACAP;
 				return;
 			}
 			w.jb[nj] = j;
+			w.jkey[nj] = key;
 			hit = nj++;
 		}
 		w.js[ns].job = hit;

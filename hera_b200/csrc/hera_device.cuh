@@ -29,7 +29,7 @@ enum : int { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4, OP_X = 8 };
 // capacity / consistency flags (OR-ed into one word per batch)
 enum : int {
 	F_ACAP = 1, F_LCAP = 2, F_CCAP = 4, F_MCAP = 8, F_BAND = 16, F_READ = 32,
-	F_SCRATCH = 64, F_QUEUE = 128
+	F_SCRATCH = 64, F_QUEUE = 128, F_SSW = 256
 };
 
 struct DevIndex {
@@ -1141,6 +1141,19 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 	const int min_y = __reduce_min_sync(FULL, best_v == max_v ? best_y : 0x7fffffff);
 	const int min_x = __reduce_min_sync(FULL, (best_v == max_v && best_y == min_y) ? best_x : 0x7fffffff);
 	__syncwarp();
+	// self-check of the end cell before the walk (a bad one reports flag
+	// F_SSW instead of reading outside the warp's area)
+	if (max_v > 0 && (min_y < 1 || min_y > ln || min_x < 0 || min_x >= L)) {
+		if (lane == 0) {
+			out.score = -1002;
+			out.skip = min_y;
+			out.pstart = min_x;
+			out.ok = 0;
+			out.cig.n = out.cig.nm = 0;
+			flags |= F_SSW;
+		}
+		return;
+	}
 
 	const uint8_t *ra = ix.seq + wstart;
 	const bool w0 = lane == 0;
@@ -1149,8 +1162,12 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 			cig_add(cig, type, n, mc, flags);
 	};
 	// block of saved columns [nb, nb + SSW_CK] around the walk
-	int nb = -1;
+	int nb = -1, bad_walk = 0;
 	auto load_block = [&](int b) {
+		if (b < 0 || b >= ln || (b & (SSW_CK - 1)) || b / SSW_CK >= SSW_NCK) {
+			bad_walk = 3;
+			return;
+		}
 		nb = b;
 		__syncwarp();
 		int H0[R];
@@ -1170,7 +1187,15 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 		});
 		__syncwarp();
 	};
-	auto HV = [&](int x, int yy) -> int { return yy == 0 ? 0 : tb[(size_t)(yy - nb) * COL + x]; };
+	auto HV = [&](int x, int yy) -> int {
+		if (yy == 0)
+			return 0;
+		if (yy - nb < 0 || yy - nb > SSW_CK || x < 0 || x >= COL) {
+			bad_walk = 5;
+			return 0;
+		}
+		return tb[(size_t)(yy - nb) * COL + x];
+	};
 	const int end_ref = max_v > 0 ? min_y - 1 : -1;
 	int begin_ref = end_ref, score = 0, end_read = L - 1;
 	if (max_v < (L >> 2) || max_v == 0) {
@@ -1202,6 +1227,10 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 		load_block((y_pos - 1) / SSW_CK * SSW_CK);
 		int cur = HV(x_pos, y_pos), dir = 0;
 		for (;;) {
+			if (bad_walk || begin_read < 0 || begin_read >= L || begin_ref < 0 || begin_ref >= ln) {
+				bad_walk = bad_walk ? bad_walk : 6;
+				break;
+			}
 			const uint8_t qb = rd_s[begin_read], rb = ref_s[begin_ref];
 			if (dir == 0) {
 				if (qb == rb) {
@@ -1262,6 +1291,15 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 		}
 	}
 	__syncwarp();
+	if (__reduce_max_sync(FULL, bad_walk)) {
+		if (lane == 0) {
+			out.score = -2000 - bad_walk;
+			out.ok = 0;
+			out.cig.n = out.cig.nm = 0;
+			flags |= F_SSW;
+		}
+		return;
+	}
 	const int n = cig.n, nm = cig.nm;
 	for (int k = lane; k < n; k += 32)
 		out.cig.op[k] = cig.op[k];

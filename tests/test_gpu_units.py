@@ -33,5 +33,6 @@ def test_rescue_dp_golden():
                 capped += 1
                 continue
             bad.append(i)
-    assert not bad, f"{len(bad)} of {len(got)} rescue DPs differ; first {bad[0]}: {got[bad[0]]}"
+    assert not bad, (f"{len(bad)} of {len(got)} rescue DPs differ (flags {flags:#x}); first "
+                     f"{[(i, got[i][:2], len(reads[i]), len(refs[i])) for i in bad[:5]]}")
     assert capped <= 8
