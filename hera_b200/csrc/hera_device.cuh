@@ -1038,69 +1038,165 @@ __host__ __device__ inline size_t ssw_smem_per_warp(int max_len)
 	return SSW_REF_B + SSW_RD_B + SSW_CIG_B + SSW_NCK * col + (((SSW_CK + 1) * col + 15) / 16) * 16;
 }
 
-// One block of the sweep: columns nb+1 .. nb+ncol, starting from the column
-// nb held in Hl (lane's rows) and bot0 (its last row); column values go to
-// `store(y, lane rows)` and the running maximum to best_*.
-template <int R, bool TRACK, typename Store>
-__device__ __forceinline__ void ssw_sweep(const uint8_t *__restrict__ ref_s, const uint8_t (&rdl)[R], int L,
-					  int nb, int ncol, int nact, int (&Hl)[R], int &best_v, int &best_y,
-					  int &best_x, Store store)
+// Score + 2 (3 for equal codes, N == N included, else 0) of every code
+// against code q, as the two words of a byte permute: bytes 0-4 codes 0-4,
+// byte 5 the code no sequence has (5), bytes 6-7 zero.
+struct ScoreT {
+	uint32_t lo, hi;
+};
+__device__ __forceinline__ ScoreT score_table(uint32_t q)
+{
+	return ScoreT{q < 4 ? 3u << (8 * q) : 0u, q == 4 ? 3u : 0u};
+}
+// byte-permute selector of code k: byte k, then three zero bytes
+__device__ __forceinline__ uint32_t score_sel(uint32_t k) { return k | 0x7770u; }
+
+// The DP keeps G = H - 4 (the value a gap step out of a cell gives), so a
+// cell is: a = G(diag) + score + 4 (capped at 253 when CAP: only reads
+// longer than 253 reach it), H = max(a, G(up), G(left), 0) in one DPX
+// three-way max, G = H - 4.
+
+// One block of the sweep, lanes over the read rows: columns nb+1 .. nb+ncol,
+// starting from column nb's values in Hl (H of the lane's rows); lane l holds
+// rows x0 = l*R .. x0+R-1 (their codes as score_sel selectors in `sel`) and
+// works on column y = nb + t - l + 1 at step t.
+// Each column's values go to `store(y, lane's H)`.  Rows past the read take
+// code 5 and are not masked: they feed no row of the read.
+template <int R, bool CAP, typename Store>
+__device__ __forceinline__ void ssw_sweep(const uint8_t *__restrict__ ref_s, const uint32_t (&sel)[R], int nb,
+					  int ncol, int nact, const int (&Hl)[R], Store store)
 {
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
-	const int x0 = lane * R;
+	int G[R], H[R];
+#pragma unroll
+	for (int r = 0; r < R; ++r)
+		G[r] = Hl[r] - 4;
 	// `bot` as of step -1: lane 0 then stands on the left-edge column nb
 	// (its saved last row feeds lane 1's first diagonal), the others before it
-	int bot = lane == 0 ? Hl[R - 1] : 0, up_prev = 0;
+	int bot = lane == 0 ? G[R - 1] : -4, up_prev = -4;
 	const int steps = ncol > 0 ? ncol + nact - 1 : 0;
 	for (int t = 0; t < steps; ++t) {
 		const int y = nb + t - lane + 1;
 		int up_in = __shfl_up_sync(FULL, bot, 1);
 		if (lane == 0)
-			up_in = 0;
+			up_in = -4;
 		const int diag_in = up_prev;
 		up_prev = up_in;
 		if (y > nb && y <= nb + ncol) {
-			const uint8_t rc = ref_s[y - 1];
-			int d = diag_in, up = up_in, cmax = 0;
+			const ScoreT T = score_table(ref_s[y - 1]);
+			int d = diag_in, up = up_in;
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
-				const int left = Hl[r];
-				// max(0, min(255, d + 3*eq) - 2, left - 4, up - 4), d <= 253
-				const int a = __viaddmin_s32(d, rdl[r] == rc ? 1 : -2, 253);
-				int v = __vimax3_s32_relu(a, left - 4, up - 4);
-				if (x0 + r >= L)
-					v = 0;
-				d = left;
-				Hl[r] = v;
-				up = v;
-				cmax = __vimax_s32_relu(cmax, v);
+				const int s2 = (int)__byte_perm(T.lo, T.hi, sel[r]);
+				const int a = CAP ? __viaddmin_s32(d + s2, 2, 253) : d + s2 + 2;
+				const int v = __vimax3_s32_relu(a, up, G[r]);
+				d = G[r];
+				H[r] = v;
+				G[r] = v - 4;
+				up = G[r];
 			}
-			if (TRACK && cmax > best_v) {   // first row of this column reaching it
-				int fx = 0;
-#pragma unroll
-				for (int r = R - 1; r >= 0; --r)
-					if (Hl[r] == cmax)
-						fx = r;
-				best_v = cmax;
-				best_y = y;
-				best_x = x0 + fx;
-			}
-			bot = Hl[R - 1];
-			store(y, Hl);
+			bot = G[R - 1];
+			store(y, H);
 		} else {
 			// column nb is the block's left edge: the lane's saved last row
-			bot = y == nb ? Hl[R - 1] : 0;
+			bot = y == nb ? G[R - 1] : -4;
 		}
 	}
 }
 
-// Called by all 32 lanes of a warp; `sm` is the warp's shared-memory area
-// (ssw_smem_per_warp(L) bytes at least).  Fills `out` (lane 0 writes the
-// scalars; the CIGAR is copied by the warp).
-template <int R>
-__device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff, int L,
-			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out, int &flags)
+// Stage a call's window and read codes into its shared-memory area.
+__device__ inline void ssw_stage(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff,
+				 int L, int orient, uint8_t *__restrict__ sm)
+{
+	const int lane = threadIdx.x & 31;
+	uint8_t *ref_s = sm;
+	uint8_t *rd_s = sm + SSW_REF_B;
+	DCig &cig = *reinterpret_cast<DCig *>(sm + SSW_REF_B + SSW_RD_B);
+	for (int i = lane; i < ln; i += 32)
+		ref_s[i] = __ldg(ix.code + wstart + i);
+	for (int i = lane; i < L; i += 32)
+		rd_s[i] = read_code(code, roff, L, orient, i);
+	if (lane == 0)
+		cig.n = cig.nm = 0;
+}
+
+// Pass 1 of one call with the lanes over the window: lane l owns columns
+// y = 32l+1 .. 32l+32 (one checkpoint block, SSW_CK == 32) and steps down
+// the read rows, row x = t - l at step t; its left edge (column 32l) comes
+// from lane l-1 a step earlier.  A cell is a byte permute for the score, an
+// add, one DPX three-way max and the G add.  Columns past the window take code 5, which equals no read code;
+// as every value there stays below one of the window's own values, they can
+// neither be the maximum nor tie it.  Writes the checkpoint columns
+// (y = 32(l+1) <= ln) and returns the end cell by the reference's rule:
+// maximum value, then first column, then first row.
+template <bool CAP>
+__device__ void ssw_pass1_cols(const uint8_t *__restrict__ ref_s, const uint8_t *__restrict__ rd_s, int ln, int L,
+			       uint8_t *__restrict__ ck, int COL, int &max_v, int &min_y, int &min_x)
+{
+	static_assert(SSW_CK == 32, "one checkpoint block per lane");
+	const unsigned FULL = 0xffffffffu;
+	const int lane = threadIdx.x & 31;
+	const int y0 = 32 * lane;
+	uint32_t sel[32];
+	int G[32];   // G of row x-1 (row -1: H = 0)
+#pragma unroll
+	for (int c = 0; c < 32; ++c) {
+		sel[c] = score_sel(y0 + c < ln ? ref_s[y0 + c] : 5u);
+		G[c] = -4;
+	}
+	uint8_t *ckl = y0 + 32 <= ln ? ck + (size_t)(lane + 1) * COL : nullptr;
+	int bv = 0, by = 0, bx = 0, last = -4, dprev = -4;
+	const int steps = ln > 0 && L > 0 ? L + 31 : 0;
+	for (int t = 0; t < steps; ++t) {
+		int lin = __shfl_up_sync(FULL, last, 1);   // G(x, y0) from lane l-1
+		if (lane == 0)
+			lin = -4;
+		const int diag0 = dprev;                   // G(x-1, y0)
+		dprev = lin;
+		const int x = t - lane;
+		if (x >= 0 && x < L) {
+			const ScoreT T = score_table(rd_s[x]);
+			int d = diag0, left = lin, cm = 0;
+#pragma unroll
+			for (int c = 0; c < 32; ++c) {
+				const int s2 = (int)__byte_perm(T.lo, T.hi, sel[c]);
+				const int a = CAP ? __viaddmin_s32(d + s2, 2, 253) : d + s2 + 2;
+				const int v = __vimax3_s32_relu(a, G[c], left);
+				d = G[c];
+				G[c] = v - 4;
+				left = G[c];
+				cm = max(cm, v);
+			}
+			if (cm >= bv && cm > 0) {
+				int fc = 0;
+#pragma unroll
+				for (int c = 31; c >= 0; --c)
+					if (G[c] == cm - 4)
+						fc = c;
+				const int yy = y0 + fc + 1;
+				if (cm > bv || yy < by) {
+					bv = cm;
+					by = yy;
+					bx = x;
+				}
+			}
+			if (ckl)
+				ckl[x] = (uint8_t)(G[31] + 4);
+			last = G[31];
+		}
+	}
+	max_v = __reduce_max_sync(FULL, bv);
+	min_y = __reduce_min_sync(FULL, bv == max_v ? by : 0x7fffffff);
+	min_x = __reduce_min_sync(FULL, (bv == max_v && by == min_y) ? bx : 0x7fffffff);
+	__syncwarp();
+}
+
+// The reference's traceback and output of one call whose sweep has run
+// (end cell max_v / min_y / min_x; checkpoints in its area).
+template <int R, bool CAP>
+__device__ void ssw_walk(const DevIndex &ix, uint32_t wstart, int ln, int L, int start, uint32_t tl,
+			 uint8_t *__restrict__ sm, SswOut &out, int &flags, int max_v, int min_y, int min_x)
 {
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
@@ -1111,36 +1207,11 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 	DCig &cig = *reinterpret_cast<DCig *>(sm + SSW_REF_B + SSW_RD_B);
 	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + SSW_CIG_B;
 	uint8_t *tb = ck + (size_t)SSW_NCK * COL;
-
-	for (int i = lane; i < ln; i += 32)
-		ref_s[i] = __ldg(ix.code + wstart + i);
-	for (int i = lane; i < L; i += 32)
-		rd_s[i] = read_code(code, roff, L, orient, i);
-	if (lane == 0)
-		cig.n = cig.nm = 0;
-	__syncwarp();
-	uint8_t rdl[R];
-	int Hl[R];
+	uint32_t rsel[R];   // the lane's read rows as score selectors
 #pragma unroll
-	for (int r = 0; r < R; ++r) {
-		rdl[r] = x0 + r < L ? rd_s[x0 + r] : (uint8_t)5;
-		Hl[r] = 0;
-	}
-	const int nact = (L + R - 1) / R;   // lanes holding read rows
-	int best_v = 0, best_y = 0, best_x = 0;
-	ssw_sweep<R, true>(ref_s, rdl, L, 0, ln, nact, Hl, best_v, best_y, best_x, [&](int y, const int (&H)[R]) {
-		if ((y & (SSW_CK - 1)) == 0) {
-			uint8_t *c = ck + (size_t)(y / SSW_CK) * COL + x0;
-#pragma unroll
-			for (int r = 0; r < R; ++r)
-				c[r] = (uint8_t)H[r];
-		}
-	});
-	// max over all cells; first column reaching it; first row in that column
-	const int max_v = __reduce_max_sync(FULL, best_v);
-	const int min_y = __reduce_min_sync(FULL, best_v == max_v ? best_y : 0x7fffffff);
-	const int min_x = __reduce_min_sync(FULL, (best_v == max_v && best_y == min_y) ? best_x : 0x7fffffff);
-	__syncwarp();
+	for (int r = 0; r < R; ++r)
+		rsel[r] = score_sel(x0 + r < L ? rd_s[x0 + r] : 5u);
+	const int nact = (L + R - 1) / R;
 	// self-check of the end cell before the walk (a bad one reports flag
 	// F_SSW instead of reading outside the warp's area)
 	if (max_v > 0 && (min_y < 1 || min_y > ln || min_x < 0 || min_x >= L)) {
@@ -1157,13 +1228,52 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 
 	const uint8_t *ra = ix.seq + wstart;
 	const bool w0 = lane == 0;
-	auto add = [&](int type, unsigned n, const uint8_t *mc) {
+	// cig_add with the CIGAR's counts and last op kept in registers (the
+	// same in every lane; lane 0 stores to the shared-memory CIGAR), so the
+	// serial walk does not reload them from shared memory at each step
+	int cn = 0, cnm = 0;
+	uint32_t clast = 0;   // op[cn - 1] when cn > 0
+	auto add = [&](int type, unsigned cnt, const uint8_t *mc) {
+		cnt &= 0xffffu;
+		if (cnt == 0)
+			return;
+		if (cn > 1 && op_type(clast) == OP_S) {
+			if (type != OP_D) {
+				clast = (((op_cnt(clast) + cnt) & 0xffffu) << 4) | OP_S;
+				if (w0)
+					cig.op[cn - 1] = clast;
+			}
+			return;
+		}
+		if (mc) {
+			if (cnm + (int)cnt > MCAP) {
+				flags |= F_MCAP;
+			} else {
+				if (w0)
+					for (unsigned t = 0; t < cnt; ++t)
+						cig.miss[cnm + t] = mc[t];
+				cnm += (int)cnt;
+			}
+		}
+		if (cn > 0 && op_type(clast) == type) {
+			clast = (((op_cnt(clast) + cnt) & 0xffffu) << 4) | (uint32_t)type;
+			if (w0)
+				cig.op[cn - 1] = clast;
+			return;
+		}
+		if (cn == CCAP) {
+			flags |= F_CCAP;
+			return;
+		}
+		clast = (cnt << 4) | (uint32_t)type;
 		if (w0)
-			cig_add(cig, type, n, mc, flags);
+			cig.op[cn] = clast;
+		++cn;
 	};
 	// block of saved columns [nb, nb + SSW_CK] around the walk
 	int nb = -1, bad_walk = 0;
-	auto load_block = [&](int b) {
+	// (rows 0 .. xmax only: the walk never goes down again)
+	auto load_block = [&](int b, int xmax) {
 		if (b < 0 || b >= ln || (b & (SSW_CK - 1)) || b / SSW_CK >= SSW_NCK) {
 			bad_walk = 3;
 			return;
@@ -1177,9 +1287,9 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 			H0[r] = b == 0 ? 0 : c0[x0 + r];
 			tb[x0 + r] = (uint8_t)H0[r];
 		}
-		int bv = 0, by = 0, bx = 0;
 		const int ncol = ln - b < SSW_CK ? ln - b : SSW_CK;
-		ssw_sweep<R, false>(ref_s, rdl, L, b, ncol, nact, H0, bv, by, bx, [&](int y, const int (&H)[R]) {
+		const int nrow = xmax / R + 1;
+		ssw_sweep<R, CAP>(ref_s, rsel, b, ncol, nrow < nact ? nrow : nact, H0, [&](int y, const int (&H)[R]) {
 			uint8_t *c = tb + (size_t)(y - b) * COL + x0;
 #pragma unroll
 			for (int r = 0; r < R; ++r)
@@ -1224,14 +1334,10 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 				add(OP_S, (unsigned)right, nullptr);
 			}
 		}
-		load_block((y_pos - 1) / SSW_CK * SSW_CK);
+		load_block((y_pos - 1) / SSW_CK * SSW_CK, x_pos);
 		int cur = HV(x_pos, y_pos), dir = 0;
-		for (;;) {
-			if (bad_walk || begin_read < 0 || begin_read >= L || begin_ref < 0 || begin_ref >= ln) {
-				bad_walk = bad_walk ? bad_walk : 6;
-				break;
-			}
-			const uint8_t qb = rd_s[begin_read], rb = ref_s[begin_ref];
+		// the op of the walk's current cell, by the move that reached it
+		auto emit = [&](uint8_t qb, uint8_t rb) {
 			if (dir == 0) {
 				if (qb == rb) {
 					add(OP_M, 1, nullptr);
@@ -1246,10 +1352,61 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 				++score;
 				add(OP_D, 1, ra + begin_ref);
 			}
+		};
+		for (;;) {
+			// Diagonal runs, up to 32 cells at once: lane k takes the cell k
+			// steps down the diagonal and tells whether the walk, there,
+			// moves diagonally again (inside the block, away from the
+			// walk's ends and bounds).  The leading run of such cells is the
+			// walk's next steps; their ops are M/X (the first cell's by the
+			// move that reached it).  The cell after the run takes the
+			// single step below.
+			if (!bad_walk) {
+				const int xk = x_pos - lane, yk = y_pos - lane;
+				bool go = false, mis = false;
+				int hd = 0;
+				if (xk >= 1 && xk < L && yk >= 2 && yk - 1 < ln && yk - 1 >= nb && yk - nb <= SSW_CK) {
+					const int hc = lane == 0 ? cur : tb[(size_t)(yk - nb) * COL + xk];
+					hd = tb[(size_t)(yk - 1 - nb) * COL + xk - 1];
+					const uint8_t q = rd_s[xk], r = ref_s[yk - 1];
+					mis = q != r;
+					go = hd != 0 && hc == hd + mat_score(q, r);
+				}
+				const unsigned run = __ballot_sync(FULL, go);
+				const int m = run == FULL ? 32 : __ffs(~run) - 1;
+				if (m > 0) {
+					const unsigned xm = __ballot_sync(FULL, mis);
+					emit(rd_s[begin_read], ref_s[begin_ref]);
+					for (int k = 1; k < m;) {
+						const unsigned rest = (xm >> k) << k;
+						int nx = rest ? __ffs(rest) - 1 : m;
+						nx = nx < m ? nx : m;
+						if (nx > k)
+							add(OP_M, (unsigned)(nx - k), nullptr);
+						if (nx < m) {
+							add(OP_X, 1, ra + (begin_ref - nx));
+							++score;
+						}
+						k = nx + 1;
+					}
+					cur = __shfl_sync(FULL, hd, m - 1);
+					x_pos -= m;
+					y_pos -= m;
+					begin_read -= m;
+					begin_ref -= m;
+					dir = 0;
+				}
+			}
+			if (bad_walk || begin_read < 0 || begin_read >= L || begin_ref < 0 || begin_ref >= ln) {
+				bad_walk = bad_walk ? bad_walk : 6;
+				break;
+			}
+			const uint8_t qb = rd_s[begin_read], rb = ref_s[begin_ref];
+			emit(qb, rb);
 			if (x_pos == 0 || y_pos == 1)
 				break;
 			if (y_pos - 1 < nb)   // the walk left the block: recompute the one before
-				load_block(nb - SSW_CK);
+				load_block(nb - SSW_CK, x_pos);
 			const int diag = HV(x_pos - 1, y_pos - 1);
 			const int up = HV(x_pos - 1, y_pos);
 			const int left = HV(x_pos, y_pos - 1);
@@ -1300,7 +1457,8 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 		}
 		return;
 	}
-	const int n = cig.n, nm = cig.nm;
+	__syncwarp();   // lane 0's CIGAR stores before the copy
+	const int n = cn, nm = cnm;
 	for (int k = lane; k < n; k += 32)
 		out.cig.op[k] = cig.op[k];
 	for (int k = lane; k < nm; k += 32)
@@ -1314,6 +1472,27 @@ __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const ui
 		out.pstart = start + skip;
 		// acceptance test of re_mapSW (src/hash_align.c:788-792)
 		out.ok = !(score > L / 2 || start + skip < 0 || (uint32_t)(start + skip + L) > tl);
+	}
+}
+
+// One call: stage, pass 1 over the window columns, walk.  Called by all
+// 32 lanes of a warp; `sm` is the warp's shared-memory area
+// (ssw_smem_per_warp(L) bytes at least).  Fills `out` (lane 0 writes the
+// scalars; the CIGAR is copied by the warp).
+template <int R>
+__device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff, int L,
+			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out, int &flags)
+{
+	ssw_stage(ix, wstart, ln, code, roff, L, orient, sm);
+	__syncwarp();
+	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + SSW_CIG_B;
+	int max_v, min_y, min_x;
+	if (L > 253) {
+		ssw_pass1_cols<true>(sm, sm + SSW_REF_B, ln, L, ck, 32 * R, max_v, min_y, min_x);
+		ssw_walk<R, true>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
+	} else {
+		ssw_pass1_cols<false>(sm, sm + SSW_REF_B, ln, L, ck, 32 * R, max_v, min_y, min_x);
+		ssw_walk<R, false>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
 	}
 }
 
