@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--paths", default="plain,batched", help="execution forms to time (batched last)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent sub-batches (0 = library default)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--no-fastq", action="store_true", help="skip the FASTQ-chunk leg")
+    ap.add_argument("--fastq-only", action="store_true",
+                    help="time only the FASTQ-chunk leg (one JSON line with the leg's numbers)")
     ap.add_argument("--pin-tuning", default="", help="BUILD_BLOCKS_PER_SM,RESCUE_WARPS_PER_BLOCK: "
                     "fixed launch shapes instead of the autotuner (reproducible profiles)")
     ap.add_argument("--serve-scale", type=float, default=0.125,
@@ -234,6 +237,11 @@ def main():
     ann, tx, ix = workloads.build(args.workload, device=f"cuda:{local}")
     log(f"[{rank}] index: {ix.n_trans} transcripts, {ix.buckets.shape[0]} k-mers, "
         f"{ix.n_pos} occurrences in {time.time() - t:.1f}s")
+    if args.fastq_only:
+        r1, r2 = workloads.pairs(args.workload, ann, tx, args.chunk, seed=100 + 1000 * rank)
+        print(json.dumps({"fastq": fastq_bench(args, ix, (r1, r2), local),
+                          "config": {"workload": args.workload, "pairs_per_step": args.chunk}}), flush=True)
+        return
     chunks = make_chunks(args.workload, ann, tx, args.chunk, args.distinct, 100 + 1000 * rank)
 
     # device-resident copies (mates interleaved) for the `value` measurement
@@ -366,6 +374,14 @@ def main():
     pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
     roof, roof_seed, roof_rescue = roofline(ktm, dpx, args, pair_bytes, max_len)
 
+    fastq = None
+    if rank == 0 and world == 1 and not args.no_fastq:
+        try:
+            fastq = fastq_bench(args, ix, chunks[0], local)
+        except Exception as e:
+            log(f"fastq leg failed: {e}")
+            fastq = {"error": str(e)}
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         try:
@@ -398,12 +414,82 @@ def main():
             "kernel_ms_per_step": None if ktm is None else {
                 k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
                                                      "rescue_kernel_ms", "resolve_ms", "pack_ms")},
-            "tuning": tuning, "serving": serving, "cpu_baseline": cpu, "e2e": e2e,
+            "tuning": tuning, "serving": serving, "fastq": fastq, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": batched["launches"], "clocks": batched["clocks"],
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        peaks = {}
+    return float(peaks.get("hbm_gbs", 6650.0)), "measured" if "hbm_gbs" in peaks else "fallback"
+
+
+def fastq_bench(args, ix, chunk, local):
+    """The step's pairs as two FASTQ chunk buffers (hera's reader input):
+    the device parse against HBM bandwidth (the parse kernels' CUDA-event
+    time, chunk copies excluded), and chunk text -> records end to end
+    through hera_gpu_align_fastq_pairs (chunk copies included)."""
+    import torch
+    from hera_b200 import api, synth
+    r1, r2 = chunk
+    left = np.frombuffer(synth.fastq_bytes(r1, 1), np.uint8).copy()
+    right = np.frombuffer(synth.fastq_bytes(r2, 2), np.uint8).copy()
+    for a in (left, right):
+        api.host_register(a)
+    ctx = api.Context(ix, device=local)
+    try:
+        for _ in range(args.warmup):
+            recs = ctx.parse_fastq_pairs(left, right)
+        parse_ms, h2d_ms = [], []
+        for _ in range(args.steps):
+            recs = ctx.parse_fastq_pairs(left, right)
+            st = ctx.fastq_stats()
+            parse_ms.append(st["parse_ms"])
+            h2d_ms.append(st["h2d_ms"])
+        assert recs.shape[0] == 2 * r1.n
+        text = int(left.size + right.size)
+        reads = int(recs.shape[0])
+        # algorithmic bytes: every chunk byte read once, one 32-byte record
+        # written per read
+        alg = text + 32 * reads
+        ms = float(np.median(parse_ms))
+        peak, src = _hbm_peak()
+        achieved = alg / (ms / 1000.0) / 1e9
+        parse = {"kernels": "k_fq_count, k_fq_scan, k_fq_lines, k_fq_ends, k_fq_recs, k_fq_pack",
+                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                 "frac": achieved / peak, "peak_source": src, "bytes_per_step": alg,
+                 "chunk_bytes": text, "reads": reads, "parse_ms": ms, "h2d_ms": float(np.median(h2d_ms))}
+        res, recs = ctx.align_fastq_pairs(left, right, args.write_bam)   # warm
+        res, recs = ctx.align_fastq_pairs(left, right, args.write_bam, out=res)
+        pinned = res.arrays() + [ctx._fq_recs]
+        for a in pinned:
+            api.host_register(a)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            res, recs = ctx.align_fastq_pairs(left, right, args.write_bam, out=res)
+            d2h += (res.recs.nbytes + 8 * int(res.c.list_used) + 4 * int(res.c.op_used)
+                    + int(res.c.miss_used) + recs.nbytes)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        for a in pinned:
+            api.host_unregister(a)
+        e2e = {"value": r1.n * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": text,
+               "d2h_bytes_per_step": d2h // args.steps,
+               "path": "FASTQ chunk text -> device parse -> align -> records (hera_gpu_align_fastq_pairs)"}
+        return {"parse": parse, "e2e": e2e}
+    finally:
+        ctx.close()
+        for a in (left, right):
+            api.host_unregister(a)
 
 
 def serve_bench(args, local):

@@ -23,7 +23,10 @@ from . import build as _build
 LIB_PATH = _build.LIB
 
 HERA_GPU_OK = 0
-ERRORS = {-1: "ENODEV", -2: "ECUDA", -3: "ENOMEM", -4: "EINVAL", -5: "ECAPACITY", -6: "ETIMEOUT"}
+ERRORS = {-1: "ENODEV", -2: "ECUDA", -3: "ENOMEM", -4: "EINVAL", -5: "ECAPACITY", -6: "ETIMEOUT",
+          -7: "EFORMAT"}
+HERA_GPU_ECAPACITY = -5
+HERA_GPU_EFORMAT = -7
 MAX_READ = 320
 CIGAR_CHARS = "MIDNSHP=XB"
 
@@ -38,6 +41,29 @@ class HeraGpuError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"hera_gpu {ERRORS.get(code, code)}: {msg}")
         self.code = code
+
+
+class FastqFormatError(HeraGpuError):
+    """A chunk hera's reader rejects ("Wrong format of file"): file 1 or 2
+    of a pair (1 for single reads) and the 0-based read of that file."""
+
+    def __init__(self, code: int, msg: str, bad_file: int, bad_read: int):
+        super().__init__(code, f"{msg} (file {bad_file}, read {bad_read})")
+        self.bad_file = bad_file
+        self.bad_read = bad_read
+
+
+# one read of a FASTQ chunk (hera_gpu_fastq_rec): byte offsets into its buffer
+FQ_DTYPE = np.dtype([("name", "<i8"), ("seq", "<i8"), ("qual", "<i8"),
+                     ("name_len", "<i4"), ("len", "<i4")])
+
+
+class FastqStats(C.Structure):
+    _fields_ = [("h2d_ms", C.c_float), ("parse_ms", C.c_float), ("gather_ms", C.c_float),
+                ("launches", C.c_int32), ("bytes", C.c_int64), ("reads", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class _IndexView(C.Structure):
@@ -169,6 +195,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
     lib.hera_gpu_server_destroy.argtypes = [C.c_void_p]
     lib.hera_gpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    lib.hera_gpu_parse_fastq_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                               C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                               C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    lib.hera_gpu_parse_fastq_single.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32,
+                                                C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    lib.hera_gpu_align_fastq_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                               C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                               C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(_Result)]
+    lib.hera_gpu_get_fastq_stats.argtypes = [C.c_void_p, C.POINTER(FastqStats)]
     _lib = lib
     return lib
 
@@ -394,6 +429,99 @@ class Context:
     @property
     def stream(self) -> int:
         return self.lib.hera_gpu_stream(self.h) or 0
+
+    # ---- FASTQ chunks -------------------------------------------------------
+
+    @staticmethod
+    def _chunk(b) -> np.ndarray:
+        a = np.frombuffer(b, np.uint8) if isinstance(b, (bytes, bytearray, memoryview)) else b
+        return np.ascontiguousarray(a, np.uint8)
+
+    def _fastq_check(self, rc: int, bf: int, br: int) -> None:
+        if rc == HERA_GPU_EFORMAT:
+            raise FastqFormatError(rc, self.lib.hera_gpu_last_error(self.h).decode(), bf, br)
+        self._check(rc)
+
+    def parse_fastq_pairs(self, left, right) -> np.ndarray:
+        """Reads of a pair of FASTQ chunk buffers (bytes or uint8 arrays),
+        parsed on the device: FQ_DTYPE records, mates interleaved."""
+        lb, rb = self._chunk(left), self._chunk(right)
+        cap = max(16, min(lb.size, rb.size) // 64 + 16)
+        while True:
+            recs = np.empty(2 * cap, FQ_DTYPE)
+            n, bf, br = C.c_int32(), C.c_int32(), C.c_int64()
+            rc = self.lib.hera_gpu_parse_fastq_pairs(self.h, _ptr(lb) if lb.size else None, lb.size,
+                                                     _ptr(rb) if rb.size else None, rb.size, _ptr(recs), cap,
+                                                     C.byref(n), C.byref(bf), C.byref(br))
+            if rc == HERA_GPU_ECAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            self._fastq_check(rc, bf.value, br.value)
+            return recs[:2 * n.value]
+
+    def parse_fastq_single(self, chunk) -> np.ndarray:
+        b = self._chunk(chunk)
+        cap = max(16, b.size // 64 + 16)
+        while True:
+            recs = np.empty(cap, FQ_DTYPE)
+            n, br = C.c_int32(), C.c_int64()
+            rc = self.lib.hera_gpu_parse_fastq_single(self.h, _ptr(b) if b.size else None, b.size, _ptr(recs),
+                                                      cap, C.byref(n), C.byref(br))
+            if rc == HERA_GPU_ECAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            self._fastq_check(rc, 1, br.value)
+            return recs[:n.value]
+
+    def align_fastq_pairs(self, left, right, write_bam: int = 1, out: Optional[Result] = None):
+        """Parse a pair of FASTQ chunk buffers and align their pairs, all on
+        the device: (Result, FQ_DTYPE records).  `out`: a Result to reuse
+        (its storage is overwritten); the records array is reused between
+        calls too (copy it to keep it)."""
+        lb, rb = self._chunk(left), self._chunk(right)
+        cap = max(16, min(lb.size, rb.size) // 64 + 16)
+        while True:
+            if getattr(self, "_fq_recs", None) is None or self._fq_recs.shape[0] < 2 * cap:
+                self._fq_recs = np.empty(2 * cap, FQ_DTYPE)
+            recs = self._fq_recs
+            if out is not None:
+                res = out.reuse(2 * cap)
+            else:
+                res = Result(2 * cap, 8 * cap + 1024, 8 * cap + 1024, (lb.size + rb.size) // 8 + 1024)
+            n, bf, br = C.c_int32(), C.c_int32(), C.c_int64()
+            rc = self.lib.hera_gpu_align_fastq_pairs(self.h, _ptr(lb) if lb.size else None, lb.size,
+                                                     _ptr(rb) if rb.size else None, rb.size, write_bam,
+                                                     _ptr(recs), cap, C.byref(n), C.byref(bf), C.byref(br),
+                                                     C.byref(res.c))
+            if rc == HERA_GPU_ECAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            if rc == HERA_GPU_ECAPACITY:   # result pools: fetch again into bigger ones
+                res._alloc(res.c.list_used + 1, res.c.op_used + 1, res.c.miss_used + 1)
+                rc = self.lib.hera_gpu_fetch_result(self.h, C.byref(res.c))
+            self._fastq_check(rc, bf.value, br.value)
+            res.recs = res._rec_buf[:2 * n.value]
+            return res, recs[:2 * n.value]
+
+    def fastq_stats(self) -> dict:
+        s = FastqStats()
+        self._check(self.lib.hera_gpu_get_fastq_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+
+class FastqReads:
+    """A read set (seq, off, len) over a FASTQ chunk buffer for the records
+    `recs` of it -- e.g. recs[0::2] of a pair's file 1 -- to pass to
+    Context.align_pairs / align_single without copying the sequences."""
+
+    def __init__(self, chunk, recs: np.ndarray):
+        self.seq = Context._chunk(chunk)
+        self.off = np.ascontiguousarray(recs["seq"], np.int64)
+        self.len = np.ascontiguousarray(recs["len"], np.int32)
+
+    @property
+    def n(self) -> int:
+        return int(self.len.shape[0])
 
 
 class Server:

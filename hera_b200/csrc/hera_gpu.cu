@@ -695,7 +695,11 @@ struct hera_gpu_ctx {
 	// lanes run their rounds under a shared lock; the autotuner's trials
 	// take it exclusively, so no other lane's kernels share the GPU with them
 	std::shared_mutex gate;
+	struct FqState *fq = nullptr;     // FASTQ chunk parsing (made on first use)
 };
+
+struct FqState;
+static void fq_release(hera_gpu_ctx *ctx);
 
 // candidate launch shapes the autotuner times
 static const int BUILD_BPS[] = {2, 4, 6, 8, 12, 16};
@@ -836,6 +840,7 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 		ctx->na->release();
 		delete ctx->na;
 	}
+	fq_release(ctx);
 	if (ctx->stream)
 		cudaStreamDestroy(ctx->stream);
 	delete ctx;
@@ -2511,3 +2516,4 @@ extern "C" int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s)
 }
 
 #include "hera_server.cuh"
+#include "hera_fastq.cuh"

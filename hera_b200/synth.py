@@ -432,6 +432,19 @@ def write_gtf(ann: Annotation, path: str) -> None:
                             f"gene_id \"{g.gene_id}\"; transcript_id \"{tid}\";\n")
 
 
+def fastq_bytes(reads: ReadSet, mate: Optional[int] = None, prefix: str = "read", qual: int = 63) -> bytes:
+    """The reads as one FASTQ chunk (names prefix<i>[/mate], quality `qual`)."""
+    suffix = f"/{mate}" if mate else ""
+    seq = reads.seq.tobytes()
+    q = bytes([qual]) * (int(reads.len.max()) if reads.n else 0)
+    off, ln = reads.off.tolist(), reads.len.tolist()
+    parts = []
+    for i in range(reads.n):
+        o, L = off[i], ln[i]
+        parts.append(b"@%s%d%s\n%s\n+\n%s\n" % (prefix.encode(), i, suffix.encode(), seq[o:o + L], q[:L]))
+    return b"".join(parts)
+
+
 def write_fastq(reads: ReadSet, path: str, mate: Optional[int] = None, prefix: str = "read") -> None:
     suffix = f"/{mate}" if mate else ""
     with open(path, "wb") as f:

@@ -35,6 +35,8 @@ extern "C" {
 #define HERA_GPU_EINVAL (-4)      /* bad argument (NULL, size, read too long) */
 #define HERA_GPU_ECAPACITY (-5)   /* a per-read capacity was exceeded */
 #define HERA_GPU_ETIMEOUT (-6)    /* a bounded device wait expired */
+#define HERA_GPU_EFORMAT (-7)     /* a chunk the reference's reader rejects
+				     ("Wrong format of file") */
 
 /* Longest read the device path accepts (hera itself has no limit; reads
  * longer than this are rejected with HERA_GPU_EINVAL). */
@@ -400,6 +402,72 @@ int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s);
  * hera_gpu_align_pairs_device, for callers that time or order work around
  * the library's launches.  Calls on one context must not overlap. */
 void *hera_gpu_stream(hera_gpu_ctx *ctx);
+
+/* ---- FASTQ chunks ---------------------------------------------------------
+ * A chunk buffer as hera's reader hands it to a worker (gb_get_pair /
+ * gb_get_single, src/get_buffer.c:191-300): whole FASTQ records, bytes
+ * [0, n) followed by a NUL.  The caller need not store that NUL; a NUL inside
+ * the buffer ends the chunk, as it ends the reference's reader.  Chunks are
+ * below 2 GiB (a pair's two together for hera_gpu_align_fastq_pairs). */
+
+/* One read of a chunk, as byte offsets into its buffer. */
+typedef struct hera_gpu_fastq_rec {
+	int64_t name;      /* the byte after '@' */
+	int64_t seq;
+	int64_t qual;
+	int32_t name_len;  /* bytes of the name line after '@' */
+	int32_t len;       /* sequence (and quality) length */
+} hera_gpu_fastq_rec;
+
+/* Device time of the last parse (CUDA events): the chunk copies, the parse
+ * kernels, and hera_gpu_align_fastq_pairs' gather of the sequences for the
+ * aligner. */
+typedef struct hera_gpu_fastq_stats {
+	float h2d_ms, parse_ms, gather_ms;
+	int32_t launches;
+	int64_t bytes;     /* chunk bytes parsed */
+	int64_t reads;     /* reads of the result */
+} hera_gpu_fastq_stats;
+
+/* Parse a pair of chunk buffers on the device: the reads hera's
+ * align_pool_pair takes from them (src/hash_align.c:1878-1929), each as
+ * get_read_from_fq_buffer reads it (src/read.c:11-63) -- file 1's read,
+ * then file 2's, until either file's last read.  recs[2i] and recs[2i+1] are
+ * the mates of pair i (room for `cap` pairs).  HERA_GPU_EFORMAT where the
+ * reference stops with "Wrong format of file": *bad_file (1 or 2) and
+ * *bad_read (0-based read of that file) name the read it rejects.
+ * HERA_GPU_ECAPACITY when the chunk holds more than `cap` pairs (*n_pairs
+ * is then the count). */
+int hera_gpu_parse_fastq_pairs(hera_gpu_ctx *ctx, const char *left, int64_t n_left,
+			       const char *right, int64_t n_right, hera_gpu_fastq_rec *recs,
+			       int32_t cap, int32_t *n_pairs, int32_t *bad_file,
+			       int64_t *bad_read);
+
+/* The same for one chunk of single reads (align_pool_single,
+ * src/hash_align.c:1966-1998). */
+int hera_gpu_parse_fastq_single(hera_gpu_ctx *ctx, const char *chunk, int64_t n,
+				hera_gpu_fastq_rec *recs, int32_t cap, int32_t *n_reads,
+				int64_t *bad_read);
+
+/* Parse a pair of chunk buffers and align their pairs on the device: the
+ * parsed sequences go to the aligner without leaving the GPU.  `out` gets
+ * what hera_gpu_align_pairs_flat gives for the same reads; recs/n_pairs and
+ * the errors as for hera_gpu_parse_fastq_pairs (reads longer than
+ * HERA_GPU_MAX_READ: HERA_GPU_EINVAL). */
+int hera_gpu_align_fastq_pairs(hera_gpu_ctx *ctx, const char *left, int64_t n_left,
+			       const char *right, int64_t n_right, int write_bam,
+			       hera_gpu_fastq_rec *recs, int32_t cap, int32_t *n_pairs,
+			       int32_t *bad_file, int64_t *bad_read, hera_gpu_result *out);
+
+int hera_gpu_get_fastq_stats(hera_gpu_ctx *ctx, hera_gpu_fastq_stats *out);
+
+/* The reader's side effects for hera's host tail: NULs over the newlines
+ * that end each read's name, sequence and quality (src/read.c:26, 36, 58),
+ * and read_inf views of the reads.  buf/n: the chunk buffer the records came
+ * from; recs[i * stride], i < count (stride 2 with recs + 0 or + 1 for one
+ * file of a pair). */
+int hera_gpu_fastq_read_inf(char *buf, int64_t n, const hera_gpu_fastq_rec *recs,
+			    int32_t count, int32_t stride, hera_read_inf *out);
 
 #ifdef __cplusplus
 }

@@ -262,3 +262,83 @@ class Reference:
 
     def ssw_align(self, ref: bytes, read: bytes):
         return _unit_ssw(self.lib.refh_ssw_align, ref, read)
+
+
+# ---- FASTQ chunk parsing -----------------------------------------------------
+
+FQ_DTYPE = np.dtype([("name", "<i8"), ("seq", "<i8"), ("qual", "<i8"),
+                     ("name_len", "<i4"), ("len", "<i4")])
+assert FQ_DTYPE.itemsize == 32
+
+
+def _as_u8(b) -> np.ndarray:
+    return np.frombuffer(bytes(b), np.uint8)
+
+
+def parse_fq_pairs(left: bytes, right: bytes, cap: Optional[int] = None):
+    """The restatement (hera_oracle.c): (status, recs[2n], n_pairs, bad_file,
+    bad_rec); status 0 ok, -1 READ_FAIL, -2 over cap."""
+    lib = C.CDLL(ORACLE_SO)
+    lb, rb = _as_u8(left), _as_u8(right)
+    if cap is None:
+        cap = max(1, (lb.size + rb.size) // 8 + 1)
+    out = np.zeros(2 * cap, FQ_DTYPE)
+    n, bf, br = C.c_int32(0), C.c_int32(0), C.c_int64(0)
+    rc = lib.ho_parse_fq_pairs(C.c_void_p(_ptr(lb)), C.c_int64(lb.size), C.c_void_p(_ptr(rb)),
+                               C.c_int64(rb.size), C.c_void_p(_ptr(out)), C.c_int32(cap),
+                               C.byref(n), C.byref(bf), C.byref(br))
+    return rc, out[:2 * min(n.value, cap)], n.value, bf.value, br.value
+
+
+def parse_fq_single(buf: bytes, cap: Optional[int] = None):
+    lib = C.CDLL(ORACLE_SO)
+    b = _as_u8(buf)
+    if cap is None:
+        cap = max(1, b.size // 4 + 1)
+    out = np.zeros(cap, FQ_DTYPE)
+    n, br = C.c_int32(0), C.c_int64(0)
+    rc = lib.ho_parse_fq_single(C.c_void_p(_ptr(b)), C.c_int64(b.size), C.c_void_p(_ptr(out)),
+                                C.c_int32(cap), C.byref(n), C.byref(br))
+    return rc, out[:min(n.value, cap)], n.value, 0, br.value
+
+
+def _nul_copy(b: bytes) -> np.ndarray:
+    a = np.zeros(len(b) + 1, np.uint8)
+    a[:len(b)] = np.frombuffer(bytes(b), np.uint8)
+    return a
+
+
+def _recs_from_i64(a: np.ndarray, n: int) -> np.ndarray:
+    a = a[:5 * n].reshape(n, 5)
+    out = np.zeros(n, FQ_DTYPE)
+    for k, f in enumerate(("name", "seq", "qual", "name_len", "len")):
+        out[f] = a[:, k]
+    return out
+
+
+def ref_parse_fq_pairs(left: bytes, right: bytes, buffers: Optional[list] = None):
+    """The reference's get_read_from_fq_buffer in align_pool_pair's loop
+    (oracle/_ref/libhera_ref.so); same return form as parse_fq_pairs.
+    `buffers`, if given, receives the two buffers as the reader left them."""
+    lib = C.CDLL(REFERENCE_SO)
+    lb, rb = _nul_copy(left), _nul_copy(right)
+    cap = max(1, (lb.size + rb.size) // 8 + 1)
+    rec = np.zeros(10 * cap, np.int64)
+    n, bf, br = C.c_int32(0), C.c_int32(0), C.c_int64(0)
+    rc = lib.refh_parse_fq_pairs(C.c_void_p(_ptr(lb)), C.c_void_p(_ptr(rb)), C.c_void_p(_ptr(rec)),
+                                 C.c_int32(cap), C.byref(n), C.byref(bf), C.byref(br))
+    m = min(n.value, cap)
+    if buffers is not None:
+        buffers[:] = [lb[:-1].tobytes(), rb[:-1].tobytes()]
+    return rc, _recs_from_i64(rec, 2 * m), n.value, bf.value, br.value
+
+
+def ref_parse_fq_single(buf: bytes):
+    lib = C.CDLL(REFERENCE_SO)
+    b = _nul_copy(buf)
+    cap = max(1, b.size // 4 + 1)
+    rec = np.zeros(5 * cap, np.int64)
+    n, br = C.c_int32(0), C.c_int64(0)
+    rc = lib.refh_parse_fq_single(C.c_void_p(_ptr(b)), C.c_void_p(_ptr(rec)), C.c_int32(cap),
+                                  C.byref(n), C.byref(br))
+    return rc, _recs_from_i64(rec, min(n.value, cap)), n.value, 0, br.value

@@ -1246,3 +1246,123 @@ int ho_align_pairs_mt(const ho_index *ix, int write_bam, int n,
 	free(jobs);
 	return 0;
 }
+
+/* ---- FASTQ chunk parsing ------------------------------------------------ */
+
+/* byte k of a chunk buffer: bytes [0, n), then the terminating NUL */
+static inline char fq_at(const char *b, int64_t n, int64_t k)
+{
+	return k < n ? b[k] : '\0';
+}
+
+/* One get_read_from_fq_buffer call (src/read.c:11-63) at *pos: 0 READ_SUCCESS
+ * (*pos moves to the next read), 1 READ_END, 2 READ_FAIL.  The reference also
+ * writes NULs over the newlines it passes; no later test reads them. */
+static int fq_one(const char *b, int64_t n, int64_t *pos, ho_fq_rec *r)
+{
+	int64_t i = *pos, prev;
+	if (fq_at(b, n, i) != '@')
+		return 2;
+	prev = i;
+	while (fq_at(b, n, i) != '\0' && fq_at(b, n, i) != '\n')
+		++i;
+	if (fq_at(b, n, i) == '\0')
+		return 2;
+	r->name = prev + 1;
+	r->name_len = (int32_t)(i - prev - 1);
+	++i;
+	prev = i;
+	while (fq_at(b, n, i) != '\0' && fq_at(b, n, i) != '\n')
+		++i;
+	if (fq_at(b, n, i) == '\0')
+		return 2;
+	r->seq = prev;
+	r->len = (int32_t)(i - prev);
+	++i;
+	if (r->len == 0)
+		return 2;
+	if (fq_at(b, n, i) != '+')
+		return 2;
+	while (fq_at(b, n, i) != '\0' && fq_at(b, n, i) != '\n')
+		++i;
+	if (fq_at(b, n, i) == '\0')
+		return 2;
+	++i;
+	prev = i;
+	while (fq_at(b, n, i) != '\0' && fq_at(b, n, i) != '\n')
+		++i;
+	if (i - prev != r->len)
+		return 2;
+	r->qual = prev;
+	if (fq_at(b, n, i) == '\0')
+		return 1;
+	if (fq_at(b, n, i + 1) == '\0')
+		return 1;
+	*pos = i + 1;
+	return 0;
+}
+
+/* align_pool_pair's read loop (src/hash_align.c:1878-1929): left read, then
+ * right read (a READ_FAIL of either ends the run with its file named), the
+ * pair, and a stop when the left read was the last (`ret_code1`, which is
+ * READ_END there) or the right one returned READ_END.  An empty buffer is a
+ * READ_FAIL at its first read, as the reader gives. */
+int ho_parse_fq_pairs(const char *left, int64_t n_left, const char *right, int64_t n_right,
+		      ho_fq_rec *out, int32_t cap, int32_t *n_pairs, int32_t *bad_file,
+		      int64_t *bad_rec)
+{
+	int64_t pl = 0, pr = 0;
+	int32_t k = 0;
+	*n_pairs = 0;
+	*bad_file = 0;
+	*bad_rec = -1;
+	for (;;) {
+		ho_fq_rec a, b;
+		const int s1 = fq_one(left, n_left, &pl, &a);
+		if (s1 == 2) {
+			*bad_file = 1;
+			*bad_rec = k;
+			return HO_FQ_FAIL;
+		}
+		const int s2 = fq_one(right, n_right, &pr, &b);
+		if (s2 == 2) {
+			*bad_file = 2;
+			*bad_rec = k;
+			return HO_FQ_FAIL;
+		}
+		if (k < cap) {
+			out[2 * (int64_t)k] = a;
+			out[2 * (int64_t)k + 1] = b;
+		}
+		++k;
+		if (s1 || s2 == 1)
+			break;
+	}
+	*n_pairs = k;
+	return k > cap ? HO_FQ_CAP : HO_FQ_OK;
+}
+
+/* align_pool_single's read loop (src/hash_align.c:1966-1998) */
+int ho_parse_fq_single(const char *buf, int64_t n, ho_fq_rec *out, int32_t cap,
+		       int32_t *n_reads, int64_t *bad_rec)
+{
+	int64_t p = 0;
+	int32_t k = 0;
+	*n_reads = 0;
+	*bad_rec = -1;
+	for (;;) {
+		ho_fq_rec a;
+		const int s = fq_one(buf, n, &p, &a);
+		if (s == 2) {
+			*bad_rec = k;
+			return HO_FQ_FAIL;
+		}
+		if (k < cap)
+			out[k] = a;
+		++k;
+		if (s == 1)
+			break;
+	}
+	*n_reads = k;
+	return k > cap ? HO_FQ_CAP : HO_FQ_OK;
+}

@@ -118,6 +118,27 @@ int ho_align_pairs_mt(const ho_index *ix, int write_bam, int n,
 		      char *seq2, const int64_t *off2, const int32_t *len2,
 		      int nthreads);
 
+/* FASTQ chunk parsing as hera's worker loops take a chunk's reads: one
+ * read per get_read_from_fq_buffer call (src/read.c:11-63), pairs until
+ * either file's READ_END (align_pool_pair, src/hash_align.c:1878-1929),
+ * single reads until READ_END (align_pool_single, :1966-1998).  A buffer is
+ * bytes [0, n) followed by a NUL; its first NUL ends it.  Offsets are byte
+ * offsets into the buffer (name: the byte after '@'). */
+typedef struct {
+	int64_t name, seq, qual;
+	int32_t name_len, len;
+} ho_fq_rec;
+#define HO_FQ_OK 0
+#define HO_FQ_FAIL (-1)   /* READ_FAIL: the reference stops with "Wrong format" */
+#define HO_FQ_CAP (-2)    /* more reads than `cap`; *n_reads holds the count */
+/* out[2i], out[2i+1]: mates 1 and 2 of pair i (cap pairs); on HO_FQ_FAIL
+ * *bad_file is 1 or 2 and *bad_rec the 0-based read of that file. */
+int ho_parse_fq_pairs(const char *left, int64_t n_left, const char *right, int64_t n_right,
+		      ho_fq_rec *out, int32_t cap, int32_t *n_pairs, int32_t *bad_file,
+		      int64_t *bad_rec);
+int ho_parse_fq_single(const char *buf, int64_t n, ho_fq_rec *out, int32_t cap,
+		       int32_t *n_reads, int64_t *bad_rec);
+
 #ifdef __cplusplus
 }
 #endif

@@ -296,3 +296,82 @@ int refh_align_pairs_mt(int write_bam, int n,
 	free(jobs);
 	return 0;
 }
+
+/* ---- FASTQ chunk parsing ------------------------------------------------ */
+
+/* The reference's read loop of align_pool_pair (src/hash_align.c:1878-1929)
+ * over two chunk buffers, each a writable NUL-terminated copy: every read
+ * comes from the reference's get_read_from_fq_buffer (src/read.c:11-63);
+ * a READ_FAIL, where the reference calls _error, is returned with its file
+ * (1 or 2) and read index.  rec: per read {name, seq, qual} offsets into its
+ * buffer and {name length, len}, as int64 x5; 0 ok, -1 fail, -2 over cap. */
+int refh_parse_fq_pairs(char *left, char *right, int64_t *rec, int32_t cap, int32_t *n_pairs,
+			int32_t *bad_file, int64_t *bad_rec)
+{
+	struct read_inf a, b;
+	int32_t lp = 0, rp = 0, k = 0;
+	*n_pairs = 0;
+	*bad_file = 0;
+	*bad_rec = -1;
+	for (;;) {
+		enum read_exit_code c1 = get_read_from_fq_buffer(&a, left, &lp);
+		if (c1 == READ_FAIL) {
+			*bad_file = 1;
+			*bad_rec = k;
+			return -1;
+		}
+		enum read_exit_code c2 = get_read_from_fq_buffer(&b, right, &rp);
+		if (c2 == READ_FAIL) {
+			*bad_file = 2;
+			*bad_rec = k;
+			return -1;
+		}
+		if (k < cap) {
+			int64_t *o = rec + 10 * (int64_t)k;
+			o[0] = a.name - left;
+			o[1] = a.seq - left;
+			o[2] = a.qual - left;
+			o[3] = (int64_t)strlen(a.name);
+			o[4] = a.len;
+			o[5] = b.name - right;
+			o[6] = b.seq - right;
+			o[7] = b.qual - right;
+			o[8] = (int64_t)strlen(b.name);
+			o[9] = b.len;
+		}
+		++k;
+		if (c1 || c2 == READ_END)
+			break;
+	}
+	*n_pairs = k;
+	return k > cap ? -2 : 0;
+}
+
+/* align_pool_single's read loop (src/hash_align.c:1966-1998) */
+int refh_parse_fq_single(char *buf, int64_t *rec, int32_t cap, int32_t *n_reads, int64_t *bad_rec)
+{
+	struct read_inf a;
+	int32_t p = 0, k = 0;
+	*n_reads = 0;
+	*bad_rec = -1;
+	for (;;) {
+		enum read_exit_code c = get_read_from_fq_buffer(&a, buf, &p);
+		if (c == READ_FAIL) {
+			*bad_rec = k;
+			return -1;
+		}
+		if (k < cap) {
+			int64_t *o = rec + 5 * (int64_t)k;
+			o[0] = a.name - buf;
+			o[1] = a.seq - buf;
+			o[2] = a.qual - buf;
+			o[3] = (int64_t)strlen(a.name);
+			o[4] = a.len;
+		}
+		++k;
+		if (c == READ_END)
+			break;
+	}
+	*n_reads = k;
+	return k > cap ? -2 : 0;
+}
