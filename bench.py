@@ -462,7 +462,7 @@ def fastq_bench(args, ix, chunk, local):
         ms = float(np.median(parse_ms))
         peak, src = _hbm_peak()
         achieved = alg / (ms / 1000.0) / 1e9
-        parse = {"kernels": "k_fq_count, k_fq_scan, k_fq_lines, k_fq_ends, k_fq_recs, k_fq_pack",
+        parse = {"kernels": "k_fq_count, k_fq_scan, k_fq_lines, k_fq_ends, k_fq_recs",
                  "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                  "frac": achieved / peak, "peak_source": src, "bytes_per_step": alg,
                  "chunk_bytes": text, "reads": reads, "parse_ms": ms, "h2d_ms": float(np.median(h2d_ms))}

@@ -6,16 +6,19 @@
 // chunk ends at its first NUL.  The device form finds every line at once and
 // then judges every read independently:
 //   k_fq_count   per 8 KiB tile: newlines (an exact SWAR zero-byte test on
-//                16-byte loads) and the first NUL;
+//                16-byte loads) as one bit a byte, with bits for a newline
+//                followed by '@' or by '+', their count, and the first NUL
+//                -- the one pass over the text;
 //   k_fq_scan    tile offsets (one block);
-//   k_fq_lines   the newline positions, in order;
+//   k_fq_lines   from the bits: the newline positions, in order, and the
+//                class of the line each one starts ('@', '+', other);
 //   k_fq_ends    per file: the newlines before its end and where they start;
 //   k_fq_recs    one thread per read: its line ends give the read's fields
 //                and the reader's verdict (another read follows / the last
-//                read / READ_FAIL); the first read not followed by another
-//                is a min over the reads;
-//   k_fq_pack    pairs interleaved in file order, and their lengths;
-//   k_fq_gather  the sequences back to back for the aligner (warp a read).
+//                read / READ_FAIL), written interleaved by pair; the first
+//                read not followed by another is a min over the reads;
+//   k_fq_gather  the sequences for the aligner, each in a 16-byte aligned
+//                slot (warp a read, 4-byte words).
 // The host reads four ints per file to settle the read (pair) count the
 // reference's loop reaches, or the read it rejects.
 #pragma once
@@ -32,7 +35,8 @@ constexpr int64_t MAX_BYTES = (int64_t)INT32_MAX - 4 * TILE;   // positions are 
 
 // info[] of a file: [0] first NUL (or n), [1] its newlines' base in nl[],
 // [2] newlines before [0], [3] 4 * first read not followed by another +
-// its verdict (1 last read, 2 READ_FAIL), [4] longest read of the result
+// its verdict (1 last read, 2 READ_FAIL); info[4] of file 1: the longest
+// read of the result (set by the gather's length scan)
 constexpr int NINFO = 8;
 
 struct File {
@@ -40,35 +44,22 @@ struct File {
 	int64_t n;
 	int32_t tiles, tile0;
 	int32_t *info;
-	hera_gpu_fastq_rec *rec;
-	int32_t max_rec;       // reads a thread grid covers (n / 8 + 1)
+	int32_t max_rec;       // reads that can be judged (n / 8 + 1)
 };
 
 struct Files {
 	File f[2];
 	int nf;
+	uint32_t *bits;            // three planes of a bit a byte (see k_fq_count)
+	size_t plane;              // words a plane
+	hera_gpu_fastq_rec *out;   // reads interleaved by pair (nf * max max_rec)
+	int32_t *len;              // their lengths
 };
 
 __device__ __forceinline__ uint32_t zero_bytes(uint32_t x)
 {
 	// 0x80 in every byte of x that is 0x00, nothing elsewhere
 	return ~(((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x | 0x7f7f7f7fu);
-}
-
-// newline and NUL flags (0x80 per byte) of the 32 bytes at p; bytes at or
-// past n carry none
-__device__ __forceinline__ void masks(const File &f, int64_t p, uint32_t (&nlm)[8], uint32_t (&nul)[8])
-{
-	const uint4 a = __ldg(reinterpret_cast<const uint4 *>(f.text + p));
-	const uint4 b = __ldg(reinterpret_cast<const uint4 *>(f.text + p + 16));
-	const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-	for (int k = 0; k < 8; ++k) {
-		const int64_t left = f.n - (p + 4 * k);
-		const uint32_t valid = left >= 4 ? 0x80808080u : (left <= 0 ? 0u : ((1u << (8 * left)) - 1u) & 0x80808080u);
-		nlm[k] = zero_bytes(w[k] ^ 0x0a0a0a0au) & valid;
-		nul[k] = zero_bytes(w[k]) & valid;
-	}
 }
 
 __device__ __forceinline__ int file_of(const Files &F, int block)
@@ -109,20 +100,68 @@ __device__ __forceinline__ int block_excl(int v, int *sh, int *total)
 	return before + x - v;
 }
 
-__global__ void __launch_bounds__(TPB) k_fq_count(Files F, int32_t *__restrict__ tile_cnt)
+// 0x80 byte flags (bits 7, 15, 23, 31) -> 4 bits: after the shift the flags
+// sit at bits 0, 8, 16, 24; the multiply by 1 + 2^7 + 2^14 + 2^21 lands them
+// at 21, 22, 23, 24 with no other term there (so no carries)
+__device__ __forceinline__ uint32_t flags4(uint32_t x)
+{
+	return (((x >> 7) * 0x00204081u) >> 21) & 15u;
+}
+
+// A tile per block of PASS_TPB threads, 128 bytes (eight 16-byte loads issued
+// together) a thread.  Bit planes of the tile, one word per 32 bytes:
+// newlines; newlines followed by '@'; newlines followed by '+' (bytes at or
+// past n carry none; a line class is checked against the file's end too).
+constexpr int PASS_TPB = TPB / 4;
+constexpr int WORDS = TILE / 32;   // bit words of a tile
+
+__global__ void __launch_bounds__(PASS_TPB) k_fq_count(Files F, int32_t *__restrict__ tile_cnt)
 {
 	__shared__ int sh[32];
 	const int fi = file_of(F, blockIdx.x);
-	const File &f = F.f[fi];
-	const int64_t p = (int64_t)(blockIdx.x - f.tile0) * TILE + threadIdx.x * 32;
-	uint32_t nlm[8], nul[8];
-	masks(f, p, nlm, nul);
-	int c = 0, z = INT32_MAX;
+	const File f = fi ? F.f[1] : F.f[0];
+	const int64_t p = (int64_t)(blockIdx.x - f.tile0) * TILE + threadIdx.x * 128;
+	uint32_t w[33];
 #pragma unroll
 	for (int k = 0; k < 8; ++k) {
-		c += __popc(nlm[k]);
-		if (nul[k] && z == INT32_MAX)
-			z = (int)(p + 4 * k + ((__ffs(nul[k]) - 1) >> 3));
+		const uint4 q = __ldg(reinterpret_cast<const uint4 *>(f.text + p) + k);
+		w[4 * k] = q.x;
+		w[4 * k + 1] = q.y;
+		w[4 * k + 2] = q.z;
+		w[4 * k + 3] = q.w;
+	}
+	w[32] = p + 128 < f.n ? f.text[p + 128] : 0u;   // the byte after the 128
+	const bool whole = p + 128 <= f.n;
+	int z = INT32_MAX, c = 0;
+#pragma unroll
+	for (int g = 0; g < 4; ++g) {   // 32-byte groups: one word of each plane
+		uint32_t nlb = 0, atb = 0, plb = 0;
+#pragma unroll
+		for (int e = 0; e < 8; ++e) {
+			const int k = 8 * g + e;
+			uint32_t valid = 0x80808080u;
+			if (!whole) {
+				const int64_t left = f.n - (p + 4 * k);
+				valid = left >= 4 ? 0x80808080u
+						  : (left <= 0 ? 0u : ((1u << (8 * left)) - 1u) & 0x80808080u);
+			}
+			const uint32_t nlf = zero_bytes(w[k] ^ 0x0a0a0a0au) & valid;
+			const uint32_t nul = zero_bytes(w[k]) & valid;
+			if (nul && z == INT32_MAX)
+				z = (int)(p + 4 * k + ((__ffs(nul) - 1) >> 3));
+			if (nlf) {
+				// each byte's next byte, and whether it is '@' / '+'
+				const uint32_t nx = __funnelshift_r(w[k], w[k + 1], 8);
+				nlb |= flags4(nlf) << (4 * e);
+				atb |= flags4(nlf & zero_bytes(nx ^ 0x40404040u)) << (4 * e);
+				plb |= flags4(nlf & zero_bytes(nx ^ 0x2b2b2b2bu)) << (4 * e);
+			}
+		}
+		const size_t wi = (size_t)blockIdx.x * WORDS + 4 * threadIdx.x + g;
+		F.bits[wi] = nlb;
+		F.bits[F.plane + wi] = atb;
+		F.bits[2 * F.plane + wi] = plb;
+		c += __popc(nlb);
 	}
 	if (z != INT32_MAX)
 		atomicMin(f.info + 0, z);
@@ -161,27 +200,33 @@ __global__ void __launch_bounds__(SCAN_TPB) k_fq_scan(const int32_t *__restrict_
 		off[n] = carry;
 }
 
-__global__ void __launch_bounds__(TPB) k_fq_lines(Files F, const int32_t *__restrict__ tile_off,
-						   int32_t *__restrict__ nl)
+// a tile per block of PASS_TPB threads, 128 bytes (four bit words) a thread;
+// cls of the line a newline starts: 1 '@', 2 '+', 0 other
+__global__ void __launch_bounds__(PASS_TPB) k_fq_lines(Files F, const int32_t *__restrict__ tile_off,
+							int32_t *__restrict__ nl, uint8_t *__restrict__ cls)
 {
 	__shared__ int sh[32];
 	const int fi = file_of(F, blockIdx.x);
-	const File &f = F.f[fi];
-	const int64_t p = (int64_t)(blockIdx.x - f.tile0) * TILE + threadIdx.x * 32;
-	uint32_t nlm[8], nul[8];
-	masks(f, p, nlm, nul);
-	int c = 0;
-#pragma unroll
-	for (int k = 0; k < 8; ++k)
-		c += __popc(nlm[k]);
+	const File f = fi ? F.f[1] : F.f[0];
+	const size_t w0 = (size_t)blockIdx.x * WORDS + 4 * threadIdx.x;
+	const int64_t p = (int64_t)(blockIdx.x - f.tile0) * TILE + threadIdx.x * 128;
+	const uint4 m4 = *reinterpret_cast<const uint4 *>(F.bits + w0);
+	const uint4 a4 = *reinterpret_cast<const uint4 *>(F.bits + F.plane + w0);
+	const uint4 p4 = *reinterpret_cast<const uint4 *>(F.bits + 2 * F.plane + w0);
+	const uint32_t m[4] = {m4.x, m4.y, m4.z, m4.w}, ma[4] = {a4.x, a4.y, a4.z, a4.w},
+		       mp[4] = {p4.x, p4.y, p4.z, p4.w};
+	const int c = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
 	int total;
 	int at = tile_off[blockIdx.x] + block_excl(c, sh, &total);
 #pragma unroll
-	for (int k = 0; k < 8; ++k) {
-		uint32_t m = nlm[k];
-		while (m) {
-			nl[at++] = (int32_t)(p + 4 * k + ((__ffs(m) - 1) >> 3));
-			m &= m - 1;
+	for (int k = 0; k < 4; ++k) {
+		uint32_t x = m[k];
+		while (x) {
+			const uint32_t lo = x & (0u - x);
+			nl[at] = (int32_t)(p + 32 * k + __ffs(x) - 1);
+			cls[at] = (ma[k] & lo) ? 1 : ((mp[k] & lo) ? 2 : 0);
+			++at;
+			x &= x - 1;
 		}
 	}
 }
@@ -192,7 +237,7 @@ __global__ void k_fq_ends(Files F, const int32_t *__restrict__ tile_off, const i
 	const int fi = threadIdx.x;
 	if (fi >= F.nf)
 		return;
-	const File &f = F.f[fi];
+	const File f = fi ? F.f[1] : F.f[0];
 	const int32_t base = tile_off[f.tile0], cnt = tile_off[f.tile0 + f.tiles] - base;
 	const int32_t z = f.info[0];
 	int lo = 0, hi = cnt;   // first newline at or past z
@@ -216,16 +261,23 @@ __global__ void k_fq_ends(Files F, const int32_t *__restrict__ tile_off, const i
 // bytes at least, so the first read not followed by another lies below
 // n / 8 + 1 (max_rec); the reads judged are r <= min(newlines / 4,
 // max_rec - 1), a grid-stride loop per file.
-__device__ __forceinline__ void fq_rec(const File &f, const int32_t *__restrict__ L, int32_t m, int64_t r)
+__device__ __forceinline__ void fq_rec(const Files &F, int fi, const int32_t *__restrict__ L,
+				       const uint8_t *__restrict__ cls, int32_t m, int64_t r)
 {
+	const File f = fi ? F.f[1] : F.f[0];
 	const int64_t z = f.info[0];
-	auto at = [&](int64_t k) -> uint8_t { return k < z ? f.text[k] : (uint8_t)0; };
+	// line j's first byte is '@' / '+' (the file's first line read from the text)
+	auto first_is = [&](int j, int64_t s, uint8_t ch, uint8_t c) -> bool {
+		if (s >= z)
+			return false;
+		return j == 0 ? f.text[0] == ch : cls[j - 1] == c;
+	};
 	const int j = (int)(4 * r);
 	int verdict = 2;
 	hera_gpu_fastq_rec o{};
 	do {
 		const int64_t s0 = j == 0 ? 0 : (int64_t)L[j - 1] + 1;
-		if (at(s0) != '@' || j >= m)
+		if (!first_is(j, s0, '@', 1) || j >= m)
 			break;
 		o.name = s0 + 1;
 		o.name_len = (int32_t)(L[j] - s0 - 1);
@@ -236,7 +288,7 @@ __device__ __forceinline__ void fq_rec(const File &f, const int32_t *__restrict_
 		if (o.len == 0)
 			break;
 		const int64_t s2 = (int64_t)L[j + 1] + 1;
-		if (at(s2) != '+' || j + 2 >= m)
+		if (!first_is(j + 2, s2, '+', 2) || j + 2 >= m)
 			break;
 		o.qual = (int64_t)L[j + 2] + 1;
 		const int64_t e3 = j + 3 < m ? (int64_t)L[j + 3] : z;
@@ -244,51 +296,45 @@ __device__ __forceinline__ void fq_rec(const File &f, const int32_t *__restrict_
 			break;
 		verdict = (j + 3 >= m || e3 + 1 == z) ? 1 : 0;
 	} while (false);
-	f.rec[r] = o;
+	F.out[(int64_t)F.nf * r + fi] = o;
+	F.len[(int64_t)F.nf * r + fi] = o.len;
 	if (verdict)
 		atomicMin(f.info + 3, (int32_t)(4 * r + verdict));
 }
 
-__global__ void __launch_bounds__(TPB) k_fq_recs(Files F, const int32_t *__restrict__ nl)
+__global__ void __launch_bounds__(TPB) k_fq_recs(Files F, const int32_t *__restrict__ nl,
+						  const uint8_t *__restrict__ cls)
 {
 	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
 	for (int fi = 0; fi < F.nf; ++fi) {
-		const File &f = F.f[fi];
+		const File f = fi ? F.f[1] : F.f[0];
 		const int32_t m = f.info[2];
 		const int64_t nrec = min((int64_t)m / 4 + 1, (int64_t)f.max_rec);
 		const int32_t *L = nl + f.info[1];
+		const uint8_t *C = cls + f.info[1];
 		for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrec; r += stride)
-			fq_rec(f, L, m, r);
+			fq_rec(F, fi, L, C, m, r);
 	}
 }
 
-// reads of the result, interleaved by pair (mate 1, mate 2) or as they are
-__global__ void k_fq_pack(Files F, int n, hera_gpu_fastq_rec *__restrict__ out, int32_t *__restrict__ len)
-{
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
-		return;
-	int mx = 0;
-	for (int fi = 0; fi < F.nf; ++fi) {
-		const hera_gpu_fastq_rec o = F.f[fi].rec[i];
-		out[(int64_t)F.nf * i + fi] = o;
-		len[(int64_t)F.nf * i + fi] = o.len;
-		mx = max(mx, o.len);
-	}
-	atomicMax(F.f[0].info + 4, mx);
-}
+// Offsets of the aligner's read slots: an exclusive scan of the lengths
+// rounded up to 16 bytes (per-block sums, a scan of those with k_fq_scan,
+// the blocks again); the first pass also takes the longest read.
+__device__ __forceinline__ int slot_bytes(int len) { return (len + 15) & ~15; }
 
-// exclusive scan of 2n lengths into int64 offsets: per-block sums, a scan of
-// those (k_fq_scan), then the blocks again
 __global__ void __launch_bounds__(SCAN_TPB) k_fq_lsum(const int32_t *__restrict__ len, int64_t n,
-						       int32_t *__restrict__ bsum)
+						       int32_t *__restrict__ bsum, int32_t *__restrict__ max_len)
 {
 	__shared__ int sh[32];
 	const int64_t i = (int64_t)blockIdx.x * SCAN_TPB + threadIdx.x;
+	const int L = i < n ? len[i] : 0;
 	int total;
-	block_excl(i < n ? len[i] : 0, sh, &total);
+	block_excl(slot_bytes(L), sh, &total);
 	if (threadIdx.x == 0)
 		bsum[blockIdx.x] = total;
+	const int mx = __reduce_max_sync(0xffffffffu, L);
+	if ((threadIdx.x & 31) == 0 && mx > 0)
+		atomicMax(max_len, mx);
 }
 
 __global__ void __launch_bounds__(SCAN_TPB) k_fq_loff(const int32_t *__restrict__ len, int64_t n,
@@ -297,12 +343,14 @@ __global__ void __launch_bounds__(SCAN_TPB) k_fq_loff(const int32_t *__restrict_
 	__shared__ int sh[32];
 	const int64_t i = (int64_t)blockIdx.x * SCAN_TPB + threadIdx.x;
 	int total;
-	const int x = block_excl(i < n ? len[i] : 0, sh, &total);
+	const int x = block_excl(i < n ? slot_bytes(len[i]) : 0, sh, &total);
 	if (i < n)
 		off[i] = (int64_t)boff[blockIdx.x] + x;
 }
 
-// warp per read: its sequence to seq + off[i]
+// warp per read: its sequence into its 16-byte aligned slot, lane k on the
+// slot's 4-byte words k, k + 32, ... (two aligned source words and a
+// funnel shift each; the slot's bytes past the read are don't-care)
 __global__ void k_fq_gather(Files F, const hera_gpu_fastq_rec *__restrict__ recs, int64_t n,
 			    const int64_t *__restrict__ off, uint8_t *__restrict__ seq)
 {
@@ -311,10 +359,14 @@ __global__ void k_fq_gather(Files F, const hera_gpu_fastq_rec *__restrict__ recs
 	if (i >= n)
 		return;
 	const hera_gpu_fastq_rec o = recs[i];
-	const uint8_t *src = F.f[F.nf > 1 ? (int)(i & 1) : 0].text + o.seq;
-	uint8_t *dst = seq + off[i];
-	for (int k = lane; k < o.len; k += 32)
-		dst[k] = src[k];
+	const uint8_t *src = (F.nf > 1 && (i & 1) ? F.f[1].text : F.f[0].text) + o.seq;
+	uint32_t *dst = reinterpret_cast<uint32_t *>(seq + off[i]);
+	const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
+	const uint32_t *sw = reinterpret_cast<const uint32_t *>(sa & ~(uintptr_t)3);
+	const unsigned sh = 8u * (unsigned)(sa & 3);
+	const int words = (o.len + 3) >> 2;
+	for (int k = lane; k < words; k += 32)
+		dst[k] = __funnelshift_r(sw[k], sw[k + 1], sh);
 }
 
 }  // namespace fq
@@ -325,7 +377,9 @@ struct FqState {
 	cudaStream_t stream = nullptr;
 	DBuf<uint8_t> text;                 // file 1 at 0, file 2 at a tile boundary
 	DBuf<int32_t> tile_cnt, tile_off, nl, info, len, bsum, boff;
-	DBuf<hera_gpu_fastq_rec> rec, out;  // per file (file 2 after file 1's max_rec), result
+	DBuf<uint32_t> bits;
+	DBuf<uint8_t> cls;
+	DBuf<hera_gpu_fastq_rec> out;       // reads interleaved by pair
 	DBuf<int64_t> off;
 	DBuf<uint8_t> seq;
 	HBuf<int32_t> h_info;
@@ -335,7 +389,8 @@ struct FqState {
 	void release()
 	{
 		text.release(); tile_cnt.release(); tile_off.release(); nl.release(); info.release();
-		len.release(); bsum.release(); boff.release(); rec.release(); out.release(); off.release();
+		len.release(); bsum.release(); boff.release(); bits.release(); cls.release(); out.release();
+		off.release();
 		seq.release(); h_info.release();
 		for (auto &e : ev)
 			if (e)
@@ -376,8 +431,9 @@ static int fq_state(hera_gpu_ctx *ctx, FqState **out)
 }
 
 // Parse nf chunk buffers on the device.  On HERA_GPU_OK, *n is the read
-// (pair) count the reference's loop reaches and S.out / S.len hold the reads
-// interleaved; HERA_GPU_EFORMAT gives the rejected file and read.
+// (pair) count the reference's loop reaches and the first nf * n entries of
+// S.out / S.len hold its reads interleaved; HERA_GPU_EFORMAT gives the
+// rejected file and read.
 static int fq_parse(hera_gpu_ctx *ctx, FqState &S, const char *const *buf, const int64_t *bytes, int nf,
 		    int32_t *n, int32_t *bad_file, int64_t *bad_read)
 {
@@ -387,7 +443,7 @@ static int fq_parse(hera_gpu_ctx *ctx, FqState &S, const char *const *buf, const
 	fq::Files F{};
 	F.nf = nf;
 	int64_t tb = 0, all = 0;
-	int32_t tiles = 0, recs = 0;
+	int32_t tiles = 0, recs = 0, most = 0;
 	int64_t start[2] = {0, 0};
 	for (int k = 0; k < nf; ++k) {
 		if (bytes[k] < 0 || bytes[k] > MAX_BYTES || (bytes[k] > 0 && !buf[k]))
@@ -402,20 +458,25 @@ static int fq_parse(hera_gpu_ctx *ctx, FqState &S, const char *const *buf, const
 		tiles += F.f[k].tiles;
 		tb += (int64_t)F.f[k].tiles * TILE;
 		recs += F.f[k].max_rec;
+		most = std::max(most, F.f[k].max_rec);
 		all += bytes[k];
 	}
+	// text: whole tiles and 64 bytes the gather's word loads may pass over;
 	// newlines: at most one a byte
-	if (S.text.ensure((size_t)tb) != cudaSuccess || S.tile_cnt.ensure(tiles) != cudaSuccess ||
+	if (S.text.ensure((size_t)tb + 64) != cudaSuccess || S.tile_cnt.ensure(tiles) != cudaSuccess ||
 	    S.tile_off.ensure(tiles + 1) != cudaSuccess || S.info.ensure(NINFO * 2) != cudaSuccess ||
-	    S.rec.ensure((size_t)recs) != cudaSuccess || S.h_info.ensure(NINFO * 2) != cudaSuccess ||
-	    S.nl.ensure((size_t)all + 16) != cudaSuccess)
+	    S.bits.ensure((size_t)tiles * fq::WORDS * 3) != cudaSuccess || S.h_info.ensure(NINFO * 2) != cudaSuccess ||
+	    S.nl.ensure((size_t)all + 16) != cudaSuccess || S.cls.ensure((size_t)all + 16) != cudaSuccess ||
+	    S.out.ensure((size_t)nf * most) != cudaSuccess ||
+	    S.len.ensure((size_t)nf * most) != cudaSuccess)
 		return fail(ctx, HERA_GPU_ENOMEM, "FASTQ parse buffers");
-	int64_t rb = 0;
+	F.bits = S.bits.p;
+	F.plane = (size_t)tiles * fq::WORDS;
+	F.out = S.out.p;
+	F.len = S.len.p;
 	for (int k = 0; k < nf; ++k) {
 		F.f[k].text = S.text.p + start[k];
 		F.f[k].info = S.info.p + NINFO * k;
-		F.f[k].rec = S.rec.p + rb;
-		rb += F.f[k].max_rec;
 	}
 	for (int k = 0; k < nf; ++k) {
 		int32_t *I = S.h_info.p + NINFO * k;
@@ -432,13 +493,14 @@ static int fq_parse(hera_gpu_ctx *ctx, FqState &S, const char *const *buf, const
 			cudaMemcpyAsync(S.text.p + start[k], buf[k], (size_t)bytes[k], cudaMemcpyHostToDevice, st);
 	cudaMemcpyAsync(S.info.p, S.h_info.p, sizeof(int32_t) * NINFO * nf, cudaMemcpyHostToDevice, st);
 	cudaEventRecord(S.ev[1], st);
-	k_fq_count<<<tiles, fq::TPB, 0, st>>>(F, S.tile_cnt.p);
+	k_fq_count<<<tiles, fq::PASS_TPB, 0, st>>>(F, S.tile_cnt.p);
 	k_fq_scan<<<1, SCAN_TPB, 0, st>>>(S.tile_cnt.p, tiles, S.tile_off.p);
-	k_fq_lines<<<tiles, fq::TPB, 0, st>>>(F, S.tile_off.p, S.nl.p);
+	k_fq_lines<<<tiles, fq::PASS_TPB, 0, st>>>(F, S.tile_off.p, S.nl.p, S.cls.p);
 	k_fq_ends<<<1, 32, 0, st>>>(F, S.tile_off.p, S.nl.p);
 	{
 		const int64_t want = (recs + fq::TPB - 1) / fq::TPB;
-		k_fq_recs<<<(unsigned)std::min<int64_t>(want, (int64_t)ctx->sms * 16), fq::TPB, 0, st>>>(F, S.nl.p);
+		k_fq_recs<<<(unsigned)std::min<int64_t>(want, (int64_t)ctx->sms * 16), fq::TPB, 0, st>>>(F, S.nl.p,
+													     S.cls.p);
 	}
 	S.stats.launches = 5;
 	cudaEventRecord(S.ev[2], st);
@@ -470,26 +532,16 @@ static int fq_parse(hera_gpu_ctx *ctx, FqState &S, const char *const *buf, const
 	*n = kk + 1;
 	*bad_file = 0;
 	*bad_read = -1;
-	if (S.out.ensure((size_t)nf * *n) != cudaSuccess || S.len.ensure((size_t)nf * *n) != cudaSuccess)
-		return fail(ctx, HERA_GPU_ENOMEM, "FASTQ parse outputs");
-	cudaEventRecord(S.ev[3], st);
-	k_fq_pack<<<(*n + 255) / 256, 256, 0, st>>>(F, *n, S.out.p, S.len.p);
-	++S.stats.launches;
-	cudaEventRecord(S.ev[4], st);
 	S.stats.reads = (int64_t)nf * *n;
 	return HERA_GPU_OK;
 }
 
-// device times: chunk copies; the parse kernels (the host's look at the
-// read counts between them left out); the sequence gather
+// device times: chunk copies, parse kernels, sequence gather
 static void fq_times(FqState &S, bool gather)
 {
-	cudaEventSynchronize(gather ? S.ev[6] : S.ev[4]);
-	float a = 0, b = 0;
+	cudaEventSynchronize(gather ? S.ev[6] : S.ev[2]);
 	cudaEventElapsedTime(&S.stats.h2d_ms, S.ev[0], S.ev[1]);
-	cudaEventElapsedTime(&a, S.ev[1], S.ev[2]);
-	cudaEventElapsedTime(&b, S.ev[3], S.ev[4]);
-	S.stats.parse_ms = a + b;
+	cudaEventElapsedTime(&S.stats.parse_ms, S.ev[1], S.ev[2]);
 	S.stats.gather_ms = 0;
 	if (gather)
 		cudaEventElapsedTime(&S.stats.gather_ms, S.ev[5], S.ev[6]);
@@ -567,15 +619,17 @@ extern "C" int hera_gpu_align_fastq_pairs(hera_gpu_ctx *ctx, const char *left, i
 	if (n > cap)
 		return fail(ctx, HERA_GPU_ECAPACITY, "more pairs than the record array holds");
 	cudaStream_t st = S->stream;
-	// sequences back to back for the aligner (read 2i mate 1, 2i+1 mate 2)
+	// sequences in rising 16-byte slots for the aligner (read 2i mate 1,
+	// 2i+1 mate 2)
 	const int64_t nr = 2 * (int64_t)n;
 	const int nb = (int)((nr + SCAN_TPB - 1) / SCAN_TPB);
 	if (S->bsum.ensure(nb + 1) != cudaSuccess || S->boff.ensure(nb + 1) != cudaSuccess ||
-	    S->off.ensure((size_t)nr + 1) != cudaSuccess || S->seq.ensure((size_t)(n_left + n_right) + 64) != cudaSuccess)
+	    S->off.ensure((size_t)nr + 1) != cudaSuccess ||
+	    S->seq.ensure((size_t)(n_left + n_right) + 16 * (size_t)nr + 64) != cudaSuccess)
 		return fail(ctx, HERA_GPU_ENOMEM, "FASTQ gather buffers");
 	const fq::Files &F = S->F;
 	cudaEventRecord(S->ev[5], st);
-	k_fq_lsum<<<nb, SCAN_TPB, 0, st>>>(S->len.p, nr, S->bsum.p);
+	k_fq_lsum<<<nb, SCAN_TPB, 0, st>>>(S->len.p, nr, S->bsum.p, S->info.p + 4);
 	k_fq_scan<<<1, SCAN_TPB, 0, st>>>(S->bsum.p, nb, S->boff.p);
 	k_fq_loff<<<nb, SCAN_TPB, 0, st>>>(S->len.p, nr, S->boff.p, S->off.p);
 	k_fq_gather<<<(unsigned)((nr * 32 + 255) / 256), 256, 0, st>>>(F, S->out.p, nr, S->off.p, S->seq.p);
