@@ -615,6 +615,13 @@ struct Lane {
 	DBuf<uint8_t> seq, code, code_r;
 	DBuf<int64_t> off;
 	DBuf<int32_t> len;
+	// a second set of staged reads, filled on the copy stream while the lane
+	// runs the set before (host calls with several sub-batches a lane)
+	cudaStream_t cstream = nullptr;
+	cudaEvent_t cev[2][2]{};             // per set: copies issued, copies done
+	DBuf<uint8_t> seq2;
+	DBuf<int64_t> off2;
+	DBuf<int32_t> len2;
 	DBuf<uint2> hits;
 	DBuf<DPair> pairs;
 	DBuf<RmReq> q[2];
@@ -652,6 +659,13 @@ struct Lane {
 
 	void release()
 	{
+		seq2.release(); off2.release(); len2.release();
+		for (auto &s2 : cev)
+			for (auto &e : s2)
+				if (e)
+					cudaEventDestroy(e);
+		if (cstream)
+			cudaStreamDestroy(cstream);
 		seq.release(); code.release(); code_r.release(); off.release(); len.release();
 		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
 		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release();
@@ -890,10 +904,14 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	for (int i = 0; i < nlanes; ++i) {
 		Lane *L = new Lane();
 		ctx->lanes.push_back(L);
-		if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess)
+		if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess ||
+		    cudaStreamCreateWithFlags(&L->cstream, cudaStreamNonBlocking) != cudaSuccess)
 			return bail(HERA_GPU_ECUDA);
 		for (auto &e : L->ev)
 			cudaEventCreate(&e);
+		for (auto &s2 : L->cev)
+			for (auto &e : s2)
+				cudaEventCreate(&e);
 	}
 	// the allocation-free entry's lane: its stream, events and 32 pinned
 	// counters are made here, so that entry point itself allocates nothing
@@ -1643,10 +1661,18 @@ static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, u
 
 // stage host reads of [lo, lo+n) into lane L's pinned memory and device
 // buffers; mates interleaved in the offset table, sequences as blocks
-static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b, int32_t lo, int32_t n,
-		       int64_t *bytes, int *max_len)
+// Stage reads [lo, lo + n) into the lane's buffer set `set` (0: seq/off/len,
+// 1: seq2/off2/len2).  Synchronous on the lane's stream, or (async) on its
+// copy stream with cev[set][1] recorded when the copies are done; stage_wait
+// then waits for them.
+static int stage_reads_to(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b, int32_t lo, int32_t n,
+			  int64_t *bytes, int *max_len, int set, bool async)
 {
-	cudaStream_t st = L.stream;
+	cudaStream_t st = async ? L.cstream : L.stream;
+	DBuf<uint8_t> &dseq = set ? L.seq2 : L.seq;
+	DBuf<int64_t> &doff = set ? L.off2 : L.off;
+	DBuf<int32_t> &dlen = set ? L.len2 : L.len;
+	cudaEvent_t e0 = async ? L.cev[set][0] : L.ev[0], e1 = async ? L.cev[set][1] : L.ev[1];
 	const int per = b ? 2 : 1;
 	const hera_gpu_reads *src[2] = {a, b};
 	int64_t total = 0;
@@ -1701,29 +1727,41 @@ static int stage_reads(Lane &L, const hera_gpu_reads *a, const hera_gpu_reads *b
 	}
 	L.timing.host_stage_ms +=
 		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - h0).count();
-	LK(L.seq.ensure(total + 64), "device reads");
-	LK(L.off.ensure((size_t)n * per), "device offsets");
-	LK(L.len.ensure((size_t)n * per), "device lengths");
-	cudaEventRecord(L.ev[0], st);
+	LK(dseq.ensure(total + 64), "device reads");
+	LK(doff.ensure((size_t)n * per), "device offsets");
+	LK(dlen.ensure((size_t)n * per), "device lengths");
+	cudaEventRecord(e0, st);
 	if (!direct[0] && !direct[1]) {
-		LK(cudaMemcpyAsync(L.seq.p, L.h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
+		LK(cudaMemcpyAsync(dseq.p, L.h_seq.p, total, cudaMemcpyHostToDevice, st), "H2D reads");
 	} else {   // per mate block: from the caller's memory or from the staging
 		for (int m = 0; m < per; ++m) {
 			const void *from = direct[m] ? (const void *)direct[m] : (const void *)(L.h_seq.p + reg_o[m]);
 			if (reg_len[m] > 0)
-				LK(cudaMemcpyAsync(L.seq.p + reg_o[m], from, (size_t)reg_len[m], cudaMemcpyHostToDevice, st),
+				LK(cudaMemcpyAsync(dseq.p + reg_o[m], from, (size_t)reg_len[m], cudaMemcpyHostToDevice, st),
 				   "H2D reads");
 		}
 	}
-	LK(cudaMemcpyAsync(L.off.p, L.h_off.p, (size_t)n * per * 8, cudaMemcpyHostToDevice, st), "H2D");
-	LK(cudaMemcpyAsync(L.len.p, L.h_len.p, (size_t)n * per * 4, cudaMemcpyHostToDevice, st), "H2D");
-	cudaEventRecord(L.ev[1], st);
-	LK(cudaEventSynchronize(L.ev[1]), "H2D");
-	float ms = 0;
-	cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]);
-	L.timing.h2d_ms += ms;
+	LK(cudaMemcpyAsync(doff.p, L.h_off.p, (size_t)n * per * 8, cudaMemcpyHostToDevice, st), "H2D");
+	LK(cudaMemcpyAsync(dlen.p, L.h_len.p, (size_t)n * per * 4, cudaMemcpyHostToDevice, st), "H2D");
+	cudaEventRecord(e1, st);
+	if (!async) {
+		LK(cudaEventSynchronize(e1), "H2D");
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		L.timing.h2d_ms += ms;
+	}
 	*bytes = total;
 	*max_len = ml;
+	return HERA_GPU_OK;
+}
+
+// wait for an async stage_reads_to into `set`
+static int stage_wait(Lane &L, int set)
+{
+	LK(cudaEventSynchronize(L.cev[set][1]), "H2D");
+	float ms = 0;
+	cudaEventElapsedTime(&ms, L.cev[set][0], L.cev[set][1]);
+	L.timing.h2d_ms += ms;
 	return HERA_GPU_OK;
 }
 
@@ -1832,6 +1870,7 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 	int64_t ns = (n + (int64_t)ctx->max_batch - 1) / ctx->max_batch;
 	if (ns > 0 && n >= nlanes * 4096)
 		ns = (ns + nlanes - 1) / nlanes * nlanes;
+
 	const int32_t sub = ns > 0 ? (int32_t)((n + ns - 1) / ns) : 1;
 	const int nsub = (int)((n + (int64_t)sub - 1) / sub);
 	Sched S;
@@ -1844,30 +1883,58 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 	auto worker = [&](int li) {
 		cudaSetDevice(dev);
 		Lane &L = *ctx->lanes[li];
+		// a lane's sub-batches alternate between its two buffer sets: the
+		// next one is staged on the copy stream while this one runs
+		int b = 0;
+		int64_t sbytes[2] = {0, 0};
+		int smax[2] = {0, 0};
+		bool pending = false;   // an async stage into set b is in flight
+		auto drain = [&] {      // nothing left reading the caller's memory
+			if (pending)
+				cudaStreamSynchronize(L.cstream);
+			pending = false;
+		};
 		for (int k = li; k < nsub; k += nl) {
 			const int32_t lo = (int32_t)((int64_t)k * sub);
 			const int32_t m = (n - lo) < sub ? (n - lo) : sub;
-			int64_t bytes = 0;
-			int max_len = 0;
-			int rc = stage_reads(L, r1, r2, lo, m, &bytes, &max_len);
+			int rc = HERA_GPU_OK;
+			if (k == li)
+				rc = stage_reads_to(L, r1, r2, lo, m, &sbytes[b], &smax[b], b, false);
+			else if (pending)
+				rc = stage_wait(L, b);
+			pending = false;
+			const int kn = k + nl;
+			if (!rc && kn < nsub) {
+				const int32_t lon = (int32_t)((int64_t)kn * sub);
+				const int32_t mn = (n - lon) < sub ? (n - lon) : sub;
+				rc = stage_reads_to(L, r1, r2, lon, mn, &sbytes[b ^ 1], &smax[b ^ 1], b ^ 1, true);
+				pending = rc == HERA_GPU_OK;
+			}
 			if (!rc)
-				rc = run_batch(ctx, L, L.seq.p, L.off.p, L.len.p, m, paired, write_bam, max_len, bytes);
+				rc = run_batch(ctx, L, b ? L.seq2.p : L.seq.p, b ? L.off2.p : L.off.p, b ? L.len2.p : L.len.p, m,
+					       paired, write_bam, smax[b], sbytes[b]);
 			if (rc) {
+				drain();
 				S.failed(k, rc, L.err);
 				return;
 			}
 			S.publish(k, L.nl, L.no, L.nm);
 			uint64_t bl, bo, bm;
-			if (!S.prefix(k, bl, bo, bm))
+			if (!S.prefix(k, bl, bo, bm)) {
+				drain();
 				return;
+			}
 			if (bl + L.nl <= out->list_cap && bo + L.no <= out->op_cap && bm + L.nm <= out->miss_cap) {
 				rc = copy_out(L, out, (uint64_t)lo * ncand, bl, bo, bm);
 				if (rc) {
+					drain();
 					S.failed(k, rc, L.err);
 					return;
 				}
 			}
+			b ^= 1;
 		}
+		drain();
 	};
 	std::vector<std::thread> th;
 	for (int i = 1; i < nl; ++i)
