@@ -201,3 +201,28 @@ def test_align_fastq_rejects_like_reference(fq_ctx, config1):
     with pytest.raises(api.FastqFormatError) as e:
         fq_ctx.align_fastq_pairs(left, bad, 1)
     assert (e.value.bad_file, e.value.bad_read) == (2, 2)
+
+
+@pytest.mark.gpu
+def test_parse_grows_record_array(fq_ctx):
+    """Many one-base reads: more reads than the first record array holds,
+    so the call reports the count and is repeated with room for all."""
+    n = 12000
+    left = b"".join(b"@%d\nA\n+\nI\n" % i for i in range(n))
+    right = b"".join(b"@%d\nC\n+\nI\n" % i for i in range(n))
+    recs = fq_ctx.parse_fastq_pairs(left, right)
+    assert recs.shape[0] == 2 * n
+    assert np.array_equal(recs, oracle.parse_fq_pairs(left, right)[1])
+
+
+@pytest.mark.gpu
+def test_align_fastq_rejects_overlong_read(fq_ctx):
+    """Reads the aligner cannot take (longer than HERA_GPU_MAX_READ) are
+    refused with HERA_GPU_EINVAL, after a parse that accepts them."""
+    long = b"A" * (api.MAX_READ + 1)
+    left = b"@a\n" + long + b"\n+\n" + b"I" * len(long) + b"\n"
+    right = b"@a\nACGT\n+\nIIII\n"
+    assert fq_ctx.parse_fastq_pairs(left, right).shape[0] == 2
+    with pytest.raises(api.HeraGpuError) as e:
+        fq_ctx.align_fastq_pairs(left, right, 1)
+    assert e.value.code == -4
