@@ -95,6 +95,50 @@ def _pool_caps(n_recs: int, total_len: int):
     return n_recs * 64 + 1024, n_recs * 16 + total_len * 2 + 1024, total_len * 2 + 1024
 
 
+class ClassTable:
+    """The add_class state after a run (src/hash_align.c:1564-1602): classes
+    in first-insertion order (XXH32 id, read count, transcript list),
+    REF_INF->count per transcript, PAIRED and MEAN_FRAG's sum."""
+
+    def __init__(self, ids, counts, ns, ref_off, ref, tx_count, paired, mean_frag):
+        self.ids = np.asarray(ids, dtype=np.uint32)
+        self.counts = np.asarray(counts, dtype=np.float64)
+        self.ns = np.asarray(ns, dtype=np.uint32)
+        self.ref_off = np.asarray(ref_off, dtype=np.uint64)
+        self.ref = np.asarray(ref, dtype=np.uint32)
+        self.tx_count = np.asarray(tx_count, dtype=np.uint32)
+        self.paired = int(paired)
+        self.mean_frag = float(mean_frag)
+
+    @property
+    def n_classes(self) -> int:
+        return len(self.ids)
+
+    def lists(self):
+        return [tuple(self.ref[int(o):int(o) + int(n)]) for o, n in zip(self.ref_off, self.ns)]
+
+    def key(self):
+        """Everything the EM and the summary read, as plain values."""
+        return (tuple(self.ids.tolist()), tuple(self.counts.tolist()), tuple(self.lists()),
+                tuple(self.tx_count.tolist()), self.paired, self.mean_frag)
+
+
+def _export_classes(sizes, export, n_trans: int) -> ClassTable:
+    nc, rn = C.c_uint32(), C.c_uint64()
+    sizes(C.byref(nc), C.byref(rn))
+    nc, rn = nc.value, rn.value
+    ids = np.zeros(max(nc, 1), np.uint32)
+    counts = np.zeros(max(nc, 1), np.float64)
+    ns = np.zeros(max(nc, 1), np.uint32)
+    offs = np.zeros(max(nc, 1), np.uint64)
+    ref = np.zeros(max(rn, 1), np.uint32)
+    tx = np.zeros(max(n_trans, 1), np.uint32)
+    paired, mf = C.c_uint32(), C.c_double()
+    export(C.c_void_p(_ptr(ids)), C.c_void_p(_ptr(counts)), C.c_void_p(_ptr(ns)), C.c_void_p(_ptr(offs)),
+           C.c_void_p(_ptr(ref)), C.c_void_p(_ptr(tx)), C.byref(paired), C.byref(mf))
+    return ClassTable(ids[:nc], counts[:nc], ns[:nc], offs[:nc], ref[:rn], tx[:n_trans], paired.value, mf.value)
+
+
 class Oracle:
     """The C restatement (oracle/hera_oracle.c) bound to one index."""
 
@@ -141,6 +185,30 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle result pools too small")
         return res
+
+    def classes(self, results, paired: bool = True) -> ClassTable:
+        """add_class as the host tail calls it, over a sequence of flat
+        results (one per batch, in input order), on one class table."""
+        L = self.lib
+        L.ho_classes_new.restype = C.c_void_p
+        L.ho_classes_add.restype = C.c_int
+        h = L.ho_classes_new(C.c_uint32(self.ix.n_trans))
+        try:
+            for res in results:
+                n = len(res.recs) // 2 if paired else len(res.recs)
+                rc = L.ho_classes_add(C.c_void_p(h), C.c_void_p(_ptr(res.recs)), C.c_void_p(_ptr(res.pos_pool)),
+                                      C.c_void_p(_ptr(res.p_pool)), n, 1 if paired else 0)
+                if rc != 0:
+                    raise RuntimeError("a hit list names a transcript outside the index")
+            return _export_classes(lambda a, b: L.ho_classes_sizes(C.c_void_p(h), a, b),
+                                   lambda *a: L.ho_classes_export(C.c_void_p(h), *a), self.ix.n_trans)
+        finally:
+            L.ho_classes_free(C.c_void_p(h))
+
+    def xxh32(self, data: bytes, seed: int = 0) -> int:
+        self.lib.ho_xxh32.restype = C.c_uint32
+        b = _as_u8(data)
+        return int(self.lib.ho_xxh32(C.c_void_p(_ptr(b)), C.c_size_t(len(data)), C.c_uint32(seed)))
 
     def align_pairs_mt(self, r1, r2, write_bam: int, nthreads: int) -> None:
         self.lib.ho_align_pairs_mt(C.byref(self.cix), write_bam, r1.n,
@@ -249,6 +317,26 @@ class Reference:
         if rc != 0:
             raise RuntimeError("reference result pools too small")
         return res
+
+    def classes(self, r1, r2=None, n_trans: Optional[int] = None) -> ClassTable:
+        """The reference's whole worker per read (align_pair_read, or
+        align_single_read when r2 is None) with WRITE_BAM = 1, then its
+        add_class state.  Works on copies of the reads."""
+        L = self.lib
+        s1, o1, l1 = r1.seq.copy(), r1.off, r1.len
+        if r2 is not None:
+            s2, o2, l2 = r2.seq.copy(), r2.off, r2.len
+        else:
+            s2, o2, l2 = s1, o1, l1
+        L.refh_classes_run(1 if r2 is not None else 0, r1.n,
+                           C.c_void_p(_ptr(s1)), C.c_void_p(_ptr(o1)), C.c_void_p(_ptr(l1)),
+                           C.c_void_p(_ptr(s2)), C.c_void_p(_ptr(o2)), C.c_void_p(_ptr(l2)))
+        return _export_classes(L.refh_classes_sizes, L.refh_classes_export, n_trans)
+
+    def xxh32(self, data: bytes, seed: int = 0) -> int:
+        self.lib.refh_xxh32.restype = C.c_uint32
+        b = _as_u8(data)
+        return int(self.lib.refh_xxh32(C.c_void_p(_ptr(b)), C.c_size_t(len(data)), C.c_uint32(seed)))
 
     def align_pairs_mt(self, r1, r2, write_bam: int, nthreads: int) -> None:
         self.lib.refh_align_pairs_mt(write_bam, r1.n,

@@ -1366,3 +1366,247 @@ int ho_parse_fq_single(const char *buf, int64_t n, ho_fq_rec *out, int32_t cap,
 	*n_reads = k;
 	return k > cap ? HO_FQ_CAP : HO_FQ_OK;
 }
+
+/* ===========================================================================
+ * Equivalence classes: the host tail's add_class calls
+ * ======================================================================== */
+
+/* XXH32, restated from the published xxHash specification (32-bit variant,
+ * little-endian input).  hera vendors it as src/xxhash.c and calls it once
+ * per class key in add_class (src/hash_align.c:1576). */
+#define XP1 2654435761u
+#define XP2 2246822519u
+#define XP3 3266489917u
+#define XP4 668265263u
+#define XP5 374761393u
+static uint32_t xrotl(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
+static uint32_t xrd32(const uint8_t *p)
+{
+	return (uint32_t)p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24;
+}
+static uint32_t xround(uint32_t acc, uint32_t in) { return xrotl(acc + in * XP2, 13) * XP1; }
+
+uint32_t ho_xxh32(const void *buf, size_t len, uint32_t seed)
+{
+	const uint8_t *p = (const uint8_t *)buf, *end = p + len;
+	uint32_t h;
+	if (len >= 16) {
+		uint32_t v1 = seed + XP1 + XP2, v2 = seed + XP2, v3 = seed, v4 = seed - XP1;
+		const uint8_t *lim = end - 16;
+		do {
+			v1 = xround(v1, xrd32(p));
+			v2 = xround(v2, xrd32(p + 4));
+			v3 = xround(v3, xrd32(p + 8));
+			v4 = xround(v4, xrd32(p + 12));
+			p += 16;
+		} while (p <= lim);
+		h = xrotl(v1, 1) + xrotl(v2, 7) + xrotl(v3, 12) + xrotl(v4, 18);
+	} else {
+		h = seed + XP5;
+	}
+	h += (uint32_t)len;
+	for (; p + 4 <= end; p += 4)
+		h = xrotl(h + xrd32(p) * XP3, 17) * XP4;
+	for (; p < end; ++p)
+		h = xrotl(h + *p * XP5, 11) * XP1;
+	h ^= h >> 15;
+	h *= XP2;
+	h ^= h >> 13;
+	h *= XP3;
+	h ^= h >> 16;
+	return h;
+}
+
+struct ho_classes {
+	uint32_t n_trans;
+	uint32_t n, cap;            /* classes in first-insertion order */
+	uint32_t *id, *cn;
+	double *count;
+	uint64_t *ref_off;
+	uint32_t *ref;              /* class lists back to back */
+	uint64_t ref_n, ref_cap;
+	uint32_t *map;              /* open addressing on id: class index + 1 */
+	uint64_t map_slots;
+	uint32_t *tx_count;         /* REF_INF->count */
+	uint32_t paired;            /* PAIRED */
+	double mean_frag;           /* MEAN_FRAG before main.c divides it */
+};
+
+ho_classes *ho_classes_new(uint32_t n_trans)
+{
+	ho_classes *c = calloc(1, sizeof *c);
+	c->n_trans = n_trans;
+	c->tx_count = calloc(n_trans ? n_trans : 1, sizeof(uint32_t));
+	c->map_slots = 1024;
+	c->map = calloc(c->map_slots, sizeof(uint32_t));
+	return c;
+}
+
+void ho_classes_free(ho_classes *c)
+{
+	if (!c)
+		return;
+	free(c->id); free(c->cn); free(c->count); free(c->ref_off); free(c->ref);
+	free(c->map); free(c->tx_count); free(c);
+}
+
+/* Slot of `id` in the map: the slot holding it, or the empty slot where it
+ * goes.  hera probes a 2^27-slot map the same way (src/hash_align.c:
+ * 1576-1584); the class an id lands in depends only on the id, because a
+ * class is found by comparing ids, so the map's size is not visible. */
+static uint64_t cls_slot(const ho_classes *c, uint32_t id)
+{
+	uint64_t s = id & (c->map_slots - 1);
+	while (c->map[s] && c->id[c->map[s] - 1] != id)
+		s = (s + 1) & (c->map_slots - 1);
+	return s;
+}
+
+static void cls_grow_map(ho_classes *c)
+{
+	free(c->map);
+	c->map_slots *= 2;
+	c->map = calloc(c->map_slots, sizeof(uint32_t));
+	for (uint32_t i = 0; i < c->n; ++i)
+		c->map[cls_slot(c, c->id[i])] = i + 1;
+}
+
+/* add_class (src/hash_align.c:1564-1602) for a Candidate whose list 0 is
+ * the concatenation a[0..na) ++ b[0..nb) (concate_candidate :1604-1618 and
+ * the single-read merges :1842-1850 build such lists). */
+static int cls_add(ho_classes *c, const uint32_t *a, uint32_t na, const uint32_t *b, uint32_t nb,
+		   int err_sum, int pair, int32_t p00, int32_t p10)
+{
+	++c->paired;
+	if (pair == 1) {
+		int32_t d = p00 - p10;
+		c->mean_frag += d < 0 ? -d : d;
+	}
+	const uint32_t n = na + nb;
+	if (n == 1) {
+		uint32_t t = na ? a[0] : b[0];
+		if (t >= c->n_trans)
+			return -1;
+		++c->tx_count[t];
+		return 0;
+	}
+	if (err_sum >= HO_ERR)
+		return 0;
+	uint32_t *key = malloc((n ? n : 1) * sizeof(uint32_t));
+	if (na)
+		memcpy(key, a, na * sizeof(uint32_t));
+	if (nb)
+		memcpy(key + na, b, nb * sizeof(uint32_t));
+	uint32_t id = ho_xxh32(key, (size_t)n * sizeof(uint32_t), 0);
+	uint64_t s = cls_slot(c, id);
+	if (c->map[s]) {
+		c->count[c->map[s] - 1] += 1;
+		free(key);
+		return 0;
+	}
+	if (c->n == c->cap) {
+		c->cap = c->cap ? 2 * c->cap : 1024;
+		c->id = realloc(c->id, c->cap * sizeof(uint32_t));
+		c->cn = realloc(c->cn, c->cap * sizeof(uint32_t));
+		c->count = realloc(c->count, c->cap * sizeof(double));
+		c->ref_off = realloc(c->ref_off, c->cap * sizeof(uint64_t));
+	}
+	if (c->ref_n + n > c->ref_cap) {
+		while (c->ref_n + n > c->ref_cap)
+			c->ref_cap = c->ref_cap ? 2 * c->ref_cap : 4096;
+		c->ref = realloc(c->ref, c->ref_cap * sizeof(uint32_t));
+	}
+	c->id[c->n] = id;
+	c->cn[c->n] = n;
+	c->count[c->n] = 1;
+	c->ref_off[c->n] = c->ref_n;
+	memcpy(c->ref + c->ref_n, key, (size_t)n * sizeof(uint32_t));
+	c->ref_n += n;
+	c->map[s] = ++c->n;
+	free(key);
+	if (2 * (uint64_t)c->n > c->map_slots)
+		cls_grow_map(c);
+	return 0;
+}
+
+int ho_classes_add(ho_classes *c, const ho_rec *recs, const uint32_t *pos_pool,
+		   const int32_t *p_pool, int n, int paired)
+{
+	for (int i = 0; i < n; ++i) {
+		int rc = 0;
+		if (paired) {
+			/* align_pair_read's tail (src/hash_align.c:1735-1760); with
+			 * FMINDEX NULL check_in_genome changes nothing (:1697-1701) */
+			const ho_rec *a = &recs[2 * i], *b = &recs[2 * i + 1];
+			int pa = a->pair, pb = b->pair;
+			const int sa = a->err[0] + a->err[1], sb = b->err[0] + b->err[1];
+			if (sa < sb)
+				pb = -1;
+			else if (sa > sb)
+				pa = -1;
+			const ho_rec *r = NULL, *m = NULL;   /* class source, appended mate */
+			if (pa > 1 && pb > 1) {
+				if ((pa & 1) + (pb & 1) == 0) {
+					r = a;
+					m = b;
+				}
+			} else if (pa > 1) {
+				if ((pa & 1) == 0)
+					r = a;
+			} else if (pb > 1) {
+				if ((pb & 1) == 0)
+					r = b;
+			}
+			if (!r)
+				continue;
+			const uint32_t *l0 = pos_pool + r->list_off[0];
+			const uint32_t *l1 = m ? pos_pool + m->list_off[0] : NULL;
+			const uint32_t n0 = (uint32_t)r->n[0], n1 = m ? (uint32_t)m->n[0] : 0;
+			/* p[0][0] / p[1][0] after concate_candidate: r's first entry
+			 * when r has one, else the appended mate's */
+			int32_t p00 = n0 ? p_pool[r->list_off[0]] : (n1 ? p_pool[m->list_off[0]] : 0);
+			int32_t p10 = r->n[1] ? p_pool[r->list_off[1]]
+					      : (m && m->n[1] ? p_pool[m->list_off[1]] : 0);
+			rc = cls_add(c, l0, n0, l1, n1, r->err[0] + r->err[1], 1, p00, p10);
+		} else {
+			/* align_single_read's tail (src/hash_align.c:1825-1851) */
+			const ho_rec *r = &recs[i];
+			if (r->n[0] == 0 && r->n[1] == 0)
+				continue;
+			const uint32_t *l0 = pos_pool + r->list_off[0], *l1 = pos_pool + r->list_off[1];
+			const int es = r->err[0] + r->err[1];
+			if (r->err[0] > r->err[1])          /* move_candidate(r, 0, 1) */
+				rc = cls_add(c, l1, (uint32_t)r->n[1], NULL, 0, es, 0, 0, 0);
+			else if (r->err[0] == r->err[1])    /* list 1 appended to list 0 */
+				rc = cls_add(c, l0, (uint32_t)r->n[0], l1, (uint32_t)r->n[1], es, 0, 0, 0);
+			else
+				rc = cls_add(c, l0, (uint32_t)r->n[0], NULL, 0, es, 0, 0, 0);
+		}
+		if (rc)
+			return rc;
+	}
+	return 0;
+}
+
+void ho_classes_sizes(const ho_classes *c, uint32_t *n_classes, uint64_t *ref_n)
+{
+	*n_classes = c->n;
+	*ref_n = c->ref_n;
+}
+
+void ho_classes_export(const ho_classes *c, uint32_t *id, double *count, uint32_t *n,
+		       uint64_t *ref_off, uint32_t *ref, uint32_t *tx_count,
+		       uint32_t *paired, double *mean_frag)
+{
+	if (c->n) {
+		memcpy(id, c->id, c->n * sizeof(uint32_t));
+		memcpy(count, c->count, c->n * sizeof(double));
+		memcpy(n, c->cn, c->n * sizeof(uint32_t));
+		memcpy(ref_off, c->ref_off, c->n * sizeof(uint64_t));
+	}
+	if (c->ref_n)
+		memcpy(ref, c->ref, c->ref_n * sizeof(uint32_t));
+	memcpy(tx_count, c->tx_count, c->n_trans * sizeof(uint32_t));
+	*paired = c->paired;
+	*mean_frag = c->mean_frag;
+}

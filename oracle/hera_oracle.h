@@ -139,6 +139,27 @@ int ho_parse_fq_pairs(const char *left, int64_t n_left, const char *right, int64
 int ho_parse_fq_single(const char *buf, int64_t n, ho_fq_rec *out, int32_t cap,
 		       int32_t *n_reads, int64_t *bad_rec);
 
+/* Equivalence classes as the host tail builds them: the add_class calls of
+ * align_pair_read (src/hash_align.c:1735-1760) and align_single_read
+ * (:1835-1851), applied in input order to records in the flat layout.
+ * State: the class table (id = XXH32 of the class's transcript list, count,
+ * list), per-transcript counts of single-hit reads (REF_INF->count), PAIRED
+ * and MEAN_FRAG's running sum. */
+typedef struct ho_classes ho_classes;
+ho_classes *ho_classes_new(uint32_t n_trans);
+void ho_classes_free(ho_classes *c);
+/* paired = 1: n pairs, recs[2i] / recs[2i+1] = r[0] / r[1]; paired = 0: n
+ * single reads.  Returns 0, or -1 on a list entry outside the transcripts. */
+int ho_classes_add(ho_classes *c, const ho_rec *recs, const uint32_t *pos_pool,
+		   const int32_t *p_pool, int n, int paired);
+void ho_classes_sizes(const ho_classes *c, uint32_t *n_classes, uint64_t *ref_n);
+/* id/count/n/ref_off: n_classes entries; ref: ref_n; tx_count: n_trans. */
+void ho_classes_export(const ho_classes *c, uint32_t *id, double *count, uint32_t *n,
+		       uint64_t *ref_off, uint32_t *ref, uint32_t *tx_count,
+		       uint32_t *paired, double *mean_frag);
+/* XXH32 (the published xxHash 32-bit algorithm) as add_class uses it. */
+uint32_t ho_xxh32(const void *buf, size_t len, uint32_t seed);
+
 #ifdef __cplusplus
 }
 #endif

@@ -375,3 +375,101 @@ int refh_parse_fq_single(char *buf, int64_t *rec, int32_t cap, int32_t *n_reads,
 	*n_reads = k;
 	return k > cap ? -2 : 0;
 }
+
+/* ---- equivalence classes: the reference's whole per-read worker ---------
+ * align_pair_read / align_single_read (src/hash_align.c:1717-1853) run
+ * unchanged with WRITE_BAM = 1 (no `-w`: bam_write_pair and
+ * bam_write_single return at once, src/bam_write.c:386-387, 421-422), on a
+ * fresh class table (init_class, :1161-1167) and zeroed REF_INF->count,
+ * PAIRED and MEAN_FRAG.  The sequences are modified in place (the tail's
+ * reverse_str calls), so callers pass copies.  Afterwards refh_classes_*
+ * read the add_class state back. */
+void init_class();
+void align_pair_read(struct read_inf *r1, struct read_inf *r2, char *stream, unsigned int *slen);
+void align_single_read(struct read_inf *read, char *stream, unsigned int *slen);
+unsigned int XXH32(const void *input, size_t len, unsigned int seed);
+
+static void classes_reset(void)
+{
+	uint32_t i;
+	if (CLASS) {
+		for (i = 0; i < CLASS->n; ++i)
+			if (CLASS->cls[i].n)
+				free(CLASS->cls[i].ref);
+		free(CLASS->cls);
+		free(CLASS->map);
+		free(CLASS);
+		CLASS = NULL;
+	}
+	init_class();
+	memset(REF_INF->count, 0, REF_INF->n * sizeof(int));
+	PAIRED = 0;
+	MEAN_FRAG = 0;
+}
+
+int refh_classes_run(int paired, int n, char *seq1, const int64_t *off1, const int32_t *len1,
+		     char *seq2, const int64_t *off2, const int32_t *len2)
+{
+	int i, max_len = 1;
+	char name[] = "r/1";
+	unsigned int slen = 0;
+	char *q1, *q2;
+
+	/* the tail reverses the quality strings with the sequences */
+	for (i = 0; i < n; ++i) {
+		if (len1[i] > max_len)
+			max_len = len1[i];
+		if (paired && len2[i] > max_len)
+			max_len = len2[i];
+	}
+	q1 = malloc(max_len + 1);
+	q2 = malloc(max_len + 1);
+	WRITE_BAM = 1;
+	classes_reset();
+	for (i = 0; i < n; ++i) {
+		struct read_inf a = {seq1 + off1[i], name, q1, len1[i]};
+		if (paired) {
+			struct read_inf b = {seq2 + off2[i], name, q2, len2[i]};
+			align_pair_read(&a, &b, NULL, &slen);
+		} else {
+			align_single_read(&a, NULL, &slen);
+		}
+	}
+	free(q1);
+	free(q2);
+	return 0;
+}
+
+void refh_classes_sizes(uint32_t *n_classes, uint64_t *ref_n)
+{
+	uint64_t s = 0;
+	uint32_t i;
+	for (i = 0; i < CLASS->n; ++i)
+		s += CLASS->cls[i].n;
+	*n_classes = CLASS->n;
+	*ref_n = s;
+}
+
+void refh_classes_export(uint32_t *id, double *count, uint32_t *n, uint64_t *ref_off,
+			 uint32_t *ref, uint32_t *tx_count, uint32_t *paired, double *mean_frag)
+{
+	uint64_t s = 0;
+	uint32_t i;
+	for (i = 0; i < CLASS->n; ++i) {
+		id[i] = CLASS->cls[i].id;
+		count[i] = CLASS->cls[i].count;
+		n[i] = CLASS->cls[i].n;
+		ref_off[i] = s;
+		if (CLASS->cls[i].n)
+			memcpy(ref + s, CLASS->cls[i].ref, CLASS->cls[i].n * sizeof(uint32_t));
+		s += CLASS->cls[i].n;
+	}
+	memcpy(tx_count, REF_INF->count, REF_INF->n * sizeof(uint32_t));
+	*paired = PAIRED;
+	*mean_frag = MEAN_FRAG;
+}
+
+unsigned int refh_xxh32(const void *buf, size_t len, unsigned int seed)
+{
+	return XXH32(buf, len, seed);
+}

@@ -119,3 +119,37 @@ def test_single_records_golden(orc, wb):
     got = orc.align_single(rs, wb).canonical()
     want = _golden_result(d, f"single_wb{wb}")
     assert got == want
+
+
+def test_xxh32_golden(orc):
+    """XXH32 as add_class keys classes with it (src/hash_align.c:1576)."""
+    d = np.load(os.path.join(GOLD, "classes.npz"))
+    buf, lens = d["xxh_buf"].tobytes(), d["xxh_len"]
+    off = np.concatenate([[0], np.cumsum(lens)])
+    for k in range(len(lens)):
+        assert orc.xxh32(buf[off[k]:off[k + 1]]) == int(d["xxh_id"][k]), f"length {lens[k]}"
+
+
+def _golden_classes(d, name):
+    return oracle.ClassTable(d[f"{name}_ids"], d[f"{name}_counts"], d[f"{name}_ns"], d[f"{name}_ref_off"],
+                             d[f"{name}_ref"], d[f"{name}_tx"], int(d[f"{name}_paired"][0]),
+                             float(d[f"{name}_mean_frag"][0]))
+
+
+def _golden_records(d, key):
+    res = oracle.Result(d[f"{key}_recs"].shape[0], 1, 1, 1)
+    res.recs = d[f"{key}_recs"]
+    res.pos_pool, res.p_pool = d[f"{key}_pos"], d[f"{key}_p"]
+    return res
+
+
+@pytest.mark.parametrize("name", SETS + ["single"])
+def test_classes_golden(orc, name):
+    """The host tail's add_class calls restated over the golden records give
+    the class table, REF_INF->count, PAIRED and MEAN_FRAG that the
+    reference's own worker built from the same reads."""
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "classes.npz"))
+    got = orc.classes([_golden_records(c, f"{name}_wb1")], paired=name != "single")
+    want = _golden_classes(d, name)
+    assert got.key() == want.key()

@@ -36,3 +36,23 @@ def test_reads_modified_like_reference(both):
     ref.align_pairs(b1, b2, 1)
     assert np.array_equal(a1.seq, b1.seq) and np.array_equal(a2.seq, b2.seq)
     assert not np.isin(a1.seq, np.frombuffer(b"acgt", np.uint8)).any()
+
+
+@pytest.mark.parametrize("wl", ["config1", "config4"])
+def test_classes_match_reference(both, wl):
+    """add_class restated over the oracle's records, in batches, against the
+    reference's whole worker (align_pair_read, add_class included)."""
+    ann, tx, o, ref = both
+    r1, r2 = workloads.pairs(wl, ann, tx, 6000, seed=103)
+    want = ref.classes(r1, r2, o.ix.n_trans)
+    whole = o.align_pairs(r1.copy(), r2.copy(), 1)
+    assert o.classes([whole]).key() == want.key()
+    parts = [o.align_pairs(r1.subset(np.arange(a, b)), r2.subset(np.arange(a, b)), 1) for a, b in ((0, 1000), (1000, 3500), (3500, 6000))]
+    assert o.classes(parts).key() == want.key()
+
+
+def test_single_classes_match_reference(both):
+    ann, tx, o, ref = both
+    rs = synth.simulate_single(tx, 3000, seed=104)
+    want = ref.classes(rs, None, o.ix.n_trans)
+    assert o.classes([o.align_single(rs.copy(), 1)], paired=False).key() == want.key()
