@@ -317,8 +317,15 @@ def main():
                                     args.write_bam, kctx.stream)
         torch.cuda.synchronize()
         tm = kctx.timing()
+        cls = None
+        if rank == 0 and world == 1:
+            try:
+                cls = classes_leg(kctx, args.chunk)
+            except Exception as e:
+                log(f"classes leg failed: {e}")
+                cls = {"error": str(e)}
         kctx.close()
-        return tm
+        return tm, cls
 
     paths = [p for p in args.paths.split(",") if p]
     plain = None
@@ -369,7 +376,7 @@ def main():
     st = batched["stage"]
     tuning = ctx.tuning() if main_path == "batched" else None
     ctx.close()
-    ktm = kernel_pass() if main_path == "batched" else None
+    ktm, classes = kernel_pass() if main_path == "batched" else (None, None)
     dpx = api.dpx_peak(local)
     pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
     roof, roof_seed, roof_rescue = roofline(ktm, dpx, args, pair_bytes, max_len)
@@ -414,12 +421,43 @@ def main():
             "kernel_ms_per_step": None if ktm is None else {
                 k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
                                                      "rescue_kernel_ms", "resolve_ms", "pack_ms")},
-            "tuning": tuning, "serving": serving, "fastq": fastq, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": batched["launches"], "clocks": batched["clocks"],
+            "tuning": tuning, "serving": serving, "fastq": fastq, "classes": classes, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": batched["launches"], "clocks": batched["clocks"],
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def classes_leg(kctx, pairs: int) -> dict:
+    """hera's add_class on the device (hera_gpu_classes_add_last) over the
+    device-resident records of the step kctx just ran: kernel time with a
+    fresh table (every class inserted) and with the same records again
+    (every class found).  Bytes counted: each pair's two 52-byte records
+    plus 4 B per list entry the tail hashes."""
+    from hera_b200 import api
+    out = {}
+    cls = api.Classes(kctx, max_classes=1 << 22, max_list=1 << 26)
+    try:
+        cls.add_last(kctx)
+        first = cls.timing()
+        t = cls.fetch()
+        cls.add_last(kctx)
+        again = cls.timing()
+    finally:
+        cls.close()
+    hashed = int(t.ns.sum()) + int(t.tx_count.sum())
+    algo = 104 * pairs + 4 * hashed
+    peak = _hbm_peak()
+    for tag, tm in (("insert", first), ("lookup", again)):
+        ms = tm["kernel_ms"]
+        gbs = algo / (ms / 1e3) / 1e9 if ms > 0 else None
+        out[tag] = {"kernel_ms": round(ms, 4), "pairs_per_s": pairs / (ms / 1e3) if ms > 0 else None,
+                    "launches": tm["launches"], "achieved_gbs": gbs,
+                    "frac_of_hbm": None if gbs is None else gbs / peak[0]}
+    out.update({"classes": t.n_classes, "paired": t.paired, "single_transcript_reads": int(t.tx_count.sum()),
+                "algorithmic_bytes": algo, "hbm_peak": peak[1]})
+    return out
 
 
 def _hbm_peak():

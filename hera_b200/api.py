@@ -156,6 +156,13 @@ class Timing(C.Structure):
 _lib = None
 
 
+class _ClassTable(C.Structure):
+    _fields_ = [("class_cap", C.c_uint32), ("id", C.c_void_p), ("count", C.c_void_p), ("n", C.c_void_p),
+                ("list_off", C.c_void_p), ("list_cap", C.c_uint64), ("list", C.c_void_p),
+                ("tx_count", C.c_void_p), ("n_classes", C.c_uint32), ("list_used", C.c_uint64),
+                ("paired", C.c_uint32), ("mean_frag_sum", C.c_double)]
+
+
 def load_library(path: str = LIB_PATH) -> C.CDLL:
     """Load libhera_b200.so (raises if it has not been built)."""
     global _lib
@@ -204,6 +211,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                                C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                                C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(_Result)]
     lib.hera_gpu_get_fastq_stats.argtypes = [C.c_void_p, C.POINTER(FastqStats)]
+    lib.hera_gpu_classes_create.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]
+    lib.hera_gpu_classes_destroy.argtypes = [C.c_void_p]
+    lib.hera_gpu_classes_add_last.argtypes = [C.c_void_p, C.c_void_p]
+    lib.hera_gpu_classes_add_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                                C.c_int, C.c_void_p]
+    lib.hera_gpu_classes_fetch.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
+    lib.hera_gpu_classes_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]
+    lib.hera_gpu_classes_last_error.restype = C.c_char_p
+    lib.hera_gpu_classes_last_error.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -594,3 +610,88 @@ def tally(res: Result) -> dict:
     return {"pairs": int(a.shape[0]), "mapped": int((hits > 0).sum()), "paired": int((a["pair"] == 2).sum()),
             "hits": int(hits.sum()),
             "cigar_ops": int(a["n_cigar"].astype(np.int64).sum() + b["n_cigar"].astype(np.int64).sum())}
+
+
+class ClassTable:
+    """A class table copied off the device: hera's CLASS (classes in
+    first-insertion order: XXH32 id, read count, transcript list),
+    REF_INF->count, PAIRED and MEAN_FRAG's running sum."""
+
+    def __init__(self, ids, counts, ns, list_off, lists, tx_count, paired, mean_frag):
+        self.ids, self.counts, self.ns = ids, counts, ns
+        self.ref_off, self.ref, self.tx_count = list_off, lists, tx_count
+        self.paired, self.mean_frag = int(paired), float(mean_frag)
+
+    @property
+    def n_classes(self) -> int:
+        return len(self.ids)
+
+    def lists(self):
+        return [tuple(self.ref[int(o):int(o) + int(n)]) for o, n in zip(self.ref_off, self.ns)]
+
+    def key(self):
+        """Everything hera's EM and summary read, as plain values."""
+        return (tuple(self.ids.tolist()), tuple(self.counts.tolist()), tuple(self.lists()),
+                tuple(self.tx_count.tolist()), self.paired, self.mean_frag)
+
+
+class Classes:
+    """hera's add_class (src/hash_align.c:1564-1602) on the device: one class
+    table that the records of a run are added to batch by batch, in input
+    order.  A context's device-resident results go in with add_last(),
+    records already in device memory with add_device()."""
+
+    def __init__(self, ctx: "Context", max_classes: int = 1 << 20, max_list: int = 1 << 24):
+        self.lib = ctx.lib
+        self.n_trans = ctx.index.n_trans
+        h = C.c_void_p()
+        ctx._check(self.lib.hera_gpu_classes_create(ctx.h, max_classes, max_list, C.byref(h)))
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != HERA_GPU_OK:
+            raise HeraGpuError(rc, self.lib.hera_gpu_classes_last_error(self.h).decode())
+
+    def add_last(self, ctx: "Context") -> None:
+        """The pairs of ctx's last align_pairs_device call."""
+        self._check(self.lib.hera_gpu_classes_add_last(self.h, ctx.h))
+
+    def add_device(self, d_recs: int, d_pos_pool: int, d_p_pool: int, n: int, paired: bool = True,
+                   stream: Optional[int] = None) -> None:
+        self._check(self.lib.hera_gpu_classes_add_device(self.h, d_recs, d_pos_pool, d_p_pool, n,
+                                                         1 if paired else 0, stream))
+
+    def timing(self) -> dict:
+        ms, n = C.c_float(), C.c_uint32()
+        self.lib.hera_gpu_classes_timing(self.h, C.byref(ms), C.byref(n))
+        return {"kernel_ms": ms.value, "launches": n.value}
+
+    def fetch(self) -> ClassTable:
+        t = _ClassTable()
+        rc = self.lib.hera_gpu_classes_fetch(self.h, C.byref(t))
+        if rc != HERA_GPU_OK and rc != HERA_GPU_ECAPACITY:
+            self._check(rc)
+        nc, nl = t.n_classes, t.list_used
+        ids = np.zeros(max(nc, 1), np.uint32)
+        counts = np.zeros(max(nc, 1), np.float64)
+        ns = np.zeros(max(nc, 1), np.uint32)
+        offs = np.zeros(max(nc, 1), np.uint64)
+        lists = np.zeros(max(nl, 1), np.uint32)
+        tx = np.zeros(max(self.n_trans, 1), np.uint32)
+        t.class_cap, t.list_cap = nc, nl
+        t.id, t.count, t.n, t.list_off = _ptr(ids), _ptr(counts), _ptr(ns), _ptr(offs)
+        t.list, t.tx_count = _ptr(lists), _ptr(tx)
+        self._check(self.lib.hera_gpu_classes_fetch(self.h, C.byref(t)))
+        return ClassTable(ids[:nc], counts[:nc], ns[:nc], offs[:nc], lists[:nl], tx[:self.n_trans],
+                          t.paired, t.mean_frag_sum)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hera_gpu_classes_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -656,6 +656,9 @@ struct Lane {
 	// result of the last batch this lane ran (held in its device pools)
 	int32_t items = 0, ncand = 0;
 	uint64_t nl = 0, no = 0, nm = 0;
+	// pool offsets the device records were last rebased by (a fetch into
+	// page-locked memory rebases them in place); 0 after each batch
+	uint32_t rb_l = 0, rb_o = 0, rb_m = 0;
 
 	void release()
 	{
@@ -1385,6 +1388,7 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 		       tm = (uint32_t)L.h_small.p[4];
 	const int fl = L.h_small.p[5];
 	L.items = items;
+	L.rb_l = L.rb_o = L.rb_m = 0;
 	L.nl = tl;
 	L.no = to;
 	L.nm = tm;
@@ -1427,6 +1431,7 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 	T.launches += launches;
 	T.rescue_rounds += rounds;
 	L.items = items;
+	L.rb_l = L.rb_o = L.rb_m = 0;
 	L.ncand = ncand;
 	L.nl = tl;
 	L.no = to;
@@ -1567,6 +1572,7 @@ static bool host_pinned(const void *p, size_t bytes)
 }
 
 // records of a sub-batch rebased to the caller's pool offsets on the device
+// (by the difference to the offsets they were last rebased to; u32 wrap-around)
 __global__ void k_rebase_recs(hera_cand_rec *__restrict__ r, int n, uint32_t bl, uint32_t bo, uint32_t bm)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1592,8 +1598,11 @@ static int copy_out(Lane &L, hera_gpu_result *out, uint64_t rec0, uint64_t bl, u
 	    (!L.no || host_pinned(out->op_pool + bo, L.no * 4)) && (!L.nm || host_pinned(out->miss_pool + bm, L.nm))) {
 		cudaEventRecord(L.ev[6], st);
 		if (items > 0)
-			k_rebase_recs<<<blocks_for(items, 256), 256, 0, st>>>(L.recs.p, items, (uint32_t)bl, (uint32_t)bo,
-									       (uint32_t)bm);
+			k_rebase_recs<<<blocks_for(items, 256), 256, 0, st>>>(L.recs.p, items, (uint32_t)bl - L.rb_l,
+									       (uint32_t)bo - L.rb_o, (uint32_t)bm - L.rb_m);
+		L.rb_l = (uint32_t)bl;
+		L.rb_o = (uint32_t)bo;
+		L.rb_m = (uint32_t)bm;
 		LK(cudaMemcpyAsync(out->recs + rec0, L.recs.p, items * sizeof(hera_cand_rec), cudaMemcpyDeviceToHost, st),
 		   "D2H");
 		if (L.nl) {
@@ -2584,3 +2593,4 @@ extern "C" int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s)
 
 #include "hera_server.cuh"
 #include "hera_fastq.cuh"
+#include "hera_classes.cuh"

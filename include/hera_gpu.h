@@ -469,6 +469,65 @@ int hera_gpu_get_fastq_stats(hera_gpu_ctx *ctx, hera_gpu_fastq_stats *out);
 int hera_gpu_fastq_read_inf(char *buf, int64_t n, const hera_gpu_fastq_rec *recs,
 			    int32_t count, int32_t stride, hera_read_inf *out);
 
+/* ---- equivalence classes ---------------------------------------------------
+ * The add_class calls of hera's host tail (src/hash_align.c:1564-1602), made
+ * by align_pair_read (:1735-1760) and align_single_read (:1825-1851), run on
+ * the device over flat records.  A class table holds, like hera's CLASS and
+ * REF_INF->count globals: the classes in first-insertion order (XXH32 id of
+ * the transcript list, read count, the list), the per-transcript count of
+ * reads with a one-entry list, PAIRED and the running sum behind MEAN_FRAG
+ * (before src/main.c:30 divides it).  Adding the records of a run batch by
+ * batch, in input order, gives exactly the table hera's `-t 1` worker
+ * builds.  With FMINDEX NULL (no `-f`), as everywhere in this library. */
+typedef struct hera_gpu_classes hera_gpu_classes;
+
+/* Host buffers for hera_gpu_classes_fetch.  On return n_classes and
+ * list_used hold the table's sizes; with class_cap or list_cap too small the
+ * call returns HERA_GPU_ECAPACITY and fills only those. */
+typedef struct hera_gpu_class_table {
+	uint32_t class_cap;
+	uint32_t *id;            /* Class.id    [class_cap] */
+	double *count;           /* Class.count [class_cap] */
+	uint32_t *n;             /* Class.n     [class_cap] */
+	uint64_t *list_off;      /* class i's list: list[list_off[i] .. + n[i]) */
+	uint64_t list_cap;
+	uint32_t *list;          /* Class.ref lists back to back [list_cap] */
+	uint32_t *tx_count;      /* REF_INF->count [n_trans]; may be NULL */
+	uint32_t n_classes;
+	uint64_t list_used;
+	uint32_t paired;         /* PAIRED */
+	double mean_frag_sum;    /* MEAN_FRAG before the division */
+} hera_gpu_class_table;
+
+/* A class table on ctx's device holding at most max_classes classes and
+ * max_list list entries in total (device memory: about 24 B a class slot,
+ * 28 B a class, 4 B a list entry, 4 B a transcript).  Replaces hera's
+ * init_class (src/hash_align.c:1161-1167) and the zeroing of REF_INF->count,
+ * PAIRED and MEAN_FRAG. */
+int hera_gpu_classes_create(hera_gpu_ctx *ctx, uint32_t max_classes, uint64_t max_list,
+			    hera_gpu_classes **out);
+void hera_gpu_classes_destroy(hera_gpu_classes *c);
+
+/* add_class for the pairs of the last hera_gpu_align_pairs_device call on
+ * ctx, in pair order, without the records leaving the device. */
+int hera_gpu_classes_add_last(hera_gpu_classes *c, hera_gpu_ctx *ctx);
+
+/* add_class for n records in device memory (layout of hera_gpu_result:
+ * paired = 1, n pairs, d_recs[2i] / [2i+1] = r[0] / r[1]; paired = 0, n
+ * single reads).  `stream` (a cudaStream_t, may be NULL) is the stream that
+ * wrote the records.  More classes or list entries than the table holds:
+ * HERA_GPU_ECAPACITY, and the table is unusable from then on. */
+int hera_gpu_classes_add_device(hera_gpu_classes *c, const hera_cand_rec *d_recs,
+				const uint32_t *d_pos_pool, const int32_t *d_p_pool, int32_t n,
+				int paired, void *stream);
+
+/* Copy the table out (see hera_gpu_class_table). */
+int hera_gpu_classes_fetch(hera_gpu_classes *c, hera_gpu_class_table *out);
+
+/* Device time (CUDA events) and kernel launches of the last add call. */
+int hera_gpu_classes_timing(const hera_gpu_classes *c, float *kernel_ms, uint32_t *launches);
+const char *hera_gpu_classes_last_error(const hera_gpu_classes *c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,144 @@
+"""Equivalence classes on the device (hera_gpu_classes_*): the add_class calls
+of hera's host tail (src/hash_align.c:1564-1602) over the records, checked
+against the reference's class goldens and against the oracle's restatement
+on the config-1/config-4 read models, in one batch and in several."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from hera_b200 import api, index, synth, workloads
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SETS = ["pairs100", "pairs150div", "pairs_mixed", "pairs_long", "pairs_n", "single"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _to_device(torch, recs, pos, p):
+    d_recs = torch.from_numpy(np.frombuffer(recs.tobytes(), np.uint8).copy()).cuda()
+    d_pos = torch.from_numpy(np.ascontiguousarray(pos).view(np.int32).copy()).cuda()
+    d_p = torch.from_numpy(np.ascontiguousarray(p, dtype=np.int32).copy()).cuda()
+    torch.cuda.synchronize()
+    return d_recs, d_pos, d_p
+
+
+def _add(cls, torch, recs, pos, p, paired):
+    n = recs.shape[0] // 2 if paired else recs.shape[0]
+    d = _to_device(torch, recs, np.append(pos, np.uint32(0)), np.append(p, np.int32(0)))
+    cls.add_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), n, paired)
+    return d
+
+
+@pytest.fixture(scope="module")
+def small_ctx():
+    torch = _torch()
+    meta = json.load(open(os.path.join(GOLD, "golden.json")))
+    prm = dict(meta["index"])
+    for k in ("exons", "intron"):
+        prm[k] = tuple(prm[k])
+    ix = index.build_index(synth.transcriptome(synth.make_annotation(**prm)))
+    ctx = api.Context(ix)
+    yield torch, ix, ctx
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_device_classes_golden(small_ctx, name):
+    """Device class table over the golden records == the table the
+    reference's own worker built from the same reads."""
+    torch, ix, ctx = small_ctx
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "classes.npz"))
+    key = f"{name}_wb1"
+    cls = api.Classes(ctx, max_classes=4096, max_list=1 << 16)
+    try:
+        _add(cls, torch, c[f"{key}_recs"], c[f"{key}_pos"], c[f"{key}_p"], name != "single")
+        got = cls.fetch()
+    finally:
+        cls.close()
+    want = oracle.ClassTable(d[f"{name}_ids"], d[f"{name}_counts"], d[f"{name}_ns"], d[f"{name}_ref_off"],
+                             d[f"{name}_ref"], d[f"{name}_tx"], int(d[f"{name}_paired"][0]),
+                             float(d[f"{name}_mean_frag"][0]))
+    assert got.key() == want.key()
+
+
+@pytest.fixture(scope="module")
+def cfg1_ctx(config1):
+    torch = _torch()
+    ann, tx, ix = config1
+    ctx = api.Context(ix)
+    yield torch, ann, tx, ix, ctx
+    ctx.close()
+
+
+@pytest.mark.parametrize("wl", ["config1", "config4"])
+@pytest.mark.parametrize("write_bam", [1, 0])
+def test_classes_after_device_align(cfg1_ctx, oracle1, wl, write_bam):
+    """Align on the device, classes from the device-resident results
+    (add_last), batch by batch; equal to the oracle's add_class over its own
+    records for the same reads, and to one table built in a single batch."""
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    r1, r2 = workloads.pairs(wl, ann, tx, 30000, seed=211)
+    want = oracle1.classes([oracle1.align_pairs(r1.copy(), r2.copy(), write_bam)])
+    assert want.n_classes > 0
+    cuts = (0, 5000, 17000, 30000)
+    cls = api.Classes(ctx, max_classes=1 << 16, max_list=1 << 20)
+    keep = []
+    try:
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            s1, s2 = r1.subset(np.arange(a, b)), r2.subset(np.arange(a, b))
+            seq, off, lens = workloads.interleave(s1, s2)
+            d = [torch.from_numpy(x).cuda() for x in (seq, off, lens)]
+            keep.append(d)
+            torch.cuda.synchronize()
+            ctx.align_pairs_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), b - a,
+                                   int(lens.max()), write_bam)
+            cls.add_last(ctx)
+        got = cls.fetch()
+        t = cls.timing()
+    finally:
+        cls.close()
+    assert got.key() == want.key()
+    assert t["launches"] >= 4
+
+
+def test_single_read_classes(cfg1_ctx, oracle1):
+    """Single reads (align_single_read's merges before add_class)."""
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    rs = synth.simulate_single(tx, 8000, seed=212)
+    res = ctx.align_single(rs, 1)
+    want = oracle1.classes([oracle1.align_single(rs.copy(), 1)], paired=False)
+    cls = api.Classes(ctx, max_classes=4096, max_list=1 << 16)
+    try:
+        keep = _add(cls, torch, res.recs, res.pos_pool, res.p_pool, False)
+        got = cls.fetch()
+    finally:
+        cls.close()
+    del keep
+    assert got.key() == want.key()
+
+
+def test_class_table_capacity(cfg1_ctx, oracle1):
+    """A table too small for the classes fails with ECAPACITY, not silently."""
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    r1, r2 = workloads.pairs("config1", ann, tx, 8000, seed=213)
+    res = ctx.align_pairs(r1, r2, 1)
+    assert oracle1.classes([res]).n_classes > 2
+    cls = api.Classes(ctx, max_classes=2, max_list=1 << 16)
+    try:
+        with pytest.raises(api.HeraGpuError) as e:
+            keep = _add(cls, torch, res.recs, res.pos_pool, res.p_pool, True)
+            del keep
+        assert e.value.code == api.HERA_GPU_ECAPACITY
+    finally:
+        cls.close()
