@@ -195,9 +195,9 @@ __global__ void k_cls_items(const hera_cand_rec *recs, const uint32_t *pos, cons
 	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
 		unsigned long long frag = 0;
 		uint32_t called = 0;
+		uint32_t at = NONE, k = 0, tx = NONE;   // id slot, its class + 1; one-entry transcript
 		if (i < n) {
 			const Call c = decide(recs, pos, pp, i, paired, lbase);
-			uint32_t s = NONE;
 			if (c.on) {
 				called = 1;
 				if (c.pair == 1) {
@@ -208,40 +208,54 @@ __global__ void k_cls_items(const hera_cand_rec *recs, const uint32_t *pos, cons
 				if (nw == 1) {
 					const uint32_t t = c.na ? c.a[0] : c.b[0];
 					if (t < T.n_trans)
-						atomicAdd(&T.tx_count[t], 1u);
+						tx = t;
 					else
 						atomicOr(&T.st->flags, F_TX);
 				} else if (c.err_sum < ERR_CAP) {
 					const uint32_t id = xxh32_list(c);
 					const unsigned long long key = (unsigned long long)id + 1;
-					uint32_t at = id & T.mask;
+					uint32_t a = id & T.mask;
 					bool got = false;
+					// a key already in place is read, not CASed: common
+					// classes are read by many threads at once
 					for (uint32_t probe = 0; probe <= T.mask; ++probe) {
-						const unsigned long long cur = atomicCAS(&T.keys[at], 0ull, key);
+						unsigned long long cur = *(volatile unsigned long long *)&T.keys[a];
+						if (cur == 0ull)
+							cur = atomicCAS(&T.keys[a], 0ull, key);
 						if (cur == 0ull || cur == key) {
 							got = true;
 							break;
 						}
-						at = (at + 1) & T.mask;
+						a = (a + 1) & T.mask;
 					}
 					if (!got) {
 						atomicOr(&T.st->flags, F_MAP);
 					} else {
-						const uint32_t k = T.cls_of[at];
-						if (k) {
-							atomicAdd(&T.count[k - 1], 1ull);
-						} else {
-							atomicMin(&T.first[at], base + (uint32_t)i);
-							atomicAdd(&T.pend[at], 1u);
-							s = at;
-						}
+						at = a;
+						k = T.cls_of[a];
 					}
 					ids[i] = id;
 					nl[i] = nw;
 				}
 			}
-			slot[i] = s;
+			slot[i] = (at != NONE && k == 0) ? at : NONE;
 		}
+		// one atomic per distinct slot (and transcript) in the warp: lanes
+		// holding the same one combine, the lowest lane -- the smallest
+		// item index of the group -- adds for all of them
+		const uint32_t lane = threadIdx.x & 31;
+		const unsigned g = __match_any_sync(0xffffffffu, at);
+		if (at != NONE && lane == (uint32_t)(__ffs(g) - 1)) {
+			if (k) {
+				atomicAdd(&T.count[k - 1], (unsigned long long)__popc(g));
+			} else {
+				atomicMin(&T.first[at], base + (uint32_t)i);
+				atomicAdd(&T.pend[at], (uint32_t)__popc(g));
+			}
+		}
+		const unsigned gt = __match_any_sync(0xffffffffu, tx);
+		if (tx != NONE && lane == (uint32_t)(__ffs(gt) - 1))
+			atomicAdd(&T.tx_count[tx], (uint32_t)__popc(gt));
 		// PAIRED and MEAN_FRAG's sum: one atomic a warp
 		for (int o = 16; o; o >>= 1)
 			frag += __shfl_down_sync(0xffffffffu, frag, o);
@@ -323,6 +337,7 @@ struct hera_gpu_classes {
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	float kernel_ms = 0;
 	uint32_t launches = 0;
+	bool timed = false;              // ev0 recorded for the current add call
 	std::string err = "no error";
 	std::vector<void *> owned;
 };
@@ -430,6 +445,10 @@ static int cls_add_part(hera_gpu_classes *c, const hera_cand_rec *recs, const ui
 	if ((e = c->cub_tmp.ensure(tmp + 16)) != cudaSuccess)
 		return cls_fail(c, HERA_GPU_ENOMEM, "class scan", e);
 	const cudaStream_t st = c->stream;
+	if (!c->timed) {   // the device time of an add call starts after its allocations
+		cudaEventRecord(c->ev0, st);
+		c->timed = true;
+	}
 	const uint32_t base = c->items_done;
 	const int sms = 148;
 	const unsigned g1 = (unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)sms * 8);
@@ -471,7 +490,8 @@ static int cls_begin(hera_gpu_classes *c)
 	if (cudaSetDevice(c->device) != cudaSuccess)
 		return cls_fail(c, HERA_GPU_ENODEV, "cudaSetDevice");
 	c->launches = 0;
-	cudaEventRecord(c->ev0, c->stream);
+	c->timed = false;
+	c->kernel_ms = 0;
 	return HERA_GPU_OK;
 }
 
@@ -481,7 +501,7 @@ static int cls_end(hera_gpu_classes *c, int rc)
 	if (rc != HERA_GPU_OK)
 		return rc;
 	rc = cls_check(c);
-	if (rc == HERA_GPU_OK)
+	if (rc == HERA_GPU_OK && c->timed)
 		cudaEventElapsedTime(&c->kernel_ms, c->ev0, c->ev1);
 	return rc;
 }
@@ -516,7 +536,6 @@ extern "C" int hera_gpu_classes_add_device(hera_gpu_classes *c, const hera_cand_
 	if (stream) {   // order after the caller's work that wrote the records
 		cudaEventRecord(c->ev1, (cudaStream_t)stream);
 		cudaStreamWaitEvent(c->stream, c->ev1, 0);
-		cudaEventRecord(c->ev0, c->stream);
 	}
 	rc = cls_add_part(c, d_recs, d_pos_pool, d_p_pool, n, paired, 0);
 	return cls_end(c, rc);

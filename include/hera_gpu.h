@@ -524,7 +524,9 @@ int hera_gpu_classes_add_device(hera_gpu_classes *c, const hera_cand_rec *d_recs
 /* Copy the table out (see hera_gpu_class_table). */
 int hera_gpu_classes_fetch(hera_gpu_classes *c, hera_gpu_class_table *out);
 
-/* Device time (CUDA events) and kernel launches of the last add call. */
+/* Device time (CUDA events, from the first kernel of the last add call to
+ * its end; the call's first-use allocations are not in it) and the
+ * kernels it launched. */
 int hera_gpu_classes_timing(const hera_gpu_classes *c, float *kernel_ms, uint32_t *launches);
 const char *hera_gpu_classes_last_error(const hera_gpu_classes *c);
 

@@ -142,3 +142,35 @@ def test_class_table_capacity(cfg1_ctx, oracle1):
         assert e.value.code == api.HERA_GPU_ECAPACITY
     finally:
         cls.close()
+
+
+def test_classes_after_page_locked_fetch(cfg1_ctx, oracle1):
+    """Fetching device-resident results into page-locked memory rebases the
+    records on the device; fetching twice gives the same records, and the
+    class table built afterwards from the same device records is unchanged."""
+    import ctypes as C
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    r1, r2 = workloads.pairs("config1", ann, tx, 20000, seed=214)
+    want = oracle1.align_pairs(r1.copy(), r2.copy(), 1)
+    seq, off, lens = workloads.interleave(r1, r2)
+    d = [torch.from_numpy(x).cuda() for x in (seq, off, lens)]
+    torch.cuda.synchronize()
+    ctx.align_pairs_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), r1.n, int(lens.max()), 1)
+    out = api.Result(2 * r1.n, 16 * r1.n + 1024, 16 * r1.n + 1024, 16 * r1.n + 1024)
+    arrs = out.arrays()
+    for a in arrs:
+        api.host_register(a)
+    try:
+        for _ in range(2):
+            ctx._check(ctx.lib.hera_gpu_fetch_result(ctx.h, C.byref(out.c)))
+            assert out.canonical() == want.canonical()
+    finally:
+        for a in arrs:
+            api.host_unregister(a)
+    cls = api.Classes(ctx, max_classes=1 << 16, max_list=1 << 20)
+    try:
+        cls.add_last(ctx)
+        got = cls.fetch()
+    finally:
+        cls.close()
+    assert got.key() == oracle1.classes([want]).key()
