@@ -216,6 +216,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_classes_add_last.argtypes = [C.c_void_p, C.c_void_p]
     lib.hera_gpu_classes_add_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                 C.c_int, C.c_void_p]
+    lib.hera_gpu_classes_add_host.argtypes = [C.c_void_p, C.POINTER(_Result), C.c_int32, C.c_int]
     lib.hera_gpu_classes_fetch.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
     lib.hera_gpu_classes_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]
     lib.hera_gpu_classes_last_error.restype = C.c_char_p
@@ -660,6 +661,12 @@ class Classes:
                    stream: Optional[int] = None) -> None:
         self._check(self.lib.hera_gpu_classes_add_device(self.h, d_recs, d_pos_pool, d_p_pool, n,
                                                          1 if paired else 0, stream))
+
+    def add_result(self, res: "Result", paired: bool = True) -> None:
+        """Records in host memory (a Result from an align call or a server
+        wait), copied to the device and added."""
+        n = res.recs.shape[0] // 2 if paired else res.recs.shape[0]
+        self._check(self.lib.hera_gpu_classes_add_host(self.h, C.byref(res.c), n, 1 if paired else 0))
 
     def timing(self) -> dict:
         ms, n = C.c_float(), C.c_uint32()

@@ -334,6 +334,9 @@ struct hera_gpu_classes {
 	DBuf<uint32_t> slot, ids, nl;
 	DBuf<unsigned long long> mark, xs;
 	DBuf<uint8_t> cub_tmp;
+	DBuf<hera_cand_rec> in_recs;     // hera_gpu_classes_add_host's copies
+	DBuf<uint32_t> in_pos;
+	DBuf<int32_t> in_p;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	float kernel_ms = 0;
 	uint32_t launches = 0;
@@ -358,6 +361,7 @@ extern "C" void hera_gpu_classes_destroy(hera_gpu_classes *c)
 		cudaFree(p);
 	c->slot.release(); c->ids.release(); c->nl.release(); c->mark.release(); c->xs.release();
 	c->cub_tmp.release();
+	c->in_recs.release(); c->in_pos.release(); c->in_p.release();
 	if (c->ev0)
 		cudaEventDestroy(c->ev0);
 	if (c->ev1)
@@ -538,6 +542,34 @@ extern "C" int hera_gpu_classes_add_device(hera_gpu_classes *c, const hera_cand_
 		cudaStreamWaitEvent(c->stream, c->ev1, 0);
 	}
 	rc = cls_add_part(c, d_recs, d_pos_pool, d_p_pool, n, paired, 0);
+	return cls_end(c, rc);
+}
+
+extern "C" int hera_gpu_classes_add_host(hera_gpu_classes *c, const hera_gpu_result *res, int32_t n,
+					 int paired)
+{
+	if (!c)
+		return HERA_GPU_EINVAL;
+	if (!res || n < 0 || (paired != 0 && paired != 1) || (n > 0 && !res->recs) ||
+	    (res->list_used > 0 && (!res->pos_pool || !res->p_pool)))
+		return cls_fail(c, HERA_GPU_EINVAL, "bad argument");
+	int rc = cls_begin(c);
+	if (rc)
+		return rc;
+	const size_t nr = (size_t)n * (paired ? 2 : 1);
+	const size_t nl = (size_t)res->list_used;
+	cudaError_t e;
+	if ((e = c->in_recs.ensure(nr + 1)) != cudaSuccess || (e = c->in_pos.ensure(nl + 1)) != cudaSuccess ||
+	    (e = c->in_p.ensure(nl + 1)) != cudaSuccess)
+		return cls_fail(c, HERA_GPU_ENOMEM, "class input copies", e);
+	if ((nr && (e = cudaMemcpyAsync(c->in_recs.p, res->recs, nr * sizeof(hera_cand_rec), cudaMemcpyHostToDevice,
+					c->stream)) != cudaSuccess) ||
+	    (nl && (e = cudaMemcpyAsync(c->in_pos.p, res->pos_pool, nl * 4, cudaMemcpyHostToDevice, c->stream)) !=
+			   cudaSuccess) ||
+	    (nl && (e = cudaMemcpyAsync(c->in_p.p, res->p_pool, nl * 4, cudaMemcpyHostToDevice, c->stream)) !=
+			   cudaSuccess))
+		return cls_fail(c, HERA_GPU_ECUDA, "class input copies", e);
+	rc = cls_add_part(c, c->in_recs.p, c->in_pos.p, c->in_p.p, n, paired, 0);
 	return cls_end(c, rc);
 }
 

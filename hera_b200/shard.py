@@ -3,9 +3,10 @@ the index, read chunks dealt round robin, no collective on the data path.
 
 hera's per-chunk results are consumed in input order by its host tail
 (add_class order fixes the EM's class order), so the only exchange is an
-ordered merge of per-chunk results on one rank, plus the max-over-ranks of
-the device timing.  Both are small host-side steps over torch.distributed
-(gloo on CPU, nccl on GPUs).
+ordered merge of per-chunk results on one rank -- the records, or only the
+per-chunk class tables when the ranks build those on their devices -- plus
+the max-over-ranks of the device timing.  Both are small host-side steps
+over torch.distributed (gloo on CPU, nccl on GPUs).
 """
 from __future__ import annotations
 
@@ -56,3 +57,44 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def merge_class_tables(tables: List[Any]):
+    """Per-chunk class tables (each built from one chunk's records alone,
+    given in chunk order) -> the table hera's add_class builds over all
+    chunks in order (src/hash_align.c:1564-1602).  A class first seen in
+    chunk c is numbered after every class of earlier chunks and, among
+    chunk c's new classes, in chunk c's own first-insertion order, keeping
+    chunk c's transcript list; counts, REF_INF->count, PAIRED and the
+    fragment sum add up.  Tables need ids, counts, ns, ref_off, ref,
+    tx_count, paired and mean_frag (hera_b200.api.ClassTable has them)."""
+    import numpy as np
+    from .api import ClassTable
+    if not tables:
+        raise ValueError("no class tables")
+    index = {}
+    ids, counts, ns, lists = [], [], [], []
+    tx = np.zeros_like(np.asarray(tables[0].tx_count, dtype=np.uint64))
+    paired, frag = 0, 0.0
+    for t in tables:
+        ref = np.asarray(t.ref)
+        for k, cid in enumerate(np.asarray(t.ids).tolist()):
+            j = index.get(cid)
+            if j is None:
+                index[cid] = len(ids)
+                ids.append(cid)
+                counts.append(float(t.counts[k]))
+                ns.append(int(t.ns[k]))
+                o = int(t.ref_off[k])
+                lists.append(ref[o:o + int(t.ns[k])])
+            else:
+                counts[j] += float(t.counts[k])
+        tx += np.asarray(t.tx_count, dtype=np.uint64)
+        paired = (paired + int(t.paired)) & 0xFFFFFFFF   # PAIRED is an unsigned int
+        frag += float(t.mean_frag)
+    off = np.zeros(len(ns), np.uint64)
+    if ns:
+        off[1:] = np.cumsum(np.asarray(ns[:-1], np.uint64))
+    ref = np.concatenate(lists).astype(np.uint32) if lists else np.zeros(0, np.uint32)
+    return ClassTable(np.asarray(ids, np.uint32), np.asarray(counts, np.float64), np.asarray(ns, np.uint32),
+                      off, ref, (tx & 0xFFFFFFFF).astype(np.uint32), paired, frag)

@@ -521,6 +521,13 @@ int hera_gpu_classes_add_device(hera_gpu_classes *c, const hera_cand_rec *d_recs
 				const uint32_t *d_pos_pool, const int32_t *d_p_pool, int32_t n,
 				int paired, void *stream);
 
+/* add_class for n pairs (paired = 1) or single reads (paired = 0) whose flat
+ * records are in host memory, as an align call left them in `res` (records,
+ * and the pos/p pools up to res->list_used).  The records are copied to the
+ * device first; for results already there use the two calls above. */
+int hera_gpu_classes_add_host(hera_gpu_classes *c, const hera_gpu_result *res, int32_t n,
+			      int paired);
+
 /* Copy the table out (see hera_gpu_class_table). */
 int hera_gpu_classes_fetch(hera_gpu_classes *c, hera_gpu_class_table *out);
 

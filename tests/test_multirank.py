@@ -59,3 +59,77 @@ def test_gloo_two_ranks():
         assert p.exitcode == 0
     assert merged == [f"chunk{i}:rank{i % 2}" for i in range(7)]
     assert t == 2.0
+
+
+def _small_index():
+    from hera_b200 import index, synth
+    ann = synth.make_annotation(seed=11, genome_len=300_000, n_genes=30, n_transcripts=75)
+    tx = synth.transcriptome(ann)
+    return ann, tx, index.build_index(tx)
+
+
+def _chunk_classes(orc, ann, tx, cid):
+    """The class table of chunk `cid` aligned alone (the oracle's records)."""
+    from hera_b200 import workloads
+    r1, r2 = workloads.pairs("config1" if cid % 2 else "config4", ann, tx, 1500 + 300 * cid, seed=400 + cid)
+    return orc.classes([orc.align_pairs(r1, r2, 1)]), (r1, r2)
+
+
+def test_class_tables_merge_equals_one_pass():
+    """Per-chunk tables merged in chunk order == add_class over all chunks."""
+    import oracle
+    if not os.path.exists(oracle.ORACLE_SO):
+        pytest.skip("oracle not built")
+    ann, tx, ix = _small_index()
+    orc = oracle.Oracle(ix)
+    per, results = [], []
+    for cid in range(5):
+        t, (r1, r2) = _chunk_classes(orc, ann, tx, cid)
+        per.append(t)
+        results.append(orc.align_pairs(r1, r2, 1))
+    whole = orc.classes(results)
+    assert whole.n_classes > max(t.n_classes for t in per)
+    assert shard.merge_class_tables(per).key() == whole.key()
+
+
+def _class_worker(rank, world, port, q):
+    import torch.distributed as dist
+    import oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ann, tx, ix = _small_index()
+        orc = oracle.Oracle(ix)
+        n = 5
+        local = {cid: _chunk_classes(orc, ann, tx, cid)[0] for cid in shard.chunk_ids(n, rank, world)}
+        merged = shard.gather_in_order(local, n)
+        if rank == 0:
+            q.put(shard.merge_class_tables(merged).key())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_class_tables():
+    """Two ranks build the class tables of their own chunks; rank 0 merges
+    them in chunk order into the one-pass table."""
+    import oracle
+    if not os.path.exists(oracle.ORACLE_SO):
+        pytest.skip("oracle not built")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_class_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ann, tx, ix = _small_index()
+    orc = oracle.Oracle(ix)
+    results = []
+    for cid in range(5):
+        _, (r1, r2) = _chunk_classes(orc, ann, tx, cid)
+        results.append(orc.align_pairs(r1, r2, 1))
+    assert got == orc.classes(results).key()

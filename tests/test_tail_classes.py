@@ -174,3 +174,37 @@ def test_classes_after_page_locked_fetch(cfg1_ctx, oracle1):
     finally:
         cls.close()
     assert got.key() == oracle1.classes([want]).key()
+
+
+def test_per_sample_classes_served_equal_alone(cfg1_ctx, oracle1):
+    """Serving: one class table per sample, fed with the sample's served
+    chunks in its own order (add_host), equals the table of the sample's
+    chunks aligned alone, and the oracle's -- the EM input of every sample
+    is the same in the mix as alone."""
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    sizes = [3000, 11000, 700, 5000, 16000, 2500, 9000]
+    models = ["config1", "config3", "config4"]
+    chunks = []
+    for k, n in enumerate(sizes):
+        r1, r2 = workloads.pairs(models[k % 3], ann, tx, n, seed=300 + k)
+        chunks.append((k % 3, r1, r2))
+    alone = [ctx.align_pairs(r1, r2, 1) for _, r1, r2 in chunks]
+    srv = api.Server(ctx, batch_pairs=4096, max_slots=3, write_bam=1, max_samples=4)
+    try:
+        tickets = [srv.submit(s, r1, r2) for s, r1, r2 in chunks]
+        served = [srv.wait(t)[0] for t in tickets]
+    finally:
+        srv.close()
+    for s in range(3):
+        ks = [k for k, (si, _, _) in enumerate(chunks) if si == s]
+        tabs = []
+        for src in (served, alone):
+            cls = api.Classes(ctx, max_classes=1 << 14, max_list=1 << 18)
+            try:
+                for k in ks:
+                    cls.add_result(src[k], paired=True)
+                tabs.append(cls.fetch())
+            finally:
+                cls.close()
+        want = oracle1.classes([oracle1.align_pairs(chunks[k][1].copy(), chunks[k][2].copy(), 1) for k in ks])
+        assert tabs[0].key() == tabs[1].key() == want.key(), f"sample {s}"
