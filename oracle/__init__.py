@@ -123,6 +123,18 @@ class ClassTable:
                 tuple(self.tx_count.tolist()), self.paired, self.mean_frag)
 
 
+def _em_args(table: ClassTable, ix):
+    """ctypes arguments of ho_em after n_trans: len, tx_count, n_classes,
+    count, n, ref_off, ref (arrays kept alive on the table)."""
+    table._em_keep = [np.ascontiguousarray(ix.length, np.uint32), np.ascontiguousarray(table.tx_count, np.uint32),
+                      np.ascontiguousarray(table.counts, np.float64), np.ascontiguousarray(table.ns, np.uint32),
+                      np.ascontiguousarray(table.ref_off, np.uint64),
+                      np.ascontiguousarray(np.append(table.ref, np.uint32(0)), np.uint32)]
+    ln, tx, cnt, ns, offs, ref = table._em_keep
+    return [C.c_void_p(_ptr(ln)), C.c_void_p(_ptr(tx)), C.c_uint32(table.n_classes), C.c_void_p(_ptr(cnt)),
+            C.c_void_p(_ptr(ns)), C.c_void_p(_ptr(offs)), C.c_void_p(_ptr(ref))]
+
+
 def _export_classes(sizes, export, n_trans: int) -> ClassTable:
     nc, rn = C.c_uint32(), C.c_uint64()
     sizes(C.byref(nc), C.byref(rn))
@@ -204,6 +216,15 @@ class Oracle:
                                    lambda *a: L.ho_classes_export(C.c_void_p(h), *a), self.ix.n_trans)
         finally:
             L.ho_classes_free(C.c_void_p(h))
+
+    def em(self, table: "ClassTable"):
+        """estimate_count over a class table: (grama, overlap, rounds)."""
+        n = self.ix.n_trans
+        g, o = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        rounds = C.c_uint32()
+        a = _em_args(table, self.ix)
+        self.lib.ho_em(C.c_uint32(n), *a[:1], *a[1:], C.c_void_p(_ptr(g)), C.c_void_p(_ptr(o)), C.byref(rounds))
+        return g[:n], o[:n], rounds.value
 
     def xxh32(self, data: bytes, seed: int = 0) -> int:
         self.lib.ho_xxh32.restype = C.c_uint32
@@ -332,6 +353,19 @@ class Reference:
                            C.c_void_p(_ptr(s1)), C.c_void_p(_ptr(o1)), C.c_void_p(_ptr(l1)),
                            C.c_void_p(_ptr(s2)), C.c_void_p(_ptr(o2)), C.c_void_p(_ptr(l2)))
         return _export_classes(L.refh_classes_sizes, L.refh_classes_export, n_trans)
+
+    def em(self, table: "ClassTable", n_trans: int):
+        """The reference's estimate_count over a class table: (grama, overlap)."""
+        g, o = np.zeros(max(n_trans, 1)), np.zeros(max(n_trans, 1))
+        cnt = np.ascontiguousarray(table.counts, np.float64)
+        ns = np.ascontiguousarray(table.ns, np.uint32)
+        offs = np.ascontiguousarray(table.ref_off, np.uint64)
+        ref = np.ascontiguousarray(np.append(table.ref, np.uint32(0)), np.uint32)
+        tx = np.ascontiguousarray(table.tx_count, np.uint32)
+        self.lib.refh_em(C.c_uint32(table.n_classes), C.c_void_p(_ptr(cnt)), C.c_void_p(_ptr(ns)),
+                         C.c_void_p(_ptr(offs)), C.c_void_p(_ptr(ref)), C.c_void_p(_ptr(tx)),
+                         C.c_void_p(_ptr(g)), C.c_void_p(_ptr(o)))
+        return g[:n_trans], o[:n_trans]
 
     def xxh32(self, data: bytes, seed: int = 0) -> int:
         self.lib.refh_xxh32.restype = C.c_uint32

@@ -24,6 +24,7 @@
 
 #include <stdlib.h>
 #include <string.h>
+#include <math.h>
 #include <pthread.h>
 
 enum { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4, OP_X = 8 };
@@ -1609,4 +1610,107 @@ void ho_classes_export(const ho_classes *c, uint32_t *id, double *count, uint32_
 	memcpy(tx_count, c->tx_count, c->n_trans * sizeof(uint32_t));
 	*paired = c->paired;
 	*mean_frag = c->mean_frag;
+}
+
+/* ===========================================================================
+ * The EM over the class table: estimate_count (src/EM.c:315-387)
+ * ======================================================================== */
+
+/* Norm (src/hash_align.c:150-164): the sample standard deviation, two
+ * passes in index order. */
+static double em_norm(const double *a, uint32_t n)
+{
+	double sum = 0, total = 0;
+	for (uint32_t i = 0; i < n; ++i)
+		sum += a[i];
+	sum /= n;
+	for (uint32_t i = 0; i < n; ++i)
+		total += (a[i] - sum) * (a[i] - sum);
+	total /= n - 1;
+	return sqrt(total);
+}
+
+/* M_step (src/EM.c:271-302): per class, its share of the class count
+ * goes to each listed transcript in proportion to grama; overlap
+ * accumulates in class order and is cleared again. */
+static double *em_m_step(uint32_t n_trans, const uint32_t *len, const uint32_t *tx_count,
+			 uint32_t n_classes, const double *count, const uint32_t *n,
+			 const uint64_t *ref_off, const uint32_t *ref, double *grama, double *overlap,
+			 uint32_t *stop)
+{
+	double *next = calloc(n_trans ? n_trans : 1, sizeof(double));
+	for (uint32_t i = 0; i < n_classes; ++i) {
+		const uint32_t *l = ref + ref_off[i];
+		double total = 0.0;
+		for (uint32_t k = 0; k < n[i]; ++k)
+			total += grama[l[k]];
+		if (total == 0)
+			continue;
+		for (uint32_t k = 0; k < n[i]; ++k)
+			overlap[l[k]] += grama[l[k]] * count[i] / total;
+	}
+	double max_err = 0.0;
+	*stop = 1;
+	for (uint32_t i = 0; i < n_trans; ++i) {
+		next[i] = (double)(tx_count[i] + overlap[i]) / len[i];
+		overlap[i] = 0.0;
+		if (next[i] > 1e-3) {
+			double d = next[i] - grama[i];
+			double err = (d < 0 ? -d : d) / next[i];
+			max_err = err > max_err ? err : max_err;
+			if (max_err > 0.01)
+				*stop = 0;
+		}
+	}
+	return next;
+}
+
+void ho_em(uint32_t n_trans, const uint32_t *len, const uint32_t *tx_count, uint32_t n_classes,
+	   const double *count, const uint32_t *n, const uint64_t *ref_off, const uint32_t *ref,
+	   double *grama_out, double *overlap_out, uint32_t *rounds)
+{
+	const uint32_t N = n_trans ? n_trans : 1;
+	double *grama = calloc(N, sizeof(double));
+	double *overlap = calloc(N, sizeof(double));
+	double *r = malloc(N * sizeof(double)), *v = malloc(N * sizeof(double));
+	for (uint32_t i = 0; i < n_trans; ++i)          /* E_step */
+		grama[i] = (double)1 / n_trans;
+	uint32_t k = 0, stop = 0;
+	while (k < 50 || (k < 1000 && stop == 0)) {
+		double *u = grama;
+		double *u1 = em_m_step(n_trans, len, tx_count, n_classes, count, n, ref_off, ref, u, overlap, &stop);
+		double *u2 = em_m_step(n_trans, len, tx_count, n_classes, count, n, ref_off, ref, u1, overlap, &stop);
+		for (uint32_t i = 0; i < n_trans; ++i) {
+			r[i] = u1[i] - u[i];
+			v[i] = (u2[i] - u1[i]) - r[i];
+		}
+		double n_r = em_norm(r, n_trans), n_v = em_norm(v, n_trans);
+		double alpha = n_v != 0 ? -n_r / n_v : -1;
+		if (alpha > -1)
+			alpha = -1;
+		free(u2);
+		for (uint32_t i = 0; i < n_trans; ++i) {
+			u1[i] = u[i] - 2 * alpha * r[i] + alpha * alpha * v[i];
+			if (u1[i] < 0)
+				u1[i] = 0;
+		}
+		grama = em_m_step(n_trans, len, tx_count, n_classes, count, n, ref_off, ref, u1, overlap, &stop);
+		free(u);
+		free(u1);
+		++k;
+	}
+	double sum = 0.0;
+	for (uint32_t i = 0; i < n_trans; ++i)
+		sum += grama[i];
+	for (uint32_t i = 0; i < n_trans; ++i) {
+		if (sum == 0) {
+			overlap_out[i] = 0;
+			grama_out[i] = 0;
+		} else {
+			overlap_out[i] = grama[i] * len[i];
+			grama_out[i] = grama[i] * 1000000 / sum;
+		}
+	}
+	*rounds = k;
+	free(grama); free(overlap); free(r); free(v);
 }

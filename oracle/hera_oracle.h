@@ -157,6 +157,15 @@ void ho_classes_sizes(const ho_classes *c, uint32_t *n_classes, uint64_t *ref_n)
 void ho_classes_export(const ho_classes *c, uint32_t *id, double *count, uint32_t *n,
 		       uint64_t *ref_off, uint32_t *ref, uint32_t *tx_count,
 		       uint32_t *paired, double *mean_frag);
+/* estimate_count (src/EM.c:315-387): SQUAREM over M_step (:271-302) with
+ * E_step's uniform start (:304-313), on a class table given as arrays
+ * (class i: count[i], list ref[ref_off[i] .. + n[i])), REF_INF->count
+ * (tx_count) and REF_INF->len.  Writes em_val->grama and ->overlap as the
+ * reference leaves them; *rounds = the SQUAREM iterations run. */
+void ho_em(uint32_t n_trans, const uint32_t *len, const uint32_t *tx_count, uint32_t n_classes,
+	   const double *count, const uint32_t *n, const uint64_t *ref_off, const uint32_t *ref,
+	   double *grama, double *overlap, uint32_t *rounds);
+
 /* XXH32 (the published xxHash 32-bit algorithm) as add_class uses it. */
 uint32_t ho_xxh32(const void *buf, size_t len, uint32_t seed);
 

@@ -13,6 +13,7 @@
  */
 #include "hash_align.h"
 #include "ssw.h"
+#include "EM.h"
 
 #include <stdint.h>
 #include <pthread.h>
@@ -472,4 +473,40 @@ void refh_classes_export(uint32_t *id, double *count, uint32_t *n, uint64_t *ref
 unsigned int refh_xxh32(const void *buf, size_t len, unsigned int seed)
 {
 	return XXH32(buf, len, seed);
+}
+
+/* ---- the EM: the reference's estimate_count (src/EM.c:315-387) ----------
+ * run on a class table given as arrays (installed as CLASS, with the
+ * per-transcript counts as REF_INF->count), on the installed index's
+ * REF_INF->len; em_val->grama and ->overlap are copied out. */
+EM_val *estimate_count(unsigned int *count, unsigned int order);
+
+int refh_em(uint32_t n_classes, const double *count, const uint32_t *n, const uint64_t *ref_off,
+	    const uint32_t *ref, const uint32_t *tx_count, double *grama, double *overlap)
+{
+	uint32_t i;
+	Gclass *saved = CLASS;
+	Gclass g;
+	EM_val *em;
+
+	g.n = n_classes;
+	g.map = NULL;
+	g.cls = calloc(n_classes ? n_classes : 1, sizeof(Class));
+	for (i = 0; i < n_classes; ++i) {
+		g.cls[i].n = n[i];
+		g.cls[i].ref = (unsigned int *)(ref + ref_off[i]);
+		g.cls[i].count = count[i];
+		g.cls[i].id = 0;
+	}
+	CLASS = &g;
+	memcpy(REF_INF->count, tx_count, REF_INF->n * sizeof(uint32_t));
+	em = estimate_count(REF_INF->count, 0);
+	memcpy(grama, em->grama, REF_INF->n * sizeof(double));
+	memcpy(overlap, em->overlap, REF_INF->n * sizeof(double));
+	free(em->grama);
+	free(em->overlap);
+	free(em);
+	free(g.cls);
+	CLASS = saved;
+	return 0;
 }

@@ -8,8 +8,10 @@ Expected values come from the reference's own code
 align_single_read (src/hash_align.c:1717-1853), run without `-w` over the
 read sets stored in candidates.npz, after which the add_class state is read
 back -- the class table in first-insertion order (XXH32 id, count,
-transcript list), REF_INF->count, PAIRED and MEAN_FRAG's sum.  Also XXH32
-(src/xxhash.c) of seeded random buffers of every length 0..96.
+transcript list), REF_INF->count, PAIRED and MEAN_FRAG's sum -- and the
+reference's estimate_count (src/EM.c:315-387) over each of those tables
+(em_val->grama and ->overlap, bit for bit).  Also XXH32 (src/xxhash.c) of
+seeded random buffers of every length 0..96.
 """
 import os
 import sys
@@ -49,7 +51,23 @@ def main():
         out[f"{name}_ref_off"], out[f"{name}_ref"], out[f"{name}_tx"] = t.ref_off, t.ref, t.tx_count
         out[f"{name}_paired"] = np.array([t.paired], np.uint32)
         out[f"{name}_mean_frag"] = np.array([t.mean_frag], np.float64)
+        g, o = ref.em(t, ix.n_trans)
+        out[f"{name}_em_grama"], out[f"{name}_em_overlap"] = g, o
         print(name, "classes", t.n_classes, "paired", t.paired, "one-transcript reads", int(t.tx_count.sum()))
+    # a constructed table: triples of transcripts with one heavy shared
+    # class and a light class on two of them, no single-transcript reads
+    lists, counts = [], []
+    for i in range(0, ix.n_trans - 2, 3):
+        lists += [[i, i + 1, i + 2], [i, i + 1]]
+        counts += [1e5, 1.0]
+    ns = np.array([len(x) for x in lists], np.uint32)
+    off = np.zeros(len(ns), np.uint64)
+    off[1:] = np.cumsum(ns[:-1])
+    slow = oracle.ClassTable(np.arange(len(ns), dtype=np.uint32), np.array(counts), ns, off,
+                             np.concatenate([np.array(x, np.uint32) for x in lists]),
+                             np.zeros(ix.n_trans, np.uint32), 0, 0.0)
+    out["slow_counts"], out["slow_ns"], out["slow_ref_off"], out["slow_ref"] = slow.counts, ns, off, slow.ref
+    out["slow_em_grama"], out["slow_em_overlap"] = ref.em(slow, ix.n_trans)
     np.savez_compressed(os.path.join(HERE, "classes.npz"), **out)
 
 

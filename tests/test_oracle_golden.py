@@ -153,3 +153,19 @@ def test_classes_golden(orc, name):
     got = orc.classes([_golden_records(c, f"{name}_wb1")], paired=name != "single")
     want = _golden_classes(d, name)
     assert got.key() == want.key()
+
+
+def _slow_table(d, n_trans):
+    return oracle.ClassTable(np.arange(len(d["slow_ns"]), dtype=np.uint32), d["slow_counts"], d["slow_ns"],
+                             d["slow_ref_off"], d["slow_ref"], np.zeros(n_trans, np.uint32), 0, 0.0)
+
+
+@pytest.mark.parametrize("name", SETS + ["single", "slow"])
+def test_em_golden(orc, small, name):
+    """estimate_count restated, over the golden class tables, against the
+    reference's own EM on the same tables: bit for bit."""
+    d = np.load(os.path.join(GOLD, "classes.npz"))
+    t = _slow_table(d, small[1].n_trans) if name == "slow" else _golden_classes(d, name)
+    g, o, rounds = orc.em(t)
+    assert np.array_equal(g.view(np.uint64), d[f"{name}_em_grama"].view(np.uint64))
+    assert np.array_equal(o.view(np.uint64), d[f"{name}_em_overlap"].view(np.uint64))
