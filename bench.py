@@ -320,7 +320,7 @@ def main():
         cls = None
         if rank == 0 and world == 1:
             try:
-                cls = classes_leg(kctx, args.chunk)
+                cls = classes_leg(kctx, args.chunk, ix.length)
             except Exception as e:
                 log(f"classes leg failed: {e}")
                 cls = {"error": str(e)}
@@ -429,12 +429,14 @@ def main():
         dist.destroy_process_group()
 
 
-def classes_leg(kctx, pairs: int) -> dict:
+def classes_leg(kctx, pairs: int, length) -> dict:
     """hera's add_class on the device (hera_gpu_classes_add_last) over the
     device-resident records of the step kctx just ran: kernel time with a
     fresh table (every class inserted) and with the same records again
     (every class found).  Bytes counted: each pair's two 52-byte records
-    plus 4 B per list entry the tail hashes."""
+    plus 4 B per list entry the tail hashes.  Then hera's EM on the device
+    over the first table, against the EM restated in C (one host thread)
+    on the same table: time and bit-for-bit equality."""
     from hera_b200 import api
     out = {}
     cls = api.Classes(kctx, max_classes=1 << 22, max_list=1 << 26)
@@ -442,10 +444,23 @@ def classes_leg(kctx, pairs: int) -> dict:
         cls.add_last(kctx)
         first = cls.timing()
         t = cls.fetch()
+        g, o, rounds, em_ms = cls.em(kctx)
         cls.add_last(kctx)
         again = cls.timing()
     finally:
         cls.close()
+    em = {"device_ms": round(em_ms, 3), "rounds": rounds, "transcripts": len(length)}
+    try:
+        import oracle   # the CPU baseline of this leg: the EM restated in C
+        t0 = time.perf_counter()
+        g0, o0, k0 = oracle.em_port(t, length)
+        cpu_s = time.perf_counter() - t0
+        em.update({"cpu_port_ms": round(cpu_s * 1e3, 3), "cpu_cores": 1,
+                   "bit_exact": bool(k0 == rounds and np.array_equal(g.view(np.uint64), g0.view(np.uint64))
+                                     and np.array_equal(o.view(np.uint64), o0.view(np.uint64)))})
+    except Exception as e:
+        em["cpu_error"] = str(e)
+    out["em"] = em
     hashed = int(t.ns.sum()) + int(t.tx_count.sum())
     algo = 104 * pairs + 4 * hashed
     peak = _hbm_peak()

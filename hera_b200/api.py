@@ -216,6 +216,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_classes_add_last.argtypes = [C.c_void_p, C.c_void_p]
     lib.hera_gpu_classes_add_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                 C.c_int, C.c_void_p]
+    lib.hera_gpu_classes_em.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_float)]
+    lib.hera_gpu_classes_load.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
     lib.hera_gpu_classes_add_host.argtypes = [C.c_void_p, C.POINTER(_Result), C.c_int32, C.c_int]
     lib.hera_gpu_classes_fetch.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
     lib.hera_gpu_classes_timing.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]
@@ -667,6 +670,33 @@ class Classes:
         wait), copied to the device and added."""
         n = res.recs.shape[0] // 2 if paired else res.recs.shape[0]
         self._check(self.lib.hera_gpu_classes_add_host(self.h, C.byref(res.c), n, 1 if paired else 0))
+
+    def load(self, table) -> None:
+        """Replace the contents with a class table held on the host (any
+        object with ids, counts, ns, ref_off, ref, tx_count, paired and
+        mean_frag, e.g. a ClassTable)."""
+        keep = [np.ascontiguousarray(table.ids, np.uint32), np.ascontiguousarray(table.counts, np.float64),
+                np.ascontiguousarray(table.ns, np.uint32), np.ascontiguousarray(table.ref_off, np.uint64),
+                np.ascontiguousarray(np.append(np.asarray(table.ref, np.uint32), np.uint32(0))),
+                np.ascontiguousarray(table.tx_count, np.uint32)]
+        ids, cnt, ns, offs, ref, tx = keep
+        t = _ClassTable()
+        t.class_cap = t.n_classes = len(ids)
+        t.id, t.count, t.n, t.list_off = _ptr(ids), _ptr(cnt), _ptr(ns), _ptr(offs)
+        t.list_cap = t.list_used = len(ref) - 1
+        t.list, t.tx_count = _ptr(ref), _ptr(tx)
+        t.paired, t.mean_frag_sum = int(table.paired), float(table.mean_frag)
+        self._check(self.lib.hera_gpu_classes_load(self.h, C.byref(t)))
+
+    def em(self, ctx: "Context"):
+        """hera's estimate_count on the device over this table:
+        (grama, overlap, rounds, device ms), the arrays bit for bit as hera's
+        em_val leaves them."""
+        n = self.n_trans
+        g, o = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        rounds, ms = C.c_uint32(), C.c_float()
+        self._check(self.lib.hera_gpu_classes_em(self.h, ctx.h, _ptr(g), _ptr(o), C.byref(rounds), C.byref(ms)))
+        return g[:n], o[:n], rounds.value, ms.value
 
     def timing(self) -> dict:
         ms, n = C.c_float(), C.c_uint32()

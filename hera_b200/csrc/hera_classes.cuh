@@ -573,6 +573,113 @@ extern "C" int hera_gpu_classes_add_host(hera_gpu_classes *c, const hera_gpu_res
 	return cls_end(c, rc);
 }
 
+namespace cls {
+// hera_gpu_classes_load: class i's id into the table (ids are distinct in
+// a table add_class built; a repeated id keeps its first class)
+__global__ void k_cls_load_keys(Table T, uint32_t nc)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nc)
+		return;
+	const uint32_t id = T.id[i];
+	const unsigned long long key = (unsigned long long)id + 1;
+	uint32_t a = id & T.mask;
+	for (uint32_t probe = 0; probe <= T.mask; ++probe) {
+		const unsigned long long cur = atomicCAS(&T.keys[a], 0ull, key);
+		if (cur == 0ull || cur == key) {
+			atomicMin(&T.first[a], i);
+			return;
+		}
+		a = (a + 1) & T.mask;
+	}
+	atomicOr(&T.st->flags, F_MAP);
+}
+
+__global__ void k_cls_load_number(Table T, uint32_t nc)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nc)
+		return;
+	const uint32_t id = T.id[i];
+	const unsigned long long key = (unsigned long long)id + 1;
+	uint32_t a = id & T.mask;
+	for (uint32_t probe = 0; probe <= T.mask; ++probe) {
+		if (T.keys[a] == key) {
+			if (T.first[a] == i)
+				T.cls_of[a] = i + 1;
+			return;
+		}
+		a = (a + 1) & T.mask;
+	}
+}
+
+__global__ void k_cls_load_reset(Table T)
+{
+	const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+	if (a > T.mask)
+		return;
+	T.first[a] = NONE;   // the load used first[] for its own numbering
+}
+}   // namespace cls
+
+extern "C" int hera_gpu_classes_load(hera_gpu_classes *c, const hera_gpu_class_table *in)
+{
+	if (!c)
+		return HERA_GPU_EINVAL;
+	if (!in || (in->n_classes && (!in->id || !in->count || !in->n || !in->list_off)) ||
+	    (in->list_used && !in->list))
+		return cls_fail(c, HERA_GPU_EINVAL, "bad argument");
+	if (in->n_classes > c->T.max_classes || in->list_used > c->T.ref_cap)
+		return cls_fail(c, HERA_GPU_ECAPACITY, "class table too small for the classes loaded");
+	const uint32_t nc = in->n_classes;
+	std::vector<unsigned long long> cnt(nc), off(nc);
+	for (uint32_t i = 0; i < nc; ++i) {
+		const double x = in->count[i];
+		if (!(x >= 0) || x != (double)(unsigned long long)x || x >= 9007199254740992.0)
+			return cls_fail(c, HERA_GPU_EINVAL, "class counts must be whole numbers below 2^53");
+		if (in->list_off[i] + in->n[i] > in->list_used)
+			return cls_fail(c, HERA_GPU_EINVAL, "a class list lies outside the list entries");
+		cnt[i] = (unsigned long long)x;
+		off[i] = in->list_off[i];
+	}
+	if (!(in->mean_frag_sum >= 0) || in->mean_frag_sum >= 9007199254740992.0)
+		return cls_fail(c, HERA_GPU_EINVAL, "bad fragment sum");
+	if (cudaSetDevice(c->device) != cudaSuccess)
+		return cls_fail(c, HERA_GPU_ENODEV, "cudaSetDevice");
+	cls::Table &T = c->T;
+	const cudaStream_t st = c->stream;
+	cls::State s{};
+	s.n_classes = nc;
+	s.ref_used = in->list_used;
+	s.paired = in->paired;
+	s.frag = (unsigned long long)in->mean_frag_sum;
+	const size_t slots = (size_t)T.mask + 1;
+	cudaError_t e;
+	if ((e = cudaMemsetAsync(T.keys, 0, slots * 8, st)) != cudaSuccess ||
+	    (e = cudaMemsetAsync(T.cls_of, 0, slots * 4, st)) != cudaSuccess ||
+	    (e = cudaMemsetAsync(T.first, 0xff, slots * 4, st)) != cudaSuccess ||
+	    (e = cudaMemsetAsync(T.pend, 0, slots * 4, st)) != cudaSuccess ||
+	    (nc && (e = cudaMemcpyAsync(T.id, in->id, (size_t)nc * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+	    (nc && (e = cudaMemcpyAsync(T.count, cnt.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+	    (nc && (e = cudaMemcpyAsync(T.n, in->n, (size_t)nc * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+	    (nc && (e = cudaMemcpyAsync(T.ref_off, off.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+	    (in->list_used && (e = cudaMemcpyAsync(T.ref, in->list, (size_t)in->list_used * 4, cudaMemcpyHostToDevice,
+						   st)) != cudaSuccess) ||
+	    (e = (in->tx_count ? cudaMemcpyAsync(T.tx_count, in->tx_count, (size_t)T.n_trans * 4,
+						 cudaMemcpyHostToDevice, st)
+			       : cudaMemsetAsync(T.tx_count, 0, (size_t)T.n_trans * 4, st))) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(T.st, &s, sizeof s, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+		return cls_fail(c, HERA_GPU_ECUDA, "class table load", e);
+	if (nc) {
+		cls::k_cls_load_keys<<<blocks_for(nc, 256), 256, 0, st>>>(T, nc);
+		cls::k_cls_load_number<<<blocks_for(nc, 256), 256, 0, st>>>(T, nc);
+	}
+	cls::k_cls_load_reset<<<blocks_for((int64_t)slots, 256), 256, 0, st>>>(T);
+	c->broken = false;
+	c->items_done = 0;
+	return cls_check(c);
+}
+
 extern "C" int hera_gpu_classes_fetch(hera_gpu_classes *c, hera_gpu_class_table *out)
 {
 	if (!c || !out)
@@ -632,4 +739,333 @@ extern "C" int hera_gpu_classes_timing(const hera_gpu_classes *c, float *kernel_
 extern "C" const char *hera_gpu_classes_last_error(const hera_gpu_classes *c)
 {
 	return c ? c->err.c_str() : "null class table";
+}
+
+// ---------------------------------------------------------------------------
+// The EM over the class table: hera's estimate_count (src/EM.c:315-387),
+// SQUAREM over M_step (:271-302), bit for bit.
+//
+// Every floating-point operation is the reference's, in its order, with
+// explicit round-to-nearest intrinsics (nothing is contracted into an FMA):
+//   - a class's total (sum of grama over its list) is summed in list order
+//     by one thread per class;
+//   - a transcript's overlap is summed in class order by one thread per
+//     transcript over the table's list entries sorted stably by transcript
+//     (a radix sort keeps entry order, which is class order);
+//   - the two Norm sums (src/hash_align.c:150-164) and the final sum run in
+//     index order in one warp each (seq_sum) -- a sequential double sum has
+//     only one rounding sequence;
+//   - the convergence flag is an "any transcript moved > 1%", which does
+//     not depend on order.
+namespace em {
+
+__global__ void k_em_entries(const unsigned long long *ref_off, const uint32_t *n, uint32_t nc, uint32_t *ecls)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nc)
+		return;
+	const unsigned long long o = ref_off[i];
+	for (uint32_t k = 0; k < n[i]; ++k)
+		ecls[o + k] = i;
+}
+
+__global__ void k_em_hist(const uint32_t *ref, int64_t L, uint32_t nt, uint32_t *hist, uint32_t *flags)
+{
+	const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= L)
+		return;
+	const uint32_t t = ref[e];
+	if (t < nt)
+		atomicAdd(&hist[t], 1u);
+	else
+		atomicOr(flags, 1u);
+}
+
+__global__ void k_em_prep(const unsigned long long *cnt, uint32_t nc, double *dc, double *g, uint32_t nt)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < nc)
+		dc[i] = (double)cnt[i];
+	if (i < nt)
+		g[i] = __ddiv_rn(1.0, (double)nt);            // E_step (src/EM.c:304-313)
+}
+
+__global__ void k_em_total(const unsigned long long *ref_off, const uint32_t *n, const uint32_t *ref, uint32_t nc,
+			   const double *g, double *tot)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nc)
+		return;
+	const uint32_t *l = ref + ref_off[i];
+	double total = 0.0;
+	for (uint32_t k = 0; k < n[i]; ++k)
+		total = __dadd_rn(total, g[l[k]]);
+	tot[i] = total;
+}
+
+__global__ void k_em_tx(const uint32_t *seg, const uint32_t *ecls, const double *dc, const double *tot,
+			const double *g, const uint32_t *txc, const uint32_t *len, uint32_t nt, double *next,
+			int *busy)
+{
+	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= nt)
+		return;
+	const double gt = g[t];
+	double acc = 0.0;
+	for (uint32_t e = seg[t]; e < seg[t + 1]; ++e) {
+		const uint32_t i = ecls[e];
+		const double total = tot[i];
+		if (total == 0)
+			continue;
+		acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(gt, dc[i]), total));
+	}
+	const double x = __ddiv_rn(__dadd_rn((double)txc[t], acc), (double)len[t]);
+	next[t] = x;
+	if (x > 1e-3) {
+		const double d = __dsub_rn(x, gt);
+		const double err = __ddiv_rn(d < 0 ? -d : d, x);
+		if (err > 0.01)
+			*busy = 1;
+	}
+}
+
+__global__ void k_em_rv(const double *u, const double *u1, const double *u2, double *r, double *v, uint32_t nt)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nt)
+		return;
+	const double ri = __dsub_rn(u1[i], u[i]);
+	r[i] = ri;
+	v[i] = __dsub_rn(__dsub_rn(u2[i], u1[i]), ri);
+}
+
+// Sum of f(a[0]), f(a[1]), ... in index order, rounded after every add, as
+// a C loop does it.  One warp: 256 elements at a time go through shared
+// memory (8 coalesced loads a lane), the next 256 are loaded into registers
+// while these are added, and every lane runs the same add chain over the
+// staged values (broadcast reads), so every lane ends with the same sum.
+// The chain of dependent adds is the bound.
+template <typename F>
+__device__ double seq_sum(const double *a, uint32_t n, F f, double *sm)
+{
+	const uint32_t lane = threadIdx.x & 31;
+	double nxt[8];
+#pragma unroll
+	for (int u = 0; u < 8; ++u) {
+		const uint32_t i = u * 32 + lane;
+		sm[i] = i < n ? a[i] : 0.0;
+	}
+	__syncwarp();
+	double s = 0.0;
+	for (uint32_t base = 0; base < n; base += 256) {
+#pragma unroll
+		for (int u = 0; u < 8; ++u) {
+			const uint64_t i = (uint64_t)base + 256 + u * 32 + lane;
+			nxt[u] = i < n ? a[i] : 0.0;
+		}
+		const uint32_t m = n - base < 256 ? n - base : 256;
+		if (m == 256) {
+#pragma unroll 32
+			for (int j = 0; j < 256; ++j)
+				s = __dadd_rn(s, f(sm[j]));
+		} else {
+			for (uint32_t j = 0; j < m; ++j)
+				s = __dadd_rn(s, f(sm[j]));
+		}
+		__syncwarp();
+#pragma unroll
+		for (int u = 0; u < 8; ++u)
+			sm[u * 32 + lane] = nxt[u];
+		__syncwarp();
+	}
+	return s;
+}
+
+// Norm (src/hash_align.c:150-164), one warp a vector: block 0 r -> scal[0],
+// block 1 v -> scal[1]
+__global__ void k_em_norms(const double *r, const double *v, uint32_t nt, double *scal)
+{
+	__shared__ double sm[256];
+	const double *a = blockIdx.x ? v : r;
+	double mean = seq_sum(a, nt, [](double x) { return x; }, sm);
+	mean = __ddiv_rn(mean, (double)nt);
+	double total = seq_sum(a, nt, [mean](double x) {
+		const double d = __dsub_rn(x, mean);
+		return __dmul_rn(d, d);
+	}, sm);
+	total = __ddiv_rn(total, (double)(nt - 1));
+	if (threadIdx.x == 0)
+		scal[blockIdx.x] = __dsqrt_rn(total);
+}
+
+__global__ void k_em_step(const double *u, const double *r, const double *v, const double *scal, double *u1,
+			  uint32_t nt)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nt)
+		return;
+	const double n_r = scal[0], n_v = scal[1];
+	double alpha = n_v != 0 ? __ddiv_rn(-n_r, n_v) : -1.0;
+	if (alpha > -1)
+		alpha = -1.0;
+	double x = __dadd_rn(__dsub_rn(u[i], __dmul_rn(__dmul_rn(2.0, alpha), r[i])),
+			     __dmul_rn(__dmul_rn(alpha, alpha), v[i]));
+	if (x < 0)
+		x = 0;
+	u1[i] = x;
+}
+
+__global__ void k_em_sum(const double *g, uint32_t nt, double *sum)
+{
+	__shared__ double sm[256];
+	const double s = seq_sum(g, nt, [](double x) { return x; }, sm);
+	if (threadIdx.x == 0)
+		*sum = s;
+}
+
+__global__ void k_em_final(const double *g, const uint32_t *len, const double *sum, double *grama, double *overlap,
+			   uint32_t nt)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nt)
+		return;
+	const double s = *sum;
+	if (s == 0) {
+		grama[i] = 0;
+		overlap[i] = 0;
+	} else {
+		overlap[i] = __dmul_rn(g[i], (double)len[i]);
+		grama[i] = __ddiv_rn(__dmul_rn(g[i], 1000000.0), s);
+	}
+}
+
+}   // namespace em
+
+extern "C" int hera_gpu_classes_em(hera_gpu_classes *c, hera_gpu_ctx *ctx, double *grama, double *overlap,
+				   uint32_t *rounds, float *em_ms)
+{
+	if (!c)
+		return HERA_GPU_EINVAL;
+	if (!ctx || ctx->device != c->device || !grama || !overlap || ctx->ix.n_trans != c->T.n_trans ||
+	    c->T.n_trans < 1)
+		return cls_fail(c, HERA_GPU_EINVAL, "bad argument");
+	if (c->broken)
+		return cls_fail(c, HERA_GPU_ECAPACITY, "class table overflowed earlier");
+	if (cudaSetDevice(c->device) != cudaSuccess)
+		return cls_fail(c, HERA_GPU_ENODEV, "cudaSetDevice");
+	cls::State s{};
+	cudaError_t e = cudaMemcpyAsync(&s, c->T.st, sizeof s, cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(c->stream);
+	if (e != cudaSuccess)
+		return cls_fail(c, HERA_GPU_ECUDA, "class table state", e);
+	const uint32_t nt = c->T.n_trans, nc = s.n_classes;
+	const int64_t L = (int64_t)s.ref_used;
+	if (L >= (1ll << 31))
+		return cls_fail(c, HERA_GPU_ECAPACITY, "more than 2^31 list entries");
+	const cudaStream_t st = c->stream;
+	// buffers: 6 transcript vectors, 2 class vectors, entries x3, segments, flags
+	double *d = nullptr, *dc = nullptr;
+	uint32_t *ecls = nullptr, *keys = nullptr, *vals = nullptr, *seg = nullptr;
+	int *busy = nullptr;
+	void *tmp = nullptr;
+	size_t tmp_sort = 0, tmp_scan = 0;
+	cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+					(const uint32_t *)nullptr, (uint32_t *)nullptr, (int)std::max<int64_t>(L, 1), 0, 32,
+					st);
+	cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, (uint32_t *)nullptr, (uint32_t *)nullptr, nt + 1, st);
+	const size_t tmp_bytes = std::max(tmp_sort, tmp_scan) + 16;
+	int rc = HERA_GPU_OK;
+	auto grab = [&](void **p, size_t bytes) {
+		if (rc != HERA_GPU_OK)
+			return;
+		cudaError_t ee = cudaMalloc(p, bytes);
+		if (ee != cudaSuccess)
+			rc = cls_fail(c, HERA_GPU_ENOMEM, "EM buffers", ee);
+	};
+	grab((void **)&d, (size_t)8 * nt * 7 + 16);      // u, A, B, C, r, v, scalars
+	grab((void **)&dc, (size_t)16 * (nc ? nc : 1));  // class counts as double, class totals
+	grab((void **)&ecls, (size_t)4 * (L ? L : 1));
+	grab((void **)&keys, (size_t)4 * (L ? L : 1));
+	grab((void **)&vals, (size_t)4 * (L ? L : 1));
+	grab((void **)&seg, (size_t)8 * (nt + 2));      // per-transcript counts, then their offsets
+	grab((void **)&busy, 16);
+	grab(&tmp, tmp_bytes);
+	auto release = [&]() {
+		cudaFree(d); cudaFree(dc); cudaFree(ecls); cudaFree(keys); cudaFree(vals); cudaFree(seg);
+		cudaFree(busy); cudaFree(tmp);
+	};
+	if (rc != HERA_GPU_OK) {
+		release();
+		return rc;
+	}
+	double *vec[4] = {d, d + nt, d + 2 * (size_t)nt, d + 3 * (size_t)nt};   // u, A, B, C
+	double *r = d + 4 * (size_t)nt, *v = d + 5 * (size_t)nt, *scal = d + 6 * (size_t)nt;
+	double *tot = dc + (nc ? nc : 1);
+	const unsigned bt = blocks_for(nt, 256), bc = blocks_for(nc ? nc : 1, 256);
+	cudaEventRecord(c->ev0, st);
+	// transcript-major view of the lists, entries in class order
+	uint32_t *hist = seg + (nt + 2);
+	cudaMemsetAsync(hist, 0, (size_t)4 * (nt + 2), st);
+	cudaMemsetAsync(busy, 0, 16, st);
+	if (L > 0) {
+		em::k_em_entries<<<bc, 256, 0, st>>>(c->T.ref_off, c->T.n, nc, ecls);
+		em::k_em_hist<<<blocks_for(L, 256), 256, 0, st>>>(c->T.ref, L, nt, hist, (uint32_t *)(busy + 2));
+		size_t tb = tmp_bytes;
+		cub::DeviceRadixSort::SortPairs(tmp, tb, c->T.ref, keys, ecls, vals, (int)L, 0, 32, st);
+	}
+	{
+		size_t tb = tmp_bytes;
+		cub::DeviceScan::ExclusiveSum(tmp, tb, hist, seg, nt + 1, st);
+	}
+	em::k_em_prep<<<std::max(bt, bc), 256, 0, st>>>(c->T.count, nc, dc, vec[0], nt);
+	auto m_step = [&](const double *g, double *next, int *flag) {
+		if (nc)
+			em::k_em_total<<<bc, 256, 0, st>>>(c->T.ref_off, c->T.n, c->T.ref, nc, g, tot);
+		em::k_em_tx<<<bt, 256, 0, st>>>(seg, vals, dc, tot, g, c->T.tx_count, ctx->d_tlen, nt, next, flag);
+	};
+	uint32_t k = 0;
+	int host_busy = 1;
+	while (k < 50 || (k < 1000 && host_busy)) {
+		double *u = vec[0], *A = vec[1], *B = vec[2], *C = vec[3];
+		m_step(u, A, busy + 1);
+		m_step(A, B, busy + 1);
+		em::k_em_rv<<<bt, 256, 0, st>>>(u, A, B, r, v, nt);
+		em::k_em_norms<<<2, 32, 0, st>>>(r, v, nt, scal);
+		em::k_em_step<<<bt, 256, 0, st>>>(u, r, v, scal, A, nt);
+		cudaMemsetAsync(busy, 0, 4, st);
+		m_step(A, C, busy);
+		vec[0] = C;
+		vec[3] = u;
+		++k;
+		if (k >= 50) {   // the loop test reads the last M_step's flag
+			if ((e = cudaMemcpyAsync(&host_busy, busy, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+			    (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+				rc = cls_fail(c, HERA_GPU_ECUDA, "EM", e);
+				break;
+			}
+		}
+	}
+	if (rc == HERA_GPU_OK) {
+		em::k_em_sum<<<1, 32, 0, st>>>(vec[0], nt, scal + 2);
+		// results into r and v, then to the host
+		em::k_em_final<<<bt, 256, 0, st>>>(vec[0], ctx->d_tlen, scal + 2, r, v, nt);
+		cudaEventRecord(c->ev1, st);
+		int hflags = 0;
+		if ((e = cudaMemcpyAsync(grama, r, (size_t)8 * nt, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+		    (e = cudaMemcpyAsync(overlap, v, (size_t)8 * nt, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+		    (e = cudaMemcpyAsync(&hflags, busy + 2, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+		    (e = cudaStreamSynchronize(st)) != cudaSuccess)
+			rc = cls_fail(c, HERA_GPU_ECUDA, "EM results", e);
+		else if (hflags)
+			rc = cls_fail(c, HERA_GPU_EINVAL, "a class list names no transcript of the index");
+		float ms = 0;
+		cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+		if (em_ms)
+			*em_ms = ms;
+		if (rounds)
+			*rounds = k;
+	}
+	release();
+	return rc;
 }

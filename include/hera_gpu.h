@@ -531,6 +531,24 @@ int hera_gpu_classes_add_host(hera_gpu_classes *c, const hera_gpu_result *res, i
 /* Copy the table out (see hera_gpu_class_table). */
 int hera_gpu_classes_fetch(hera_gpu_classes *c, hera_gpu_class_table *out);
 
+/* Replace the table's contents with a class table given in host memory
+ * (the layout hera_gpu_classes_fetch fills: n_classes classes with whole-
+ * number counts, list_used list entries, tx_count or NULL for zeros, PAIRED
+ * and the fragment sum): hera's CLASS and REF_INF->count as its own
+ * add_class built them, for callers that keep the tail on the host and run
+ * the EM below on the device.  Later adds continue the table. */
+int hera_gpu_classes_load(hera_gpu_classes *c, const hera_gpu_class_table *in);
+
+/* hera's EM, estimate_count (src/EM.c:315-387: SQUAREM over M_step with
+ * E_step's uniform start, Norm of src/hash_align.c:150-164), over the
+ * table's classes, its per-transcript counts and ctx's transcript lengths
+ * (REF_INF->len).  grama and overlap (n_trans doubles each, host memory)
+ * receive em_val->grama and em_val->overlap bit for bit as the reference
+ * leaves them; *rounds the SQUAREM iterations, *em_ms the device time
+ * (either may be NULL).  Allocates its working memory per call. */
+int hera_gpu_classes_em(hera_gpu_classes *c, hera_gpu_ctx *ctx, double *grama, double *overlap,
+			uint32_t *rounds, float *em_ms);
+
 /* Device time (CUDA events, from the first kernel of the last add call to
  * its end; the call's first-use allocations are not in it) and the
  * kernels it launched. */

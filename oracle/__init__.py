@@ -135,6 +135,24 @@ def _em_args(table: ClassTable, ix):
             C.c_void_p(_ptr(ns)), C.c_void_p(_ptr(offs)), C.c_void_p(_ptr(ref))]
 
 
+def em_port(table, length) -> tuple:
+    """estimate_count restated (ho_em) over any class table with counts, ns,
+    ref_off, ref, tx_count and n_classes, with transcript lengths `length`:
+    (grama, overlap, rounds).  No index needed."""
+    lib = C.CDLL(ORACLE_SO)
+    n = len(length)
+
+    class _Ix:
+        pass
+    ix = _Ix()
+    ix.length = np.ascontiguousarray(length, np.uint32)
+    g, o = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+    rounds = C.c_uint32()
+    a = _em_args(table, ix)
+    lib.ho_em(C.c_uint32(n), *a, C.c_void_p(_ptr(g)), C.c_void_p(_ptr(o)), C.byref(rounds))
+    return g[:n], o[:n], rounds.value
+
+
 def _export_classes(sizes, export, n_trans: int) -> ClassTable:
     nc, rn = C.c_uint32(), C.c_uint64()
     sizes(C.byref(nc), C.byref(rn))
@@ -223,7 +241,7 @@ class Oracle:
         g, o = np.zeros(max(n, 1)), np.zeros(max(n, 1))
         rounds = C.c_uint32()
         a = _em_args(table, self.ix)
-        self.lib.ho_em(C.c_uint32(n), *a[:1], *a[1:], C.c_void_p(_ptr(g)), C.c_void_p(_ptr(o)), C.byref(rounds))
+        self.lib.ho_em(C.c_uint32(n), *a, C.c_void_p(_ptr(g)), C.c_void_p(_ptr(o)), C.byref(rounds))
         return g[:n], o[:n], rounds.value
 
     def xxh32(self, data: bytes, seed: int = 0) -> int:

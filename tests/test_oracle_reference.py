@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import oracle
+from tests import em_cases
 from hera_b200 import synth, workloads
 
 pytestmark = pytest.mark.skipif(not oracle.reference_available(), reason="reference not built")
@@ -71,25 +72,9 @@ def test_em_matches_reference(both, wl):
     assert np.array_equal(ov.view(np.uint64), OV.view(np.uint64))
 
 
-def slow_table(n_trans: int) -> "oracle.ClassTable":
-    """Triples of transcripts, each with one heavy shared class (1e5 reads)
-    and a light class (1 read) on two of them: on the config-1 index SQUAREM
-    runs past its 50-round minimum here, so the convergence test decides."""
-    lists, counts = [], []
-    for i in range(0, n_trans - 2, 3):
-        lists += [[i, i + 1, i + 2], [i, i + 1]]
-        counts += [1e5, 1.0]
-    ns = np.array([len(x) for x in lists], np.uint32)
-    off = np.zeros(len(ns), np.uint64)
-    off[1:] = np.cumsum(ns[:-1])
-    return oracle.ClassTable(np.arange(len(ns), dtype=np.uint32), np.array(counts), ns, off,
-                             np.concatenate([np.array(x, np.uint32) for x in lists]),
-                             np.zeros(n_trans, np.uint32), 0, 0.0)
-
-
 def test_em_past_minimum_rounds_matches_reference(both):
     ann, tx, o, ref = both
-    t = slow_table(o.ix.n_trans)
+    t = em_cases.slow_table(o.ix.n_trans)
     g, ov, rounds = o.em(t)
     assert rounds > 50
     G, OV = ref.em(t, o.ix.n_trans)

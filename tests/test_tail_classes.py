@@ -208,3 +208,68 @@ def test_per_sample_classes_served_equal_alone(cfg1_ctx, oracle1):
                 cls.close()
         want = oracle1.classes([oracle1.align_pairs(chunks[k][1].copy(), chunks[k][2].copy(), 1) for k in ks])
         assert tabs[0].key() == tabs[1].key() == want.key(), f"sample {s}"
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.uint64)
+
+
+@pytest.mark.parametrize("name", ["pairs100", "pairs_mixed", "pairs_n"])
+def test_device_em_golden(small_ctx, name):
+    """hera's EM on the device over the class table of the golden records:
+    grama and overlap bit for bit as the reference's estimate_count left
+    them on the same table."""
+    torch, ix, ctx = small_ctx
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "classes.npz"))
+    key = f"{name}_wb1"
+    cls = api.Classes(ctx, max_classes=4096, max_list=1 << 16)
+    try:
+        keep = _add(cls, torch, c[f"{key}_recs"], c[f"{key}_pos"], c[f"{key}_p"], True)
+        g, o, rounds, ms = cls.em(ctx)
+    finally:
+        cls.close()
+    del keep
+    assert np.array_equal(_bits(g), _bits(d[f"{name}_em_grama"]))
+    assert np.array_equal(_bits(o), _bits(d[f"{name}_em_overlap"]))
+    assert rounds >= 50 and ms > 0
+
+
+def test_device_em_after_align(cfg1_ctx, oracle1):
+    """Align, classes and EM all on the device; equal to the oracle's EM
+    (pinned to the reference's) over the oracle's own classes."""
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    r1, r2 = workloads.pairs("config4", ann, tx, 20000, seed=215)
+    want_t = oracle1.classes([oracle1.align_pairs(r1.copy(), r2.copy(), 1)])
+    g0, o0, k0 = oracle1.em(want_t)
+    seq, off, lens = workloads.interleave(r1, r2)
+    dv = [torch.from_numpy(x).cuda() for x in (seq, off, lens)]
+    torch.cuda.synchronize()
+    ctx.align_pairs_device(dv[0].data_ptr(), dv[1].data_ptr(), dv[2].data_ptr(), r1.n, int(lens.max()), 1)
+    cls = api.Classes(ctx, max_classes=1 << 16, max_list=1 << 20)
+    try:
+        cls.add_last(ctx)
+        g, o, k, _ = cls.em(ctx)
+    finally:
+        cls.close()
+    assert k == k0
+    assert np.array_equal(_bits(g), _bits(g0)) and np.array_equal(_bits(o), _bits(o0))
+
+
+def test_device_em_loaded_table_past_minimum(cfg1_ctx, oracle1):
+    """A class table loaded from the host (hera's own CLASS), on which
+    SQUAREM runs past 50 rounds: same rounds and arrays as the oracle."""
+    from tests import em_cases
+    torch, ann, tx, ix, ctx = cfg1_ctx
+    t = em_cases.slow_table(ix.n_trans)
+    g0, o0, k0 = oracle1.em(t)
+    assert k0 > 50
+    cls = api.Classes(ctx, max_classes=1 << 12, max_list=1 << 14)
+    try:
+        cls.load(t)
+        assert cls.fetch().key()[1:] == t.key()[1:]
+        g, o, k, _ = cls.em(ctx)
+    finally:
+        cls.close()
+    assert k == k0
+    assert np.array_equal(_bits(g), _bits(g0)) and np.array_equal(_bits(o), _bits(o0))
