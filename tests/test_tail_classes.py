@@ -179,8 +179,8 @@ def test_classes_after_page_locked_fetch(cfg1_ctx, oracle1):
 def test_per_sample_classes_served_equal_alone(cfg1_ctx, oracle1):
     """Serving: one class table per sample, fed with the sample's served
     chunks in its own order (add_host), equals the table of the sample's
-    chunks aligned alone, and the oracle's -- the EM input of every sample
-    is the same in the mix as alone."""
+    chunks aligned alone, and the oracle's; the sample's EM abundances on
+    the device are the oracle's (the reference's) bit for bit."""
     torch, ann, tx, ix, ctx = cfg1_ctx
     sizes = [3000, 11000, 700, 5000, 16000, 2500, 9000]
     models = ["config1", "config3", "config4"]
@@ -197,17 +197,21 @@ def test_per_sample_classes_served_equal_alone(cfg1_ctx, oracle1):
         srv.close()
     for s in range(3):
         ks = [k for k, (si, _, _) in enumerate(chunks) if si == s]
-        tabs = []
+        tabs, ems = [], []
         for src in (served, alone):
             cls = api.Classes(ctx, max_classes=1 << 14, max_list=1 << 18)
             try:
                 for k in ks:
                     cls.add_result(src[k], paired=True)
                 tabs.append(cls.fetch())
+                ems.append(cls.em(ctx))
             finally:
                 cls.close()
         want = oracle1.classes([oracle1.align_pairs(chunks[k][1].copy(), chunks[k][2].copy(), 1) for k in ks])
         assert tabs[0].key() == tabs[1].key() == want.key(), f"sample {s}"
+        g0, o0, k0 = oracle1.em(want)
+        for g, o, k, _ in ems:
+            assert k == k0 and np.array_equal(_bits(g), _bits(g0)) and np.array_equal(_bits(o), _bits(o0))
 
 
 def _bits(a):
