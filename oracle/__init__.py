@@ -153,6 +153,75 @@ def em_port(table, length) -> tuple:
     return g[:n], o[:n], rounds.value
 
 
+class GeneMap:
+    """GENE_MAP as hera builds it from reference.inf (contruct_gene_map,
+    src/bam_write.c:22-57, after init_bam_header's reference block)."""
+
+    def __init__(self, path: str, n_trans: int):
+        b = open(path, "rb").read()
+        u32 = lambda o, k=1: np.frombuffer(b, np.uint32, k, o)
+        o = 4 + int(u32(0)[0])
+        n_chr, l_chr = (int(x) for x in u32(o, 2))
+        o += 8 + n_chr * l_chr
+        self.chr_len = u32(o, n_chr).copy()
+        o += 4 * n_chr
+        n_gene, l_gene = (int(x) for x in u32(o, 2))
+        o += 8 + n_gene * l_gene
+        starts, ends, off = [], [], [0]
+        for _ in range(n_trans):
+            ne = int(u32(o)[0]) & 0xFFFF   # read into an unsigned short
+            starts.append(u32(o + 4, ne))
+            ends.append(u32(o + 4 + 4 * ne, ne))
+            o += 4 + 8 * ne
+            off.append(off[-1] + ne)
+        self.exon_off = np.array(off, np.uint32)
+        self.starts = np.concatenate(starts).astype(np.uint32)
+        self.ends = np.concatenate(ends).astype(np.uint32)
+        self.chr = u32(o, n_trans).copy()
+        self.gene = u32(o + 4 * n_trans, n_trans).copy()
+
+    def c_struct(self):
+        class _GM(C.Structure):
+            _fields_ = [("n_chr", C.c_uint32), ("chr_len", C.c_void_p), ("exon_off", C.c_void_p),
+                        ("starts", C.c_void_p), ("ends", C.c_void_p), ("chr", C.c_void_p), ("gene", C.c_void_p)]
+        return _GM(len(self.chr_len), _ptr(self.chr_len), _ptr(self.exon_off), _ptr(self.starts),
+                   _ptr(self.ends), _ptr(self.chr), _ptr(self.gene))
+
+
+def read_names(n: int, mate: int, stride: int = 16) -> np.ndarray:
+    """Mutable NUL-padded names r000000/1 ... as the BAM writer expects."""
+    a = np.zeros((n, stride), np.uint8)
+    for i in range(n):
+        s = f"r{i:06d}/{mate}".encode()
+        a[i, :len(s)] = np.frombuffer(s, np.uint8)
+    return a
+
+
+def _bam_args(r1, r2, quals, names):
+    q1, q2 = quals
+    n1, n2 = names
+    return [C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)), C.c_void_p(_ptr(q1)),
+            C.c_void_p(_ptr(n1)), C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+            C.c_void_p(_ptr(q2)), C.c_void_p(_ptr(n2)), C.c_int32(n1.shape[1])]
+
+
+def bam_pairs(gm: GeneMap, res: "Result", r1, r2, quals, names, cap: int = 1 << 26):
+    """ho_bam_pairs: the tail's uncompressed BAM records per pair, from the
+    oracle's `-w` records.  Returns (bytes, offsets)."""
+    lib = C.CDLL(ORACLE_SO)
+    n = r1.n
+    out = np.zeros(cap, np.uint8)
+    off = np.zeros(n + 1, np.uint64)
+    g = gm.c_struct()
+    rc = lib.ho_bam_pairs(C.byref(g), C.c_void_p(_ptr(res.recs)), C.c_void_p(_ptr(res.pos_pool)),
+                          C.c_void_p(_ptr(res.p_pool)), C.c_void_p(_ptr(res.op_pool)), C.c_void_p(_ptr(res.miss_pool)),
+                          n, *_bam_args(r1, r2, quals, names), C.c_void_p(_ptr(out)), C.c_uint64(cap),
+                          C.c_void_p(_ptr(off)))
+    if rc != 0:
+        raise RuntimeError("BAM output buffer too small")
+    return out[:int(off[-1])].copy(), off
+
+
 def _export_classes(sizes, export, n_trans: int) -> ClassTable:
     nc, rn = C.c_uint32(), C.c_uint64()
     sizes(C.byref(nc), C.byref(rn))

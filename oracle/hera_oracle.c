@@ -25,6 +25,8 @@
 #include <stdlib.h>
 #include <string.h>
 #include <math.h>
+#include <stddef.h>
+#include <stdio.h>
 #include <pthread.h>
 
 enum { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4, OP_X = 8 };
@@ -1713,4 +1715,435 @@ void ho_em(uint32_t n_trans, const uint32_t *len, const uint32_t *tx_count, uint
 	}
 	*rounds = k;
 	free(grama); free(overlap); free(r); free(v);
+}
+
+/* ===========================================================================
+ * BAM records of the host tail (`-w`)
+ * ======================================================================== */
+
+enum { B_MATCH = 0, B_DELETE = 2, B_SKIP = 3, B_DIFF = 8 };
+
+/* bam_nt16_table (src/bam_write.c:3-20): =ACMGRSVTWYHKDBN -> 0..15 */
+static unsigned char b_nt16(unsigned char c)
+{
+	switch (c) {
+	case '=': return 0;
+	case 'A': case 'a': return 1;
+	case 'C': case 'c': return 2;
+	case 'M': case 'm': return 3;
+	case 'G': case 'g': return 4;
+	case 'R': case 'r': return 5;
+	case 'S': case 's': return 6;
+	case 'V': case 'v': return 7;
+	case 'T': case 't': return 8;
+	case 'W': case 'w': return 9;
+	case 'Y': case 'y': return 10;
+	case 'H': case 'h': return 11;
+	case 'K': case 'k': return 12;
+	case 'D': case 'd': return 13;
+	case 'B': case 'b': return 14;
+	default: return 15;
+	}
+}
+
+/* One strand of a Candidate as the tail sees it. */
+typedef struct {
+	uint32_t n;
+	const uint32_t *pos;
+	const int32_t *p;
+	uint32_t n_cigar, n_miss;
+	const uint32_t *ops;    /* (count << 4) | type */
+	const char *miss;
+} b_strand;
+
+typedef struct {
+	b_strand s[2];
+	int err[2];
+	int pair;
+} b_cand;
+
+static void b_swap(b_cand *a, int pa, b_cand *b, int pb)   /* swap_candidate (:1640-1661) */
+{
+	b_strand t = a->s[pa];
+	a->s[pa] = b->s[pb];
+	b->s[pb] = t;
+}
+
+static uint32_t b_exon_start(const ho_gene_map *g, uint32_t t, uint32_t e) { return g->starts[g->exon_off[t] + e]; }
+static uint32_t b_exon_end(const ho_gene_map *g, uint32_t t, uint32_t e) { return g->ends[g->exon_off[t] + e]; }
+
+/* check_overlapGene (src/hash_align.c:395-414) */
+static int b_overlap_gene(const ho_gene_map *g, uint32_t t1, uint32_t t2)
+{
+	if (t1 == t2 || g->gene[t1] == g->gene[t2])
+		return 1;
+	if (g->chr[t1] != g->chr[t2])
+		return 0;
+	uint32_t s0 = b_exon_start(g, t1, 0), s1 = b_exon_start(g, t2, 0);
+	uint32_t e0 = b_exon_end(g, t1, g->exon_off[t1 + 1] - g->exon_off[t1] - 1);
+	uint32_t e1 = b_exon_end(g, t2, g->exon_off[t2 + 1] - g->exon_off[t2] - 1);
+	return !(s1 > e0 || s0 > e1);
+}
+
+/* check_quanlity (:416-427): genes among the hits, counted by runs */
+static unsigned b_genes(const ho_gene_map *g, const b_strand *s)
+{
+	if (s->n == 0)
+		return 0;
+	unsigned k = 1;
+	for (uint32_t i = 1; i < s->n; ++i)
+		if (!b_overlap_gene(g, s->pos[i], s->pos[i - 1]))
+			++k;
+	return k;
+}
+
+/* get_qual (src/bam_write.c:199-205) */
+static unsigned int b_qual(unsigned int n)
+{
+	double error = 1 - (1.0 / n);
+	if (error == 0)
+		error = 0.0000001;
+	return -10 * log10(error);
+}
+
+static int b_reg2bin(unsigned int beg, unsigned int end)   /* bam_reg2bin (:59-68) */
+{
+	--end;
+	if (beg >> 14 == end >> 14) return 4681 + (beg >> 14);
+	if (beg >> 17 == end >> 17) return 585 + (beg >> 17);
+	if (beg >> 20 == end >> 20) return 73 + (beg >> 20);
+	if (beg >> 23 == end >> 23) return 9 + (beg >> 23);
+	if (beg >> 26 == end >> 26) return 1 + (beg >> 26);
+	return 0;
+}
+
+static unsigned int b_flag(unsigned pair, unsigned proper, unsigned map, unsigned mmap, unsigned rev,
+			   unsigned mrev, unsigned first, unsigned last)   /* make_flag (:70-86) */
+{
+	return last << 7 | first << 6 | mrev << 5 | rev << 4 | mmap << 3 | map << 2 | proper << 1 | pair;
+}
+
+typedef struct {
+	int bin, qual, ref, pos, n_cigar;
+	unsigned int len, block_len, coord, match, align_len;
+	char md[2048];
+	uint32_t cig[1024];
+	uint8_t data[8192];
+} b_core;
+
+/* add_padding (:89-116): a match run over exon junctions gets N ops */
+static void b_pad(const ho_gene_map *g, b_core *c, unsigned int *n, unsigned int *l, uint32_t t,
+		  unsigned int len, unsigned int type, unsigned int genome)
+{
+	if ((type != B_MATCH && type != B_DIFF) || genome == 1) {
+		c->cig[(*n)++] = len << 4 | type;
+		return;
+	}
+	*l += len;
+	while (*l > b_exon_end(g, t, c->coord) + 1) {
+		len -= *l - b_exon_end(g, t, c->coord) - 1;
+		c->cig[(*n)++] = len << 4 | type;
+		len = b_exon_start(g, t, c->coord + 1) - b_exon_end(g, t, c->coord) - 1;
+		c->align_len += len;
+		c->cig[(*n)++] = len << 4 | B_SKIP;
+		len = *l - b_exon_end(g, t, c->coord) - 1;
+		*l += b_exon_start(g, t, c->coord + 1) - b_exon_end(g, t, c->coord) - 1;
+		++c->coord;
+	}
+	c->cig[(*n)++] = len << 4 | type;
+}
+
+/* convert_cigar (:118-197): position on the genome, MD string, CIGAR */
+static void b_convert(const ho_gene_map *g, b_core *c, const b_strand *s, uint32_t hit, unsigned int genome)
+{
+	const uint32_t t = s->pos[hit];
+	if (genome == 0) {
+		c->ref = g->chr[t];
+		/* gene_coord (src/hash_align.c:320-334) */
+		int pos = s->p[hit];
+		if (pos <= 0) {
+			c->coord = 0;
+			c->pos = b_exon_start(g, t, 0);
+		} else {
+			unsigned int len = 0, i = 0;
+			for (; len <= (unsigned int)pos; ++i)
+				len += b_exon_end(g, t, i) - b_exon_start(g, t, i) + 1;
+			c->coord = i - 1;
+			c->pos = b_exon_end(g, t, c->coord) - (len - pos) + 1;
+		}
+	} else {
+		/* chr_coord (src/hash_align.c:307-318) */
+		unsigned int sum = 0, i;
+		for (i = 0; i < g->n_chr; ++i) {
+			if (sum + g->chr_len[i] > t)
+				break;
+			sum += g->chr_len[i];
+		}
+		c->ref = i;
+		c->pos = t - sum;
+	}
+	unsigned int match = 0, k = 0;
+	for (uint32_t i = 0; i < s->n_cigar; ++i) {
+		const unsigned type = s->ops[i] & 15, cnt = s->ops[i] >> 4;
+		if (type == B_MATCH) {
+			unsigned int n = cnt;
+			++i;
+			while (i < s->n_cigar && (s->ops[i] & 15) != B_DIFF && (s->ops[i] & 15) != B_DELETE) {
+				if ((s->ops[i] & 15) == B_MATCH)
+					n += s->ops[i] >> 4;
+				++i;
+			}
+			--i;
+			match += n;
+			c->len += sprintf(c->md + c->len, "%u", n);
+		} else if (type == B_DIFF) {
+			c->md[c->len++] = s->miss[k++];
+			for (unsigned j = 1; j < cnt; ++j) {
+				c->md[c->len++] = '0';
+				c->md[c->len++] = s->miss[k++];
+			}
+			c->md[c->len] = 0;
+		} else if (type == B_DELETE) {
+			c->md[c->len++] = '^';
+			for (unsigned j = 0; j < cnt; ++j)
+				c->md[c->len++] = s->miss[k++];
+			c->md[c->len] = 0;
+		}
+		c->len = strlen(c->md);
+	}
+	unsigned int n = 0, l = c->pos;
+	for (uint32_t i = 0; i < s->n_cigar; ++i) {
+		unsigned int run = 0;
+		while (i < s->n_cigar && ((s->ops[i] & 15) == B_DIFF || (s->ops[i] & 15) == B_MATCH))
+			run += s->ops[i++] >> 4;
+		if (run > 0)
+			b_pad(g, c, &n, &l, t, run, B_MATCH, genome);
+		if (i < s->n_cigar)
+			b_pad(g, c, &n, &l, t, s->ops[i] >> 4, s->ops[i] & 15, genome);
+	}
+	c->n_cigar = n;
+	c->match = match;
+}
+
+/* pack_bam_core + compact_inf (:206-240, 265-283) */
+static void b_pack_core(const ho_gene_map *g, b_core *c, const b_cand *r, int p, const char *seq,
+			const char *qual, int rlen, const char *name, unsigned int name_len, uint32_t hit)
+{
+	const unsigned int genome = r->pair & 1;
+	const b_strand *s = &r->s[p];
+	memset(c, 0, offsetof(b_core, md));
+	c->md[0] = 0;
+	c->ref = c->pos = -1;
+	if (s->n > 0)
+		b_convert(g, c, s, hit, genome);
+	c->bin = b_reg2bin(c->pos, c->pos + c->match);
+	const unsigned int n = genome == 1 ? s->n : b_genes(g, s);
+	c->qual = b_qual(n);
+	unsigned int len = 36;
+	memcpy(c->data + len, name, name_len);
+	len += name_len;
+	memcpy(c->data + len, c->cig, 4 * c->n_cigar);
+	len += 4 * c->n_cigar;
+	int i;
+	for (i = 0, c->data[len] = 0; i < rlen; ++i) {
+		c->data[len] = (uint8_t)(c->data[len] << 4 | b_nt16((unsigned char)seq[i]));
+		if (i & 1)
+			c->data[++len] = 0;
+	}
+	if (i & 1) {
+		c->data[len] = (uint8_t)(c->data[len] << 4);
+		++len;
+	}
+	for (i = 0; i < rlen; ++i)
+		c->data[len + i] = (uint8_t)(qual[i] - 33);
+	len += rlen;
+	if (c->match > 0) {
+		const uint32_t nm = s->n_miss;
+		memcpy(c->data + len, "NMi", 3);
+		memcpy(c->data + len + 3, &nm, 4);
+		len += 7;
+		memcpy(c->data + len, "MDZ", 3);
+		memcpy(c->data + len + 3, c->md, c->len + 1);
+		len += 3 + c->len + 1;
+	}
+	memcpy(c->data + len, "ASi", 3);
+	memcpy(c->data + len + 3, &c->match, 4);
+	len += 7;
+	c->block_len = len;
+}
+
+typedef struct {
+	uint8_t *out;
+	uint64_t used, cap;
+	int full;
+} b_stream;
+
+/* pack_bam_block (:285-310) */
+static void b_block(b_stream *st, b_core *c, const b_core *mate, unsigned int name_len, int rlen,
+		    unsigned int flag, int size)
+{
+	int x[8];
+	x[0] = c->ref;
+	x[1] = c->pos;
+	x[2] = (unsigned int)c->bin << 16 | c->qual << 8 | name_len;
+	x[3] = flag << 16 | c->n_cigar;
+	x[4] = rlen;
+	x[5] = mate->ref;
+	x[6] = mate->pos;
+	x[7] = size;
+	const unsigned int blen = c->block_len - 4;
+	memcpy(c->data, &blen, 4);
+	memcpy(c->data + 4, x, 32);
+	if (st->used + c->block_len > st->cap) {
+		st->full = 1;
+		return;
+	}
+	memcpy(st->out + st->used, c->data, c->block_len);
+	st->used += c->block_len;
+}
+
+typedef struct {
+	char *seq, *qual, *name;
+	int len;
+} b_read;
+
+/* write_alignment_pair (:349-380): both mates' records of hit `hit` */
+static void b_write_alignment(const ho_gene_map *g, b_stream *st, b_read *a, b_read *b, const unsigned int *flag,
+			      const b_cand *r, uint32_t hit)
+{
+	static b_core c0, c1;
+	unsigned int name_len = strlen(a->name);
+	if (name_len > 2 && a->name[name_len - 2] == '/') {
+		a->name[name_len - 2] = 0;
+		--name_len;
+	} else {
+		++name_len;
+	}
+	b_pack_core(g, &c0, r, 0, a->seq, a->qual, a->len, a->name, name_len, hit);
+	/* the mate record takes name_len bytes of the mate's own name */
+	b_pack_core(g, &c1, r, 1, b->seq, b->qual, b->len, b->name, name_len, hit);
+	int size = 0;
+	if (c0.ref >= 0 && c0.ref == c1.ref) {
+		if (c0.pos < c1.pos)
+			size = c1.pos + b->len + c1.align_len - c0.pos;
+		else
+			size = c0.pos + a->len + c0.align_len - c1.pos;
+	}
+	b_block(st, &c0, &c1, name_len, a->len, flag[0], size);
+	b_block(st, &c1, &c0, name_len, b->len, flag[1], -size);
+}
+
+/* bam_write_pair (:382-416): the primary records, then one secondary pair
+ * per further hit that is not in the same gene as the one before it */
+static void b_write_pair(const ho_gene_map *g, b_stream *st, b_read *a, b_read *b, const b_cand *r,
+			 unsigned proper, unsigned first, unsigned rev, unsigned mrev)
+{
+	unsigned int flag[2];
+	flag[0] = b_flag(1, proper, r->s[0].n == 0, r->s[1].n == 0, rev, mrev, 1, 0);
+	flag[1] = b_flag(1, proper, r->s[1].n == 0, r->s[0].n == 0, mrev, rev, 0, 1);
+	b_write_alignment(g, st, a, b, flag, r, 0);
+	flag[0] |= 1 << 8;
+	flag[1] |= 1 << 8;
+	if (proper == 0 || r->s[0].n < 2)
+		return;
+	for (uint32_t i = 1; i < r->s[0].n; ++i) {
+		while (i < r->s[0].n && (r->pair & 1) == 0 && b_overlap_gene(g, r->s[0].pos[i], r->s[0].pos[i - 1]))
+			++i;
+		if (i == r->s[0].n)
+			break;
+		b_write_alignment(g, st, a, b, flag, r, i);
+	}
+}
+
+static void b_rev(b_read *x)   /* reverse_str + reverse_qual (:217-245) */
+{
+	o_reverse_str(x->seq, x->len);
+	for (int i = 0; i < (x->len >> 1); ++i) {
+		char t = x->qual[i];
+		x->qual[i] = x->qual[x->len - 1 - i];
+		x->qual[x->len - 1 - i] = t;
+	}
+}
+
+static b_cand b_from_rec(const ho_rec *rec, const uint32_t *pos_pool, const int32_t *p_pool,
+			 const uint32_t *op_pool, const char *miss_pool)
+{
+	b_cand c;
+	for (int s = 0; s < 2; ++s) {
+		c.s[s].n = (uint32_t)rec->n[s];
+		c.s[s].pos = pos_pool + rec->list_off[s];
+		c.s[s].p = p_pool + rec->list_off[s];
+		c.s[s].n_cigar = rec->n_cigar[s];
+		c.s[s].n_miss = rec->n_miss[s];
+		c.s[s].ops = op_pool + rec->cig_off[s];
+		c.s[s].miss = miss_pool + rec->miss_off[s];
+		c.err[s] = rec->err[s];
+	}
+	c.pair = rec->pair;
+	return c;
+}
+
+int ho_bam_pairs(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_pool,
+		 const int32_t *p_pool, const uint32_t *op_pool, const char *miss_pool, int n,
+		 char *seq1, const int64_t *off1, const int32_t *len1, char *qual1, char *name1,
+		 char *seq2, const int64_t *off2, const int32_t *len2, char *qual2, char *name2,
+		 int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off)
+{
+	b_stream st = {out, 0, cap, 0};
+	for (int i = 0; i < n; ++i) {
+		out_off[i] = st.used;
+		b_read x1 = {seq1 + off1[i], qual1 + off1[i], name1 + (int64_t)i * name_stride, len1[i]};
+		b_read x2 = {seq2 + off2[i], qual2 + off2[i], name2 + (int64_t)i * name_stride, len2[i]};
+		b_cand r0 = b_from_rec(&recs[2 * i], pos_pool, p_pool, op_pool, miss_pool);
+		b_cand r1 = b_from_rec(&recs[2 * i + 1], pos_pool, p_pool, op_pool, miss_pool);
+		const int s0 = r0.err[0] + r0.err[1], s1 = r1.err[0] + r1.err[1];
+		/* align_pair_read's branches (src/hash_align.c:1735-1804) */
+		if (s0 < s1)
+			r1.pair = -1;
+		else if (s0 > s1)
+			r0.pair = -1;
+		if (r0.pair > 1 && r1.pair > 1) {
+			b_rev(&x2);
+			b_write_pair(gm, &st, &x1, &x2, &r0, 1, 1, 0, 1);
+			b_rev(&x2);
+			b_rev(&x1);
+			b_write_pair(gm, &st, &x2, &x1, &r1, 1, 0, 0, 1);
+		} else if (r0.pair > 1) {
+			b_rev(&x2);
+			b_write_pair(gm, &st, &x1, &x2, &r0, 1, 1, 0, 1);
+		} else if (r1.pair > 1) {
+			b_rev(&x1);
+			b_write_pair(gm, &st, &x2, &x1, &r1, 1, 0, 0, 1);
+		} else if (r0.s[0].n > 0 && r0.s[1].n > 0 && s0 < s1) {
+			b_rev(&x2);
+			b_write_pair(gm, &st, &x1, &x2, &r0, 0, 1, 0, 1);
+		} else if (r1.s[0].n > 0 && r1.s[1].n > 0) {
+			b_rev(&x1);
+			b_write_pair(gm, &st, &x2, &x1, &r1, 0, 0, 0, 1);
+		} else if (r0.s[0].n > 0 && r1.s[0].n > 0 && (r0.pair & 1) == (r1.pair & 1)) {
+			b_swap(&r0, 1, &r1, 0);
+			r0.pair = -10;
+			b_write_pair(gm, &st, &x1, &x2, &r0, 0, 1, 0, 0);
+		} else if (r0.s[1].n > 0 && r1.s[1].n > 0 && (r0.pair & 1) == (r1.pair & 1)) {
+			b_rev(&x1);
+			b_rev(&x2);
+			b_swap(&r0, 0, &r1, 1);
+			r0.pair = -20;
+			b_write_pair(gm, &st, &x1, &x2, &r0, 0, 0, 1, 1);
+		} else if (r0.s[0].n > 0) {
+			b_write_pair(gm, &st, &x1, &x2, &r0, 0, 1, 0, 0);
+		} else if (r0.s[1].n > 0) {
+			b_rev(&x2);
+			b_write_pair(gm, &st, &x1, &x2, &r0, 0, 1, 0, 1);
+		} else if (r1.s[0].n > 0) {
+			b_write_pair(gm, &st, &x2, &x1, &r1, 0, 0, 0, 0);
+		} else {
+			b_rev(&x1);
+			b_write_pair(gm, &st, &x2, &x1, &r1, 0, 0, 0, 1);
+		}
+		if (st.full)
+			return -1;
+	}
+	out_off[n] = st.used;
+	return 0;
 }

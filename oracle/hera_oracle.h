@@ -166,6 +166,30 @@ void ho_em(uint32_t n_trans, const uint32_t *len, const uint32_t *tx_count, uint
 	   const double *count, const uint32_t *n, const uint64_t *ref_off, const uint32_t *ref,
 	   double *grama, double *overlap, uint32_t *rounds);
 
+/* BAM records as the host tail writes them with `-w` (WRITE_BAM = 0):
+ * align_pair_read's branches (src/hash_align.c:1735-1804) over bam_write_pair
+ * (src/bam_write.c:382-416), write_alignment_pair (:349-380), pack_bam_core,
+ * convert_cigar, add_padding, compact_inf and pack_bam_block (:89-310),
+ * with the transcript -> genome map of reference.inf (GENE_MAP, :22-57).
+ * Per pair, the uncompressed records it appends to the BGZF stream. */
+typedef struct {
+	uint32_t n_chr;
+	const uint32_t *chr_len;     /* [n_chr] */
+	const uint32_t *exon_off;    /* [n_trans + 1]: transcript t's exons are [exon_off[t], exon_off[t+1]) */
+	const uint32_t *starts, *ends;
+	const uint32_t *chr, *gene;  /* [n_trans] */
+} ho_gene_map;
+/* recs/pools: the pair records of ho_align_pairs with write_bam = 0.  Reads
+ * as the tail gets them (seq after the front half, qual, NUL-terminated
+ * names at name + i * name_stride); all three are modified in place as the
+ * tail modifies them.  out_off[i] .. out_off[i+1]: pair i's bytes.  Returns
+ * 0, or -1 if `cap` is too small. */
+int ho_bam_pairs(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_pool,
+		 const int32_t *p_pool, const uint32_t *op_pool, const char *miss_pool, int n,
+		 char *seq1, const int64_t *off1, const int32_t *len1, char *qual1, char *name1,
+		 char *seq2, const int64_t *off2, const int32_t *len2, char *qual2, char *name2,
+		 int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off);
+
 /* XXH32 (the published xxHash 32-bit algorithm) as add_class uses it. */
 uint32_t ho_xxh32(const void *buf, size_t len, uint32_t seed);
 

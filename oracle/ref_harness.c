@@ -510,3 +510,58 @@ int refh_em(uint32_t n_classes, const double *count, const uint32_t *n, const ui
 	CLASS = saved;
 	return 0;
 }
+
+/* ---- BAM records: the tail's bam_write_pair calls -----------------------
+ * refh_bam_setup loads an index directory written by hera_build + `hera
+ * index` with the reference's loader (load_index, src/hash_align.c:1195)
+ * and builds GENE_MAP from its reference.inf through init_bam_header
+ * (src/bam_write.c:448-495) with WRITE_BAM = 1, so nothing is written.
+ * refh_bam_pairs then runs align_pair_read (src/hash_align.c:1717-1812)
+ * with WRITE_BAM = 0 (`-w`) for each pair and copies out the uncompressed
+ * BAM records the tail appended to the stream (bam_write_pair,
+ * src/bam_write.c:382-416), pair by pair.  Names and qualities are
+ * modified in place (the writer trims "/1", the tail reverses qualities). */
+void init_bam_header(char *idx_dir, int argc, char *argv[]);
+void init_class();
+
+int refh_bam_setup(const char *dir)
+{
+	char *argv[] = {"hera", NULL};
+	WRITE_BAM = 1;
+	init_refInf();
+	init_hash();
+	load_index((char *)dir, NULL);
+	init_bam_header((char *)dir, 1, argv);
+	if (!CLASS)
+		init_class();
+	return REF_INF->n;
+}
+
+int refh_bam_pairs(int n, char *seq1, const int64_t *off1, const int32_t *len1, char *qual1, char *name1,
+		   char *seq2, const int64_t *off2, const int32_t *len2, char *qual2, char *name2,
+		   int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off)
+{
+	int i;
+	char *stream = malloc(MAX_COMPRESS + 1);
+	uint64_t used = 0;
+
+	WRITE_BAM = 0;
+	for (i = 0; i < n; ++i) {
+		unsigned int slen = 0;
+		struct read_inf a = {seq1 + off1[i], name1 + (int64_t)i * name_stride, qual1 + off1[i], len1[i]};
+		struct read_inf b = {seq2 + off2[i], name2 + (int64_t)i * name_stride, qual2 + off2[i], len2[i]};
+		out_off[i] = used;
+		align_pair_read(&a, &b, stream, &slen);
+		if (used + slen > cap) {
+			free(stream);
+			WRITE_BAM = 1;
+			return -1;
+		}
+		memcpy(out + used, stream, slen);
+		used += slen;
+	}
+	out_off[n] = used;
+	free(stream);
+	WRITE_BAM = 1;
+	return 0;
+}
