@@ -163,6 +163,11 @@ class _ClassTable(C.Structure):
                 ("paired", C.c_uint32), ("mean_frag_sum", C.c_double)]
 
 
+class _GeneMap(C.Structure):
+    _fields_ = [("n_chr", C.c_uint32), ("chr_len", C.c_void_p), ("exon_off", C.c_void_p), ("starts", C.c_void_p),
+                ("ends", C.c_void_p), ("chr", C.c_void_p), ("gene", C.c_void_p)]
+
+
 def load_library(path: str = LIB_PATH) -> C.CDLL:
     """Load libhera_b200.so (raises if it has not been built)."""
     global _lib
@@ -218,6 +223,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                                 C.c_int, C.c_void_p]
     lib.hera_gpu_classes_em.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32),
                                         C.POINTER(C.c_float)]
+    lib.hera_gpu_bam_create.argtypes = [C.c_void_p, C.POINTER(_GeneMap), C.POINTER(C.c_void_p)]
+    lib.hera_gpu_bam_destroy.argtypes = [C.c_void_p]
+    lib.hera_gpu_bam_last_error.restype = C.c_char_p
+    lib.hera_gpu_bam_last_error.argtypes = [C.c_void_p]
+    lib.hera_gpu_bam_pairs.argtypes = [C.c_void_p, C.POINTER(_Result), C.c_int32, C.POINTER(_Reads), C.POINTER(_Reads),
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                       C.c_uint64, C.c_void_p, C.POINTER(C.c_float)]
     lib.hera_gpu_classes_load.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
     lib.hera_gpu_classes_add_host.argtypes = [C.c_void_p, C.POINTER(_Result), C.c_int32, C.c_int]
     lib.hera_gpu_classes_fetch.argtypes = [C.c_void_p, C.POINTER(_ClassTable)]
@@ -725,6 +737,53 @@ class Classes:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hera_gpu_classes_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BamWriter:
+    """The tail's BAM records (`-w`) on the device: hera_gpu_bam_pairs.
+    `gene_map`: any object with chr_len, exon_off, starts, ends, chr and
+    gene arrays (hera's GENE_MAP)."""
+
+    def __init__(self, ctx: "Context", gene_map):
+        self.lib = ctx.lib
+        self._gm = [np.ascontiguousarray(getattr(gene_map, k), np.uint32)
+                    for k in ("chr_len", "exon_off", "starts", "ends", "chr", "gene")]
+        g = _GeneMap(len(self._gm[0]), *[_ptr(a) for a in self._gm])
+        h = C.c_void_p()
+        ctx._check(self.lib.hera_gpu_bam_create(ctx.h, C.byref(g), C.byref(h)))
+        self.h = h
+
+    def pairs(self, res: "Result", r1, r2, qual1: np.ndarray, qual2: np.ndarray, names1: np.ndarray,
+              names2: np.ndarray, cap: int = 0):
+        """(bytes, per-pair offsets, device ms) of the records of r1.n pairs;
+        names: (n, stride) uint8 arrays, NUL-terminated rows."""
+        n = r1.n
+        a, b = Context._reads(r1), Context._reads(r2)
+        cap = cap or int(r1.len.sum() + r2.len.sum()) * 8 + 4096 * n + 4096
+        out = np.zeros(cap, np.uint8)
+        off = np.zeros(n + 1, np.uint64)
+        ms = C.c_float()
+        args = (self.h, C.byref(res.c), n, C.byref(a), C.byref(b), _ptr(qual1), _ptr(qual2), _ptr(names1),
+                _ptr(names2), names1.shape[1])
+        rc = self.lib.hera_gpu_bam_pairs(*args, _ptr(out), cap, _ptr(off), C.byref(ms))
+        if rc == HERA_GPU_ECAPACITY and int(off[-1]) > cap:
+            cap = int(off[-1])
+            out = np.zeros(cap, np.uint8)
+            rc = self.lib.hera_gpu_bam_pairs(*args, _ptr(out), cap, _ptr(off), C.byref(ms))
+        if rc != HERA_GPU_OK:
+            raise HeraGpuError(rc, self.lib.hera_gpu_bam_last_error(self.h).decode())
+        return out[:int(off[-1])], off, ms.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.hera_gpu_bam_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -2594,3 +2594,4 @@ extern "C" int hera_gpu_dpx_peak(int device, float ms, double *instr_per_s)
 #include "hera_server.cuh"
 #include "hera_fastq.cuh"
 #include "hera_classes.cuh"
+#include "hera_bam.cuh"

@@ -549,6 +549,49 @@ int hera_gpu_classes_load(hera_gpu_classes *c, const hera_gpu_class_table *in);
 int hera_gpu_classes_em(hera_gpu_classes *c, hera_gpu_ctx *ctx, double *grama, double *overlap,
 			uint32_t *rounds, float *em_ms);
 
+/* ---- BAM records ------------------------------------------------------------
+ * With `-w` hera's tail writes each pair's alignment records
+ * (align_pair_read's branches, src/hash_align.c:1735-1804, over
+ * bam_write_pair, src/bam_write.c:382-416) into the stream it then BGZF-
+ * compresses.  hera_gpu_bam_pairs produces those uncompressed bytes for a
+ * batch of pairs on the device, identical to hera's; compression stays with
+ * the caller (bam_write). */
+
+/* GENE_MAP (src/bam_write.c:22-57): chromosome lengths, each transcript's
+ * exons [exon_off[t], exon_off[t+1]) of starts/ends (genome coordinates),
+ * and its chromosome and gene.  Host memory; copied at creation. */
+typedef struct hera_gpu_gene_map {
+	uint32_t n_chr;
+	const uint32_t *chr_len;     /* [n_chr] */
+	const uint32_t *exon_off;    /* [n_trans + 1] */
+	const uint32_t *starts;      /* [exon_off[n_trans]] */
+	const uint32_t *ends;
+	const uint32_t *chr;         /* [n_trans] */
+	const uint32_t *gene;        /* [n_trans] */
+} hera_gpu_gene_map;
+
+typedef struct hera_gpu_bam hera_gpu_bam;
+
+/* A BAM record writer for ctx's index with this gene map. */
+int hera_gpu_bam_create(hera_gpu_ctx *ctx, const hera_gpu_gene_map *gm, hera_gpu_bam **out);
+void hera_gpu_bam_destroy(hera_gpu_bam *b);
+const char *hera_gpu_bam_last_error(const hera_gpu_bam *b);
+
+/* The records hera's tail writes for n pairs (host memory throughout):
+ * `res` as hera_gpu_align_pairs_flat left it with write_bam = 0; r1/r2 the
+ * pairs' sequences and qual1/qual2 their qualities at the same offsets;
+ * name1/name2 the NUL-terminated names, pair i's at i * name_stride (a NUL
+ * inside each slot).  The inputs are not modified (hera's tail reverses
+ * reads and cuts "/1" off names while it writes; the records show that).
+ * Pair i's bytes are out[out_off[i] .. out_off[i+1]); out_off has n + 1
+ * entries.  With `cap` too small: HERA_GPU_ECAPACITY, out_off[n] = the
+ * bytes needed.  *kernel_ms (may be NULL): device time of the call. */
+int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n,
+		       const hera_gpu_reads *r1, const hera_gpu_reads *r2,
+		       const char *qual1, const char *qual2, const char *name1,
+		       const char *name2, int32_t name_stride, uint8_t *out, uint64_t cap,
+		       uint64_t *out_off, float *kernel_ms);
+
 /* Device time (CUDA events, from the first kernel of the last add call to
  * its end; the call's first-use allocations are not in it) and the
  * kernels it launched. */

@@ -1,8 +1,9 @@
-"""BAM records of the host tail (`-w`), restated in the oracle: the records
-align_pair_read appends per pair (bam_write_pair, src/bam_write.c:382-416),
-from the `-w` Candidate records and GENE_MAP, against the reference's own
-bytes.  The device form of this step is not built yet; these tests pin the
-checker it will be held to."""
+"""BAM records of the host tail (`-w`): the records align_pair_read appends
+per pair (bam_write_pair, src/bam_write.c:382-416), from the `-w` Candidate
+records and GENE_MAP.  The oracle's restatement against the reference's own
+bytes (golden and live), and the device writer's code
+(hera_b200/csrc/hera_bam_core.h) compiled for the host against the golden
+bytes; tests/test_tail_classes.py runs the writer on the GPU."""
 import json
 import multiprocessing as mp
 import os
@@ -111,3 +112,54 @@ def test_bam_records_match_reference(tmp_path, wl):
     assert p.exitcode == 0
     rc, nbytes, bad = q.get(timeout=10)
     assert rc == 0 and nbytes > 0 and bad == 0
+
+
+@pytest.fixture(scope="module")
+def host_writer(tmp_path_factory):
+    """tests/bam_host_check.cpp (the device writer's code on the host)."""
+    import ctypes as C
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    so = str(tmp_path_factory.mktemp("bamw") / "bam_host_check.so")
+    here = os.path.dirname(os.path.abspath(__file__))
+    subprocess.run([gxx, "-O2", "-std=c++17", "-shared", "-fPIC", os.path.join(here, "bam_host_check.cpp"),
+                    "-o", so], check=True)
+    return C.CDLL(so)
+
+
+def host_records(lib, gm, res, r1, r2, cap=1 << 26):
+    import ctypes as C
+    n = r1.n
+    q = [np.full(r1.seq.shape[0] + 1, ord("?"), np.uint8), np.full(r2.seq.shape[0] + 1, ord("?"), np.uint8)]
+    names = [oracle.read_names(n, 1), oracle.read_names(n, 2)]
+    out = np.zeros(cap, np.uint8)
+    off = np.zeros(n + 1, np.uint64)
+    err = C.c_uint32()
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (gm.chr_len, gm.exon_off, gm.starts, gm.ends, gm.chr, gm.gene)]
+    lib.bam_host_pairs(C.c_uint32(len(arrs[0])), *[p(a) for a in arrs], p(res.recs), p(res.pos_pool), p(res.p_pool),
+                       p(res.op_pool), p(res.miss_pool), n, p(r1.seq), p(r1.off), p(r1.len), p(q[0]), p(names[0]),
+                       p(r2.seq), p(r2.off), p(r2.len), p(q[1]), p(names[1]), C.c_int32(names[0].shape[1]),
+                       p(out), p(off), C.byref(err))
+    return out[:int(off[-1])].copy(), off, err.value
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_device_writer_code_on_host_golden(small, host_writer, name):
+    """The writer the kernels run, compiled for the host, gives the
+    reference's bytes for every golden pair; the inputs stay unmodified."""
+    ix, orc = small
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    n = int(d[f"{name}_n"][0])
+    r1 = synth.ReadSet(c[f"{name}_r1_seq"], c[f"{name}_r1_off"], c[f"{name}_r1_len"]).subset(np.arange(n))
+    r2 = synth.ReadSet(c[f"{name}_r2_seq"], c[f"{name}_r2_off"], c[f"{name}_r2_len"]).subset(np.arange(n))
+    res = orc.align_pairs(r1, r2, 0)
+    before = (r1.seq.copy(), r2.seq.copy())
+    got, off, err = host_records(host_writer, _GM(d), res, r1, r2)
+    assert err == 0
+    assert np.array_equal(before[0], r1.seq) and np.array_equal(before[1], r2.seq)
+    want, woff = d[f"{name}_bam"], d[f"{name}_bam_off"]
+    bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
+    assert not bad, f"{name}: {len(bad)} pairs' records differ, first {bad[0]}"
