@@ -65,9 +65,10 @@ def test_bam_records_golden(small, name):
 LIVE_ANNOTATION = dict(seed=8, genome_len=400_000, n_genes=40, n_transcripts=90, n_chrom=2)
 
 
-def _live(d, wl, n, q):
+def _live(d, wl, n, q, host_so=None, lower=False):
     """Child process: the reference loads its own index directory (its
-    globals would otherwise outlive this test)."""
+    globals would otherwise outlive this test).  With host_so, the device
+    writer's code compiled for the host is held to the same bytes."""
     import ctypes as C
     ann = synth.make_annotation(**LIVE_ANNOTATION)
     tx = synth.transcriptome(ann)
@@ -76,6 +77,10 @@ def _live(d, wl, n, q):
     lib.refh_bam_setup(os.path.join(d, "idx").encode())
     gm = oracle.GeneMap(os.path.join(d, "idx", "reference.inf"), ix.n_trans)
     r1, r2 = workloads.pairs(wl, ann, tx, n, seed=77)
+    if lower:   # lower-case bases, which the front half upper-cases
+        for rs in (r1, r2):
+            m = np.isin(rs.seq, np.frombuffer(b"ACGT", np.uint8)) & (np.arange(rs.seq.shape[0]) % 3 == 0)
+            rs.seq[m] += 32
     a1, a2 = r1.copy(), r2.copy()
     qa = [np.full(a1.seq.shape[0] + 1, ord("?"), np.uint8), np.full(a2.seq.shape[0] + 1, ord("?"), np.uint8)]
     names = [oracle.read_names(n, 1), oracle.read_names(n, 2)]   # alive through the call
@@ -83,17 +88,26 @@ def _live(d, wl, n, q):
     off = np.zeros(n + 1, np.uint64)
     rc = lib.refh_bam_pairs(n, *oracle._bam_args(a1, a2, qa, names), C.c_void_p(buf.ctypes.data),
                             C.c_uint64(buf.size), C.c_void_p(off.ctypes.data))
-    got, goff = _records(oracle.Oracle(ix), gm, r1.copy(), r2.copy())
+    orc = oracle.Oracle(ix)
+    got, goff = _records(orc, gm, r1.copy(), r2.copy())
     bad = [i for i in range(n) if got[goff[i]:goff[i + 1]].tobytes() != buf[off[i]:off[i + 1]].tobytes()]
-    q.put((rc, int(off[-1]), len(bad)))
+    bad_host = 0
+    if host_so:
+        h1, h2 = r1.copy(), r2.copy()
+        res = orc.align_pairs(h1.copy(), h2.copy(), 0)   # the writer gets the caller's reads as they were
+        hb, hoff, herr = host_records(C.CDLL(host_so), gm, res, h1, h2)
+        bad_host = herr + sum(1 for i in range(n) if hb[hoff[i]:hoff[i + 1]].tobytes() != buf[off[i]:off[i + 1]].tobytes())
+    q.put((rc, int(off[-1]), len(bad), bad_host))
 
 
 @pytest.mark.skipif(not oracle.reference_available() or not os.path.exists("/root/reference/src/hera_build"),
                     reason="reference not built here")
-@pytest.mark.parametrize("wl", ["config1", "config4"])
-def test_bam_records_match_reference(tmp_path, wl):
+@pytest.mark.parametrize("wl,lower", [("config1", False), ("config4", False), ("config4", True)])
+def test_bam_records_match_reference(tmp_path, host_writer, wl, lower):
     """Two chromosomes, the config-1 and config-4 read models (the latter
-    with unmapped and rescued mates): every pair's records byte for byte."""
+    with unmapped and rescued mates), and lower-case bases: every pair's
+    records byte for byte, from the oracle and from the device writer's code
+    compiled for the host."""
     ann = synth.make_annotation(**LIVE_ANNOTATION)
     d = str(tmp_path)
     synth.write_genome_fasta(ann, os.path.join(d, "g.fa"))
@@ -104,14 +118,14 @@ def test_bam_records_match_reference(tmp_path, wl):
                     os.path.join(d, "g.gtf"), "--outdir", os.path.join(d, "idx")], check=True, capture_output=True)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    p = ctx.Process(target=_live, args=(d, wl, 2000, q))
+    p = ctx.Process(target=_live, args=(d, wl, 2000, q, host_writer._name, lower))
     p.start()
     p.join(timeout=240)
     if p.exitcode is None:
         p.kill()
     assert p.exitcode == 0
-    rc, nbytes, bad = q.get(timeout=10)
-    assert rc == 0 and nbytes > 0 and bad == 0
+    rc, nbytes, bad, bad_host = q.get(timeout=10)
+    assert rc == 0 and nbytes > 0 and bad == 0 and bad_host == 0
 
 
 @pytest.fixture(scope="module")
