@@ -8,7 +8,10 @@
  * read the Candidate after its two get_position calls
  * (src/hash_align.c:1819-1823).  The host tail of align_pair_read
  * (src/hash_align.c:1735-1811: pair choice, BAM records, add_class,
- * counters) and everything around it stay hera's own C code.
+ * counters) and everything around it stay hera's own C code -- or, where a
+ * caller wants them on the GPU as well, the entry points at the end of this
+ * file produce the same bytes: FASTQ chunk parsing, the class table
+ * (add_class), the EM over it (estimate_count) and the `-w` BAM records.
  *
  * Plain C types and pointers only.  Every entry point returns 0 on success
  * or a negative HERA_GPU_E* code; hera_gpu_last_error() describes the last
