@@ -133,3 +133,31 @@ def test_gloo_two_ranks_class_tables():
         _, (r1, r2) = _chunk_classes(orc, ann, tx, cid)
         results.append(orc.align_pairs(r1, r2, 1))
     assert got == orc.classes(results).key()
+
+
+def test_class_table_merge_edges():
+    """Chunks without classes, repeated ids keeping the first list, and
+    PAIRED wrapping like hera's unsigned int."""
+    import numpy as np
+    from hera_b200.api import ClassTable
+
+    def table(ids, counts, lists, tx, paired, frag):
+        ns = np.array([len(x) for x in lists], np.uint32)
+        off = np.zeros(len(ns), np.uint64)
+        off[1:] = np.cumsum(ns[:-1])
+        ref = np.concatenate([np.array(x, np.uint32) for x in lists]) if lists else np.zeros(0, np.uint32)
+        return ClassTable(np.array(ids, np.uint32), np.array(counts, np.float64), ns, off, ref,
+                          np.array(tx, np.uint32), paired, frag)
+
+    a = table([7, 3], [2, 1], [[1, 2], [0, 3]], [1, 0, 0, 0], 0xFFFFFFFF, 10.0)
+    empty = table([], [], [], [0, 2, 0, 0], 3, 4.0)
+    b = table([9, 7], [5, 4], [[2, 3], [0, 1, 2]], [0, 0, 1, 0], 2, 1.0)
+    m = shard.merge_class_tables([a, empty, b])
+    assert m.ids.tolist() == [7, 3, 9]
+    assert m.counts.tolist() == [6.0, 1.0, 5.0]
+    assert m.lists() == [(1, 2), (0, 3), (2, 3)]   # id 7 keeps its first list
+    assert m.tx_count.tolist() == [1, 2, 1, 0]
+    assert m.paired == (0xFFFFFFFF + 3 + 2) & 0xFFFFFFFF
+    assert m.mean_frag == 15.0
+    with pytest.raises(ValueError):
+        shard.merge_class_tables([])
