@@ -154,6 +154,41 @@ def transcriptome(ann: Annotation) -> Transcriptome:
     return Transcriptome(names, seq, length, np.cumsum(length, dtype=np.uint64).astype(np.uint32))
 
 
+@dataclasses.dataclass
+class GeneMap:
+    """hera's GENE_MAP for an annotation, as hera_build writes it to
+    reference.inf and contruct_gene_map reads it (src/bam_write.c:22-57):
+    chromosome lengths; per transcript (transcriptome order) its exons as
+    0-based inclusive [start, end] genome coordinates sorted by start, its
+    chromosome and its gene (numbered in the same order)."""
+    chr_len: np.ndarray
+    exon_off: np.ndarray
+    starts: np.ndarray
+    ends: np.ndarray
+    chr: np.ndarray
+    gene: np.ndarray
+
+
+def gene_map(ann: Annotation) -> GeneMap:
+    starts, ends, off, chrs, genes = [], [], [0], [], []
+    g_idx = 0
+    for c in sorted(range(len(ann.chrom_names))):
+        for g in ann.genes:
+            if g.chrom != c:
+                continue
+            for iso in g.isoforms:
+                ex = sorted(g.exons[k] for k in iso)
+                starts += [a for a, _ in ex]
+                ends += [b - 1 for _, b in ex]
+                off.append(off[-1] + len(ex))
+                chrs.append(c)
+                genes.append(g_idx)
+            g_idx += 1
+    return GeneMap(np.array([x.shape[0] for x in ann.chroms], np.uint32), np.array(off, np.uint32),
+                   np.array(starts, np.uint32), np.array(ends, np.uint32), np.array(chrs, np.uint32),
+                   np.array(genes, np.uint32))
+
+
 def random_transcriptome(seed: int, n: int, mean_len: float = 1800.0, sigma: float = 0.5,
                          gc: float = 0.41, min_len: int = 200) -> Transcriptome:
     """Transcripts drawn directly (no genome): log-normal lengths with the

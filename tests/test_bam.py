@@ -97,7 +97,10 @@ def _live(d, wl, n, q, host_so=None, lower=False):
         res = orc.align_pairs(h1.copy(), h2.copy(), 0)   # the writer gets the caller's reads as they were
         hb, hoff, herr = host_records(C.CDLL(host_so), gm, res, h1, h2)
         bad_host = herr + sum(1 for i in range(n) if hb[hoff[i]:hoff[i + 1]].tobytes() != buf[off[i]:off[i + 1]].tobytes())
-    q.put((rc, int(off[-1]), len(bad), bad_host))
+    sg = synth.gene_map(ann)
+    gm_same = all(np.array_equal(getattr(sg, k), getattr(gm, k))
+                  for k in ("chr_len", "exon_off", "starts", "ends", "chr", "gene"))
+    q.put((rc, int(off[-1]), len(bad), bad_host, gm_same))
 
 
 @pytest.mark.skipif(not oracle.reference_available() or not os.path.exists("/root/reference/src/hera_build"),
@@ -124,8 +127,8 @@ def test_bam_records_match_reference(tmp_path, host_writer, wl, lower):
     if p.exitcode is None:
         p.kill()
     assert p.exitcode == 0
-    rc, nbytes, bad, bad_host = q.get(timeout=10)
-    assert rc == 0 and nbytes > 0 and bad == 0 and bad_host == 0
+    rc, nbytes, bad, bad_host, gm_same = q.get(timeout=10)
+    assert rc == 0 and nbytes > 0 and bad == 0 and bad_host == 0 and gm_same
 
 
 @pytest.fixture(scope="module")
@@ -177,3 +180,16 @@ def test_device_writer_code_on_host_golden(small, host_writer, name):
     want, woff = d[f"{name}_bam"], d[f"{name}_bam_off"]
     bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
     assert not bad, f"{name}: {len(bad)} pairs' records differ, first {bad[0]}"
+
+
+def test_gene_map_from_annotation_matches_hera_build():
+    """synth.gene_map gives the GENE_MAP hera_build's reference.inf holds
+    (the golden copy was read from the file hera_build wrote)."""
+    meta = json.load(open(os.path.join(GOLD, "golden.json")))
+    p = dict(meta["index"])
+    for k in ("exons", "intron"):
+        p[k] = tuple(p[k])
+    gm = synth.gene_map(synth.make_annotation(**p))
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    for k in ("chr_len", "exon_off", "starts", "ends", "chr", "gene"):
+        assert np.array_equal(getattr(gm, k), d[f"gm_{k}"]), k
