@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-fastq", action="store_true", help="skip the FASTQ-chunk leg")
     ap.add_argument("--fastq-only", action="store_true",
                     help="time only the FASTQ-chunk leg (one JSON line with the leg's numbers)")
+    ap.add_argument("--bam-only", action="store_true",
+                    help="time only the BAM-record leg (the -w tail's records on the device; one JSON line)")
     ap.add_argument("--pin-tuning", default="", help="BUILD_BLOCKS_PER_SM,RESCUE_WARPS_PER_BLOCK: "
                     "fixed launch shapes instead of the autotuner (reproducible profiles)")
     ap.add_argument("--serve-scale", type=float, default=0.125,
@@ -240,6 +242,11 @@ def main():
     if args.fastq_only:
         r1, r2 = workloads.pairs(args.workload, ann, tx, args.chunk, seed=100 + 1000 * rank)
         print(json.dumps({"fastq": fastq_bench(args, ix, (r1, r2), local),
+                          "config": {"workload": args.workload, "pairs_per_step": args.chunk}}), flush=True)
+        return
+    if args.bam_only:
+        r1, r2 = workloads.pairs(args.workload, ann, tx, args.chunk, seed=100 + 1000 * rank)
+        print(json.dumps({"bam": bam_bench(args, ix, ann, (r1, r2), local),
                           "config": {"workload": args.workload, "pairs_per_step": args.chunk}}), flush=True)
         return
     chunks = make_chunks(args.workload, ann, tx, args.chunk, args.distinct, 100 + 1000 * rank)
@@ -482,6 +489,61 @@ def _hbm_peak():
     except OSError:
         peaks = {}
     return float(peaks.get("hbm_gbs", 6650.0)), "measured" if "hbm_gbs" in peaks else "fallback"
+
+
+def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
+    """The -w tail's BAM records for one chunk of pairs: aligned with
+    traceback through the flat C ABI, then written by hera_gpu_bam_pairs
+    (host buffers in and out; the reported device time covers the input
+    copies and both writer passes).  The oracle's restatement on one host
+    thread over a sample is the CPU baseline of this leg."""
+    from hera_b200 import api, synth
+    r1, r2 = chunk
+    n = r1.n
+    q1 = np.full(r1.seq.shape[0] + 1, ord("?"), np.uint8)
+    q2 = np.full(r2.seq.shape[0] + 1, ord("?"), np.uint8)
+    names = []
+    for mate in (1, 2):
+        a = np.zeros((n, 16), np.uint8)
+        digits = np.char.zfill(np.arange(n).astype(str), 7)
+        rows = np.char.add(np.char.add("r", digits), f"/{mate}")
+        raw = np.frombuffer("".join(rows).encode(), np.uint8).reshape(n, -1)
+        a[:, :raw.shape[1]] = raw
+        names.append(a)
+    gm = synth.gene_map(ann)
+    ctx = api.Context(ix, device=local)
+    try:
+        res = ctx.align_pairs(r1, r2, 0)
+        w = api.BamWriter(ctx, gm)
+        try:
+            w.pairs(res, r1, r2, q1, q2, names[0], names[1])   # warm
+            t0 = time.perf_counter()
+            out, off, ms = w.pairs(res, r1, r2, q1, q2, names[0], names[1])
+            wall = time.perf_counter() - t0
+        finally:
+            w.close()
+    finally:
+        ctx.close()
+    leg = {"pairs": n, "record_bytes": int(off[-1]), "device_ms": round(ms, 3),
+           "pairs_per_s_device": n / (ms / 1e3), "pairs_per_s_call": n / wall,
+           "record_gbs_device": int(off[-1]) / (ms / 1e3) / 1e9}
+    try:
+        import oracle   # the CPU baseline of this leg: the writer restated in C
+        k = min(cpu_sample, n)
+        idx = np.arange(k)
+        a1, a2 = r1.subset(idx), r2.subset(idx)
+        orc = oracle.Oracle(ix)
+        ores = orc.align_pairs(a1, a2, 0)
+        c1 = np.full(a1.seq.shape[0] + 1, ord("?"), np.uint8)
+        c2 = np.full(a2.seq.shape[0] + 1, ord("?"), np.uint8)
+        t0 = time.perf_counter()
+        ob, ooff = oracle.bam_pairs(gm, ores, a1, a2, [c1, c2], [names[0][:k].copy(), names[1][:k].copy()])
+        cpu_s = time.perf_counter() - t0
+        leg["cpu_port"] = {"pairs_per_s": k / cpu_s, "cores": 1, "sample": f"first {k} pairs",
+                           "bytes_equal": bool(ob.tobytes() == out[:int(off[k])].tobytes())}
+    except Exception as e:
+        leg["cpu_port"] = {"error": str(e)}
+    return leg
 
 
 def fastq_bench(args, ix, chunk, local):

@@ -181,11 +181,22 @@ class GeneMap:
         self.gene = u32(o + 4 * n_trans, n_trans).copy()
 
     def c_struct(self):
-        class _GM(C.Structure):
-            _fields_ = [("n_chr", C.c_uint32), ("chr_len", C.c_void_p), ("exon_off", C.c_void_p),
-                        ("starts", C.c_void_p), ("ends", C.c_void_p), ("chr", C.c_void_p), ("gene", C.c_void_p)]
-        return _GM(len(self.chr_len), _ptr(self.chr_len), _ptr(self.exon_off), _ptr(self.starts),
-                   _ptr(self.ends), _ptr(self.chr), _ptr(self.gene))
+        return _gene_map_struct(self)
+
+
+class _GMStruct(C.Structure):
+    _fields_ = [("n_chr", C.c_uint32), ("chr_len", C.c_void_p), ("exon_off", C.c_void_p),
+                ("starts", C.c_void_p), ("ends", C.c_void_p), ("chr", C.c_void_p), ("gene", C.c_void_p)]
+
+
+def _gene_map_struct(gm):
+    """ho_gene_map over any object with chr_len, exon_off, starts, ends, chr
+    and gene arrays (the arrays are kept alive on the struct)."""
+    keep = [np.ascontiguousarray(getattr(gm, k), np.uint32)
+            for k in ("chr_len", "exon_off", "starts", "ends", "chr", "gene")]
+    g = _GMStruct(len(keep[0]), *[_ptr(a) for a in keep])
+    g._keep = keep
+    return g
 
 
 def read_names(n: int, mate: int, stride: int = 16) -> np.ndarray:
@@ -212,7 +223,7 @@ def bam_pairs(gm: GeneMap, res: "Result", r1, r2, quals, names, cap: int = 1 << 
     n = r1.n
     out = np.zeros(cap, np.uint8)
     off = np.zeros(n + 1, np.uint64)
-    g = gm.c_struct()
+    g = _gene_map_struct(gm)
     rc = lib.ho_bam_pairs(C.byref(g), C.c_void_p(_ptr(res.recs)), C.c_void_p(_ptr(res.pos_pool)),
                           C.c_void_p(_ptr(res.p_pool)), C.c_void_p(_ptr(res.op_pool)), C.c_void_p(_ptr(res.miss_pool)),
                           n, *_bam_args(r1, r2, quals, names), C.c_void_p(_ptr(out)), C.c_uint64(cap),
