@@ -28,7 +28,7 @@ from hera_b200 import synth  # noqa: E402
 import oracle  # noqa: E402
 from make_golden import small_index  # noqa: E402
 
-SETS = {"pairs100": 1200, "pairs150div": 600, "pairs_mixed": 600, "pairs_n": 600}
+SETS = {"pairs100": 1200, "pairs150div": 600, "pairs_mixed": 600, "pairs_n": 600, "pairs_long": 300}
 
 
 def main():

@@ -17,7 +17,7 @@ import oracle
 from hera_b200 import index, synth, workloads
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SETS = ["pairs100", "pairs150div", "pairs_mixed", "pairs_n"]
+SETS = ["pairs100", "pairs150div", "pairs_mixed", "pairs_n", "pairs_long"]
 
 
 @pytest.fixture(scope="module")
