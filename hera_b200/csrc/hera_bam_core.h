@@ -377,8 +377,8 @@ BAM_HD inline void emit(Sink &o, const Core &c, const Core &mate, const Read &rd
 	o.u32((uint32_t)size);
 	for (unsigned int j = 0; j < name_len; ++j)
 		o.put((uint8_t)rd.name_byte((int)j));
-	for (int j = 0; j < c.n_cigar; ++j)
-		o.u32(c.cig[j]);
+	for (int j = 0; j < c.n_cigar; ++j)   // past MAX_CIG the call fails (E_CIG); the bytes only keep the count
+		o.u32(j < MAX_CIG ? c.cig[j] : 0u);
 	for (int j = 0; j < rd.len; j += 2) {
 		const uint8_t hi = nt16((unsigned char)rd.base(j));
 		const uint8_t lo = j + 1 < rd.len ? nt16((unsigned char)rd.base(j + 1)) : 0;
@@ -390,8 +390,8 @@ BAM_HD inline void emit(Sink &o, const Core &c, const Core &mate, const Read &rd
 		o.put('N'); o.put('M'); o.put('i');
 		o.u32(n_miss);
 		o.put('M'); o.put('D'); o.put('Z');
-		for (unsigned int j = 0; j < c.md_len; ++j)
-			o.put((uint8_t)c.md[j]);
+		for (unsigned int j = 0; j < c.md_len; ++j)   // likewise past MAX_MD (E_MD)
+			o.put(j < (unsigned)MAX_MD ? (uint8_t)c.md[j] : (uint8_t)0);
 		o.put(0);
 	}
 	o.put('A'); o.put('S'); o.put('i');
