@@ -503,6 +503,57 @@ BAM_HD inline void tail(Ctx &x, Sink &o, Core *cc, Cand r0, Cand r1, Read x1, Re
 	}
 }
 
+// write_alignment_single (src/bam_write.c:312-347): one record, no mate
+BAM_HD inline void write_alignment_single(Ctx &x, Sink &o, Core *cc, Read &a, unsigned int flag, const Cand &r,
+					  int p, uint32_t hit)
+{
+	unsigned int name_len = (unsigned int)a.name_l;
+	if (name_len > 2 && a.name_byte((int)name_len - 2) == '/') {
+		if (a.cut >= 0)
+			x.err |= E_NAME;
+		a.cut = (int)name_len - 2;
+		a.name_l = (int)name_len - 2;
+		--name_len;
+	} else {
+		++name_len;
+	}
+	core(x, cc[0], r, p, hit);
+	cc[1].ref = cc[1].pos = -1;
+	emit(o, cc[0], cc[1], a, name_len, flag, 0, r.s[p].n_miss);
+}
+
+// bam_write_single (src/bam_write.c:418-446)
+BAM_HD inline void write_single(Ctx &x, Sink &o, Core *cc, Read &a, const Cand &r, unsigned rev, int p)
+{
+	unsigned int flag = make_flag(0, 0, r.s[p].n == 0, 1, rev, 0, 1, 0);
+	write_alignment_single(x, o, cc, a, flag, r, p, 0);
+	flag |= 1 << 8;
+	if (r.s[p].n < 2)
+		return;
+	for (uint32_t i = 1; i < r.s[p].n; ++i) {
+		while (i < r.s[p].n && overlap_gene(x.g, r.s[p].pos[i], r.s[p].pos[i - 1]))
+			++i;
+		if (i == r.s[p].n)
+			break;
+		write_alignment_single(x, o, cc, a, flag, r, p, i);
+	}
+}
+
+// align_single_read's writes (src/hash_align.c:1825-1834) for one read.
+BAM_HD inline void tail_single(Ctx &x, Sink &o, Core *cc, const Cand &r, Read a)
+{
+	if (r.s[0].n == 0 && r.s[1].n == 0) {
+		write_single(x, o, cc, a, r, 0, 0);
+		return;
+	}
+	if (r.s[0].n > 0) {
+		write_single(x, o, cc, a, r, 0, 0);
+	} else {
+		a.rev = !a.rev;
+		write_single(x, o, cc, a, r, 1, 1);
+	}
+}
+
 // Candidate view of a flat record (hera_cand_rec layout).
 template <typename Rec>
 BAM_HD inline Cand cand(const Rec &rec, const uint32_t *pos, const int32_t *pp, const uint32_t *ops, const char *miss)

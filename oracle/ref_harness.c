@@ -565,3 +565,32 @@ int refh_bam_pairs(int n, char *seq1, const int64_t *off1, const int32_t *len1, 
 	WRITE_BAM = 1;
 	return 0;
 }
+
+/* The same for single reads: align_single_read (src/hash_align.c:1814-1853)
+ * with WRITE_BAM = 0, the records bam_write_single appends, read by read. */
+int refh_bam_single(int n, char *seq, const int64_t *off, const int32_t *len, char *qual, char *name,
+		    int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off)
+{
+	int i;
+	char *stream = malloc(MAX_COMPRESS + 1);
+	uint64_t used = 0;
+
+	WRITE_BAM = 0;
+	for (i = 0; i < n; ++i) {
+		unsigned int slen = 0;
+		struct read_inf a = {seq + off[i], name + (int64_t)i * name_stride, qual + off[i], len[i]};
+		out_off[i] = used;
+		align_single_read(&a, stream, &slen);
+		if (used + slen > cap) {
+			free(stream);
+			WRITE_BAM = 1;
+			return -1;
+		}
+		memcpy(out + used, stream, slen);
+		used += slen;
+	}
+	out_off[n] = used;
+	free(stream);
+	WRITE_BAM = 1;
+	return 0;
+}

@@ -46,3 +46,29 @@ extern "C" int bam_host_pairs(uint32_t n_chr, const uint32_t *chr_len, const uin
 	out_off[n] = at;
 	return 0;
 }
+
+extern "C" int bam_host_single(uint32_t n_chr, const uint32_t *chr_len, const uint32_t *exon_off,
+			       const uint32_t *starts, const uint32_t *ends, const uint32_t *chr, const uint32_t *gene,
+			       const Rec *recs, const uint32_t *pos, const int32_t *pp, const uint32_t *ops,
+			       const char *miss, int n, const char *seq, const int64_t *off, const int32_t *len,
+			       const char *qual, const char *name, int32_t stride, uint8_t *out, uint64_t *out_off,
+			       uint32_t *err)
+{
+	uint32_t qt[bamw::QUAL_TABLE];
+	bamw::qual_table_host(qt);
+	bamw::GeneMap g{n_chr, chr_len, exon_off, starts, ends, chr, gene};
+	uint64_t at = 0;
+	*err = 0;
+	for (int i = 0; i < n; ++i) {
+		bamw::Ctx x{g, qt, 0};
+		bamw::Sink o{out, at};
+		bamw::Read a{seq + off[i], qual + off[i], name + (int64_t)i * stride, len[i], false, 0, -1};
+		a.name_l = bamw::name_length(a.name, stride);
+		out_off[i] = at;
+		bamw::tail_single(x, o, cc, bamw::cand(recs[i], pos, pp, ops, miss), a);
+		at = o.at;
+		*err |= x.err;
+	}
+	out_off[n] = at;
+	return 0;
+}

@@ -9,7 +9,9 @@ reference.inf they write.  The reference's whole per-pair worker,
 align_pair_read (src/hash_align.c:1717-1812), then runs with `-w`
 (WRITE_BAM = 0) over the golden read sets of candidates.npz, and the
 uncompressed BAM records it appends per pair (bam_write_pair,
-src/bam_write.c:382-416) are stored with the gene map they were made with.
+src/bam_write.c:382-416) are stored with the gene map they were made with;
+likewise align_single_read's records (bam_write_single, :418-446) for the
+golden single reads.
 """
 import ctypes as C
 import os
@@ -65,6 +67,21 @@ def main():
         out[f"{name}_bam_off"] = off
         out[f"{name}_n"] = np.array([n])
         print(name, n, "pairs,", int(off[-1]), "bytes of records")
+    # single reads: align_single_read with `-w` (src/hash_align.c:1814-1853)
+    n = 800
+    rs = synth.ReadSet(c["single_seq"], c["single_off"], c["single_len"]).subset(np.arange(n))
+    q = np.full(rs.seq.shape[0] + 1, ord("?"), np.uint8)
+    nm = oracle.read_names(n, 1)
+    buf = np.zeros(1 << 26, np.uint8)
+    off = np.zeros(n + 1, np.uint64)
+    a = rs.copy()
+    rc = lib.refh_bam_single(n, C.c_void_p(a.seq.ctypes.data), C.c_void_p(a.off.ctypes.data),
+                             C.c_void_p(a.len.ctypes.data), C.c_void_p(q.ctypes.data), C.c_void_p(nm.ctypes.data),
+                             C.c_int32(nm.shape[1]), C.c_void_p(buf.ctypes.data), C.c_uint64(buf.size),
+                             C.c_void_p(off.ctypes.data))
+    assert rc == 0
+    out["single_bam"], out["single_bam_off"], out["single_n"] = buf[:int(off[-1])].copy(), off, np.array([n])
+    print("single", n, "reads,", int(off[-1]), "bytes of records")
     np.savez_compressed(os.path.join(HERE, "bam.npz"), **out)
 
 

@@ -193,3 +193,35 @@ def test_gene_map_from_annotation_matches_hera_build():
     d = np.load(os.path.join(GOLD, "bam.npz"))
     for k in ("chr_len", "exon_off", "starts", "ends", "chr", "gene"):
         assert np.array_equal(getattr(gm, k), d[f"gm_{k}"]), k
+
+
+def host_records_single(lib, gm, res, rs, cap=1 << 25):
+    import ctypes as C
+    n = rs.n
+    q = np.full(rs.seq.shape[0] + 1, ord("?"), np.uint8)
+    names = oracle.read_names(n, 1)
+    out = np.zeros(cap, np.uint8)
+    off = np.zeros(n + 1, np.uint64)
+    err = C.c_uint32()
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (gm.chr_len, gm.exon_off, gm.starts, gm.ends, gm.chr, gm.gene)]
+    lib.bam_host_single(C.c_uint32(len(arrs[0])), *[p(a) for a in arrs], p(res.recs), p(res.pos_pool),
+                        p(res.p_pool), p(res.op_pool), p(res.miss_pool), n, p(rs.seq), p(rs.off), p(rs.len), p(q),
+                        p(names), C.c_int32(names.shape[1]), p(out), p(off), C.byref(err))
+    return out[:int(off[-1])].copy(), off, err.value
+
+
+def test_device_writer_code_on_host_single_golden(small, host_writer):
+    """Single reads: align_single_read's records (bam_write_single), the
+    device writer's code built for the host against the reference's bytes."""
+    ix, orc = small
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    n = int(d["single_n"][0])
+    rs = synth.ReadSet(c["single_seq"], c["single_off"], c["single_len"]).subset(np.arange(n))
+    res = orc.align_single(rs.copy(), 0)
+    got, off, err = host_records_single(host_writer, _GM(d), res, rs)
+    assert err == 0
+    want, woff = d["single_bam"], d["single_bam_off"]
+    bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
+    assert not bad, f"{len(bad)} reads' records differ, first {bad[0]}"
