@@ -233,6 +233,24 @@ def bam_pairs(gm: GeneMap, res: "Result", r1, r2, quals, names, cap: int = 1 << 
     return out[:int(off[-1])].copy(), off
 
 
+def bam_single(gm, res: "Result", rs, qual, names, cap: int = 1 << 25):
+    """ho_bam_single: the records align_single_read writes with `-w`, per
+    read, from the oracle's `-w` single-read records."""
+    lib = C.CDLL(ORACLE_SO)
+    n = rs.n
+    out = np.zeros(cap, np.uint8)
+    off = np.zeros(n + 1, np.uint64)
+    g = _gene_map_struct(gm)
+    rc = lib.ho_bam_single(C.byref(g), C.c_void_p(_ptr(res.recs)), C.c_void_p(_ptr(res.pos_pool)),
+                           C.c_void_p(_ptr(res.p_pool)), C.c_void_p(_ptr(res.op_pool)),
+                           C.c_void_p(_ptr(res.miss_pool)), n, C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)),
+                           C.c_void_p(_ptr(rs.len)), C.c_void_p(_ptr(qual)), C.c_void_p(_ptr(names)),
+                           C.c_int32(names.shape[1]), C.c_void_p(_ptr(out)), C.c_uint64(cap), C.c_void_p(_ptr(off)))
+    if rc != 0:
+        raise RuntimeError("BAM output buffer too small")
+    return out[:int(off[-1])].copy(), off
+
+
 def _export_classes(sizes, export, n_trans: int) -> ClassTable:
     nc, rn = C.c_uint32(), C.c_uint64()
     sizes(C.byref(nc), C.byref(rn))

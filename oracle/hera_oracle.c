@@ -2147,3 +2147,63 @@ int ho_bam_pairs(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_
 	out_off[n] = st.used;
 	return 0;
 }
+
+/* write_alignment_single (src/bam_write.c:314-347) */
+static void b_write_alignment_single(const ho_gene_map *g, b_stream *st, b_read *a, unsigned int flag,
+				     const b_cand *r, int p, uint32_t hit)
+{
+	static b_core c0, c1;
+	unsigned int name_len = strlen(a->name);
+	if (name_len > 2 && a->name[name_len - 2] == '/') {
+		a->name[name_len - 2] = 0;
+		--name_len;
+	} else {
+		++name_len;
+	}
+	b_pack_core(g, &c0, r, p, a->seq, a->qual, a->len, a->name, name_len, hit);
+	c1.ref = c1.pos = -1;
+	b_block(st, &c0, &c1, name_len, a->len, flag, 0);
+}
+
+/* bam_write_single (src/bam_write.c:418-446) */
+static void b_write_single(const ho_gene_map *g, b_stream *st, b_read *a, const b_cand *r, unsigned rev, int p)
+{
+	unsigned int flag = b_flag(0, 0, r->s[p].n == 0, 1, rev, 0, 1, 0);
+	b_write_alignment_single(g, st, a, flag, r, p, 0);
+	flag |= 1 << 8;
+	if (r->s[p].n < 2)
+		return;
+	for (uint32_t i = 1; i < r->s[p].n; ++i) {
+		while (i < r->s[p].n && b_overlap_gene(g, r->s[p].pos[i], r->s[p].pos[i - 1]))
+			++i;
+		if (i == r->s[p].n)
+			break;
+		b_write_alignment_single(g, st, a, flag, r, p, i);
+	}
+}
+
+int ho_bam_single(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_pool,
+		  const int32_t *p_pool, const uint32_t *op_pool, const char *miss_pool, int n,
+		  char *seq, const int64_t *off, const int32_t *len, char *qual, char *name,
+		  int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off)
+{
+	b_stream st = {out, 0, cap, 0};
+	for (int i = 0; i < n; ++i) {
+		out_off[i] = st.used;
+		b_read x = {seq + off[i], qual + off[i], name + (int64_t)i * name_stride, len[i]};
+		b_cand r = b_from_rec(&recs[i], pos_pool, p_pool, op_pool, miss_pool);
+		/* align_single_read (src/hash_align.c:1825-1834) */
+		if (r.s[0].n == 0 && r.s[1].n == 0) {
+			b_write_single(gm, &st, &x, &r, 0, 0);
+		} else if (r.s[0].n > 0) {
+			b_write_single(gm, &st, &x, &r, 0, 0);
+		} else {
+			b_rev(&x);
+			b_write_single(gm, &st, &x, &r, 1, 1);
+		}
+		if (st.full)
+			return -1;
+	}
+	out_off[n] = st.used;
+	return 0;
+}

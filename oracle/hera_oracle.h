@@ -190,6 +190,14 @@ int ho_bam_pairs(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_
 		 char *seq2, const int64_t *off2, const int32_t *len2, char *qual2, char *name2,
 		 int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off);
 
+/* The same for single reads: align_single_read's writes (src/hash_align.c:
+ * 1825-1834) over bam_write_single (src/bam_write.c:418-446); recs from
+ * ho_align_single with write_bam = 0. */
+int ho_bam_single(const ho_gene_map *gm, const ho_rec *recs, const uint32_t *pos_pool,
+		  const int32_t *p_pool, const uint32_t *op_pool, const char *miss_pool, int n,
+		  char *seq, const int64_t *off, const int32_t *len, char *qual, char *name,
+		  int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off);
+
 /* XXH32 (the published xxHash 32-bit algorithm) as add_class uses it. */
 uint32_t ho_xxh32(const void *buf, size_t len, uint32_t seed);
 

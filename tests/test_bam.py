@@ -225,3 +225,19 @@ def test_device_writer_code_on_host_single_golden(small, host_writer):
     want, woff = d["single_bam"], d["single_bam_off"]
     bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
     assert not bad, f"{len(bad)} reads' records differ, first {bad[0]}"
+
+
+def test_bam_single_records_golden(small):
+    """The oracle's restatement of the single-read writes against the
+    reference's golden bytes."""
+    ix, orc = small
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    n = int(d["single_n"][0])
+    rs = synth.ReadSet(c["single_seq"], c["single_off"], c["single_len"]).subset(np.arange(n))
+    res = orc.align_single(rs, 0)
+    q = np.full(rs.seq.shape[0] + 1, ord("?"), np.uint8)
+    got, off = oracle.bam_single(_GM(d), res, rs, q, oracle.read_names(n, 1))
+    want, woff = d["single_bam"], d["single_bam_off"]
+    bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
+    assert not bad, f"{len(bad)} reads' records differ, first {bad[0]}"
