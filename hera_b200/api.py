@@ -147,7 +147,7 @@ class Timing(C.Structure):
         ("dp_jobs", C.c_uint64), ("dp_calls", C.c_uint64)] + [
         (k, C.c_float) for k in ("seed_kernel_ms", "dp_kernel_ms", "rescue_kernel_ms",
                                  "host_stage_ms", "host_out_ms")] + [
-        (k, C.c_uint64) for k in ("probes", "seed_hits", "sw_cells", "ssw_cells")]
+        (k, C.c_uint64) for k in ("probes", "seed_hits", "sw_cells", "ssw_cells", "wide_items")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -197,7 +197,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     lib.hera_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
     lib.hera_gpu_unit_ssw.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.POINTER(C.c_int32)]
+                                      C.c_int32, C.POINTER(C.c_int32)]
+    lib.hera_gpu_unit_sw.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_int32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
     lib.hera_gpu_host_unregister.argtypes = [C.c_void_p]
     lib.hera_gpu_server_create.argtypes = [C.c_void_p, C.POINTER(_ServerOptions), C.POINTER(C.c_void_p)]
     lib.hera_gpu_server_submit.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_Reads), C.POINTER(_Reads),
@@ -265,8 +268,9 @@ def host_unregister(a: np.ndarray) -> None:
     lib.hera_gpu_host_unregister(C.c_void_p(a.ctypes.data))
 
 
-def unit_ssw(refs, reads, device: int = 0):
-    """ssw_align as the mate-rescue kernel computes it, for lists of ASCII
+def unit_ssw(refs, reads, device: int = 0, cap: int = 1344):
+    """ssw_align as the mate-rescue kernel computes it (the wide pass's form
+    for CIGARs past the first pass's capacities), for lists of ASCII
     (window, read) pairs: [(score, skip, cigar, miss)] (a kernel-level check
     against the reference's golden vectors)."""
     lib = load_library()
@@ -278,19 +282,49 @@ def unit_ssw(refs, reads, device: int = 0):
     qoff = np.zeros(n + 1, np.int64)
     qoff[1:] = np.cumsum([len(q) for q in reads])
     score, skip = np.zeros(n, np.int32), np.zeros(n, np.int32)
-    ops = np.zeros(n * 96, np.uint32)
-    miss = np.zeros(n * 96, np.uint8)
+    ops = np.zeros(n * cap, np.uint32)
+    miss = np.zeros(n * cap, np.uint8)
     n_ops, n_miss = np.zeros(n, np.int32), np.zeros(n, np.int32)
     flags = C.c_int32(0)
     rc = lib.hera_gpu_unit_ssw(device, _ptr(rcat), _ptr(roff), _ptr(qcat), _ptr(qoff), n, _ptr(score), _ptr(skip),
-                               _ptr(ops), _ptr(n_ops), _ptr(miss), _ptr(n_miss), C.byref(flags))
+                               _ptr(ops), _ptr(n_ops), _ptr(miss), _ptr(n_miss), cap, C.byref(flags))
     if rc != HERA_GPU_OK:
         raise HeraGpuError(rc, "unit ssw failed")
     out = []
     for i in range(n):
-        o = ops[i * 96:i * 96 + min(int(n_ops[i]), 96)]
+        o = ops[i * cap:i * cap + min(int(n_ops[i]), cap)]
         cig = "".join(f"{int(x) >> 4}{CIGAR_CHARS[int(x) & 15]}" for x in o)
-        out.append((int(score[i]), int(skip[i]), cig, bytes(miss[i * 96:i * 96 + min(int(n_miss[i]), 96)])))
+        out.append((int(score[i]), int(skip[i]), cig, bytes(miss[i * cap:i * cap + min(int(n_miss[i]), cap)])))
+    return out, flags.value
+
+
+def unit_sw(refs, qs, errs, write_bam: int, device: int = 0, cap: int = 64):
+    """SW_align as the batched form's gap-DP kernels compute it, for lists
+    of ASCII windows, queries and error caps: [(score, cigar, miss)] (a
+    kernel-level check against the reference's golden vectors)."""
+    lib = load_library()
+    n = len(refs)
+    rcat = np.frombuffer(b"".join(refs), np.uint8).copy()
+    qcat = np.frombuffer(b"".join(qs), np.uint8).copy()
+    roff = np.zeros(n + 1, np.int64)
+    roff[1:] = np.cumsum([len(r) for r in refs])
+    qoff = np.zeros(n + 1, np.int64)
+    qoff[1:] = np.cumsum([len(q) for q in qs])
+    err = np.asarray(errs, np.int32)
+    score = np.zeros(n, np.int32)
+    ops = np.zeros(n * cap, np.uint32)
+    miss = np.zeros(n * cap, np.uint8)
+    n_ops, n_miss = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    flags = C.c_int32(0)
+    rc = lib.hera_gpu_unit_sw(device, _ptr(rcat), _ptr(roff), _ptr(qcat), _ptr(qoff), _ptr(err), n, write_bam,
+                              _ptr(score), _ptr(ops), _ptr(n_ops), _ptr(miss), _ptr(n_miss), cap, C.byref(flags))
+    if rc != HERA_GPU_OK:
+        raise HeraGpuError(rc, "unit sw failed")
+    out = []
+    for i in range(n):
+        o = ops[i * cap:i * cap + min(int(n_ops[i]), cap)]
+        cig = "".join(f"{int(x) >> 4}{CIGAR_CHARS[int(x) & 15]}" for x in o)
+        out.append((int(score[i]), cig, bytes(miss[i * cap:i * cap + min(int(n_miss[i]), cap)])))
     return out, flags.value
 
 

@@ -61,7 +61,9 @@ struct DpJob {
 
 struct DpResHdr {
 	int16_t score, sub;
-	uint8_t n, nm, pad[2];
+	uint8_t n, nm;
+	uint8_t caps;             // 1: the CIGAR passed a capacity (the job's pairs go to the wide pass)
+	uint8_t pad;
 };
 
 __host__ __device__ constexpr int res_stride(int cap)
@@ -168,6 +170,7 @@ __global__ void k_task_list(Batch b, int ntask, const uint2 *__restrict__ hits, 
 	if ((t & 3) == 0) {
 		P.stage = 0;
 		P.rm_ret = 0;
+		P.ovf = 0;
 	}
 	tinfo[t].chain0 = 0;
 	tinfo[t].nch = -1;
@@ -333,6 +336,7 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 		cur ^= 1;
 	}
 	if (na == 0) {
+		pair_flags(b, pi, flags);
 		flag(b.flags, flags);
 		return;
 	}
@@ -426,6 +430,7 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 	const int st = atomicAdd(R.cnt + 2, ns);
 	if (at + nch > R.chain_cap || jt + nj > R.job_cap || st + ns > R.slot_cap) {
 		R.tinfo[t].nch = -2;
+		pair_flags(b, pi, flags);
 		flag(b.flags, flags);
 		return;
 	}
@@ -443,6 +448,7 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 		ch.js0 += st;
 		R.chains[at + q] = ch;
 	}
+	pair_flags(b, pi, flags);
 	flag(b.flags, flags);
 }
 
@@ -556,7 +562,8 @@ __device__ inline void store_res(const DCig &cig, int score, uint8_t *o, int rca
 	h.sub = (int16_t)sub;
 	h.n = (uint8_t)(cig.n < rcap ? cig.n : rcap);
 	h.nm = (uint8_t)(cig.nm < rcap ? cig.nm : rcap);
-	h.pad[0] = h.pad[1] = 0;
+	h.caps = (flags & F_CAPS) ? 1 : 0;
+	h.pad = 0;
 	*reinterpret_cast<DpResHdr *>(o) = h;
 	uint32_t *ops = reinterpret_cast<uint32_t *>(o + sizeof(DpResHdr));
 	for (int k = 0; k < h.n; ++k)
@@ -606,7 +613,7 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 		const int score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig,
 							reinterpret_cast<uint8_t *>(rows), flags, cells);
 		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-		flag(b.flags, flags);
+		flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
 }
@@ -630,14 +637,16 @@ __global__ void __launch_bounds__(128) k_dp_generic(Batch b, const DpJob *__rest
 					 flags, &cells);
 		}
 		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-		flag(b.flags, flags);
+		flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
 }
 
-__device__ inline void load_res_cig(const uint8_t *o, int rcap, DCig &c)
+__device__ inline void load_res_cig(const uint8_t *o, int rcap, DCig &c, int &flags)
 {
 	const DpResHdr h = *reinterpret_cast<const DpResHdr *>(o);
+	if (h.caps)
+		flags |= F_CCAP;
 	const uint32_t *ops = reinterpret_cast<const uint32_t *>(o + sizeof(DpResHdr));
 	const uint8_t *miss = o + sizeof(DpResHdr) + 4 * rcap;
 	c.n = h.n;
@@ -687,6 +696,8 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 			bool ok = true;
 			if (ch.has_prefix) {
 				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)R.slots[j].job * stride);
+				if (h.caps)
+					flags |= F_CCAP;
 				err += h.score;
 				if (err > L / 2 || (uint32_t)err > max)
 					ok = false;
@@ -695,6 +706,8 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 			}
 			for (; ok && j < ch.js0 + ch.njs; ++j) {
 				const DpResHdr h = *reinterpret_cast<const DpResHdr *>(R.res + (size_t)R.slots[j].job * stride);
+				if (h.caps)
+					flags |= F_CCAP;
 				err += h.score;
 				if (err > L / 2 || (uint32_t)err > max + 1)
 					ok = false;
@@ -718,6 +731,7 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 	if (n1 == 0) {   // miss exit (src/hash_align.c:1461-1466)
 		S.n = 0;
 		S.err = L;
+		pair_flags(b, pi, flags);
 		flag(b.flags, flags);
 		return;
 	}
@@ -730,16 +744,17 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 	int j = ch.js0;
 	cig.n = cig.nm = 0;
 	if (ch.has_prefix) {
-		load_res_cig(R.res + (size_t)R.slots[j].job * stride, R.rcap, cig);
+		load_res_cig(R.res + (size_t)R.slots[j].job * stride, R.rcap, cig, flags);
 		++j;
 	}
 	for (; j < ch.js0 + ch.njs; ++j) {
 		const JobSlot js = R.slots[j];
 		cig_add(cig, OP_M, js.mrun, nullptr, flags);
-		load_res_cig(R.res + (size_t)js.job * stride, R.rcap, tmp);
+		load_res_cig(R.res + (size_t)js.job * stride, R.rcap, tmp, flags);
 		cig_concat(cig, tmp, flags);
 	}
 	cig_copy(S.cig, cig);
+	pair_flags(b, pi, flags);
 	flag(b.flags, flags);
 }
 

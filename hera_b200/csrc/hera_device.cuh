@@ -19,18 +19,40 @@ constexpr uint64_t HMASK = (1ull << HBITS) - 1;
 constexpr int MAX_READ = 320;          // HERA_GPU_MAX_READ
 constexpr int MAX_DP_ROWS = MAX_READ;  // rows of one gap DP (<= read length)
 constexpr int BW = 24;                 // gap-DP band width (bound: 2*error+2 = 18)
-constexpr int ACAP = 256;              // anchors of one get_position call
-constexpr int LCAP = 64;               // hits kept per Candidate strand
-constexpr int CCAP = 96;               // CIGAR ops per Candidate strand
-constexpr int MCAP = 96;               // miss chars per Candidate strand
+// Per-read capacities.  The reference grows every list without bound; the
+// device keeps fixed-size per-task state, in two sizes.  The first pass
+// (every pair) uses CapsStd.  A pair that passes one of its capacities is
+// flagged and aligned again, alone, in a second pass with CapsWide, whose
+// CIGAR and miss bounds hold for any read up to MAX_READ (a traceback takes
+// at most read + window steps, 320 + 1000) and whose anchor and list bounds
+// are 32x the first pass's.
+struct CapsStd {
+	static constexpr int A = 256;     // anchors of one get_position call
+	static constexpr int L = 64;      // hits kept per Candidate strand
+	static constexpr int C = 96;      // CIGAR ops per Candidate strand
+	static constexpr int M = 96;      // miss chars per Candidate strand
+};
+struct CapsWide {
+	static constexpr int A = 8192;
+	static constexpr int L = 8192;
+	static constexpr int C = 1344;
+	static constexpr int M = 1344;
+};
+constexpr int ACAP = CapsStd::A;
+constexpr int LCAP = CapsStd::L;
+constexpr int CCAP = CapsStd::C;
+constexpr int MCAP = CapsStd::M;
 
 enum : int { OP_M = 0, OP_I = 1, OP_D = 2, OP_S = 4, OP_X = 8 };
 
 // capacity / consistency flags (OR-ed into one word per batch)
 enum : int {
 	F_ACAP = 1, F_LCAP = 2, F_CCAP = 4, F_MCAP = 8, F_BAND = 16, F_READ = 32,
-	F_SCRATCH = 64, F_QUEUE = 128, F_SSW = 256
+	F_SCRATCH = 64, F_QUEUE = 128, F_SSW = 256,
+	F_WIDE = 512    // (host) a capacity was met again in the wide pass
 };
+// the flags a second, wide pass clears (per-read list capacities)
+constexpr int F_CAPS = F_ACAP | F_LCAP | F_CCAP | F_MCAP;
 
 struct DevIndex {
 	const uint32_t *boff;    // [2^27 + 1] bucket start offsets
@@ -58,18 +80,23 @@ __device__ __forceinline__ uint8_t comp_code(uint8_t c)
 // ---------------------------------------------------------------------
 // CIGAR algebra
 // ---------------------------------------------------------------------
-struct DCig {
+template <class K>
+struct DCigT {
+	static constexpr int CC = K::C, MC = K::M;
 	int n, nm;
-	uint32_t op[CCAP];       // (count << 4) | op
-	uint8_t miss[MCAP];
+	uint32_t op[K::C];       // (count << 4) | op
+	uint8_t miss[K::M];
 };
+using DCig = DCigT<CapsStd>;
 
 __device__ __forceinline__ int op_type(uint32_t o) { return (int)(o & 15u); }
 __device__ __forceinline__ unsigned op_cnt(uint32_t o) { return o >> 4; }
 
 // add_cigar (src/hash_align.c:526-565)
-__device__ inline void cig_add(DCig &c, int type, unsigned add, const uint8_t *mc, int &flags)
+template <class Cig>
+__device__ inline void cig_add(Cig &c, int type, unsigned add, const uint8_t *mc, int &flags)
 {
+	constexpr int MCAP = Cig::MC, CCAP = Cig::CC;
 	add &= 0xffffu;
 	if (add == 0)
 		return;
@@ -99,7 +126,8 @@ __device__ inline void cig_add(DCig &c, int type, unsigned add, const uint8_t *m
 }
 
 // reverse_cigar (src/hash_align.c:567-587)
-__device__ inline void cig_reverse(DCig &c)
+template <class Cig>
+__device__ inline void cig_reverse(Cig &c)
 {
 	for (int i = 0; i < c.n / 2; ++i) {
 		uint32_t t = c.op[i];
@@ -114,7 +142,8 @@ __device__ inline void cig_reverse(DCig &c)
 }
 
 // concat_cigar (src/hash_align.c:589-603)
-__device__ inline void cig_concat(DCig &d, DCig &t, int &flags)
+template <class Cig>
+__device__ inline void cig_concat(Cig &d, Cig &t, int &flags)
 {
 	cig_reverse(t);
 	int k = 0;
@@ -130,7 +159,8 @@ __device__ inline void cig_concat(DCig &d, DCig &t, int &flags)
 	}
 }
 
-__device__ inline void cig_copy(DCig &d, const DCig &s)
+template <class Cig>
+__device__ inline void cig_copy(Cig &d, const Cig &s)
 {
 	d.n = s.n;
 	d.nm = s.nm;
@@ -181,9 +211,10 @@ struct RefWin {
 };
 
 // q: query codes (already oriented), qlen; qrev: read q backwards (prefix DP)
+template <class Cig>
 __device__ inline int sw_align(const DevIndex &ix, uint32_t rstart, const uint8_t *q,
 			       uint32_t ref_len, uint32_t len, int err, bool score_only,
-			       DCig &cig, SwWork &w, int &flags, uint32_t *cells = nullptr)
+			       Cig &cig, SwWork &w, int &flags, uint32_t *cells = nullptr)
 {
 	cig.n = 0;
 	cig.nm = 0;
@@ -365,9 +396,9 @@ struct QView {   // query codes: q(x) = p[x * step]
 	__device__ __forceinline__ uint8_t operator()(int x) const { return p[x * step]; }
 };
 
-template <int E, bool STORE>
+template <int E, bool STORE, class Cig>
 __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
-				   bool score_only, DCig &cig, uint8_t *__restrict__ rows, int &flags,
+				   bool score_only, Cig &cig, uint8_t *__restrict__ rows, int &flags,
 				   uint32_t &cells)
 {
 	constexpr int W = 2 * E + 2;
@@ -567,8 +598,9 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 // register footprint small where neighbouring threads diverge.  The batched
 // path runs sw_align_reg on length-sorted jobs instead.  q: oriented read
 // codes of the gap.
+template <class Cig>
 __device__ inline int gap_dp(const DevIndex &ix, uint32_t rstart, const uint8_t *q, int qstep,
-			     uint32_t ref_len, uint32_t len, int err, bool score_only, DCig &cig,
+			     uint32_t ref_len, uint32_t len, int err, bool score_only, Cig &cig,
 			     SwWork &w, int &flags)
 {
 	cig.n = 0;
@@ -677,45 +709,55 @@ __device__ __forceinline__ uint64_t kmer_at(const uint8_t *rd, int i)
 // ---------------------------------------------------------------------
 // Per-pair Candidate state in HBM
 // ---------------------------------------------------------------------
-struct DSlot {              // one strand of a Candidate (src/hash_align.h:90-97)
+template <class K>
+struct DSlotT {             // one strand of a Candidate (src/hash_align.h:90-97)
+	static constexpr int LC = K::L;
 	int32_t n, err;
-	uint32_t t[LCAP];       // transcript ids   (Candidate.pos)
-	int32_t p[LCAP];        // positions        (Candidate.p)
-	DCig cig;
+	uint32_t t[K::L];       // transcript ids   (Candidate.pos)
+	int32_t p[K::L];        // positions        (Candidate.p)
+	DCigT<K> cig;
 };
+using DSlot = DSlotT<CapsStd>;
 
-struct DPair {
-	DSlot s[2][2];          // [candidate r[0]/r[1]][strand]
+template <class K>
+struct DPairT {
+	DSlotT<K> s[2][2];      // [candidate r[0]/r[1]][strand]
 	int32_t pair[2];
 	int32_t stage;
 	int32_t rm_ret;
 	int32_t rm_i;
-	int32_t pad;
+	int32_t ovf;            // F_CAPS flags met by this pair (first pass)
 };
+using DPair = DPairT<CapsStd>;
 
 // Anchors of one get_position call: pos2[0..2] of the reference, one
 // 12-byte record per anchor so a call's few anchors share cache lines.
 struct Anc {
 	uint32_t t, tp, off;    // transcript, transcript position, read offset
 };
-struct Anchors {
-	Anc a[ACAP];
+template <class K>
+struct AnchorsT {
+	Anc a[K::A];
 };
 
-struct GpWork {
-	Anchors a[2];
-	DCig c1, c2;
+template <class K>
+struct GpWorkT {
+	AnchorsT<K> a[2];
+	DCigT<K> c1, c2;
 	SwWork sw;
 	uint8_t rd[MAX_READ];
 };
+using GpWork = GpWorkT<CapsStd>;
 
 // merge_sort (src/hash_align.c:257-297): new hit list (all at read offset
 // idx) merged into the anchors by transcript; on an equal transcript the
 // existing anchor goes first when the unsigned wrapped diagonal difference
 // is < 2*ERR, else the smaller tpos.
-__device__ inline int merge_hits(const Anchors &A, int na, Anchors &B, const uint2 *occ,
+template <class K>
+__device__ inline int merge_hits(const AnchorsT<K> &A, int na, AnchorsT<K> &B, const uint2 *occ,
 				 uint32_t nh, uint32_t idx, int &flags)
 {
+	constexpr int ACAP = K::A;
 	if (na + (int)nh > ACAP) {
 		flags |= F_ACAP;
 		nh = (uint32_t)(ACAP - na);
@@ -757,9 +799,10 @@ __device__ inline int merge_hits(const Anchors &A, int na, Anchors &B, const uin
 }
 
 // get_SWalign (src/hash_align.c:1242-1320)
-__device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rlen, Anchors &A,
+template <class K>
+__device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rlen, AnchorsT<K> &A,
 				   uint32_t id, uint32_t n, uint32_t &store, uint32_t &max,
-				   DSlot &S, bool score_only, GpWork &w, int &flags)
+				   DSlotT<K> &S, bool score_only, GpWorkT<K> &w, int &flags)
 {
 	if (n > 1 && A.a[id + n - 1].tp - A.a[id].tp > (uint32_t)rlen)
 		return;
@@ -770,8 +813,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 	uint32_t add = start < ERR ? (uint32_t)start : (uint32_t)ERR;
 	const uint32_t ref_start = __ldg(ix.tstart + tr) + (uint32_t)start;
 	int err = 0, sub = 0, score;
-	DCig &cig = w.c1;
-	DCig &tmp = w.c2;
+	DCigT<K> &cig = w.c1;
+	DCigT<K> &tmp = w.c2;
 	cig.n = cig.nm = 0;
 	if (A.a[id].off > 0) {
 		const uint32_t o0 = A.a[id].off;
@@ -813,7 +856,8 @@ __device__ inline void get_swalign(const DevIndex &ix, const uint8_t *rd, int rl
 	++store;
 }
 
-__device__ __forceinline__ bool chain_next(const Anchors &A, int na, uint32_t i, uint32_t n,
+template <class K>
+__device__ __forceinline__ bool chain_next(const AnchorsT<K> &A, int na, uint32_t i, uint32_t n,
 					   int rlen, bool stop_consumed)
 {
 	if (i + 1 >= (uint32_t)na)
@@ -832,12 +876,14 @@ __device__ __forceinline__ bool chain_next(const Anchors &A, int na, uint32_t i,
 // get_position (src/hash_align.c:1322-1467).  `rd` holds the read already
 // in the strand's orientation (reverse complement for str 1).  Seed hits
 // come from `pre` (one {start, count} per seed) when given, else are probed.
-__device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int rlen, DPair &P,
+template <class K>
+__device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int rlen, DPairT<K> &P,
 				    int c, int str, int space, const uint2 *pre, bool score_only,
-				    GpWork &w, int &flags)
+				    GpWorkT<K> &w, int &flags)
 {
-	DSlot &S = P.s[c][str];
-	const DSlot &Mt = P.s[c][1 - str];
+	constexpr int ACAP = K::A, LCAP = K::L;
+	DSlotT<K> &S = P.s[c][str];
+	const DSlotT<K> &Mt = P.s[c][1 - str];
 	int cur = 0, na = 0;
 	const uint32_t step = (uint32_t)(space < 0 ? -space : space);
 
@@ -853,7 +899,7 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 				flags |= F_ACAP;
 				nh = ACAP;
 			}
-			Anchors &A = w.a[cur];
+			AnchorsT<K> &A = w.a[cur];
 			for (uint32_t k = 0; k < nh; ++k) {
 				uint2 o = __ldg(occ + k);
 				A.a[k].t = o.x;
@@ -866,7 +912,7 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 		na = merge_hits(w.a[cur], na, w.a[cur ^ 1], occ, h.y, i, flags);
 		cur ^= 1;
 	}
-	Anchors &A = w.a[cur];
+	AnchorsT<K> &A = w.a[cur];
 	uint32_t n1 = 0, max = 0, n;
 	if (na == 0)
 		goto miss;
@@ -945,10 +991,11 @@ miss:
 
 // intersect2 list step (src/hash_align.c:1528-1556): returns the number of
 // pairs kept (lists compacted in place), 0 if none.
-__device__ inline int intersect_lists(DPair &P, int c, uint32_t add)
+template <class K>
+__device__ inline int intersect_lists(DPairT<K> &P, int c, uint32_t add)
 {
-	DSlot &X = P.s[c][0];
-	DSlot &Y = P.s[c][1];
+	DSlotT<K> &X = P.s[c][0];
+	DSlotT<K> &Y = P.s[c][1];
 	int i = 0, k = 0, n = 0;
 	while (i < X.n && k < Y.n) {
 		if (X.t[i] < Y.t[k]) {
@@ -1009,10 +1056,12 @@ __device__ __forceinline__ int mat_score(uint8_t a, uint8_t b)
 	return a == b ? 1 : -2;
 }
 
-struct SswOut {
+template <class K>
+struct SswOutT {
 	int32_t score, skip, pstart, ok;
-	DCig cig;
+	DCigT<K> cig;
 };
+using SswOut = SswOutT<CapsStd>;
 
 // oriented read code x of read (o, L)
 __device__ __forceinline__ uint8_t read_code(const uint8_t *code, int64_t o, int L, int orient, int x)
@@ -1030,12 +1079,28 @@ __host__ __device__ inline int ssw_rows(int L)
 // shared-memory layout of one warp's area
 constexpr int SSW_REF_B = ((MAX_FRAG + 32 + 15) / 16) * 16;
 constexpr int SSW_RD_B = ((MAX_READ + 15) / 16) * 16;
-constexpr int SSW_CIG_B = (int)((sizeof(DCig) + 15) / 16) * 16;
+template <class K>
+__host__ __device__ constexpr int ssw_cig_b()
+{
+	return (int)((sizeof(DCigT<K>) + 15) / 16) * 16;
+}
+// an area for R rows a lane and a CIGAR of capacities K
+template <class K>
+__host__ __device__ inline size_t ssw_smem_rows(int R)
+{
+	const size_t col = (size_t)32 * R;   // bytes of one saved column
+	return SSW_REF_B + SSW_RD_B + ssw_cig_b<K>() + SSW_NCK * col + (((SSW_CK + 1) * col + 15) / 16) * 16;
+}
 __host__ __device__ inline size_t ssw_smem_per_warp(int max_len)
 {
-	const int R = ssw_rows(max_len);
-	const size_t col = (size_t)32 * R;   // bytes of one saved column
-	return SSW_REF_B + SSW_RD_B + SSW_CIG_B + SSW_NCK * col + (((SSW_CK + 1) * col + 15) / 16) * 16;
+	return ssw_smem_rows<CapsStd>(ssw_rows(max_len));
+}
+// the wide pass runs every call with the widest row layout (rows past the
+// read take code 5 and feed no row of the read, so results do not change)
+constexpr int SSW_WIDE_R = 10;
+__host__ __device__ inline size_t ssw_smem_wide()
+{
+	return ssw_smem_rows<CapsWide>(SSW_WIDE_R);
 }
 
 // Score + 2 (3 for equal codes, N == N included, else 0) of every code
@@ -1112,13 +1177,13 @@ __device__ inline void ssw_stage(const DevIndex &ix, uint32_t wstart, int ln, co
 	const int lane = threadIdx.x & 31;
 	uint8_t *ref_s = sm;
 	uint8_t *rd_s = sm + SSW_REF_B;
-	DCig &cig = *reinterpret_cast<DCig *>(sm + SSW_REF_B + SSW_RD_B);
+	int *cig_n = reinterpret_cast<int *>(sm + SSW_REF_B + SSW_RD_B);   // DCigT's n, nm
 	for (int i = lane; i < ln; i += 32)
 		ref_s[i] = __ldg(ix.code + wstart + i);
 	for (int i = lane; i < L; i += 32)
 		rd_s[i] = read_code(code, roff, L, orient, i);
 	if (lane == 0)
-		cig.n = cig.nm = 0;
+		cig_n[0] = cig_n[1] = 0;
 }
 
 // Pass 1 of one call with the lanes over the window: lane l owns columns
@@ -1194,18 +1259,19 @@ __device__ void ssw_pass1_cols(const uint8_t *__restrict__ ref_s, const uint8_t 
 
 // The reference's traceback and output of one call whose sweep has run
 // (end cell max_v / min_y / min_x; checkpoints in its area).
-template <int R, bool CAP>
+template <int R, bool CAP, class K>
 __device__ void ssw_walk(const DevIndex &ix, uint32_t wstart, int ln, int L, int start, uint32_t tl,
-			 uint8_t *__restrict__ sm, SswOut &out, int &flags, int max_v, int min_y, int min_x)
+			 uint8_t *__restrict__ sm, SswOutT<K> &out, int &flags, int max_v, int min_y, int min_x)
 {
+	constexpr int MCAP = K::M, CCAP = K::C;
 	const unsigned FULL = 0xffffffffu;
 	const int lane = threadIdx.x & 31;
 	const int x0 = lane * R;
 	const int COL = 32 * R;
 	uint8_t *ref_s = sm;
 	uint8_t *rd_s = sm + SSW_REF_B;
-	DCig &cig = *reinterpret_cast<DCig *>(sm + SSW_REF_B + SSW_RD_B);
-	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + SSW_CIG_B;
+	DCigT<K> &cig = *reinterpret_cast<DCigT<K> *>(sm + SSW_REF_B + SSW_RD_B);
+	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + ssw_cig_b<K>();
 	uint8_t *tb = ck + (size_t)SSW_NCK * COL;
 	uint32_t rsel[R];   // the lane's read rows as score selectors
 #pragma unroll
@@ -1479,20 +1545,20 @@ __device__ void ssw_walk(const DevIndex &ix, uint32_t wstart, int ln, int L, int
 // 32 lanes of a warp; `sm` is the warp's shared-memory area
 // (ssw_smem_per_warp(L) bytes at least).  Fills `out` (lane 0 writes the
 // scalars; the CIGAR is copied by the warp).
-template <int R>
+template <int R, class K = CapsStd>
 __device__ void ssw_warp_r(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff, int L,
-			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOut &out, int &flags)
+			   int orient, int start, uint32_t tl, uint8_t *__restrict__ sm, SswOutT<K> &out, int &flags)
 {
 	ssw_stage(ix, wstart, ln, code, roff, L, orient, sm);
 	__syncwarp();
-	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + SSW_CIG_B;
+	uint8_t *ck = sm + SSW_REF_B + SSW_RD_B + ssw_cig_b<K>();
 	int max_v, min_y, min_x;
 	if (L > 253) {
 		ssw_pass1_cols<true>(sm, sm + SSW_REF_B, ln, L, ck, 32 * R, max_v, min_y, min_x);
-		ssw_walk<R, true>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
+		ssw_walk<R, true, K>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
 	} else {
 		ssw_pass1_cols<false>(sm, sm + SSW_REF_B, ln, L, ck, 32 * R, max_v, min_y, min_x);
-		ssw_walk<R, false>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
+		ssw_walk<R, false, K>(ix, wstart, ln, L, start, tl, sm, out, flags, max_v, min_y, min_x);
 	}
 }
 
@@ -1511,6 +1577,15 @@ __device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, con
 	case 8: ssw_warp_r<8>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
 	default: ssw_warp_r<10>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags); break;
 	}
+}
+
+// The wide pass's form: every read length in the widest row layout, the
+// CIGAR in a CapsWide area (ssw_smem_wide() bytes).
+__device__ inline void ssw_warp(const DevIndex &ix, uint32_t wstart, int ln, const uint8_t *code, int64_t roff,
+				int L, int orient, int start, uint32_t tl, uint8_t *__restrict__ sm,
+				SswOutT<CapsWide> &out, int &flags)
+{
+	ssw_warp_r<SSW_WIDE_R, CapsWide>(ix, wstart, ln, code, roff, L, orient, start, tl, sm, out, flags);
 }
 
 }  // namespace hg

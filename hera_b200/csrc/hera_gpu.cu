@@ -51,18 +51,55 @@ struct RmReq {
 	int16_t c, str;
 };
 
-struct Batch {
+template <class K>
+struct BatchT {
 	DevIndex ix;
 	const uint8_t *code;     // read codes
 	const uint8_t *code_r;   // reverse-complement codes (read i at the same offset)
 	const int64_t *off;      // read offsets (2 per pair: mate 1, mate 2)
 	const int32_t *len;
-	DPair *P;
+	DPairT<K> *P;
 	int *flags;
 	unsigned long long *stats;   // work counters, ST_* slots
 	int score_only;
 	int max_len;             // longest read of the batch (seed table stride)
+	// wide pass only: P[i] is the pair (or single read) pmap[i] of the
+	// batch, and thread t of a per-task kernel works in work[t] (the
+	// CapsWide working set is too large for local memory)
+	const int *pmap;
+	GpWorkT<K> *work;
+	__device__ __forceinline__ int item(int i) const { return pmap ? pmap[i] : i; }
+	// read of candidate c, strand str of the pair in P[i] (c ^ str == 0:
+	// mate 1, src/hash_align.c:1667-1670)
+	__device__ __forceinline__ int read_of(int i, int c, int str) const
+	{
+		return 2 * item(i) + ((c ^ str) == 0 ? 0 : 1);
+	}
 };
+using Batch = BatchT<CapsStd>;
+
+// per-task working set: a local variable in the first pass, the task's
+// slot of b.work in the wide pass
+template <class K, bool GLOBAL = (K::A > CapsStd::A)>
+struct TaskWork;
+template <class K>
+struct TaskWork<K, false> {
+	GpWorkT<K> w;
+	__device__ __forceinline__ GpWorkT<K> &get(const BatchT<K> &, int) { return w; }
+};
+template <class K>
+struct TaskWork<K, true> {
+	__device__ __forceinline__ GpWorkT<K> &get(const BatchT<K> &b, int t) { return b.work[t]; }
+};
+
+// the capacity flags a pair met, kept with the pair (the wide pass re-runs
+// it); every flag also goes to the batch's word
+template <class K>
+__device__ __forceinline__ void pair_flags(const BatchT<K> &b, int i, int f)
+{
+	if (f & F_CAPS)
+		atomicOr(&b.P[i].ovf, f & F_CAPS);
+}
 
 // work counters (hera_gpu_timing's probes .. ssw_cells)
 enum { ST_PROBES = 0, ST_SEED_HITS = 1, ST_SW_CELLS = 2, ST_SSW_CELLS = 3, ST_N = 4 };
@@ -82,7 +119,8 @@ __device__ __forceinline__ void warp_stat(unsigned long long *c, uint32_t v)
 }
 
 // read `ri` in orientation `orient` (1 = reverse complement) into rd
-__device__ __forceinline__ int load_read(const Batch &b, int ri, int orient, uint8_t *rd)
+template <class K>
+__device__ __forceinline__ int load_read(const BatchT<K> &b, int ri, int orient, uint8_t *rd)
 {
 	const int64_t o = b.off[ri];
 	int L = b.len[ri];
@@ -189,7 +227,8 @@ __global__ void __launch_bounds__(256) k_seed(DevIndex ix, const uint8_t *__rest
 	warp_stat(stats + ST_SEED_HITS, found);
 }
 
-__device__ __forceinline__ void slot_reset(DSlot &S)
+template <class K>
+__device__ __forceinline__ void slot_reset(DSlotT<K> &S)
 {
 	S.n = 0;
 	S.err = 0;
@@ -199,18 +238,20 @@ __device__ __forceinline__ void slot_reset(DSlot &S)
 
 // the four space-31 get_position calls of check_in_transcriptome
 // (src/hash_align.c:1667-1670); independent because pass A needs space < 31
-__global__ void __launch_bounds__(TPB) k_position(Batch b, int n_pairs, int spr, const uint2 *__restrict__ hits)
+template <class K>
+__global__ void __launch_bounds__(TPB) k_position(BatchT<K> b, int n_pairs, int spr, const uint2 *__restrict__ hits)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n_pairs * 4)
 		return;
 	const int pi = t >> 2, task = t & 3;
 	const int c = task >> 1, str = task & 1;
-	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
-	GpWork w;
+	const int ri = b.read_of(pi, c, str);
+	TaskWork<K> tw;
+	GpWorkT<K> &w = tw.get(b, t);
 	int flags = 0;
-	DPair &P = b.P[pi];
-	DSlot &S = P.s[c][str];
+	DPairT<K> &P = b.P[pi];
+	DSlotT<K> &S = P.s[c][str];
 	slot_reset(S);
 	if (str == 0) {
 		P.pair[c] = 0;
@@ -235,24 +276,27 @@ __global__ void __launch_bounds__(TPB) k_position(Batch b, int n_pairs, int spr,
 	}
 	const int L = load_read(b, ri, str, w.rd);
 	get_position(b.ix, w.rd, L, P, c, str, KMER, pre, b.score_only != 0, w, flags);
+	pair_flags(b, pi, flags);
 	flag(b.flags, flags);
 }
 
 // per-pair control flow after the space-31 calls (src/hash_align.c:1672-1695
 // and :1730-1733 with intersect2/re_map :1504-1562).  A pair that needs a
 // mate rescue enqueues it and stops; it resumes at P.stage next round.
-__global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restrict__ resume, int n,
+template <class K>
+__global__ void __launch_bounds__(TPB) k_resolve(BatchT<K> b, const RmReq *__restrict__ resume, int n,
 						  RmReq *__restrict__ q, int *__restrict__ qn)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n)
 		return;
 	const int pi = resume ? resume[t].pair : t;
-	DPair &P = b.P[pi];
-	GpWork w;
+	DPairT<K> &P = b.P[pi];
+	TaskWork<K> tw;
+	GpWorkT<K> &w = tw.get(b, t);
 	int flags = 0;
 	auto gp = [&](int c, int str) {
-		const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+		const int ri = b.read_of(pi, c, str);
 		const int L = load_read(b, ri, str, w.rd);
 		get_position(b.ix, w.rd, L, P, c, str, 2 * ERR, nullptr, b.score_only != 0, w, flags);
 	};
@@ -263,7 +307,11 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 		q[k].str = (int16_t)str;
 		P.stage = next;
 	};
-	if (b.len[2 * pi] > b.max_len || b.len[2 * pi + 1] > b.max_len) {
+	auto done = [&]() {
+		pair_flags(b, pi, flags);
+		flag(b.flags, flags);
+	};
+	if (b.len[b.read_of(pi, 0, 0)] > b.max_len || b.len[b.read_of(pi, 0, 1)] > b.max_len) {
 		P.stage = 7;
 		return;
 	}
@@ -284,13 +332,13 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 		}
 		case 1: case 2: case 3: case 4: {   // get_position2 x4 (:1683-1694)
 			const int c = (st - 1) >> 1, s = (st - 1) & 1;
-			const DSlot &X = P.s[c][s], &Y = P.s[c][1 - s];
-			const DSlot &O0 = P.s[1 - c][0], &O1 = P.s[1 - c][1];
+			const DSlotT<K> &X = P.s[c][s], &Y = P.s[c][1 - s];
+			const DSlotT<K> &O0 = P.s[1 - c][0], &O1 = P.s[1 - c][1];
 			if (X.n == 0 && Y.n > 0 && Y.err < ERR && O0.err + O1.err > ERR) {
 				gp(c, s);
 				if (P.s[c][s].n == 0) {
 					rescue(c, s, 10 + st);
-					flag(b.flags, flags);
+					done();
 					return;
 				}
 			}
@@ -307,7 +355,7 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 					const int i = P.s[c][0].err < P.s[c][1].err ? 1 : 0;   // re_map
 					P.rm_i = i;
 					rescue(c, i, 20 + 2 * c);
-					flag(b.flags, flags);
+					done();
 					return;
 				}
 			}
@@ -318,7 +366,7 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 			const int c = (st - 20) >> 1;
 			if (P.rm_ret == 0) {
 				rescue(c, 1 - P.rm_i, st + 1);
-				flag(b.flags, flags);
+				done();
 				return;
 			}
 			P.pair[c] = 2;
@@ -334,7 +382,7 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 		}
 		default:
 			P.stage = 7;
-			flag(b.flags, flags);
+			done();
 			return;
 		}
 	}
@@ -342,7 +390,8 @@ __global__ void __launch_bounds__(TPB) k_resolve(Batch b, const RmReq *__restric
 
 // re_mapSW (src/hash_align.c:762-846), in three steps.
 // 1) one ssw_align call per (queued request, mate hit)
-__global__ void k_rescue_expand(Batch b, const RmReq *__restrict__ q, int nq, int2 *__restrict__ calls,
+template <class K>
+__global__ void k_rescue_expand(BatchT<K> b, const RmReq *__restrict__ q, int nq, int2 *__restrict__ calls,
 				int *__restrict__ base, int *__restrict__ ncalls)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -359,9 +408,11 @@ __global__ void k_rescue_expand(Batch b, const RmReq *__restrict__ q, int nq, in
 // 2) one warp per call: local SW over the MAX_FRAG window at the mate hit;
 // each warp works in its own `per` bytes of the block's shared memory
 constexpr int RESCUE_TPB = 256;   // at most 8 calls (warps) per block
-__global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *__restrict__ q,
+constexpr int WIDE_RESCUE_WPB = 4;   // calls per block in the wide pass (CapsWide areas)
+template <class K>
+__global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(BatchT<K> b, const RmReq *__restrict__ q,
 							   const int2 *__restrict__ calls, int c0, int nc,
-							   SswOut *__restrict__ out, int per)
+							   SswOutT<K> *__restrict__ out, int per)
 {
 	extern __shared__ __align__(16) uint8_t ssw_sm[];
 	const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // warp within launch
@@ -369,12 +420,12 @@ __global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *
 		return;
 	const int2 cl = calls[c0 + wl];
 	const RmReq rq = q[cl.x];
-	const DPair &P = b.P[rq.pair];
+	const DPairT<K> &P = b.P[rq.pair];
 	const int c = rq.c, str = rq.str;
 	const int type = str == 0 ? -1 : 1;
-	const int ri = 2 * rq.pair + ((c ^ str) == 0 ? 0 : 1);
+	const int ri = b.read_of(rq.pair, c, str);
 	const int L = b.len[ri];
-	const DSlot &M = P.s[c][1 - str];
+	const DSlotT<K> &M = P.s[c][1 - str];
 	const uint32_t tr = M.t[cl.y];
 	const uint32_t tl = __ldg(b.ix.tlen + tr);
 	int start = M.p[cl.y] + (type > 0 ? 0 : L - MAX_FRAG);
@@ -398,6 +449,7 @@ __global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *
 	ssw_warp(b.ix, __ldg(b.ix.tstart + tr) + (uint32_t)start, ln, b.code, b.off[ri], L, str, start, tl,
 		 ssw_sm + (size_t)(threadIdx.x >> 5) * per, out[c0 + wl], flags);
 	if ((threadIdx.x & 31) == 0) {
+		pair_flags(b, rq.pair, flags);
 		flag(b.flags, flags);
 		atomicAdd(b.stats + ST_SSW_CELLS, (unsigned long long)ln * (unsigned long long)L);
 	}
@@ -405,21 +457,22 @@ __global__ void __launch_bounds__(RESCUE_TPB) k_rescue_sw(Batch b, const RmReq *
 
 // 3) per request: min score wins, ties append in hit order; the mate's list
 // is compacted to the rescued subset (src/hash_align.c:794-845)
-__global__ void k_rescue_fin(Batch b, const RmReq *__restrict__ q, int nq, const int *__restrict__ base,
-			     const SswOut *__restrict__ out)
+template <class K>
+__global__ void k_rescue_fin(BatchT<K> b, const RmReq *__restrict__ q, int nq, const int *__restrict__ base,
+			     const SswOutT<K> *__restrict__ out)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= nq)
 		return;
 	const RmReq rq = q[t];
-	DPair &P = b.P[rq.pair];
+	DPairT<K> &P = b.P[rq.pair];
 	const int c = rq.c, str = rq.str;
-	DSlot &S = P.s[c][str];
-	DSlot &M = P.s[c][1 - str];
+	DSlotT<K> &S = P.s[c][str];
+	DSlotT<K> &M = P.s[c][1 - str];
 	const int n = M.n, b0 = base[t];
 	int new_n = 0, score2 = 0, best = -1;
 	for (int i = 0; i < n; ++i) {
-		const SswOut &o = out[b0 + i];
+		const SswOutT<K> &o = out[b0 + i];
 		if (!o.ok)
 			continue;
 		const uint32_t tr = M.t[i];
@@ -451,66 +504,115 @@ __global__ void k_rescue_fin(Batch b, const RmReq *__restrict__ q, int nq, const
 }
 
 // align_single_read front half (src/hash_align.c:1822-1823)
-__global__ void __launch_bounds__(TPB) k_single(Batch b, int n)
+template <class K>
+__global__ void __launch_bounds__(TPB) k_single(BatchT<K> b, int n)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n)
 		return;
-	DPair &P = b.P[t];
-	GpWork w;
+	DPairT<K> &P = b.P[t];
+	const int ri = b.item(t);
+	TaskWork<K> tw;
+	GpWorkT<K> &w = tw.get(b, t);
 	int flags = 0;
 	slot_reset(P.s[0][0]);
 	slot_reset(P.s[0][1]);
 	P.pair[0] = 0;
-	if (b.len[t] > b.max_len) {
+	P.ovf = 0;
+	if (b.len[ri] > b.max_len) {
 		flag(b.flags, F_READ);
-		P.s[0][0].err = P.s[0][1].err = b.len[t];
+		P.s[0][0].err = P.s[0][1].err = b.len[ri];
 		return;
 	}
-	int L = load_read(b, t, 0, w.rd);
+	int L = load_read(b, ri, 0, w.rd);
 	get_position(b.ix, w.rd, L, P, 0, 0, 2 * ERR, nullptr, b.score_only != 0, w, flags);
-	L = load_read(b, t, 1, w.rd);
+	L = load_read(b, ri, 1, w.rd);
 	get_position(b.ix, w.rd, L, P, 0, 1, 2 * ERR, nullptr, b.score_only != 0, w, flags);
+	pair_flags(b, t, flags);
 	flag(b.flags, flags);
 }
 
+// Records of the pairs that ran the wide pass, already packed (their own
+// records and pools); the first pass's state of those pairs is ignored.
+struct Side {
+	const int *slot;            // per item of the batch: its side index, or -1
+	const hera_cand_rec *recs;  // [side index * ncand + c]
+	const uint32_t *pos;
+	const int32_t *p;
+	const uint32_t *op;
+	const uint8_t *miss;
+};
+
 // per record: entries of the list / op / miss pools
-__global__ void k_count(const DPair *__restrict__ P, int n_items, int ncand, uint32_t *__restrict__ cl,
-			uint32_t *__restrict__ co, uint32_t *__restrict__ cm)
+template <class K>
+__global__ void k_count(const DPairT<K> *__restrict__ P, int n_items, int ncand, uint32_t *__restrict__ cl,
+			uint32_t *__restrict__ co, uint32_t *__restrict__ cm, Side side)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n_items * ncand)
 		return;
-	const DPair &p = P[t / ncand];
 	const int c = t % ncand;
+	const int so = side.slot ? side.slot[t / ncand] : -1;
 	uint32_t l = 0, o = 0, m = 0;
-	for (int s = 0; s < 2; ++s) {
-		l += (uint32_t)p.s[c][s].n;
-		o += (uint32_t)p.s[c][s].cig.n;
-		m += (uint32_t)p.s[c][s].cig.nm;
+	if (so >= 0) {
+		const hera_cand_rec &r = side.recs[(size_t)so * ncand + c];
+		l = (uint32_t)(r.n[0] + r.n[1]);
+		o = (uint32_t)r.n_cigar[0] + r.n_cigar[1];
+		m = (uint32_t)r.n_miss[0] + r.n_miss[1];
+	} else {
+		const DPairT<K> &p = P[t / ncand];
+		for (int s = 0; s < 2; ++s) {
+			l += (uint32_t)p.s[c][s].n;
+			o += (uint32_t)p.s[c][s].cig.n;
+			m += (uint32_t)p.s[c][s].cig.nm;
+		}
 	}
 	cl[t] = l;
 	co[t] = o;
 	cm[t] = m;
 }
 
-__global__ void k_emit(const DPair *__restrict__ P, int n_items, int ncand,
+template <class K>
+__global__ void k_emit(const DPairT<K> *__restrict__ P, int n_items, int ncand,
 		       const uint32_t *__restrict__ xl, const uint32_t *__restrict__ xo,
 		       const uint32_t *__restrict__ xm, hera_cand_rec *__restrict__ recs,
 		       uint32_t *__restrict__ pos_pool, int32_t *__restrict__ p_pool,
 		       uint32_t *__restrict__ op_pool, uint8_t *__restrict__ miss_pool,
-		       uint64_t base_l, uint64_t base_o, uint64_t base_m)
+		       uint64_t base_l, uint64_t base_o, uint64_t base_m, Side side)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n_items * ncand)
 		return;
-	const DPair &p = P[t / ncand];
 	const int c = t % ncand;
 	uint32_t l = xl[t], o = xo[t], m = xm[t];
+	const int so = side.slot ? side.slot[t / ncand] : -1;
 	hera_cand_rec r;
+	if (so >= 0) {
+		const hera_cand_rec &w = side.recs[(size_t)so * ncand + c];
+		r = w;
+		for (int s = 0; s < 2; ++s) {
+			r.list_off[s] = (uint32_t)(base_l + l);
+			r.cig_off[s] = (uint32_t)(base_o + o);
+			r.miss_off[s] = (uint32_t)(base_m + m);
+			for (int i = 0; i < w.n[s]; ++i) {
+				pos_pool[l + i] = side.pos[w.list_off[s] + i];
+				p_pool[l + i] = side.p[w.list_off[s] + i];
+			}
+			for (int i = 0; i < w.n_cigar[s]; ++i)
+				op_pool[o + i] = side.op[w.cig_off[s] + i];
+			for (int i = 0; i < w.n_miss[s]; ++i)
+				miss_pool[m + i] = side.miss[w.miss_off[s] + i];
+			l += (uint32_t)w.n[s];
+			o += (uint32_t)w.n_cigar[s];
+			m += (uint32_t)w.n_miss[s];
+		}
+		recs[t] = r;
+		return;
+	}
+	const DPairT<K> &p = P[t / ncand];
 	r.pair = p.pair[c];
 	for (int s = 0; s < 2; ++s) {
-		const DSlot &S = p.s[c][s];
+		const DSlotT<K> &S = p.s[c][s];
 		r.n[s] = S.n;
 		r.err[s] = S.err;
 		r.list_off[s] = (uint32_t)(base_l + l);
@@ -531,6 +633,31 @@ __global__ void k_emit(const DPair *__restrict__ P, int n_items, int ncand,
 		m += (uint32_t)S.cig.nm;
 	}
 	recs[t] = r;
+}
+
+// the plain form's pairs start with no capacity flags (k_position's four
+// tasks of a pair would race to clear them)
+__global__ void k_ovf_reset(DPair *__restrict__ P, int n)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < n)
+		P[t].ovf = 0;
+}
+
+// the pairs (items) the first pass flagged: their list, and each item's
+// position in it (-1 for the others)
+__global__ void k_ovf_list(const DPair *__restrict__ P, int n, int *__restrict__ list, int *__restrict__ nlist,
+			   int *__restrict__ slot)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n)
+		return;
+	int k = -1;
+	if (P[t].ovf)
+		k = atomicAdd(nlist, 1);
+	if (k >= 0)
+		list[k] = t;
+	slot[t] = k;
 }
 
 #include "hera_batched.cuh"
@@ -577,6 +704,16 @@ struct DBuf {   // growable device buffer
 		fixed = false;
 	}
 };
+
+// an output pool of n entries: an owned pool grows with one spare entry (so
+// it is never empty); a bound pool must hold n as it is
+template <typename T>
+static cudaError_t pool_ensure(DBuf<T> &b, size_t n)
+{
+	if (b.fixed)
+		return n <= b.cap ? cudaSuccess : cudaErrorMemoryAllocation;
+	return b.ensure(n + 1);
+}
 
 template <typename T>
 struct HBuf {   // growable pinned host buffer
@@ -632,6 +769,16 @@ struct Lane {
 	DBuf<int2> calls;
 	DBuf<int> rq_base;
 	DBuf<SswOut> ssw_out;
+	// the wide pass (pairs past a first-pass capacity): made on first use
+	bool no_wide = false;                // the allocation-free lane has none
+	DBuf<int> ovf_list, ovf_slot;
+	DBuf<DPairT<CapsWide>> wpairs;
+	DBuf<GpWorkT<CapsWide>> wwork;
+	DBuf<SswOutT<CapsWide>> wssw_out;
+	DBuf<hera_cand_rec> side_recs;
+	DBuf<uint32_t> side_pos, side_op;
+	DBuf<int32_t> side_p;
+	DBuf<uint8_t> side_miss;
 	DBuf<TaskInfo> tinfo;
 	DBuf<Chain> chains;
 	DBuf<JobSlot> slots;
@@ -656,6 +803,9 @@ struct Lane {
 	// result of the last batch this lane ran (held in its device pools)
 	int32_t items = 0, ncand = 0;
 	uint64_t nl = 0, no = 0, nm = 0;
+	// set while the output pools are sized: a failure then means the pools
+	// (not the working buffers) were too small, and nl/no/nm are the sizes
+	bool pools_short = false;
 	// pool offsets the device records were last rebased by (a fetch into
 	// page-locked memory rebases them in place); 0 after each batch
 	uint32_t rb_l = 0, rb_o = 0, rb_m = 0;
@@ -673,6 +823,8 @@ struct Lane {
 		hits.release(); pairs.release(); q[0].release(); q[1].release(); qg[0].release();
 		qg[1].release(); counters.release(); cnt.release(); cub_tmp.release();
 		calls.release(); rq_base.release(); ssw_out.release(); tinfo.release(); chains.release();
+		ovf_list.release(); ovf_slot.release(); wpairs.release(); wwork.release(); wssw_out.release();
+		side_recs.release(); side_pos.release(); side_op.release(); side_p.release(); side_miss.release();
 		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
@@ -896,8 +1048,10 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
 	// the rescue kernel's per-warp shared-memory areas (up to ~177 KiB a block)
-	if (cudaFuncSetAttribute(k_rescue_sw, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				 (int)((RESCUE_TPB / 32) * ssw_smem_per_warp(MAX_READ))) != cudaSuccess)
+	if (cudaFuncSetAttribute(k_rescue_sw<CapsStd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				 (int)((RESCUE_TPB / 32) * ssw_smem_per_warp(MAX_READ))) != cudaSuccess ||
+	    cudaFuncSetAttribute(k_rescue_sw<CapsWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				 (int)(WIDE_RESCUE_WPB * ssw_smem_wide())) != cudaSuccess)
 		return bail(fail(ctx, HERA_GPU_ECUDA, "rescue kernel shared-memory size"));
 	if (cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess ||
 	    ctx->sms <= 0)
@@ -919,6 +1073,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	// the allocation-free entry's lane: its stream, events and 32 pinned
 	// counters are made here, so that entry point itself allocates nothing
 	ctx->na = new Lane();
+	ctx->na->no_wide = true;
 	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    ctx->na->h_small.ensure(32) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
@@ -988,12 +1143,24 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 // ---- pipeline pieces --------------------------------------------------
 
 // one rescue round (re_mapSW for every queued request)
-static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq *q, int nq,
+// the lane's rescue outputs for the first pass / the wide pass
+template <class K>
+static DBuf<SswOutT<K>> &ssw_outputs(Lane &L)
+{
+	if constexpr (std::is_same<K, CapsStd>::value)
+		return L.ssw_out;
+	else
+		return L.wssw_out;
+}
+
+template <class K>
+static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const BatchT<K> &b, const RmReq *q, int nq,
 			int max_len, uint32_t &launches, float &ms_acc)
 {
+	constexpr bool wide = !std::is_same<K, CapsStd>::value;
 	cudaStream_t st = L.stream;
 	std::shared_lock<std::shared_mutex> shared(ctx->gate);
-	LK(L.calls.ensure((size_t)nq * LCAP), "rescue calls");
+	LK(L.calls.ensure((size_t)nq * K::L), "rescue calls");
 	LK(L.rq_base.ensure(nq), "rescue bases");
 	int *d_nc = L.counters.p + 4;
 	LK(cudaMemsetAsync(d_nc, 0, sizeof(int), st), "memset");
@@ -1004,17 +1171,18 @@ static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq 
 	LK(cudaMemcpyAsync(L.h_small.p + 1, d_nc, sizeof(int), cudaMemcpyDeviceToHost, st), "calls");
 	LK(cudaStreamSynchronize(st), "rescue expand");
 	const int ncalls = L.h_small.p[1];
-	LK(L.ssw_out.ensure(ncalls + 1), "rescue outputs");
-	const int per = (int)ssw_smem_per_warp(max_len);
+	DBuf<SswOutT<K>> &outs = ssw_outputs<K>(L);
+	LK(outs.ensure(ncalls + 1), "rescue outputs");
+	const int per = wide ? (int)ssw_smem_wide() : (int)ssw_smem_per_warp(max_len);
 	auto launch = [&](int wpb) {
 		k_rescue_sw<<<blocks_for((int64_t)ncalls * 32, 32 * wpb), 32 * wpb, wpb * per, st>>>(
-			b, q, L.calls.p, 0, ncalls, L.ssw_out.p, per);
+			b, q, L.calls.p, 0, ncalls, outs.p, per);
 		++launches;
 	};
 	// autotune: the first large rescue round times each candidate (every
 	// run writes the same outputs)
 	std::unique_lock<std::shared_mutex> excl(ctx->gate, std::defer_lock);
-	if (ncalls >= 2048 && claim_tuning(ctx, ctx->rescue_tuning)) {
+	if (!wide && ncalls >= 2048 && claim_tuning(ctx, ctx->rescue_tuning)) {
 		shared.unlock();   // nothing of this lane is in flight (synchronised above)
 		excl.lock();
 		int best = 0;
@@ -1047,9 +1215,9 @@ static int rescue_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, const RmReq 
 	}
 	cudaEventRecord(L.ev[10], st);
 	if (ncalls > 0)
-		launch(tuned_rescue_wpb(ctx));
+		launch(wide ? WIDE_RESCUE_WPB : tuned_rescue_wpb(ctx));
 	cudaEventRecord(L.ev[11], st);
-	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.rq_base.p, L.ssw_out.p);
+	k_rescue_fin<<<blocks_for(nq, 256), 256, 0, st>>>(b, q, nq, L.rq_base.p, outs.p);
 	++launches;
 	cudaEventRecord(e1, st);
 	LK(cudaStreamSynchronize(st), "rescue");
@@ -1200,6 +1368,161 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 	return HERA_GPU_OK;
 }
 
+// The plain form's pair control flow after the space-31 calls: rounds of
+// k_resolve and mate rescues until no pair waits (n pairs in b.P).
+template <class K>
+static int plain_rounds(hera_gpu_ctx *ctx, Lane &L, const BatchT<K> &b, int n, int max_len, uint32_t &launches,
+			float &resolve_ms, float &rescue_ms, uint32_t &rounds)
+{
+	cudaStream_t st = L.stream;
+	const RmReq *resume = nullptr;
+	int nact = n, qi = 0;
+	while (nact > 0) {
+		int *qn = L.counters.p + 1 + qi;
+		LK(cudaMemsetAsync(qn, 0, sizeof(int), st), "memset");
+		cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
+		cudaEventRecord(e0, st);
+		k_resolve<<<blocks_for(nact), TPB, 0, st>>>(b, resume, nact, L.q[qi].p, qn);
+		++launches;
+		cudaEventRecord(e1, st);
+		LK(cudaMemcpyAsync(L.h_small.p, qn, sizeof(int), cudaMemcpyDeviceToHost, st), "queue size");
+		LK(cudaStreamSynchronize(st), "resolve");
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		resolve_ms += ms;
+		const int nq = L.h_small.p[0];
+		if (nq == 0)
+			break;
+		++rounds;
+		int rc = rescue_round(ctx, L, b, L.q[qi].p, nq, max_len, launches, rescue_ms);
+		if (rc)
+			return rc;
+		resume = L.q[qi].p;
+		nact = nq;
+		qi ^= 1;
+	}
+	return HERA_GPU_OK;
+}
+
+// a device buffer grown to n entries with its first `keep` entries kept
+template <typename T>
+static cudaError_t grow_keep(DBuf<T> &d, size_t n, size_t keep, cudaStream_t st)
+{
+	if (n <= d.cap)
+		return cudaSuccess;
+	DBuf<T> nd;
+	cudaError_t e = nd.ensure(n + n / 2);
+	if (e == cudaSuccess && keep && d.p)
+		e = cudaMemcpyAsync(nd.p, d.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(st);
+	if (e != cudaSuccess) {
+		nd.release();
+		return e;
+	}
+	d.release();
+	d = nd;
+	return cudaSuccess;
+}
+
+// The second, wide pass.  Every pair (or single read) whose first pass met
+// a per-read capacity (its DPair.ovf) is aligned again from the start with
+// CapsWide -- the same code, larger lists, working sets in device memory --
+// WIDE_WAVE at a time, and its records are packed into the lane's side
+// pools.  A pair's result depends on that pair alone, so this is exactly
+// the result an unbounded first pass would have given.  `side` then
+// routes the final pack to those records.
+constexpr int WIDE_WAVE = 128;
+
+static int wide_pass(hera_gpu_ctx *ctx, Lane &L, const Batch &b, int32_t n, bool paired, int spr, int max_len,
+		     uint32_t &launches, float &resolve_ms, float &rescue_ms, uint32_t &rounds, Side &side, int &wflags)
+{
+	cudaStream_t st = L.stream;
+	const int ncand = paired ? 2 : 1;
+	LK(L.ovf_list.ensure(n), "wide pass list");
+	LK(L.ovf_slot.ensure(n), "wide pass list");
+	int *d_nw = L.counters.p + 28, *d_wf = L.counters.p + 29;
+	LK(cudaMemsetAsync(d_nw, 0, 2 * sizeof(int), st), "memset");
+	k_ovf_list<<<blocks_for(n, 256), 256, 0, st>>>(b.P, n, L.ovf_list.p, d_nw, L.ovf_slot.p);
+	++launches;
+	LK(cudaMemcpyAsync(L.h_small.p + 28, d_nw, sizeof(int), cudaMemcpyDeviceToHost, st), "wide pass count");
+	LK(cudaStreamSynchronize(st), "wide pass list");
+	const int nw = L.h_small.p[28];
+	if (nw <= 0)
+		return set_err(L.err, HERA_GPU_ECAPACITY, "a per-read capacity flag that no pair holds");
+	const int wave = nw < WIDE_WAVE ? nw : WIDE_WAVE;
+	LK(L.wpairs.ensure(wave), "wide pass state");
+	LK(L.wwork.ensure((size_t)(paired ? 4 : 1) * wave), "wide pass working sets");
+	LK(L.side_recs.ensure((size_t)nw * ncand), "wide pass records");
+	BatchT<CapsWide> bw;
+	bw.ix = b.ix;
+	bw.code = b.code;
+	bw.code_r = b.code_r;
+	bw.off = b.off;
+	bw.len = b.len;
+	bw.P = L.wpairs.p;
+	bw.flags = d_wf;
+	bw.stats = b.stats;
+	bw.score_only = b.score_only;
+	bw.max_len = b.max_len;
+	bw.work = L.wwork.p;
+	uint64_t fl = 0, fo = 0, fm = 0;   // side pools filled so far
+	for (int w0 = 0; w0 < nw; w0 += wave) {
+		const int nv = nw - w0 < wave ? nw - w0 : wave;
+		bw.pmap = L.ovf_list.p + w0;
+		if (paired) {
+			k_position<<<blocks_for((int64_t)nv * 4), TPB, 0, st>>>(bw, nv, spr, L.hits.p);
+			++launches;
+			const int rc = plain_rounds(ctx, L, bw, nv, max_len, launches, resolve_ms, rescue_ms, rounds);
+			if (rc)
+				return rc;
+		} else {
+			k_single<<<blocks_for(nv), TPB, 0, st>>>(bw, nv);
+			++launches;
+		}
+		// pack the wave's records into the side pools
+		const int items = nv * ncand;
+		uint32_t *cl = L.cnt.p, *co = cl + (items + 1), *cm = co + (items + 1);
+		uint32_t *xl = cm + (items + 1), *xo = xl + (items + 1), *xm = xo + (items + 1);
+		LK(cudaMemsetAsync(cl, 0, 3 * sizeof(uint32_t) * (items + 1), st), "memset");
+		k_count<<<blocks_for(items, 256), 256, 0, st>>>(bw.P, nv, ncand, cl, co, cm, Side{});
+		size_t tmp_bytes = 0;
+		cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cl, xl, items + 1, st);
+		LK(L.cub_tmp.ensure(tmp_bytes), "scan scratch");
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cl, xl, items + 1, st);
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, co, xo, items + 1, st);
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cm, xm, items + 1, st);
+		LK(cudaMemcpyAsync(L.h_small.p + 2, xl + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaMemcpyAsync(L.h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaMemcpyAsync(L.h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaStreamSynchronize(st), "wide pass scan");
+		const uint64_t tl = (uint32_t)L.h_small.p[2], to = (uint32_t)L.h_small.p[3], tm = (uint32_t)L.h_small.p[4];
+		LK(grow_keep(L.side_pos, fl + tl + 1, fl, st), "wide pass pools");
+		LK(grow_keep(L.side_p, fl + tl + 1, fl, st), "wide pass pools");
+		LK(grow_keep(L.side_op, fo + to + 1, fo, st), "wide pass pools");
+		LK(grow_keep(L.side_miss, fm + tm + 1, fm, st), "wide pass pools");
+		k_emit<<<blocks_for(items, 256), 256, 0, st>>>(bw.P, nv, ncand, xl, xo, xm, L.side_recs.p + (size_t)w0 * ncand,
+								L.side_pos.p + fl, L.side_p.p + fl, L.side_op.p + fo,
+								L.side_miss.p + fm, fl, fo, fm, Side{});
+		launches += 5;
+		fl += tl;
+		fo += to;
+		fm += tm;
+		if (fl >= (1ull << 32) || fo >= (1ull << 32) || fm >= (1ull << 32))
+			return set_err(L.err, HERA_GPU_ECAPACITY, "wide pass pools beyond 2^32 entries");
+	}
+	LK(cudaMemcpyAsync(L.h_small.p + 29, d_wf, sizeof(int), cudaMemcpyDeviceToHost, st), "wide pass flags");
+	LK(cudaStreamSynchronize(st), "wide pass");
+	wflags = L.h_small.p[29];
+	side.slot = L.ovf_slot.p;
+	side.recs = L.side_recs.p;
+	side.pos = L.side_pos.p;
+	side.p = L.side_p.p;
+	side.op = L.side_op.p;
+	side.miss = L.side_miss.p;
+	return HERA_GPU_OK;
+}
+
 // Run the device pipeline for one sub-batch on lane L.  Reads: d_seq holds
 // seq_bytes bytes, d_off/d_len are lane-local (offsets into d_seq), 2n
 // reads for pairs (mates interleaved), n for singles.  Leaves the packed
@@ -1282,35 +1605,13 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 		cudaEventRecord(L.ev[3], st);
 	} else if (!batched) {
 		// plain form: one thread per get_position call / pair
+		k_ovf_reset<<<blocks_for(n, 256), 256, 0, st>>>(L.pairs.p, n);
 		k_position<<<blocks_for((int64_t)n * 4), TPB, 0, st>>>(b, n, spr, L.hits.p);
-		++launches;
+		launches += 2;
 		cudaEventRecord(L.ev[3], st);
-		const RmReq *resume = nullptr;
-		int nact = n, qi = 0;
-		while (nact > 0) {
-			int *qn = L.counters.p + 1 + qi;
-			LK(cudaMemsetAsync(qn, 0, sizeof(int), st), "memset");
-			cudaEvent_t e0 = L.ev[6], e1 = L.ev[7];
-			cudaEventRecord(e0, st);
-			k_resolve<<<blocks_for(nact), TPB, 0, st>>>(b, resume, nact, L.q[qi].p, qn);
-			++launches;
-			cudaEventRecord(e1, st);
-			LK(cudaMemcpyAsync(L.h_small.p, qn, sizeof(int), cudaMemcpyDeviceToHost, st), "queue size");
-			LK(cudaStreamSynchronize(st), "resolve");
-			float ms = 0;
-			cudaEventElapsedTime(&ms, e0, e1);
-			resolve_ms += ms;
-			const int nq = L.h_small.p[0];
-			if (nq == 0)
-				break;
-			++rounds;
-			int rc = rescue_round(ctx, L, b, L.q[qi].p, nq, max_len, launches, rescue_ms);
-			if (rc)
-				return rc;
-			resume = L.q[qi].p;
-			nact = nq;
-			qi ^= 1;
-		}
+		const int rc = plain_rounds(ctx, L, b, n, max_len, launches, resolve_ms, rescue_ms, rounds);
+		if (rc)
+			return rc;
 	} else {
 		// batched form: rounds of batched get_position calls and rescues
 		LK(L.qg[0].ensure(n), "gp queue");
@@ -1365,39 +1666,66 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 		}
 	}
 	cudaEventRecord(L.ev[4], st);
-	// pack
+	// pack: per-record pool sizes, their offsets and totals (and the
+	// batch's flags and work counters)
 	uint32_t *cl = L.cnt.p, *co = cl + (items + 1), *cm = co + (items + 1);
 	uint32_t *xl = cm + (items + 1), *xo = xl + (items + 1), *xm = xo + (items + 1);
-	LK(cudaMemsetAsync(cl, 0, 3 * sizeof(uint32_t) * (items + 1), st), "memset");
-	k_count<<<blocks_for(items, 256), 256, 0, st>>>(L.pairs.p, n, ncand, cl, co, cm);
-	++launches;
-	size_t tmp_bytes = 0;
-	cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cl, xl, items + 1, st);
-	LK(L.cub_tmp.ensure(tmp_bytes), "scan scratch");
-	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cl, xl, items + 1, st);
-	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, co, xo, items + 1, st);
-	cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cm, xm, items + 1, st);
-	LK(cudaMemcpyAsync(L.h_small.p + 2, xl + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	LK(cudaMemcpyAsync(L.h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	LK(cudaMemcpyAsync(L.h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
-	LK(cudaMemcpyAsync(L.h_small.p + 5, d_flags, 4, cudaMemcpyDeviceToHost, st), "flags");
-	LK(cudaMemcpyAsync(L.h_small.p + 16, d_stats, ST_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
-	   "counters");
-	LK(cudaStreamSynchronize(st), "scan");
+	auto count_scan = [&](const Side &side) -> int {
+		LK(cudaMemsetAsync(cl, 0, 3 * sizeof(uint32_t) * (items + 1), st), "memset");
+		k_count<<<blocks_for(items, 256), 256, 0, st>>>(L.pairs.p, n, ncand, cl, co, cm, side);
+		++launches;
+		size_t tmp_bytes = 0;
+		cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cl, xl, items + 1, st);
+		LK(L.cub_tmp.ensure(tmp_bytes), "scan scratch");
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cl, xl, items + 1, st);
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, co, xo, items + 1, st);
+		cub::DeviceScan::ExclusiveSum(L.cub_tmp.p, tmp_bytes, cm, xm, items + 1, st);
+		LK(cudaMemcpyAsync(L.h_small.p + 2, xl + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaMemcpyAsync(L.h_small.p + 3, xo + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaMemcpyAsync(L.h_small.p + 4, xm + items, 4, cudaMemcpyDeviceToHost, st), "totals");
+		LK(cudaMemcpyAsync(L.h_small.p + 5, d_flags, 4, cudaMemcpyDeviceToHost, st), "flags");
+		LK(cudaMemcpyAsync(L.h_small.p + 16, d_stats, ST_N * sizeof(unsigned long long),
+				   cudaMemcpyDeviceToHost, st),
+		   "counters");
+		LK(cudaStreamSynchronize(st), "scan");
+		return HERA_GPU_OK;
+	};
+	Side side{};
+	int rc = count_scan(side);
+	if (rc)
+		return rc;
+	int fl = L.h_small.p[5];
+	if ((fl & F_CAPS) && !L.no_wide) {
+		// pairs past a first-pass capacity: aligned again in the wide pass,
+		// then the records packed with theirs in place
+		int wf = 0;
+		rc = wide_pass(ctx, L, b, n, paired, spr, max_len, launches, resolve_ms, rescue_ms, rounds, side, wf);
+		if (rc)
+			return rc;
+		T.wide_items += (uint64_t)L.h_small.p[28];
+		fl = (fl & ~F_CAPS) | (wf & ~F_CAPS) | ((wf & F_CAPS) ? F_WIDE : 0);
+		rc = count_scan(side);
+		if (rc)
+			return rc;
+	}
 	const uint32_t tl = (uint32_t)L.h_small.p[2], to = (uint32_t)L.h_small.p[3],
 		       tm = (uint32_t)L.h_small.p[4];
-	const int fl = L.h_small.p[5];
 	L.items = items;
 	L.rb_l = L.rb_o = L.rb_m = 0;
 	L.nl = tl;
 	L.no = to;
 	L.nm = tm;
-	LK(L.pos_pool.ensure(tl + 1), "list pool");
-	LK(L.p_pool.ensure(tl + 1), "list pool");
-	LK(L.op_pool.ensure(to + 1), "op pool");
-	LK(L.miss_pool.ensure(tm + 1), "miss pool");
+	// owned pools keep one spare entry; pools bound to a caller's buffers
+	// are held to exactly the capacity the caller gave (nothing is ever
+	// written at index tl / to / tm)
+	L.pools_short = true;
+	LK(pool_ensure(L.pos_pool, tl), "list pool");
+	LK(pool_ensure(L.p_pool, tl), "list pool");
+	LK(pool_ensure(L.op_pool, to), "op pool");
+	LK(pool_ensure(L.miss_pool, tm), "miss pool");
+	L.pools_short = false;
 	k_emit<<<blocks_for(items, 256), 256, 0, st>>>(L.pairs.p, n, ncand, xl, xo, xm, L.recs.p, L.pos_pool.p,
-							L.p_pool.p, L.op_pool.p, L.miss_pool.p, 0, 0, 0);
+							L.p_pool.p, L.op_pool.p, L.miss_pool.p, 0, 0, 0, side);
 	++launches;
 	cudaEventRecord(L.ev[5], st);
 	LK(cudaGetLastError(), "kernel launch");
@@ -1437,8 +1765,15 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 	L.no = to;
 	L.nm = tm;
 	if (fl) {
-		char buf[160];
-		snprintf(buf, sizeof buf, "per-read capacity exceeded (flags 0x%x)", fl);
+		char buf[200];
+		if (fl & F_WIDE)
+			snprintf(buf, sizeof buf, "a read passed the wide pass's capacities (%d anchors or hits of one "
+				 "get_position call; flags 0x%x)", CapsWide::A, fl);
+		else if ((fl & F_CAPS) && L.no_wide)
+			snprintf(buf, sizeof buf, "per-read capacity exceeded (flags 0x%x); this entry has no wide pass",
+				 fl);
+		else
+			snprintf(buf, sizeof buf, "per-read capacity exceeded (flags 0x%x)", fl);
 		return set_err(L.err, HERA_GPU_ECAPACITY, buf);
 	}
 	return HERA_GPU_OK;
@@ -1856,6 +2191,7 @@ static void sum_timing(hera_gpu_ctx *ctx)
 		t.seed_hits += a.seed_hits;
 		t.sw_cells += a.sw_cells;
 		t.ssw_cells += a.ssw_cells;
+		t.wide_items += a.wide_items;
 	}
 	t.total_ms = ctx->timing.total_ms;
 	ctx->timing = t;
@@ -2224,13 +2560,17 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 	L.slot_cap = na::SLOTS;
 	// outputs: the caller's device buffers (records: 2 n entries)
 	L.recs.bind(d_out->recs, 2 * (size_t)n);
-	L.pos_pool.bind(d_out->pos_pool, d_out->pos_pool ? d_out->list_cap + 1 : 0);
-	L.p_pool.bind(d_out->p_pool, d_out->p_pool ? d_out->list_cap + 1 : 0);
-	L.op_pool.bind(d_out->op_pool, d_out->op_pool ? d_out->op_cap + 1 : 0);
-	L.miss_pool.bind(d_out->miss_pool, d_out->miss_pool ? d_out->miss_cap + 1 : 0);
+	// exactly the caller's capacities: the pools are written below the
+	// sizes the count pass found and nowhere else
+	L.pos_pool.bind(d_out->pos_pool, d_out->pos_pool ? d_out->list_cap : 0);
+	L.p_pool.bind(d_out->p_pool, d_out->p_pool ? d_out->list_cap : 0);
+	L.op_pool.bind(d_out->op_pool, d_out->op_pool ? d_out->op_cap : 0);
+	L.miss_pool.bind(d_out->miss_pool, d_out->miss_pool ? d_out->miss_cap : 0);
 
 	L.timing = hera_gpu_timing{};
 	L.err.clear();
+	L.nl = L.no = L.nm = 0;
+	L.pools_short = false;
 	cudaEventRecord(L.ev[0], caller);
 	cudaStreamWaitEvent(L.stream, L.ev[0], 0);
 	k_rebase<<<blocks_for(2 * (int64_t)n, 256), 256, 0, L.stream>>>(d_off, 2 * (int64_t)n, base, L.off.p);
@@ -2238,13 +2578,21 @@ extern "C" int hera_gpu_align_pairs_device_noalloc(hera_gpu_ctx *ctx, const uint
 	cudaEventRecord(L.ev[5], L.stream);
 	cudaStreamWaitEvent(caller, L.ev[5], 0);
 	ctx->timing = L.timing;
-	if (rc == HERA_GPU_ENOMEM) {
+	if (rc == HERA_GPU_ENOMEM && L.pools_short) {
+		// the batch ran; only the caller's pools were too small
 		d_out->list_used = L.nl;
 		d_out->op_used = L.no;
 		d_out->miss_used = L.nm;
 		return fail(ctx, HERA_GPU_ECAPACITY,
-			    (std::string("allocation-free entry: fixed scratch or output buffer too small (") + L.err +
+			    (std::string("allocation-free entry: output pools too small (") + L.err +
 			     "); *_used hold the pool sizes needed")
+				    .c_str());
+	}
+	if (rc == HERA_GPU_ENOMEM) {
+		// the batch's working set outgrew the fixed scratch: *_used stay 0
+		return fail(ctx, HERA_GPU_ECAPACITY,
+			    (std::string("allocation-free entry: the batch's working set outgrew the fixed scratch (") +
+			     L.err + "); align fewer pairs per call")
 				    .c_str());
 	}
 	if (rc != HERA_GPU_OK)
@@ -2394,37 +2742,178 @@ extern "C" int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, in
 	return align_dropin(ctx, reads, nullptr, n, write_bam, out);
 }
 
-// ---- kernel-level check of the mate-rescue DP ----------------------------
+// ---- kernel-level check of the gap DP ------------------------------------
+//
+// One SW_align call (src/hash_align.c:627-760) per (window, query, err),
+// run by the batched form's own DP kernels: the register form k_dp_reg<4|8>
+// for the live error caps, k_dp_generic for everything else (empty queries,
+// windows shorter than error + 1 whose row 0 spills into row 1).  Windows
+// are laid out 16 zero bytes apart, like the reference's zero-padded calls.
 
 namespace {
-__global__ void __launch_bounds__(RESCUE_TPB) k_unit_ssw(DevIndex ix, const int64_t *__restrict__ ref_off,
+__global__ void k_unit_jobs(const int64_t *__restrict__ ref_at, const int64_t *__restrict__ ref_off,
+			    const int64_t *__restrict__ q_off, const int32_t *__restrict__ err, int n,
+			    DpJob *__restrict__ jobs, int *__restrict__ perm)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n)
+		return;
+	DpJob j{};
+	j.rstart = (uint32_t)ref_at[t];
+	j.ref_len = (uint16_t)(ref_off[t + 1] - ref_off[t]);
+	j.len = (uint16_t)(q_off[t + 1] - q_off[t]);
+	j.qoff = 0;
+	j.err = (int8_t)err[t];
+	j.orient = 0;
+	j.read = t;
+	jobs[t] = j;
+	perm[t] = t;
+}
+}  // namespace
+
+extern "C" int hera_gpu_unit_sw(int device, const char *refs, const int64_t *ref_off, const char *qs,
+				const int64_t *q_off, const int32_t *err, int32_t n, int write_bam, int32_t *score,
+				uint32_t *ops, int32_t *n_ops, char *miss, int32_t *n_miss, int32_t cap,
+				int32_t *flags)
+{
+	if (!refs || !ref_off || !qs || !q_off || !err || n < 0 || !score || !ops || !n_ops || !miss || !n_miss ||
+	    !flags || cap < 1 || (write_bam != 0 && write_bam != 1))
+		return HERA_GPU_EINVAL;
+	*flags = 0;
+	if (n == 0)
+		return HERA_GPU_OK;
+	if (cudaSetDevice(device) != cudaSuccess)
+		return HERA_GPU_ENODEV;
+	std::vector<int64_t> at((size_t)n);
+	int64_t rb = 0;
+	for (int i = 0; i < n; ++i) {
+		const int64_t rl = ref_off[i + 1] - ref_off[i], ql = q_off[i + 1] - q_off[i];
+		const int e = err[i] < 0 ? -err[i] : err[i];
+		if (rl < 0 || rl > 65535 || ql < 0 || ql > MAX_DP_ROWS || e < 1 || e > 12)
+			return HERA_GPU_EINVAL;
+		at[i] = rb;
+		rb += rl + 16;
+	}
+	const int64_t qb = q_off[n];
+	std::vector<uint8_t> seq((size_t)rb + 64, 0);
+	for (int i = 0; i < n; ++i)
+		memcpy(seq.data() + at[i], refs + ref_off[i], (size_t)(ref_off[i + 1] - ref_off[i]));
+	const int rcap = write_bam == 1 ? 2 : JCAP;
+	const size_t stride = (size_t)res_stride(rcap);
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	const size_t o_rcode = al((size_t)rb + 64), o_q = o_rcode + al((size_t)rb + 64),
+		     o_qc = o_q + al((size_t)qb + 64), o_at = o_qc + al((size_t)qb + 64),
+		     o_roff = o_at + al((size_t)n * 8), o_qoff = o_roff + al((size_t)(n + 1) * 8),
+		     o_err = o_qoff + al((size_t)(n + 1) * 8), o_jobs = o_err + al((size_t)n * 4),
+		     o_perm = o_jobs + al((size_t)n * sizeof(DpJob)), o_res = o_perm + al((size_t)n * 4),
+		     o_cnt = o_res + al((size_t)n * stride), need = o_cnt + 256;
+	uint8_t *d = nullptr;
+	if (cudaMalloc(&d, need) != cudaSuccess)
+		return HERA_GPU_ENOMEM;
+	int rc = HERA_GPU_OK;
+	int *d_cnt = reinterpret_cast<int *>(d + o_cnt);
+	cudaGetLastError();
+	if (cudaMemcpy(d, seq.data(), (size_t)rb + 64, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d + o_q, qs, (size_t)qb, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemset(d + o_q + qb, 0, 64) != cudaSuccess ||
+	    cudaMemcpy(d + o_at, at.data(), (size_t)n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d + o_roff, ref_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d + o_qoff, q_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d + o_err, err, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemset(d_cnt, 0, 256) != cudaSuccess)
+		rc = HERA_GPU_ECUDA;
+	if (rc == HERA_GPU_OK) {
+		k_codes<<<64, 256>>>(d, d + o_rcode, rb + 64);
+		k_codes<<<64, 256>>>(d + o_q, d + o_qc, qb + 64);
+		DpJob *jobs = reinterpret_cast<DpJob *>(d + o_jobs);
+		int *perm = reinterpret_cast<int *>(d + o_perm);
+		k_unit_jobs<<<blocks_for(n, 256), 256>>>(reinterpret_cast<int64_t *>(d + o_at),
+							 reinterpret_cast<int64_t *>(d + o_roff),
+							 reinterpret_cast<int64_t *>(d + o_qoff),
+							 reinterpret_cast<int32_t *>(d + o_err), n, jobs, perm);
+		Batch b{};
+		b.ix.code = d + o_rcode;
+		b.ix.seq = d;
+		b.code = d + o_qc;
+		b.code_r = d + o_qc;
+		b.off = reinterpret_cast<int64_t *>(d + o_qoff);
+		b.flags = d_cnt;
+		b.stats = reinterpret_cast<unsigned long long *>(d_cnt + 16);
+		b.score_only = write_bam == 1;
+		b.max_len = MAX_READ;
+		uint8_t *res = d + o_res;
+		k_dp_reg<4><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		k_dp_reg<8><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		k_dp_generic<<<blocks_for(n), 128>>>(b, jobs, n, res, rcap);
+		std::vector<uint8_t> h((size_t)n * stride);
+		cudaError_t e = cudaGetLastError();
+		if (e == cudaSuccess)
+			e = cudaDeviceSynchronize();
+		if (e == cudaSuccess)
+			e = cudaMemcpy(h.data(), res, h.size(), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess)
+			e = cudaMemcpy(flags, d_cnt, 4, cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) {
+			fprintf(stderr, "hera_gpu_unit_sw: %s\n", cudaGetErrorString(e));
+			rc = HERA_GPU_ECUDA;
+		} else {
+			for (int i = 0; i < n; ++i) {
+				const uint8_t *o = h.data() + (size_t)i * stride;
+				DpResHdr hd;
+				memcpy(&hd, o, sizeof hd);
+				score[i] = hd.score;
+				n_ops[i] = hd.n;
+				n_miss[i] = hd.nm;
+				if (hd.caps)
+					*flags |= F_CCAP;
+				for (int k = 0; k < hd.n && k < cap; ++k)
+					memcpy(ops + (size_t)i * cap + k, o + sizeof(DpResHdr) + 4 * k, 4);
+				for (int k = 0; k < hd.nm && k < cap; ++k)
+					miss[(size_t)i * cap + k] = (char)o[sizeof(DpResHdr) + 4 * rcap + k];
+			}
+		}
+	}
+	cudaFree(d);
+	return rc;
+}
+
+// ---- kernel-level check of the mate-rescue DP ----------------------------
+
+// As in the aligner, a call whose CIGAR passes the first pass's capacities
+// runs again in the wide pass's form.
+namespace {
+template <class K>
+__global__ void __launch_bounds__(RESCUE_TPB) k_unit_ssw(DevIndex ix, const int *__restrict__ which,
+							  const int64_t *__restrict__ ref_off,
 							  const uint8_t *__restrict__ rcode, const int64_t *__restrict__ read_off,
-							  int n, SswOut *__restrict__ out, int per, int *__restrict__ flags)
+							  int n, SswOutT<K> *__restrict__ out, int per, int *__restrict__ flags)
 {
 	extern __shared__ __align__(16) uint8_t ssw_sm[];
 	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (w >= n)
 		return;
-	const int ln = (int)(ref_off[w + 1] - ref_off[w]), L = (int)(read_off[w + 1] - read_off[w]);
+	const int i = which ? which[w] : w;
+	const int ln = (int)(ref_off[i + 1] - ref_off[i]), L = (int)(read_off[i + 1] - read_off[i]);
 	int f = 0;
-	if ((size_t)((threadIdx.x >> 5) + 1) * per > dyn_smem_bytes() || (size_t)per < ssw_smem_per_warp(L)) {
+	const size_t need = std::is_same<K, CapsStd>::value ? ssw_smem_per_warp(L) : ssw_smem_wide();
+	if ((size_t)((threadIdx.x >> 5) + 1) * per > dyn_smem_bytes() || (size_t)per < need) {
 		if ((threadIdx.x & 31) == 0)
-			atomicOr(flags, F_SCRATCH);
+			flags[w] = F_SCRATCH;
 		return;
 	}
-	ssw_warp(ix, (uint32_t)ref_off[w], ln, rcode, read_off[w], L, 0, 0, 0xffffffffu,
+	ssw_warp(ix, (uint32_t)ref_off[i], ln, rcode, read_off[i], L, 0, 0, 0xffffffffu,
 		 ssw_sm + (size_t)(threadIdx.x >> 5) * per, out[w], f);
-	if ((threadIdx.x & 31) == 0 && f)
-		atomicOr(flags, f);
+	if ((threadIdx.x & 31) == 0)
+		flags[w] = f;
 }
 }  // namespace
 
 extern "C" int hera_gpu_unit_ssw(int device, const char *refs, const int64_t *ref_off, const char *reads,
 				 const int64_t *read_off, int32_t n, int32_t *score, int32_t *skip, uint32_t *ops,
-				 int32_t *n_ops, char *miss, int32_t *n_miss, int32_t *flags)
+				 int32_t *n_ops, char *miss, int32_t *n_miss, int32_t cap, int32_t *flags)
 {
 	if (!refs || !ref_off || !reads || !read_off || n < 0 || !score || !skip || !ops || !n_ops || !miss ||
-	    !n_miss || !flags)
+	    !n_miss || !flags || cap < 1)
 		return HERA_GPU_EINVAL;
 	*flags = 0;
 	if (n == 0)
@@ -2441,64 +2930,105 @@ extern "C" int hera_gpu_unit_ssw(int device, const char *refs, const int64_t *re
 	const int64_t rb = ref_off[n], qb = read_off[n];
 	std::vector<uint8_t> seq((size_t)rb + 64, 0);
 	memcpy(seq.data(), refs, (size_t)rb);
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	const size_t o_rcode = al((size_t)rb + 64), o_read = o_rcode + al((size_t)rb + 64),
+		     o_qcode = o_read + al((size_t)qb + 64), o_roff = o_qcode + al((size_t)qb + 64),
+		     o_qoff = o_roff + al((size_t)(n + 1) * 8), o_flags = o_qoff + al((size_t)(n + 1) * 8),
+		     o_which = o_flags + al((size_t)n * 4), o_out = o_which + al((size_t)n * 4),
+		     o_wout = o_out + al((size_t)n * sizeof(SswOut));
 	uint8_t *d = nullptr;
-	const size_t per = ssw_smem_per_warp(max_len);
-	const size_t bytes_s = 2 * ((size_t)rb + 64) + 2 * ((size_t)qb + 64);
-	const size_t off_s = (bytes_s + 255) & ~(size_t)255;
-	const size_t need = off_s + (size_t)(n + 1) * 16 + 256 + (size_t)n * sizeof(SswOut);
-	if (cudaMalloc(&d, need) != cudaSuccess)
+	if (cudaMalloc(&d, o_wout) != cudaSuccess)
 		return HERA_GPU_ENOMEM;
-	uint8_t *d_seq = d, *d_rcode = d_seq + rb + 64, *d_read = d_rcode + rb + 64, *d_qcode = d_read + qb + 64;
-	int64_t *d_roff = reinterpret_cast<int64_t *>(d + off_s);
-	int64_t *d_qoff = d_roff + n + 1;
-	int *d_flags = reinterpret_cast<int *>(d_qoff + n + 1);
-	SswOut *d_out = reinterpret_cast<SswOut *>(reinterpret_cast<uint8_t *>(d_flags) + 256);
+	int64_t *d_roff = reinterpret_cast<int64_t *>(d + o_roff), *d_qoff = reinterpret_cast<int64_t *>(d + o_qoff);
+	int *d_flags = reinterpret_cast<int *>(d + o_flags), *d_which = reinterpret_cast<int *>(d + o_which);
+	SswOut *d_out = reinterpret_cast<SswOut *>(d + o_out);
+	SswOutT<CapsWide> *d_wout = nullptr;
 	int rc = HERA_GPU_OK;
 	cudaGetLastError();
-	if (cudaMemcpy(d_seq, seq.data(), rb + 64, cudaMemcpyHostToDevice) != cudaSuccess ||
-	    cudaMemcpy(d_read, reads, qb, cudaMemcpyHostToDevice) != cudaSuccess ||
-	    cudaMemset(d_read + qb, 0, 64) != cudaSuccess ||
+	if (cudaMemcpy(d, seq.data(), rb + 64, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemcpy(d + o_read, reads, qb, cudaMemcpyHostToDevice) != cudaSuccess ||
+	    cudaMemset(d + o_read + qb, 0, 64) != cudaSuccess ||
 	    cudaMemcpy(d_roff, ref_off, (n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
 	    cudaMemcpy(d_qoff, read_off, (n + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-	    cudaMemset(d_flags, 0, 4) != cudaSuccess)
+	    cudaMemset(d_flags, 0, (size_t)n * 4) != cudaSuccess)
 		rc = HERA_GPU_ECUDA;
-	if (rc == HERA_GPU_OK) {
-		k_codes<<<64, 256>>>(d_seq, d_rcode, rb + 64);
-		k_codes<<<64, 256>>>(d_read, d_qcode, qb + 64);
-		DevIndex ix{};
-		ix.code = d_rcode;
-		ix.seq = d_seq;
-		const int wpb = 4;
-		const cudaError_t ea =
-			cudaFuncSetAttribute(k_unit_ssw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * per));
-		if (ea != cudaSuccess)
-			fprintf(stderr, "hera_gpu_unit_ssw: shared-memory size: %s\n", cudaGetErrorString(ea));
-		k_unit_ssw<<<(n + wpb - 1) / wpb, 32 * wpb, wpb * per>>>(ix, d_roff, d_qcode, d_qoff, n, d_out, (int)per,
-									   d_flags);
-		std::vector<SswOut> h((size_t)n);
-		cudaError_t e = cudaGetLastError();
-		if (e == cudaSuccess)
-			e = cudaDeviceSynchronize();
-		if (e == cudaSuccess)
-			e = cudaMemcpy(h.data(), d_out, n * sizeof(SswOut), cudaMemcpyDeviceToHost);
-		if (e == cudaSuccess)
-			e = cudaMemcpy(flags, d_flags, 4, cudaMemcpyDeviceToHost);
-		if (e != cudaSuccess) {
-			fprintf(stderr, "hera_gpu_unit_ssw: %s\n", cudaGetErrorString(e));
+	std::vector<int> hf((size_t)n), wide;
+	std::vector<SswOut> h((size_t)n);
+	std::vector<SswOutT<CapsWide>> hw;
+	DevIndex ix{};
+	ix.code = d + o_rcode;
+	ix.seq = d;
+	auto check = [&](const char *what, cudaError_t e) {
+		if (e != cudaSuccess && rc == HERA_GPU_OK) {
+			fprintf(stderr, "hera_gpu_unit_ssw: %s: %s\n", what, cudaGetErrorString(e));
 			rc = HERA_GPU_ECUDA;
-		} else {
-			for (int i = 0; i < n; ++i) {
-				score[i] = h[i].score;
-				skip[i] = h[i].skip;
-				n_ops[i] = h[i].cig.n;
-				n_miss[i] = h[i].cig.nm;
-				for (int k = 0; k < h[i].cig.n && k < CCAP; ++k)
-					ops[(size_t)i * CCAP + k] = h[i].cig.op[k];
-				for (int k = 0; k < h[i].cig.nm && k < MCAP; ++k)
-					miss[(size_t)i * MCAP + k] = (char)h[i].cig.miss[k];
-			}
+		}
+	};
+	if (rc == HERA_GPU_OK) {
+		k_codes<<<64, 256>>>(d, d + o_rcode, rb + 64);
+		k_codes<<<64, 256>>>(d + o_read, d + o_qcode, qb + 64);
+		const int wpb = 4;
+		const size_t per = ssw_smem_per_warp(max_len);
+		check("shared-memory size",
+		      cudaFuncSetAttribute(k_unit_ssw<CapsStd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * per)));
+		k_unit_ssw<CapsStd><<<(n + wpb - 1) / wpb, 32 * wpb, wpb * per>>>(ix, nullptr, d_roff, d + o_qcode, d_qoff, n,
+										  d_out, (int)per, d_flags);
+		check("launch", cudaGetLastError());
+		check("run", cudaDeviceSynchronize());
+		check("copy", cudaMemcpy(h.data(), d_out, n * sizeof(SswOut), cudaMemcpyDeviceToHost));
+		check("copy", cudaMemcpy(hf.data(), d_flags, (size_t)n * 4, cudaMemcpyDeviceToHost));
+		for (int i = 0; i < n; ++i)
+			if (hf[i] & F_CAPS)
+				wide.push_back(i);
+	}
+	if (rc == HERA_GPU_OK && !wide.empty()) {
+		const int nw = (int)wide.size();
+		const size_t per = ssw_smem_wide();
+		hw.resize((size_t)nw);
+		check("wide outputs", cudaMalloc(&d_wout, (size_t)nw * sizeof(SswOutT<CapsWide>)));
+		if (rc == HERA_GPU_OK) {
+			check("copy", cudaMemcpy(d_which, wide.data(), (size_t)nw * 4, cudaMemcpyHostToDevice));
+			check("copy", cudaMemset(d_flags, 0, (size_t)nw * 4));
+			check("shared-memory size",
+			      cudaFuncSetAttribute(k_unit_ssw<CapsWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+						   (int)(WIDE_RESCUE_WPB * per)));
+			k_unit_ssw<CapsWide><<<(nw + WIDE_RESCUE_WPB - 1) / WIDE_RESCUE_WPB, 32 * WIDE_RESCUE_WPB,
+					       WIDE_RESCUE_WPB * per>>>(ix, d_which, d_roff, d + o_qcode, d_qoff, nw, d_wout,
+									 (int)per, d_flags);
+			check("launch", cudaGetLastError());
+			check("run", cudaDeviceSynchronize());
+			check("copy", cudaMemcpy(hw.data(), d_wout, (size_t)nw * sizeof(SswOutT<CapsWide>),
+						 cudaMemcpyDeviceToHost));
+			std::vector<int> wf((size_t)nw);
+			check("copy", cudaMemcpy(wf.data(), d_flags, (size_t)nw * 4, cudaMemcpyDeviceToHost));
+			for (int k = 0; k < nw; ++k)
+				hf[wide[k]] = wf[k] ? (wf[k] | F_WIDE) : 0;
 		}
 	}
+	if (rc == HERA_GPU_OK) {
+		auto put = [&](int i, const auto &o) {
+			score[i] = o.score;
+			skip[i] = o.skip;
+			n_ops[i] = o.cig.n;
+			n_miss[i] = o.cig.nm;
+			for (int k = 0; k < o.cig.n && k < cap; ++k)
+				ops[(size_t)i * cap + k] = o.cig.op[k];
+			for (int k = 0; k < o.cig.nm && k < cap; ++k)
+				miss[(size_t)i * cap + k] = (char)o.cig.miss[k];
+		};
+		std::vector<int> wpos((size_t)n, -1);
+		for (size_t k = 0; k < wide.size(); ++k)
+			wpos[wide[k]] = (int)k;
+		for (int i = 0; i < n; ++i) {
+			if (wpos[i] >= 0)
+				put(i, hw[wpos[i]]);
+			else
+				put(i, h[i]);
+			*flags |= hf[i];
+		}
+	}
+	if (d_wout)
+		cudaFree(d_wout);
 	cudaFree(d);
 	return rc;
 }

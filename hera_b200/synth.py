@@ -202,6 +202,55 @@ def random_transcriptome(seed: int, n: int, mean_len: float = 1800.0, sigma: flo
     return Transcriptome(names, seq, length, np.cumsum(length, dtype=np.uint64).astype(np.uint32))
 
 
+def family_transcriptome(seed: int, families=((80, 500),), n_other: int = 40, tail: int = 300,
+                         other_len: int = 1500, gc: float = 0.41) -> Transcriptome:
+    """Transcripts in paralog families: the members of a family of
+    (size, shared) share one `shared`-bp sequence, each followed by a
+    `tail`-bp sequence of its own; `n_other` unrelated transcripts follow.
+    A read from a shared sequence hits every member of its family, so a
+    family larger than a per-read list capacity exercises the long-list
+    path."""
+    rng = np.random.default_rng(seed)
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+
+    def rand(n):
+        return _ACGT[rng.choice(4, size=n, p=p).astype(np.uint8)]
+
+    parts = []
+    for size, shared in families:
+        core = rand(shared)
+        parts += [np.concatenate([core, rand(tail)]) for _ in range(size)]
+    parts += [rand(other_len) for _ in range(n_other)]
+    length = np.array([x.shape[0] for x in parts], np.uint32)
+    names = [f"{_ids('HTRAN', i + 1)}:{_ids('HGENE', i + 1)}" for i in range(len(parts))]
+    return Transcriptome(names, np.concatenate(parts), length,
+                         np.cumsum(length, dtype=np.uint64).astype(np.uint32))
+
+
+def family_pairs(tx: Transcriptome, n: int, seed: int, shared: int, read_len: int = 100,
+                 sub_rate: float = 0.005, mate2_random: bool = False) -> tuple:
+    """Pairs whose mate 1 comes from the shared sequence of the first
+    family (transcript 0's first `shared` bases), forward strand; mate 2 is
+    the reverse complement of a later stretch of the same sequence, or
+    random sequence (unmappable: the pair then needs a mate rescue over
+    every member of the family)."""
+    rng = np.random.default_rng(seed)
+    src = tx.seq[:shared]
+    m1 = np.empty((n, read_len), np.uint8)
+    m2 = np.empty((n, read_len), np.uint8)
+    for i in range(n):
+        a = int(rng.integers(0, max(1, shared - 2 * read_len)))
+        m1[i] = src[a:a + read_len]
+        if mate2_random:
+            m2[i] = _ACGT[rng.integers(0, 4, read_len)]
+        else:
+            b = int(rng.integers(a, max(a + 1, shared - read_len)))
+            m2[i] = revcomp(src[b:b + read_len])
+    _substitute(rng, m1, sub_rate)
+    _substitute(rng, m2, sub_rate)
+    return _pack_matrix(m1), _pack_matrix(m2)
+
+
 @dataclasses.dataclass
 class ReadSet:
     """Reads packed back to back: read i is seq[off[i]:off[i]+len[i]]."""

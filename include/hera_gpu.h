@@ -179,6 +179,11 @@ typedef struct hera_gpu_timing {
 	uint64_t sw_cells;       /* SW_align cells evaluated, counted the way
 				    src/hash_align.c:659-681 visits them */
 	uint64_t ssw_cells;      /* ssw_align cells: ref_len x read_len per call */
+	uint64_t wide_items;     /* pairs (or single reads) aligned again in the
+				    wide pass: their first pass met a per-read
+				    capacity (more than 256 anchors in one
+				    get_position call, 64 hits, 96 CIGAR ops or
+				    miss chars) */
 } hera_gpu_timing;
 
 /* ---- entry points ------------------------------------------------------ */
@@ -254,10 +259,17 @@ int hera_gpu_fetch_result(hera_gpu_ctx *ctx, hera_gpu_result *out);
  * device memory: d_out->recs with room for 2n records and the three pools
  * with their capacities; *_used returns the pool sizes.
  *   - n <= HERA_GPU_NOALLOC_MAX_PAIRS, reads <= HERA_GPU_MAX_READ bytes;
- *     larger batches fail with HERA_GPU_EINVAL.  A batch whose internal
- *     work (DP jobs, rescue calls) outgrows the static array, or whose
- *     output outgrows d_out, fails with HERA_GPU_ECAPACITY (*_used then
- *     give the pool sizes needed).
+ *     larger batches fail with HERA_GPU_EINVAL.
+ *   - A batch whose output outgrows d_out fails with HERA_GPU_ECAPACITY,
+ *     and *_used then give the pool sizes needed.  A batch whose internal
+ *     work (DP jobs, rescue calls) outgrows the static array also fails
+ *     with HERA_GPU_ECAPACITY, with *_used left at 0: align fewer pairs per
+ *     call.  So does a pair that passes a per-read capacity (its second,
+ *     wide pass would need memory of its own): hera_gpu_align_pairs_device
+ *     aligns such pairs.
+ *   - The pools are written only below the capacities given, never past.
+ *   - Every call reads the batch's byte range back from d_off and waits for
+ *     the caller's stream to do so.
  *   - The first call on a device looks up the static array's device
  *     address (cudaGetSymbolAddress); make that first call before any
  *     stream capture.
@@ -385,12 +397,27 @@ void hera_gpu_server_destroy(hera_gpu_server *s);
 /* Kernel-level check, no counterpart in hera: ssw_align (src/ssw.c:81-321)
  * as the mate-rescue kernel computes it, for n (window, read) cases given as
  * ASCII strings back to back (refs[ref_off[i] .. ref_off[i+1]), same for
- * reads; windows up to 1000 bases, reads up to HERA_GPU_MAX_READ).  Per case:
- * score, skip, and the CIGAR (ops[i*96 ..], n_ops[i]; miss[i*96 ..],
- * n_miss[i]); *flags ORs capacity flags.  Allocates device memory. */
+ * reads; windows up to 1000 bases, reads up to HERA_GPU_MAX_READ).  As in
+ * the aligner, a case whose CIGAR passes the first pass's capacities (96
+ * ops, 96 miss chars) runs again in the wide pass's form.  Per case: score,
+ * skip, and the CIGAR (ops[i*cap ..], n_ops[i]; miss[i*cap ..], n_miss[i]);
+ * *flags ORs the flags left after that.  Allocates device memory. */
 int hera_gpu_unit_ssw(int device, const char *refs, const int64_t *ref_off, const char *reads,
 		      const int64_t *read_off, int32_t n, int32_t *score, int32_t *skip, uint32_t *ops,
-		      int32_t *n_ops, char *miss, int32_t *n_miss, int32_t *flags);
+		      int32_t *n_ops, char *miss, int32_t *n_miss, int32_t cap, int32_t *flags);
+
+/* Kernel-level check, no counterpart in hera: SW_align
+ * (src/hash_align.c:627-760) as the batched form's gap-DP kernels compute
+ * it, for n (window, query, err) cases given as ASCII strings back to back
+ * (refs[ref_off[i] .. ref_off[i+1]), queries likewise, up to
+ * HERA_GPU_MAX_READ bases; err as the reference passes it, negative for a
+ * prefix DP).  write_bam is hera's WRITE_BAM (1: score-only, one M op).
+ * Per case: score and the CIGAR (ops[i*cap ..], n_ops[i]; miss[i*cap ..],
+ * n_miss[i]); *flags ORs capacity flags.  Allocates device memory. */
+int hera_gpu_unit_sw(int device, const char *refs, const int64_t *ref_off, const char *qs,
+		     const int64_t *q_off, const int32_t *err, int32_t n, int write_bam, int32_t *score,
+		     uint32_t *ops, int32_t *n_ops, char *miss, int32_t *n_miss, int32_t cap,
+		     int32_t *flags);
 
 /* Measurement helper, no counterpart in hera: the device's throughput of
  * the DPX instruction the gap DP's cell update is built on (packed 16x2

@@ -25,6 +25,10 @@ REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(REF_DIR, "libhera_oracle.so")
 REFERENCE_SO = os.path.join(REF_DIR, "libhera_ref.so")
 REFERENCE_BIN = os.path.join(REF_DIR, "hera")
+# the reference's source tree, where the checkers are built from (only in a
+# container that holds it; the GPU box uses the prebuilt oracle/_ref files)
+REF_SRC = os.environ.get("HERA_REF_SRC", "/root/reference/src")
+REF_HERA_BUILD = os.path.join(REF_SRC, "hera_build")
 
 REC_DTYPE = np.dtype([
     ("n", "<i4", (2,)), ("err", "<i4", (2,)), ("pair", "<i4"),
@@ -91,8 +95,19 @@ class Result:
         return [self.candidate(i) for i in range(self.recs.shape[0])]
 
 
-def _pool_caps(n_recs: int, total_len: int):
-    return n_recs * 64 + 1024, n_recs * 16 + total_len * 2 + 1024, total_len * 2 + 1024
+def _pool_caps(n_recs: int, total_len: int, scale: int = 1):
+    return ((n_recs * 64 + 1024) * scale, (n_recs * 16 + total_len * 2 + 1024) * scale,
+            (total_len * 2 + 1024) * scale)
+
+
+def _run_grown(n_recs: int, total_len: int, run, what: str) -> "Result":
+    """run(res) -> status, retried with larger pools while they are too
+    small (the lists of reads in large paralog families are long)."""
+    for scale in (1, 16, 256):
+        res = Result(n_recs, *_pool_caps(n_recs, total_len, scale))
+        if run(res) == 0:
+            return res
+    raise RuntimeError(f"{what} result pools too small")
 
 
 class ClassTable:
@@ -295,24 +310,18 @@ class Oracle:
         synth.ReadSet objects; their sequences are modified in place exactly
         as the reference modifies them (lower-case ACGT become upper-case)."""
         n = r1.n
-        res = Result(2 * n, *_pool_caps(2 * n, int(r1.len.sum() + r2.len.sum())))
-        rc = self.lib.ho_align_pairs(C.byref(self.cix), write_bam, n,
-                                     C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
-                                     C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
-                                     C.byref(res.c))
-        if rc != 0:
-            raise RuntimeError("oracle result pools too small")
-        return res
+        return _run_grown(2 * n, int(r1.len.sum() + r2.len.sum()), lambda res: self.lib.ho_align_pairs(
+            C.byref(self.cix), write_bam, n,
+            C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+            C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+            C.byref(res.c)), "oracle")
 
     def align_single(self, rs, write_bam: int = 1) -> Result:
         n = rs.n
-        res = Result(n, *_pool_caps(n, int(rs.len.sum())))
-        rc = self.lib.ho_align_single(C.byref(self.cix), write_bam, n,
-                                      C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
-                                      C.byref(res.c))
-        if rc != 0:
-            raise RuntimeError("oracle result pools too small")
-        return res
+        return _run_grown(n, int(rs.len.sum()), lambda res: self.lib.ho_align_single(
+            C.byref(self.cix), write_bam, n,
+            C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
+            C.byref(res.c)), "oracle")
 
     def classes(self, results, paired: bool = True) -> ClassTable:
         """add_class as the host tail calls it, over a sequence of flat
@@ -436,24 +445,18 @@ class Reference:
 
     def align_pairs(self, r1, r2, write_bam: int = 1) -> Result:
         n = r1.n
-        res = Result(2 * n, *_pool_caps(2 * n, int(r1.len.sum() + r2.len.sum())))
-        rc = self.lib.refh_align_pairs(write_bam, n,
-                                       C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
-                                       C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
-                                       C.byref(res.c))
-        if rc != 0:
-            raise RuntimeError("reference result pools too small")
-        return res
+        return _run_grown(2 * n, int(r1.len.sum() + r2.len.sum()), lambda res: self.lib.refh_align_pairs(
+            write_bam, n,
+            C.c_void_p(_ptr(r1.seq)), C.c_void_p(_ptr(r1.off)), C.c_void_p(_ptr(r1.len)),
+            C.c_void_p(_ptr(r2.seq)), C.c_void_p(_ptr(r2.off)), C.c_void_p(_ptr(r2.len)),
+            C.byref(res.c)), "reference")
 
     def align_single(self, rs, write_bam: int = 1) -> Result:
         n = rs.n
-        res = Result(n, *_pool_caps(n, int(rs.len.sum())))
-        rc = self.lib.refh_align_single(write_bam, n,
-                                        C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
-                                        C.byref(res.c))
-        if rc != 0:
-            raise RuntimeError("reference result pools too small")
-        return res
+        return _run_grown(n, int(rs.len.sum()), lambda res: self.lib.refh_align_single(
+            write_bam, n,
+            C.c_void_p(_ptr(rs.seq)), C.c_void_p(_ptr(rs.off)), C.c_void_p(_ptr(rs.len)),
+            C.byref(res.c)), "reference")
 
     def classes(self, r1, r2=None, n_trans: Optional[int] = None) -> ClassTable:
         """The reference's whole worker per read (align_pair_read, or

@@ -34,6 +34,25 @@ def config1():
 
 
 @pytest.fixture(scope="session")
+def config2s():
+    """Config 2's gene and read model on a 40 Mbp genome: 6k genes, 20k
+    transcripts, isoform families as in config 2 (the benched model at a
+    size the oracle finishes in seconds)."""
+    from hera_b200 import workloads
+    return workloads.build("config2s", device="cuda" if gpu_available() else None)
+
+
+@pytest.fixture(scope="session")
+def family():
+    """Paralog families larger than the per-read list capacities: 96
+    transcripts sharing 600 bp (a read from it has 96 hits a strand and, at
+    seed spacing 14, over 256 anchors), 40 sharing 400 bp, 30 unrelated."""
+    from hera_b200 import index, synth
+    tx = synth.family_transcriptome(21, families=((96, 600), (40, 400)), n_other=30)
+    return tx, index.build_index(tx)
+
+
+@pytest.fixture(scope="session")
 def oracle1(config1):
     import oracle
     if not os.path.exists(oracle.ORACLE_SO):

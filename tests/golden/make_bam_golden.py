@@ -39,7 +39,7 @@ def main():
     try:   # the reference's loader reads the index directory into memory
         synth.write_genome_fasta(ann, os.path.join(d, "g.fa"))
         synth.write_gtf(ann, os.path.join(d, "g.gtf"))
-        shutil.copy("/root/reference/src/hera_build", os.path.join(d, "hera_build"))
+        shutil.copy(oracle.REF_HERA_BUILD, os.path.join(d, "hera_build"))
         shutil.copy(oracle.REFERENCE_BIN, os.path.join(d, "hera"))
         subprocess.run(["python3", os.path.join(d, "hera_build"), "--fasta", os.path.join(d, "g.fa"), "--gtf",
                         os.path.join(d, "g.gtf"), "--outdir", os.path.join(d, "idx")], check=True,

@@ -103,7 +103,7 @@ def _live(d, wl, n, q, host_so=None, lower=False):
     q.put((rc, int(off[-1]), len(bad), bad_host, gm_same))
 
 
-@pytest.mark.skipif(not oracle.reference_available() or not os.path.exists("/root/reference/src/hera_build"),
+@pytest.mark.skipif(not oracle.reference_available() or not os.path.exists(oracle.REF_HERA_BUILD),
                     reason="reference not built here")
 @pytest.mark.parametrize("wl,lower", [("config1", False), ("config4", False), ("config4", True)])
 def test_bam_records_match_reference(tmp_path, host_writer, wl, lower):
@@ -115,7 +115,7 @@ def test_bam_records_match_reference(tmp_path, host_writer, wl, lower):
     d = str(tmp_path)
     synth.write_genome_fasta(ann, os.path.join(d, "g.fa"))
     synth.write_gtf(ann, os.path.join(d, "g.gtf"))
-    shutil.copy("/root/reference/src/hera_build", os.path.join(d, "hera_build"))
+    shutil.copy(oracle.REF_HERA_BUILD, os.path.join(d, "hera_build"))
     shutil.copy(oracle.REFERENCE_BIN, os.path.join(d, "hera"))
     subprocess.run(["python3", os.path.join(d, "hera_build"), "--fasta", os.path.join(d, "g.fa"), "--gtf",
                     os.path.join(d, "g.gtf"), "--outdir", os.path.join(d, "idx")], check=True, capture_output=True)

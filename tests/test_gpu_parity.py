@@ -227,3 +227,64 @@ def test_page_locked_buffers_same_records(config1, gpu_ctx1):
     finally:
         for a in arrs:
             api.host_unregister(a)
+
+
+@pytest.fixture(scope="module", params=["batched", "plain"])
+def ctx2s(request, config2s):
+    from hera_b200 import api
+    ctx = api.Context(config2s[2], path=request.param)
+    yield ctx
+    ctx.close()
+
+
+@pytest.fixture(scope="module")
+def oracle2s(config2s):
+    import oracle
+    return oracle.Oracle(config2s[2])
+
+
+@pytest.mark.parametrize("write_bam", [1, 0])
+def test_pairs_config2s(config2s, oracle2s, ctx2s, write_bam):
+    """Config 2's isoform structure (20k transcripts: buckets with several
+    entries, long occurrence lists, many-isoform merge_sort ties), 60k pairs
+    of its read model, record for record."""
+    ann, tx, _ = config2s
+    r1, r2 = workloads.pairs("config2s", ann, tx, 60000, seed=17)
+    _assert_same(ctx2s.align_pairs(r1, r2, write_bam), oracle2s.align_pairs(r1.copy(), r2.copy(), write_bam),
+                 f"config2s wb={write_bam}")
+
+
+@pytest.fixture(scope="module", params=["batched", "plain"])
+def ctx_family(request, family):
+    from hera_b200 import api
+    ctx = api.Context(family[1], path=request.param)
+    yield ctx
+    ctx.close()
+
+
+@pytest.mark.parametrize("mate2_random", [False, True])
+def test_pairs_past_list_capacities(family, ctx_family, mate2_random):
+    """Reads with 96 hits a strand and over 256 anchors at seed spacing 14,
+    among ordinary reads, and mates rescued over every family member: the
+    pairs past the first pass's per-read capacities run a second, wide pass
+    and every record equals the oracle's (no capacity error)."""
+    import oracle
+    tx, ix = family
+    orc = oracle.Oracle(ix)
+    f1, f2 = synth.family_pairs(tx, 500, seed=18, shared=600, mate2_random=mate2_random)
+    o1, o2 = synth.simulate_pairs(tx, 1500, seed=19, read_len=100, sub_rate=0.01)
+    r1, r2 = synth.concat_pairs([(f1, f2), (o1, o2)], seed=20)
+    for wb in (1, 0):
+        got = ctx_family.align_pairs(r1, r2, wb)
+        want = orc.align_pairs(r1.copy(), r2.copy(), wb)
+        assert int(want.recs["n"].max()) > 64
+        _assert_same(got, want, f"family mate2_random={mate2_random} wb={wb}")
+
+
+def test_single_past_list_capacities(family, ctx_family):
+    import oracle
+    tx, ix = family
+    orc = oracle.Oracle(ix)
+    f1, _ = synth.family_pairs(tx, 400, seed=21, shared=600)
+    for wb in (1, 0):
+        _assert_same(ctx_family.align_single(f1, wb), orc.align_single(f1.copy(), wb), f"family single wb={wb}")

@@ -32,7 +32,7 @@ def test_index_file_round_trip(tmp_path, config1):
     _same(ix, index.read_index(path))
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/src/hera_build") or
+@pytest.mark.skipif(not os.path.exists(oracle.REF_HERA_BUILD) or
                     not os.path.exists(oracle.REFERENCE_BIN), reason="reference not available")
 def test_matches_hera_index(tmp_path):
     """hera_build + `hera index` on the same genome/GTF give the same bytes."""
@@ -40,7 +40,7 @@ def test_matches_hera_index(tmp_path):
     d = tmp_path
     synth.write_genome_fasta(ann, str(d / "g.fa"))
     synth.write_gtf(ann, str(d / "g.gtf"))
-    shutil.copy("/root/reference/src/hera_build", d / "hera_build")
+    shutil.copy(oracle.REF_HERA_BUILD, d / "hera_build")
     shutil.copy(oracle.REFERENCE_BIN, d / "hera")
     r = subprocess.run(["python3", str(d / "hera_build"), "--fasta", str(d / "g.fa"), "--gtf",
                         str(d / "g.gtf"), "--outdir", str(d / "idx")], capture_output=True, text=True)

@@ -80,3 +80,28 @@ def test_em_past_minimum_rounds_matches_reference(both):
     G, OV = ref.em(t, o.ix.n_trans)
     assert np.array_equal(g.view(np.uint64), G.view(np.uint64))
     assert np.array_equal(ov.view(np.uint64), OV.view(np.uint64))
+
+
+def test_config2s_pairs_match_reference(config2s):
+    """The oracle against the reference on config 2's isoform structure
+    (6k genes, 20k transcripts), both WRITE_BAM modes."""
+    ann, tx, ix = config2s
+    o, ref = oracle.Oracle(ix), oracle.Reference(ix)
+    r1, r2 = workloads.pairs("config2s", ann, tx, 10000, seed=106)
+    for wb in (1, 0):
+        assert o.align_pairs(r1.copy(), r2.copy(), wb).canonical() == \
+            ref.align_pairs(r1.copy(), r2.copy(), wb).canonical()
+
+
+@pytest.mark.parametrize("mate2_random", [False, True])
+def test_long_lists_match_reference(family, mate2_random):
+    """Reads with 96 hits a strand (over 256 anchors at spacing 14), and
+    mates that need a rescue over every family member: the oracle's lists
+    are unbounded like the reference's."""
+    tx, ix = family
+    o, ref = oracle.Oracle(ix), oracle.Reference(ix)
+    r1, r2 = synth.family_pairs(tx, 400, seed=107, shared=600, mate2_random=mate2_random)
+    for wb in (1, 0):
+        a = o.align_pairs(r1.copy(), r2.copy(), wb)
+        assert a.canonical() == ref.align_pairs(r1.copy(), r2.copy(), wb).canonical()
+    assert int(a.recs["n"].max()) > 64

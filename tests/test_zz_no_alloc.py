@@ -5,13 +5,15 @@ align: they run inside a memory pool they do not own, or under a hard memory
 budget where a cudaMalloc would fail or synchronise the device.  For them
 the library has one entry point that allocates nothing: it runs the same
 kernels as hera_gpu_align_pairs_device with all of its working memory --
-the mate-rescue DP's matrix scratch among it -- in one static device array
-(limit: 1024 pairs per call), and writes its records into device buffers
-the caller owns.  This file checks, through the C ABI, that its records are
-identical to those of hera_gpu_align_pairs_device on two calls in a row (the
-array keeps the previous call's contents), and that oversized batches are
-refused.  It is collected last so that a run stopping at the first failure
-has already run every other test.
+DP jobs, per-pair state, queues and mate-rescue outputs -- in one static
+device array (limit: 1024 pairs per call), and writes its records into
+device buffers the caller owns.  This file checks, through the C ABI, that
+its records are identical to those of hera_gpu_align_pairs_device on two
+calls in a row (the array keeps the previous call's contents), that
+oversized batches are refused, and that a batch whose working set outgrows
+the static array fails cleanly (no pool sizes claimed) and leaves the next
+call correct.  It is collected last so that a run stopping at the first
+failure has already run every other test.
 """
 import ctypes as C
 
@@ -111,3 +113,69 @@ def test_noalloc_reports_small_output(setup):
                                                       r1.n, max_len, 1, C.byref(res), None)
     assert rc == -5
     assert res.list_used > 4
+
+
+def test_noalloc_scratch_overflow_then_normal_call(setup):
+    """1024 pairs from a sequence shared by 48 transcripts: every
+    get_position call forms 48 chains, far more than the static array holds
+    for 1024 pairs.  The call fails with HERA_GPU_ECAPACITY, says to align
+    fewer pairs, and claims no pool sizes; the next call, on ordinary
+    reads, still equals hera_gpu_align_pairs_device."""
+    torch, ann, tx, ctx = setup
+    from hera_b200 import index, synth
+    ftx = synth.family_transcriptome(5, families=((48, 600),), n_other=20)
+    fctx = api.Context(index.build_index(ftx))
+    try:
+        lib = fctx.lib
+        f1, f2 = synth.family_pairs(ftx, MAX_PAIRS, seed=6, shared=600)
+        (s, o, ln), max_len = _device_reads(torch, f1, f2)
+        res, bufs = _device_out(torch, f1.n, 64 * f1.n)
+        rc = lib.hera_gpu_align_pairs_device_noalloc(fctx.h, s.data_ptr(), o.data_ptr(), ln.data_ptr(),
+                                                     f1.n, max_len, 1, C.byref(res), None)
+        msg = lib.hera_gpu_last_error(fctx.h).decode()
+        assert rc == -5, msg
+        assert "fewer pairs" in msg, msg
+        assert res.list_used == res.op_used == res.miss_used == 0
+        # the same context, ordinary reads from its own transcripts
+        r1, r2 = synth.simulate_pairs(ftx, 300, seed=7, read_len=100, sub_rate=0.005)
+        (s, o, ln), max_len = _device_reads(torch, r1, r2)
+        fctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), r1.n, max_len, 1, None)
+        want = fctx.fetch(2 * r1.n).canonical()
+        res, bufs = _device_out(torch, r1.n, 256 * r1.n)
+        rc = lib.hera_gpu_align_pairs_device_noalloc(fctx.h, s.data_ptr(), o.data_ptr(), ln.data_ptr(),
+                                                     r1.n, max_len, 1, C.byref(res), None)
+        assert rc == 0, lib.hera_gpu_last_error(fctx.h).decode()
+        torch.cuda.synchronize()
+        assert _to_host(res, bufs, r1.n) == want
+    finally:
+        fctx.close()
+
+
+def test_noalloc_output_pools_exact_capacity(setup):
+    """Pools given exactly the sizes a batch needs are enough (nothing is
+    written at or past the capacity); one entry less is refused with the
+    sizes needed."""
+    torch, ann, tx, ctx = setup
+    r1, r2 = workloads.pairs("config1", ann, tx, 300, seed=45)
+    (s, o, ln), max_len = _device_reads(torch, r1, r2)
+    res, bufs = _device_out(torch, r1.n, 64 * r1.n)
+    rc = ctx.lib.hera_gpu_align_pairs_device_noalloc(ctx.h, s.data_ptr(), o.data_ptr(), ln.data_ptr(),
+                                                      r1.n, max_len, 0, C.byref(res), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    want = _to_host(res, bufs, r1.n)
+    need = (res.list_used, res.op_used, res.miss_used)
+    assert min(need) > 0
+    res2, bufs2 = _device_out(torch, r1.n, max(need))
+    res2.list_cap, res2.op_cap, res2.miss_cap = need
+    rc = ctx.lib.hera_gpu_align_pairs_device_noalloc(ctx.h, s.data_ptr(), o.data_ptr(), ln.data_ptr(),
+                                                      r1.n, max_len, 0, C.byref(res2), None)
+    assert rc == 0, ctx.lib.hera_gpu_last_error(ctx.h).decode()
+    torch.cuda.synchronize()
+    assert _to_host(res2, bufs2, r1.n) == want
+    res3, bufs3 = _device_out(torch, r1.n, max(need))
+    res3.list_cap, res3.op_cap, res3.miss_cap = need[0] - 1, need[1], need[2]
+    rc = ctx.lib.hera_gpu_align_pairs_device_noalloc(ctx.h, s.data_ptr(), o.data_ptr(), ln.data_ptr(),
+                                                      r1.n, max_len, 0, C.byref(res3), None)
+    assert rc == -5
+    assert (res3.list_used, res3.op_used, res3.miss_used) == need
