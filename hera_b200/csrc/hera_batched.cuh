@@ -588,12 +588,13 @@ __device__ __forceinline__ int job_form(const DpJob &j)
 }
 
 // one thread per job, jobs in (error cap, length) order; threads whose job
-// is not of cap E leave at once (whole warps, the order is by cap).  Every
-// row is kept (4 bits a slot, in local memory), so a DP that stops early runs
-// its shrink loop in place: in the score-only mode 18% of the error-8 calls
-// stop early, nearly every warp holds one, and a rerun would redo the DP.
+// is not of cap E leave at once (whole warps, the order is by cap).  The
+// DP runs in the bit-plane form (sw_align_bits).  Every row is kept (4 bits
+// a slot, in local memory), so a DP that stops early runs its shrink loop in
+// place: in the score-only mode 18% of the error-8 calls stop early, nearly
+// every warp holds one, and a rerun would redo the DP.
 template <int E>
-__global__ void __launch_bounds__(128, E == 4 ? 8 : 6)
+__global__ void __launch_bounds__(128, 8)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
 	 int rcap)
 {
@@ -602,7 +603,7 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
 		const DpJob jb = jobs[id];
-		__align__(16) uint32_t rows[(MAX_DP_ROWS + 1) * ((2 * E + 2 + 7) / 8)];
+		typename BitRows<E>::T rows[MAX_DP_ROWS + 1];
 		DCig cig;
 		int flags = 0;
 		cig.n = cig.nm = 0;
@@ -610,8 +611,7 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
 		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
 		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-		const int score = sw_align_reg<E, true>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig,
-							reinterpret_cast<uint8_t *>(rows), flags, cells);
+		const int score = sw_align_bits<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, cells);
 		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
 		flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
 	}

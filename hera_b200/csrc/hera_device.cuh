@@ -594,6 +594,261 @@ __device__ inline int sw_align_reg(const RefWin &r, QView qc, uint32_t ref_len, 
 	}
 }
 
+// ---------------------------------------------------------------------
+// Gap DP, bit-plane form.  Same semantics as sw_align_reg (and so as
+// SW_align) for the two live error caps, with a row's W = 2*error + 2
+// diagonal slots held as thermometer bit planes: bit q of plane t is set
+// when slot q's value is >= t.  Values never exceed error + 2 (the left
+// edge, one more than a break or j marker above it), so planes t = 1 ..
+// error + 2 hold a row exactly.  In this form a cell's min is an AND, +1
+// renames planes, and the left-neighbour term of the recurrence,
+// V[q] = min(T[q], V[q-1] + 1), unrolls plane by plane to
+// A_t = T_t & ((A_{t-1} << 1) | 1): a whole row is a few word operations
+// per plane instead of ~20 predicated operations per slot.  The left edge,
+// the break marker, the row's min / rightmost xmin, the j marker, ferr and
+// the advance of s are masks and bit scans over single words.  Rows are
+// kept in binary (as planes of the 4-bit values) for the early-stop shrink
+// loop and the traceback.
+// ---------------------------------------------------------------------
+template <int E>
+struct BitRows;
+template <>
+struct BitRows<8> {            // W = 18: planes b0..b3 of 18 bits, 16 bytes a row
+	using T = uint4;
+	static __device__ __forceinline__ T pack(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3)
+	{
+		return make_uint4(b0, b1, b2, b3);
+	}
+	static __device__ __forceinline__ unsigned at(const T &r, int q)
+	{
+		return ((r.x >> q) & 1u) | (((r.y >> q) & 1u) << 1) | (((r.z >> q) & 1u) << 2) | (((r.w >> q) & 1u) << 3);
+	}
+};
+template <>
+struct BitRows<4> {            // W = 10, values <= 6: planes b0..b2 in one word, 4 bytes a row
+	using T = uint32_t;
+	static __device__ __forceinline__ T pack(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t)
+	{
+		return b0 | (b1 << 10) | (b2 << 20);
+	}
+	static __device__ __forceinline__ unsigned at(const T &r, int q)
+	{
+		return ((r >> q) & 1u) | (((r >> (q + 10)) & 1u) << 1) | (((r >> (q + 20)) & 1u) << 2);
+	}
+};
+
+template <int E, class Cig>
+__device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
+				    bool score_only, Cig &cig, typename BitRows<E>::T *__restrict__ rows, int &flags,
+				    uint32_t &cells)
+{
+	constexpr int W = 2 * E + 2;
+	constexpr int NT = E + 2;              // planes t = 1 .. error + 2
+	constexpr uint32_t FULL = (1u << W) - 1;
+	constexpr unsigned error = E;
+	using RB = BitRows<E>;
+	// reference code at window position x, clamped (values outside the
+	// window are never used, the clamp only keeps the address valid)
+	auto rcode = [&](int x) -> uint32_t {
+		x = x < 0 ? 0 : (x >= (int)ref_len ? (int)ref_len - 1 : x);
+		return r.c(x);
+	};
+	// a thermometer row stored as planes of its binary values
+	auto store = [&](int k, const uint32_t (&G)[NT + 1]) {
+		uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+#pragma unroll
+		for (int t = 1; t <= NT; ++t) {
+			const uint32_t only = G[t] & ~(t < NT ? G[t + 1] : 0u);   // value == t
+			if (t & 1) b0 |= only;
+			if (t & 2) b1 |= only;
+			if (t & 4) b2 |= only;
+			if (t & 8) b3 |= only;
+		}
+		rows[k] = RB::pack(b0, b1, b2, b3);
+	};
+	auto get = [&](int k, int c) -> unsigned {
+		const int q = c - k + E;
+		return (q >= 0 && q < W) ? RB::at(rows[k], q) : 0u;
+	};
+	// reference codes of row k's slots (x = k + q - error - 1) as three
+	// planes; row 1 first
+	uint32_t R0 = 0, R1 = 0, R2 = 0;
+#pragma unroll
+	for (int q = 0; q < W; ++q) {
+		const uint32_t c = rcode(q - E);
+		R0 |= (c & 1u) << q;
+		R1 |= ((c >> 1) & 1u) << q;
+		R2 |= ((c >> 2) & 1u) << q;
+	}
+	// row 0: slot q holds q - error (M[0][c] = c for c <= error + 1), 0 left of it
+	uint32_t G[NT + 1];
+	G[0] = FULL;
+#pragma unroll
+	for (int t = 1; t <= NT; ++t)
+		G[t] = (E + t < W) ? (FULL & ~((1u << (E + t)) - 1)) : 0u;
+	store(0, G);
+
+	int s = 0, ferr = -1, k, i = 0;
+	unsigned min = 0, xmin = 0;
+	for (k = 1; k <= (int)len; ++k) {
+		if (k > 1) {   // slide the reference planes one slot
+			const uint32_t c = rcode(k + W - E - 2);
+			R0 = (R0 >> 1) | ((c & 1u) << (W - 1));
+			R1 = (R1 >> 1) | (((c >> 1) & 1u) << (W - 1));
+			R2 = (R2 >> 1) | (((c >> 2) & 1u) << (W - 1));
+		}
+		const uint32_t qk = qc(k - 1);
+		const int qs = s - k + E;              // slot of the left edge
+		if (qs < 0) {   // outside the proven band: cannot happen
+			flags |= F_BAND;
+			return 0;
+		}
+		const uint32_t EQ = 1u << qs;
+		const uint32_t LT = EQ - 1, LE = (EQ << 1) - 1;
+		const int qr = (int)ref_len - k + E;   // last slot with c <= ref_len
+		const uint32_t RL = qr >= W - 1 ? FULL : (qr < 0 ? 0u : (2u << qr) - 1);
+		// the break: first slot past the left edge (within the window) whose
+		// diagonal neighbour is error + 1
+		const uint32_t BR = G[E + 1] & ~LE & RL;
+		const uint32_t BM = BR & (0u - BR);
+		const uint32_t COMP = ~LE & RL & (BM ? BM - 1 : FULL);   // the cells the row computes
+		// mismatch slots; the penalty only where the diagonal is < error
+		const uint32_t MM = (R0 ^ (0u - (qk & 1u))) | (R1 ^ (0u - ((qk >> 1) & 1u))) |
+				    (R2 ^ (0u - ((qk >> 2) & 1u)));
+		const uint32_t PEN = MM & ~G[E];
+		// T = min(diag + pen, up + 1); slots left of the edge infinite, the
+		// edge up + 1; then the left-neighbour prefix, plane by plane
+		uint32_t V[NT + 1];
+		V[0] = FULL;
+		uint32_t A = FULL;
+#pragma unroll
+		for (int t = 1; t <= NT; ++t) {
+			const uint32_t DG = t <= E ? (G[t] | (PEN & G[t - 1])) : G[t];
+			const uint32_t U = t == 1 ? FULL : ((G[t - 1] >> 1) & FULL);
+			const uint32_t T = (DG | LE) & (U | LT);
+			A = T & ((A << 1) | 1u);
+			V[t] = A;
+		}
+		// the written row: the edge and the computed cells, the break
+		// marker error + 1, zero elsewhere
+		const uint32_t LIVE = COMP | EQ;
+#pragma unroll
+		for (int t = 1; t <= NT; ++t)
+			V[t] = (V[t] & LIVE) | (t <= E + 1 ? BM : 0u);
+		i = BM ? k + (__ffs(BM) - 1) - E : (int)ref_len + 1;
+		cells += i > s + 1 ? (uint32_t)(i - s - 1) : 0u;   // the cells the reference visits
+		// min (from error) and the rightmost slot holding it, over the
+		// computed cells (their values are <= error)
+		min = error;
+		uint32_t XM = COMP;
+#pragma unroll
+		for (int t = E; t >= 1; --t) {
+			const uint32_t X = ~V[t] & COMP;   // cells < t
+			if (X) {
+				min = (unsigned)(t - 1);
+				XM = X;
+			}
+		}
+		if (COMP)
+			xmin = (unsigned)(k + (31 - __clz(XM)) - E);
+		// j: the first cell == error after the last cell < error
+		const uint32_t LTE = ~V[E] & COMP, EQE = V[E] & COMP;
+		const uint32_t above = LTE ? ~((2u << (31 - __clz(LTE))) - 1) : 0xffffffffu;
+		const uint32_t JC = EQE & above;
+		const int j = JC ? k + (__ffs(JC) - 1) - E : 0;
+		if (ferr == -1 && ((COMP & V[1]) >> E) & 1u)   // slot error is column k
+			ferr = k;
+		if (min != error) {
+			// while (M[k][s] >= error && s < i) ++s
+			const uint32_t run = ~(V[E] >> qs);
+			const int n = __ffs(run) - 1;
+			s = s + n < i ? s + n : (i > s ? i : s);
+			if ((unsigned)j > xmin && (unsigned)j < ref_len) {
+				const uint32_t JM = 1u << (j - k + E);
+#pragma unroll
+				for (int t = 1; t <= NT; ++t)
+					V[t] = t <= E + 1 ? (V[t] | JM) : (V[t] & ~JM);
+			}
+		}
+#pragma unroll
+		for (int t = 1; t <= NT; ++t)
+			G[t] = V[t];
+		store(k, G);
+		if (min == error) {
+			++k;
+			break;
+		}
+	}
+	--k;
+
+	int score = 0;
+	if (min >= error) {
+		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+			--k;
+			// The reference scans row k from column 0 to its break.  Cells
+			// left of the window are zero there and here (no effect: jj
+			// stays 0), and the break marker or ref_len lies inside the
+			// window, so the scan covers the window only.
+			int jj = 0;
+			const int c_lo = k - E > 0 ? k - E : 0;
+			const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
+			for (int c = c_lo; c < c_hi; ++c) {
+				const unsigned v = get(k, c);
+				if (v == error + 1)
+					break;
+				if (v > 0)
+					jj = (int)error;
+				if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
+					min = v;
+					xmin = (unsigned)c;
+				}
+			}
+		}
+		if (k < 5) {
+			cig_add(cig, OP_S, len, nullptr, flags);
+			return (int)len;
+		}
+		cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
+		score = (int)len - k;
+		i = k;
+	} else {
+		if (xmin < len && k == (int)len) {
+			min += len - xmin;
+			xmin = len;
+		}
+		i = (int)len;
+	}
+	k = (int)xmin;
+	score += (int)min;
+	if (score_only) {
+		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
+		return score;
+	}
+	while (i > 0 && k > 0) {
+		const unsigned cur = get(i, k);
+		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
+		if (cur == get(i - 1, k - 1) + pen) {
+			if (pen == 0)
+				cig_add(cig, OP_M, 1, nullptr, flags);
+			else
+				cig_add(cig, OP_X, 1, r.a(k - 1), flags);
+			--i;
+			--k;
+		} else if (cur == get(i - 1, k) + 1) {
+			cig_add(cig, OP_I, 1, nullptr, flags);
+			--i;
+		} else {
+			cig_add(cig, OP_D, 1, r.a(k - 1), flags);
+			--k;
+		}
+	}
+	if (i > 0)
+		cig_add(cig, OP_I, (unsigned)i, nullptr, flags);
+	for (int t = 1; t <= k; ++t)
+		cig_add(cig, OP_D, 1, r.a(k - t), flags);
+	return score;
+}
+
 // Entry used by the per-task (plain) path: the banded form, which keeps the
 // register footprint small where neighbouring threads diverge.  The batched
 // path runs sw_align_reg on length-sorted jobs instead.  q: oriented read
