@@ -12,9 +12,17 @@ Candidate records inside the timed region).  Under torchrun each rank runs a
 replica of the index on its own GPU over its own chunks (weak scaling, no
 data-path collective); the reported time is the max over ranks.
 
+Besides the headline, the default run checks the last timed step's records
+against the oracle on a sample (`bit_exact`, outside the timed region) and
+adds legs: the drop-in Candidate call, the -w tail's BAM records, FASTQ
+chunk text -> records, add_class and the EM, config 3 (mixed lengths,
+batched vs plain, single-end reads), config 4 (high divergence, mate-rescue
+roofline) and the config-5 serving loop with each sample's EM checked bit for
+bit against the oracle's.
+
 `--impl reference` times the reference program's own CPU implementation of
 the same path (oracle/_ref/libhera_ref.so: check_in_transcriptome +
-intersect2 per pair) on all host cores over bounded samples of the workload.
+intersect2 per pair) on all host cores, on steps of the same size.
 """
 from __future__ import annotations
 
@@ -48,7 +56,9 @@ def parse():
     ap.add_argument("--chunk", type=int, default=1_000_000)
     ap.add_argument("--distinct", type=int, default=3, help="distinct chunks generated per rank")
     ap.add_argument("--write-bam", type=int, default=1, help="hera WRITE_BAM (1 = no -w)")
-    ap.add_argument("--cpu-sample", type=int, default=200_000, help="pairs per CPU-baseline slice")
+    ap.add_argument("--cpu-sample", type=int, default=200_000,
+                    help="pairs per slice of the in-run CPU baseline (the reference arm times whole "
+                         "--chunk steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--paths", default="plain,batched", help="execution forms to time (batched last)")
@@ -61,8 +71,15 @@ def parse():
                     help="time only the BAM-record leg (the -w tail's records on the device; one JSON line)")
     ap.add_argument("--pin-tuning", default="", help="BUILD_BLOCKS_PER_SM,RESCUE_WARPS_PER_BLOCK: "
                     "fixed launch shapes instead of the autotuner (reproducible profiles)")
-    ap.add_argument("--serve-scale", type=float, default=0.125,
+    ap.add_argument("--serve-scale", type=float, default=1.0,
                     help="sample sizes of the serving leg as a fraction of 0.5M-8M pairs")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle checks of the timed records")
+    ap.add_argument("--parity-pairs", type=int, default=20_000,
+                    help="pairs of the last timed step checked against the oracle")
+    ap.add_argument("--no-config-legs", action="store_true", help="skip the config-3 and config-4 legs")
+    ap.add_argument("--no-bam", action="store_true", help="skip the BAM-record leg")
+    ap.add_argument("--leg-pairs", type=int, default=500_000, help="pairs per step of the config-3/4 legs")
+    ap.add_argument("--leg-steps", type=int, default=5, help="timed steps of the config-3/4 legs")
     return ap.parse_args()
 
 
@@ -184,7 +201,7 @@ def run_reference(args):
     log(f"index {time.time() - t:.1f}s")
     ref = oracle.Reference(ix)
     threads = os.cpu_count() or 1
-    sample = args.cpu_sample
+    sample = args.chunk   # the same pairs per step as the device arm
     chunks = make_chunks(args.workload, ann, tx, sample, min(args.distinct, args.steps + args.warmup), 1000)
     times = []
     for s in range(args.warmup + args.steps):
@@ -203,7 +220,8 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic",
         "config": {"workload": f"{args.workload}: {workloads.DESCRIPTION[args.workload]}",
-                   "pairs_per_step": sample, "write_bam": args.write_bam},
+                   "pairs_per_step": sample, "write_bam": args.write_bam,
+                   "parallelism": f"replicas x{args.gpus}"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{sample} pairs per step, reference code on {threads} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -217,6 +235,104 @@ def _maybe_cuda():
         return "cuda" if torch.cuda.is_available() else None
     except Exception:
         return None
+
+
+def to_device(chunks):
+    """Device-resident copies of the chunks (mates interleaved), the layout
+    of the device-resident entry point."""
+    import torch
+    from hera_b200 import workloads
+    dev, max_len = [], 0
+    for r1, r2 in chunks:
+        seq, off, lens = workloads.interleave(r1, r2)
+        max_len = max(max_len, int(lens.max()))
+        dev.append((torch.from_numpy(seq).cuda(), torch.from_numpy(off).cuda(), torch.from_numpy(lens).cuda()))
+    torch.cuda.synchronize()
+    return dev, max_len
+
+
+def measure(ix, dev, max_len, chunk, path, args, local, world, steps=None, warmup=None):
+    """`steps` device-resident calls of `chunk` pairs on one context, timed
+    with CUDA events on the context's stream (max over ranks).  Returns the
+    context (its last call's records still on the device) and the numbers."""
+    import torch
+    import torch.distributed as dist
+    from hera_b200 import api, shard
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    # the plain form is one pass per chunk: one lane
+    lanes = 1 if path == "plain" else args.lanes
+    ctx = api.Context(ix, device=local, path=path, lanes=lanes, max_batch=chunk if path == "plain" else 0)
+    if args.pin_tuning:
+        ctx.set_tuning(*[int(x) for x in args.pin_tuning.split(",")])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step(i):
+        s, o, ln = dev[i % len(dev)]
+        ctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), chunk, max_len, args.write_bam,
+                               ctx.stream)
+
+    for i in range(warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    stage = {k: 0.0 for k in STAGES}
+    counts = {k: 0 for k in COUNTS}
+    launches, jobs, calls, lookups, wide = 0, 0, 0, 0, 0
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    torch.cuda.synchronize()
+    evs[0].record(stream)
+    for i in range(steps):
+        step(i)
+        evs[i + 1].record(stream)
+        tm = ctx.timing()
+        launches += int(tm["launches"])
+        jobs += int(tm["dp_jobs"])
+        calls += int(tm["dp_calls"])
+        lookups += int(tm["lookups"])
+        wide += int(tm["wide_items"])
+        for k in stage:
+            stage[k] += float(tm[k])
+        for k in counts:
+            counts[k] += int(tm[k])
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    ms = evs[0].elapsed_time(evs[-1])
+    ms = shard.max_over_ranks(ms, device="cuda")
+    if world > 1:
+        dist.barrier()
+    out = {"path": path, "ms": ms, "per_step_ms": per, "stage": stage, "launches": launches,
+           "dp_jobs": jobs, "dp_calls": calls, "lookups": lookups, "counts": counts, "wide_items": wide,
+           "clocks": clocks, "last": (steps - 1) % len(dev), "steps": steps,
+           "value": chunk * steps * world / (ms / 1000.0)}
+    return ctx, out
+
+
+def bit_exact(ctx, orc, chunk_pairs, n_pairs, k, write_bam):
+    """The records of the context's last device-resident call against the
+    oracle (the reference's algorithm restated in C), on the first k pairs
+    of that call's chunk: checked outside the timed region."""
+    r1, r2 = chunk_pairs
+    k = min(k, r1.n)
+    res = ctx.fetch(2 * n_pairs)
+    idx = np.arange(k)
+    want = orc.align_pairs(r1.subset(idx), r2.subset(idx), write_bam)
+    got = res.canonical(0, 2 * k)
+    exp = want.canonical()
+    bad = sum(1 for a, b in zip(got, exp) if a != b)
+    return {"bit_exact": bad == 0 and len(got) == len(exp), "pairs_checked": k, "records_differing": bad}
+
+
+def leg_summary(m):
+    per = sorted(m["per_step_ms"])
+    return {"value": m["value"], "ms_per_step": m["ms"] / m["steps"], "gpu_launches": m["launches"],
+            "wide_pass_pairs": m["wide_items"],
+            "stage_ms_per_step": {k: round(v / m["steps"], 4) for k, v in m["stage"].items()},
+            "p50_ms": per[len(per) // 2]}
 
 
 def main():
@@ -237,7 +353,7 @@ def main():
     from hera_b200 import shard
     t = time.time()
     ann, tx, ix = workloads.build(args.workload, device=f"cuda:{local}")
-    log(f"[{rank}] index: {ix.n_trans} transcripts, {ix.buckets.shape[0]} k-mers, "
+    log(f"[{rank}] index: {ix.n_trans} transcripts, {int(ix.length.sum())} bases, {ix.buckets.shape[0]} k-mers, "
         f"{ix.n_pos} occurrences in {time.time() - t:.1f}s")
     if args.fastq_only:
         r1, r2 = workloads.pairs(args.workload, ann, tx, args.chunk, seed=100 + 1000 * rank)
@@ -250,99 +366,31 @@ def main():
                           "config": {"workload": args.workload, "pairs_per_step": args.chunk}}), flush=True)
         return
     chunks = make_chunks(args.workload, ann, tx, args.chunk, args.distinct, 100 + 1000 * rank)
-
-    # device-resident copies (mates interleaved) for the `value` measurement
-    dev = []
-    max_len = 0
-    for r1, r2 in chunks:
-        seq, off, lens = workloads.interleave(r1, r2)
-        max_len = max(max_len, int(lens.max()))
-        dev.append((torch.from_numpy(seq).cuda(), torch.from_numpy(off).cuda(),
-                    torch.from_numpy(lens).cuda()))
-    torch.cuda.synchronize()
-
-    def pin(c):
-        if args.pin_tuning:
-            c.set_tuning(*[int(x) for x in args.pin_tuning.split(",")])
-        return c
-
-    def measure(path):
-        # the plain form is one pass per chunk: one lane
-        lanes = 1 if path == "plain" else args.lanes
-        ctx = pin(api.Context(ix, device=local, path=path, lanes=lanes, max_batch=args.chunk if path == "plain" else 0))
-        stream = torch.cuda.ExternalStream(ctx.stream)
-
-        def step(i):
-            s, o, ln = dev[i % len(dev)]
-            ctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
-                                   args.write_bam, ctx.stream)
-
-        for i in range(args.warmup):
-            step(i)
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        sampler = ClockSampler(local)
-        sampler.start()
-        stage = {k: 0.0 for k in STAGES}
-        counts = {k: 0 for k in COUNTS}
-        launches, jobs, calls, lookups = 0, 0, 0, 0
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-        torch.cuda.synchronize()
-        evs[0].record(stream)
-        for i in range(args.steps):
-            step(i)
-            evs[i + 1].record(stream)
-            tm = ctx.timing()
-            launches += int(tm["launches"])
-            jobs += int(tm["dp_jobs"])
-            calls += int(tm["dp_calls"])
-            lookups += int(tm["lookups"])
-            for k in stage:
-                stage[k] += float(tm[k])
-            for k in counts:
-                counts[k] += int(tm[k])
-        torch.cuda.synchronize()
-        clocks = sampler.stop()
-        per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
-        ms = evs[0].elapsed_time(evs[-1])
-        ms = shard.max_over_ranks(ms, device="cuda")
-        if world > 1:
-            dist.barrier()
-        out = {"path": path, "ms": ms, "per_step_ms": per, "stage": stage, "launches": launches,
-               "dp_jobs": jobs, "dp_calls": calls, "lookups": lookups, "counts": counts,
-               "clocks": clocks}
-        return ctx, out
-
-    def kernel_pass():
-        """One step on a single-lane context, so each kernel's CUDA-event
-        duration is its own (the timed run overlaps three lanes)."""
-        kctx = pin(api.Context(ix, device=local, path="batched", lanes=1))
-        s, o, ln = dev[0]
-        for _ in range(2):
-            kctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
-                                    args.write_bam, kctx.stream)
-        torch.cuda.synchronize()
-        tm = kctx.timing()
-        cls = None
-        if rank == 0 and world == 1:
-            try:
-                cls = classes_leg(kctx, args.chunk, ix.length)
-            except Exception as e:
-                log(f"classes leg failed: {e}")
-                cls = {"error": str(e)}
-        kctx.close()
-        return tm, cls
+    dev, max_len = to_device(chunks)
+    solo = rank == 0 and world == 1
+    orc = None
+    if solo and not args.no_parity:
+        try:
+            import oracle   # the checker: outside every timed region
+            orc = oracle.Oracle(ix)
+        except Exception as e:
+            log(f"oracle unavailable: {e}")
 
     paths = [p for p in args.paths.split(",") if p]
-    plain = None
+    plain = parity_plain = None
     if "plain" in paths:
-        ctx_p, plain = measure("plain")
+        ctx_p, plain = measure(ix, dev, max_len, args.chunk, "plain", args, local, world)
+        if orc is not None:
+            parity_plain = bit_exact(ctx_p, orc, chunks[plain["last"]], args.chunk, args.parity_pairs,
+                                     args.write_bam)
         ctx_p.close()
     main_path = "batched" if "batched" in paths else "plain"
-    ctx, batched = measure(main_path)
-    value = args.chunk * args.steps * world / (batched["ms"] / 1000.0)
-    plain_value = args.chunk * args.steps * world / (plain["ms"] / 1000.0) if plain else None
+    ctx, batched = measure(ix, dev, max_len, args.chunk, main_path, args, local, world)
+    value = batched["value"]
+    parity = None
+    if orc is not None:
+        parity = bit_exact(ctx, orc, chunks[batched["last"]], args.chunk, args.parity_pairs, args.write_bam)
+        log(f"parity ({main_path}, last step, first {parity['pairs_checked']} pairs): {parity}")
 
     # end to end through the public C ABI with host buffers
     e2e = None
@@ -372,9 +420,14 @@ def main():
                "host_memory": "reads and result pools page-locked (registered once before timing)"}
         for a in pinned:
             api.host_unregister(a)
+        if solo:
+            try:
+                e2e["dropin"] = dropin_bench(ctx, chunks[0], args)
+            except Exception as e:
+                e2e["dropin"] = {"error": str(e)}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if solo and not args.no_cpu_baseline:
         try:
             cpu = cpu_baseline(ix, chunks, args.cpu_sample, args.write_bam)
         except Exception as e:   # the checker is optional on a box without it
@@ -383,26 +436,43 @@ def main():
     st = batched["stage"]
     tuning = ctx.tuning() if main_path == "batched" else None
     ctx.close()
-    ktm, classes = kernel_pass() if main_path == "batched" else (None, None)
+    ktm, classes = kernel_pass(ix, dev[0], max_len, args, local, rank, world) if main_path == "batched" \
+        else (None, None)
     dpx = api.dpx_peak(local)
     pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
-    roof, roof_seed, roof_rescue = roofline(ktm, dpx, args, pair_bytes, max_len)
+    roof, roof_seed, roof_rescue = roofline(ktm, dpx, args.chunk, pair_bytes, max_len)
+    del dev
 
-    fastq = None
-    if rank == 0 and world == 1 and not args.no_fastq:
-        try:
-            fastq = fastq_bench(args, ix, chunks[0], local)
-        except Exception as e:
-            log(f"fastq leg failed: {e}")
-            fastq = {"error": str(e)}
-
-    serving = None
-    if rank == 0 and world == 1 and not args.no_serve:
-        try:
-            serving = serve_bench(args, local)
-        except Exception as e:
-            log(f"serving leg failed: {e}")
-            serving = {"error": str(e)}
+    legs = {}
+    if solo:
+        for name, fn in (("bam", lambda: None if args.no_bam else bam_bench(args, ix, ann, chunks[0], local)),
+                         ("fastq", lambda: None if args.no_fastq else fastq_bench(args, ix, chunks[0], local))):
+            try:
+                legs[name] = fn()
+            except Exception as e:
+                log(f"{name} leg failed: {e}")
+                legs[name] = {"error": str(e)}
+        del orc, chunks
+        if not args.no_config_legs or not args.no_serve:
+            ann1, tx1, ix1 = workloads.build("config1", device=f"cuda:{local}")
+            orc1 = None
+            if not args.no_parity:
+                try:
+                    import oracle
+                    orc1 = oracle.Oracle(ix1)
+                except Exception as e:
+                    log(f"oracle unavailable: {e}")
+            for name, fn in (("config3", lambda: None if args.no_config_legs else
+                              config3_leg(args, ann1, tx1, ix1, orc1, local)),
+                             ("config4", lambda: None if args.no_config_legs else
+                              config4_leg(args, ann1, tx1, ix1, orc1, local, dpx)),
+                             ("serving", lambda: None if args.no_serve else
+                              serve_bench(args, ann1, tx1, ix1, orc1, local))):
+                try:
+                    legs[name] = fn()
+                except Exception as e:
+                    log(f"{name} leg failed: {e}")
+                    legs[name] = {"error": str(e)}
 
     if rank == 0:
         per = sorted(batched["per_step_ms"])
@@ -412,28 +482,153 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {workloads.DESCRIPTION[args.workload]}",
                        "pairs_per_step": args.chunk, "write_bam": args.write_bam,
-                       "path": ("batched (build / length-binned DP jobs / replay rounds)"
-                                if main_path == "batched" else "plain (thread per call / pair)"),
-                       "l2": "inputs larger than L2 (reads 200 MB/step, index in HBM)",
                        "parallelism": f"replicas x{world}"},
-            "latency_ms": {"p50": per[len(per) // 2], "p99": per[min(len(per) - 1, int(0.99 * len(per)))]},
+            "bit_exact": None if parity is None else parity["bit_exact"],
+            "parity": {main_path: parity, "plain": parity_plain},
             "plain": None if plain is None else {
-                "value": plain_value, "ms_per_step": plain["ms"] / args.steps,
-                "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
-                "gpu_launches": plain["launches"]},
-            "stage_ms_per_step": {k: v / args.steps for k, v in st.items()},
-            "dp_jobs_per_step": batched["dp_jobs"] // args.steps,
-            "dp_calls_per_step": batched["dp_calls"] // args.steps,
-            "roofline": roof, "roofline_seed": roof_seed, "roofline_rescue": roof_rescue,
+                "value": plain["value"], "ms_per_step": plain["ms"] / args.steps,
+                "batched_over_plain": value / plain["value"], "gpu_launches": plain["launches"]},
+            "roofline": _short_roof(roof), "roofline_seed": _short_roof(roof_seed),
+            "roofline_rescue": _short_roof(roof_rescue),
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": batched["launches"], "clocks": batched["clocks"],
+            "setup": {"path": ("batched (build / length-binned DP jobs / replay rounds)"
+                               if main_path == "batched" else "plain (thread per call / pair)"),
+                      "l2": "inputs larger than L2 (reads 200 MB/step, index in HBM)"},
+            "latency_ms": {"p50": per[len(per) // 2], "p99": per[min(len(per) - 1, int(0.99 * len(per)))]},
+            "wide_pass_pairs": batched["wide_items"],
             "kernel_ms_per_step": None if ktm is None else {
                 k: round(float(ktm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
                                                      "rescue_kernel_ms", "resolve_ms", "pack_ms")},
-            "tuning": tuning, "serving": serving, "fastq": fastq, "classes": classes, "cpu_baseline": cpu,
-            "e2e": e2e, "gpu_launches": batched["launches"], "clocks": batched["clocks"],
+            "stage_ms_per_step": {k: round(v / args.steps, 4) for k, v in st.items()},
+            "plain_stage_ms_per_step": None if plain is None else
+            {k: round(v / args.steps, 4) for k, v in plain["stage"].items()},
+            "dp_jobs_per_step": batched["dp_jobs"] // args.steps,
+            "dp_calls_per_step": batched["dp_calls"] // args.steps,
+            "roofline_detail": {"dp": roof, "seed": roof_seed, "rescue": roof_rescue},
+            "tuning": tuning, "classes": classes, **legs,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _short_roof(r):
+    if r is None:
+        return None
+    return {k: r.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "traffic", "kernel")}
+
+
+def kernel_pass(ix, dv, max_len, args, local, rank, world):
+    """One step on a single-lane context, so each kernel's CUDA-event
+    duration is its own (the timed run overlaps several lanes)."""
+    import torch
+    from hera_b200 import api
+    kctx = api.Context(ix, device=local, path="batched", lanes=1)
+    if args.pin_tuning:
+        kctx.set_tuning(*[int(x) for x in args.pin_tuning.split(",")])
+    s, o, ln = dv
+    for _ in range(2):
+        kctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), args.chunk, max_len,
+                                args.write_bam, kctx.stream)
+    torch.cuda.synchronize()
+    tm = kctx.timing()
+    cls = None
+    if rank == 0 and world == 1:
+        try:
+            cls = classes_leg(kctx, args.chunk, ix.length)
+        except Exception as e:
+            log(f"classes leg failed: {e}")
+            cls = {"error": str(e)}
+    kctx.close()
+    return tm, cls
+
+
+def dropin_bench(ctx, chunk, args, k: int = 200_000):
+    """hera's own call shape: reads as struct read_inf, results as
+    heap-allocated Candidate pairs for the unchanged host tail
+    (hera_gpu_align_pairs), on the first k pairs of a chunk; the Candidates
+    are freed afterwards as hera's destroy_candidate would."""
+    r1, r2 = chunk
+    idx = np.arange(min(k, r1.n))
+    a, b = r1.subset(idx), r2.subset(idx)
+    ctx.align_pairs_dropin(a, b, args.write_bam)   # warm
+    ms = ctx.align_pairs_dropin(a, b, args.write_bam)
+    return {"value": a.n / (ms / 1e3), "unit": UNIT, "pairs": a.n, "call_ms": round(ms, 3),
+            "path": "hera_gpu_align_pairs: read_inf in, malloc'd Candidates out (freed after the clock)"}
+
+
+def config3_leg(args, ann, tx, ix, orc, local):
+    """Config 3's batching comparison: mixed 50/75/100/150 bp reads (1:1:2:1)
+    on the config-1 index, half in pairs and half single-end.  Pairs: the
+    batched form (length-binned persistent build, autotuned launch shapes)
+    against the plain one-launch-per-chunk form, device-resident, records
+    checked against the oracle on a sample.  Single-end reads: through the
+    flat C ABI (host buffers; align_single_read's two get_position calls)."""
+    from hera_b200 import api, workloads
+    n = args.leg_pairs
+    chunks = make_chunks("config3", ann, tx, n, 2, 3000)
+    dev, max_len = to_device(chunks)
+    out = {"workload": f"config3: {workloads.DESCRIPTION['config3']}", "pairs_per_step": n}
+    for path in ("plain", "batched"):
+        ctx, m = measure(ix, dev, max_len, n, path, args, local, 1, steps=args.leg_steps)
+        out[path] = leg_summary(m)
+        if orc is not None:
+            out[path].update(bit_exact(ctx, orc, chunks[m["last"]], n, args.parity_pairs // 4, args.write_bam))
+        ctx.close()
+    out["batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
+    rs = workloads.singles("config3", tx, n, 3100)
+    ctx = api.Context(ix, device=local)
+    try:
+        got = ctx.align_single(rs, args.write_bam)   # warm
+        t0 = time.perf_counter()
+        for _ in range(args.leg_steps):
+            got = ctx.align_single(rs, args.write_bam)
+        wall = time.perf_counter() - t0
+        single = {"reads_per_s": n * args.leg_steps / wall, "reads_per_step": n,
+                  "path": "hera_gpu_align_single_flat (host buffers)"}
+        if orc is not None:
+            k = min(args.parity_pairs // 4, n)
+            sub = rs.subset(np.arange(k))
+            single["bit_exact"] = got.canonical(0, k) == orc.align_single(sub, args.write_bam).canonical()
+            single["reads_checked"] = k
+        out["single"] = single
+    finally:
+        ctx.close()
+    return out
+
+
+def config4_leg(args, ann, tx, ix, orc, local, dpx):
+    """Config 4, high divergence: 2x150 bp, 3% substitutions, 0.5% 1-8 bp
+    indels, 5% pairs from mutated unannotated loci (they fall through
+    unmapped and take the mate rescue); batched and plain, device-resident,
+    with the rescue kernel's roofline from a single-lane pass."""
+    import torch
+    from hera_b200 import api, workloads
+    n = args.leg_pairs
+    chunks = make_chunks("config4", ann, tx, n, 1, 4000)
+    dev, max_len = to_device(chunks)
+    out = {"workload": f"config4: {workloads.DESCRIPTION['config4']}", "pairs_per_step": n}
+    for path in ("plain", "batched"):
+        ctx, m = measure(ix, dev, max_len, n, path, args, local, 1, steps=args.leg_steps)
+        out[path] = leg_summary(m)
+        if orc is not None:
+            out[path].update(bit_exact(ctx, orc, chunks[m["last"]], n, args.parity_pairs // 4, args.write_bam))
+        ctx.close()
+    out["batched_over_plain"] = out["batched"]["value"] / out["plain"]["value"]
+    kctx = api.Context(ix, device=local, path="batched", lanes=1)
+    s, o, ln = dev[0]
+    for _ in range(2):
+        kctx.align_pairs_device(s.data_ptr(), o.data_ptr(), ln.data_ptr(), n, max_len, args.write_bam, kctx.stream)
+    torch.cuda.synchronize()
+    tm = kctx.timing()
+    kctx.close()
+    roof, _, rescue = roofline(tm, dpx, n, int(chunks[0][0].len.sum() + chunks[0][1].len.sum()), max_len)
+    out["roofline"] = _short_roof(roof)
+    out["roofline_rescue"] = _short_roof(rescue)
+    out["kernel_ms_per_step"] = {k: round(float(tm[k]), 4) for k in ("seed_kernel_ms", "build_ms", "dp_kernel_ms",
+                                                                     "rescue_kernel_ms", "resolve_ms", "pack_ms")}
+    out["ssw_cells"] = int(tm["ssw_cells"])
+    return out
 
 
 def classes_leg(kctx, pairs: int, length) -> dict:
@@ -607,14 +802,18 @@ def fastq_bench(args, ix, chunk, local):
             api.host_unregister(a)
 
 
-def serve_bench(args, local):
+def serve_bench(args, ann, tx, ix, orc, local):
     """The serving loop on the config-5 shape: the config-1 index resident,
     64 samples of log-uniform 0.5M-8M pairs (times --serve-scale), read
     lengths 75-150 bp, arriving as 131072-pair (256k-read) chunks by a
-    Poisson process at 1.5x the plain path's measured capacity."""
+    Poisson process at 1.5x the plain path's measured capacity.  During the
+    Poisson run each waited chunk's records go into its sample's class table
+    on the device (hera's add_class, in the sample's chunk order); after it,
+    every sample's EM on the device is checked bit for bit against the EM
+    the oracle computes over the class table of the oracle's own records
+    for the same chunks."""
     import types
-    from hera_b200 import api, synth, workloads
-    ann, tx, ix = workloads.build("config1")
+    from hera_b200 import api, synth
     CH = 131072
     pool = []   # one chunk per read length; chunks of a sample reuse its pool chunk
     for k, L in enumerate((75, 100, 125, 150)):
@@ -644,29 +843,32 @@ def serve_bench(args, local):
                 left[s] -= n
     gaps = rng.exponential(1.0, len(plan))
     gaps *= np.array([n for _, n in plan]) / rate   # mean gap = chunk size / rate
-    ctx = api.Context(ix, device=local)
-    srv = api.Server(ctx, batch_pairs=CH, write_bam=args.write_bam, max_samples=64)
-    # warm the slots (buffers at the longest reads, autotuner) before the clock
-    warm = [srv.submit(0, *pool[3]) for _ in range(2 * srv.stats()["slots"])]
-    keep = None   # one host result reused by the waiter (records are not inspected here)
-    for tk in warm:
-        keep = srv.wait(tk, out=keep)[0]
-    # capacity: the whole plan submitted at once
-    t = time.perf_counter()
-    sat = []
-    for s, n in plan:
+
+    def chunk_of(s, n):
         r1, r2 = pool[rlen[s]]
         if n < CH:
             r1 = types.SimpleNamespace(n=n, seq=r1.seq, off=r1.off[:n], len=r1.len[:n])
             r2 = types.SimpleNamespace(n=n, seq=r2.seq, off=r2.off[:n], len=r2.len[:n])
-        sat.append(srv.submit(s, r1, r2))
+        return r1, r2
+
+    ctx = api.Context(ix, device=local)
+    srv = api.Server(ctx, batch_pairs=CH, write_bam=args.write_bam, max_samples=64)
+    # warm the slots (buffers at the longest reads, autotuner) before the clock
+    warm = [srv.submit(0, *pool[3]) for _ in range(2 * srv.stats()["slots"])]
+    keep = None   # one host result reused by the waiter
+    for tk in warm:
+        keep = srv.wait(tk, out=keep)[0]
+    # capacity: the whole plan submitted at once
+    t = time.perf_counter()
+    sat = [srv.submit(s, *chunk_of(s, n)) for s, n in plan]
     t_sub = time.perf_counter() - t
     for tk in sat:
         srv.wait(tk, out=keep)
-
     capacity = float(sizes.sum()) / (time.perf_counter() - t)
     log(f"serving capacity run: submit {t_sub:.2f}s, total {float(sizes.sum()) / capacity:.2f}s, "
         f"{srv.stats()}")
+    # per-sample class tables on the device, filled as chunks are waited for
+    tables = [api.Classes(ctx, max_classes=1 << 14, max_list=1 << 18) for _ in range(64)]
     tickets, infos = [], []
     lock = threading.Lock()
     done = threading.Event()
@@ -679,48 +881,76 @@ def serve_bench(args, local):
             d = due - (time.perf_counter() - t0)
             if d > 0:
                 time.sleep(d)
-            r1, r2 = pool[rlen[s]]
-            if n < CH:
-                r1 = types.SimpleNamespace(n=n, seq=r1.seq, off=r1.off[:n], len=r1.len[:n])
-                r2 = types.SimpleNamespace(n=n, seq=r2.seq, off=r2.off[:n], len=r2.len[:n])
-            tk = srv.submit(s, r1, r2)
+            tk = srv.submit(s, *chunk_of(s, n))
             with lock:
-                tickets.append(tk)
+                tickets.append((s, tk))
         done.set()
 
     th = threading.Thread(target=feed)
     t0 = time.perf_counter()
     th.start()
     k = 0
-    while True:
-        with lock:
-            tk = tickets[k] if k < len(tickets) else None
-        if tk is None:
-            if done.is_set() and k >= len(tickets):
-                break
-            time.sleep(0.0005)
-            continue
-        infos.append(srv.wait(tk, out=keep)[1])
-        k += 1
-    th.join()
-    wall = time.perf_counter() - t0
-    st = srv.stats()
-    srv.close()
-    ctx.close()
-    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
-    wt = np.array([i["admit_ms"] - i["submit_ms"] for i in infos])
-    span_s = (max(i["done_ms"] for i in infos) - min(i["submit_ms"] for i in infos)) / 1e3
-    return {"workload": "config5 shape: config1 index, 64 samples of log-uniform 0.5M-8M pairs x "
-                        f"{args.serve_scale}, 75-150 bp, 131072-pair chunks, Poisson arrivals",
-            "samples": 64, "chunks": len(plan), "pairs": int(sizes.sum()),
-            "plain_pairs_per_s": plain, "arrival_pairs_per_s": rate, "capacity_pairs_per_s": capacity,
-            "sustained_pairs_per_s": float(sizes.sum()) / span_s, "wall_s": wall,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "p50_wait_ms": float(np.percentile(wt, 50)), "p99_wait_ms": float(np.percentile(wt, 99)),
-            "slots": st["slots"], "batches": st["batches"], "batch_pairs": CH}
+    try:
+        while True:
+            with lock:
+                item = tickets[k] if k < len(tickets) else None
+            if item is None:
+                if done.is_set() and k >= len(tickets):
+                    break
+                time.sleep(0.0005)
+                continue
+            s, tk = item
+            res, info = srv.wait(tk, out=keep)
+            tables[s].add_result(res)
+            infos.append(info)
+            k += 1
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+        wt = np.array([i["admit_ms"] - i["submit_ms"] for i in infos])
+        span_s = (max(i["done_ms"] for i in infos) - min(i["submit_ms"] for i in infos)) / 1e3
+        out = {"workload": "config5 shape: config1 index, 64 samples of log-uniform 0.5M-8M pairs x "
+                           f"{args.serve_scale}, 75-150 bp, 131072-pair chunks, Poisson arrivals",
+               "samples": 64, "chunks": len(plan), "pairs": int(sizes.sum()),
+               "plain_pairs_per_s": plain, "arrival_pairs_per_s": rate, "capacity_pairs_per_s": capacity,
+               "sustained_pairs_per_s": float(sizes.sum()) / span_s, "wall_s": wall,
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+               "p50_wait_ms": float(np.percentile(wt, 50)), "p99_wait_ms": float(np.percentile(wt, 99)),
+               "slots": st["slots"], "batches": st["batches"], "batch_pairs": CH}
+        # per-sample EM: the device EM over the served table against the
+        # oracle's EM over the oracle's table of the same chunks (a served
+        # chunk's records are those of the chunk aligned alone)
+        em_ms, rounds, same_tab, same_em = [], [], 0, 0
+        ores = [orc.align_pairs(r1.copy(), r2.copy(), args.write_bam) for r1, r2 in pool] if orc is not None else None
+        for s in range(64):
+            g, o, k_r, ms = tables[s].em(ctx)
+            em_ms.append(ms)
+            rounds.append(k_r)
+            if orc is None:
+                continue
+            r = ores[rlen[s]]
+            parts = [types.SimpleNamespace(recs=r.recs[:2 * n], pos_pool=r.pos_pool, p_pool=r.p_pool)
+                     for s2, n in plan if s2 == s]
+            want = orc.classes(parts)
+            same_tab += int(tables[s].fetch().key() == want.key())
+            g0, o0, k0 = orc.em(want)
+            same_em += int(k0 == k_r and np.array_equal(g.view(np.uint64), g0.view(np.uint64))
+                           and np.array_equal(o.view(np.uint64), o0.view(np.uint64)))
+        out["em"] = {"samples": 64, "device_ms_total": round(float(np.sum(em_ms)), 2),
+                     "rounds_median": int(np.median(rounds)),
+                     "class_tables_equal": None if orc is None else same_tab,
+                     "em_bit_exact": None if orc is None else same_em,
+                     "bit_exact": None if orc is None else bool(same_tab == 64 and same_em == 64)}
+    finally:
+        for tb in tables:
+            tb.close()
+        ctx.close()
+    return out
 
 
-def roofline(tm, dpx_instr_s, args, read_bytes, max_len):
+def roofline(tm, dpx_instr_s, chunk, read_bytes, max_len):
     """Rooflines of one single-lane step of the batched form.
 
     Gap DP (the dominant kernels): SW_align cells evaluated (counted the
@@ -755,7 +985,7 @@ def roofline(tm, dpx_instr_s, args, read_bytes, max_len):
           "work": {"sw_cells": cells, "dp_jobs": int(tm["dp_jobs"]), "dp_calls": int(tm["dp_calls"]),
                    "kernel_ms": float(tm["dp_kernel_ms"])}}
 
-    n_reads = 2 * args.chunk
+    n_reads = 2 * chunk
     lookups, probes = int(tm["lookups"]), int(tm["probes"])
     spr = (max_len - 31) // 31 + 1 if max_len >= 31 else 1
     slots = n_reads * 2 * spr

@@ -13,6 +13,7 @@ There is no CPU fallback: a missing library or device raises.
 from __future__ import annotations
 
 import ctypes as C
+import time
 import os
 from typing import List, Optional
 
@@ -379,8 +380,9 @@ class Result:
                         bytes(self.miss_pool[mo:mo + nm])))
         return (int(r["pair"]), tuple(out))
 
-    def canonical(self) -> List[tuple]:
-        return [self.candidate(i) for i in range(self.recs.shape[0])]
+    def canonical(self, lo: int = 0, hi: Optional[int] = None) -> List[tuple]:
+        hi = self.recs.shape[0] if hi is None else hi
+        return [self.candidate(i) for i in range(lo, hi)]
 
 
 class Context:
@@ -465,6 +467,45 @@ class Context:
         interleaved).  Results stay on the device until fetch()."""
         self._check(self.lib.hera_gpu_align_pairs_device(self.h, d_seq, d_off, d_len, n, max_len,
                                                          write_bam, stream))
+
+    # struct read_inf (src/read.h:16-21) as a numpy record: seq, name, qual
+    # pointers and the length
+    READ_INF = np.dtype([("seq", "<u8"), ("name", "<u8"), ("qual", "<u8"), ("len", "<i4"), ("pad", "<i4")])
+
+    @classmethod
+    def _read_infs(cls, rs):
+        """read_inf entries over a NUL-separated copy of the reads (the
+        copy is returned too: it must outlive the call)."""
+        lens = rs.len.astype(np.int64)
+        total = int(lens.sum())
+        starts = np.cumsum(lens) - lens
+        within = np.arange(total) - np.repeat(starts, lens)
+        dst = np.zeros(rs.n, np.int64)
+        dst[1:] = np.cumsum(lens[:-1] + 1)
+        buf = np.zeros(total + rs.n + 1, np.uint8)
+        buf[np.repeat(dst, lens) + within] = rs.seq[np.repeat(rs.off, lens) + within]
+        ri = np.zeros(rs.n, cls.READ_INF)
+        ri["seq"] = buf.ctypes.data + dst
+        ri["len"] = rs.len
+        return ri, buf
+
+    def align_pairs_dropin(self, r1, r2, write_bam: int = 1) -> float:
+        """The drop-in call hera's worker makes (hera_gpu_align_pairs:
+        read_inf in, malloc'd Candidates out); the Candidates are freed
+        afterwards as hera's destroy_candidate would.  Returns the call's
+        wall milliseconds (the free excluded)."""
+        a, ba = self._read_infs(r1)
+        b, bb = self._read_infs(r2)
+        out = np.zeros(2 * r1.n, np.uint64)
+        self.lib.hera_gpu_align_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int,
+                                                  C.c_void_p]
+        self.lib.hera_gpu_free_candidates.argtypes = [C.c_void_p, C.c_int64]
+        t0 = time.perf_counter()
+        rc = self.lib.hera_gpu_align_pairs(self.h, _ptr(a), _ptr(b), r1.n, write_bam, _ptr(out))
+        ms = (time.perf_counter() - t0) * 1e3
+        self.lib.hera_gpu_free_candidates(_ptr(out), out.shape[0])
+        self._check(rc)
+        return ms
 
     def fetch(self, n_recs: int) -> Result:
         res = Result(n_recs, n_recs * 8 + 1024, n_recs * 8 + 1024, n_recs * 8 + 1024)

@@ -152,9 +152,14 @@ __device__ inline int merge_packed(const PAnchors &A, int na, PAnchors &B, const
 }
 
 // round 0: reset every pair's Candidate state and list the get_position
-// calls that have at least one seed hit (the others take the miss exit)
+// calls that have at least one seed hit (the others take the miss exit).
+// With `key`, every call gets its anchor count (the seeds' hits, capped at
+// 255; 0 for a call with none) and `list` the identity, for a sort that
+// hands the build its calls largest first, so that a warp's 32 calls are of
+// like size; without, `list` holds the calls with hits in no set order.
 __global__ void k_task_list(Batch b, int ntask, const uint2 *__restrict__ hits, int spr,
-			    TaskInfo *__restrict__ tinfo, int *__restrict__ list, int *__restrict__ nlist)
+			    TaskInfo *__restrict__ tinfo, int *__restrict__ list, int *__restrict__ nlist,
+			    uint8_t *__restrict__ key)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= ntask)
@@ -176,16 +181,26 @@ __global__ void k_task_list(Batch b, int ntask, const uint2 *__restrict__ hits, 
 	tinfo[t].nch = -1;
 	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
 	const int L = b.len[ri];
+	if (key) {
+		key[t] = 0;
+		list[t] = t;
+	}
 	if (L > b.max_len) {
 		flag(b.flags, F_READ);
 		return;
 	}
 	const uint2 *h = hits + ((int64_t)ri * 2 + str) * spr;
-	bool any = false;
+	uint32_t w = 0;
 	for (int j = 0; j * KMER + KMER <= L; ++j)
-		any |= h[j].y != 0;
-	if (any)
+		w += h[j].y;
+	if (w == 0)
+		return;
+	if (key) {
+		key[t] = (uint8_t)(w < 255 ? w : 255);
+		atomicAdd(nlist, 1);
+	} else {
 		list[atomicAdd(nlist, 1)] = t;
+	}
 }
 
 __device__ __forceinline__ void task_of(const Round &R, int t, int &pi, int &c, int &str)

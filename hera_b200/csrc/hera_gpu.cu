@@ -785,6 +785,9 @@ struct Lane {
 	DBuf<DpJob> jobs;
 	DBuf<uint8_t> res;
 	DBuf<int> perm, hist, tlist;
+	DBuf<int> tval;                      // round 0's calls before the sort by size
+	DBuf<uint8_t> tkey;                  // their anchor counts (2 halves: in, out)
+	bool sort_tasks = true;              // the allocation-free lane keeps the unsorted list
 	size_t chain_cap = 0, job_cap = 0, slot_cap = 0;
 	DBuf<hera_cand_rec> recs;
 	DBuf<uint32_t> pos_pool, op_pool;
@@ -826,6 +829,7 @@ struct Lane {
 		ovf_list.release(); ovf_slot.release(); wpairs.release(); wwork.release(); wssw_out.release();
 		side_recs.release(); side_pos.release(); side_op.release(); side_p.release(); side_miss.release();
 		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
+		tval.release(); tkey.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
 		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
@@ -1074,6 +1078,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	// counters are made here, so that entry point itself allocates nothing
 	ctx->na = new Lane();
 	ctx->na->no_wide = true;
+	ctx->na->sort_tasks = false;
 	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    ctx->na->h_small.ensure(32) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
@@ -1258,8 +1263,25 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		LK(L.tlist.ensure(R.ntask), "task list");
 		int *d_nl = L.counters.p + 15;
 		LK(cudaMemsetAsync(d_nl, 0, sizeof(int), st), "memset");
-		k_task_list<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R.ntask, R.hits, R.spr, L.tinfo.p, L.tlist.p, d_nl);
-		++launches;
+		if (L.sort_tasks) {
+			// calls largest first (anchor count, descending): a warp of the
+			// build then takes calls of like size
+			LK(L.tval.ensure(R.ntask), "task list");
+			LK(L.tkey.ensure(2 * (size_t)R.ntask), "task keys");
+			k_task_list<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R.ntask, R.hits, R.spr, L.tinfo.p,
+									       L.tval.p, d_nl, L.tkey.p);
+			size_t tmp = 0;
+			cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p,
+								  L.tlist.p, R.ntask, 0, 8, st);
+			LK(L.cub_tmp.ensure(tmp), "sort scratch");
+			cub::DeviceRadixSort::SortPairsDescending(L.cub_tmp.p, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p,
+								  L.tlist.p, R.ntask, 0, 8, st);
+			launches += 2;
+		} else {
+			k_task_list<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R.ntask, R.hits, R.spr, L.tinfo.p,
+									       L.tlist.p, d_nl, nullptr);
+			++launches;
+		}
 		R.list = L.tlist.p;
 		R.nlist = d_nl;
 	}
@@ -2740,6 +2762,29 @@ extern "C" int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, in
 				     hera_candidate **out)
 {
 	return align_dropin(ctx, reads, nullptr, n, write_bam, out);
+}
+
+extern "C" void hera_gpu_free_candidates(hera_candidate **c, int64_t n)
+{
+	if (!c)
+		return;
+	for (int64_t i = 0; i < n; ++i) {
+		hera_candidate *x = c[i];
+		if (!x)
+			continue;
+		for (int s = 0; s < 2; ++s) {
+			free(x->pos[s]);
+			free(x->p[s]);
+			if (x->cigar[s]) {
+				free(x->cigar[s]->count);
+				free(x->cigar[s]->type);
+				free(x->cigar[s]->miss);
+				free(x->cigar[s]);
+			}
+		}
+		free(x);
+		c[i] = nullptr;
+	}
 }
 
 // ---- kernel-level check of the gap DP ------------------------------------

@@ -6,7 +6,7 @@ config1  small transcriptome: 2 Mbp genome (GC 0.41), 200 genes of 2-8
          log-normal(sigma 2) abundances, 0.5% substitutions, 0.01% 1-3 bp
          indels.
 config2  transcriptome scale: 400 Mbp genome in 8 chromosomes, 60k genes,
-         200k transcripts (~300 Mbp transcriptome, ~1.5 kb mean); 2x100 bp
+         200k transcripts (352 Mbp transcriptome, 1.76 kb mean); 2x100 bp
          pairs, 0.5% substitutions, 0.02% indels; 1M-pair chunks.
 config2s config 2's gene and read model on a 40 Mbp genome (6k genes,
          20k transcripts): the profiling case.
@@ -31,18 +31,19 @@ ANNOTATIONS = {
     "config1": dict(seed=1, genome_len=2_000_000, n_genes=200, n_transcripts=500, n_chrom=1,
                     exons=(2, 8), exon_median=150.0, intron=(200, 5000)),
     "config2": dict(seed=2, genome_len=400_000_000, n_genes=60_000, n_transcripts=200_000,
-                    n_chrom=8, exons=(2, 16), exon_median=180.0, intron=(200, 3000)),
+                    n_chrom=8, exons=(2, 16), exon_median=208.0, intron=(200, 3000)),
 }
 # config 2's gene and read model on a tenth of the genome (profiling case:
 # same isoform structure, ~1 GB of index on the device)
 ANNOTATIONS["config2s"] = dict(seed=2, genome_len=40_000_000, n_genes=6_000, n_transcripts=20_000,
-                               n_chrom=2, exons=(2, 16), exon_median=180.0, intron=(200, 3000))
+                               n_chrom=2, exons=(2, 16), exon_median=208.0, intron=(200, 3000))
 ANNOTATIONS["config3"] = ANNOTATIONS["config1"]
 ANNOTATIONS["config4"] = ANNOTATIONS["config1"]
 
 DESCRIPTION = {
     "config1": "2 Mbp genome, 200 genes, 500 isoforms; 2x100 bp, 0.5% subs, 0.01% indels",
-    "config2": "400 Mbp genome, 60k genes, 200k transcripts; 2x100 bp, 0.5% subs, 0.02% indels",
+    "config2": "400 Mbp genome, 60k genes, 200k transcripts (352 Mbp, 1.76 kb mean); 2x100 bp, "
+               "0.5% subs, 0.02% indels",
     "config2s": "40 Mbp genome, 6k genes, 20k transcripts; config-2 read model",
     "config3": "config1 index; 50/75/100/150 bp mixed, U(0.1-2%) subs, 0.05% indels",
     "config4": "config1 index; 2x150 bp, 3% subs, 0.5% 1-8 bp indels, 5% mutated loci",

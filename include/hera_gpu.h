@@ -230,6 +230,11 @@ int hera_gpu_align_pairs(hera_gpu_ctx *ctx, hera_read_inf *r1, hera_read_inf *r2
 int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, int32_t n,
 			  int write_bam, hera_candidate **out);
 
+/* Free n Candidates of the drop-in forms as hera's destroy_candidate
+ * (src/hash_align.c:973-989) does, for callers outside hera's C (NULL
+ * entries are skipped; each entry is set to NULL). */
+void hera_gpu_free_candidates(hera_candidate **c, int64_t n);
+
 /* Device-resident batch (inputs already in HBM): the same computation as
  * hera_gpu_align_pairs_flat on device pointers (seq, off, len for 2n reads:
  * read 2i is mate 1 and read 2i+1 mate 2 of pair i; reads back to back with

@@ -91,8 +91,9 @@ class Result:
                         bytes(self.miss_pool[mo:mo + nm])))
         return (int(r["pair"]), tuple(out))
 
-    def canonical(self) -> List[tuple]:
-        return [self.candidate(i) for i in range(self.recs.shape[0])]
+    def canonical(self, lo: int = 0, hi: Optional[int] = None) -> List[tuple]:
+        hi = self.recs.shape[0] if hi is None else hi
+        return [self.candidate(i) for i in range(lo, hi)]
 
 
 def _pool_caps(n_recs: int, total_len: int, scale: int = 1):
