@@ -1476,7 +1476,7 @@ static int wide_pass(hera_gpu_ctx *ctx, Lane &L, const Batch &b, int32_t n, bool
 	LK(L.wpairs.ensure(wave), "wide pass state");
 	LK(L.wwork.ensure((size_t)(paired ? 4 : 1) * wave), "wide pass working sets");
 	LK(L.side_recs.ensure((size_t)nw * ncand), "wide pass records");
-	BatchT<CapsWide> bw;
+	BatchT<CapsWide> bw{};
 	bw.ix = b.ix;
 	bw.code = b.code;
 	bw.code_r = b.code_r;
@@ -1575,7 +1575,7 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 	unsigned long long *d_stats = reinterpret_cast<unsigned long long *>(L.counters.p + 16);
 	LK(cudaMemsetAsync(L.counters.p, 0, 32 * sizeof(int), st), "memset");
 
-	Batch b;
+	Batch b{};   // value-initialised: no pair map, no per-task work areas
 	b.ix = ctx->ix;
 	b.code = L.code.p;
 	b.code_r = batched ? L.code_r.p : nullptr;
