@@ -215,6 +215,54 @@ def write_index(ix: HeraIndex, path: str) -> None:
         f.write(ix.p.astype(np.uint32).tobytes())
 
 
+def write_reference_inf(ann, path: str) -> None:
+    """hera's reference.inf for an annotation written as synth.write_gtf and
+    synth.write_genome_fasta write it (the file hera_build makes beside the
+    index; hera quant reads it at start-up, init_bam_header and
+    contruct_gene_map, src/bam_write.c:22-57, 448-496):
+      - the BAM header's reference block, led by its byte count: chromosome
+        count, then per chromosome name length, name, sequence length;
+      - chromosome names as fixed-width NUL-padded rows and their lengths;
+      - gene labels (strand + gene_id + gene_name) as fixed-width rows;
+      - per transcript, in index order: exon count, exon starts, exon ends
+        (inclusive, 0-based), then every transcript's chromosome and gene."""
+    import struct
+    from . import synth
+    names = [n.encode() for n in ann.chrom_names]
+    lens = [int(c.shape[0]) for c in ann.chroms]
+    out = bytearray()
+    block = 4 + sum(8 + len(n) for n in names)
+    out += struct.pack("<II", block, len(names))
+    for n, ln in zip(names, lens):
+        out += struct.pack("<I", len(n)) + n + struct.pack("<I", ln)
+    w = max(len(n) for n in names) + 1
+    out += struct.pack("<II", len(names), w)
+    for n in names:
+        out += n + b"\0" * (w - len(n))
+    out += struct.pack(f"<{len(lens)}I", *lens)
+    labels = [(g.strand + g.gene_id + g.gene_name).encode() for g in ann.genes]
+    w = max(len(x) for x in labels) + 1
+    out += struct.pack("<II", len(labels), w)
+    for x in labels:
+        out += x + b"\0" * (w - len(x))
+    gm = synth.gene_map(ann)
+    for t in range(len(gm.chr)):
+        a, b = int(gm.exon_off[t]), int(gm.exon_off[t + 1])
+        out += struct.pack("<I", b - a)
+        out += gm.starts[a:b].astype("<u4").tobytes() + gm.ends[a:b].astype("<u4").tobytes()
+    out += gm.chr.astype("<u4").tobytes() + gm.gene.astype("<u4").tobytes()
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+
+
+def write_index_dir(ann, ix: HeraIndex, directory: str) -> None:
+    """The index directory hera quant reads: `index` and `reference.inf`."""
+    import os
+    os.makedirs(directory, exist_ok=True)
+    write_index(ix, os.path.join(directory, "index"))
+    write_reference_inf(ann, os.path.join(directory, "reference.inf"))
+
+
 def read_index(path: str) -> HeraIndex:
     """Read the reference's index file (src/hash_align.c:1195-1234)."""
     with open(path, "rb") as f:

@@ -48,3 +48,5 @@ def test_matches_hera_index(tmp_path):
     mine = index.build_index(synth.transcriptome(ann))
     index.write_index(mine, str(d / "mine"))
     assert open(d / "mine", "rb").read() == open(d / "idx" / "index", "rb").read()
+    index.write_reference_inf(ann, str(d / "mine.inf"))
+    assert open(d / "mine.inf", "rb").read() == open(d / "idx" / "reference.inf", "rb").read()
