@@ -25,9 +25,10 @@ LIB_PATH = _build.LIB
 
 HERA_GPU_OK = 0
 ERRORS = {-1: "ENODEV", -2: "ECUDA", -3: "ENOMEM", -4: "EINVAL", -5: "ECAPACITY", -6: "ETIMEOUT",
-          -7: "EFORMAT"}
+          -7: "EFORMAT", -8: "ECANCELED"}
 HERA_GPU_ECAPACITY = -5
 HERA_GPU_EFORMAT = -7
+HERA_GPU_ECANCELED = -8
 MAX_READ = 320
 CIGAR_CHARS = "MIDNSHP=XB"
 
@@ -111,7 +112,7 @@ class Tuning(C.Structure):
 
 class _ServerOptions(C.Structure):
     _fields_ = [("batch_pairs", C.c_uint32), ("max_slots", C.c_int), ("hbm_reserve", C.c_uint64),
-                ("write_bam", C.c_int), ("max_samples", C.c_uint32)]
+                ("write_bam", C.c_int), ("max_samples", C.c_uint32), ("borrow_reads", C.c_int)]
 
 
 class ChunkInfo(C.Structure):
@@ -414,6 +415,7 @@ class Context:
         if rc != HERA_GPU_OK:
             raise HeraGpuError(rc, "context creation failed")
         self.h = h
+        self._inflight = {}   # asynchronous calls: ticket -> (reads structs, result)
         self._keep = None
 
     def close(self) -> None:
@@ -455,6 +457,26 @@ class Context:
         return self._run(self.lib.hera_gpu_align_pairs_flat, 2 * r1.n,
                          int(r1.len.sum()) + int(r2.len.sum()),
                          (self.h, C.byref(a), C.byref(b), r1.n, write_bam), out)
+
+    def submit_pairs(self, r1, r2, write_bam: int, out: Result) -> int:
+        """Start an asynchronous flat call (hera_gpu_align_pairs_submit);
+        returns a ticket.  r1, r2 and out must stay alive and untouched
+        until complete_pairs(ticket); out's pools must be large enough."""
+        a, b = self._reads(r1), self._reads(r2)
+        res = out.reuse(2 * r1.n)
+        t = C.c_uint64()
+        self.lib.hera_gpu_align_pairs_submit.argtypes = [C.c_void_p, C.POINTER(_Reads), C.POINTER(_Reads), C.c_int32,
+                                                         C.c_int, C.POINTER(_Result), C.POINTER(C.c_uint64)]
+        self.lib.hera_gpu_align_pairs_complete.argtypes = [C.c_void_p, C.c_uint64]
+        self._check(self.lib.hera_gpu_align_pairs_submit(self.h, C.byref(a), C.byref(b), r1.n, write_bam,
+                                                         C.byref(res.c), C.byref(t)))
+        self._inflight[t.value] = (a, b, res)   # the structs the call reads
+        return t.value
+
+    def complete_pairs(self, ticket: int) -> Result:
+        a, b, res = self._inflight.pop(ticket)
+        self._check(self.lib.hera_gpu_align_pairs_complete(self.h, ticket))
+        return res
 
     def align_single(self, rs, write_bam: int = 1, out: Optional[Result] = None) -> Result:
         a = self._reads(rs)
@@ -637,10 +659,12 @@ class Server:
     free HBM, per-sample counters on the device."""
 
     def __init__(self, ctx: "Context", batch_pairs: int = 0, max_slots: int = 0, write_bam: int = 1,
-                 max_samples: int = 0, hbm_reserve: int = 0):
+                 max_samples: int = 0, hbm_reserve: int = 0, borrow_reads: bool = False):
+        """borrow_reads: submit keeps pointers to the caller's reads (no
+        copy); they must stay alive and unchanged until the chunk's wait."""
         self.ctx = ctx
         self.lib = ctx.lib
-        opt = _ServerOptions(batch_pairs, max_slots, hbm_reserve, write_bam, max_samples)
+        opt = _ServerOptions(batch_pairs, max_slots, hbm_reserve, write_bam, max_samples, 1 if borrow_reads else 0)
         h = C.c_void_p()
         ctx._check(self.lib.hera_gpu_server_create(ctx.h, C.byref(opt), C.byref(h)))
         self.h = h
@@ -669,6 +693,13 @@ class Server:
             rc = self.lib.hera_gpu_server_wait(self.h, ticket, C.byref(res.c), C.byref(info))
         self.ctx._check(rc)
         return res, info.as_dict()
+
+    def cancel(self, sample: int) -> int:
+        """Drop the sample's queued work; returns the chunks cancelled."""
+        k = C.c_int32(0)
+        self.lib.hera_gpu_server_cancel.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_int32)]
+        self.ctx._check(self.lib.hera_gpu_server_cancel(self.h, sample, C.byref(k)))
+        return k.value
 
     def sample_stats(self, sample: int) -> dict:
         st = SampleStats()

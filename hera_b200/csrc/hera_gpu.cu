@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
+#include <algorithm>
 #include <atomic>
 #include <condition_variable>
 #include <deque>
@@ -869,6 +870,21 @@ struct hera_gpu_ctx {
 	// take it exclusively, so no other lane's kernels share the GPU with them
 	std::shared_mutex gate;
 	struct FqState *fq = nullptr;     // FASTQ chunk parsing (made on first use)
+	// asynchronous flat calls: two in flight at most, each on a lane group
+	// of its own (the second group is made on first use)
+	struct AsyncCall {
+		std::thread th;
+		bool busy = false;
+		uint64_t ticket = 0;
+		int rc = 0;
+		std::string err;
+		hera_gpu_timing tm{};
+		hera_gpu_reads r1{}, r2{};
+	};
+	std::mutex async_mu;
+	AsyncCall async[2];
+	std::vector<Lane *> lanes2;
+	uint64_t next_async = 1;
 };
 
 struct FqState;
@@ -997,6 +1013,9 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	if (!ctx)
 		return;
 	cudaSetDevice(ctx->device);
+	for (auto &a : ctx->async)   // asynchronous calls not completed
+		if (a.th.joinable())
+			a.th.join();
 	cudaDeviceSynchronize();
 	cudaFree(ctx->d_boff);
 	cudaFree(ctx->d_bk);
@@ -1009,6 +1028,10 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 		L->release();
 		delete L;
 	}
+	for (Lane *L : ctx->lanes2) {
+		L->release();
+		delete L;
+	}
 	if (ctx->na) {
 		ctx->na->release();
 		delete ctx->na;
@@ -1017,6 +1040,24 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	if (ctx->stream)
 		cudaStreamDestroy(ctx->stream);
 	delete ctx;
+}
+
+// n lanes, each with its streams and events
+static int make_lanes(std::vector<Lane *> &lanes, int n)
+{
+	for (int i = 0; i < n; ++i) {
+		Lane *L = new Lane();
+		lanes.push_back(L);
+		if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess ||
+		    cudaStreamCreateWithFlags(&L->cstream, cudaStreamNonBlocking) != cudaSuccess)
+			return HERA_GPU_ECUDA;
+		for (auto &e : L->ev)
+			cudaEventCreate(&e);
+		for (auto &s2 : L->cev)
+			for (auto &e : s2)
+				cudaEventCreate(&e);
+	}
+	return HERA_GPU_OK;
 }
 
 extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_options *opt,
@@ -1062,18 +1103,8 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 		return bail(fail(ctx, HERA_GPU_ECUDA, "SM count"));
 	ctx->tune.build_blocks_per_sm = 8;
 	ctx->tune.rescue_warps_per_block = 4;
-	for (int i = 0; i < nlanes; ++i) {
-		Lane *L = new Lane();
-		ctx->lanes.push_back(L);
-		if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess ||
-		    cudaStreamCreateWithFlags(&L->cstream, cudaStreamNonBlocking) != cudaSuccess)
-			return bail(HERA_GPU_ECUDA);
-		for (auto &e : L->ev)
-			cudaEventCreate(&e);
-		for (auto &s2 : L->cev)
-			for (auto &e : s2)
-				cudaEventCreate(&e);
-	}
+	if (make_lanes(ctx->lanes, nlanes) != HERA_GPU_OK)
+		return bail(HERA_GPU_ECUDA);
 	// the allocation-free entry's lane: its stream, events and 32 pinned
 	// counters are made here, so that entry point itself allocates nothing
 	ctx->na = new Lane();
@@ -2185,10 +2216,10 @@ struct Sched {
 	}
 };
 
-static void sum_timing(hera_gpu_ctx *ctx)
+static hera_gpu_timing sum_lanes(const std::vector<Lane *> &lanes)
 {
 	hera_gpu_timing t{};
-	for (Lane *L : ctx->lanes) {
+	for (Lane *L : lanes) {
 		const hera_gpu_timing &a = L->timing;
 		t.h2d_ms += a.h2d_ms;
 		t.seed_ms += a.seed_ms;
@@ -2215,25 +2246,34 @@ static void sum_timing(hera_gpu_ctx *ctx)
 		t.ssw_cells += a.ssw_cells;
 		t.wide_items += a.wide_items;
 	}
+	return t;
+}
+
+static void sum_timing(hera_gpu_ctx *ctx)
+{
+	hera_gpu_timing t = sum_lanes(ctx->lanes);
 	t.total_ms = ctx->timing.total_ms;
 	ctx->timing = t;
 }
 
-static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gpu_reads *r2, int32_t n,
-		      int write_bam, hera_gpu_result *out)
+// One flat call on a group of lanes; its status, error text and timing go
+// to rc / err / tm (the context's own fields are left to the caller).
+static int align_flat_on(hera_gpu_ctx *ctx, const std::vector<Lane *> &lanes, const hera_gpu_reads *r1,
+			 const hera_gpu_reads *r2, int32_t n, int write_bam, hera_gpu_result *out, std::string &err,
+			 hera_gpu_timing &tm)
 {
-	if (!ctx || !r1 || !out || n < 0 || (write_bam != 0 && write_bam != 1))
-		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
-	if (cudaSetDevice(ctx->device) != cudaSuccess)
-		return fail(ctx, HERA_GPU_ENODEV, "cudaSetDevice");
+	if (cudaSetDevice(ctx->device) != cudaSuccess) {
+		err = "cudaSetDevice";
+		return HERA_GPU_ENODEV;
+	}
 	const auto t0 = std::chrono::steady_clock::now();
 	const bool paired = r2 != nullptr;
 	const int ncand = paired ? 2 : 1;
-	for (Lane *L : ctx->lanes)
+	for (Lane *L : lanes)
 		L->timing = hera_gpu_timing{};
 	// sub-batches of at most max_batch pairs, as many as a multiple of the
 	// lane count (each lane then carries an equal share of the call)
-	const int64_t nlanes = (int64_t)ctx->lanes.size();
+	const int64_t nlanes = (int64_t)lanes.size();
 	int64_t ns = (n + (int64_t)ctx->max_batch - 1) / ctx->max_batch;
 	if (ns > 0 && n >= nlanes * 4096)
 		ns = (ns + nlanes - 1) / nlanes * nlanes;
@@ -2245,11 +2285,11 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 	S.nl.assign(nsub, 0);
 	S.no.assign(nsub, 0);
 	S.nm.assign(nsub, 0);
-	const int nl = (int)ctx->lanes.size() < nsub ? (int)ctx->lanes.size() : nsub;
+	const int nl = (int)lanes.size() < nsub ? (int)lanes.size() : nsub;
 	const int dev = ctx->device;
 	auto worker = [&](int li) {
 		cudaSetDevice(dev);
-		Lane &L = *ctx->lanes[li];
+		Lane &L = *lanes[li];
 		// a lane's sub-batches alternate between its two buffer sets: the
 		// next one is staged on the copy stream while this one runs
 		int b = 0;
@@ -2310,23 +2350,38 @@ static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gp
 		worker(0);
 	for (auto &t : th)
 		t.join();
-	ctx->timing.total_ms =
-		std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
-	sum_timing(ctx);
-	if (S.abort)
-		return fail(ctx, S.rc, S.err.c_str());
-	uint64_t tl = 0, to = 0, tm = 0;
+	tm = sum_lanes(lanes);
+	tm.total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+	if (S.abort) {
+		err = S.err;
+		return S.rc;
+	}
+	uint64_t tl = 0, to = 0, tmm = 0;
 	for (int k = 0; k < nsub; ++k) {
 		tl += S.nl[k];
 		to += S.no[k];
-		tm += S.nm[k];
+		tmm += S.nm[k];
 	}
 	out->list_used = tl;
 	out->op_used = to;
-	out->miss_used = tm;
-	if (tl > out->list_cap || to > out->op_cap || tm > out->miss_cap)
-		return fail(ctx, HERA_GPU_ECAPACITY, "result pools too small (see *_used for the sizes needed)");
+	out->miss_used = tmm;
+	if (tl > out->list_cap || to > out->op_cap || tmm > out->miss_cap) {
+		err = "result pools too small (see *_used for the sizes needed)";
+		return HERA_GPU_ECAPACITY;
+	}
 	return HERA_GPU_OK;
+}
+
+static int align_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gpu_reads *r2, int32_t n,
+		      int write_bam, hera_gpu_result *out)
+{
+	if (!ctx || !r1 || !out || n < 0 || (write_bam != 0 && write_bam != 1))
+		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
+	std::string err;
+	hera_gpu_timing tm{};
+	const int rc = align_flat_on(ctx, ctx->lanes, r1, r2, n, write_bam, out, err, tm);
+	ctx->timing = tm;
+	return rc ? fail(ctx, rc, err.c_str()) : HERA_GPU_OK;
 }
 
 extern "C" int hera_gpu_align_pairs_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1,
@@ -2342,6 +2397,63 @@ extern "C" int hera_gpu_align_single_flat(hera_gpu_ctx *ctx, const hera_gpu_read
 					  int write_bam, hera_gpu_result *out)
 {
 	return align_flat(ctx, reads, nullptr, n, write_bam, out);
+}
+
+// ---- asynchronous flat calls --------------------------------------------
+
+extern "C" int hera_gpu_align_pairs_submit(hera_gpu_ctx *ctx, const hera_gpu_reads *r1, const hera_gpu_reads *r2,
+					   int32_t n, int write_bam, hera_gpu_result *out, uint64_t *ticket)
+{
+	if (!ctx || !r1 || !r2 || !out || !ticket || n < 0 || (write_bam != 0 && write_bam != 1))
+		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
+	std::lock_guard<std::mutex> g(ctx->async_mu);
+	int k = -1;
+	for (int i = 0; i < 2 && k < 0; ++i)
+		if (!ctx->async[i].busy)
+			k = i;
+	if (k < 0)
+		return fail(ctx, HERA_GPU_EINVAL, "two asynchronous calls in flight: complete one first");
+	if (k == 1 && ctx->lanes2.empty()) {
+		if (cudaSetDevice(ctx->device) != cudaSuccess)
+			return fail(ctx, HERA_GPU_ENODEV, "cudaSetDevice");
+		if (make_lanes(ctx->lanes2, (int)ctx->lanes.size()) != HERA_GPU_OK)
+			return fail(ctx, HERA_GPU_ECUDA, "lanes of the second asynchronous call");
+	}
+	auto &a = ctx->async[k];
+	if (a.th.joinable())
+		a.th.join();
+	a.busy = true;
+	a.ticket = ctx->next_async++;
+	a.r1 = *r1;
+	a.r2 = *r2;
+	a.rc = HERA_GPU_OK;
+	a.err.clear();
+	const std::vector<Lane *> *group = k == 0 ? &ctx->lanes : &ctx->lanes2;
+	a.th = std::thread([ctx, &a, group, n, write_bam, out] {
+		a.rc = align_flat_on(ctx, *group, &a.r1, &a.r2, n, write_bam, out, a.err, a.tm);
+	});
+	*ticket = a.ticket;
+	return HERA_GPU_OK;
+}
+
+extern "C" int hera_gpu_align_pairs_complete(hera_gpu_ctx *ctx, uint64_t ticket)
+{
+	if (!ctx)
+		return HERA_GPU_EINVAL;
+	hera_gpu_ctx::AsyncCall *a = nullptr;
+	{
+		std::lock_guard<std::mutex> g(ctx->async_mu);
+		for (auto &c : ctx->async)
+			if (c.busy && c.ticket == ticket)
+				a = &c;
+	}
+	if (!a)
+		return fail(ctx, HERA_GPU_EINVAL, "unknown or completed ticket");
+	a->th.join();
+	std::lock_guard<std::mutex> g(ctx->async_mu);
+	a->busy = false;
+	ctx->timing = a->tm;
+	return a->rc ? fail(ctx, a->rc, a->err.c_str()) : HERA_GPU_OK;
 }
 
 // lane-local offsets of a device-resident sub-batch
@@ -2678,6 +2790,20 @@ static hera_candidate *materialize(const hera_gpu_result *res, uint64_t ri)
 	return c;
 }
 
+// f(lo, hi) over [0, n) in contiguous parts on up to 16 host threads
+template <class F>
+static void par_for(int64_t n, F f)
+{
+	const int64_t T = std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(),
+								   n / 4096 + 1}));
+	std::vector<std::thread> th;
+	for (int64_t t = 1; t < T; ++t)
+		th.emplace_back([&, t] { f(n * t / T, n * (t + 1) / T); });
+	f(0, n / T);
+	for (auto &x : th)
+		x.join();
+}
+
 static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, int32_t n, int write_bam,
 			hera_candidate **out)
 {
@@ -2686,12 +2812,7 @@ static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, i
 	const int per = b ? 2 : 1;
 	std::vector<int64_t> off[2];
 	std::vector<int32_t> len[2];
-	std::vector<char> seq;
 	int64_t total = 0;
-	for (int32_t i = 0; i < n; ++i)
-		total += a[i].len + (b ? b[i].len : 0);
-	seq.resize((size_t)total + 1);
-	int64_t o = 0;
 	for (int m = 0; m < per; ++m) {
 		hera_read_inf *r = m ? b : a;
 		off[m].resize(n);
@@ -2699,31 +2820,39 @@ static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, i
 		for (int32_t i = 0; i < n; ++i) {
 			if (!r[i].seq || r[i].len < 0)
 				return fail(ctx, HERA_GPU_EINVAL, "read without sequence");
-			memcpy(seq.data() + o, r[i].seq, (size_t)r[i].len);
-			off[m][i] = o;
+			off[m][i] = total;
 			len[m][i] = r[i].len;
-			o += r[i].len;
+			total += r[i].len;
 		}
 	}
-	hera_gpu_reads ra{seq.data(), off[0].data(), len[0].data()};
-	hera_gpu_reads rb{seq.data(), b ? off[1].data() : nullptr, b ? len[1].data() : nullptr};
+	// the reads gathered back to back (host threads), then one flat call
+	std::unique_ptr<char[]> seq(new char[(size_t)total + 1]);
+	for (int m = 0; m < per; ++m) {
+		hera_read_inf *r = m ? b : a;
+		par_for(n, [&](int64_t lo, int64_t hi) {
+			for (int64_t i = lo; i < hi; ++i)
+				memcpy(seq.get() + off[m][i], r[i].seq, (size_t)r[i].len);
+		});
+	}
+	hera_gpu_reads ra{seq.get(), off[0].data(), len[0].data()};
+	hera_gpu_reads rb{seq.get(), b ? off[1].data() : nullptr, b ? len[1].data() : nullptr};
 	const uint64_t items = (uint64_t)n * per;
-	std::vector<hera_cand_rec> recs(items ? items : 1);
+	std::unique_ptr<hera_cand_rec[]> recs(new hera_cand_rec[items ? items : 1]);
 	hera_gpu_result res{};
-	res.recs = recs.data();
-	std::vector<uint32_t> pos, ops;
-	std::vector<int32_t> p;
-	std::vector<char> miss;
+	res.recs = recs.get();
+	std::unique_ptr<uint32_t[]> pos, ops;
+	std::unique_ptr<int32_t[]> p;
+	std::unique_ptr<char[]> miss;
 	uint64_t cl = items * 8 + 64, co = items * 8 + 64, cm = items * 8 + 64;
 	for (int attempt = 0; attempt < 2; ++attempt) {
-		pos.resize(cl);
-		p.resize(cl);
-		ops.resize(co);
-		miss.resize(cm);
-		res.pos_pool = pos.data();
-		res.p_pool = p.data();
-		res.op_pool = ops.data();
-		res.miss_pool = miss.data();
+		pos.reset(new uint32_t[cl]);
+		p.reset(new int32_t[cl]);
+		ops.reset(new uint32_t[co]);
+		miss.reset(new char[cm]);
+		res.pos_pool = pos.get();
+		res.p_pool = p.get();
+		res.op_pool = ops.get();
+		res.miss_pool = miss.get();
 		res.list_cap = cl;
 		res.op_cap = co;
 		res.miss_cap = cm;
@@ -2737,16 +2866,27 @@ static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, i
 		co = res.op_used + 1;
 		cm = res.miss_used + 1;
 	}
-	for (uint64_t i = 0; i < items; ++i) {
-		out[i] = materialize(&res, i);
-		if (!out[i])
-			return fail(ctx, HERA_GPU_ENOMEM, "candidate allocation");
+	// hera's malloc'd Candidates, and the reads upper-cased as hera leaves
+	// them, on host threads
+	std::atomic<int> nomem{0};
+	par_for((int64_t)items, [&](int64_t lo, int64_t hi) {
+		for (int64_t i = lo; i < hi; ++i) {
+			out[i] = materialize(&res, (uint64_t)i);
+			if (!out[i])
+				nomem = 1;
+		}
+	});
+	if (nomem) {
+		hera_gpu_free_candidates(out, (int64_t)items);
+		return fail(ctx, HERA_GPU_ENOMEM, "candidate allocation");
 	}
-	for (int32_t i = 0; i < n; ++i) {
-		upper_acgt(a[i].seq, a[i].len);
-		if (b)
-			upper_acgt(b[i].seq, b[i].len);
-	}
+	par_for(n, [&](int64_t lo, int64_t hi) {
+		for (int64_t i = lo; i < hi; ++i) {
+			upper_acgt(a[i].seq, a[i].len);
+			if (b)
+				upper_acgt(b[i].seq, b[i].len);
+		}
+	});
 	return HERA_GPU_OK;
 }
 

@@ -86,6 +86,7 @@ struct SrvChunk {
 	uint32_t sample = 0;
 	int32_t n = 0;
 	RawBuf<char> seq[2];          // mate 1 and mate 2 reads, back to back
+	const char *src[2] = {nullptr, nullptr};   // borrowed: the caller's reads (off[] index it)
 	RawBuf<int64_t> off[2];       // n each, into seq[m]
 	RawBuf<int32_t> len[2];
 	int max_len = 0;
@@ -113,6 +114,7 @@ struct hera_gpu_server {
 	int write_bam = 1;
 	uint32_t batch_pairs = 131072;
 	uint32_t max_samples = 1024;
+	bool borrow = false;             // submit keeps the caller's read pointers
 	uint64_t slot_bytes = 0;
 	std::vector<Lane *> slots;
 	std::vector<std::thread> workers;
@@ -207,7 +209,7 @@ static int srv_stage(Lane &L, const std::vector<SrvPiece> &pc, int32_t npairs, i
 		for (int m = 0; m < 2; ++m) {
 			int64_t a, e;
 			range(c, m, q.lo, q.cnt, a, e);
-			pcopy(L.h_seq.p + o, c.seq[m].data() + a, (size_t)(e - a));
+			pcopy(L.h_seq.p + o, (c.src[m] ? c.src[m] : c.seq[m].data()) + a, (size_t)(e - a));
 			for (int32_t i = 0; i < q.cnt; ++i) {
 				L.h_off.p[2 * (r + i) + m] = c.off[m][q.lo + i] - a + o;
 				L.h_len.p[2 * (r + i) + m] = c.len[m][q.lo + i];
@@ -377,6 +379,7 @@ extern "C" int hera_gpu_server_create(hera_gpu_ctx *ctx, const hera_gpu_server_o
 		S->write_bam = opt->write_bam;
 		if (opt->max_samples)
 			S->max_samples = opt->max_samples;
+		S->borrow = opt->borrow_reads != 0;
 	}
 	if (S->batch_pairs > (1u << 20))
 		S->batch_pairs = 1u << 20;
@@ -457,6 +460,22 @@ extern "C" int hera_gpu_server_submit(hera_gpu_server *S, uint32_t sample, const
 				contig = false;
 			c->max_len = Ln > c->max_len ? Ln : c->max_len;
 			total += Ln;
+		}
+		c->src[m] = nullptr;
+		if (S->borrow) {   // the caller's memory, read by the slots at staging
+			// a piece is staged as one byte range: reads in rising order
+			for (int32_t i = 1; i < n; ++i)
+				if (R.off[i] < R.off[i - 1] + R.len[i - 1]) {
+					delete c;
+					return fail(S->ctx, HERA_GPU_EINVAL,
+						    "borrowed reads must lie in rising order without overlap");
+				}
+			c->src[m] = R.seq;
+			for (int32_t i = 0; i < n; ++i) {
+				c->off[m][i] = R.off[i];
+				c->len[m][i] = R.len[i];
+			}
+			continue;
 		}
 		c->seq[m].need((size_t)total + 1);
 		if (contig && n > 0) {   // one copy of the block
@@ -568,6 +587,36 @@ extern "C" int hera_gpu_server_wait(hera_gpu_server *S, uint64_t ticket, hera_gp
 	S->chunks.erase(ticket);
 	g.unlock();
 	srv_release(S, c);
+	return HERA_GPU_OK;
+}
+
+extern "C" int hera_gpu_server_cancel(hera_gpu_server *S, uint32_t sample, int32_t *n_chunks)
+{
+	if (!S)
+		return HERA_GPU_EINVAL;
+	if (sample >= S->max_samples)
+		return fail(S->ctx, HERA_GPU_EINVAL, "sample id beyond max_samples");
+	int32_t k = 0;
+	{
+		std::lock_guard<std::mutex> g(S->mu);
+		// queued chunks of the sample: the parts not yet in a batch are
+		// dropped; pieces already in a batch finish (they share it with
+		// other samples' pieces) and are then discarded with the chunk
+		for (auto it = S->pending.begin(); it != S->pending.end();) {
+			SrvChunk *c = *it;
+			if (c->sample == sample) {
+				c->rc = HERA_GPU_ECANCELED;
+				c->err = "the chunk's sample was cancelled";
+				it = S->pending.erase(it);
+				++k;
+			} else {
+				++it;
+			}
+		}
+		S->cv_done.notify_all();
+	}
+	if (n_chunks)
+		*n_chunks = k;
 	return HERA_GPU_OK;
 }
 

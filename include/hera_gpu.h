@@ -40,6 +40,7 @@ extern "C" {
 #define HERA_GPU_ETIMEOUT (-6)    /* a bounded device wait expired */
 #define HERA_GPU_EFORMAT (-7)     /* a chunk the reference's reader rejects
 				     ("Wrong format of file") */
+#define HERA_GPU_ECANCELED (-8)   /* a served chunk whose sample was cancelled */
 
 /* Longest read the device path accepts (hera itself has no limit; reads
  * longer than this are rejected with HERA_GPU_EINVAL). */
@@ -217,6 +218,21 @@ int hera_gpu_align_pairs_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *r1,
 int hera_gpu_align_single_flat(hera_gpu_ctx *ctx, const hera_gpu_reads *reads,
 			       int32_t n, int write_bam, hera_gpu_result *out);
 
+/* Asynchronous form of hera_gpu_align_pairs_flat, no counterpart in hera:
+ * submit starts the call and returns at once with a ticket; complete waits
+ * for it and returns its status (out is then filled as the synchronous
+ * call fills it; hera_gpu_get_timing then describes that call).  Two calls
+ * may be in flight, each on a group of lanes of its own (the second group
+ * is made on first use), so one call's copies to and from the host overlap
+ * the other's kernels.  r1, r2 and out -- the structs and the memory they
+ * point to -- must stay valid and untouched until the call completes; no
+ * other call may use the context while asynchronous calls are in flight.
+ * A third submit fails with HERA_GPU_EINVAL. */
+int hera_gpu_align_pairs_submit(hera_gpu_ctx *ctx, const hera_gpu_reads *r1,
+				const hera_gpu_reads *r2, int32_t n, int write_bam,
+				hera_gpu_result *out, uint64_t *ticket);
+int hera_gpu_align_pairs_complete(hera_gpu_ctx *ctx, uint64_t ticket);
+
 /* Drop-in form of hera_gpu_align_pairs_flat for hera's worker loop
  * (align_pool_pair, src/hash_align.c:1878-1929): reads as struct read_inf,
  * results as heap-allocated Candidate pairs (out[2i] = r[0],
@@ -344,6 +360,12 @@ typedef struct hera_gpu_server_options {
 	uint64_t hbm_reserve;    /* device bytes to leave free; 0 = 4 GiB */
 	int write_bam;           /* hera's WRITE_BAM for every chunk */
 	uint32_t max_samples;    /* per-sample state slots; 0 = 1024 */
+	int borrow_reads;        /* 1: submit keeps pointers to the caller's
+				    reads instead of copying them; the caller
+				    leaves that memory valid and unchanged until
+				    the chunk's wait returns (or the server is
+				    destroyed).  The batch slots then stage
+				    reads straight from it. */
 } hera_gpu_server_options;
 
 typedef struct hera_gpu_chunk_info {
@@ -390,6 +412,16 @@ int hera_gpu_server_submit(hera_gpu_server *s, uint32_t sample, const hera_gpu_r
  * concurrent wait fails with HERA_GPU_EINVAL).  `info` may be NULL. */
 int hera_gpu_server_wait(hera_gpu_server *s, uint64_t ticket, hera_gpu_result *out,
 			 hera_gpu_chunk_info *info);
+
+/* Drop the queued work of `sample` (no counterpart in hera: a client that
+ * goes away mid-run).  Its chunks not yet fully admitted to a batch stop:
+ * their remaining pairs are never aligned, and hera_gpu_server_wait on
+ * their tickets returns HERA_GPU_ECANCELED once the pieces already in
+ * batches have finished.  Chunks already fully admitted complete normally,
+ * and every other sample's chunks are unaffected (their records stay those
+ * of the chunk aligned alone).  *n_chunks (may be NULL): chunks cancelled.
+ * Later submits for the sample are accepted. */
+int hera_gpu_server_cancel(hera_gpu_server *s, uint32_t sample, int32_t *n_chunks);
 
 /* Per-sample counters (read from the device) and server-wide figures. */
 int hera_gpu_server_get_sample_stats(hera_gpu_server *s, uint32_t sample, hera_gpu_sample_stats *out);

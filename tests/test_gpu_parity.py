@@ -288,3 +288,29 @@ def test_single_past_list_capacities(family, ctx_family):
     f1, _ = synth.family_pairs(tx, 400, seed=21, shared=600)
     for wb in (1, 0):
         _assert_same(ctx_family.align_single(f1, wb), orc.align_single(f1.copy(), wb), f"family single wb={wb}")
+
+
+def test_async_calls_equal_sync(config1, oracle1):
+    """Two asynchronous flat calls in flight at once (each on its own lane
+    group) give the records of the synchronous call; a third submit is
+    refused while both are in flight."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ann, tx, ix = config1
+    ctx = api.Context(ix, max_batch=1 << 14, lanes=2)
+    try:
+        sets = [workloads.pairs(wl, ann, tx, 9000, seed=70 + k) for k, wl in enumerate(("config1", "config4", "config3"))]
+        want = [ctx.align_pairs(r1, r2, 0).canonical() for r1, r2 in sets]
+        outs = [api.Result(2 * 9000, 1 << 20, 1 << 20, 1 << 20) for _ in range(2)]
+        t0 = ctx.submit_pairs(*sets[0], 0, outs[0])
+        t1 = ctx.submit_pairs(*sets[1], 0, outs[1])
+        with pytest.raises(api.HeraGpuError):
+            ctx.submit_pairs(*sets[2], 0, api.Result(2 * 9000, 1 << 20, 1 << 20, 1 << 20))
+        assert ctx.complete_pairs(t0).canonical() == want[0]
+        t2 = ctx.submit_pairs(*sets[2], 0, outs[0])
+        assert ctx.complete_pairs(t1).canonical() == want[1]
+        assert ctx.complete_pairs(t2).canonical() == want[2]
+        assert want[1] == oracle1.align_pairs(sets[1][0].copy(), sets[1][1].copy(), 0).canonical()
+    finally:
+        ctx.close()

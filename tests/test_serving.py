@@ -25,7 +25,10 @@ def _chunks(config1):
     return out
 
 
-def test_mix_equals_alone_and_oracle(config1, oracle1):
+@pytest.mark.parametrize("borrow", [False, True])
+def test_mix_equals_alone_and_oracle(config1, oracle1, borrow):
+    """borrow: submit keeps the caller's read pointers (no copy); the reads
+    stay alive here until every wait has returned."""
     if not __import__("torch").cuda.is_available():
         pytest.skip("no CUDA device")
     from hera_b200 import api
@@ -34,7 +37,7 @@ def test_mix_equals_alone_and_oracle(config1, oracle1):
     try:
         alone = [ctx.align_pairs(r1, r2, 1) for _, r1, r2 in chunks]
         # a small batch size, so batches span chunks and chunks span batches
-        srv = api.Server(ctx, batch_pairs=4096, max_slots=3, write_bam=1, max_samples=8)
+        srv = api.Server(ctx, batch_pairs=4096, max_slots=3, write_bam=1, max_samples=8, borrow_reads=borrow)
         tickets = [None] * len(chunks)
 
         def feed(ks):
@@ -97,6 +100,93 @@ def test_server_rejects_bad_sample(config1):
         t = srv.submit(3, r1, r2)
         res, info = srv.wait(t)
         assert res.recs.shape[0] == 20 and info["batches"] == 1
+        srv.close()
+    finally:
+        ctx.close()
+
+
+# ---- failures met on the host: nothing here faults a GPU ------
+
+def test_server_creation_without_room_is_enomem(config1):
+    """A reserve above the free device memory leaves no room for a batch
+    slot: creation fails with HERA_GPU_ENOMEM and the context stays usable."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ann, tx, ix = config1
+    ctx = api.Context(ix)
+    try:
+        with pytest.raises(api.HeraGpuError) as e:
+            api.Server(ctx, batch_pairs=4096, hbm_reserve=1 << 50)
+        assert e.value.code == -3
+        r1, r2 = workloads.pairs("config1", ann, tx, 200, seed=6)
+        assert ctx.align_pairs(r1, r2, 1).recs.shape[0] == 400
+    finally:
+        ctx.close()
+
+
+def test_cancel_drops_one_sample_only(config1):
+    """A sample cancelled while its chunks wait in the queue: its chunks not
+    yet admitted end with HERA_GPU_ECANCELED, and every other sample's
+    chunks come back exactly as aligned alone."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api
+    ann, tx, ix = config1
+    ctx = api.Context(ix)
+    try:
+        chunks = []
+        for k in range(12):
+            r1, r2 = workloads.pairs("config1", ann, tx, 6000, seed=300 + k)
+            chunks.append((k % 3, r1, r2))
+        alone = [ctx.align_pairs(r1, r2, 1).canonical() for _, r1, r2 in chunks]
+        # one slot and small batches: most of the plan waits in the queue
+        srv = api.Server(ctx, batch_pairs=1024, max_slots=1, write_bam=1, max_samples=4)
+        tickets = [srv.submit(s, r1, r2) for s, r1, r2 in chunks]
+        n = srv.cancel(1)
+        assert n >= 1
+        cancelled = 0
+        for k, (s, r1, r2) in enumerate(chunks):
+            if s == 1:
+                try:
+                    res, _ = srv.wait(tickets[k])
+                    assert res.canonical() == alone[k]   # admitted before the cancel
+                except api.HeraGpuError as e:
+                    assert e.code == api.HERA_GPU_ECANCELED
+                    cancelled += 1
+            else:
+                res, _ = srv.wait(tickets[k])
+                assert res.canonical() == alone[k], f"chunk {k} of sample {s}"
+        assert cancelled == n
+        # the sample can submit again
+        t = srv.submit(1, chunks[1][1], chunks[1][2])
+        assert srv.wait(t)[0].canonical() == alone[1]
+        srv.close()
+    finally:
+        ctx.close()
+
+
+def test_bad_chunk_in_a_mix_fails_alone(config1):
+    """A chunk with a read longer than HERA_GPU_MAX_READ, submitted between
+    others, is refused at submit with HERA_GPU_EINVAL; the chunks around it
+    are served as if it had never come."""
+    if not __import__("torch").cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hera_b200 import api, synth
+    ann, tx, ix = config1
+    ctx = api.Context(ix)
+    try:
+        good = [workloads.pairs("config1", ann, tx, 3000, seed=400 + k) for k in range(4)]
+        alone = [ctx.align_pairs(r1, r2, 1).canonical() for r1, r2 in good]
+        b1, b2 = synth.simulate_pairs(tx, 50, seed=410, read_len=api.MAX_READ + 40)
+        srv = api.Server(ctx, batch_pairs=2048, max_slots=2, write_bam=1, max_samples=4)
+        tickets = [srv.submit(0, *good[0]), srv.submit(1, *good[1])]
+        with pytest.raises(api.HeraGpuError) as e:
+            srv.submit(2, b1, b2)
+        assert e.value.code == -4
+        tickets += [srv.submit(2, *good[2]), srv.submit(3, *good[3])]
+        for k, t in enumerate(tickets):
+            assert srv.wait(t)[0].canonical() == alone[k]
         srv.close()
     finally:
         ctx.close()
