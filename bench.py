@@ -746,6 +746,37 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
     leg = {"pairs": n, "record_bytes": int(off[-1]), "device_ms": round(ms, 3),
            "pairs_per_s_device": n / (ms / 1e3), "pairs_per_s_call": n / wall,
            "record_gbs_device": int(off[-1]) / (ms / 1e3) / 1e9}
+    # BGZF framing stays with the caller: what it costs on the host cores.
+    # The records in 64 KiB blocks, each deflated at zlib's default level
+    # (hera's COMPRESS_LEVEL -1) as its own raw stream, on 1 thread and on
+    # all threads (zlib releases the GIL).
+    try:
+        import zlib
+        from concurrent.futures import ThreadPoolExecutor
+        data = memoryview(out)
+        B = 0xff00
+
+        def deflate(lo):
+            c = zlib.compressobj(-1, zlib.DEFLATED, -15)
+            return len(c.compress(data[lo:lo + B])) + len(c.flush())
+
+        starts = list(range(0, len(data), B))
+        one = starts[:max(1, min(len(starts), (64 << 20) // B))]
+        t0 = time.perf_counter()
+        for lo in one:
+            deflate(lo)
+        t1 = time.perf_counter() - t0
+        cores = os.cpu_count() or 1
+        with ThreadPoolExecutor(cores) as ex:
+            t0 = time.perf_counter()
+            zbytes = sum(ex.map(deflate, starts))
+            tn = time.perf_counter() - t0
+        mb1 = len(one) * B / t1 / 1e6
+        leg["host_bgzf"] = {"mb_per_s_1_thread": round(mb1, 1), "mb_per_s_all": round(len(data) / tn / 1e6, 1),
+                            "threads": cores, "pairs_per_s_all": n / tn, "ratio": round(len(data) / zbytes, 2),
+                            "note": "deflate of the records (hera's bam_write on the host cores)"}
+    except Exception as e:
+        leg["host_bgzf"] = {"error": str(e)}
     try:
         import oracle   # the CPU baseline of this leg: the writer restated in C
         k = min(cpu_sample, n)

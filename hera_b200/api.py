@@ -887,6 +887,28 @@ class BamWriter:
             raise HeraGpuError(rc, self.lib.hera_gpu_bam_last_error(self.h).decode())
         return out[:int(off[-1])], off, ms.value
 
+    def single(self, res: "Result", rs, qual: np.ndarray, names: np.ndarray, cap: int = 0):
+        """(bytes, per-read offsets, device ms) of the records of rs.n single
+        reads (align_single_read's writes)."""
+        n = rs.n
+        a = Context._reads(rs)
+        cap = cap or int(rs.len.sum()) * 8 + 4096 * n + 4096
+        out = np.zeros(cap, np.uint8)
+        off = np.zeros(n + 1, np.uint64)
+        ms = C.c_float()
+        self.lib.hera_gpu_bam_single.argtypes = [C.c_void_p, C.POINTER(_Result), C.c_int32, C.POINTER(_Reads),
+                                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_uint64,
+                                                 C.c_void_p, C.POINTER(C.c_float)]
+        args = (self.h, C.byref(res.c), n, C.byref(a), _ptr(qual), _ptr(names), names.shape[1])
+        rc = self.lib.hera_gpu_bam_single(*args, _ptr(out), cap, _ptr(off), C.byref(ms))
+        if rc == HERA_GPU_ECAPACITY and int(off[-1]) > cap:
+            cap = int(off[-1])
+            out = np.zeros(cap, np.uint8)
+            rc = self.lib.hera_gpu_bam_single(*args, _ptr(out), cap, _ptr(off), C.byref(ms))
+        if rc != HERA_GPU_OK:
+            raise HeraGpuError(rc, self.lib.hera_gpu_bam_last_error(self.h).decode())
+        return out[:int(off[-1])], off, ms.value
+
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.hera_gpu_bam_destroy(self.h)

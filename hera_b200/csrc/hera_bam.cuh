@@ -16,6 +16,7 @@ struct Inputs {
 	const int64_t *off1, *off2;
 	const int32_t *len1, *len2;
 	int32_t stride;
+	int paired;             // 0: single reads (align_single_read's writes)
 	bamw::GeneMap g;
 	const uint32_t *qual_table;
 };
@@ -37,6 +38,27 @@ __device__ __forceinline__ uint32_t one_pair(const Inputs &in, int64_t i, uint8_
 	return x.err;
 }
 
+// align_single_read's records of read i (src/hash_align.c:1825-1834)
+__device__ __forceinline__ uint32_t one_single(const Inputs &in, int64_t i, uint8_t *out, uint64_t at,
+					       uint64_t *bytes)
+{
+	bamw::Ctx x{in.g, in.qual_table, 0};
+	bamw::Core cc[2];
+	bamw::Sink o{out, at};
+	bamw::Read a{in.seq1 + in.off1[i], in.qual1 + in.off1[i], in.name1 + i * in.stride, in.len1[i], false, 0, -1};
+	a.name_l = bamw::name_length(a.name, in.stride);
+	const bamw::Cand r = bamw::cand(in.recs[i], in.pos, in.pp, in.ops, in.miss);
+	bamw::tail_single(x, o, cc, r, a);
+	*bytes = o.at - at;
+	return x.err;
+}
+
+__device__ __forceinline__ uint32_t one_item(const Inputs &in, int64_t i, uint8_t *out, uint64_t at,
+					     uint64_t *bytes)
+{
+	return in.paired ? one_pair(in, i, out, at, bytes) : one_single(in, i, out, at, bytes);
+}
+
 __global__ void k_bam_size(Inputs in, int64_t n, unsigned long long *size, uint32_t *err)
 {
 	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -47,7 +69,7 @@ __global__ void k_bam_size(Inputs in, int64_t n, unsigned long long *size, uint3
 		return;
 	}
 	uint64_t bytes = 0;
-	const uint32_t e = one_pair(in, i, nullptr, 0, &bytes);
+	const uint32_t e = one_item(in, i, nullptr, 0, &bytes);
 	size[i] = bytes;
 	if (e)
 		atomicOr(err, e);
@@ -59,7 +81,7 @@ __global__ void k_bam_write(Inputs in, int64_t n, const unsigned long long *off,
 	if (i >= n)
 		return;
 	uint64_t bytes = 0;
-	one_pair(in, i, out, off[i], &bytes);
+	one_item(in, i, out, off[i], &bytes);
 }
 
 }   // namespace bamk
@@ -147,15 +169,18 @@ extern "C" const char *hera_gpu_bam_last_error(const hera_gpu_bam *b)
 	return b ? b->err.c_str() : "null BAM writer";
 }
 
-extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const hera_gpu_reads *r1,
-				  const hera_gpu_reads *r2, const char *qual1, const char *qual2, const char *name1,
-				  const char *name2, int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off,
-				  float *kernel_ms)
+// the records of n pairs (r2 given) or n single reads (r2, qual2 and
+// name2 null): inputs copied to the device, size pass, scan, write pass
+static int bam_run(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const hera_gpu_reads *r1,
+		   const hera_gpu_reads *r2, const char *qual1, const char *qual2, const char *name1,
+		   const char *name2, int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off,
+		   float *kernel_ms)
 {
-	if (!b)
-		return HERA_GPU_EINVAL;
-	if (!res || n < 0 || !r1 || !r2 || !qual1 || !qual2 || !name1 || !name2 || name_stride < 1 || !out_off ||
-	    (n > 0 && (!res->recs || !r1->seq || !r1->off || !r1->len || !r2->seq || !r2->off || !r2->len)))
+	const bool paired = r2 != nullptr;
+	if (!res || n < 0 || !r1 || !qual1 || !name1 || name_stride < 1 || !out_off ||
+	    (paired && (!qual2 || !name2)) ||
+	    (n > 0 && (!res->recs || !r1->seq || !r1->off || !r1->len ||
+		       (paired && (!r2->seq || !r2->off || !r2->len)))))
 		return bam_fail(b, HERA_GPU_EINVAL, "bad argument");
 	out_off[0] = 0;
 	if (n == 0)
@@ -163,35 +188,37 @@ extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, i
 	if (cudaSetDevice(b->device) != cudaSuccess)
 		return bam_fail(b, HERA_GPU_ENODEV, "cudaSetDevice");
 	// the extents of the host inputs
+	const int per = paired ? 2 : 1;
 	int64_t ext1 = 0, ext2 = 0;
 	for (int32_t i = 0; i < n; ++i) {
-		if (r1->len[i] < 0 || r2->len[i] < 0 || r1->off[i] < 0 || r2->off[i] < 0)
+		if (r1->len[i] < 0 || r1->off[i] < 0 || (paired && (r2->len[i] < 0 || r2->off[i] < 0)))
 			return bam_fail(b, HERA_GPU_EINVAL, "negative read offset or length");
 		ext1 = std::max<int64_t>(ext1, r1->off[i] + r1->len[i]);
-		ext2 = std::max<int64_t>(ext2, r2->off[i] + r2->len[i]);
+		if (paired)
+			ext2 = std::max<int64_t>(ext2, r2->off[i] + r2->len[i]);
 	}
-	for (int64_t k = 0; k < 2 * (int64_t)n; ++k)
+	for (int64_t k = 0; k < per * (int64_t)n; ++k)
 		for (int s = 0; s < 2; ++s)
 			if ((uint64_t)res->recs[k].list_off[s] + (uint32_t)res->recs[k].n[s] > res->list_used ||
 			    (uint64_t)res->recs[k].cig_off[s] + res->recs[k].n_cigar[s] > res->op_used ||
 			    (uint64_t)res->recs[k].miss_off[s] + res->recs[k].n_miss[s] > res->miss_used ||
 			    res->recs[k].n[s] < 0)
 				return bam_fail(b, HERA_GPU_EINVAL, "a record points outside its pools");
-	for (int64_t k = 0; k < 2 * (int64_t)n; ++k)
+	for (int64_t k = 0; k < per * (int64_t)n; ++k)
 		for (int s = 0; s < 2; ++s)
 			for (int32_t j = 0; j < res->recs[k].n[s]; ++j)
 				if (res->pos_pool[res->recs[k].list_off[s] + j] >= b->n_trans)
 					return bam_fail(b, HERA_GPU_EINVAL, "a hit names no transcript of the gene map");
 	for (int32_t i = 0; i < n; ++i)   // names end within their slots
 		if (bamw::name_length(name1 + (int64_t)i * name_stride, name_stride) >= name_stride ||
-		    bamw::name_length(name2 + (int64_t)i * name_stride, name_stride) >= name_stride)
+		    (paired && bamw::name_length(name2 + (int64_t)i * name_stride, name_stride) >= name_stride))
 			return bam_fail(b, HERA_GPU_EINVAL, "a read name without a NUL inside its slot");
 	const cudaStream_t st = b->stream;
-	const size_t nrec = 2 * (size_t)n, nl = res->list_used, no = res->op_used, nm = res->miss_used;
-	const size_t names = (size_t)n * name_stride;
+	const size_t nrec = (size_t)per * n, nl = res->list_used, no = res->op_used, nm = res->miss_used;
+	const size_t names = (size_t)n * name_stride, names2 = paired ? names : 0;
 	// one device block for the inputs, 16-byte aligned pieces
 	size_t sz[12] = {nrec * sizeof(hera_cand_rec), nl * 4 + 4, nl * 4 + 4, no * 4 + 4, nm + 1,
-			 (size_t)ext1 + 1, (size_t)ext2 + 1, (size_t)ext1 + 1, (size_t)ext2 + 1, names, names,
+			 (size_t)ext1 + 1, (size_t)ext2 + 1, (size_t)ext1 + 1, (size_t)ext2 + 1, names, names2,
 			 (size_t)n * 2 * 8 + (size_t)n * 2 * 4};
 	size_t at[12], total = 0;
 	for (int k = 0; k < 12; ++k) {
@@ -220,13 +247,15 @@ extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, i
 	std::vector<int64_t> offs(2 * (size_t)n);
 	std::vector<int32_t> lens(2 * (size_t)n);
 	std::memcpy(offs.data(), r1->off, n * 8ull);
-	std::memcpy(offs.data() + n, r2->off, n * 8ull);
 	std::memcpy(lens.data(), r1->len, n * 4ull);
-	std::memcpy(lens.data() + n, r2->len, n * 4ull);
-	const void *src[11] = {res->recs, res->pos_pool, res->p_pool, res->op_pool, res->miss_pool, r1->seq, r2->seq,
-			       qual1, qual2, name1, name2};
+	if (paired) {
+		std::memcpy(offs.data() + n, r2->off, n * 8ull);
+		std::memcpy(lens.data() + n, r2->len, n * 4ull);
+	}
+	const void *src[11] = {res->recs, res->pos_pool, res->p_pool, res->op_pool, res->miss_pool, r1->seq,
+			       paired ? r2->seq : nullptr, qual1, qual2, name1, name2};
 	const size_t len_src[11] = {nrec * sizeof(hera_cand_rec), nl * 4, nl * 4, no * 4, nm, (size_t)ext1,
-				    (size_t)ext2, (size_t)ext1, (size_t)ext2, names, names};
+				    (size_t)ext2, (size_t)ext1, (size_t)ext2, names, names2};
 	cudaEventRecord(b->ev0, st);
 	for (int k = 0; k < 11 && rc == HERA_GPU_OK; ++k)
 		if (len_src[k] && (e = cudaMemcpyAsync(d_in + at[k], src[k], len_src[k], cudaMemcpyHostToDevice, st)) !=
@@ -260,6 +289,7 @@ extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, i
 	in.len1 = (const int32_t *)(d_in + at[11] + n * 16ull);
 	in.len2 = in.len1 + n;
 	in.stride = name_stride;
+	in.paired = paired ? 1 : 0;
 	const uint32_t *m = b->d_map;
 	in.g = bamw::GeneMap{b->n_chr, m + b->off_chr_len, m + b->off_exon_off, m + b->off_starts, m + b->off_ends,
 			     m + b->off_chr, m + b->off_gene};
@@ -302,4 +332,26 @@ extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, i
 		*kernel_ms = b->kernel_ms;
 	release();
 	return HERA_GPU_OK;
+}
+
+extern "C" int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const hera_gpu_reads *r1,
+				  const hera_gpu_reads *r2, const char *qual1, const char *qual2, const char *name1,
+				  const char *name2, int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off,
+				  float *kernel_ms)
+{
+	if (!b)
+		return HERA_GPU_EINVAL;
+	if (!r2 || !qual2 || !name2)
+		return bam_fail(b, HERA_GPU_EINVAL, "bad argument");
+	return bam_run(b, res, n, r1, r2, qual1, qual2, name1, name2, name_stride, out, cap, out_off, kernel_ms);
+}
+
+extern "C" int hera_gpu_bam_single(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n,
+				   const hera_gpu_reads *reads, const char *qual, const char *name,
+				   int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off, float *kernel_ms)
+{
+	if (!b)
+		return HERA_GPU_EINVAL;
+	return bam_run(b, res, n, reads, nullptr, qual, nullptr, name, nullptr, name_stride, out, cap, out_off,
+		       kernel_ms);
 }

@@ -659,6 +659,15 @@ int hera_gpu_bam_pairs(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n,
 		       const char *name2, int32_t name_stride, uint8_t *out, uint64_t cap,
 		       uint64_t *out_off, float *kernel_ms);
 
+/* The records align_single_read writes for n single reads
+ * (src/hash_align.c:1825-1834, bam_write_single src/bam_write.c:418-446):
+ * `res` as hera_gpu_align_single_flat left it with write_bam = 0; the rest
+ * as for hera_gpu_bam_pairs with one read, quality and name per item. */
+int hera_gpu_bam_single(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n,
+			const hera_gpu_reads *reads, const char *qual, const char *name,
+			int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off,
+			float *kernel_ms);
+
 /* Device time (CUDA events, from the first kernel of the last add call to
  * its end; the call's first-use allocations are not in it) and the
  * kernels it launched. */

@@ -1,7 +1,8 @@
-"""The tail's BAM records (`-w`) on the device (hera_gpu_bam_pairs): the
-pairs aligned on the device with traceback, then their records written on
-the device, against the bytes the reference's own align_pair_read wrote for
-the same reads (tests/golden/bam.npz)."""
+"""The tail's BAM records (`-w`) on the device (hera_gpu_bam_pairs,
+hera_gpu_bam_single): the reads aligned on the device with traceback, then
+their records written on the device, against the bytes the reference's own
+align_pair_read / align_single_read wrote for the same reads
+(tests/golden/bam.npz)."""
 import json
 import os
 
@@ -56,3 +57,19 @@ def test_device_bam_records_golden(writer, name):
     bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
     assert not bad, f"{name}: {len(bad)} pairs' records differ, first {bad[0]}"
     assert ms > 0
+
+
+def test_device_bam_single_records_golden(writer):
+    """The 800 golden single reads: align_single_read's records."""
+    ctx, w = writer
+    c = np.load(os.path.join(GOLD, "candidates.npz"))
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    n = int(d["single_n"][0])
+    rs = synth.ReadSet(c["single_seq"], c["single_off"], c["single_len"]).subset(np.arange(n))
+    res = ctx.align_single(rs, 0)
+    q = np.full(rs.seq.shape[0] + 1, ord("?"), np.uint8)
+    got, off, ms = w.single(res, rs, q, oracle.read_names(n, 1))
+    want, woff = d["single_bam"], d["single_bam_off"]
+    bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
+    assert not bad, f"{len(bad)} reads' records differ, first {bad[0]}"
+    assert n >= 800 and ms > 0
