@@ -741,11 +741,25 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
             wall = time.perf_counter() - t0
         finally:
             w.close()
+        # the records' BGZF framing on the device (hera_gpu_bgzf, host buffers)
+        bgz = None
+        try:
+            import gzip
+            ctx.bgzf(out[:1 << 20])   # warm
+            t0 = time.perf_counter()
+            z, zms = ctx.bgzf(out)
+            zwall = time.perf_counter() - t0
+            bgz = {"device_ms": round(zms, 3), "call_ms": round(zwall * 1e3, 3),
+                   "gbs_device": len(out) / (zms / 1e3) / 1e9, "pairs_per_s_call": n / zwall,
+                   "ratio": round(len(out) / max(1, len(z)), 2),
+                   "decompresses_to_records": bool(gzip.decompress(z.tobytes()) == out.tobytes())}
+        except Exception as e:
+            bgz = {"error": str(e)}
     finally:
         ctx.close()
     leg = {"pairs": n, "record_bytes": int(off[-1]), "device_ms": round(ms, 3),
            "pairs_per_s_device": n / (ms / 1e3), "pairs_per_s_call": n / wall,
-           "record_gbs_device": int(off[-1]) / (ms / 1e3) / 1e9}
+           "record_gbs_device": int(off[-1]) / (ms / 1e3) / 1e9, "bgzf_device": bgz}
     # BGZF framing stays with the caller: what it costs on the host cores.
     # The records in 64 KiB blocks, each deflated at zlib's default level
     # (hera's COMPRESS_LEVEL -1) as its own raw stream, on 1 thread and on

@@ -529,6 +529,19 @@ class Context:
         self._check(rc)
         return ms
 
+    def bgzf(self, data) -> tuple:
+        """(BGZF bytes, device ms) of a byte buffer (hera_gpu_bgzf)."""
+        a = np.frombuffer(data, np.uint8) if not isinstance(data, np.ndarray) else data
+        a = np.ascontiguousarray(a, np.uint8)
+        cap = a.size + (a.size // 0xff00 + 1) * 64 + 64
+        out = np.empty(cap, np.uint8)
+        used, ms = C.c_uint64(), C.c_float()
+        self.lib.hera_gpu_bgzf.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                           C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        self._check(self.lib.hera_gpu_bgzf(self.h, _ptr(a) if a.size else None, a.size, _ptr(out), cap,
+                                           C.byref(used), C.byref(ms)))
+        return out[:used.value], ms.value
+
     def fetch(self, n_recs: int) -> Result:
         res = Result(n_recs, n_recs * 8 + 1024, n_recs * 8 + 1024, n_recs * 8 + 1024)
         rc = self.lib.hera_gpu_fetch_result(self.h, C.byref(res.c))

@@ -18,7 +18,8 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhera_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("hera_gpu.cu",)]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("hera_device.cuh", "hera_batched.cuh", "hera_server.cuh", "hera_fastq.cuh",
-                                                                   "hera_classes.cuh", "hera_bam.cuh", "hera_bam_core.h")] + [
+                                                                   "hera_classes.cuh", "hera_bam.cuh", "hera_bam_core.h",
+                                                                   "hera_bgzf.cuh", "hera_bgzf_core.h")] + [
                   os.path.join(ROOT, "include", "hera_gpu.h")]
 
 NVCC_FLAGS = [

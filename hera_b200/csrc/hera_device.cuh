@@ -637,7 +637,10 @@ struct BitRows<4> {            // W = 10, values <= 6: planes b0..b2 in one word
 	}
 };
 
-template <int E, class Cig>
+// STORE = false: no row is kept, and a DP that stops early returns -1
+// without a result (its shrink loop needs the rows: the caller reruns it
+// with STORE = true); only for the score-only mode.
+template <int E, bool STORE, class Cig>
 __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
 				    bool score_only, Cig &cig, typename BitRows<E>::T *__restrict__ rows, int &flags,
 				    uint32_t &cells)
@@ -655,6 +658,8 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 	};
 	// a thermometer row stored as planes of its binary values
 	auto store = [&](int k, const uint32_t (&G)[NT + 1]) {
+		if (!STORE)
+			return;
 		uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
 #pragma unroll
 		for (int t = 1; t <= NT; ++t) {
@@ -775,6 +780,8 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 			G[t] = V[t];
 		store(k, G);
 		if (min == error) {
+			if (!STORE)
+				return -1;   // early stop: the shrink loop needs the rows
 			++k;
 			break;
 		}
@@ -783,6 +790,8 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 
 	int score = 0;
 	if (min >= error) {
+		if constexpr (!STORE)
+			return -1;
 		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
 			--k;
 			// The reference scans row k from column 0 to its break.  Cells
@@ -824,6 +833,9 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}
+	if constexpr (!STORE)
+		return -1;
+	else {
 	while (i > 0 && k > 0) {
 		const unsigned cur = get(i, k);
 		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
@@ -847,6 +859,7 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 	for (int t = 1; t <= k; ++t)
 		cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	return score;
+	}
 }
 
 // Entry used by the per-task (plain) path: the banded form, which keeps the

@@ -668,6 +668,19 @@ int hera_gpu_bam_single(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n,
 			int32_t name_stride, uint8_t *out, uint64_t cap, uint64_t *out_off,
 			float *kernel_ms);
 
+/* BGZF, the BAM container (hera's bam_write, src/hash_align.c:48-136), on
+ * the device: in[0 .. n) (host memory) becomes back-to-back BGZF blocks of
+ * at most 65280 input bytes each in out (host, cap bytes); *out_len = the
+ * bytes written (or needed, with HERA_GPU_ECAPACITY).  Each block is a
+ * gzip member with the BGZF extra field, a DEFLATE stream (greedy LZ77,
+ * fixed Huffman codes, or stored when that is not smaller) and the CRC-32
+ * and size of its input: the bytes differ from zlib's, the decompressed
+ * stream is the input.  No end-of-file block is added (hera's bam_close
+ * writes it).  Allocates device memory.  *kernel_ms (may be NULL): device
+ * time of the compression and packing. */
+int hera_gpu_bgzf(hera_gpu_ctx *ctx, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t cap,
+		  uint64_t *out_len, float *kernel_ms);
+
 /* Device time (CUDA events, from the first kernel of the last add call to
  * its end; the call's first-use allocations are not in it) and the
  * kernels it launched. */

@@ -73,3 +73,30 @@ def test_device_bam_single_records_golden(writer):
     bad = [i for i in range(n) if got[off[i]:off[i + 1]].tobytes() != want[woff[i]:woff[i + 1]].tobytes()]
     assert not bad, f"{len(bad)} reads' records differ, first {bad[0]}"
     assert n >= 800 and ms > 0
+
+
+def test_device_bgzf_decompresses_to_input(writer):
+    """BGZF on the device (hera_gpu_bgzf): the golden BAM records of every
+    set, random and constant buffers, and sizes at the block boundary; each
+    result a valid BGZF stream that decompresses to its input, and the
+    records' stream at most half their size."""
+    import gzip
+    import struct
+    ctx, _ = writer
+    d = np.load(os.path.join(GOLD, "bam.npz"))
+    rng = np.random.default_rng(9)
+    recs = b"".join(d[f"{k}_bam"].tobytes() for k in SETS)
+    cases = [recs, rng.integers(0, 256, 300_000, dtype=np.uint8).tobytes(), b"Q" * 0xff00, b"Q" * (0xff00 + 1),
+             b"ACGT", recs * 9]
+    for data in cases:
+        z, ms = ctx.bgzf(data)
+        z = z.tobytes()
+        o, blocks = 0, 0
+        while o < len(z):
+            assert z[o:o + 4] == b"\x1f\x8b\x08\x04" and z[o + 12:o + 16] == b"BC\x02\x00"
+            o += struct.unpack_from("<H", z, o + 16)[0] + 1
+            blocks += 1
+        assert o == len(z) and blocks == -(-len(data) // 0xff00)
+        assert gzip.decompress(z) == data
+    z, _ = ctx.bgzf(recs)
+    assert len(z) < len(recs) / 2
