@@ -790,36 +790,38 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 
 	int score = 0;
 	if (min >= error) {
-		if constexpr (!STORE)
+		if constexpr (!STORE) {
 			return -1;
-		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
-			--k;
-			// The reference scans row k from column 0 to its break.  Cells
-			// left of the window are zero there and here (no effect: jj
-			// stays 0), and the break marker or ref_len lies inside the
-			// window, so the scan covers the window only.
-			int jj = 0;
-			const int c_lo = k - E > 0 ? k - E : 0;
-			const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
-			for (int c = c_lo; c < c_hi; ++c) {
-				const unsigned v = get(k, c);
-				if (v == error + 1)
-					break;
-				if (v > 0)
-					jj = (int)error;
-				if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
-					min = v;
-					xmin = (unsigned)c;
+		} else {
+			while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+				--k;
+				// The reference scans row k from column 0 to its break.  Cells
+				// left of the window are zero there and here (no effect: jj
+				// stays 0), and the break marker or ref_len lies inside the
+				// window, so the scan covers the window only.
+				int jj = 0;
+				const int c_lo = k - E > 0 ? k - E : 0;
+				const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
+				for (int c = c_lo; c < c_hi; ++c) {
+					const unsigned v = get(k, c);
+					if (v == error + 1)
+						break;
+					if (v > 0)
+						jj = (int)error;
+					if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
+						min = v;
+						xmin = (unsigned)c;
+					}
 				}
 			}
+			if (k < 5) {
+				cig_add(cig, OP_S, len, nullptr, flags);
+				return (int)len;
+			}
+			cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
+			score = (int)len - k;
+			i = k;
 		}
-		if (k < 5) {
-			cig_add(cig, OP_S, len, nullptr, flags);
-			return (int)len;
-		}
-		cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
-		score = (int)len - k;
-		i = k;
 	} else {
 		if (xmin < len && k == (int)len) {
 			min += len - xmin;
