@@ -477,8 +477,15 @@ def main():
                 log(f"{name} leg failed: {e}")
                 legs[name] = {"error": str(e)}
         del orc, chunks
+        ix1 = None
         if not args.no_config_legs or not args.no_serve:
-            ann1, tx1, ix1 = workloads.build("config1", device=f"cuda:{local}")
+            try:
+                ann1, tx1, ix1 = workloads.build("config1", device=f"cuda:{local}")
+            except Exception as e:   # the line is still printed, the legs carry the error
+                log(f"config1 index failed: {e}")
+                for name in ("config3", "config4", "serving"):
+                    legs[name] = {"error": f"config1 index: {e}"}
+        if ix1 is not None:
             orc1 = None
             if not args.no_parity:
                 try:

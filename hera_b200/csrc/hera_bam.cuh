@@ -1,7 +1,8 @@
 // hera_bam.cuh -- the host tail's BAM records (`-w`) on the device: one
-// thread per read pair runs hera_bam_core.h's writer twice, first for the
-// pair's byte count, then -- after a scan of the counts -- into its place
-// in the output.  BGZF compression stays with the caller (hera's bam_write).
+// thread per read pair (or single read) runs hera_bam_core.h's writer
+// twice, first for the item's byte count, then -- after a scan of the
+// counts -- into its place in the output.  The records leave uncompressed
+// (BGZF: hera's bam_write, or hera_gpu_bgzf).
 
 #include "hera_bam_core.h"
 
@@ -16,49 +17,69 @@ struct Inputs {
 	const int64_t *off1, *off2;
 	const int32_t *len1, *len2;
 	int32_t stride;
-	int paired;             // 0: single reads (align_single_read's writes)
+	int64_t ext1, ext2;     // bytes of seq1/qual1 and seq2/qual2 on the device
+	uint64_t nl, no, nm;    // entries of the list, op and miss pools
 	bamw::GeneMap g;
 	const uint32_t *qual_table;
 };
 
-__device__ __forceinline__ uint32_t one_pair(const Inputs &in, int64_t i, uint8_t *out, uint64_t at,
-					     uint64_t *bytes)
+// an item's inputs lie inside the device copies (the host checked the
+// same on its side; this re-checks what arrived, so that a bad copy is an
+// error bit rather than a stray read)
+constexpr uint32_t E_INPUT = 1u << 30;
+
+__device__ __forceinline__ bool rec_ok(const Inputs &in, const hera_cand_rec &r)
 {
-	bamw::Ctx x{in.g, in.qual_table, 0};
-	bamw::Core cc[2];
-	bamw::Sink o{out, at};
-	bamw::Read a{in.seq1 + in.off1[i], in.qual1 + in.off1[i], in.name1 + i * in.stride, in.len1[i], false, 0, -1};
-	bamw::Read b{in.seq2 + in.off2[i], in.qual2 + in.off2[i], in.name2 + i * in.stride, in.len2[i], false, 0, -1};
-	a.name_l = bamw::name_length(a.name, in.stride);
-	b.name_l = bamw::name_length(b.name, in.stride);
-	const bamw::Cand r0 = bamw::cand(in.recs[2 * i], in.pos, in.pp, in.ops, in.miss);
-	const bamw::Cand r1 = bamw::cand(in.recs[2 * i + 1], in.pos, in.pp, in.ops, in.miss);
-	bamw::tail(x, o, cc, r0, r1, a, b);
-	*bytes = o.at - at;
-	return x.err;
+	for (int s = 0; s < 2; ++s)
+		if (r.n[s] < 0 || (uint64_t)r.list_off[s] + (uint32_t)r.n[s] > in.nl ||
+		    (uint64_t)r.cig_off[s] + r.n_cigar[s] > in.no || (uint64_t)r.miss_off[s] + r.n_miss[s] > in.nm)
+			return false;
+	return true;
 }
 
-// align_single_read's records of read i (src/hash_align.c:1825-1834)
-__device__ __forceinline__ uint32_t one_single(const Inputs &in, int64_t i, uint8_t *out, uint64_t at,
-					       uint64_t *bytes)
+template <bool PAIRED>
+__device__ __forceinline__ bool item_ok(const Inputs &in, int64_t i)
 {
-	bamw::Ctx x{in.g, in.qual_table, 0};
-	bamw::Core cc[2];
-	bamw::Sink o{out, at};
-	bamw::Read a{in.seq1 + in.off1[i], in.qual1 + in.off1[i], in.name1 + i * in.stride, in.len1[i], false, 0, -1};
-	a.name_l = bamw::name_length(a.name, in.stride);
-	const bamw::Cand r = bamw::cand(in.recs[i], in.pos, in.pp, in.ops, in.miss);
-	bamw::tail_single(x, o, cc, r, a);
-	*bytes = o.at - at;
-	return x.err;
+	if (in.off1[i] < 0 || in.len1[i] < 0 || in.off1[i] + in.len1[i] > in.ext1)
+		return false;
+	if (PAIRED) {
+		if (in.off2[i] < 0 || in.len2[i] < 0 || in.off2[i] + in.len2[i] > in.ext2)
+			return false;
+		return rec_ok(in, in.recs[2 * i]) && rec_ok(in, in.recs[2 * i + 1]);
+	}
+	return rec_ok(in, in.recs[i]);
 }
 
+// the records of item i (a pair: align_pair_read's writes; a single read:
+// align_single_read's, src/hash_align.c:1825-1834); size pass: out null
+template <bool PAIRED>
 __device__ __forceinline__ uint32_t one_item(const Inputs &in, int64_t i, uint8_t *out, uint64_t at,
-					     uint64_t *bytes)
+					     uint64_t end, uint64_t *bytes)
 {
-	return in.paired ? one_pair(in, i, out, at, bytes) : one_single(in, i, out, at, bytes);
+	*bytes = 0;
+	if (!item_ok<PAIRED>(in, i))
+		return E_INPUT;
+	bamw::Ctx x{in.g, in.qual_table, 0};
+	bamw::Core cc[2];
+	bamw::Sink o{out, at, end};
+	bamw::Read a{in.seq1 + in.off1[i], in.qual1 + in.off1[i], in.name1 + i * in.stride, in.len1[i], false, 0, -1};
+	a.name_l = bamw::name_length(a.name, in.stride);
+	if constexpr (PAIRED) {
+		bamw::Read b{in.seq2 + in.off2[i], in.qual2 + in.off2[i], in.name2 + i * in.stride, in.len2[i], false, 0,
+			     -1};
+		b.name_l = bamw::name_length(b.name, in.stride);
+		const bamw::Cand r0 = bamw::cand(in.recs[2 * i], in.pos, in.pp, in.ops, in.miss);
+		const bamw::Cand r1 = bamw::cand(in.recs[2 * i + 1], in.pos, in.pp, in.ops, in.miss);
+		bamw::tail(x, o, cc, r0, r1, a, b);
+	} else {
+		const bamw::Cand r = bamw::cand(in.recs[i], in.pos, in.pp, in.ops, in.miss);
+		bamw::tail_single(x, o, cc, r, a);
+	}
+	*bytes = o.at - at;
+	return x.err;
 }
 
+template <bool PAIRED>
 __global__ void k_bam_size(Inputs in, int64_t n, unsigned long long *size, uint32_t *err)
 {
 	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -69,19 +90,25 @@ __global__ void k_bam_size(Inputs in, int64_t n, unsigned long long *size, uint3
 		return;
 	}
 	uint64_t bytes = 0;
-	const uint32_t e = one_item(in, i, nullptr, 0, &bytes);
+	const uint32_t e = one_item<PAIRED>(in, i, nullptr, 0, 0, &bytes);
 	size[i] = bytes;
 	if (e)
 		atomicOr(err, e);
 }
 
-__global__ void k_bam_write(Inputs in, int64_t n, const unsigned long long *off, uint8_t *out)
+// the write pass, into the places the scan of the sizes gave; no byte
+// lands past an item's place, and an item whose bytes differ from its size
+// pass is an error
+template <bool PAIRED>
+__global__ void k_bam_write(Inputs in, int64_t n, const unsigned long long *off, uint8_t *out, uint32_t *err)
 {
 	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
 		return;
 	uint64_t bytes = 0;
-	one_item(in, i, out, off[i], &bytes);
+	const uint32_t e = one_item<PAIRED>(in, i, out, off[i], off[i + 1], &bytes);
+	if ((e & E_INPUT) || off[i] + bytes != off[i + 1])
+		atomicOr(err, E_INPUT);
 }
 
 }   // namespace bamk
@@ -272,7 +299,7 @@ static int bam_run(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const
 		release();
 		return rc;
 	}
-	bamk::Inputs in;
+	bamk::Inputs in{};
 	in.recs = (const hera_cand_rec *)(d_in + at[0]);
 	in.pos = (const uint32_t *)(d_in + at[1]);
 	in.pp = (const int32_t *)(d_in + at[2]);
@@ -289,12 +316,19 @@ static int bam_run(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const
 	in.len1 = (const int32_t *)(d_in + at[11] + n * 16ull);
 	in.len2 = in.len1 + n;
 	in.stride = name_stride;
-	in.paired = paired ? 1 : 0;
+	in.ext1 = ext1;
+	in.ext2 = ext2;
+	in.nl = nl;
+	in.no = no;
+	in.nm = nm;
 	const uint32_t *m = b->d_map;
 	in.g = bamw::GeneMap{b->n_chr, m + b->off_chr_len, m + b->off_exon_off, m + b->off_starts, m + b->off_ends,
 			     m + b->off_chr, m + b->off_gene};
 	in.qual_table = m + b->off_qual;
-	bamk::k_bam_size<<<blocks_for((int64_t)n + 1, 128), 128, 0, st>>>(in, n, d_size, d_err);
+	if (paired)
+		bamk::k_bam_size<true><<<blocks_for((int64_t)n + 1, 128), 128, 0, st>>>(in, n, d_size, d_err);
+	else
+		bamk::k_bam_size<false><<<blocks_for((int64_t)n + 1, 128), 128, 0, st>>>(in, n, d_size, d_err);
 	cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_size, d_off, n + 1, st);
 	unsigned long long used = 0;
 	uint32_t herr = 0;
@@ -303,6 +337,10 @@ static int bam_run(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const
 	    (e = cudaStreamSynchronize(st)) != cudaSuccess) {
 		release();
 		return bam_fail(b, HERA_GPU_ECUDA, "BAM sizes", e);
+	}
+	if (herr & bamk::E_INPUT) {
+		release();
+		return bam_fail(b, HERA_GPU_EINVAL, "BAM inputs on the device outside their copies");
 	}
 	if (herr) {
 		release();
@@ -319,13 +357,21 @@ static int bam_run(hera_gpu_bam *b, const hera_gpu_result *res, int32_t n, const
 		release();
 		return bam_fail(b, HERA_GPU_ENOMEM, "BAM output", e);
 	}
-	bamk::k_bam_write<<<blocks_for((int64_t)n, 128), 128, 0, st>>>(in, n, d_off, d_out);
+	if (paired)
+		bamk::k_bam_write<true><<<blocks_for((int64_t)n, 128), 128, 0, st>>>(in, n, d_off, d_out, d_err);
+	else
+		bamk::k_bam_write<false><<<blocks_for((int64_t)n, 128), 128, 0, st>>>(in, n, d_off, d_out, d_err);
 	cudaEventRecord(b->ev1, st);
 	if ((e = cudaMemcpyAsync(out, d_out, used, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
 	    (e = cudaMemcpyAsync(out_off, d_off, (n + 1) * 8ull, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
 	    (e = cudaStreamSynchronize(st)) != cudaSuccess) {
 		release();
 		return bam_fail(b, HERA_GPU_ECUDA, "BAM records", e);
+	}
+	if (herr) {
+		release();
+		return bam_fail(b, HERA_GPU_EINVAL, "BAM write pass: a pair's bytes differ from its size pass");
 	}
 	cudaEventElapsedTime(&b->kernel_ms, b->ev0, b->ev1);
 	if (kernel_ms)

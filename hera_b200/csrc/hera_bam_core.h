@@ -138,9 +138,10 @@ struct Read {
 struct Sink {
 	uint8_t *out;
 	uint64_t at;
+	uint64_t end = ~0ull;   // no byte is stored at or past end
 	BAM_HD void put(uint8_t b)
 	{
-		if (out)
+		if (out && at < end)
 			out[at] = b;
 		++at;
 	}
