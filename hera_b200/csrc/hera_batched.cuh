@@ -79,6 +79,8 @@ struct Round {
 	int space;
 	const uint2 *hits;        // precomputed seeds (round 0) or null
 	int spr;
+	const uint2 *thits;       // precomputed seeds per task (later rounds: k_seed_req) or null
+	int tspr;
 	TaskInfo *tinfo;
 	Chain *chains;
 	JobSlot *slots;
@@ -216,6 +218,65 @@ __device__ __forceinline__ void task_of(const Round &R, int t, int &pi, int &c, 
 	}
 }
 
+// The seeds of a later round's get_position calls (space 2*ERR on the
+// oriented read, :1322-1344), one thread per (call, seed): the hash
+// lookups the build would make one after another, made side by side so
+// that their latencies overlap.  A seed past the read's end, or a read
+// longer than the batch's maximum, gets no hits (the build never reads it).
+__global__ void __launch_bounds__(256) k_seed_req(Batch b, Round R, uint2 *__restrict__ thits)
+{
+	const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= (int64_t)R.ntask * R.tspr)
+		return;
+	const int t = (int)(idx / R.tspr), sj = (int)(idx % R.tspr);
+	int pi, c, str;
+	task_of(R, t, pi, c, str);
+	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	const int i = sj * R.space;
+	uint2 h = make_uint2(0, 0);
+	if (L <= b.max_len && i + KMER <= L)
+		h = probe(b.ix, kmer_words((str ? b.code_r : b.code) + b.off[ri] + i, false));
+	thits[idx] = h;
+}
+
+// A later round's calls listed largest first, as k_task_list lists round
+// 0's: every call's task info reset, its anchor count (capped at 255) as
+// the sort key, and the number with any hit at *nlist.  A read longer than
+// the batch's maximum flags F_READ (the build's own check).
+__global__ void k_task_key(Batch b, Round R, TaskInfo *__restrict__ tinfo, int *__restrict__ list,
+			   int *__restrict__ nlist, uint8_t *__restrict__ key)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= R.ntask)
+		return;
+	int pi, c, str;
+	task_of(R, t, pi, c, str);
+	tinfo[t].chain0 = 0;
+	tinfo[t].nch = -1;
+	key[t] = 0;
+	list[t] = t;
+	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
+	const int L = b.len[ri];
+	if (L > b.max_len) {
+		flag(b.flags, F_READ);
+		return;
+	}
+	const uint2 *h = R.thits + (int64_t)t * R.tspr;
+	uint32_t w = 0;
+	for (int j = 0; j < R.tspr && j * R.space + KMER <= L; ++j)
+		w += h[j].y;
+	if (w == 0)
+		return;
+	key[t] = (uint8_t)(w < 255 ? w : 255);
+	atomicAdd(nlist, 1);
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+	asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Enumerate the chains of one get_position call in the reference's order
 // (pass A :1367-1390, pass B :1392-1412, pass C :1414-1434); pass A's
 // consumed marks are kept in a bitmask so the walk can be repeated.
@@ -327,10 +388,21 @@ __device__ void build_one(const Batch &b, const Round &R, int t)
 	}
 	const uint8_t *rd = (str ? b.code_r : b.code) + b.off[ri];
 	const uint32_t step = (uint32_t)R.space;
+	// the seeds' hits, when a kernel before this one looked them up
+	const uint2 *pre = R.hits ? R.hits + ((int64_t)ri * 2 + str) * R.spr
+				  : (R.thits ? R.thits + (int64_t)t * R.tspr : nullptr);
+	if (pre) {   // their hit lists' first lines on their way to L2 before the merge
+		int j = 0;
+		for (uint32_t i = 0; i + KMER <= (uint32_t)L; i += step, ++j) {
+			const uint2 h = pre[j];
+			if (h.y)
+				prefetch_l2(b.ix.occ + h.x);
+		}
+	}
 	BuildWork w;
 	int cur = 0, na = 0, sj = 0;
 	for (uint32_t i = 0; i + KMER <= (uint32_t)L; i += step, ++sj) {
-		uint2 h = R.hits ? R.hits[((int64_t)ri * 2 + str) * R.spr + sj] : probe(b.ix, kmer_words(rd + i, false));
+		uint2 h = pre ? pre[sj] : probe(b.ix, kmer_words(rd + i, false));
 		if (h.y == 0)
 			continue;
 		const uint2 *occ = b.ix.occ + h.x;

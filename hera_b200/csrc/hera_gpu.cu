@@ -788,6 +788,8 @@ struct Lane {
 	DBuf<int> perm, hist, tlist;
 	DBuf<int> redo;                      // score-only DP jobs rerun with their rows
 	bool redo_pass = true;               // the allocation-free lane keeps every row instead
+	DBuf<uint2> thits;                   // a later round's seeds, looked up before its build
+	bool seed_req = true;                // the allocation-free lane's build looks them up itself
 	DBuf<int> tval;                      // round 0's calls before the sort by size
 	DBuf<uint8_t> tkey;                  // their anchor counts (2 halves: in, out)
 	bool sort_tasks = true;              // the allocation-free lane keeps the unsorted list
@@ -832,7 +834,7 @@ struct Lane {
 		ovf_list.release(); ovf_slot.release(); wpairs.release(); wwork.release(); wssw_out.release();
 		side_recs.release(); side_pos.release(); side_op.release(); side_p.release(); side_miss.release();
 		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
-		tval.release(); tkey.release(); redo.release();
+		tval.release(); tkey.release(); redo.release(); thits.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
 		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
@@ -1113,6 +1115,7 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	ctx->na->no_wide = true;
 	ctx->na->sort_tasks = false;
 	ctx->na->redo_pass = false;
+	ctx->na->seed_req = false;
 	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    ctx->na->h_small.ensure(32) != cudaSuccess)
 		return bail(HERA_GPU_ECUDA);
@@ -1316,6 +1319,28 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 									       L.tlist.p, d_nl, nullptr);
 			++launches;
 		}
+		R.list = L.tlist.p;
+		R.nlist = d_nl;
+	} else if (L.seed_req) {
+		// a later round: its seeds looked up side by side first, then its
+		// calls sorted largest first as round 0's are
+		R.tspr = b.max_len >= KMER ? (b.max_len - KMER) / R.space + 1 : 1;
+		LK(L.thits.ensure((size_t)R.ntask * R.tspr), "round seeds");
+		k_seed_req<<<blocks_for((int64_t)R.ntask * R.tspr, 256), 256, 0, st>>>(b, R, L.thits.p);
+		R.thits = L.thits.p;
+		LK(L.tlist.ensure(R.ntask), "task list");
+		LK(L.tval.ensure(R.ntask), "task list");
+		LK(L.tkey.ensure(2 * (size_t)R.ntask), "task keys");
+		int *d_nl = L.counters.p + 15;
+		LK(cudaMemsetAsync(d_nl, 0, sizeof(int), st), "memset");
+		k_task_key<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R, L.tinfo.p, L.tval.p, d_nl, L.tkey.p);
+		size_t tmp = 0;
+		cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p, L.tlist.p,
+							  R.ntask, 0, 8, st);
+		LK(L.cub_tmp.ensure(tmp), "sort scratch");
+		cub::DeviceRadixSort::SortPairsDescending(L.cub_tmp.p, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p,
+							  L.tlist.p, R.ntask, 0, 8, st);
+		launches += 3;
 		R.list = L.tlist.p;
 		R.nlist = d_nl;
 	}
