@@ -704,25 +704,28 @@ __device__ __forceinline__ bool dp_job(const Batch &b, const DpJob *__restrict__
 // DP runs in the bit-plane form (sw_align_bits).  With traceback every row
 // is kept (4 bits a slot, in local memory).  In the score-only mode rows
 // serve only the shrink loop of a DP that stops early (18% of the error-8
-// calls): this pass keeps none, and lists those jobs in `redo` (count at
-// *nredo) for k_dp_redo, which runs them again with their rows.
+// calls): this pass keeps none and marks those jobs' places in the order
+// (`rerun[t]` = 1); a stable compaction of the order by the marks lists
+// them, still by (cap, length), for k_dp_redo, which runs them again with
+// their rows.
 template <int E, bool STORE>
 __global__ void __launch_bounds__(128, 8)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
-	 int rcap, int *__restrict__ redo, int *__restrict__ nredo)
+	 int rcap, uint8_t *__restrict__ rerun)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t cells = 0;
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
 		if (!dp_job<E, STORE>(b, jobs, id, res, rcap, cells))
-			redo[atomicAdd(nredo, 1)] = id;
+			rerun[t] = 1;
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
 }
 
 // the score-only mode's early-stopped jobs, with their rows (a grid-stride
-// pass over the list the first pass made; its length is read on the device)
+// pass over the list compacted from the first pass's marks; its length is
+// read on the device)
 template <int E>
 __global__ void __launch_bounds__(128, 8)
 k_dp_redo(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ redo, const int *__restrict__ nredo,
