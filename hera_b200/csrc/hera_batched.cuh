@@ -674,71 +674,37 @@ __device__ __forceinline__ int job_form(const DpJob &j)
 	return 0;
 }
 
-// one DP job of cap E in the bit-plane form; false when a STORE = false
-// run stopped early (no result written: the job is rerun with its rows)
-template <int E, bool STORE>
-__device__ __forceinline__ bool dp_job(const Batch &b, const DpJob *__restrict__ jobs, int id,
-				       uint8_t *__restrict__ res, int rcap, uint32_t &cells)
-{
-	const DpJob jb = jobs[id];
-	typename BitRows<E>::T rows[STORE ? MAX_DP_ROWS + 1 : 1];
-	DCig cig;
-	int flags = 0;
-	uint32_t c = 0;
-	cig.n = cig.nm = 0;
-	const bool rev = jb.err < 0;
-	const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
-	RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
-	QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-	const int score = sw_align_bits<E, STORE>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, c);
-	if (!STORE && score == -1)
-		return false;   // its cells are counted by the rerun
-	cells += c;
-	store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
-	flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
-	return true;
-}
-
 // one thread per job, jobs in (error cap, length) order; threads whose job
 // is not of cap E leave at once (whole warps, the order is by cap).  The
-// DP runs in the bit-plane form (sw_align_bits).  With traceback every row
-// is kept (4 bits a slot, in local memory).  In the score-only mode rows
-// serve only the shrink loop of a DP that stops early (18% of the error-8
-// calls): this pass keeps none and marks those jobs' places in the order
-// (`rerun[t]` = 1); a stable compaction of the order by the marks lists
-// them, still by (cap, length), for k_dp_redo, which runs them again with
-// their rows.
-template <int E, bool STORE>
+// DP runs in the bit-plane form (sw_align_bits).  Every row is kept (4 bits
+// a slot, in local memory), so a DP that stops early runs its shrink loop in
+// place: in the score-only mode 18% of the error-8 calls stop early, nearly
+// every warp holds one, and a rerun would redo the DP (a score-only first
+// pass without rows, the early stops run again with theirs, measured 40%
+// slower on config-2s).
+template <int E>
 __global__ void __launch_bounds__(128, 8)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
-	 int rcap, uint8_t *__restrict__ rerun)
+	 int rcap)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t cells = 0;
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
-		if (!dp_job<E, STORE>(b, jobs, id, res, rcap, cells))
-			rerun[t] = 1;
+		const DpJob jb = jobs[id];
+		typename BitRows<E>::T rows[MAX_DP_ROWS + 1];
+		DCig cig;
+		int flags = 0;
+		cig.n = cig.nm = 0;
+		const bool rev = jb.err < 0;
+		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
+		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
+		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
+		const int score = sw_align_bits<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, cells);
+		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
+		flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
 	}
 	warp_stat(b.stats + ST_SW_CELLS, cells);
-}
-
-// the score-only mode's early-stopped jobs, with their rows (a grid-stride
-// pass over the list compacted from the first pass's marks; its length is
-// read on the device)
-template <int E>
-__global__ void __launch_bounds__(128, 8)
-k_dp_redo(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ redo, const int *__restrict__ nredo,
-	  uint8_t *__restrict__ res, int rcap)
-{
-	const int n = *nredo;
-	for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x) {
-		const int t = t0 + threadIdx.x;
-		uint32_t cells = 0;
-		if (t < n && job_form(jobs[redo[t]]) == E)
-			dp_job<E, true>(b, jobs, redo[t], res, rcap, cells);
-		warp_stat(b.stats + ST_SW_CELLS, cells);
-	}
 }
 
 // the jobs outside the register form (empty gaps, spill cases)

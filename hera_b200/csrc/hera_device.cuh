@@ -637,10 +637,7 @@ struct BitRows<4> {            // W = 10, values <= 6: planes b0..b2 in one word
 	}
 };
 
-// STORE = false: no row is kept, and a DP that stops early returns -1
-// without a result (its shrink loop needs the rows: the caller reruns it
-// with STORE = true); only for the score-only mode.
-template <int E, bool STORE, class Cig>
+template <int E, class Cig>
 __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
 				    bool score_only, Cig &cig, typename BitRows<E>::T *__restrict__ rows, int &flags,
 				    uint32_t &cells)
@@ -658,8 +655,6 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 	};
 	// a thermometer row stored as planes of its binary values
 	auto store = [&](int k, const uint32_t (&G)[NT + 1]) {
-		if (!STORE)
-			return;
 		uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
 #pragma unroll
 		for (int t = 1; t <= NT; ++t) {
@@ -780,8 +775,6 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 			G[t] = V[t];
 		store(k, G);
 		if (min == error) {
-			if (!STORE)
-				return -1;   // early stop: the shrink loop needs the rows
 			++k;
 			break;
 		}
@@ -790,38 +783,34 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 
 	int score = 0;
 	if (min >= error) {
-		if constexpr (!STORE) {
-			return -1;
-		} else {
-			while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
-				--k;
-				// The reference scans row k from column 0 to its break.  Cells
-				// left of the window are zero there and here (no effect: jj
-				// stays 0), and the break marker or ref_len lies inside the
-				// window, so the scan covers the window only.
-				int jj = 0;
-				const int c_lo = k - E > 0 ? k - E : 0;
-				const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
-				for (int c = c_lo; c < c_hi; ++c) {
-					const unsigned v = get(k, c);
-					if (v == error + 1)
-						break;
-					if (v > 0)
-						jj = (int)error;
-					if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
-						min = v;
-						xmin = (unsigned)c;
-					}
+		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+			--k;
+			// The reference scans row k from column 0 to its break.  Cells
+			// left of the window are zero there and here (no effect: jj
+			// stays 0), and the break marker or ref_len lies inside the
+			// window, so the scan covers the window only.
+			int jj = 0;
+			const int c_lo = k - E > 0 ? k - E : 0;
+			const int c_hi = k - E + W < (int)ref_len ? k - E + W : (int)ref_len;
+			for (int c = c_lo; c < c_hi; ++c) {
+				const unsigned v = get(k, c);
+				if (v == error + 1)
+					break;
+				if (v > 0)
+					jj = (int)error;
+				if (v <= min && jj > 0 && c > 0 && r.c(c - 1) == qc(k - 1) && v == get(k - 1, c - 1)) {
+					min = v;
+					xmin = (unsigned)c;
 				}
 			}
-			if (k < 5) {
-				cig_add(cig, OP_S, len, nullptr, flags);
-				return (int)len;
-			}
-			cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
-			score = (int)len - k;
-			i = k;
 		}
+		if (k < 5) {
+			cig_add(cig, OP_S, len, nullptr, flags);
+			return (int)len;
+		}
+		cig_add(cig, OP_S, len - (unsigned)k, nullptr, flags);
+		score = (int)len - k;
+		i = k;
 	} else {
 		if (xmin < len && k == (int)len) {
 			min += len - xmin;
@@ -835,9 +824,6 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}
-	if constexpr (!STORE)
-		return -1;
-	else {
 	while (i > 0 && k > 0) {
 		const unsigned cur = get(i, k);
 		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
@@ -861,7 +847,6 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 	for (int t = 1; t <= k; ++t)
 		cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	return score;
-	}
 }
 
 // Entry used by the per-task (plain) path: the banded form, which keeps the

@@ -786,9 +786,6 @@ struct Lane {
 	DBuf<DpJob> jobs;
 	DBuf<uint8_t> res;
 	DBuf<int> perm, hist, tlist;
-	DBuf<int> redo;                      // score-only DP jobs rerun with their rows
-	DBuf<uint8_t> rerun;                 // ... marked at their places in the DP order
-	bool redo_pass = true;               // the allocation-free lane keeps every row instead
 	DBuf<uint2> thits;                   // a later round's seeds, looked up before its build
 	bool seed_req = true;                // the allocation-free lane's build looks them up itself
 	DBuf<int> tval;                      // round 0's calls before the sort by size
@@ -835,7 +832,7 @@ struct Lane {
 		ovf_list.release(); ovf_slot.release(); wpairs.release(); wwork.release(); wssw_out.release();
 		side_recs.release(); side_pos.release(); side_op.release(); side_p.release(); side_miss.release();
 		slots.release(); jobs.release(); res.release(); perm.release(); hist.release(); tlist.release();
-		tval.release(); tkey.release(); redo.release(); rerun.release(); thits.release();
+		tval.release(); tkey.release(); thits.release();
 		recs.release(); pos_pool.release(); op_pool.release(); p_pool.release(); miss_pool.release();
 		h_seq.release(); h_off.release(); h_len.release(); h_small.release(); h_recs.release();
 		h_pos.release(); h_ops.release(); h_p.release(); h_miss.release();
@@ -1115,7 +1112,6 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	ctx->na = new Lane();
 	ctx->na->no_wide = true;
 	ctx->na->sort_tasks = false;
-	ctx->na->redo_pass = false;
 	ctx->na->seed_req = false;
 	if (cudaStreamCreateWithFlags(&ctx->na->stream, cudaStreamNonBlocking) != cudaSuccess ||
 	    ctx->na->h_small.ensure(32) != cudaSuccess)
@@ -1429,30 +1425,8 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
 		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
 		cudaEventRecord(L.ev[10], st);
-		if (b.score_only && L.redo_pass) {
-			// no rows kept; the jobs that stop early run again with theirs
-			LK(L.redo.ensure(nj), "dp reruns");
-			LK(L.rerun.ensure(nj), "dp reruns");
-			int *d_nredo = L.counters.p + 27;
-			LK(cudaMemsetAsync(L.rerun.p, 0, nj, st), "memset");
-			k_dp_reg<4, false><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap,
-									   L.rerun.p);
-			k_dp_reg<8, false><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap,
-									   L.rerun.p);
-			size_t tmp = 0;
-			cub::DeviceSelect::Flagged(nullptr, tmp, L.perm.p, L.rerun.p, L.redo.p, d_nredo, nj, st);
-			LK(L.cub_tmp.ensure(tmp), "dp rerun scratch");
-			cub::DeviceSelect::Flagged(L.cub_tmp.p, tmp, L.perm.p, L.rerun.p, L.redo.p, d_nredo, nj, st);
-			const unsigned g = std::min<unsigned>(blocks_for(nj), (unsigned)ctx->sms * 8);
-			k_dp_redo<4><<<g, 128, 0, st>>>(b, L.jobs.p, L.redo.p, d_nredo, L.res.p, rcap);
-			k_dp_redo<8><<<g, 128, 0, st>>>(b, L.jobs.p, L.redo.p, d_nredo, L.res.p, rcap);
-			launches += 4;
-		} else {
-			k_dp_reg<4, true><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap,
-									  nullptr);
-			k_dp_reg<8, true><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap,
-									  nullptr);
-		}
+		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
 		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
 		cudaEventRecord(L.ev[11], st);
 		launches += 6;
@@ -3042,12 +3016,7 @@ extern "C" int hera_gpu_unit_sw(int device, const char *refs, const int64_t *ref
 		     o_roff = o_at + al((size_t)n * 8), o_qoff = o_roff + al((size_t)(n + 1) * 8),
 		     o_err = o_qoff + al((size_t)(n + 1) * 8), o_jobs = o_err + al((size_t)n * 4),
 		     o_perm = o_jobs + al((size_t)n * sizeof(DpJob)), o_res = o_perm + al((size_t)n * 4),
-		     o_redo = o_res + al((size_t)n * stride), o_rerun = o_redo + al((size_t)n * 4),
-		     o_cnt = o_rerun + al((size_t)n), o_sel = o_cnt + 256;
-	size_t sel_bytes = 0;
-	cub::DeviceSelect::Flagged(nullptr, sel_bytes, (const int *)nullptr, (const uint8_t *)nullptr, (int *)nullptr,
-				   (int *)nullptr, n);
-	const size_t need = o_sel + al(sel_bytes);
+		     o_cnt = o_res + al((size_t)n * stride), need = o_cnt + 256;
 	uint8_t *d = nullptr;
 	if (cudaMalloc(&d, need) != cudaSuccess)
 		return HERA_GPU_ENOMEM;
@@ -3083,19 +3052,8 @@ extern "C" int hera_gpu_unit_sw(int device, const char *refs, const int64_t *ref
 		b.score_only = write_bam == 1;
 		b.max_len = MAX_READ;
 		uint8_t *res = d + o_res;
-		if (write_bam == 1) {   // as the aligner runs the score-only mode
-			int *redo = reinterpret_cast<int *>(d + o_redo), *nredo = d_cnt + 24;
-			uint8_t *rerun = d + o_rerun;
-			cudaMemset(rerun, 0, (size_t)n);
-			k_dp_reg<4, false><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap, rerun);
-			k_dp_reg<8, false><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap, rerun);
-			cub::DeviceSelect::Flagged(d + o_sel, sel_bytes, perm, rerun, redo, nredo, n);
-			k_dp_redo<4><<<blocks_for(n), 128>>>(b, jobs, redo, nredo, res, rcap);
-			k_dp_redo<8><<<blocks_for(n), 128>>>(b, jobs, redo, nredo, res, rcap);
-		} else {
-			k_dp_reg<4, true><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap, nullptr);
-			k_dp_reg<8, true><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap, nullptr);
-		}
+		k_dp_reg<4><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		k_dp_reg<8><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
 		k_dp_generic<<<blocks_for(n), 128>>>(b, jobs, n, res, rcap);
 		std::vector<uint8_t> h((size_t)n * stride);
 		cudaError_t e = cudaGetLastError();
