@@ -240,38 +240,6 @@ __global__ void __launch_bounds__(256) k_seed_req(Batch b, Round R, uint2 *__res
 	thits[idx] = h;
 }
 
-// A later round's calls listed largest first, as k_task_list lists round
-// 0's: every call's task info reset, its anchor count (capped at 255) as
-// the sort key, and the number with any hit at *nlist.  A read longer than
-// the batch's maximum flags F_READ (the build's own check).
-__global__ void k_task_key(Batch b, Round R, TaskInfo *__restrict__ tinfo, int *__restrict__ list,
-			   int *__restrict__ nlist, uint8_t *__restrict__ key)
-{
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= R.ntask)
-		return;
-	int pi, c, str;
-	task_of(R, t, pi, c, str);
-	tinfo[t].chain0 = 0;
-	tinfo[t].nch = -1;
-	key[t] = 0;
-	list[t] = t;
-	const int ri = 2 * pi + ((c ^ str) == 0 ? 0 : 1);
-	const int L = b.len[ri];
-	if (L > b.max_len) {
-		flag(b.flags, F_READ);
-		return;
-	}
-	const uint2 *h = R.thits + (int64_t)t * R.tspr;
-	uint32_t w = 0;
-	for (int j = 0; j < R.tspr && j * R.space + KMER <= L; ++j)
-		w += h[j].y;
-	if (w == 0)
-		return;
-	key[t] = (uint8_t)(w < 255 ? w : 255);
-	atomicAdd(nlist, 1);
-}
-
 __device__ __forceinline__ void prefetch_l2(const void *p)
 {
 	asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
@@ -676,13 +644,14 @@ __device__ __forceinline__ int job_form(const DpJob &j)
 
 // one thread per job, jobs in (error cap, length) order; threads whose job
 // is not of cap E leave at once (whole warps, the order is by cap).  The
-// DP runs in the bit-plane form (sw_align_bits).  Every row is kept (4 bits
-// a slot, in local memory), so a DP that stops early runs its shrink loop in
-// place: in the score-only mode 18% of the error-8 calls stop early, nearly
-// every warp holds one, and a rerun would redo the DP (a score-only first
-// pass without rows, the early stops run again with theirs, measured 40%
-// slower on config-2s).
-template <int E>
+// DP runs in the bit-plane form (sw_align_bits).  With traceback every row
+// is kept (4 bits a slot, in local memory).  In the score-only mode (SUM)
+// rows serve only the shrink loop of a DP that stops early (18% of the
+// error-8 calls, nearly every warp holds one), so each row keeps the
+// loop's 2-byte summary instead and the loop reads one summary a row.  (A
+// score-only first pass keeping no rows, with the early stops run again,
+// measured 40% slower on config-2s: the reruns redid most of the DP.)
+template <int E, bool SUM>
 __global__ void __launch_bounds__(128, 8)
 k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, int n, uint8_t *__restrict__ res,
 	 int rcap)
@@ -692,7 +661,7 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 	const int id = t < n ? perm[t] : 0;
 	if (t < n && job_form(jobs[id]) == E) {
 		const DpJob jb = jobs[id];
-		typename BitRows<E>::T rows[MAX_DP_ROWS + 1];
+		typename DpRow<E, SUM>::T rows[MAX_DP_ROWS + 1];
 		DCig cig;
 		int flags = 0;
 		cig.n = cig.nm = 0;
@@ -700,7 +669,8 @@ k_dp_reg(Batch b, const DpJob *__restrict__ jobs, const int *__restrict__ perm, 
 		const uint8_t *q = (jb.orient ? b.code_r : b.code) + b.off[jb.read] + jb.qoff;
 		RefWin r{b.ix.code, b.ix.seq, jb.rstart, jb.ref_len, rev};
 		QView qv{rev ? q + (jb.len - 1) : q, rev ? -1 : 1};
-		const int score = sw_align_bits<E>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags, cells);
+		const int score = sw_align_bits<E, SUM>(r, qv, jb.ref_len, jb.len, b.score_only != 0, cig, rows, flags,
+							cells);
 		store_res(cig, score, res + (size_t)id * res_stride(rcap), rcap, flags);
 		flag(b.flags, flags & ~F_CAPS);   // capacity: in the result header, for k_replay
 	}

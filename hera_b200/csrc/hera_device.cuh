@@ -637,9 +637,21 @@ struct BitRows<4> {            // W = 10, values <= 6: planes b0..b2 in one word
 	}
 };
 
-template <int E, class Cig>
+// What the bit-plane DP keeps of each row: the whole row (4 binary planes)
+// for the traceback, or, in the score-only mode (SUM), the 2-byte summary
+// the shrink loop needs (below).
+template <int E, bool SUM>
+struct DpRow {
+	using T = typename BitRows<E>::T;
+};
+template <int E>
+struct DpRow<E, true> {
+	using T = uint16_t;
+};
+
+template <int E, bool SUM, class Cig>
 __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len, uint32_t len,
-				    bool score_only, Cig &cig, typename BitRows<E>::T *__restrict__ rows, int &flags,
+				    bool score_only, Cig &cig, typename DpRow<E, SUM>::T *__restrict__ rows, int &flags,
 				    uint32_t &cells)
 {
 	constexpr int W = 2 * E + 2;
@@ -653,8 +665,10 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 		x = x < 0 ? 0 : (x >= (int)ref_len ? (int)ref_len - 1 : x);
 		return r.c(x);
 	};
-	// a thermometer row stored as planes of its binary values
+	// a thermometer row stored as planes of its binary values (traceback mode)
 	auto store = [&](int k, const uint32_t (&G)[NT + 1]) {
+		if constexpr (SUM)
+			return;
 		uint32_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
 #pragma unroll
 		for (int t = 1; t <= NT; ++t) {
@@ -664,11 +678,16 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 			if (t & 4) b2 |= only;
 			if (t & 8) b3 |= only;
 		}
-		rows[k] = RB::pack(b0, b1, b2, b3);
+		if constexpr (!SUM)
+			rows[k] = RB::pack(b0, b1, b2, b3);
 	};
 	auto get = [&](int k, int c) -> unsigned {
-		const int q = c - k + E;
-		return (q >= 0 && q < W) ? RB::at(rows[k], q) : 0u;
+		if constexpr (SUM) {
+			return 0u;   // not used: the score-only mode keeps summaries
+		} else {
+			const int q = c - k + E;
+			return (q >= 0 && q < W) ? RB::at(rows[k], q) : 0u;
+		}
 	};
 	// reference codes of row k's slots (x = k + q - error - 1) as three
 	// planes; row 1 first
@@ -770,6 +789,41 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 					V[t] = t <= E + 1 ? (V[t] | JM) : (V[t] & ~JM);
 			}
 		}
+		if constexpr (SUM) {
+			// The shrink loop's scan of row k (below), as one summary: the
+			// scan runs over the window's columns up to the first cell ==
+			// error + 1; a cell is a candidate from the first cell > 0 on,
+			// at a column > 0, where the diagonal codes match and the cell
+			// equals its up-left neighbour (same slot of row k - 1, still in
+			// G).  Scanning in column order with `v <= min`, the scan ends
+			// with min = the smallest candidate value m (when m <= min) and
+			// xmin = the last candidate column holding m: the summary keeps
+			// m and that slot.
+			const int qlo = E - k > 0 ? E - k : 0;
+			const int qhi = (int)ref_len - k + E < W ? (int)ref_len - k + E : W;
+			const uint32_t SR = qhi > qlo ? ((1u << qhi) - 1u) & ~((1u << qlo) - 1u) : 0u;
+			const uint32_t E1 = V[E + 1] & ~V[E + 2] & SR;
+			const uint32_t SCAN = SR & (E1 ? (E1 & (0u - E1)) - 1u : 0xffffffffu);
+			const uint32_t NZ = V[1] & SCAN;
+			const uint32_t ALW = NZ ? ~((NZ & (0u - NZ)) - 1u) : 0u;
+			const int q0 = E - k + 1;                 // column > 0
+			const uint32_t C0 = q0 <= 0 ? 0xffffffffu : ~((1u << q0) - 1u);
+			uint32_t DIFF = 0;
+#pragma unroll
+			for (int t = 1; t <= NT; ++t)
+				DIFF |= V[t] ^ G[t];
+			const uint32_t CAND = SCAN & ALW & C0 & ~MM & ~DIFF;
+			uint32_t X = 0, m = 0;
+#pragma unroll
+			for (int t = E + 1; t >= 1; --t) {
+				const uint32_t Y = CAND & ~V[t];   // candidates < t
+				if (Y) {
+					X = Y;
+					m = (uint32_t)(t - 1);
+				}
+			}
+			rows[k] = X ? (uint16_t)(0x8000u | (m << 8) | (uint32_t)(31 - __clz(X))) : (uint16_t)0;
+		}
 #pragma unroll
 		for (int t = 1; t <= NT; ++t)
 			G[t] = V[t];
@@ -783,7 +837,17 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 
 	int score = 0;
 	if (min >= error) {
-		while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+		if constexpr (SUM) {
+			while (k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
+				--k;
+				const uint32_t sm = rows[k];   // the row's scan, summarised as it was computed
+				if ((sm & 0x8000u) && ((sm >> 8) & 15u) <= min) {
+					min = (sm >> 8) & 15u;
+					xmin = (unsigned)(k + (int)(sm & 31u) - E);
+				}
+			}
+		}
+		while (!SUM && k >= 5 && (min > (unsigned)(k / 10) || min * 2 > (unsigned)(k - ferr))) {
 			--k;
 			// The reference scans row k from column 0 to its break.  Cells
 			// left of the window are zero there and here (no effect: jj
@@ -820,7 +884,7 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 	}
 	k = (int)xmin;
 	score += (int)min;
-	if (score_only) {
+	if (SUM || score_only) {
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}

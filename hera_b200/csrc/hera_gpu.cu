@@ -138,11 +138,35 @@ __device__ __forceinline__ int load_read(const BatchT<K> &b, int ri, int orient,
 	return L;
 }
 
+// code_of of four bytes at once: A/a 0, C/c 1, G/g 2, T/t 3, anything else 4
+__device__ __forceinline__ uint32_t codes4(uint32_t v)
+{
+	const uint32_t x = v | 0x20202020u;
+	const uint32_t a = __vcmpeq4(x, 0x61616161u), c = __vcmpeq4(x, 0x63636363u),
+		       g = __vcmpeq4(x, 0x67676767u), t = __vcmpeq4(x, 0x74747474u);
+	return (0x04040404u & ~(a | c | g | t)) | (c & 0x01010101u) | (g & 0x02020202u) | (t & 0x03030303u);
+}
+
+// ASCII -> codes, four bytes a thread: one aligned 4-byte store of `code`
+// (whose base is 4-byte aligned) from the two aligned input words around
+// the four bytes (`ascii` may start anywhere); a group whose second input
+// word would reach past byte n - 1 is read byte by byte.
 __global__ void k_codes(const uint8_t *__restrict__ ascii, uint8_t *__restrict__ code, int64_t n)
 {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-	     i += (int64_t)gridDim.x * blockDim.x)
-		code[i] = code_of(ascii[i]);
+	const int s = (int)(reinterpret_cast<uintptr_t>(ascii) & 3);
+	const uint32_t *w = reinterpret_cast<const uint32_t *>(ascii - s);
+	const int64_t nw = (n + 3) >> 2;
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nw;
+	     i += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t b0 = 4 * i;
+		if (b0 + 7 - s < n) {
+			const uint32_t v = s ? __funnelshift_r(__ldg(w + i), __ldg(w + i + 1), 8 * s) : __ldg(w + i);
+			reinterpret_cast<uint32_t *>(code)[i] = codes4(v);
+		} else {
+			for (int64_t k = b0; k < b0 + 4 && k < n; ++k)
+				code[k] = code_of(ascii[k]);
+		}
+	}
 }
 
 // reverse-complement codes of every read, at the read's own offset (one
@@ -1319,27 +1343,14 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		R.list = L.tlist.p;
 		R.nlist = d_nl;
 	} else if (L.seed_req) {
-		// a later round: its seeds looked up side by side first, then its
-		// calls sorted largest first as round 0's are
+		// a later round: its seeds looked up side by side first (its calls
+		// stay in request order: sorted by anchor count, as round 0's are,
+		// the build of these rounds measured 70% slower)
 		R.tspr = b.max_len >= KMER ? (b.max_len - KMER) / R.space + 1 : 1;
 		LK(L.thits.ensure((size_t)R.ntask * R.tspr), "round seeds");
 		k_seed_req<<<blocks_for((int64_t)R.ntask * R.tspr, 256), 256, 0, st>>>(b, R, L.thits.p);
+		++launches;
 		R.thits = L.thits.p;
-		LK(L.tlist.ensure(R.ntask), "task list");
-		LK(L.tval.ensure(R.ntask), "task list");
-		LK(L.tkey.ensure(2 * (size_t)R.ntask), "task keys");
-		int *d_nl = L.counters.p + 15;
-		LK(cudaMemsetAsync(d_nl, 0, sizeof(int), st), "memset");
-		k_task_key<<<blocks_for(R.ntask, 256), 256, 0, st>>>(b, R, L.tinfo.p, L.tval.p, d_nl, L.tkey.p);
-		size_t tmp = 0;
-		cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p, L.tlist.p,
-							  R.ntask, 0, 8, st);
-		LK(L.cub_tmp.ensure(tmp), "sort scratch");
-		cub::DeviceRadixSort::SortPairsDescending(L.cub_tmp.p, tmp, L.tkey.p, L.tkey.p + R.ntask, L.tval.p,
-							  L.tlist.p, R.ntask, 0, 8, st);
-		launches += 3;
-		R.list = L.tlist.p;
-		R.nlist = d_nl;
 	}
 	for (int attempt = 0; attempt < 2; ++attempt) {
 		LK(L.chains.ensure(L.chain_cap), "chains");
@@ -1425,8 +1436,13 @@ static int gp_round(hera_gpu_ctx *ctx, Lane &L, const Batch &b, Round R, uint32_
 		k_bin_scan<<<1, 256, 0, st>>>(L.hist.p, NBIN);
 		k_bin_scatter<<<blocks_for(nj, 1024), 1024, 0, st>>>(L.jobs.p, nj, L.hist.p, L.perm.p);
 		cudaEventRecord(L.ev[10], st);
-		k_dp_reg<4><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
-		k_dp_reg<8><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		if (b.score_only) {
+			k_dp_reg<4, true><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+			k_dp_reg<8, true><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		} else {
+			k_dp_reg<4, false><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+			k_dp_reg<8, false><<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, L.perm.p, nj, L.res.p, rcap);
+		}
 		k_dp_generic<<<blocks_for(nj), 128, 0, st>>>(b, L.jobs.p, nj, L.res.p, rcap);
 		cudaEventRecord(L.ev[11], st);
 		launches += 6;
@@ -3052,8 +3068,13 @@ extern "C" int hera_gpu_unit_sw(int device, const char *refs, const int64_t *ref
 		b.score_only = write_bam == 1;
 		b.max_len = MAX_READ;
 		uint8_t *res = d + o_res;
-		k_dp_reg<4><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
-		k_dp_reg<8><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		if (write_bam == 1) {   // the score-only mode, as the aligner runs it
+			k_dp_reg<4, true><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+			k_dp_reg<8, true><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		} else {
+			k_dp_reg<4, false><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+			k_dp_reg<8, false><<<blocks_for(n), 128>>>(b, jobs, perm, n, res, rcap);
+		}
 		k_dp_generic<<<blocks_for(n), 128>>>(b, jobs, n, res, rcap);
 		std::vector<uint8_t> h((size_t)n * stride);
 		cudaError_t e = cudaGetLastError();
