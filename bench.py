@@ -78,6 +78,9 @@ def parse():
                     help="pairs of the last timed step checked against the oracle")
     ap.add_argument("--no-config-legs", action="store_true", help="skip the config-3 and config-4 legs")
     ap.add_argument("--no-bam", action="store_true", help="skip the BAM-record leg")
+    ap.add_argument("--no-hera-quant", action="store_true",
+                    help="skip the leg that times hera quant against hera quant with the library inside")
+    ap.add_argument("--quant-pairs", type=int, default=2_000_000, help="read pairs of the hera quant leg")
     ap.add_argument("--leg-pairs", type=int, default=500_000, help="pairs per step of the config-3/4 legs")
     ap.add_argument("--leg-steps", type=int, default=5, help="timed steps of the config-3/4 legs")
     return ap.parse_args()
@@ -470,7 +473,8 @@ def main():
     legs = {}
     if solo:
         for name, fn in (("bam", lambda: None if args.no_bam else bam_bench(args, ix, ann, chunks[0], local)),
-                         ("fastq", lambda: None if args.no_fastq else fastq_bench(args, ix, chunks[0], local))):
+                         ("fastq", lambda: None if args.no_fastq else fastq_bench(args, ix, chunks[0], local)),
+                         ("hera_quant", lambda: None if args.no_hera_quant else hera_quant_bench(args, local))):
             try:
                 legs[name] = fn()
             except Exception as e:
@@ -705,6 +709,70 @@ def classes_leg(kctx, pairs: int, length) -> dict:
                     "frac_of_hbm": None if gbs is None else gbs / peak[0]}
     out.update({"classes": t.n_classes, "paired": t.paired, "single_transcript_reads": int(t.tx_count.sum()),
                 "algorithmic_bytes": algo, "hbm_peak": peak[1]})
+    return out
+
+
+def _write_fastq_fast(reads, path: str, mate: int) -> None:
+    """FASTQ of a read set ('?' qualities, names read<i>/<mate>), built as
+    one buffer: hera's parser sees the same text synth.write_fastq writes."""
+    n = reads.n
+    parts = []
+    step = 200_000
+    for lo in range(0, n, step):
+        hi = min(n, lo + step)
+        buf = []
+        for i in range(lo, hi):
+            s = reads.seq[reads.off[i]:reads.off[i] + reads.len[i]].tobytes()
+            buf.append(b"@read%d/%d\n%s\n+\n%s\n" % (i, mate, s, b"?" * len(s)))
+        parts.append(b"".join(buf))
+    with open(path, "wb") as f:
+        for b in parts:
+            f.write(b)
+
+
+def hera_quant_bench(args, local):
+    """hera's own program end to end, twice on the same index directory and
+    FASTQ files: the unmodified reference (oracle/_ref/hera) and the same
+    program with the library in its paired-end worker loop
+    (oracle/_ref/hera_gpu: hera_gpu_align_pairs per chunk, hera's own
+    align_pair_read tail, add_class, EM and output), both with -t = all
+    host cores.  Wall time of each process: index load, FASTQ parsing,
+    alignment, EM and output files included."""
+    import oracle
+    from hera_b200 import index, workloads
+    hera, hera_gpu = oracle.REFERENCE_BIN, os.path.join(oracle.REF_DIR, "hera_gpu")
+    if not (os.path.exists(hera) and os.path.exists(hera_gpu)):
+        return {"unavailable": "oracle/_ref/hera or hera_gpu not built (make -C oracle ref dropin)"}
+    import tempfile
+    cores = os.cpu_count() or 1
+    wl = "config2s"
+    ann, tx, ix = workloads.build(wl)
+    n = args.quant_pairs
+    r1, r2 = workloads.pairs("config2", ann, tx, n, seed=71)
+    with tempfile.TemporaryDirectory(dir=os.environ.get("TMPDIR")) as d:
+        index.write_index_dir(ann, ix, os.path.join(d, "idx"))
+        a, b = os.path.join(d, "r_1.fq"), os.path.join(d, "r_2.fq")
+        _write_fastq_fast(r1, a, 1)
+        _write_fastq_fast(r2, b, 2)
+        out = {}
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+        for name, binary in (("hera", hera), ("hera_gpu", hera_gpu)):
+            o = os.path.join(d, name)
+            t = time.perf_counter()
+            p = subprocess.run([binary, "quant", "-i", os.path.join(d, "idx"), "-1", a, "-2", b, "-o", o,
+                                "-t", str(cores)], capture_output=True, text=True, timeout=1200, env=env)
+            wall = time.perf_counter() - t
+            if p.returncode != 0:
+                return {"error": f"{name} exited {p.returncode}: {p.stderr[-300:]}"}
+            out[name] = {"wall_s": round(wall, 3), "pairs_per_s": n / wall}
+        same = {f: open(os.path.join(d, "hera", f), "rb").read() == open(os.path.join(d, "hera_gpu", f), "rb").read()
+                for f in ("abundance.tsv", "abundance.gene.tsv")}
+    out.update({"workload": f"{wl} index, {n} config-2-model pairs (2x100 bp)", "threads": cores,
+                "speedup": out["hera"]["wall_s"] / out["hera_gpu"]["wall_s"],
+                "files_identical": same,
+                "note": "whole program wall time; with -t > 1 hera's own add_class order follows thread "
+                        "timing, so the files may differ in the last bits (-t 1 identity: "
+                        "tests/test_hera_dropin.py)"})
     return out
 
 
