@@ -1031,6 +1031,7 @@ def serve_bench(args, ann, tx, ix, orc, local):
                 tickets.append((s, tk))
         done.set()
 
+    add_ms = []
     th = threading.Thread(target=feed)
     t0 = time.perf_counter()
     th.start()
@@ -1046,7 +1047,9 @@ def serve_bench(args, ann, tx, ix, orc, local):
                 continue
             s, tk = item
             res, info = srv.wait(tk, out=keep)
+            ta = time.perf_counter()
             tables[s].add_result(res)
+            add_ms.append((time.perf_counter() - ta) * 1e3)
             infos.append(info)
             k += 1
         th.join()
@@ -1064,6 +1067,16 @@ def serve_bench(args, ann, tx, ix, orc, local):
                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                "p50_wait_ms": float(np.percentile(wt, 50)), "p99_wait_ms": float(np.percentile(wt, 99)),
                "slots": st["slots"], "batches": st["batches"], "batch_pairs": CH}
+        # where the tail comes from: the slowest chunks (arrival order, time
+        # since the first submit) and the waiter's class-table inserts
+        first = min(i["submit_ms"] for i in infos)
+        slow = np.argsort(lat)[::-1][:5]
+        out["slowest"] = [{"chunk": int(c), "submit_s": round((infos[c]["submit_ms"] - first) / 1e3, 3),
+                           "latency_ms": round(float(lat[c]), 1), "admit_wait_ms": round(float(wt[c]), 1)}
+                          for c in slow]
+        out["class_insert_ms"] = {"p50": round(float(np.percentile(add_ms, 50)), 3),
+                                  "max": round(float(np.max(add_ms)), 1),
+                                  "max_at_chunk": int(np.argmax(add_ms))}
         # per-sample EM: the device EM over the served table against the
         # oracle's EM over the oracle's table of the same chunks (a served
         # chunk's records are those of the chunk aligned alone)

@@ -888,28 +888,30 @@ __device__ inline int sw_align_bits(const RefWin &r, QView qc, uint32_t ref_len,
 		cig_add(cig, OP_M, (unsigned)k, nullptr, flags);
 		return score;
 	}
-	while (i > 0 && k > 0) {
-		const unsigned cur = get(i, k);
-		const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
-		if (cur == get(i - 1, k - 1) + pen) {
-			if (pen == 0)
-				cig_add(cig, OP_M, 1, nullptr, flags);
-			else
-				cig_add(cig, OP_X, 1, r.a(k - 1), flags);
-			--i;
-			--k;
-		} else if (cur == get(i - 1, k) + 1) {
-			cig_add(cig, OP_I, 1, nullptr, flags);
-			--i;
-		} else {
-			cig_add(cig, OP_D, 1, r.a(k - 1), flags);
-			--k;
+	if constexpr (!SUM) {   // the traceback over the kept rows
+		while (i > 0 && k > 0) {
+			const unsigned cur = get(i, k);
+			const unsigned pen = r.c(k - 1) == qc(i - 1) ? 0u : 1u;
+			if (cur == get(i - 1, k - 1) + pen) {
+				if (pen == 0)
+					cig_add(cig, OP_M, 1, nullptr, flags);
+				else
+					cig_add(cig, OP_X, 1, r.a(k - 1), flags);
+				--i;
+				--k;
+			} else if (cur == get(i - 1, k) + 1) {
+				cig_add(cig, OP_I, 1, nullptr, flags);
+				--i;
+			} else {
+				cig_add(cig, OP_D, 1, r.a(k - 1), flags);
+				--k;
+			}
 		}
+		if (i > 0)
+			cig_add(cig, OP_I, (unsigned)i, nullptr, flags);
+		for (int t = 1; t <= k; ++t)
+			cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	}
-	if (i > 0)
-		cig_add(cig, OP_I, (unsigned)i, nullptr, flags);
-	for (int t = 1; t <= k; ++t)
-		cig_add(cig, OP_D, 1, r.a(k - t), flags);
 	return score;
 }
 
