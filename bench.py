@@ -731,13 +731,14 @@ def _write_fastq_fast(reads, path: str, mate: int) -> None:
 
 
 def hera_quant_bench(args, local):
-    """hera's own program end to end, twice on the same index directory and
-    FASTQ files: the unmodified reference (oracle/_ref/hera) and the same
-    program with the library in its paired-end worker loop
-    (oracle/_ref/hera_gpu: hera_gpu_align_pairs per chunk, hera's own
-    align_pair_read tail, add_class, EM and output), both with -t = all
-    host cores.  Wall time of each process: index load, FASTQ parsing,
-    alignment, EM and output files included."""
+    """hera's own program end to end on the same index directory and FASTQ
+    files: the unmodified reference (oracle/_ref/hera) and the same program
+    with the library in its paired-end worker loop (oracle/_ref/hera_gpu:
+    hera_gpu_align_pairs per chunk, hera's own align_pair_read tail,
+    add_class, EM and output), both with -t = all host cores.  Each runs on
+    N/4 and on N pairs: the whole-program wall time of each run, and from
+    their difference the per-pair rate with the fixed costs (index load,
+    the library's context and index upload, EM, output) taken out."""
     import oracle
     from hera_b200 import index, workloads
     hera, hera_gpu = oracle.REFERENCE_BIN, os.path.join(oracle.REF_DIR, "hera_gpu")
@@ -748,31 +749,43 @@ def hera_quant_bench(args, local):
     wl = "config2s"
     ann, tx, ix = workloads.build(wl)
     n = args.quant_pairs
+    n_small = n // 4
     r1, r2 = workloads.pairs("config2", ann, tx, n, seed=71)
     with tempfile.TemporaryDirectory(dir=os.environ.get("TMPDIR")) as d:
         index.write_index_dir(ann, ix, os.path.join(d, "idx"))
-        a, b = os.path.join(d, "r_1.fq"), os.path.join(d, "r_2.fq")
-        _write_fastq_fast(r1, a, 1)
-        _write_fastq_fast(r2, b, 2)
+        fq = {}
+        for tag, k in (("small", n_small), ("full", n)):
+            idx = np.arange(k)
+            a, b = os.path.join(d, f"{tag}_1.fq"), os.path.join(d, f"{tag}_2.fq")
+            _write_fastq_fast(r1.subset(idx) if k < n else r1, a, 1)
+            _write_fastq_fast(r2.subset(idx) if k < n else r2, b, 2)
+            fq[tag] = (a, b)
         out = {}
         env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
         for name, binary in (("hera", hera), ("hera_gpu", hera_gpu)):
-            o = os.path.join(d, name)
-            t = time.perf_counter()
-            p = subprocess.run([binary, "quant", "-i", os.path.join(d, "idx"), "-1", a, "-2", b, "-o", o,
-                                "-t", str(cores)], capture_output=True, text=True, timeout=1200, env=env)
-            wall = time.perf_counter() - t
-            if p.returncode != 0:
-                return {"error": f"{name} exited {p.returncode}: {p.stderr[-300:]}"}
-            out[name] = {"wall_s": round(wall, 3), "pairs_per_s": n / wall}
-        same = {f: open(os.path.join(d, "hera", f), "rb").read() == open(os.path.join(d, "hera_gpu", f), "rb").read()
+            walls = {}
+            for tag in ("small", "full"):
+                a, b = fq[tag]
+                o = os.path.join(d, f"{name}_{tag}")
+                t = time.perf_counter()
+                p = subprocess.run([binary, "quant", "-i", os.path.join(d, "idx"), "-1", a, "-2", b, "-o", o,
+                                    "-t", str(cores)], capture_output=True, text=True, timeout=1200, env=env)
+                walls[tag] = time.perf_counter() - t
+                if p.returncode != 0:
+                    return {"error": f"{name} exited {p.returncode}: {p.stderr[-300:]}"}
+            rate = (n - n_small) / max(1e-9, walls["full"] - walls["small"])
+            out[name] = {"wall_s": round(walls["full"], 3), "wall_s_quarter": round(walls["small"], 3),
+                         "pairs_per_s": n / walls["full"], "pairs_per_s_incremental": rate,
+                         "fixed_s": round(walls["small"] - n_small / rate, 3)}
+        same = {f: open(os.path.join(d, "hera_full", f), "rb").read()
+                == open(os.path.join(d, "hera_gpu_full", f), "rb").read()
                 for f in ("abundance.tsv", "abundance.gene.tsv")}
-    out.update({"workload": f"{wl} index, {n} config-2-model pairs (2x100 bp)", "threads": cores,
-                "speedup": out["hera"]["wall_s"] / out["hera_gpu"]["wall_s"],
+    out.update({"workload": f"{wl} index, {n_small} and {n} config-2-model pairs (2x100 bp)", "threads": cores,
+                "speedup_wall": out["hera"]["wall_s"] / out["hera_gpu"]["wall_s"],
+                "speedup_per_pair": out["hera_gpu"]["pairs_per_s_incremental"] / out["hera"]["pairs_per_s_incremental"],
                 "files_identical": same,
-                "note": "whole program wall time; with -t > 1 hera's own add_class order follows thread "
-                        "timing, so the files may differ in the last bits (-t 1 identity: "
-                        "tests/test_hera_dropin.py)"})
+                "note": "with -t > 1 hera's own add_class order follows thread timing, so the files can "
+                        "differ in the last bits (-t 1 identity: tests/test_hera_dropin.py)"})
     return out
 
 

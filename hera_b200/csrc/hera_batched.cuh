@@ -275,7 +275,9 @@ __device__ inline void enum_chains(const PAnchors &A, int na, const DSlot &Mt, i
 			return false;
 		return true;
 	};
-	bool passA = Mt.n > 0 && space < KMER && space > 0;
+	// (the spacing first: at spacing 31 pass A never runs, and the mate's
+	// slot, a random read of the pair state, is not touched)
+	bool passA = space < KMER && space > 0 && Mt.n > 0;
 	if (passA) {
 		const uint32_t mn = (uint32_t)Mt.n;
 		uint32_t k = 0;
@@ -738,7 +740,7 @@ __global__ void __launch_bounds__(128) k_replay(Batch b, Round R)
 	for (int pass = 0; pass < 3 && ti.nch > 0; ++pass) {
 		bool runs;
 		if (pass == 0)
-			runs = P.s[c][1 - str].n > 0 && R.space < KMER && R.space > 0;
+			runs = R.space < KMER && R.space > 0 && P.s[c][1 - str].n > 0;
 		else if (pass == 1)
 			runs = n1 == 0;
 		else

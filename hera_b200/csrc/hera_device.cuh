@@ -1004,14 +1004,34 @@ __device__ __forceinline__ bool bytes_equal(const uint8_t *s, uint32_t a, uint32
 {
 	if (a == b)
 		return true;
-	for (uint32_t x = 0; x < n; x += 8) {
-		uint64_t u = load8(s + a + x), v = load8(s + b + x);
-		if (n - x < 8) {
-			const uint64_t m = (1ull << (8 * (n - x))) - 1;
-			u &= m;
-			v &= m;
+	// 32 bytes a step: the five aligned words around each string's piece
+	// are loaded together (one load latency a step, not one per 8 bytes),
+	// then shifted into place; the buffers carry 64 bytes of padding past
+	// their data, so the last step's extra words are readable
+	const unsigned long long *wa = reinterpret_cast<const unsigned long long *>((uintptr_t)(s + a) & ~(uintptr_t)7);
+	const unsigned long long *wb = reinterpret_cast<const unsigned long long *>((uintptr_t)(s + b) & ~(uintptr_t)7);
+	const int sa = (int)((a & 7) * 8), sb = (int)((b & 7) * 8);
+	for (uint32_t x = 0; x < n; x += 32) {
+		uint64_t A[5], B[5];
+#pragma unroll
+		for (int k = 0; k < 5; ++k) {
+			A[k] = __ldg(wa + x / 8 + k);
+			B[k] = __ldg(wb + x / 8 + k);
 		}
-		if (u != v)
+		bool same = true;
+#pragma unroll
+		for (int k = 0; k < 4; ++k) {
+			uint64_t u = sa ? (A[k] >> sa) | (A[k + 1] << (64 - sa)) : A[k];
+			uint64_t v = sb ? (B[k] >> sb) | (B[k + 1] << (64 - sb)) : B[k];
+			const uint32_t at = x + 8 * k;
+			if (at < n && n - at < 8) {
+				const uint64_t m = (1ull << (8 * (n - at))) - 1;
+				u &= m;
+				v &= m;
+			}
+			same = same && (at >= n || u == v);
+		}
+		if (!same)
 			return false;
 	}
 	return true;
@@ -1239,7 +1259,7 @@ __device__ inline void get_position(const DevIndex &ix, const uint8_t *rd, int r
 		goto miss;
 
 	// pass A, mate-guided (:1367-1390)
-	if (Mt.n > 0 && space < KMER && space > 0) {
+	if (space < KMER && space > 0 && Mt.n > 0) {
 		const uint32_t mn = (uint32_t)Mt.n;
 		uint32_t k = 0;
 		max = (uint32_t)(rlen / 2);
