@@ -777,6 +777,8 @@ def hera_quant_bench(args, local):
             out[name] = {"wall_s": round(walls["full"], 3), "wall_s_quarter": round(walls["small"], 3),
                          "pairs_per_s": n / walls["full"], "pairs_per_s_incremental": rate,
                          "fixed_s": round(walls["small"] - n_small / rate, 3)}
+            if name == "hera_gpu":   # the worker's own account of its threads' time (full run)
+                out[name]["worker"] = [ln for ln in p.stderr.splitlines() if ln.startswith("hera_gpu:")]
         same = {f: open(os.path.join(d, "hera_full", f), "rb").read()
                 == open(os.path.join(d, "hera_gpu_full", f), "rb").read()
                 for f in ("abundance.tsv", "abundance.gene.tsv")}

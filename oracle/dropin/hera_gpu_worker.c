@@ -27,6 +27,7 @@
  * with -t 1 for the reference's add_class order.
  */
 #include <pthread.h>
+#include <time.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -44,12 +45,21 @@ static pthread_mutex_t CNT_LOCK = PTHREAD_MUTEX_INITIALIZER;
 static __thread Candidate **CUR;      /* the current pair's r[0], r[1] */
 static __thread int CUR_TAKEN;
 static unsigned long long GPU_PAIRS, GPU_CALLS;
-static double GPU_MS;
+static double GPU_MS, CALL_MS, WAIT_MS, TAIL_MS, PARSE_MS;
+
+static double now_ms(void)
+{
+	struct timespec ts;
+	clock_gettime(CLOCK_MONOTONIC, &ts);
+	return ts.tv_sec * 1e3 + ts.tv_nsec / 1e6;
+}
 
 static void report(void)
 {
 	fprintf(stderr, "hera_gpu: %llu pairs aligned on the device in %llu calls, %.1f ms in the calls\n",
 		GPU_PAIRS, GPU_CALLS, GPU_MS);
+	fprintf(stderr, "hera_gpu: worker threads' time: parsing %.1f ms, waiting for the device %.1f ms, "
+		"in hera_gpu_align_pairs %.1f ms, hera's tail %.1f ms\n", PARSE_MS, WAIT_MS, CALL_MS, TAIL_MS);
 }
 
 static void make_context(void)
@@ -121,6 +131,7 @@ void *align_pool_pair(void *thr_data)
 			break;
 		}
 		/* every read pair of the chunk, with the loop's stop rules */
+		double t0 = now_ms();
 		int32_t left_pos = 0, right_pos = 0, n = 0, len_read = 0;
 		while (1) {
 			if (n == cap) {
@@ -154,9 +165,15 @@ void *align_pool_pair(void *thr_data)
 		}
 		/* one device call for the chunk */
 		Candidate **cand = malloc(2 * (size_t)n * sizeof *cand);
+		double t1 = now_ms();
 		pthread_mutex_lock(&GPU_LOCK);
+		double t2 = now_ms();
 		int st = hera_gpu_align_pairs(CTX, (hera_read_inf *)L, (hera_read_inf *)R, n, (int)WRITE_BAM,
 					      (hera_candidate **)cand);
+		double t3 = now_ms();
+		PARSE_MS += t1 - t0;
+		WAIT_MS += t2 - t1;
+		CALL_MS += t3 - t2;
 		hera_gpu_timing tm;
 		if (hera_gpu_get_timing(CTX, &tm) == HERA_GPU_OK)
 			GPU_MS += tm.total_ms;
@@ -179,6 +196,7 @@ void *align_pool_pair(void *thr_data)
 		}
 		free(cand);
 		pthread_mutex_lock(&CNT_LOCK);
+		TAIL_MS += now_ms() - t3;
 		N_READ += n;
 		MEAN_LEN += len_read;
 		_verbose("\rNumber of processed read pairs: %u", N_READ);
