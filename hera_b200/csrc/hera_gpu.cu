@@ -12,6 +12,7 @@
 //                rescue alternate until no pair is waiting
 //   k_count/k_emit  compact the Candidate records into flat pools
 #include "hera_device.cuh"
+#include "hera_combine.h"
 #include "../../include/hera_gpu.h"
 
 #include <cuda_runtime.h>
@@ -936,6 +937,9 @@ struct hera_gpu_ctx {
 	AsyncCall async[2];
 	std::vector<Lane *> lanes2;
 	uint64_t next_async = 1;
+	// drop-in calls made at the same time by several host threads run as
+	// one device batch (up to 2^20 pairs)
+	hcomb::Combiner dropin{1 << 20};
 };
 
 struct FqState;
@@ -2886,38 +2890,63 @@ static void par_for(int64_t n, F f)
 		x.join();
 }
 
-static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, int32_t n, int write_bam,
-			hera_candidate **out)
+// one drop-in call's arguments, queued for a combined batch
+struct DropinArgs {
+	hera_read_inf *a, *b;
+	int32_t n;
+	int write_bam;
+	hera_candidate **out;
+};
+
+// A batch of drop-in calls of one kind (pairs or single reads, one
+// WRITE_BAM) as one flat call: the calls' reads gathered back to back, the
+// records of call k at its pairs' place, each call's Candidates made from
+// its own records (host threads over all of the batch's items).
+static void dropin_batch(hera_gpu_ctx *ctx, std::vector<hcomb::Request *> &batch)
 {
-	if (!ctx || !a || !out || n < 0)
-		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
-	const int per = b ? 2 : 1;
+	const DropinArgs &first = *static_cast<DropinArgs *>(batch[0]->user);
+	const bool paired = first.b != nullptr;
+	const int per = paired ? 2 : 1;
+	const int write_bam = first.write_bam;
+	const size_t nk = batch.size();
+	std::vector<int64_t> pair0(nk + 1, 0);   // first pair of call k in the batch
+	for (size_t k = 0; k < nk; ++k)
+		pair0[k + 1] = pair0[k] + static_cast<DropinArgs *>(batch[k]->user)->n;
+	const int64_t n = pair0[nk];
+	auto finish = [&](int rc) {
+		for (hcomb::Request *r : batch)
+			r->rc = rc;
+	};
 	std::vector<int64_t> off[2];
 	std::vector<int32_t> len[2];
 	int64_t total = 0;
 	for (int m = 0; m < per; ++m) {
-		hera_read_inf *r = m ? b : a;
 		off[m].resize(n);
 		len[m].resize(n);
-		for (int32_t i = 0; i < n; ++i) {
-			if (!r[i].seq || r[i].len < 0)
-				return fail(ctx, HERA_GPU_EINVAL, "read without sequence");
-			off[m][i] = total;
-			len[m][i] = r[i].len;
-			total += r[i].len;
+		for (size_t k = 0; k < nk; ++k) {
+			const DropinArgs &c = *static_cast<DropinArgs *>(batch[k]->user);
+			const hera_read_inf *r = m ? c.b : c.a;
+			for (int32_t i = 0; i < c.n; ++i) {
+				off[m][pair0[k] + i] = total;
+				len[m][pair0[k] + i] = r[i].len;
+				total += r[i].len;
+			}
 		}
 	}
 	// the reads gathered back to back (host threads), then one flat call
 	std::unique_ptr<char[]> seq(new char[(size_t)total + 1]);
-	for (int m = 0; m < per; ++m) {
-		hera_read_inf *r = m ? b : a;
-		par_for(n, [&](int64_t lo, int64_t hi) {
-			for (int64_t i = lo; i < hi; ++i)
-				memcpy(seq.get() + off[m][i], r[i].seq, (size_t)r[i].len);
-		});
-	}
+	for (int m = 0; m < per; ++m)
+		for (size_t k = 0; k < nk; ++k) {
+			const DropinArgs &c = *static_cast<DropinArgs *>(batch[k]->user);
+			const hera_read_inf *r = m ? c.b : c.a;
+			const int64_t p0 = pair0[k];
+			par_for(c.n, [&](int64_t lo, int64_t hi) {
+				for (int64_t i = lo; i < hi; ++i)
+					memcpy(seq.get() + off[m][p0 + i], r[i].seq, (size_t)r[i].len);
+			});
+		}
 	hera_gpu_reads ra{seq.get(), off[0].data(), len[0].data()};
-	hera_gpu_reads rb{seq.get(), b ? off[1].data() : nullptr, b ? len[1].data() : nullptr};
+	hera_gpu_reads rb{seq.get(), paired ? off[1].data() : nullptr, paired ? len[1].data() : nullptr};
 	const uint64_t items = (uint64_t)n * per;
 	std::unique_ptr<hera_cand_rec[]> recs(new hera_cand_rec[items ? items : 1]);
 	hera_gpu_result res{};
@@ -2938,38 +2967,72 @@ static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, i
 		res.list_cap = cl;
 		res.op_cap = co;
 		res.miss_cap = cm;
-		int rc = align_flat(ctx, &ra, b ? &rb : nullptr, n, write_bam, &res);
+		int rc = align_flat(ctx, &ra, paired ? &rb : nullptr, (int32_t)n, write_bam, &res);
 		if (rc == HERA_GPU_OK)
 			break;
 		if (rc != HERA_GPU_ECAPACITY || attempt == 1 ||
 		    (res.list_used <= cl && res.op_used <= co && res.miss_used <= cm))
-			return rc;
+			return finish(rc);
 		cl = res.list_used + 1;
 		co = res.op_used + 1;
 		cm = res.miss_used + 1;
 	}
 	// hera's malloc'd Candidates, and the reads upper-cased as hera leaves
-	// them, on host threads
+	// them, on host threads: item j of the batch is item j - per * pair0[k]
+	// of call k
 	std::atomic<int> nomem{0};
 	par_for((int64_t)items, [&](int64_t lo, int64_t hi) {
-		for (int64_t i = lo; i < hi; ++i) {
-			out[i] = materialize(&res, (uint64_t)i);
-			if (!out[i])
+		size_t k = std::upper_bound(pair0.begin(), pair0.end(), lo / per) - pair0.begin() - 1;
+		for (int64_t j = lo; j < hi; ++j) {
+			while (j >= per * pair0[k + 1])
+				++k;
+			const DropinArgs &c = *static_cast<DropinArgs *>(batch[k]->user);
+			hera_candidate *x = materialize(&res, (uint64_t)j);
+			c.out[j - per * pair0[k]] = x;
+			if (!x)
 				nomem = 1;
 		}
 	});
 	if (nomem) {
-		hera_gpu_free_candidates(out, (int64_t)items);
-		return fail(ctx, HERA_GPU_ENOMEM, "candidate allocation");
-	}
-	par_for(n, [&](int64_t lo, int64_t hi) {
-		for (int64_t i = lo; i < hi; ++i) {
-			upper_acgt(a[i].seq, a[i].len);
-			if (b)
-				upper_acgt(b[i].seq, b[i].len);
+		for (size_t k = 0; k < nk; ++k) {
+			const DropinArgs &c = *static_cast<DropinArgs *>(batch[k]->user);
+			hera_gpu_free_candidates(c.out, (int64_t)c.n * per);
 		}
-	});
-	return HERA_GPU_OK;
+		finish(fail(ctx, HERA_GPU_ENOMEM, "candidate allocation"));
+		return;
+	}
+	for (size_t k = 0; k < nk; ++k) {
+		const DropinArgs &c = *static_cast<DropinArgs *>(batch[k]->user);
+		par_for(c.n, [&](int64_t lo, int64_t hi) {
+			for (int64_t i = lo; i < hi; ++i) {
+				upper_acgt(c.a[i].seq, c.a[i].len);
+				if (c.b)
+					upper_acgt(c.b[i].seq, c.b[i].len);
+			}
+		});
+	}
+	finish(HERA_GPU_OK);
+}
+
+static int align_dropin(hera_gpu_ctx *ctx, hera_read_inf *a, hera_read_inf *b, int32_t n, int write_bam,
+			hera_candidate **out)
+{
+	if (!ctx || !a || !out || n < 0 || (write_bam != 0 && write_bam != 1))
+		return fail(ctx, HERA_GPU_EINVAL, "bad argument");
+	for (int m = 0; m < (b ? 2 : 1); ++m) {
+		const hera_read_inf *r = m ? b : a;
+		for (int32_t i = 0; i < n; ++i)
+			if (!r[i].seq || r[i].len < 0)
+				return fail(ctx, HERA_GPU_EINVAL, "read without sequence");
+	}
+	if (n == 0)
+		return HERA_GPU_OK;
+	DropinArgs args{a, b, n, write_bam, out};
+	hcomb::Request req;
+	req.kind = (b ? 1 : 0) | (write_bam << 1);
+	req.items = n;
+	req.user = &args;
+	return ctx->dropin.call(req, [ctx](std::vector<hcomb::Request *> &batch) { dropin_batch(ctx, batch); });
 }
 
 extern "C" int hera_gpu_align_pairs(hera_gpu_ctx *ctx, hera_read_inf *r1, hera_read_inf *r2, int32_t n,

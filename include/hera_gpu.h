@@ -244,6 +244,12 @@ int hera_gpu_align_pairs_complete(hera_gpu_ctx *ctx, uint64_t ticket);
  * lower-case a/c/g/t in r1[i].seq and r2[i].seq become upper-case. */
 int hera_gpu_align_pairs(hera_gpu_ctx *ctx, hera_read_inf *r1, hera_read_inf *r2,
 			 int32_t n, int write_bam, hera_candidate **out);
+/* The two drop-in forms (hera_gpu_align_pairs, hera_gpu_align_single) may be
+ * called by several host threads at once on one context, as hera's -t N
+ * workers do: calls that meet are combined into one device batch (the
+ * first caller runs it, the others wait; each gets its own Candidates),
+ * which keeps hera's 1 MB chunks from paying a device call each.  No other
+ * entry point may run on the context while they do. */
 
 /* Drop-in form for align_pool_single (src/hash_align.c:1966-1998). */
 int hera_gpu_align_single(hera_gpu_ctx *ctx, hera_read_inf *reads, int32_t n,

@@ -164,6 +164,70 @@ def test_dropin_candidate_entry(config1, oracle1, gpu_ctx1):
     assert bufs[0].value.upper() == bufs[0].value
 
 
+def _candidates(lib, h, r1, r2, write_bam):
+    """hera_gpu_align_pairs on (r1, r2) as read_inf arrays; the Candidates
+    decoded into the oracle's canonical tuples, then freed."""
+    n = r1.n
+    bufs = []
+    arr1, arr2 = (ReadInf * n)(), (ReadInf * n)()
+    for rs, arr in ((r1, arr1), (r2, arr2)):
+        for i in range(n):
+            b = C.create_string_buffer(rs.read(i))
+            bufs.append(b)
+            arr[i].seq = C.cast(b, C.c_char_p)
+            arr[i].len = int(rs.len[i])
+    out = (C.POINTER(Candidate) * (2 * n))()
+    rc = lib.hera_gpu_align_pairs(h, arr1, arr2, n, write_bam, out)
+    assert rc == 0
+    chars = "MIDNSHP=XB"
+    got = []
+    for i in range(2 * n):
+        c = out[i].contents
+        strands = []
+        for s in range(2):
+            k = c.n[s]
+            g = c.cigar[s].contents
+            cig = "".join(f"{g.count[j]}{chars[g.type[j][0]]}" for j in range(g.n_cigar))
+            miss = bytes(g.miss[j][0] for j in range(g.n_miss))
+            strands.append((k, c.err[s], tuple(c.pos[s][j] for j in range(k)),
+                            tuple(c.p[s][j] for j in range(k)), cig, miss))
+        got.append((c.pair, tuple(strands)))
+    lib.hera_gpu_free_candidates(out, 2 * n)
+    return got
+
+
+@pytest.mark.parametrize("write_bam", [1, 0])
+def test_dropin_calls_from_threads_combine(config1, oracle1, gpu_ctx1, write_bam):
+    """hera's -t N workers call hera_gpu_align_pairs on one context at the
+    same time: the calls are combined into shared device batches and every
+    call still gets exactly its own pairs' Candidates."""
+    import threading
+    ann, tx, _ = config1
+    r1, r2 = workloads.pairs("config1", ann, tx, 4800, seed=29)
+    lib = gpu_ctx1.lib
+    lib.hera_gpu_align_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int, C.c_void_p]
+    lib.hera_gpu_free_candidates.argtypes = [C.c_void_p, C.c_int64]
+    want = oracle1.align_pairs(r1.copy(), r2.copy(), write_bam).canonical()
+    parts = np.array_split(np.arange(r1.n), 12)
+    got, errs = [None] * len(parts), []
+
+    def work(k):
+        try:
+            idx = parts[k]
+            got[k] = _candidates(lib, gpu_ctx1.h, r1.subset(idx), r2.subset(idx), write_bam)
+        except Exception as e:   # reported below
+            errs.append(e)
+    for _ in range(3):
+        th = [threading.Thread(target=work, args=(k,)) for k in range(len(parts))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not errs, errs[0]
+        for k, idx in enumerate(parts):
+            assert got[k] == [want[j] for i in idx for j in (2 * i, 2 * i + 1)], k
+
+
 @pytest.mark.parametrize("shape", [(1, 1), (16, 8), (3, 2)])
 def test_launch_shapes_do_not_change_results(config1, oracle1, shape):
     """The autotuner's choices (build residency, rescue calls per block) only
