@@ -1160,23 +1160,21 @@ def roofline(tm, dpx_instr_s, chunk, read_bytes, max_len):
 
     n_reads = 2 * chunk
     lookups, probes = int(tm["lookups"]), int(tm["probes"])
-    buckets = int(tm.get("bucket_reads", lookups))   # lookups the membership filter passed
     spr = (max_len - 31) // 31 + 1 if max_len >= 31 else 1
     slots = n_reads * 2 * spr
     fixed = read_bytes + 12 * n_reads + 8 * slots
-    useful = fixed + 8 * buckets + 16 * probes
-    sectors = fixed + 32 * buckets + 32 * probes
+    useful = fixed + 8 * lookups + 16 * probes
+    sectors = fixed + 32 * lookups + 32 * probes
     sd_s = float(tm["seed_kernel_ms"]) / 1e3
     seed = {"kernel": "k_seed (seed_probe: hash_get gathers, space 31)", "bound": "hbm",
             "achieved": sectors / sd_s / 1e9 if sd_s > 0 else None, "peak": hbm, "unit": "GB/s",
             "frac": (sectors / sd_s / 1e9) / hbm if sd_s > 0 else None,
             "traffic": traffic.get("k_seed_bytes_per_lookup", 0) * lookups or None,
             "peak_source": src,
-            "sector_efficiency": (8 * buckets + 16 * probes) / (32 * buckets + 32 * probes)
-            if buckets + probes else None,
-            "work": {"lookups": lookups, "bucket_reads": buckets, "probes": probes,
-                     "seed_hits": int(tm["seed_hits"]), "useful_bytes": useful, "sector_bytes": sectors,
-                     "filter_bytes_l2": 32 * lookups, "kernel_ms": float(tm["seed_kernel_ms"])}}
+            "sector_efficiency": (8 * lookups + 16 * probes) / (32 * lookups + 32 * probes)
+            if lookups else None,
+            "work": {"lookups": lookups, "probes": probes, "seed_hits": int(tm["seed_hits"]),
+                     "useful_bytes": useful, "sector_bytes": sectors, "kernel_ms": float(tm["seed_kernel_ms"])}}
 
     rs_s = float(tm["rescue_kernel_ms"]) / 1e3
     sc = int(tm["ssw_cells"])

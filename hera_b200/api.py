@@ -149,7 +149,7 @@ class Timing(C.Structure):
         ("dp_jobs", C.c_uint64), ("dp_calls", C.c_uint64)] + [
         (k, C.c_float) for k in ("seed_kernel_ms", "dp_kernel_ms", "rescue_kernel_ms",
                                  "host_stage_ms", "host_out_ms")] + [
-        (k, C.c_uint64) for k in ("probes", "seed_hits", "sw_cells", "ssw_cells", "wide_items", "bucket_reads")]
+        (k, C.c_uint64) for k in ("probes", "seed_hits", "sw_cells", "ssw_cells", "wide_items")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

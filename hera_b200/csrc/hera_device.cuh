@@ -63,23 +63,7 @@ struct DevIndex {
 	const uint32_t *tlen;    // transcript lengths
 	const uint32_t *tstart;  // transcript start offsets in seq
 	uint32_t n_trans;
-	// membership filter of the table's k-mer ids: bit fhash(id) is set for
-	// every id the table holds, so a clear bit means "not in the table"
-	// without the bucket reads (a set bit can be a collision: the search
-	// then runs as before).  2^fbits bits.
-	const uint32_t *filt;
-	uint32_t fbits;
 };
-
-__host__ __device__ __forceinline__ uint32_t fhash(uint64_t id, uint32_t fbits)
-{
-	return (uint32_t)((id * 0x9E3779B97F4A7C15ull) >> (64 - fbits));
-}
-__device__ __forceinline__ bool filter_has(const DevIndex &ix, uint64_t id)
-{
-	const uint32_t h = fhash(id, ix.fbits);
-	return (__ldg(ix.filt + (h >> 5)) >> (h & 31)) & 1u;
-}
 
 // ascii_table (src/hash_align.c:6-23): A/a 0, C/c 1, G/g 2, T/t 3, else 4
 __device__ __forceinline__ uint8_t code_of(uint8_t c)
@@ -960,8 +944,6 @@ __device__ inline int gap_dp(const DevIndex &ix, uint32_t rstart, const uint8_t 
 // ---------------------------------------------------------------------
 __device__ __forceinline__ uint2 probe(const DevIndex &ix, uint64_t id, uint32_t *n_probes = nullptr)
 {
-	if (!filter_has(ix, id))
-		return make_uint2(0, 0);
 	const uint32_t mod = (uint32_t)(id & HMASK);
 	uint32_t lo = __ldg(ix.boff + mod);
 	uint32_t hi = __ldg(ix.boff + mod + 1);

@@ -104,7 +104,7 @@ __device__ __forceinline__ void pair_flags(const BatchT<K> &b, int i, int f)
 }
 
 // work counters (hera_gpu_timing's probes .. ssw_cells)
-enum { ST_PROBES = 0, ST_SEED_HITS = 1, ST_SW_CELLS = 2, ST_SSW_CELLS = 3, ST_BUCKETS = 4, ST_N = 5 };
+enum { ST_PROBES = 0, ST_SEED_HITS = 1, ST_SW_CELLS = 2, ST_SSW_CELLS = 3, ST_N = 4 };
 
 __device__ __forceinline__ void flag(int *f, int v)
 {
@@ -170,17 +170,6 @@ __global__ void k_codes(const uint8_t *__restrict__ ascii, uint8_t *__restrict__
 	}
 }
 
-// the membership filter: one bit per table id (a grid-stride pass over the
-// bucket records)
-__global__ void k_filter(const uint4 *__restrict__ bk, uint64_t n, uint32_t *__restrict__ filt, uint32_t fbits)
-{
-	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-		const uint4 b = bk[i];
-		const uint32_t h = fhash(((uint64_t)b.y << 32) | b.x, fbits);
-		atomicOr(filt + (h >> 5), 1u << (h & 31));
-	}
-}
-
 // reverse-complement codes of every read, at the read's own offset (one
 // warp per read, lanes over bases: coalesced)
 __global__ void k_rc(const uint8_t *__restrict__ code, const int64_t *__restrict__ off,
@@ -208,40 +197,28 @@ __global__ void __launch_bounds__(256) k_seed(DevIndex ix, const uint8_t *__rest
 					       unsigned long long *__restrict__ stats)
 {
 	const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-	uint32_t np = 0, found = 0, nb = 0;
+	uint32_t np = 0, found = 0;
 	if (t < (int64_t)n_reads * 2) {
 		const int orient = (int)(t & 1);
 		const int ri = (int)(t >> 1);
 		const int L = len[ri];
 		const uint8_t *src = code + off[ri];
 		uint64_t id[S];
-		uint32_t lo[S], hi[S], fw[S];
+		uint32_t lo[S], hi[S];
 		uint2 h[S];
-		// the S ids, then their filter words (one L2-sized bit table), then
-		// the bucket offsets of the ids the filter passes: each step's
-		// loads are issued together
 #pragma unroll
 		for (int j = 0; j < S; ++j) {
 			const int i = j * KMER;
 			h[j] = make_uint2(0, 0);
 			lo[j] = hi[j] = 0;
 			id[j] = 0;
-			fw[j] = 0;
 			if (i + KMER <= L) {
 				// orientation 1: the reverse complement's k-mer at i covers
 				// bytes [L-1-i-30, L-1-i] of the read
 				id[j] = orient == 0 ? kmer_words(src + i, false) : kmer_words(src + (L - KMER - i), true);
-				const uint32_t fh = fhash(id[j], ix.fbits);
-				fw[j] = (__ldg(ix.filt + (fh >> 5)) >> (fh & 31)) & 1u;
-			}
-		}
-#pragma unroll
-		for (int j = 0; j < S; ++j) {
-			if (fw[j]) {
 				const uint32_t mod = (uint32_t)(id[j] & HMASK);
 				lo[j] = __ldg(ix.boff + mod);
 				hi[j] = __ldg(ix.boff + mod + 1);
-				++nb;
 			}
 		}
 		bool more = true;
@@ -274,7 +251,6 @@ __global__ void __launch_bounds__(256) k_seed(DevIndex ix, const uint8_t *__rest
 	}
 	warp_stat(stats + ST_PROBES, np);
 	warp_stat(stats + ST_SEED_HITS, found);
-	warp_stat(stats + ST_BUCKETS, nb);
 }
 
 template <class K>
@@ -902,7 +878,6 @@ struct hera_gpu_ctx {
 	uint2 *d_occ = nullptr;
 	uint8_t *d_seq = nullptr, *d_tcode = nullptr;
 	uint32_t *d_tlen = nullptr, *d_tstart = nullptr;
-	uint32_t *d_filt = nullptr;      // membership filter of the table's ids
 	uint32_t max_batch = 1u << 18;    // pairs per sub-batch
 	uint64_t scratch_bytes = 0;       // accepted for compatibility; unused
 	int batched = 1;
@@ -1074,7 +1049,6 @@ extern "C" void hera_gpu_ctx_destroy(hera_gpu_ctx *ctx)
 	cudaDeviceSynchronize();
 	cudaFree(ctx->d_boff);
 	cudaFree(ctx->d_bk);
-	cudaFree(ctx->d_filt);
 	cudaFree(ctx->d_occ);
 	cudaFree(ctx->d_seq);
 	cudaFree(ctx->d_tcode);
@@ -1217,17 +1191,6 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	    (e = cudaMemcpy(ctx->d_tlen, v->len, n * 4ull, cudaMemcpyHostToDevice)) != cudaSuccess ||
 	    (e = cudaMemcpy(ctx->d_tstart, tstart.data(), n * 4ull, cudaMemcpyHostToDevice)) != cudaSuccess)
 		return bail(fail(ctx, HERA_GPU_ECUDA, "index upload", e));
-	// the membership filter: about two bits a table id (2^20 .. 2^28 bits,
-	// at most 32 MB, so that it stays in L2 beside the lookups' traffic)
-	uint32_t fbits = 20;
-	while (fbits < 28 && (1ull << fbits) < 2 * acc)
-		++fbits;
-	if ((e = cudaMalloc(&ctx->d_filt, (1ull << fbits) / 8)) != cudaSuccess)
-		return bail(fail(ctx, HERA_GPU_ENOMEM, "index allocation", e));
-	if ((e = cudaMemsetAsync(ctx->d_filt, 0, (1ull << fbits) / 8, ctx->stream)) != cudaSuccess)
-		return bail(fail(ctx, HERA_GPU_ECUDA, "index upload", e));
-	if (acc)
-		k_filter<<<1184, 256, 0, ctx->stream>>>(ctx->d_bk, acc, ctx->d_filt, fbits);
 	// transcript codes; the zero padding after the last transcript codes as 4
 	k_codes<<<1184, 256, 0, ctx->stream>>>(ctx->d_seq, ctx->d_tcode, (int64_t)(seq_len + pad));
 	if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
@@ -1240,8 +1203,6 @@ extern "C" int hera_gpu_ctx_create(const hera_gpu_index_view *v, const hera_gpu_
 	ctx->ix.tlen = ctx->d_tlen;
 	ctx->ix.tstart = ctx->d_tstart;
 	ctx->ix.n_trans = n;
-	ctx->ix.filt = ctx->d_filt;
-	ctx->ix.fbits = fbits;
 	*out = ctx;
 	return HERA_GPU_OK;
 }
@@ -1880,7 +1841,6 @@ static int run_batch(hera_gpu_ctx *ctx, Lane &L, const uint8_t *d_seq, const int
 		T.seed_hits += hs[ST_SEED_HITS];
 		T.sw_cells += hs[ST_SW_CELLS];
 		T.ssw_cells += hs[ST_SSW_CELLS];
-		T.bucket_reads += hs[ST_BUCKETS];
 	}
 	if (!batched) {
 		cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]);
@@ -2326,7 +2286,6 @@ static hera_gpu_timing sum_lanes(const std::vector<Lane *> &lanes)
 		t.host_stage_ms += a.host_stage_ms;
 		t.host_out_ms += a.host_out_ms;
 		t.probes += a.probes;
-		t.bucket_reads += a.bucket_reads;
 		t.seed_hits += a.seed_hits;
 		t.sw_cells += a.sw_cells;
 		t.ssw_cells += a.ssw_cells;

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define HERA_GPU_ABI_VERSION 3
+#define HERA_GPU_ABI_VERSION 2
 
 /* status codes */
 #define HERA_GPU_OK 0
@@ -185,9 +185,6 @@ typedef struct hera_gpu_timing {
 				    capacity (more than 256 anchors in one
 				    get_position call, 64 hits, 96 CIGAR ops or
 				    miss chars) */
-	uint64_t bucket_reads;   /* seed lookups that read their bucket's offsets
-				    (the others' ids are absent from the
-				    context's membership filter) */
 } hera_gpu_timing;
 
 /* ---- entry points ------------------------------------------------------ */

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared() if not hasattr(lib, n)]
     assert not missing, missing
     lib.hera_gpu_abi_version.restype = C.c_int
-    assert lib.hera_gpu_abi_version() == 3
+    assert lib.hera_gpu_abi_version() == 2
 
 
 def test_no_device_fails_loudly():
