@@ -105,7 +105,7 @@ def test_server_rejects_bad_sample(config1):
         ctx.close()
 
 
-# ---- failures met on the host: nothing here faults a GPU ------
+# ---- failures met on the host: nothing here faults a GPU ------------------
 
 def test_server_creation_without_room_is_enomem(config1):
     """A reserve above the free device memory leaves no room for a batch
