@@ -90,6 +90,16 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+_T0 = [time.perf_counter()]
+
+
+def phase(name: str) -> None:
+    """Log the wall seconds since the previous phase mark (stderr)."""
+    t = time.perf_counter()
+    log(f"[phase] {name}: {t - _T0[0]:.1f}s")
+    _T0[0] = t
+
+
 class ClockSampler:
     """nvidia-smi SM clock / throttle samples while the timed region runs."""
 
@@ -371,6 +381,7 @@ def main():
     chunks = make_chunks(args.workload, ann, tx, args.chunk, args.distinct, 100 + 1000 * rank)
     dev, max_len = to_device(chunks)
     solo = rank == 0 and world == 1
+    phase("index and chunks")
     orc = None
     if solo and not args.no_parity:
         try:
@@ -379,6 +390,7 @@ def main():
         except Exception as e:
             log(f"oracle unavailable: {e}")
 
+    phase("oracle")
     paths = [p for p in args.paths.split(",") if p]
     plain = parity_plain = None
     if "plain" in paths:
@@ -395,6 +407,7 @@ def main():
         parity = bit_exact(ctx, orc, chunks[batched["last"]], args.chunk, args.parity_pairs, args.write_bam)
         log(f"parity ({main_path}, last step, first {parity['pairs_checked']} pairs): {parity}")
 
+    phase("plain and batched steps, parity")
     # end to end through the public C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -453,6 +466,7 @@ def main():
             except Exception as e:
                 e2e["dropin"] = {"error": str(e)}
 
+    phase("end to end and drop-in")
     cpu = None
     if solo and not args.no_cpu_baseline:
         try:
@@ -460,6 +474,7 @@ def main():
         except Exception as e:   # the checker is optional on a box without it
             log(f"cpu baseline failed: {e}")
 
+    phase("cpu baseline")
     st = batched["stage"]
     tuning = ctx.tuning() if main_path == "batched" else None
     ctx.close()
@@ -468,6 +483,7 @@ def main():
     dpx = api.dpx_peak(local)
     pair_bytes = int(chunks[0][0].len.sum() + chunks[0][1].len.sum())
     roof, roof_seed, roof_rescue = roofline(ktm, dpx, args.chunk, pair_bytes, max_len)
+    phase("kernel pass and classes")
     del dev
 
     legs = {}
@@ -480,8 +496,10 @@ def main():
             except Exception as e:
                 log(f"{name} leg failed: {e}")
                 legs[name] = {"error": str(e)}
+            phase(f"{name} leg")
         del orc, chunks
         ix1 = None
+        phase("config-1 workloads start")
         if not args.no_config_legs or not args.no_serve:
             try:
                 ann1, tx1, ix1 = workloads.build("config1", device=f"cuda:{local}")
@@ -508,6 +526,7 @@ def main():
                 except Exception as e:
                     log(f"{name} leg failed: {e}")
                     legs[name] = {"error": str(e)}
+                phase(f"{name} leg")
 
     if rank == 0:
         per = sorted(batched["per_step_ms"])
