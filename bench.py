@@ -839,9 +839,13 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
         a[:, :raw.shape[1]] = raw
         names.append(a)
     gm = synth.gene_map(ann)
+    phase("bam: names and gene map")
     ctx = api.Context(ix, device=local)
+    phase("bam: context")
     try:
         res = ctx.align_pairs(r1, r2, 0)
+        tmb = ctx.timing()
+        phase(f"bam: traceback alignment ({int(tmb.get('wide_items', 0))} pairs through the wide pass)")
         w = api.BamWriter(ctx, gm)
         try:
             w.pairs(res, r1, r2, q1, q2, names[0], names[1])   # warm
@@ -850,6 +854,7 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
             wall = time.perf_counter() - t0
         finally:
             w.close()
+        phase("bam: device records")
         # the records' BGZF framing on the device (hera_gpu_bgzf, host buffers)
         bgz = None
         try:
@@ -905,8 +910,10 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
         k = min(cpu_sample, n)
         idx = np.arange(k)
         a1, a2 = r1.subset(idx), r2.subset(idx)
+        phase("bam: bgzf (device and host)")
         orc = oracle.Oracle(ix)
         ores = orc.align_pairs(a1, a2, 0)
+        phase("bam: oracle traceback alignment of the sample")
         c1 = np.full(a1.seq.shape[0] + 1, ord("?"), np.uint8)
         c2 = np.full(a2.seq.shape[0] + 1, ord("?"), np.uint8)
         t0 = time.perf_counter()
