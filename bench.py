@@ -731,6 +731,20 @@ def classes_leg(kctx, pairs: int, length) -> dict:
     return out
 
 
+def _read_names(n: int, mate: int) -> np.ndarray:
+    """Rows "r<i, 7+ digits>/<mate>" NUL-padded to 16 bytes (more when i
+    needs over 10 digits), built with digit arithmetic."""
+    w = max(7, len(str(max(n - 1, 0))))
+    a = np.zeros((n, max(16, w + 4)), np.uint8)
+    a[:, 0] = ord("r")
+    i = np.arange(n, dtype=np.int64)
+    for k in range(w):
+        a[:, 1 + k] = 48 + (i // 10 ** (w - 1 - k)) % 10
+    a[:, 1 + w] = ord("/")
+    a[:, 2 + w] = 48 + mate
+    return a
+
+
 def _bgzf_inflate(z: bytes) -> bytes:
     """The data of back-to-back BGZF blocks, block by block (each block's
     size from its BC extra field; each member's CRC-32 and length checked).
@@ -851,14 +865,7 @@ def bam_bench(args, ix, ann, chunk, local, cpu_sample: int = 50_000):
     n = r1.n
     q1 = np.full(r1.seq.shape[0] + 1, ord("?"), np.uint8)
     q2 = np.full(r2.seq.shape[0] + 1, ord("?"), np.uint8)
-    names = []
-    for mate in (1, 2):
-        a = np.zeros((n, 16), np.uint8)
-        digits = np.char.zfill(np.arange(n).astype(str), 7)
-        rows = np.char.add(np.char.add("r", digits), f"/{mate}")
-        raw = np.frombuffer("".join(rows).encode(), np.uint8).reshape(n, -1)
-        a[:, :raw.shape[1]] = raw
-        names.append(a)
+    names = [_read_names(n, mate) for mate in (1, 2)]
     gm = synth.gene_map(ann)
     phase("bam: names and gene map")
     ctx = api.Context(ix, device=local)
